@@ -1,0 +1,275 @@
+// capi.cu -- the extern "C" surface of libpcf.so (include/pcf.h): contexts,
+// grids and the pair-histogram entry point.  Triplet / analytic / batched
+// entry points live in their own files.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "pcf_internal.cuh"
+#include "../../include/pcf_bench.h"
+
+
+extern "C" {
+
+int pcf_version(void) { return 1; }
+
+const char *pcf_status_string(pcf_status s) {
+    switch (s) {
+    case PCF_OK: return "ok";
+    case PCF_ERR_INVALID_ARG: return "invalid argument";
+    case PCF_ERR_CUDA: return "CUDA error";
+    case PCF_ERR_NO_MEMORY: return "out of memory";
+    case PCF_ERR_UNSUPPORTED: return "unsupported configuration";
+    case PCF_ERR_OUT_OF_BOX: return "coordinate outside [0, box)";
+    case PCF_ERR_TIMEOUT: return "device wait timed out";
+    case PCF_ERR_IO: return "I/O error";
+    case PCF_ERR_MISMATCH: return "grids do not share box / partitions";
+    }
+    return "unknown status";
+}
+
+const char *pcf_last_error(const pcf_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+pcf_status pcf_ctx_create(int device, pcf_ctx **out) {
+    if (!out) return PCF_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return PCF_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return PCF_ERR_INVALID_ARG;
+    pcf_ctx *c = new pcf_ctx;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return PCF_ERR_CUDA;
+    }
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    *out = c;
+    return PCF_OK;
+}
+
+pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
+    if (!ctx) return PCF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    cudaEventDestroy(ctx->ev0);
+    cudaEventDestroy(ctx->ev1);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PCF_OK;
+}
+
+void *pcf_ctx_stream(pcf_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int64_t pcf_ctx_launch_count(const pcf_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+static bool is_device_ptr(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+pcf_status pcf_grid_build(pcf_ctx *ctx, const pcf_point *pts, int64_t n, float box,
+                          int partitions, pcf_grid **out) {
+    if (!ctx || !pts || !out || n < 1 || !(box > 0.f) || partitions < 0 || partitions > 320)
+        return PCF_ERR_INVALID_ARG;
+    if (n > (int64_t)INT32_MAX / 2) return PCF_ERR_UNSUPPORTED;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    std::unique_ptr<pcf_grid> g(new pcf_grid);
+    g->n = n;
+    g->box = box;
+    PCF_CU(ctx, g->raw.ensure(sizeof(float4) * (size_t)n));
+    PCF_CU(ctx, cudaMemcpyAsync(g->raw.p, pts, sizeof(float4) * (size_t)n,
+                                is_device_ptr(pts) ? cudaMemcpyDeviceToDevice
+                                                   : cudaMemcpyHostToDevice,
+                                ctx->stream));
+    int P = partitions > 0 ? partitions : choose_partitions(n, box, box / 8.f, PCF_ISO, false, 4);
+    pcf_status s = grid_ensure_cells(ctx, g.get(), P);
+    if (s != PCF_OK) return s;
+    *out = g.release();
+    return PCF_OK;
+}
+
+pcf_status pcf_grid_free(pcf_ctx *ctx, pcf_grid *g) {
+    if (!g) return PCF_ERR_INVALID_ARG;
+    if (ctx) {
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    delete g;
+    return PCF_OK;
+}
+
+pcf_status pcf_grid_info(const pcf_grid *g, int64_t *n, float *box, int *partitions,
+                         int64_t *nonempty_cells, int *unit_weights) {
+    if (!g) return PCF_ERR_INVALID_ARG;
+    if (n) *n = g->n;
+    if (box) *box = g->box;
+    if (partitions) *partitions = g->cells ? g->cells->P : 0;
+    if (nonempty_cells) {
+        int64_t c = 0;
+        if (g->cells) {
+            const auto &h = g->cells->h_start;
+            for (size_t i = 0; i + 1 < h.size(); ++i) c += h[i + 1] > h[i];
+        }
+        *nonempty_cells = c;
+    }
+    if (unit_weights) *unit_weights = g->unit_weights ? 1 : 0;
+    return PCF_OK;
+}
+
+pcf_status pcf_grid_download(pcf_ctx *ctx, const pcf_grid *g, pcf_point *pts_out,
+                             int32_t *cell_start_out) {
+    if (!ctx || !g || !g->cells) return PCF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (pts_out)
+        PCF_CU(ctx, cudaMemcpyAsync(pts_out, g->cells->pts.p, sizeof(float4) * (size_t)g->n,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+    PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (cell_start_out)
+        memcpy(cell_start_out, g->cells->h_start.data(), sizeof(int) * g->cells->h_start.size());
+    return PCF_OK;
+}
+
+int pcf_autotune_partitions(pcf_ctx *ctx, int64_t n, float box, float dmax, int kind,
+                            uint32_t flags) {
+    (void)ctx;
+    return choose_partitions(n, box, dmax, kind, (flags & PCF_BPC) != 0, 0);
+}
+
+}  // extern "C"
+
+// Reference rule of a pair variant (see the oracle's reference_rule):
+//   iso: XX d>0, XY none (2iso_k.cuh:50,107; 2isoBPC_k.cuh:62,338)
+//   ani plain: every component > 0 (2ani_k.cuh:52,121)
+//   ani BPC: XX > 0 and <=, XY <= (2aniBPC_k.cuh:63,401)
+unsigned reference_pair_rule(bool ani, bool bpc, bool cross) {
+    if (!ani) return cross ? 0u : PCF_RULE_EXCL;
+    if (!bpc) return PCF_RULE_EXCL;
+    return cross ? PCF_RULE_LE : (PCF_RULE_LE | PCF_RULE_EXCL);
+}
+
+PairRule make_pair_rule(int bins, float dmax, uint32_t flags, bool ani, bool bpc, bool cross) {
+    PairRule r;
+    double q = (double)bins / (double)dmax;
+    r.ds = (flags & PCF_DS_EXACT) ? q : std::floor(q * 1000000.0) / 1000000.0;
+    float ddf = dmax * dmax;
+    r.dd = (double)ddf;
+    r.bins = bins;
+    if (flags & PCF_RULE_CUSTOM) {
+        r.flags = ((flags & PCF_RULE_EXCL_ZERO) ? PCF_RULE_EXCL : 0u) |
+                  ((flags & PCF_RULE_INCLUSIVE) ? PCF_RULE_LE : 0u);
+    } else {
+        r.flags = reference_pair_rule(ani, bpc, cross);
+    }
+    return r;
+}
+
+// Shared validation + re-gridding of the counting calls.
+pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int kind,
+                         bool bpc, int *P_out) {
+    if (b && b->box != a->box) return PCF_ERR_MISMATCH;
+    const float box = a->box;
+    if (bpc && !(2.0 * (double)dmax < (double)box)) {
+        ctx->last_error = "periodic boundaries need dmax < box/2";
+        return PCF_ERR_UNSUPPORTED;
+    }
+    int64_t n = std::max<int64_t>(a->n, b ? b->n : 0);
+    int P = choose_partitions(n, box, dmax, kind, bpc, 0);
+    if (bpc) {
+        double cell = (double)box / P;
+        int k = (int)std::ceil(((double)dmax + 1e-4 * cell + 8.0 * box * 1.2e-7) / cell);
+        if (2 * k + 2 > P) {
+            ctx->last_error = "dmax too close to box/2 for the periodic stencil";
+            return PCF_ERR_UNSUPPORTED;
+        }
+    }
+    pcf_status s = grid_ensure_cells(ctx, a, P);
+    if (s != PCF_OK) return s;
+    if (b) {
+        s = grid_ensure_cells(ctx, b, P);
+        if (s != PCF_OK) return s;
+    }
+    *P_out = P;
+    return PCF_OK;
+}
+
+// Device scratch for one histogram: [u64 counts nb][f64 sums nb][u64 stats 8][f64 out nb]
+static pcf_status hist_scratch(pcf_ctx *ctx, int nb, unsigned long long **cnt, double **ws,
+                               unsigned long long **stats, double **out) {
+    size_t bytes = (size_t)nb * 8 * 3 + 64;
+    PCF_CU(ctx, ctx->d_hist.ensure(bytes));
+    char *p = ctx->d_hist.as<char>();
+    *cnt = reinterpret_cast<unsigned long long *>(p);
+    *ws = reinterpret_cast<double *>(p + (size_t)nb * 8);
+    *stats = reinterpret_cast<unsigned long long *>(p + (size_t)nb * 16);
+    *out = reinterpret_cast<double *>(p + (size_t)nb * 16 + 64);
+    PCF_CU(ctx, cudaMemsetAsync(p, 0, (size_t)nb * 16 + 64, ctx->stream));
+    return PCF_OK;
+}
+
+extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_,
+                                      const pcf_grid *b_, int bins, float dmax, uint32_t flags,
+                                      double *hist, pcf_stats *stats) {
+    if (!ctx || !a_ || !hist || bins < 1 || !(dmax > 0.f) || (kind != PCF_ISO && kind != PCF_ANI))
+        return PCF_ERR_INVALID_ARG;
+    if (kind == PCF_ANI && (int64_t)bins * bins > (1 << 24)) return PCF_ERR_UNSUPPORTED;
+    cudaSetDevice(ctx->device);
+    pcf_grid *a = const_cast<pcf_grid *>(a_);
+    pcf_grid *b = const_cast<pcf_grid *>(b_);
+    const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0, cross = b != nullptr;
+    int P = 0;
+    pcf_status s = prepare_grids(ctx, a, b, dmax, kind, bpc, &P);
+    if (s != PCF_OK) return s;
+    PairPlan plan;
+    plan_pairs(*a->cells, cross ? b->cells.get() : nullptr, a->box, dmax, ani, bpc, !cross, 128, 0,
+               plan, ctx->sm_count);
+    const int nb = ani ? bins * bins : bins;
+    unsigned long long *d_cnt, *d_stats;
+    double *d_ws, *d_out;
+    s = hist_scratch(ctx, nb, &d_cnt, &d_ws, &d_stats, &d_out);
+    if (s != PCF_OK) return s;
+    PairLaunch pl;
+    pl.ani = ani;
+    pl.bpc = bpc;
+    pl.self = !cross;
+    pl.weighted = !(a->unit_weights && (!cross || b->unit_weights));
+    pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, cross);
+    pl.mult = cross ? 1.0 : 2.0;
+    s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
+                     d_stats);
+    if (s != PCF_OK) return s;
+    const bool dev_out = (flags & PCF_DEVICE_OUT) != 0;
+    s = finalize_hist(ctx, d_cnt, d_ws, pl.weighted, pl.mult, nb, dev_out ? hist : d_out);
+    if (s != PCF_OK) return s;
+    if (!dev_out)
+        PCF_CU(ctx, cudaMemcpyAsync(hist, d_out, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    if (stats || !dev_out) {
+        unsigned long long hs[4] = {0, 0, 0, 0};
+        PCF_CU(ctx, cudaMemcpyAsync(hs, d_stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+        PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        if (stats) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            stats->rechecks = (double)hs[0];
+            stats->candidates = (double)hs[1];
+            stats->pairs = (double)hs[2];
+            stats->kernel_ms = ms;
+            stats->partitions = P;
+            stats->work_items = (int)plan.items.size();
+        }
+    }
+    return PCF_OK;
+}

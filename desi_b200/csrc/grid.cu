@@ -1,0 +1,216 @@
+// grid.cu -- GPU counting sort of a catalog into a uniform cell grid.
+//
+// Replaces the host grid builder of the reference (open_files/make_nodos/add
+// in cuda/create_grid.cuh:35-139 and the flattening in cuda/main.cu:248-329,
+// an O(sum len^2) reallocation per insert followed by a serial copy): three
+// HBM-bound passes over the points --
+//   1. cell id + per-cell count (atomic), with out-of-box / weight checks,
+//   2. exclusive scan of the counts into the dense cell table,
+//   3. scatter of the float4 points into cell order.
+// Cell id = (ix*P + iy)*P + iz with ix = (int)(x / cell), the reference's
+// binning (create_grid.cuh:131-133) clamped to [0, P-1].
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "pcf_internal.cuh"
+
+DevBuf::~DevBuf() {
+    if (p) cudaFree(p);
+}
+
+cudaError_t DevBuf::ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(n, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+}
+
+namespace {
+
+constexpr int kScanItems = 1024;  // per block (256 threads x 4)
+
+__global__ void k_cell_ids(const float4 *__restrict__ pts, int64_t n, int P, float cell, float box,
+                           int *__restrict__ cid, int *__restrict__ rank,
+                           int *__restrict__ counts, int *__restrict__ flags) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pts[i];
+    bool ok = (p.x >= 0.f) && (p.x < box) && (p.y >= 0.f) && (p.y < box) && (p.z >= 0.f) &&
+              (p.z < box);
+    if (!ok) atomicOr(flags, 1);
+    if (p.w != 1.0f) atomicOr(flags, 2);
+    int ix = (int)__fdiv_rn(p.x, cell), iy = (int)__fdiv_rn(p.y, cell),
+        iz = (int)__fdiv_rn(p.z, cell);
+    ix = min(max(ix, 0), P - 1);
+    iy = min(max(iy, 0), P - 1);
+    iz = min(max(iz, 0), P - 1);
+    int c = (ix * P + iy) * P + iz;
+    cid[i] = c;
+    rank[i] = atomicAdd(&counts[c], 1);
+}
+
+// Exclusive scan of one 1024-element chunk per block; the chunk total goes to
+// sums[blockIdx.x].
+__global__ void __launch_bounds__(256) k_scan_chunk(const int *__restrict__ in, int *__restrict__ out,
+                                                   int *__restrict__ sums, int64_t n) {
+    __shared__ int s[256];
+    const int t = threadIdx.x;
+    const int64_t base = (int64_t)blockIdx.x * kScanItems + t * 4;
+    int v0 = base + 0 < n ? in[base + 0] : 0;
+    int v1 = base + 1 < n ? in[base + 1] : 0;
+    int v2 = base + 2 < n ? in[base + 2] : 0;
+    int v3 = base + 3 < n ? in[base + 3] : 0;
+    int tot = v0 + v1 + v2 + v3;
+    s[t] = tot;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {
+        int x = t >= off ? s[t - off] : 0;
+        __syncthreads();
+        s[t] += x;
+        __syncthreads();
+    }
+    int ex = s[t] - tot;
+    if (base + 0 < n) out[base + 0] = ex;
+    if (base + 1 < n) out[base + 1] = ex + v0;
+    if (base + 2 < n) out[base + 2] = ex + v0 + v1;
+    if (base + 3 < n) out[base + 3] = ex + v0 + v1 + v2;
+    if (t == 255) sums[blockIdx.x] = s[255];
+}
+
+__global__ void k_scan_add(int *__restrict__ out, const int *__restrict__ offs, int64_t n) {
+    int64_t i = (int64_t)blockIdx.x * kScanItems + threadIdx.x;
+    int add = offs[blockIdx.x];
+    for (int k = 0; k < 4; ++k, i += 256)
+        if (i < n) out[i] += add;
+}
+
+__global__ void k_scatter(const float4 *__restrict__ pts, int64_t n, const int *__restrict__ cid,
+                          const int *__restrict__ rank, const int *__restrict__ start,
+                          float4 *__restrict__ out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[start[cid[i]] + rank[i]] = pts[i];
+}
+
+// Exclusive scan of n ints, in -> out, using tmp for the per-chunk sums
+// (recursive on the sums).  tmp must hold ceil(n/1024) * 2 + ... ints; the
+// caller passes a buffer of at least n/512 + 64 ints.
+int scan_exclusive(const int *in, int *out, int64_t n, int *tmp, cudaStream_t st) {
+    int64_t nb = (n + kScanItems - 1) / kScanItems;
+    int *sums = tmp;
+    int *sums_ex = tmp + nb;
+    int launches = 1;
+    k_scan_chunk<<<(unsigned)nb, 256, 0, st>>>(in, out, sums, n);
+    if (nb > 1) {
+        launches += scan_exclusive(sums, sums_ex, nb, tmp + 2 * nb, st);
+        k_scan_add<<<(unsigned)nb, 256, 0, st>>>(out, sums_ex, n);
+        ++launches;
+    }
+    return launches;
+}
+
+}  // namespace
+
+pcf_status pcf_fail(pcf_ctx *ctx, cudaError_t e, const char *what) {
+    if (ctx) {
+        ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    }
+    cudaGetLastError();  // clear a sticky-free error so the context stays usable
+    return e == cudaErrorMemoryAllocation ? PCF_ERR_NO_MEMORY : PCF_ERR_CUDA;
+}
+
+pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes) {
+    if (ctx->h_pinned_bytes >= bytes) return PCF_OK;
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    ctx->h_pinned = nullptr;
+    ctx->h_pinned_bytes = 0;
+    size_t want = std::max<size_t>(bytes, 1 << 20);
+    PCF_CU(ctx, cudaMallocHost(&ctx->h_pinned, want));
+    ctx->h_pinned_bytes = want;
+    return PCF_OK;
+}
+
+// Build (or rebuild) the cell structure of g for P cells per side.
+pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
+    if (g->cells && g->cells->P == P) return PCF_OK;
+    if (P < 1 || P > 320) return PCF_ERR_INVALID_ARG;
+    std::unique_ptr<CellGrid> cg(new CellGrid);
+    cg->P = P;
+    cg->cell = g->box / (float)P;
+    const int64_t n = g->n;
+    const int64_t ncell = (int64_t)P * P * P;
+    cudaStream_t st = ctx->stream;
+    PCF_CU(ctx, cg->pts.ensure(sizeof(float4) * (size_t)n));
+    PCF_CU(ctx, cg->cell_start.ensure(sizeof(int) * (size_t)(ncell + 1)));
+    // scratch: cid, rank (n each); counts (ncell + 1); scan tmp.
+    PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(int) * (size_t)n * 2));
+    PCF_CU(ctx, ctx->scratch_b.ensure(sizeof(int) * (size_t)(ncell + 1)));
+    PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(int) * (size_t)((ncell + 1) / 256 + 256)));
+    PCF_CU(ctx, ctx->d_flag.ensure(sizeof(int) * 4));
+    int *cid = ctx->scratch_a.as<int>();
+    int *rank = cid + n;
+    int *counts = ctx->scratch_b.as<int>();
+    int *flags = ctx->d_flag.as<int>();
+    PCF_CU(ctx, cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)(ncell + 1), st));
+    PCF_CU(ctx, cudaMemsetAsync(flags, 0, sizeof(int), st));
+    const int thr = 256;
+    unsigned blocks = (unsigned)((n + thr - 1) / thr);
+    k_cell_ids<<<blocks, thr, 0, st>>>(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank,
+                                       counts, flags);
+    PCF_CU(ctx, cudaGetLastError());
+    ctx->launches += 2 + scan_exclusive(counts, cg->cell_start.as<int>(), ncell + 1,
+                                        ctx->scratch_c.as<int>(), st);
+    PCF_CU(ctx, cudaGetLastError());
+    k_scatter<<<blocks, thr, 0, st>>>(g->raw.as<float4>(), n, cid, rank,
+                                      cg->cell_start.as<int>(), cg->pts.as<float4>());
+    PCF_CU(ctx, cudaGetLastError());
+    cg->h_start.resize((size_t)(ncell + 1));
+    int hflags = 0;
+    PCF_CU(ctx, cudaMemcpyAsync(cg->h_start.data(), cg->cell_start.p, sizeof(int) * (ncell + 1),
+                                cudaMemcpyDeviceToHost, st));
+    PCF_CU(ctx, cudaMemcpyAsync(&hflags, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PCF_CU(ctx, cudaStreamSynchronize(st));
+    if (hflags & 1) {
+        ctx->last_error = "a coordinate lies outside [0, box)";
+        return PCF_ERR_OUT_OF_BOX;
+    }
+    g->unit_weights = (hflags & 2) == 0;
+    g->cells = std::move(cg);
+    return PCF_OK;
+}
+
+// Cells per side for a counting call: cell size about dmax/4 (so the
+// stencil hugs the dmax sphere), coarsened while cells would hold fewer
+// than ~6 points on average, and kept so that a periodic stencil never
+// wraps onto itself (2k+1 <= P).
+int choose_partitions(int64_t n, float box, float dmax, int kind, bool bpc, int refine) {
+    if (refine <= 0) refine = 4;
+    double L = box, R = dmax;
+    int P = (int)std::floor(L / (R / refine));
+    // mean occupancy floor
+    while (P > 1) {
+        double occ = (double)n / ((double)P * P * P);
+        if (occ >= 6.0) break;
+        int nr = refine - 1;
+        if (nr < 1) break;
+        refine = nr;
+        P = (int)std::floor(L / (R / refine));
+    }
+    P = std::max(1, std::min(P, 256));
+    if (bpc) {
+        // need 2k+1 <= P with k = ceil(R / (L/P)) (+1 for the tile span)
+        for (;;) {
+            double cell = L / P;
+            int k = (int)std::ceil((R + 1e-4 * cell + 8.0 * L * 1.2e-7) / cell);
+            if (2 * k + 2 <= P || P >= 256) break;
+            ++P;
+        }
+    }
+    (void)kind;
+    return P;
+}

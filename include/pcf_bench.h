@@ -1,0 +1,28 @@
+/*
+ * pcf_bench.h -- measurement helpers of libpcf.so (no counterpart in the
+ * reference, which publishes no throughput figures): device peak rates used as
+ * roofline denominators, and a count of the library's kernel launches.
+ */
+#ifndef PCF_BENCH_H
+#define PCF_BENCH_H
+
+#include "pcf.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { PCF_MB_FP32_FMA = 0, PCF_MB_SMEM_ATOMIC = 1 };
+
+/* PCF_MB_FP32_FMA: FP32 FMA throughput in TFLOP/s; PCF_MB_SMEM_ATOMIC:
+ * conflict-free shared-memory 32-bit atomicAdd throughput in Gop/s. */
+pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
+
+/* Kernels this context has launched since it was created. */
+int64_t pcf_ctx_launch_count(const pcf_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

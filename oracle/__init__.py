@@ -1,0 +1,222 @@
+"""CPU checkers for the pair / triplet counting library.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` import this package, and only as the
+checker: the shipped library (``desi_b200``) never calls into it.
+
+* :func:`pairs`, :func:`triplets_iso`, :func:`triplets_ani`,
+  :func:`analytic_rr`, :func:`analytic_3iso` wrap ``liboracle.so``, our FP64
+  restatement of the reference's histogram rules (``pcf_oracle.c`` cites the
+  reference file:line each rule follows).
+* :class:`RefEngine` wraps ``_ref/libref_*.so``: the reference's own CPU
+  OpenMP engines (``cpp/2PCF*/{normal,BPC}``) compiled in place by
+  ``oracle/Makefile``; used to pin the restatement and as the timed CPU
+  baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(HERE, "liboracle.so")
+
+FP64, REF32_NOFMA, REF32_FMA_A, REF32_FMA_B, REF32_FMA_C = 0, 1, 2, 3, 4
+RULE_EXCL_ZERO, RULE_INCLUSIVE = 1, 2
+
+_dptr = ctypes.POINTER(ctypes.c_double)
+_fptr = ctypes.c_void_p
+
+
+def build() -> None:
+    """Compile liboracle.so (and _ref/ when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load():
+    if not os.path.exists(_LIB):
+        build()
+    lib = ctypes.CDLL(_LIB)
+    lib.orc_pairs.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
+                              ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                              _fptr, ctypes.c_long, _fptr, ctypes.c_long, ctypes.c_float,
+                              ctypes.c_int, ctypes.c_float, _dptr]
+    lib.orc_triplets_iso.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _fptr,
+                                     ctypes.c_long, _fptr, ctypes.c_long, ctypes.c_float,
+                                     ctypes.c_int, ctypes.c_float, _dptr]
+    lib.orc_triplets_ani.argtypes = [ctypes.c_int, ctypes.c_int, _fptr, ctypes.c_long,
+                                     _fptr, ctypes.c_long, ctypes.c_float, ctypes.c_int,
+                                     ctypes.c_float, _dptr]
+    lib.orc_analytic_rr.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_int, _dptr]
+    lib.orc_analytic_3iso.argtypes = [_fptr, ctypes.c_long, ctypes.c_float, ctypes.c_int,
+                                      ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      _dptr, _dptr, _dptr, _dptr]
+    lib.orc_analytic_bin.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_float, ctypes.c_int, ctypes.c_double, _dptr,
+                                     _dptr, _dptr]
+    lib.orc_ds.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_int]
+    lib.orc_ds.restype = ctypes.c_double
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _pts(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    assert a.ndim == 2 and a.shape[1] == 4
+    return a
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dptr)
+
+
+def ds(bins: int, dmax: float, exact: bool = False) -> float:
+    return lib().orc_ds(bins, dmax, 1 if exact else 0)
+
+
+def pairs(A, B=None, *, box: float, bins: int, dmax: float, ani: bool = False,
+          bpc: bool = False, rule: int | None = None, ds_exact: bool = False,
+          ds_value: float = 0.0, prec: int = FP64) -> np.ndarray:
+    """Pair histogram.  ``B is None`` -> XX over A (ordered pairs), else XY.
+
+    ``rule`` defaults to the reference CUDA rule for the variant (see
+    :func:`reference_rule`).
+    """
+    A = _pts(A)
+    self_ = B is None
+    Bp = A if self_ else _pts(B)
+    if rule is None:
+        rule = reference_rule(ani=ani, bpc=bpc, cross=not self_)
+    nb = bins * bins if ani else bins
+    out = np.zeros(nb, np.float64)
+    rc = lib().orc_pairs(int(ani), int(bpc), int(self_), rule, int(ds_exact), float(ds_value),
+                         prec, _p(A), len(A), _p(Bp), len(Bp), box, bins, dmax, _d(out))
+    assert rc == 0
+    return out.reshape(bins, bins) if ani else out
+
+
+def reference_rule(*, ani: bool, bpc: bool, cross: bool) -> int:
+    """Rule flags of the reference CUDA kernel for one pair variant.
+
+    2iso  XX: d>0            (2iso_k.cuh:50)      XY: none   (2iso_k.cuh:107)
+    2isoB XX: d>0            (2isoBPC_k.cuh:62)   XY: none   (2isoBPC_k.cuh:338)
+    2ani  XX,XY: every component >0 (2ani_k.cuh:52,121)
+    2aniB XX: >0 and <=      (2aniBPC_k.cuh:63)   XY: <= only (2aniBPC_k.cuh:401)
+    """
+    if not ani:
+        return 0 if cross else RULE_EXCL_ZERO
+    if not bpc:
+        return RULE_EXCL_ZERO
+    return RULE_INCLUSIVE if cross else (RULE_INCLUSIVE | RULE_EXCL_ZERO)
+
+
+def triplets_iso(X, Y=None, *, box: float, bins: int, dmax: float, bpc: bool = False,
+                 prec: int = FP64):
+    X = _pts(X)
+    mixed = Y is not None
+    Yp = _pts(Y) if mixed else X
+    out = np.zeros(bins ** 3, np.float64)
+    rc = lib().orc_triplets_iso(int(bpc), int(mixed), prec, _p(X), len(X), _p(Yp), len(Yp),
+                                box, bins, dmax, _d(out))
+    assert rc == 0
+    return out.reshape(bins, bins, bins)
+
+
+def triplets_ani(X, Y=None, *, box: float, bins: int, dmax: float, bpc: bool = False):
+    X = _pts(X)
+    mixed = Y is not None
+    Yp = _pts(Y) if mixed else X
+    out = np.zeros(bins ** 5, np.float64)
+    rc = lib().orc_triplets_ani(int(bpc), int(mixed), _p(X), len(X), _p(Yp), len(Yp), box,
+                                bins, dmax, _d(out))
+    assert rc == 0
+    return out.reshape((bins,) * 5)
+
+
+def analytic_rr(bins: int, n: int, box: float, dmax: float, wrap: bool = True):
+    out = np.zeros(bins, np.float64)
+    lib().orc_analytic_rr(bins, n, box, dmax, int(wrap), _d(out))
+    return out
+
+
+def analytic_3iso(D, *, box: float, bins: int, dmax: float, ptt: int = 100,
+                  bn_ref: int = 200, wrap: bool = True):
+    """Returns (DDR, RRR, ff_av, ff_av_ref); DRR is written as a copy of DDR."""
+    D = _pts(D)
+    ddr = np.zeros(bins ** 3, np.float64)
+    rrr = np.zeros(bins ** 3, np.float64)
+    ff = np.zeros(bins, np.float64)
+    ffr = np.zeros(bins * bn_ref, np.float64)
+    rc = lib().orc_analytic_3iso(_p(D), len(D), box, bins, dmax, ptt, bn_ref, int(wrap),
+                                 _d(ddr), _d(rrr), _d(ff), _d(ffr))
+    assert rc == 0
+    s = (bins, bins, bins)
+    return ddr.reshape(s), rrr.reshape(s), ff, ffr
+
+
+def analytic_bin(i, j, k, *, bins, dmax, bn_ref, alpha_ref, ff_ref):
+    ffr = np.ascontiguousarray(ff_ref, np.float64)
+    r = ctypes.c_double()
+    d = ctypes.c_double()
+    v = lib().orc_analytic_bin(i, j, k, bins, dmax, bn_ref, alpha_ref, _d(ffr),
+                               ctypes.byref(r), ctypes.byref(d))
+    return v, r.value, d.value
+
+
+class RefEngine:
+    """The reference's CPU NODE2P engine for one variant, compiled in place.
+
+    kind: '2iso', '2iso_bpc', '2ani', '2ani_bpc'.
+    """
+
+    def __init__(self, kind: str):
+        path = os.path.join(HERE, "_ref", f"libref_{kind}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.kind = kind
+        self.lib = ctypes.CDLL(path)
+        self.lib.ref_xx.argtypes = [_fptr, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_int, _dptr]
+        self.lib.ref_xy.argtypes = [_fptr, _fptr, ctypes.c_int, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_int, _dptr]
+        self.is2d = bool(self.lib.ref_is_2d())
+
+    def set_threads(self, t: int) -> None:
+        self.lib.ref_set_threads(int(t))
+
+    def xx(self, A, *, box, size_node, bins, dmax):
+        A = _pts(A)
+        out = np.zeros(bins * bins if self.is2d else bins, np.float64)
+        self.lib.ref_xx(_p(A), len(A), box, size_node, dmax, bins, _d(out))
+        return out.reshape(bins, bins) if self.is2d else out
+
+    def xy(self, A, B, *, box, size_node, bins, dmax):
+        A, B = _pts(A), _pts(B)
+        assert len(A) == len(B), "the reference engines take catalogs of equal size"
+        out = np.zeros(bins * bins if self.is2d else bins, np.float64)
+        self.lib.ref_xy(_p(A), _p(B), len(A), box, size_node, dmax, bins, _d(out))
+        return out.reshape(bins, bins) if self.is2d else out
+
+
+def available_ref_engines():
+    d = os.path.join(HERE, "_ref")
+    if not os.path.isdir(d):
+        return []
+    return sorted(f[len("libref_"):-3] for f in os.listdir(d) if f.startswith("libref_"))

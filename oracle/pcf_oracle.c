@@ -1,0 +1,601 @@
+/*
+ * pcf_oracle.c -- CPU FP64 oracle for grid-node pair / triplet counting.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library links or calls
+ * this file; only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg load it, and only as the checker.
+ *
+ * It restates, with brute-force loops, the histogram rules of the reference
+ * CUDA kernels (3PCFGPU, paths relative to the reference root):
+ *   cuda/kernels/2iso_k.cuh:8-120        XX2iso / XY2iso
+ *   cuda/kernels/2isoBPC_k.cuh:8-565     XX2iso_BPC / XY2iso_BPC / RR analytic
+ *   cuda/kernels/2ani_k.cuh:7-135        XX2ani / XY2ani
+ *   cuda/kernels/2aniBPC_k.cuh:8-682     XX2ani_BPC / XY2ani_BPC
+ *   cuda/kernels/3iso_k.cuh:8-179        XXX3iso / XXY3iso
+ *   cuda/kernels/3isoBPC_k.cuh:8-188     count123 / count123_mixed (image rule)
+ *   cuda/kernels/3isoBPC_k.cuh:1694-2119 DD2iso_forBPC, make_ff_av(_ref),
+ *                                        make_histo_analitic
+ *   cuda/kernels/3ani_k.cuh:8-209        XXX3ani / XXY3ani
+ *   cuda/pcf2isoBPC.cuh:199-202, cuda/pcf3isoBPC.cuh:233-247 (constants)
+ *
+ * Canonical (FP64) rule, shared with the CUDA library:
+ *   separation  dx = (double)x2 - (double)x1   (exact); with periodic
+ *               boundaries the minimum image (|dx| > L/2 -> dx -+ L, exact).
+ *   d2          = (dx*dx + dy*dy) + dz*dz, each op rounded, no FMA.
+ *   in range    d2 < (double)(float)(dmax*dmax)   [or <= for 2ani BPC],
+ *               and d2 > 0 where the reference tests d > 0.
+ *   bin         = (int)(sqrt(d2) * ds), dropped when >= bins,
+ *               ds = floor(bins/dmax * 1e6)/1e6 (or bins/dmax, 2iso BPC).
+ * The reference computes d2 in FP32; ORC_REF32_* precisions reproduce that
+ * (with the FMA contraction pattern named) so that the reference's own
+ * outputs can be matched bit for bit, which is how this oracle is pinned.
+ *
+ * Built with -ffp-contract=off (see Makefile) so no FMA is formed silently.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+typedef struct { float x, y, z, w; } opt;
+
+enum {
+    ORC_FP64 = 0,          /* canonical FP64 rule                                */
+    ORC_REF32_NOFMA = 1,   /* FP32 d2, ((dx*dx + dy*dy) + dz*dz), no contraction */
+    ORC_REF32_FMA_A = 2,   /* FP32 d2 = fma(dz,dz, fma(dy,dy, dx*dx))            */
+    ORC_REF32_FMA_B = 3,   /* FP32 d2 = fma(dz,dz, fma(dx,dx, dy*dy))            */
+    ORC_REF32_FMA_C = 4    /* FP32 d2 = fma(dx,dx, fma(dy,dy, dz*dz))            */
+};
+#define RULE_EXCL_ZERO 1u  /* require d2 > 0 (every component for 2ani)          */
+#define RULE_INCLUSIVE 2u  /* d2 <= dd_max instead of d2 < dd_max                */
+
+double orc_ds(int bins, float dmax, int exact)
+{
+    /* 2iso_k.cuh:37 (floored to 1e-6) and 2isoBPC_k.cuh:36 (exact). */
+    double q = (double)bins / (double)dmax;
+    return exact ? q : floor(q * 1000000.0) / 1000000.0;
+}
+
+static inline double sep64(float a, float b, int bpc, double L)
+{
+    double d = (double)b - (double)a;
+    if (bpc) {
+        if (d > 0.5 * L) d -= L;
+        else if (d < -0.5 * L) d += L;
+    }
+    return d;
+}
+
+static inline float d2_ref32(float fx, float fy, float fz, int prec)
+{
+    switch (prec) {
+    case ORC_REF32_FMA_A: return fmaf(fz, fz, fmaf(fy, fy, fx * fx));
+    case ORC_REF32_FMA_B: return fmaf(fz, fz, fmaf(fx, fx, fy * fy));
+    case ORC_REF32_FMA_C: return fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+    default: {
+        float a = fx * fx;
+        float b = fy * fy;
+        float c = fz * fz;
+        float s = a + b;
+        return s + c;
+    }
+    }
+}
+
+/* Squared separation components of a pair: returns the three per-axis
+ * squares folded the way the rule needs (iso: total; ani: z and perp). */
+static inline void pair_d2(const opt *p, const opt *q, int bpc, double L, int prec,
+                           double *d2_iso, double *d2_z, double *d2_perp)
+{
+    if (prec == ORC_FP64 || bpc) {
+        double dx = sep64(p->x, q->x, bpc, L);
+        double dy = sep64(p->y, q->y, bpc, L);
+        double dz = sep64(p->z, q->z, bpc, L);
+        double xx = dx * dx, yy = dy * dy, zz = dz * dz;
+        double s = xx + yy;
+        *d2_iso = s + zz;
+        *d2_z = zz;
+        *d2_perp = s;
+    } else {
+        float fx = q->x - p->x, fy = q->y - p->y, fz = q->z - p->z;
+        *d2_iso = (double)d2_ref32(fx, fy, fz, prec);
+        *d2_z = (double)(fz * fz);
+        float a = fx * fx, b = fy * fy;
+        *d2_perp = (double)(a + b);
+    }
+}
+
+static inline int in_range(double d2, double ddmax, unsigned rule)
+{
+    if (rule & RULE_EXCL_ZERO) { if (!(d2 > 0.0)) return 0; }
+    if (rule & RULE_INCLUSIVE) return d2 <= ddmax;
+    return d2 < ddmax;
+}
+
+static inline int bin_of(double d2, double ds, int bins)
+{
+    int b = (int)(sqrt(d2) * ds);
+    return (b >= 0 && b < bins) ? b : -1;
+}
+
+/* Histogram slot of one pair under the rule, or -1. */
+static inline int pair_slot(const opt *p, const opt *q, int ani, int bpc, double L, int prec,
+                            unsigned rule, double ddmax, double ds, int bins)
+{
+    double d2, dz2, dp2;
+    pair_d2(p, q, bpc, L, prec, &d2, &dz2, &dp2);
+    if (!ani) {
+        if (!in_range(d2, ddmax, rule)) return -1;
+        return bin_of(d2, ds, bins);
+    }
+    if (!in_range(dz2, ddmax, rule) || !in_range(dp2, ddmax, rule)) return -1;
+    int bz = bin_of(dz2, ds, bins), bp = bin_of(dp2, ds, bins);
+    if (bz < 0 || bp < 0) return -1;
+    return bz * bins + bp;
+}
+
+/*
+ * Pair histogram.  self != 0: XX over catalog A, ordered pairs i != j
+ * (each unordered pair adds 2*w_i*w_j, as the reference launches both
+ * orders); self == 0: XY, every A x B pair once.
+ * ds <= 0 selects orc_ds(bins, dmax, ds_exact); ds > 0 is used as given.
+ * out has bins (iso) or bins*bins (ani) doubles and is overwritten.
+ */
+int orc_pairs(int ani, int bpc, int self, unsigned rule, int ds_exact, double ds_in, int prec,
+              const opt *A, long nA, const opt *B, long nB, float L, int bins, float dmax,
+              double *out)
+{
+    const int nb = ani ? bins * bins : bins;
+    const double ds = ds_in > 0 ? ds_in : orc_ds(bins, dmax, ds_exact);
+    const float ddf = dmax * dmax;
+    const double ddmax = (double)ddf;
+    const double Ld = (double)L;
+    if (self) { B = A; nB = nA; }
+    memset(out, 0, sizeof(double) * (size_t)nb);
+    int nt = omp_get_max_threads();
+    double *priv = (double *)calloc((size_t)nt * nb, sizeof(double));
+    if (!priv) return -1;
+#pragma omp parallel
+    {
+        double *h = priv + (size_t)omp_get_thread_num() * nb;
+#pragma omp for schedule(dynamic, 16)
+        for (long i = 0; i < nA; ++i) {
+            const opt *p = &A[i];
+            long j0 = self ? i + 1 : 0;
+            for (long j = j0; j < nB; ++j) {
+                int s = pair_slot(p, &B[j], ani, bpc, Ld, prec, rule, ddmax, ds, bins);
+                if (s >= 0) {
+                    double w = (double)p->w * (double)B[j].w;
+                    h[s] += self ? 2.0 * w : w;
+                }
+            }
+        }
+    }
+    for (int t = 0; t < nt; ++t)
+        for (int k = 0; k < nb; ++k) out[k] += priv[(size_t)t * nb + k];
+    free(priv);
+    return 0;
+}
+
+/* ----------------------------------------------------------------------- */
+/* Triplets (isotropic): ordered triples, bin = b(d12)*bins^2 + b(d23)*bins */
+/* + b(d31) (3iso_k.cuh:71-77), weight w1*w2*w3.  With periodic boundaries  */
+/* the consistent embedding of count123 (3isoBPC_k.cuh:56-75): points 2, 3  */
+/* take their minimum image relative to point 1 and d23 = |img3 - img2|.    */
+/* ----------------------------------------------------------------------- */
+
+typedef struct { int idx; int bin; double v[3]; } nbr_t;
+
+/* FP32 side as the plain reference kernels compute it (3iso_k.cuh:57,66,69),
+ * with the contraction pattern selected by prec. */
+static int side_bin32(const opt *p, const opt *q, int prec, double ddmax, unsigned rule,
+                      double ds, int bins)
+{
+    float fx = q->x - p->x, fy = q->y - p->y, fz = q->z - p->z;
+    double d2 = (double)d2_ref32(fx, fy, fz, prec);
+    if (!in_range(d2, ddmax, rule)) return -1;
+    return bin_of(d2, ds, bins);
+}
+
+static int side_bin(const double v[3], double ddmax, unsigned rule, double ds, int bins)
+{
+    double xx = v[0] * v[0], yy = v[1] * v[1], zz = v[2] * v[2];
+    double d2 = (xx + yy) + zz;
+    if (!in_range(d2, ddmax, rule)) return -1;
+    return bin_of(d2, ds, bins);
+}
+
+/* Neighbours of point p among Q[j0..nQ) with a valid side bin. */
+static nbr_t *neighbours(const opt *p, const opt *Q, long j0, long nQ, int bpc, double L,
+                         unsigned rule, double ddmax, double ds, int bins, int prec, long *cnt)
+{
+    long cap = 64, n = 0;
+    nbr_t *a = (nbr_t *)malloc(sizeof(nbr_t) * cap);
+    for (long j = j0; j < nQ; ++j) {
+        double v[3] = {sep64(p->x, Q[j].x, bpc, L), sep64(p->y, Q[j].y, bpc, L),
+                       sep64(p->z, Q[j].z, bpc, L)};
+        int b = prec ? side_bin32(p, &Q[j], prec, ddmax, rule, ds, bins)
+                     : side_bin(v, ddmax, rule, ds, bins);
+        if (b < 0) continue;
+        if (n == cap) { cap *= 2; a = (nbr_t *)realloc(a, sizeof(nbr_t) * cap); }
+        a[n].idx = (int)j; a[n].bin = b;
+        a[n].v[0] = v[0]; a[n].v[1] = v[1]; a[n].v[2] = v[2];
+        ++n;
+    }
+    *cnt = n;
+    return a;
+}
+
+/*
+ * mixed == 0: XXX over X (all three sides: 0 < d2 < dd_max).
+ * mixed != 0: XXY with points 1,2 from X and point 3 from Y; side 12 needs
+ *   0 < d2, sides 23 and 31 need 0 < d2 only with periodic boundaries
+ *   (3iso_k.cuh:158,160 vs 3isoBPC_k.cuh:165,170).
+ * out: bins^3 doubles, overwritten.
+ */
+int orc_triplets_iso(int bpc, int mixed, int prec, const opt *X, long nX, const opt *Y, long nY,
+                     float L, int bins, float dmax, double *out)
+{
+    if (bpc) prec = ORC_FP64; /* FP32 emulation covers the plain kernels only */
+    const long nb = (long)bins * bins * bins;
+    const double ds = orc_ds(bins, dmax, 0);
+    const float ddf = dmax * dmax;
+    const double ddmax = (double)ddf;
+    const double Ld = (double)L;
+    const unsigned rXX = RULE_EXCL_ZERO;
+    const unsigned rXY = bpc ? RULE_EXCL_ZERO : 0u;
+    const long b2 = (long)bins * bins;
+    memset(out, 0, sizeof(double) * (size_t)nb);
+    int nt = omp_get_max_threads();
+    double *priv = (double *)calloc((size_t)nt * nb, sizeof(double));
+    if (!priv) return -1;
+#pragma omp parallel
+    {
+        double *h = priv + (size_t)omp_get_thread_num() * nb;
+#pragma omp for schedule(dynamic, 1)
+        for (long i = 0; i < nX; ++i) {
+            const opt *p = &X[i];
+            long n2, n3;
+            nbr_t *N2 = neighbours(p, X, i + 1, nX, bpc, Ld, rXX, ddmax, ds, bins, prec, &n2);
+            if (!mixed) {
+                for (long a = 0; a < n2; ++a) {
+                    const nbr_t *q = &N2[a];
+                    double wij = (double)p->w * (double)X[q->idx].w;
+                    for (long b = a + 1; b < n2; ++b) {
+                        const nbr_t *r = &N2[b];
+                        double v[3] = {r->v[0] - q->v[0], r->v[1] - q->v[1], r->v[2] - q->v[2]};
+                        int bjk = prec ? side_bin32(&X[q->idx], &X[r->idx], prec, ddmax, rXX, ds, bins)
+                                       : side_bin(v, ddmax, rXX, ds, bins);
+                        if (bjk < 0) continue;
+                        double w = wij * (double)X[r->idx].w;
+                        long A = q->bin, Bb = bjk, C = r->bin; /* (ij, jk, ki) */
+                        h[A * b2 + Bb * bins + C] += w;
+                        h[Bb * b2 + C * bins + A] += w;
+                        h[C * b2 + A * bins + Bb] += w;
+                        h[C * b2 + Bb * bins + A] += w;
+                        h[Bb * b2 + A * bins + C] += w;
+                        h[A * b2 + C * bins + Bb] += w;
+                    }
+                }
+            } else {
+                nbr_t *N3 = neighbours(p, Y, 0, nY, bpc, Ld, rXY, ddmax, ds, bins, prec, &n3);
+                for (long a = 0; a < n2; ++a) {
+                    const nbr_t *q = &N2[a];
+                    double wij = (double)p->w * (double)X[q->idx].w;
+                    for (long b = 0; b < n3; ++b) {
+                        const nbr_t *r = &N3[b];
+                        double v[3] = {r->v[0] - q->v[0], r->v[1] - q->v[1], r->v[2] - q->v[2]};
+                        int bjk = prec ? side_bin32(&X[q->idx], &Y[r->idx], prec, ddmax, rXY, ds, bins)
+                                       : side_bin(v, ddmax, rXY, ds, bins);
+                        if (bjk < 0) continue;
+                        double w = wij * (double)Y[r->idx].w;
+                        long A = q->bin, Bb = bjk, C = r->bin;
+                        h[A * b2 + Bb * bins + C] += w;
+                        h[A * b2 + C * bins + Bb] += w;
+                    }
+                }
+                free(N3);
+            }
+            free(N2);
+        }
+    }
+    for (int t = 0; t < nt; ++t)
+        for (long k = 0; k < nb; ++k) out[k] += priv[(size_t)t * nb + k];
+    free(priv);
+    return 0;
+}
+
+/* ----------------------------------------------------------------------- */
+/* Triplets (anisotropic, bins^5): a=b(d12), b=b(d31), c=b(d23),            */
+/* t=(int)((1+dz12/d12)*bins/2), p=(int)((1+dz31/d31)*bins/2)               */
+/* (3ani_k.cuh:75-91), each dropped when >= bins.  Ordered triples are      */
+/* enumerated directly (no symmetry: the angles are anchored at point 1).   */
+/* ----------------------------------------------------------------------- */
+static inline int ani_angle_bin(double dz, double d, int bins)
+{
+    double c = 1.0 + dz / d;
+    double th = (double)((float)bins / 2.0f);
+    int t = (int)(c * th);
+    return (t >= 0 && t < bins) ? t : -1;
+}
+
+int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, long nY, float L,
+                     int bins, float dmax, double *out)
+{
+    const long B = bins;
+    const long nb = B * B * B * B * B;
+    const double ds = orc_ds(bins, dmax, 0);
+    const float ddf = dmax * dmax;
+    const double ddmax = (double)ddf;
+    const double Ld = (double)L;
+    const unsigned rXX = RULE_EXCL_ZERO;
+    const unsigned rXY = bpc ? RULE_EXCL_ZERO : 0u;
+    if (!mixed) { Y = X; nY = nX; }
+    memset(out, 0, sizeof(double) * (size_t)nb);
+    int nt = omp_get_max_threads();
+    double *priv = (double *)calloc((size_t)nt * nb, sizeof(double));
+    if (!priv) return -1;
+#pragma omp parallel
+    {
+        double *h = priv + (size_t)omp_get_thread_num() * nb;
+#pragma omp for schedule(dynamic, 1)
+        for (long i = 0; i < nX; ++i) {
+            const opt *p = &X[i];
+            long n2, n3;
+            nbr_t *N2 = neighbours(p, X, 0, nX, bpc, Ld, rXX, ddmax, ds, bins, 0, &n2);
+            nbr_t *N3 = neighbours(p, Y, 0, nY, bpc, Ld, mixed ? rXY : rXX, ddmax, ds, bins, 0, &n3);
+            for (long a = 0; a < n2; ++a) {
+                const nbr_t *q = &N2[a];
+                if (q->idx == i) continue;
+                double d12 = sqrt((q->v[0] * q->v[0] + q->v[1] * q->v[1]) + q->v[2] * q->v[2]);
+                int t = ani_angle_bin(q->v[2], d12, bins);
+                if (t < 0) continue;
+                double wij = (double)p->w * (double)X[q->idx].w;
+                for (long b = 0; b < n3; ++b) {
+                    const nbr_t *r = &N3[b];
+                    if (!mixed && (r->idx == i || r->idx == q->idx)) continue;
+                    double v[3] = {r->v[0] - q->v[0], r->v[1] - q->v[1], r->v[2] - q->v[2]};
+                    int c = side_bin(v, ddmax, mixed ? rXY : rXX, ds, bins);
+                    if (c < 0) continue;
+                    double d31 = sqrt((r->v[0] * r->v[0] + r->v[1] * r->v[1]) + r->v[2] * r->v[2]);
+                    int pp = ani_angle_bin(r->v[2], d31, bins);
+                    if (pp < 0) continue;
+                    double w = wij * (double)Y[r->idx].w;
+                    long slot = (((q->bin * B + r->bin) * B + c) * B + t) * B + pp;
+                    h[slot] += w;
+                }
+            }
+            free(N2);
+            free(N3);
+        }
+    }
+    for (int t = 0; t < nt; ++t)
+        for (long k = 0; k < nb; ++k) out[k] += priv[(size_t)t * nb + k];
+    free(priv);
+    return 0;
+}
+
+/* ----------------------------------------------------------------------- */
+/* Analytic periodic-box histograms.                                         */
+/* ----------------------------------------------------------------------- */
+
+/* Coefficient 3k^2+3k+1 as the reference computes it in 32-bit int
+ * (2isoBPC_k.cuh:564), i.e. wrapping modulo 2^32 once k exceeds 26754;
+ * wrap == 0 evaluates it in 64-bit instead. */
+static inline double shell_coef(long k, int wrap)
+{
+    if (wrap) {
+        uint32_t u = 3u * (uint32_t)k * (uint32_t)k + 3u * (uint32_t)k + 1u;
+        return (double)(int32_t)u;
+    }
+    return (double)(3 * k * k + 3 * k + 1);
+}
+
+/* alpha of RR2iso_BPC_analytic (pcf2isoBPC.cuh:199-202):
+ * dr = dmax/bins in FP32, beta = (np*np)/L^3 in FP32, alpha = 8 dr^3 acos(0) beta / 3. */
+static double rr_alpha(long np, float L, float dmax, long bins)
+{
+    float drf = dmax / (float)bins;
+    double dr = (double)drf;
+    float L3 = L * L * L;
+    float betaf = (float)(np * np) / L3;
+    double beta = (double)betaf;
+    return 8 * dr * dr * dr * acos(0.0) * beta / 3;
+}
+
+void orc_analytic_rr(int bins, long np, float L, float dmax, int wrap, double *out)
+{
+    double alpha = rr_alpha(np, L, dmax, bins);
+    for (long k = 0; k < bins; ++k) out[k] = alpha * shell_coef(k, wrap);
+}
+
+/* Does every corner of the cube [r1, r1+h]x[r2, r2+h]x[r3, r3+h] satisfy the
+ * triangle inequality (3isoBPC_k.cuh:2040-2052 / 2078-2090)? */
+static int all_corners(double ri, double rj, double rk, double h)
+{
+    int v = 0;
+    for (int a = 0; a < 2; ++a) {
+        double r1 = ri + (double)a * h;
+        for (int b = 0; b < 2; ++b) {
+            double r2 = rj + (double)b * h;
+            for (int c = 0; c < 2; ++c) {
+                double r3 = rk + (double)c * h;
+                if (r1 + r2 >= r3 && r1 + r3 >= r2 && r2 + r3 >= r1) ++v;
+            }
+        }
+    }
+    return v;
+}
+
+/*
+ * Analytic 3iso with periodic boundaries (pcf3isoBPC.cuh:177-347 with the
+ * kernels of 3isoBPC_k.cuh:1694-2119).  D: the data catalog (n points),
+ * ptt / bn_ref: the reference's sub-binning (100 / 200 in the reference).
+ * Produces DDR (written twice by the reference, as DDR and DRR) and RRR,
+ * bins^3 each.  Uses the canonical FP64 pair rule for the fine DD.
+ * wrap: reproduce the reference's 32-bit coefficient overflow.
+ * fine_dd / fine_dd_ref (optional, may be NULL): receive the fine DD histograms.
+ */
+int orc_analytic_3iso(const opt *D, long n, float L, int bins, float dmax, int ptt, int bn_ref,
+                      int wrap, double *DDR, double *RRR, double *ff_av_out, double *ff_ref_out)
+{
+    const long bn_ff = (long)ptt * bins;
+    const long bn_ff_ref = (long)ptt * bn_ref * bins;
+    double *dd_ff = (double *)calloc(bn_ff, sizeof(double));
+    double *dd_ref = (double *)calloc(bn_ff_ref, sizeof(double));
+    double *rr_ff = (double *)calloc(bn_ff, sizeof(double));
+    double *rr_ref = (double *)calloc(bn_ff_ref, sizeof(double));
+    double *ff_av = (double *)calloc(bins, sizeof(double));
+    double *ff_ref = (double *)calloc((long)bn_ref * bins, sizeof(double));
+    if (!dd_ff || !dd_ref || !rr_ff || !rr_ref || !ff_av || !ff_ref) return -1;
+
+    /* constants, pcf3isoBPC.cuh:233-247 */
+    float L3 = L * L * L;
+    float betaf = (float)(n * n) / L3;
+    double beta = (double)betaf;
+    float dr_ff_f = dmax / (float)bn_ff;
+    double dr_ff = (double)dr_ff_f;
+    double alpha_ff = 8 * dr_ff * dr_ff * dr_ff * acos(0.0) * beta / 3;
+    float dr_ffr_f = dmax / (float)bn_ff_ref;
+    double dr_ffr = (double)dr_ffr_f;
+    double alpha_ffr = 8 * dr_ffr * dr_ffr * dr_ffr * acos(0.0) * beta / 3;
+    double dr = dmax / (double)bins;
+    double dr_ref = dr / bn_ref;
+    float Vf = L * L;
+    double V = (double)Vf;
+    double beta_3D = n / V;
+    double gama = 8 * (4 * acos(0.0) * acos(0.0)) * (n * beta_3D * beta_3D);
+    gama /= V;
+    double alpha_ref = gama * dr_ref * dr_ref * dr_ref;
+    double alpha = gama * dr * dr * dr;
+
+    /* fine DD (DD2iso_forBPC): ordered pairs, periodic, 0 < d2 < dd_max, ds in FP32 */
+    float dsf_ref = (float)bn_ff_ref / dmax;
+    float dsf = (float)bn_ff / dmax;
+    orc_pairs(0, 1, 1, RULE_EXCL_ZERO, 0, (double)dsf_ref, ORC_FP64, D, n, 0, 0, L, (int)bn_ff_ref,
+              dmax, dd_ref);
+    orc_pairs(0, 1, 1, RULE_EXCL_ZERO, 0, (double)dsf, ORC_FP64, D, n, 0, 0, L, (int)bn_ff, dmax,
+              dd_ff);
+    for (long k = 0; k < bn_ff; ++k) rr_ff[k] = alpha_ff * shell_coef(k, wrap);
+    for (long k = 0; k < bn_ff_ref; ++k) rr_ref[k] = alpha_ffr * shell_coef(k, wrap);
+
+    /* make_ff_av (3isoBPC_k.cuh:1984) */
+    for (int i = 0; i < bins; ++i) {
+        for (int j = 0; j < ptt; ++j) {
+            long i_ = (long)i * ptt;
+            float idm = (float)i * dmax;
+            double ri = idm / (double)bins;
+            double rj = (j + 0.5) * dmax / (double)bn_ff;
+            double v = (ri + rj) * ((dd_ff[i_ + j] / rr_ff[i_ + j]) - 1) / (double)ptt;
+            ff_av[i] += v;
+        }
+    }
+    /* make_ff_av_ref (3isoBPC_k.cuh:2001) */
+    for (int i = 0; i < bins; ++i) {
+        for (int j = 0; j < bn_ref; ++j) {
+            for (int k = 0; k < ptt; ++k) {
+                double drr = dmax / (double)bins;
+                double drr_ref = drr / bn_ref;
+                double dr_ptt_ref = dmax / (double)((long)ptt * bn_ref * bins);
+                double ri = i * drr, rj = j * drr_ref, rk = (k + 0.5) * dr_ptt_ref;
+                long i_ = (long)i * bn_ref, j_ = (long)j * ptt;
+                long s = i_ * ptt + j_ + k;
+                double f = (ri + rj + rk) * ((dd_ref[s] / rr_ref[s]) - 1) / (double)ptt;
+                ff_ref[i_ + j] += f;
+            }
+        }
+    }
+    /* make_histo_analitic (3isoBPC_k.cuh:2021) */
+    const long b2 = (long)bins * bins;
+    memset(DDR, 0, sizeof(double) * b2 * bins);
+    memset(RRR, 0, sizeof(double) * b2 * bins);
+#pragma omp parallel for collapse(3) schedule(dynamic, 1)
+    for (int i = 0; i < bins; ++i)
+        for (int j = 0; j < bins; ++j)
+            for (int k = 0; k < bins; ++k) {
+                double dr2 = dr * 0.5;
+                double ri = (double)i * dr, rj = (double)j * dr, rk = (double)k * dr;
+                long i_ = (long)i * bn_ref, j_ = (long)j * bn_ref, k_ = (long)k * bn_ref;
+                int v_in = all_corners(ri, rj, rk, dr);
+                long slot = i * b2 + (long)j * bins + k;
+                if (v_in == 8) {
+                    double s = alpha * (ri + dr2) * (rj + dr2) * (rk + dr2);
+                    RRR[slot] = s;
+                    double f = 1;
+                    f += ff_av[i] / (3 * (ri + dr2));
+                    f += ff_av[j] / (3 * (rj + dr2));
+                    f += ff_av[k] / (3 * (rk + dr2));
+                    f *= s;
+                    DDR[slot] += f;
+                } else if (v_in > 0) {
+                    int con = 0;
+                    double h = dr_ref, h2 = dr_ref * 0.5;
+                    double S_av = 0.0, f_av = 0.0;
+                    for (int u = 0; u < bn_ref; ++u) {
+                        double ru = ri + ((double)u * h);
+                        for (int v = 0; v < bn_ref; ++v) {
+                            double rv = rj + ((double)v * h);
+                            for (int w = 0; w < bn_ref; ++w) {
+                                double rw = rk + ((double)w * h);
+                                if (all_corners(ru, rv, rw, h) != 8) continue;
+                                double c = (ru + h2) * (rv + h2) * (rw + h2);
+                                S_av += c;
+                                double f = 1;
+                                f += ff_ref[i_ + u] / (3 * (ru + h2));
+                                f += ff_ref[j_ + v] / (3 * (rv + h2));
+                                f += ff_ref[k_ + w] / (3 * (rw + h2));
+                                f *= c;
+                                f_av += f;
+                                con = 1;
+                            }
+                        }
+                    }
+                    if (con) {
+                        RRR[slot] += S_av * alpha_ref;
+                        DDR[slot] += f_av * alpha_ref;
+                    }
+                }
+            }
+    if (ff_av_out) memcpy(ff_av_out, ff_av, sizeof(double) * bins);
+    if (ff_ref_out) memcpy(ff_ref_out, ff_ref, sizeof(double) * bn_ref * bins);
+    free(dd_ff); free(dd_ref); free(rr_ff); free(rr_ref); free(ff_av); free(ff_ref);
+    return 0;
+}
+
+/* One partially covered coarse bin of make_histo_analitic, evaluated alone
+ * (lets tests check single bins at the reference's full 200^3 sub-grid). */
+int orc_analytic_bin(int i, int j, int k, int bins, float dmax, int bn_ref, double alpha_ref,
+                     const double *ff_ref, double *rrr, double *ddr)
+{
+    double dr = dmax / (double)bins;
+    double dr_ref = dr / bn_ref, h2 = dr_ref * 0.5;
+    double ri = (double)i * dr, rj = (double)j * dr, rk = (double)k * dr;
+    long i_ = (long)i * bn_ref, j_ = (long)j * bn_ref, k_ = (long)k * bn_ref;
+    double S_av = 0, f_av = 0;
+    int con = 0;
+    for (int u = 0; u < bn_ref; ++u) {
+        double ru = ri + ((double)u * dr_ref);
+        for (int v = 0; v < bn_ref; ++v) {
+            double rv = rj + ((double)v * dr_ref);
+            for (int w = 0; w < bn_ref; ++w) {
+                double rw = rk + ((double)w * dr_ref);
+                if (all_corners(ru, rv, rw, dr_ref) != 8) continue;
+                double c = (ru + h2) * (rv + h2) * (rw + h2);
+                S_av += c;
+                double f = 1;
+                f += ff_ref[i_ + u] / (3 * (ru + h2));
+                f += ff_ref[j_ + v] / (3 * (rv + h2));
+                f += ff_ref[k_ + w] / (3 * (rw + h2));
+                f *= c;
+                f_av += f;
+                con = 1;
+            }
+        }
+    }
+    *rrr = con ? S_av * alpha_ref : 0.0;
+    *ddr = con ? f_av * alpha_ref : 0.0;
+    return all_corners(ri, rj, rk, dr);
+}
+
+int orc_version(void) { return 1; }

@@ -1,0 +1,140 @@
+"""GPU parity of the pair histograms against the FP64 oracle.
+
+Unit weights: bit-exact.  Weighted: |gpu - oracle| <= 1e-12 * |oracle|
+(FP64 sums in a different order).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from desi_b200 import catalog
+
+pytestmark = pytest.mark.gpu
+RTOL_W = 1e-12
+
+
+def _cmp(got, want, weighted):
+    if weighted:
+        np.testing.assert_allclose(got, want, rtol=RTOL_W, atol=0)
+    else:
+        assert np.array_equal(got, want), (np.abs(got - want).max(), np.argwhere(got != want)[:5])
+
+
+CASES = [
+    # (name, n, box, bins, dmax, clustered, weights)
+    ("uniform", 3000, 250.0, 30, 80.0, False, "unit"),
+    ("clustered", 3000, 250.0, 30, 80.0, True, "unit"),
+    ("weighted", 2500, 250.0, 30, 80.0, True, "uniform"),
+    ("odd", 2000, 173.0, 17, 41.3, False, "unit"),
+]
+
+
+@pytest.mark.parametrize("name,n,box,bins,dmax,clu,w", CASES)
+@pytest.mark.parametrize("ani", [False, True])
+@pytest.mark.parametrize("bpc", [False, True])
+def test_pairs_xx_xy(ctx, name, n, box, bins, dmax, clu, w, ani, bpc):
+    gen = catalog.neyman_scott if clu else catalog.uniform
+    D = gen(n, box, seed=11, weights=w)
+    R = catalog.uniform(n + 123, box, seed=12, weights=w)
+    gd, gr = ctx.grid(D, box), ctx.grid(R, box)
+    weighted = w != "unit"
+    for (a, b, A, B) in ((gd, None, D, None), (gr, None, R, None), (gd, gr, D, R)):
+        got = ctx.count_pairs(a, b, bins=bins, dmax=dmax, ani=ani, bpc=bpc)
+        want = oracle.pairs(A, B, box=box, bins=bins, dmax=dmax, ani=ani, bpc=bpc)
+        _cmp(got, want, weighted)
+
+
+def test_reference_catalogs_1k(ctx, catalogs):
+    D, R = catalogs["data_1K"], catalogs["rand0_1K"]
+    box = 251.0
+    gd, gr = ctx.grid(D, box), ctx.grid(R, box)
+    for ani in (False, True):
+        for bpc in (False, True):
+            for a, b, A, B in ((gd, None, D, None), (gd, gr, D, R)):
+                got = ctx.count_pairs(a, b, bins=30, dmax=80.0, ani=ani, bpc=bpc)
+                want = oracle.pairs(A, B, box=box, bins=30, dmax=80.0, ani=ani, bpc=bpc)
+                _cmp(got, want, False)
+
+
+def test_lattice_exact_edges(ctx):
+    """Integer lattice: many separations sit exactly on bin edges and on dmax."""
+    g = np.stack(np.meshgrid(np.arange(12), np.arange(12), np.arange(12), indexing="ij"), -1)
+    pts = np.concatenate([g.reshape(-1, 3).astype(np.float32) * 2.5 + 0.25,
+                          np.ones((12 ** 3, 1), np.float32)], 1)
+    box = 30.0
+    gd = ctx.grid(pts, box)
+    for ani in (False, True):
+        for bpc, dmax in ((False, 10.0), (True, 10.0), (False, 12.5)):
+            for bins in (10, 20, 4):
+                got = ctx.count_pairs(gd, None, bins=bins, dmax=dmax, ani=ani, bpc=bpc)
+                want = oracle.pairs(pts, None, box=box, bins=bins, dmax=dmax, ani=ani, bpc=bpc)
+                _cmp(got, want, False)
+
+
+def test_duplicates_and_zero_separation(ctx):
+    rng = np.random.default_rng(3)
+    base = catalog.uniform(400, 100.0, seed=4)
+    pts = np.concatenate([base, base[:50], base[:10]])  # exact duplicates
+    pts = pts[rng.permutation(len(pts))]
+    other = np.concatenate([base[100:160], catalog.uniform(200, 100.0, seed=5)])
+    box = 100.0
+    a, b = ctx.grid(pts, box), ctx.grid(other, box)
+    for ani in (False, True):
+        for bpc in (False, True):
+            got = ctx.count_pairs(a, None, bins=25, dmax=30.0, ani=ani, bpc=bpc)
+            want = oracle.pairs(pts, None, box=box, bins=25, dmax=30.0, ani=ani, bpc=bpc)
+            _cmp(got, want, False)
+            got = ctx.count_pairs(a, b, bins=25, dmax=30.0, ani=ani, bpc=bpc)
+            want = oracle.pairs(pts, other, box=box, bins=25, dmax=30.0, ani=ani, bpc=bpc)
+            _cmp(got, want, False)
+
+
+def test_ds_exact_and_wide_bins(ctx):
+    D = catalog.uniform(1500, 200.0, seed=7)
+    g = ctx.grid(D, 200.0)
+    from desi_b200.api import PCF_DS_EXACT
+    got = ctx.count_pairs(g, None, bins=40, dmax=60.0, bpc=True, flags=PCF_DS_EXACT)
+    want = oracle.pairs(D, None, box=200.0, bins=40, dmax=60.0, bpc=True, ds_exact=True)
+    _cmp(got, want, False)
+    got = ctx.count_pairs(g, None, bins=700, dmax=60.0)
+    want = oracle.pairs(D, None, box=200.0, bins=700, dmax=60.0)
+    _cmp(got, want, False)
+
+
+def test_tiny_catalogs(ctx):
+    one = np.array([[1.0, 2.0, 3.0, 1.0]], np.float32)
+    two = np.array([[1.0, 2.0, 3.0, 1.0], [4.0, 2.0, 3.0, 1.0]], np.float32)
+    g1, g2 = ctx.grid(one, 10.0), ctx.grid(two, 10.0)
+    assert ctx.count_pairs(g1, None, bins=5, dmax=4.0).sum() == 0
+    h = ctx.count_pairs(g2, None, bins=5, dmax=4.0)
+    assert h[3] == 2 and h.sum() == 2
+    h = ctx.count_pairs(g1, g2, bins=5, dmax=4.0)
+    assert h[0] == 1 and h[3] == 1
+
+
+def test_out_of_box_rejected(ctx):
+    from desi_b200.api import PcfError
+    bad = np.array([[1.0, 2.0, 10.0, 1.0]], np.float32)
+    with pytest.raises(PcfError):
+        ctx.grid(bad, 10.0)
+
+
+def test_bpc_dmax_limit(ctx):
+    from desi_b200.api import PcfError
+    g = ctx.grid(catalog.uniform(100, 10.0, seed=1), 10.0)
+    with pytest.raises(PcfError):
+        ctx.count_pairs(g, None, bins=5, dmax=5.0, bpc=True)
+
+
+def test_grid_is_a_permutation_in_cell_order(ctx):
+    D = catalog.neyman_scott(5000, 250.0, seed=9)
+    g = ctx.grid(D, 250.0, partitions=17)
+    pts, cs = g.download()
+    assert cs[0] == 0 and cs[-1] == len(D) and np.all(np.diff(cs) >= 0)
+    key = lambda a: np.lexsort(a[:, :3].T)
+    assert np.array_equal(pts[key(pts)], D[key(D)])
+    P = 17
+    cell = np.float32(250.0) / np.float32(P)
+    idx = np.minimum((pts[:, :3] / cell).astype(np.int64), P - 1)
+    cid = (idx[:, 0] * P + idx[:, 1]) * P + idx[:, 2]
+    assert np.all(np.diff(cid) >= 0)
