@@ -233,7 +233,7 @@ extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_
     pcf_status s = prepare_grids(ctx, a, b, dmax, kind, bpc, &P);
     if (s != PCF_OK) return s;
     PairPlan plan;
-    plan_pairs(*a->cells, cross ? b->cells.get() : nullptr, a->box, dmax, ani, bpc, !cross, 128, 0,
+    plan_pairs(*a->cells, cross ? b->cells.get() : nullptr, a->box, dmax, ani, bpc, !cross, 32, 0,
                plan, ctx->sm_count);
     const int nb = ani ? bins * bins : bins;
     unsigned long long *d_cnt, *d_stats;
@@ -259,7 +259,17 @@ extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_
     if (stats || !dev_out) {
         unsigned long long hs[4] = {0, 0, 0, 0};
         PCF_CU(ctx, cudaMemcpyAsync(hs, d_stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+        std::vector<unsigned long long> cnt;
+        if (stats && !pl.weighted) {  // unit weights: pairs = sum of the counts
+            cnt.resize(nb);
+            PCF_CU(ctx, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(unsigned long long) * nb,
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+        }
         PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        if (!cnt.empty()) {
+            hs[2] = 0;
+            for (auto c : cnt) hs[2] += c;
+        }
         if (stats) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);

@@ -11,6 +11,7 @@
 // binning (create_grid.cuh:131-133) clamped to [0, P-1].
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "pcf_internal.cuh"
@@ -91,10 +92,16 @@ __global__ void k_scan_add(int *__restrict__ out, const int *__restrict__ offs, 
 
 __global__ void k_scatter(const float4 *__restrict__ pts, int64_t n, const int *__restrict__ cid,
                           const int *__restrict__ rank, const int *__restrict__ start,
-                          float4 *__restrict__ out) {
+                          float4 *__restrict__ out, float *__restrict__ soa, size_t plane) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[start[cid[i]] + rank[i]] = pts[i];
+    const float4 p = pts[i];
+    const int64_t d = start[cid[i]] + rank[i];
+    out[d] = p;
+    soa[d] = p.x;
+    soa[plane + d] = p.y;
+    soa[2 * plane + d] = p.z;
+    soa[3 * plane + d] = p.w;
 }
 
 // Exclusive scan of n ints, in -> out, using tmp for the per-chunk sums
@@ -146,6 +153,9 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     const int64_t ncell = (int64_t)P * P * P;
     cudaStream_t st = ctx->stream;
     PCF_CU(ctx, cg->pts.ensure(sizeof(float4) * (size_t)n));
+    cg->plane = ((size_t)n + kSoaPad + 3) & ~(size_t)3;
+    PCF_CU(ctx, cg->soa.ensure(sizeof(float) * cg->plane * 4));
+    PCF_CU(ctx, cudaMemsetAsync(cg->soa.p, 0, sizeof(float) * cg->plane * 4, ctx->stream));
     PCF_CU(ctx, cg->cell_start.ensure(sizeof(int) * (size_t)(ncell + 1)));
     // scratch: cid, rank (n each); counts (ncell + 1); scan tmp.
     PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(int) * (size_t)n * 2));
@@ -167,7 +177,8 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
                                         ctx->scratch_c.as<int>(), st);
     PCF_CU(ctx, cudaGetLastError());
     k_scatter<<<blocks, thr, 0, st>>>(g->raw.as<float4>(), n, cid, rank,
-                                      cg->cell_start.as<int>(), cg->pts.as<float4>());
+                                      cg->cell_start.as<int>(), cg->pts.as<float4>(),
+                                      cg->soa.as<float>(), cg->plane);
     PCF_CU(ctx, cudaGetLastError());
     cg->h_start.resize((size_t)(ncell + 1));
     int hflags = 0;
@@ -189,7 +200,11 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
 // than ~6 points on average, and kept so that a periodic stencil never
 // wraps onto itself (2k+1 <= P).
 int choose_partitions(int64_t n, float box, float dmax, int kind, bool bpc, int refine) {
-    if (refine <= 0) refine = 4;
+    if (refine <= 0) {
+        const char *e = getenv("PCF_REFINE");  // experiment / autotuner override
+        refine = e ? atoi(e) : 4;
+        if (refine < 1 || refine > 16) refine = 4;
+    }
     double L = box, R = dmax;
     int P = (int)std::floor(L / (R / refine));
     // mean occupancy floor

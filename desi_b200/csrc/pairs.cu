@@ -27,227 +27,345 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 
 #include "pcf_internal.cuh"
 
 namespace {
 
-constexpr int kThreads = 128;  // 4 warps
+constexpr int kThreads = 128;  // 4 independent warps per CTA
 constexpr int kWarps = kThreads / 32;
-constexpr float kMagic = 256.0f;  // r + 256 -> mantissa = round(r * 2^15)
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kMagic = 256.0f;  // r + 256 -> low mantissa bits = round(r * 2^15)
 constexpr int kFracBits = 15;
 constexpr unsigned kFracMask = (1u << kFracBits) - 1u;
+
+enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2 };
 
 // Fast-path cut constants for one range type (0: unshifted, 1: image-shifted).
 struct FastCuts {
     float dsf;        // (float)ds
+    float ds2;        // dsf * dsf
     float lo[2];      // d2 below lo (and >= tiny) is safely inside dmax
     float hi[2];      // d2 at or above hi is safely outside dmax
     unsigned w[2];    // edge window in 2^-15 units of r
     float tiny;
-    int fast_bins;    // bins the fixed-point path may produce (<= 255)
 };
 
-struct PairStats {
-    unsigned long long rechecks;
-    unsigned long long candidates;
+struct PairArgs {
+    const float *hx, *hy, *hz, *hw;  // home catalog planes (cell order)
+    const float *cx, *cy, *cz, *cw;  // candidate catalog planes
+    const int *cstart;
+    const TileDesc *tiles;
+    const RowDesc *rows;
+    const WorkItem *items;
+    int n_items;
+    int *counter;
+    int P;
+    float box;
+    int bpc;
+    PairRule rule;
+    FastCuts fc;
+    unsigned long long *g_count;
+    double *g_wsum;
+    unsigned long long *g_stats;
 };
 
-// Shared-memory histogram accumulators.
-template <bool W>
-struct Acc;
-template <>
-struct Acc<false> {
-    typedef unsigned int T;
-    __device__ static void add(T *h, int slot, float, float) { atomicAdd(h + slot, 1u); }
-};
-template <>
-struct Acc<true> {
-    typedef double T;
-    __device__ static void add(T *h, int slot, float wa, float wb) {
-        atomicAdd(h + slot, (double)wa * (double)wb);
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Fixed-point readout of r in [0, 256): q = round(r * 2^15).  The bin
+// (q >> 15) is exact unless r is within w/2^15 of an integer.
+__device__ __forceinline__ bool fix_safe(unsigned q, unsigned w) {
+    return ((q + w) & kFracMask) >= 2u * w;
+}
+
+// Predicated shared / global reductions (one instruction, no branch).
+__device__ __forceinline__ void red_s_u32(const void *p, unsigned v, bool pred) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q red.shared.add.u32 [%0], %1;\n\t}"
+                 :: "r"(a), "r"(v), "r"((unsigned)pred) : "memory");
+}
+__device__ __forceinline__ void red_s_f64(const void *p, double v, bool pred) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q red.shared.add.f64 [%0], %1;\n\t}"
+                 :: "r"(a), "d"(v), "r"((unsigned)pred) : "memory");
+}
+
+// Histogram sinks.  H_LANE: one u32 / f64 column per lane (iso, few bins),
+// no contention; H_WARP: one copy per warp with shared atomics; H_GLOBAL:
+// global atomics (very wide histograms).  add() is predicated on `pred`.
+template <bool WEIGHTED, int HM>
+struct Sink {
+    void *base;  // shared: this warp's region (lane column folded in); global: g_count / g_wsum
+    __device__ __forceinline__ void add(int slot, float wa, float wb, bool pred) const {
+        if (HM == H_LANE) {
+            if (WEIGHTED) {  // lane-private column: plain add of 0 or w_a*w_b
+                double *h = static_cast<double *>(base) + slot * 32;
+                *h += pred ? (double)wa * (double)wb : 0.0;
+            } else {
+                red_s_u32(static_cast<unsigned *>(base) + slot * 32, 1u, pred);
+            }
+        } else if (HM == H_WARP) {
+            if (WEIGHTED) red_s_f64(static_cast<double *>(base) + slot, (double)wa * (double)wb, pred);
+            else red_s_u32(static_cast<unsigned *>(base) + slot, 1u, pred);
+        } else if (pred) {
+            if (WEIGHTED) atomicAdd(static_cast<double *>(base) + slot, (double)wa * (double)wb);
+            else atomicAdd(static_cast<unsigned long long *>(base) + slot, 1ull);
+        }
     }
 };
 
-// Slow path: canonical FP64 decision for one pair.
+struct Home {
+    float x, y, z, w;  // original coordinates
+};
+
+struct Seg {
+    float sx, sy, sz;  // image shift of the candidates
+    float lo, hi;
+    unsigned w;
+};
+
+// Canonical FP64 decision for one pair (rare path): histogram slot or -1.
 template <bool ANI>
-__device__ __noinline__ int slow_slot(float hx, float hy, float hz, float4 c, float sx, float sy,
-                                      float sz, PairRule rule) {
+__device__ __noinline__ int slow_slot(float hx, float hy, float hz, float cx, float cy, float cz,
+                                      float sx, float sy, float sz, PairRule rule) {
     double dx, dy, dz;
-    exact_sep(hx, hy, hz, c.x, c.y, c.z, sx, sy, sz, dx, dy, dz);
+    exact_sep(hx, hy, hz, cx, cy, cz, sx, sy, sz, dx, dy, dz);
     return exact_slot<ANI>(dx, dy, dz, rule);
 }
 
-// Fixed-point bin of r (>= 0, < 256) with the edge test.  Returns the bin,
-// or -1 when r lies within the window of an edge (caller rechecks).
-__device__ __forceinline__ int fixed_bin(float r, unsigned w) {
-    float a = r + kMagic;
-    unsigned q = __float_as_uint(a) & 0x7FFFFFu;  // round(r * 2^15)
-    unsigned f = (q - w) & kFracMask;              // frac - w (mod 1)
-    bool edge = f >= (kFracMask + 1u - 2u * w);
-    return edge ? -1 : (int)(q >> kFracBits);
+template <bool ANI, bool WEIGHTED, int HM>
+__device__ __forceinline__ void slow_pair(const PairArgs &A, const Home &h, const Seg &sg, int j,
+                                          const Sink<WEIGHTED, HM> &sink, unsigned &n_pairs) {
+    const int slot = slow_slot<ANI>(h.x, h.y, h.z, __ldg(A.cx + j), __ldg(A.cy + j),
+                                    __ldg(A.cz + j), sg.sx, sg.sy, sg.sz, A.rule);
+    if (slot >= 0) {
+        sink.add(slot, h.w, WEIGHTED ? __ldg(A.cw + j) : 1.f, true);
+        if (WEIGHTED) ++n_pairs;
+    }
 }
 
-template <bool ANI, bool WEIGHTED, bool GLOBAL_HIST>
-__global__ void __launch_bounds__(kThreads) k_pairs(
-    const float4 *__restrict__ hpts, const float4 *__restrict__ cpts,
-    const int *__restrict__ cstart, const TileDesc *__restrict__ tiles,
-    const RowDesc *__restrict__ rows, const WorkItem *__restrict__ items, int n_items,
-    int *__restrict__ counter, int P, float box, int bpc, PairRule rule, FastCuts fc,
-    unsigned long long *__restrict__ g_count, double *__restrict__ g_wsum,
-    unsigned long long *__restrict__ g_stats) {
-    typedef typename Acc<WEIGHTED>::T HT;
+// One candidate pair of elements (packed): distance test, fixed-point bin,
+// predicated accumulate.  Pairs within the edge window of a bin, near dmax,
+// or at zero separation (frac(r) = 0 fails the window test) go to the FP64
+// rule, behind one warp-uniform branch.
+template <bool ANI, bool WEIGHTED, int HM>
+__device__ __forceinline__ void take2(const PairArgs &A, float2 DX, float2 DY, float2 DZ, bool v0,
+                                      bool v1, int j, float2 Wt, const Home &h, const Seg &sg,
+                                      const Sink<WEIGHTED, HM> &sink, unsigned &n_pairs,
+                                      unsigned &n_rechk) {
+    const FastCuts &fc = A.fc;
+    const float2 DS2 = make_float2(fc.ds2, fc.ds2);
+    const float2 MG = make_float2(kMagic, kMagic);
+    const int B1 = A.rule.bins - 1;
+    bool f0 = false, f1 = false;
+    float m0, m1;  // largest squared component, for the recheck test
+    if (!ANI) {
+        float2 D2 = __fmul2_rn(DX, DX);
+        D2 = __ffma2_rn(DY, DY, D2);
+        D2 = __ffma2_rn(DZ, DZ, D2);
+        m0 = D2.x;
+        m1 = D2.y;
+        if (HM != H_GLOBAL) {
+            const float2 U = __fmul2_rn(D2, DS2);
+            const float2 Q = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)), MG);
+            const unsigned q0 = __float_as_uint(Q.x) & 0x7FFFFFu;
+            const unsigned q1 = __float_as_uint(Q.y) & 0x7FFFFFu;
+            f0 = v0 && (D2.x < sg.lo) && fix_safe(q0, sg.w);
+            f1 = v1 && (D2.y < sg.lo) && fix_safe(q1, sg.w);
+            sink.add(min((int)(q0 >> kFracBits), B1), h.w, Wt.x, f0);
+            sink.add(min((int)(q1 >> kFracBits), B1), h.w, Wt.y, f1);
+        }
+    } else {
+        const float2 ZZ = __fmul2_rn(DZ, DZ);
+        const float2 PP = __ffma2_rn(DY, DY, __fmul2_rn(DX, DX));
+        m0 = fmaxf(ZZ.x, PP.x);
+        m1 = fmaxf(ZZ.y, PP.y);
+        if (HM != H_GLOBAL) {
+            const float2 RZ = __fmul2_rn(DZ, make_float2(fc.dsf, fc.dsf));
+            const float2 U = __fmul2_rn(PP, DS2);
+            const float2 QZ = __fadd2_rn(make_float2(fabsf(RZ.x), fabsf(RZ.y)), MG);
+            const float2 QP = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)), MG);
+            const unsigned z0 = __float_as_uint(QZ.x) & 0x7FFFFFu, z1 = __float_as_uint(QZ.y) & 0x7FFFFFu;
+            const unsigned p0 = __float_as_uint(QP.x) & 0x7FFFFFu, p1 = __float_as_uint(QP.y) & 0x7FFFFFu;
+            f0 = v0 && (m0 < sg.lo) && fix_safe(z0, sg.w) && fix_safe(p0, sg.w);
+            f1 = v1 && (m1 < sg.lo) && fix_safe(z1, sg.w) && fix_safe(p1, sg.w);
+            const int B = A.rule.bins;
+            sink.add(min((int)(z0 >> kFracBits), B1) * B + min((int)(p0 >> kFracBits), B1), h.w, Wt.x, f0);
+            sink.add(min((int)(z1 >> kFracBits), B1) * B + min((int)(p1 >> kFracBits), B1), h.w, Wt.y, f1);
+        }
+    }
+    if (WEIGHTED) n_pairs += (unsigned)f0 + (unsigned)f1;
+    const bool r0 = !f0 && v0 && m0 < sg.hi;
+    const bool r1 = !f1 && v1 && m1 < sg.hi;
+    // Lanes of different candidate streams leave the stream loop after
+    // different trip counts, so vote only among the lanes that are here.
+    if (__any_sync(__activemask(), r0 || r1)) {
+        if (r0) {
+            ++n_rechk;
+            slow_pair<ANI, WEIGHTED, HM>(A, h, sg, j, sink, n_pairs);
+        }
+        if (r1) {
+            ++n_rechk;
+            slow_pair<ANI, WEIGHTED, HM>(A, h, sg, j + 1, sink, n_pairs);
+        }
+    }
+}
+
+#ifndef PCF_PAIR_MINB
+#define PCF_PAIR_MINB 6
+#endif
+template <bool ANI, bool WEIGHTED, int HM>
+__global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArgs A) {
+    typedef typename std::conditional<WEIGHTED, double, unsigned>::type HT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     HT *hist_all = reinterpret_cast<HT *>(smem_raw);
-    __shared__ int s_item;
-
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nb = ANI ? rule.bins * rule.bins : rule.bins;
-    if (!GLOBAL_HIST) {
-        for (int k = tid; k < nb * kWarps; k += kThreads) hist_all[k] = (HT)0;
-    }
-    HT *hist = GLOBAL_HIST ? nullptr : hist_all + warp * nb;
-    unsigned long long n_recheck = 0, n_cand = 0, n_pairs = 0;
-    __syncthreads();
+    const int bins = A.rule.bins;
+    const int nb = ANI ? bins * bins : bins;
+    const int per_warp = HM == H_LANE ? nb * 32 : (HM == H_WARP ? nb : 0);
+    HT *mine = hist_all + warp * per_warp;
+    for (int k = lane; k < per_warp; k += 32) mine[k] = (HT)0;
+    __syncwarp();
+    Sink<WEIGHTED, HM> sink;
+    if (HM == H_GLOBAL) sink.base = WEIGHTED ? (void *)A.g_wsum : (void *)A.g_count;
+    else sink.base = HM == H_LANE ? (void *)(mine + lane) : (void *)mine;
+    unsigned n_pairs = 0, n_rechk = 0;
+    unsigned long long n_cand = 0;
 
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(counter, 1);
-        __syncthreads();
-        const int it_idx = s_item;
-        __syncthreads();
-        if (it_idx >= n_items) break;
-        const WorkItem it = items[it_idx];
-        const TileDesc t = tiles[it.tile];
-        const int H = t.count;
-        const int hw = H <= 32 ? 1 : (H <= 64 ? 2 : 4);  // warps per home set
-        const int G = kWarps / hw;                        // candidate split
-        const int g = warp / hw;
-        const int h = (warp % hw) * 32 + lane;
-        const bool valid = h < H;
-        const int hidx = t.start + h;
-        float4 hp = valid ? hpts[hidx] : make_float4(__int_as_float(0x7fc00000),
-                                                     __int_as_float(0x7fc00000),
-                                                     __int_as_float(0x7fc00000), 0.f);
-        for (int r = it.row_begin; r < it.row_end; ++r) {
-            const RowDesc rw = rows[r];
+    int next = 0;
+    if (lane == 0) next = atomicAdd(A.counter, 1);
+    next = __shfl_sync(kFull, next, 0);
+    while (next < A.n_items) {
+        const int it_idx = next;
+        if (lane == 0) next = atomicAdd(A.counter, 1);  // prefetch the next item
+        const WorkItem it = A.items[it_idx];
+        const TileDesc t = A.tiles[it.tile];
+        const int H = t.count;                 // 1..32 home points
+        const int S = 32 / H;                  // candidate streams per warp
+        const int sidx = lane / H;             // this lane's stream
+        const int hl = lane - sidx * H;        // this lane's home point
+        const bool valid = sidx < S;
+        const int hidx = t.start + hl;
+        Home h;
+        if (valid) {
+            h.x = A.hx[hidx]; h.y = A.hy[hidx]; h.z = A.hz[hidx]; h.w = A.hw[hidx];
+        } else {
+            h.x = h.y = h.z = __int_as_float(0x7fc00000);  // NaN: never in range
+            h.w = 0.f;
+        }
+        // Candidate ranges of all rows of the item, one row per lane, so the
+        // dependent cell-table loads of different rows overlap.
+        const int nrows = it.row_end - it.row_begin;  // <= 32 (planner)
+        int ra0 = 0, rb0 = 0, ra1 = 0, rb1 = 0, rkind = 0;
+        float rsx = 0.f, rsy = 0.f, rsz1 = 0.f;
+        if (lane < nrows) {
+            const RowDesc rw = A.rows[it.row_begin + lane];
             int nx = t.ix + rw.dx, ny = t.iy + rw.dy;
-            float sx = 0.f, sy = 0.f;
-            if (bpc) {
-                if (nx < 0) { nx += P; sx = -box; } else if (nx >= P) { nx -= P; sx = box; }
-                if (ny < 0) { ny += P; sy = -box; } else if (ny >= P) { ny -= P; sy = box; }
+            const int P = A.P;
+            bool ok = true;
+            if (A.bpc) {
+                if (nx < 0) { nx += P; rsx = -A.box; } else if (nx >= P) { nx -= P; rsx = A.box; }
+                if (ny < 0) { ny += P; rsy = -A.box; } else if (ny >= P) { ny -= P; rsy = A.box; }
             } else if (nx < 0 || nx >= P || ny < 0 || ny >= P) {
-                continue;
+                ok = false;
             }
-            const int col = (nx * P + ny) * P;
-            // up to two ranges per row
-            int a0, b0, a1 = 0, b1 = 0;
-            float sz1 = 0.f;
-            const int zhi = t.z1 + rw.kz;
-            if (rw.kind == 1) {  // forward half of the home column (XX)
-                a0 = t.start;    // intra-tile pairs use j > home index
-                b0 = cstart[col + min(zhi, P - 1) + 1];
-                if (bpc && zhi >= P) { a1 = cstart[col]; b1 = cstart[col + zhi - P + 1]; sz1 = box; }
-            } else {
-                const int zlo = t.z0 - rw.kz;
-                a0 = cstart[col + max(zlo, 0)];
-                b0 = cstart[col + min(zhi, P - 1) + 1];
-                if (bpc) {
-                    if (zlo < 0) { a1 = cstart[col + zlo + P]; b1 = cstart[col + P]; sz1 = -box; }
-                    else if (zhi >= P) { a1 = cstart[col]; b1 = cstart[col + zhi - P + 1]; sz1 = box; }
-                }
-            }
-            #pragma unroll 1
-            for (int seg = 0; seg < 2; ++seg) {
-                const int a = seg ? a1 : a0, b = seg ? b1 : b0;
-                if (a >= b) continue;
-                const float ssx = sx, ssy = sy, ssz = seg ? sz1 : 0.f;
-                const int sh = (ssx != 0.f || ssy != 0.f || ssz != 0.f) ? 1 : 0;
-                const float lo = fc.lo[sh], hi = fc.hi[sh];
-                const unsigned w = fc.w[sh];
-                const float hx = hp.x - ssx, hy = hp.y - ssy, hz = hp.z - ssz;
-                const int jmin = (rw.kind == 1 && seg == 0) ? hidx : -1;
-                if (tid == 0) n_cand += (unsigned long long)(b - a) * (unsigned long long)H;
-                #pragma unroll 4
-                for (int j = a + g; j < b; j += G) {
-                    const float4 c = __ldg(cpts + j);
-                    const float dx = c.x - hx, dy = c.y - hy, dz = c.z - hz;
-                    if (!ANI) {
-                        const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        if (d2 < hi && j > jmin) {
-                            int slot = -1;
-                            bool fast = !GLOBAL_HIST && (d2 < lo) && (d2 >= fc.tiny);
-                            if (fast) {
-                                float rr = d2 * (rsqrtf(d2) * fc.dsf);
-                                slot = fixed_bin(rr, w);
-                                fast = slot >= 0 && slot < fc.fast_bins;
-                            }
-                            if (!fast) {
-                                ++n_recheck;
-                                slot = slow_slot<false>(hp.x, hp.y, hp.z, c, ssx, ssy, ssz, rule);
-                            }
-                            if (slot >= 0) {
-                                ++n_pairs;
-                                if (GLOBAL_HIST) {
-                                    if (WEIGHTED) atomicAdd(g_wsum + slot, (double)hp.w * (double)c.w);
-                                    else atomicAdd(g_count + slot, 1ull);
-                                } else {
-                                    Acc<WEIGHTED>::add(hist, slot, hp.w, c.w);
-                                }
-                            }
-                        }
-                    } else {
-                        const float zz = dz * dz;
-                        const float pp = fmaf(dy, dy, dx * dx);
-                        if (fmaxf(zz, pp) < hi && j > jmin) {
-                            int slot = -1;
-                            bool fast = !GLOBAL_HIST && (zz < lo) && (pp < lo) && (zz >= fc.tiny) &&
-                                        (pp >= fc.tiny);
-                            if (fast) {
-                                float rz = fabsf(dz) * fc.dsf;
-                                float rp = pp * (rsqrtf(pp) * fc.dsf);
-                                int bz = fixed_bin(rz, w), bp = fixed_bin(rp, w);
-                                fast = (bz >= 0) && (bp >= 0) && bz < fc.fast_bins && bp < fc.fast_bins;
-                                slot = bz * rule.bins + bp;
-                            }
-                            if (!fast) {
-                                ++n_recheck;
-                                slot = slow_slot<true>(hp.x, hp.y, hp.z, c, ssx, ssy, ssz, rule);
-                            }
-                            if (slot >= 0) {
-                                ++n_pairs;
-                                if (GLOBAL_HIST) {
-                                    if (WEIGHTED) atomicAdd(g_wsum + slot, (double)hp.w * (double)c.w);
-                                    else atomicAdd(g_count + slot, 1ull);
-                                } else {
-                                    Acc<WEIGHTED>::add(hist, slot, hp.w, c.w);
-                                }
-                            }
-                        }
+            if (ok) {
+                const int col = (nx * P + ny) * P;
+                const int zhi = t.z1 + rw.kz;
+                rkind = rw.kind;
+                if (rw.kind == 1) {  // forward half of the home column (XX): j > home index
+                    ra0 = t.start;
+                    rb0 = A.cstart[col + min(zhi, P - 1) + 1];
+                    if (A.bpc && zhi >= P) { ra1 = A.cstart[col]; rb1 = A.cstart[col + zhi - P + 1]; rsz1 = A.box; }
+                } else {
+                    const int zlo = t.z0 - rw.kz;
+                    ra0 = A.cstart[col + max(zlo, 0)];
+                    rb0 = A.cstart[col + min(zhi, P - 1) + 1];
+                    if (A.bpc) {
+                        if (zlo < 0) { ra1 = A.cstart[col + zlo + P]; rb1 = A.cstart[col + P]; rsz1 = -A.box; }
+                        else if (zhi >= P) { ra1 = A.cstart[col]; rb1 = A.cstart[col + zhi - P + 1]; rsz1 = A.box; }
                     }
                 }
             }
         }
+        for (int r = 0; r < nrows; ++r) {
+            const int a0 = __shfl_sync(kFull, ra0, r), b0 = __shfl_sync(kFull, rb0, r);
+            const int a1 = __shfl_sync(kFull, ra1, r), b1 = __shfl_sync(kFull, rb1, r);
+            const int kind = __shfl_sync(kFull, rkind, r);
+            const float sx = __shfl_sync(kFull, rsx, r), sy = __shfl_sync(kFull, rsy, r);
+            const float sz1 = __shfl_sync(kFull, rsz1, r);
+            #pragma unroll 1
+            for (int seg = 0; seg < 2; ++seg) {
+                const int a = seg ? a1 : a0, b = seg ? b1 : b0;
+                if (a >= b) continue;
+                Seg sg;
+                sg.sx = sx; sg.sy = sy; sg.sz = seg ? sz1 : 0.f;
+                const int sh = (sg.sx != 0.f || sg.sy != 0.f || sg.sz != 0.f) ? 1 : 0;
+                sg.lo = A.fc.lo[sh];
+                sg.hi = A.fc.hi[sh];
+                sg.w = A.fc.w[sh];
+                const float2 NHX = make_float2(sg.sx - h.x, sg.sx - h.x);
+                const float2 NHY = make_float2(sg.sy - h.y, sg.sy - h.y);
+                const float2 NHZ = make_float2(sg.sz - h.z, sg.sz - h.z);
+                const int jmin = (kind == 1 && seg == 0) ? hidx : a - 1;
+                if (lane == 0) n_cand += (unsigned long long)(b - a) * (unsigned long long)H;
+                const int a2 = a & ~1;
+                #pragma unroll 1
+                for (int p = a2 + 2 * sidx; p < b; p += 2 * S) {
+                    const float2 X = __ldg(reinterpret_cast<const float2 *>(A.cx + p));
+                    const float2 Y = __ldg(reinterpret_cast<const float2 *>(A.cy + p));
+                    const float2 Z = __ldg(reinterpret_cast<const float2 *>(A.cz + p));
+                    float2 Wt = make_float2(1.f, 1.f);
+                    if (WEIGHTED) Wt = __ldg(reinterpret_cast<const float2 *>(A.cw + p));
+                    // (x_j + shift) - x_home, rounded once: same value as the
+                    // scalar (x_j - (x_home - shift)) up to the bound in make_cuts
+                    const float2 DX = __fadd2_rn(X, NHX);
+                    const float2 DY = __fadd2_rn(Y, NHY);
+                    const float2 DZ = __fadd2_rn(Z, NHZ);
+                    take2<ANI, WEIGHTED, HM>(A, DX, DY, DZ, p > jmin, (p + 1 < b) && (p + 1 > jmin),
+                                             p, Wt, h, sg, sink, n_pairs, n_rechk);
+                }
+            }
+        }
+        next = __shfl_sync(kFull, next, 0);
     }
-    __syncthreads();
-    if (!GLOBAL_HIST) {
-        for (int k = tid; k < nb; k += kThreads) {
-            HT s = 0;
-            #pragma unroll
-            for (int q = 0; q < kWarps; ++q) s += hist_all[q * nb + k];
-            if (s != (HT)0) {
-                if (WEIGHTED) atomicAdd(g_wsum + k, (double)s);
-                else atomicAdd(g_count + k, (unsigned long long)s);
+    // per-warp flush (no CTA barrier: warps leave as the queue drains)
+    __syncwarp();
+    if (HM != H_GLOBAL) {
+        if (HM == H_LANE) {
+            for (int k = 0; k < nb; ++k) {
+                HT s = mine[k * 32 + lane];
+                for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(kFull, s, off);
+                if (lane == 0 && s != (HT)0) {
+                    if (WEIGHTED) atomicAdd(A.g_wsum + k, (double)s);
+                    else atomicAdd(A.g_count + k, (unsigned long long)s);
+                }
+            }
+        } else {
+            for (int k = lane; k < nb; k += 32) {
+                const HT s = mine[k];
+                if (s != (HT)0) {
+                    if (WEIGHTED) atomicAdd(A.g_wsum + k, (double)s);
+                    else atomicAdd(A.g_count + k, (unsigned long long)s);
+                }
             }
         }
     }
-    // stats
+    unsigned long long rp = n_pairs, rr = n_rechk;
     for (int off = 16; off > 0; off >>= 1) {
-        n_recheck += __shfl_down_sync(0xffffffffu, n_recheck, off);
-        n_pairs += __shfl_down_sync(0xffffffffu, n_pairs, off);
+        rr += __shfl_down_sync(kFull, rr, off);
+        rp += __shfl_down_sync(kFull, rp, off);
     }
-    if (lane == 0 && n_recheck) atomicAdd(g_stats + 0, n_recheck);
-    if (lane == 0 && n_pairs) atomicAdd(g_stats + 2, n_pairs);
-    if (tid == 0 && n_cand) atomicAdd(g_stats + 1, n_cand);
+    if (lane == 0) {
+        if (rr) atomicAdd(A.g_stats + 0, rr);
+        if (n_cand) atomicAdd(A.g_stats + 1, n_cand);
+        if (rp) atomicAdd(A.g_stats + 2, rp);
+    }
 }
 
 // out[k] = mult * hist[k] (u64 counts or FP64 sums).
@@ -311,8 +429,10 @@ void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dma
     // tiles
     plan.tiles.clear();
     const std::vector<int> &hs = home.h_start;
-    const int span_cap = bpc ? std::max(1, std::min(P - 2 * kz_max - 1, std::max(1, k / 2) + 1))
-                             : std::max(1, k / 2 + 1);
+    // one cell per tile: the warp splits its 32 lanes into 32/H candidate
+    // streams, so small tiles keep the lanes busy without widening the
+    // candidate z-range
+    const int span_cap = 1;
     for (int ix = 0; ix < P; ++ix) {
         for (int iy = 0; iy < P; ++iy) {
             const int col = (ix * P + iy) * P;
@@ -385,7 +505,8 @@ void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dma
             total += rc[ti][ri];
         }
     }
-    const double target = std::max(total / (double)(sm_count * 16 * 4), 4096.0);
+    // ~12 items per resident warp (LPT order below) keeps the tail short
+    const double target = std::max(total / (double)(sm_count * 32 * 12), 1024.0);
     struct CI { WorkItem w; double c; };
     std::vector<CI> items;
     for (size_t ti = 0; ti < plan.tiles.size(); ++ti) {
@@ -393,7 +514,7 @@ void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dma
         double acc = 0;
         for (size_t ri = 0; ri < plan.rows.size(); ++ri) {
             acc += rc[ti][ri];
-            if (acc >= target || ri + 1 == plan.rows.size()) {
+            if (acc >= target || ri + 1 == plan.rows.size() || (int)ri + 1 - rb >= 32) {
                 if (acc > 0) items.push_back({{(int)ti, rb, (int)ri + 1, cat}, acc});
                 rb = (int)ri + 1;
                 acc = 0;
@@ -409,13 +530,15 @@ void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dma
 // ---------------------------------------------------------------------------
 // Launch one pair histogram (device side; result left in d_out as doubles).
 // ---------------------------------------------------------------------------
-static FastCuts make_cuts(const PairRule &rule, float box, float dmax, bool ani) {
+static FastCuts make_cuts(const PairRule &rule, float box, float dmax) {
     FastCuts fc;
     fc.dsf = (float)rule.ds;
+    fc.ds2 = fc.dsf * fc.dsf;
     const double dd = rule.dd;
     const double rmax = (double)dmax * rule.ds + 1.0;  // r units
-    // relative FP32 error of d2 (subtraction, 3 products/sums) <= ~2^-21:
-    // windows carry an 8x-16x margin.
+    // Relative FP32 error of d2 (one rounding in each difference, then the
+    // FMA chain) stays below ~2^-21, and of r = sqrt.approx(d2*ds^2) below
+    // ~2^-20: the windows below keep an 8x margin over those bounds.
     const double e_plain_d2 = dd * std::ldexp(1.0, -17);
     const double w_plain = rmax * std::ldexp(1.0, -17);
     // image-shifted home point: |error of dx| <= L*2^-23 per axis
@@ -425,15 +548,25 @@ static FastCuts make_cuts(const PairRule &rule, float box, float dmax, bool ani)
     fc.hi[0] = (float)(dd + e_plain_d2);
     fc.lo[1] = (float)(dd - e_shift_d2);
     fc.hi[1] = (float)(dd + e_shift_d2);
-    // fixed-point quantisation adds 2^-16
-    fc.w[0] = (unsigned)std::ceil((w_plain + std::ldexp(1.0, -16)) * 32768.0) + 1u;
-    fc.w[1] = (unsigned)std::ceil((w_shift + std::ldexp(1.0, -16)) * 32768.0) + 1u;
-    fc.w[0] = std::min(fc.w[0], 8000u);
-    fc.w[1] = std::min(fc.w[1], 8000u);
+    // + quantisation of the fixed-point readout (2^-16)
+    fc.w[0] = std::min(8000u, (unsigned)std::ceil((w_plain + std::ldexp(1.0, -16)) * 32768.0) + 1u);
+    fc.w[1] = std::min(8000u, (unsigned)std::ceil((w_shift + std::ldexp(1.0, -16)) * 32768.0) + 1u);
     fc.tiny = 1e-30f;
-    fc.fast_bins = std::min(rule.bins, 255);
-    (void)ani;
     return fc;
+}
+
+template <bool ANI, bool W, int HM>
+static pcf_status launch_one(pcf_ctx *ctx, const PairArgs &A, size_t smem, int n_items) {
+    auto kfn = k_pairs<ANI, W, HM>;
+    if (smem > 48 * 1024)
+        PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    PCF_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
+    per_sm = std::max(1, per_sm);
+    const int want = (n_items + kWarps - 1) / kWarps;
+    const int grid = std::max(1, std::min(want, ctx->sm_count * per_sm));
+    kfn<<<grid, kThreads, smem, ctx->stream>>>(A);
+    return PCF_OK;
 }
 
 // Launches the pair kernel for one (home, cand) plan into d_count/d_wsum.
@@ -452,8 +585,7 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     PCF_CU(ctx, ctx->d_counter.ensure(sizeof(int) * 16));
     pcf_status s = pcf_ensure_pinned(ctx, tb + rb + ib + 64);
     if (s != PCF_OK) return s;
-    // stage through pinned memory (the stream may still read the previous plan,
-    // so wait for it first)
+    // the staging buffer may still feed a previous copy on this stream
     PCF_CU(ctx, cudaStreamSynchronize(st));
     char *hp = static_cast<char *>(ctx->h_pinned);
     memcpy(hp, plan.tiles.data(), tb);
@@ -464,45 +596,48 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     PCF_CU(ctx, cudaMemcpyAsync(ctx->d_items.p, hp + tb + rb, ib, cudaMemcpyHostToDevice, st));
     PCF_CU(ctx, cudaMemsetAsync(ctx->d_counter.p, 0, sizeof(int), st));
 
-    FastCuts fc = make_cuts(pl.rule, box, std::sqrt((float)pl.rule.dd), pl.ani);
+    PairArgs A;
+    A.hx = home.x(); A.hy = home.y(); A.hz = home.z(); A.hw = home.w();
+    A.cx = cand.x(); A.cy = cand.y(); A.cz = cand.z(); A.cw = cand.w();
+    A.cstart = cand.cell_start.as<int>();
+    A.tiles = ctx->d_tiles.as<TileDesc>();
+    A.rows = ctx->d_rows.as<RowDesc>();
+    A.items = ctx->d_items.as<WorkItem>();
+    A.n_items = (int)plan.items.size();
+    A.counter = ctx->d_counter.as<int>();
+    A.P = plan.P;
+    A.box = box;
+    A.bpc = pl.bpc ? 1 : 0;
+    A.rule = pl.rule;
+    A.fc = make_cuts(pl.rule, box, std::sqrt((float)pl.rule.dd));
+    A.g_count = d_count;
+    A.g_wsum = d_wsum;
+    A.g_stats = d_stats;
+
     const int nb = pl.ani ? pl.rule.bins * pl.rule.bins : pl.rule.bins;
-    const size_t hbytes = (size_t)nb * kWarps * (pl.weighted ? 8 : 4);
-    const bool global_hist = hbytes > 160 * 1024 || pl.rule.bins > 255;
-    const int grid = std::max(1, std::min((int)plan.items.size(), ctx->sm_count * 8));
-    const size_t smem = global_hist ? 0 : hbytes;
-    int *counter = ctx->d_counter.as<int>();
-    const int bpc = pl.bpc ? 1 : 0;
+    const size_t ebytes = pl.weighted ? 8 : 4;
+    const size_t lane_bytes = (size_t)nb * 32 * kWarps * ebytes;
+    const size_t warp_bytes = (size_t)nb * kWarps * ebytes;
+    int hm;
+    size_t smem;
+    if (pl.rule.bins > 255 || warp_bytes > 160 * 1024) { hm = H_GLOBAL; smem = 0; }
+    else if (!pl.ani && lane_bytes <= 64 * 1024) { hm = H_LANE; smem = lane_bytes; }
+    else { hm = H_WARP; smem = warp_bytes; }
     PCF_CU(ctx, cudaEventRecord(ctx->ev0, st));
-#define PCF_LAUNCH(A, W, G)                                                                      \
-    do {                                                                                         \
-        auto kfn = k_pairs<A, W, G>;                                                             \
-        if (smem > 48 * 1024)                                                                    \
-            PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                             (int)smem));                                        \
-        kfn<<<grid, kThreads, smem, st>>>(home.pts.as<float4>(), cand.pts.as<float4>(),          \
-                                          cand.cell_start.as<int>(), ctx->d_tiles.as<TileDesc>(), \
-                                          ctx->d_rows.as<RowDesc>(), ctx->d_items.as<WorkItem>(), \
-                                          (int)plan.items.size(), counter, plan.P, box, bpc,     \
-                                          pl.rule, fc, d_count, d_wsum, d_stats);                \
-    } while (0)
-    if (global_hist) {
-        // wide histograms (e.g. the fine DD of the analytic path): every
-        // in-range pair takes the FP64 rule, accumulated in global memory
-        if (pl.ani) {
-            if (pl.weighted) PCF_LAUNCH(true, true, true);
-            else PCF_LAUNCH(true, false, true);
-        } else {
-            if (pl.weighted) PCF_LAUNCH(false, true, true);
-            else PCF_LAUNCH(false, false, true);
-        }
-    } else if (pl.ani) {
-        if (pl.weighted) PCF_LAUNCH(true, true, false);
-        else PCF_LAUNCH(true, false, false);
-    } else {
-        if (pl.weighted) PCF_LAUNCH(false, true, false);
-        else PCF_LAUNCH(false, false, false);
+    pcf_status r = PCF_OK;
+#define PCF_DISPATCH(ANI_)                                                                   \
+    if (pl.weighted) {                                                                       \
+        if (hm == H_LANE) r = launch_one<ANI_, true, H_LANE>(ctx, A, smem, A.n_items);       \
+        else if (hm == H_WARP) r = launch_one<ANI_, true, H_WARP>(ctx, A, smem, A.n_items);  \
+        else r = launch_one<ANI_, true, H_GLOBAL>(ctx, A, smem, A.n_items);                  \
+    } else {                                                                                 \
+        if (hm == H_LANE) r = launch_one<ANI_, false, H_LANE>(ctx, A, smem, A.n_items);      \
+        else if (hm == H_WARP) r = launch_one<ANI_, false, H_WARP>(ctx, A, smem, A.n_items); \
+        else r = launch_one<ANI_, false, H_GLOBAL>(ctx, A, smem, A.n_items);                 \
     }
-#undef PCF_LAUNCH
+    if (pl.ani) { PCF_DISPATCH(true) } else { PCF_DISPATCH(false) }
+#undef PCF_DISPATCH
+    if (r != PCF_OK) return r;
     PCF_CU(ctx, cudaGetLastError());
     PCF_CU(ctx, cudaEventRecord(ctx->ev1, st));
     ++ctx->launches;

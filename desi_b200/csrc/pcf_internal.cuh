@@ -122,9 +122,18 @@ struct CellGrid {
     int P = 0;
     float cell = 0.f;             // box / P
     DevBuf pts;                   // float4 x n, cell order
+    DevBuf soa;                   // x | y | z | w planes, n + kSoaPad floats each
+    size_t plane = 0;             // floats per plane
     DevBuf cell_start;            // int x (P^3 + 1)
     std::vector<int> h_start;     // host copy of cell_start
+    const float *x() const { return soa.as<float>(); }
+    const float *y() const { return soa.as<float>() + plane; }
+    const float *z() const { return soa.as<float>() + 2 * plane; }
+    const float *w() const { return soa.as<float>() + 3 * plane; }
 };
+// SoA planes are padded so that a float2 load at the last even index stays
+// inside the allocation, and each plane starts 16-byte aligned.
+constexpr int kSoaPad = 4;
 
 struct pcf_grid {
     int64_t n = 0;
