@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the periodic pair-count step on B200.
+
+Workload (one "step"): the 2-point periodic-box step of the clustering
+pipeline -- DD, RR and DR for both the isotropic and the anisotropic
+(|dz|, r_perp) histograms -- on N=32768 Neyman-Scott clustered data (512
+parents x 64 Gaussian children, sigma 5, wrapped) plus 32768 uniform
+randoms in a box of side 250, weights U(0.5, 1.5), 30 bins per axis,
+dmax = 80.  The step grids both catalogs on the device (counting sort) and
+runs the six histograms through the library's C ABI.
+
+  value  pairs/s with the catalogs already in HBM (unit: one in-range
+         unordered XX pair or one XY pair; the reference counts XX pairs
+         twice, the unit does not)
+  e2e    the same through the public API from pinned host buffers, with
+         the H2D copy of the points and the D2H copy of the histograms
+         inside the timed region
+  roofline  the pair kernel against the FP32 FMA peak measured in this run
+         (8 FP32 flops per in-range pair); the kernel is CUDA-core bound
+         (no HBM or tensor-core bound applies: inputs sit in L2)
+  cpu_baseline  the reference's own CPU OpenMP engines (oracle/_ref,
+         cpp/2PCF{isotropic,anisotropic}/BPC) on the same catalogs
+
+--impl reference times those CPU engines alone (all host threads).
+Multi-GPU: one process per GPU (torchrun); every rank runs the same step on
+its own GPU (replicas; scaling "weak"); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = {
+    "workload": "2iso+2ani periodic pair counts (DD, RR, DR each): N=32768 Neyman-Scott "
+                "clustered data (512x64, sigma 5) + 32768 uniform randoms, box 250, "
+                "w~U(0.5,1.5) float32, 30 bins, dmax 80",
+    "n_data": 32768, "n_rand": 32768, "box": 250.0, "bins": 30, "dmax": 80.0,
+    "bpc": True, "histograms": ["DDiso", "RRiso", "DRiso", "DDani", "RRani", "DRani"],
+}
+SEED_D, SEED_R = 2001, 2002
+
+
+def catalogs():
+    from desi_b200 import catalog
+    D = catalog.neyman_scott(WORKLOAD["n_data"], WORKLOAD["box"], seed=SEED_D, children=64,
+                             sigma=5.0, weights="uniform")
+    R = catalog.uniform(WORKLOAD["n_rand"], WORKLOAD["box"], seed=SEED_R, weights="uniform")
+    return D, R
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from desi_b200 import api
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    W = WORKLOAD
+    D, R = catalogs()
+    ctx = api.Context(local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    P = ctx.autotune_partitions(max(len(D), len(R)), W["box"], W["dmax"], bpc=True)
+    Dt = torch.from_numpy(D).to(dev)
+    Rt = torch.from_numpy(R).to(dev)
+    outs = torch.zeros((6, W["bins"] * W["bins"]), dtype=torch.float64, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # pinned host copies for the end-to-end path
+    Dh = torch.from_numpy(D).pin_memory()
+    Rh = torch.from_numpy(R).pin_memory()
+    torch.cuda.synchronize()
+
+    def step_device(collect, with_stats=False):
+        # asynchronous: histograms stay in HBM, no per-call host sync
+        gd = ctx.grid(None, W["box"], partitions=P, device_ptr=Dt.data_ptr(), n=len(D))
+        gr = ctx.grid(None, W["box"], partitions=P, device_ptr=Rt.data_ptr(), n=len(R))
+        k = 0
+        for ani in (False, True):
+            for a, b in ((gd, None), (gr, None), (gd, gr)):
+                r = ctx.count_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True,
+                                    stats=with_stats, out_device_ptr=outs[k].data_ptr())
+                if with_stats:
+                    collect.append(r[1])
+                k += 1
+        gd.free()
+        gr.free()
+
+    def step_e2e(collect):
+        gd = ctx.grid(Dh.numpy(), W["box"], partitions=P)
+        gr = ctx.grid(Rh.numpy(), W["box"], partitions=P)
+        hists = []
+        for ani in (False, True):
+            for a, b in ((gd, None), (gr, None), (gd, gr)):
+                h, st = ctx.count_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True,
+                                        stats=True)
+                hists.append(h)
+                collect.append(st)
+        gd.free()
+        gr.free()
+        return hists
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn([])
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        times, stats = [], []
+        launches0 = ctx.launches
+        ctx.profile(True)
+        sampler = ClockSampler(local_rank)
+        sampler.start()
+        for _ in range(steps):
+            flush.zero_()  # L2 flush between steps (outside the timed region)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn(stats)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        clocks = sampler.stop()
+        kprof = ctx.profile_read()
+        ctx.profile(False)
+        torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        if world > 1:
+            torch.distributed.barrier()
+        return times, stats, clocks, launches, kprof
+
+    # pairs per step (deterministic): one untimed pass with counters
+    probe = []
+    step_device(probe, with_stats=True)
+    times, _, clocks, launches, kprof = timed(step_device, args.steps, args.warmup)
+    tot_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    pairs_step = sum(s["pairs"] for s in probe)
+    value = world * pairs_step * args.steps / (tot_ms * 1e-3)
+
+    # end to end through the public API from pinned host buffers
+    e_times, e_stats, e_clocks, _, _ = timed(step_e2e, args.steps, max(1, args.warmup // 2))
+    e_tot = sum(e_times)
+    if world > 1:
+        t = torch.tensor([e_tot], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e_tot = float(t.item())
+    e2e_value = world * pairs_step * args.steps / (e_tot * 1e-3)
+    h2d = (len(D) + len(R)) * 16
+    d2h = 3 * W["bins"] * 8 + 3 * W["bins"] * W["bins"] * 8
+
+    # roofline of the pair kernel: 8 FP32 flops per in-range pair
+    k_ms, n_launch = kprof  # pair-kernel launches logged over the timed region
+    k_pairs = pairs_step * args.steps
+    stats = probe
+    fp32_peak = ctx.microbench(0)
+    smem_peak = ctx.microbench(1)
+    achieved = 8.0 * k_pairs / (k_ms * 1e-3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "pairs_c2_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {
+        "bound": "fp32", "kernel": "k_pairs",
+        "achieved": round(achieved, 4), "peak": round(fp32_peak, 3), "unit": "TFLOP/s",
+        "frac": round(achieved / fp32_peak, 5),
+        "peak_source": "FP32 FMA-loop microbenchmark of this run (not in MEASURED_PEAKS.json)",
+        "traffic": traffic,
+        "pairs_per_s_kernel": k_pairs / (k_ms * 1e-3),
+        "pairs_bound_per_s": min(fp32_peak * 1e12 / 8.0, smem_peak * 1e9),
+        "smem_atomic_gops": round(smem_peak, 1),
+        "avg_launch_ms": k_ms / n_launch,
+        "algorithmic_flops_per_launch": 8.0 * k_pairs / n_launch,
+        "candidates_per_pair": sum(s["candidates"] for s in stats) / max(pairs_step, 1),
+        "recheck_fraction": sum(s["rechecks"] for s in stats) / max(pairs_step, 1),
+        "kernel_share_of_step": k_ms / tot_ms if world == 1 else None,
+    }
+    out = {
+        "metric": "pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Neyman-Scott data + uniform randoms; no dataset ships with "
+                "the workload)",
+        "config": dict(W, partitions=P, parallelism=f"replicas x{world}",
+                       l2="flushed between steps (512 MB write)",
+                       pairs_per_step=pairs_step),
+        "latency_ms": {"p50": statistics.median(times),
+                       "p99": float(np.percentile(times, 99))},
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e_tot / args.steps},
+        "roofline": roofline,
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(pairs_step)
+    ctx.close()
+    return out
+
+
+def _ref_engines():
+    import oracle
+    avail = oracle.available_ref_engines()
+    if "2iso_bpc" in avail and "2ani_bpc" in avail:
+        return oracle.RefEngine("2iso_bpc"), oracle.RefEngine("2ani_bpc")
+    return None
+
+
+def _cpu_step(engines, D, R, threads, unit=False):
+    W = WORKLOAD
+    sn = 2.176 * W["box"] / (W["n_data"] ** (1.0 / 3.0))  # the engines' own main() rule
+    if unit:
+        D = D.copy(); D[:, 3] = 1.0
+        R = R.copy(); R[:, 3] = 1.0
+    tot = 0.0
+    for e in engines:
+        e.set_threads(threads)
+        a = e.xx(D, box=W["box"], size_node=sn, bins=W["bins"], dmax=W["dmax"])
+        b = e.xx(R, box=W["box"], size_node=sn, bins=W["bins"], dmax=W["dmax"])
+        c = e.xy(D, R, box=W["box"], size_node=sn, bins=W["bins"], dmax=W["dmax"])
+        tot += a.sum() / 2 + b.sum() / 2 + c.sum()
+    return tot
+
+
+def cpu_baseline(pairs_step=None, steps=1):
+    """The reference CPU engines on the full step, all host threads."""
+    D, R = catalogs()
+    threads = os.cpu_count() or 1
+    eng = _ref_engines()
+    if eng is not None:
+        if pairs_step is None:
+            pairs_step = _cpu_step(eng, D, R, threads, unit=True)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            _cpu_step(eng, D, R, threads)
+        dt = (time.perf_counter() - t0) / steps
+        return {"value": pairs_step / dt, "unit": "pairs/s", "cores": threads,
+                "kind": "reference",
+                "sample": "the full step (6 histograms, 32768+32768 points) through the "
+                          "reference engines cpp/2PCF{isotropic,anisotropic}/BPC, "
+                          f"{steps} step(s), {dt:.3f} s per step",
+                "seconds_per_step": dt}
+    # fallback: the oracle port (brute force) on a bounded sample
+    import oracle
+    n = 8192
+    Ds, Rs = D[:n], R[:n]
+    t0 = time.perf_counter()
+    cnt = 0.0
+    W = WORKLOAD
+    for ani in (False, True):
+        for A, B in ((Ds, None), (Rs, None), (Ds, Rs)):
+            oracle.pairs(A, B, box=W["box"], bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True)
+    dt = time.perf_counter() - t0
+    for ani in (False,):
+        for A, B in ((Ds, None), (Rs, None), (Ds, Rs)):
+            A1 = A.copy(); A1[:, 3] = 1
+            B1 = None if B is None else B.copy()
+            if B1 is not None:
+                B1[:, 3] = 1
+            h = oracle.pairs(A1, B1, box=W["box"], bins=W["bins"], dmax=W["dmax"], bpc=True)
+            cnt += h.sum() / (2 if B is None else 1)
+    return {"value": 2 * cnt / dt, "unit": "pairs/s", "cores": threads, "kind": "port",
+            "sample": f"oracle brute force on the first {n} points of each catalog"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    D, R = catalogs()
+    threads = os.cpu_count() or 1
+    eng = _ref_engines()
+    if eng is None:
+        return {"impl": "reference",
+                "unavailable": "oracle/_ref engines not built (needs the reference tree at "
+                               "build time)"}
+    pairs_step = _cpu_step(eng, D, R, threads, unit=True)
+    for _ in range(args.warmup):
+        _cpu_step(eng, D, R, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _cpu_step(eng, D, R, threads)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = pairs_step * args.steps / tot
+    return {
+        "impl": "reference", "metric": "pairs/s", "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, same catalogs)",
+        "config": dict(WORKLOAD, parallelism="reference CPU OpenMP engines"),
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": "full step through cpp/2PCF{isotropic,anisotropic}/BPC "
+                                   "engines (compiled in place), all host threads"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "latency_ms": {"p50": 1e3 * statistics.median(times),
+                       "p99": 1e3 * float(np.percentile(times, 99))},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        out = run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -79,6 +79,9 @@ _SIGS = {
                                                ctypes.c_int, ctypes.c_uint32]),
     "pcf_microbench": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "pcf_ctx_launch_count": (_i64, [_vp]),
+    "pcf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pcf_ctx_profile_read": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(_i64)]),
 }
 
 

@@ -179,6 +179,18 @@ class Context:
                "pcf_microbench")
         return r.value
 
+    def profile(self, enable: bool = True) -> None:
+        """Start (or stop) logging the device time of every counting kernel."""
+        _check(self.handle, self._lib.pcf_ctx_profile(self.handle, int(enable)), "pcf_ctx_profile")
+
+    def profile_read(self):
+        """(summed kernel ms, logged launches) since profile(); clears the log."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        _check(self.handle, self._lib.pcf_ctx_profile_read(self.handle, ctypes.byref(ms),
+                                                           ctypes.byref(n)), "pcf_ctx_profile_read")
+        return ms.value, n.value
+
     @property
     def launches(self) -> int:
         return int(self._lib.pcf_ctx_launch_count(self.handle))

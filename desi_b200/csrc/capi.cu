@@ -58,7 +58,16 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
     if (!ctx) return PCF_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    ctx->pool->release();
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    for (auto &sl : ctx->slots) {
+        if (sl.h_pinned) cudaFreeHost(sl.h_pinned);
+        if (sl.done) cudaEventDestroy(sl.done);
+    }
+    for (auto &e : ctx->prof_events) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
     cudaEventDestroy(ctx->ev0);
     cudaEventDestroy(ctx->ev1);
     cudaStreamDestroy(ctx->stream);
@@ -69,6 +78,29 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
 void *pcf_ctx_stream(pcf_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 int64_t pcf_ctx_launch_count(const pcf_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+pcf_status pcf_ctx_profile(pcf_ctx *ctx, int enable) {
+    if (!ctx) return PCF_ERR_INVALID_ARG;
+    ctx->profile = enable != 0;
+    ctx->prof_used = 0;
+    return PCF_OK;
+}
+
+pcf_status pcf_ctx_profile_read(pcf_ctx *ctx, double *total_ms, int64_t *n) {
+    if (!ctx) return PCF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    double tot = 0;
+    for (size_t i = 0; i < ctx->prof_used; ++i) {
+        float ms = 0.f;
+        PCF_CU(ctx, cudaEventElapsedTime(&ms, ctx->prof_events[i].first, ctx->prof_events[i].second));
+        tot += ms;
+    }
+    if (total_ms) *total_ms = tot;
+    if (n) *n = (int64_t)ctx->prof_used;
+    ctx->prof_used = 0;
+    return PCF_OK;
+}
 
 static bool is_device_ptr(const void *p) {
     cudaPointerAttributes a;
@@ -87,6 +119,8 @@ pcf_status pcf_grid_build(pcf_ctx *ctx, const pcf_point *pts, int64_t n, float b
     *out = nullptr;
     cudaSetDevice(ctx->device);
     std::unique_ptr<pcf_grid> g(new pcf_grid);
+    g->pool = ctx->pool;
+    g->raw.pool = ctx->pool;
     g->n = n;
     g->box = box;
     PCF_CU(ctx, g->raw.ensure(sizeof(float4) * (size_t)n));
@@ -103,10 +137,9 @@ pcf_status pcf_grid_build(pcf_ctx *ctx, const pcf_point *pts, int64_t n, float b
 
 pcf_status pcf_grid_free(pcf_ctx *ctx, pcf_grid *g) {
     if (!g) return PCF_ERR_INVALID_ARG;
-    if (ctx) {
-        cudaSetDevice(ctx->device);
-        cudaStreamSynchronize(ctx->stream);
-    }
+    if (ctx) cudaSetDevice(ctx->device);
+    // buffers go back to the context's pool; later users of the blocks are
+    // ordered after the work already queued on the context stream
     delete g;
     return PCF_OK;
 }
@@ -233,8 +266,7 @@ extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_
     pcf_status s = prepare_grids(ctx, a, b, dmax, kind, bpc, &P);
     if (s != PCF_OK) return s;
     PairPlan plan;
-    plan_pairs(*a->cells, cross ? b->cells.get() : nullptr, a->box, dmax, ani, bpc, !cross, 32, 0,
-               plan, ctx->sm_count);
+    plan_pairs(*a->cells, a->box, dmax, ani, !cross, plan, ctx->sm_count * 24);
     const int nb = ani ? bins * bins : bins;
     unsigned long long *d_cnt, *d_stats;
     double *d_ws, *d_out;
@@ -278,7 +310,7 @@ extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_
             stats->pairs = (double)hs[2];
             stats->kernel_ms = ms;
             stats->partitions = P;
-            stats->work_items = (int)plan.items.size();
+            stats->work_items = (int)std::min<int64_t>(plan.n_items, INT32_MAX);
         }
     }
     return PCF_OK;

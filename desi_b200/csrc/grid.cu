@@ -10,21 +10,59 @@
 // Cell id = (ix*P + iy)*P + iz with ix = (int)(x / cell), the reference's
 // binning (create_grid.cuh:131-133) clamped to [0, P-1].
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 
 #include "pcf_internal.cuh"
 
+cudaError_t MemPool::get(size_t n, void **p, size_t *got) {
+    auto it = free_blocks.lower_bound(n);
+    if (it != free_blocks.end() && it->first <= 2 * n + 4096) {
+        *p = it->second;
+        *got = it->first;
+        cached -= it->first;
+        free_blocks.erase(it);
+        return cudaSuccess;
+    }
+    size_t want = std::max<size_t>(256, (n + 255) & ~(size_t)255);
+    cudaError_t e = cudaMalloc(p, want);
+    if (e == cudaErrorMemoryAllocation && !free_blocks.empty()) {
+        cudaGetLastError();
+        release();
+        e = cudaMalloc(p, want);
+    }
+    if (e == cudaSuccess) *got = want;
+    return e;
+}
+
+void MemPool::put(void *p, size_t n) {
+    free_blocks.emplace(n, p);
+    cached += n;
+}
+
+void MemPool::release() {
+    for (auto &kv : free_blocks) cudaFree(kv.second);
+    free_blocks.clear();
+    cached = 0;
+}
+
 DevBuf::~DevBuf() {
-    if (p) cudaFree(p);
+    if (!p) return;
+    if (pool) pool->put(p, bytes);
+    else cudaFree(p);
 }
 
 cudaError_t DevBuf::ensure(size_t n) {
     if (n <= bytes && p) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) {
+        if (pool) pool->put(p, bytes);
+        else cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
+    if (pool) return pool->get(std::max<size_t>(n, 256), &p, &bytes);
     size_t want = std::max<size_t>(n, 256);
     cudaError_t e = cudaMalloc(&p, want);
     if (e == cudaSuccess) bytes = want;
@@ -147,6 +185,7 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     if (g->cells && g->cells->P == P) return PCF_OK;
     if (P < 1 || P > 320) return PCF_ERR_INVALID_ARG;
     std::unique_ptr<CellGrid> cg(new CellGrid);
+    cg->pts.pool = cg->soa.pool = cg->cell_start.pool = g->pool;
     cg->P = P;
     cg->cell = g->box / (float)P;
     const int64_t n = g->n;
@@ -191,6 +230,12 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
         return PCF_ERR_OUT_OF_BOX;
     }
     g->unit_weights = (hflags & 2) == 0;
+    build_tiles(*cg);
+    cg->d_tiles.pool = g->pool;
+    PCF_CU(ctx, cg->d_tiles.ensure(sizeof(TileDesc) * std::max<size_t>(1, cg->tiles.size())));
+    if (!cg->tiles.empty())
+        PCF_CU(ctx, cudaMemcpyAsync(cg->d_tiles.p, cg->tiles.data(),
+                                    sizeof(TileDesc) * cg->tiles.size(), cudaMemcpyHostToDevice, st));
     g->cells = std::move(cg);
     return PCF_OK;
 }

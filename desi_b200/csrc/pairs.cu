@@ -58,9 +58,11 @@ struct PairArgs {
     const int *cstart;
     const TileDesc *tiles;
     const RowDesc *rows;
-    const WorkItem *items;
-    int n_items;
-    int *counter;
+    int n_rows;
+    int rows_per_item;
+    int n_chunks;
+    long long n_items;
+    unsigned long long *counter;
     int P;
     float box;
     int bpc;
@@ -237,14 +239,17 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
     unsigned n_pairs = 0, n_rechk = 0;
     unsigned long long n_cand = 0;
 
-    int next = 0;
-    if (lane == 0) next = atomicAdd(A.counter, 1);
+    long long next = 0;
+    if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);
     next = __shfl_sync(kFull, next, 0);
     while (next < A.n_items) {
-        const int it_idx = next;
-        if (lane == 0) next = atomicAdd(A.counter, 1);  // prefetch the next item
-        const WorkItem it = A.items[it_idx];
-        const TileDesc t = A.tiles[it.tile];
+        const long long it_idx = next;
+        if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next item
+        const int tile = (int)(it_idx / A.n_chunks);
+        const int chunk = (int)(it_idx - (long long)tile * A.n_chunks);
+        const int row_begin = chunk * A.rows_per_item;
+        const int row_end = min(row_begin + A.rows_per_item, A.n_rows);
+        const TileDesc t = A.tiles[tile];
         const int H = t.count;                 // 1..32 home points
         const int S = 32 / H;                  // candidate streams per warp
         const int sidx = lane / H;             // this lane's stream
@@ -260,11 +265,11 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
         }
         // Candidate ranges of all rows of the item, one row per lane, so the
         // dependent cell-table loads of different rows overlap.
-        const int nrows = it.row_end - it.row_begin;  // <= 32 (planner)
+        const int nrows = row_end - row_begin;  // <= 32 (planner)
         int ra0 = 0, rb0 = 0, ra1 = 0, rb1 = 0, rkind = 0;
         float rsx = 0.f, rsy = 0.f, rsz1 = 0.f;
         if (lane < nrows) {
-            const RowDesc rw = A.rows[it.row_begin + lane];
+            const RowDesc rw = A.rows[row_begin + lane];
             int nx = t.ix + rw.dx, ny = t.iy + rw.dy;
             const int P = A.P;
             bool ok = true;
@@ -382,8 +387,29 @@ __global__ void k_finalize(const unsigned long long *__restrict__ cnt, const dou
 // ---------------------------------------------------------------------------
 // Host planning.
 // ---------------------------------------------------------------------------
-void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dmax, bool ani,
-                bool bpc, bool self, int tile_cap, int cat, PairPlan &plan, int sm_count) {
+void build_tiles(CellGrid &g) {
+    const int P = g.P;
+    const std::vector<int> &hs = g.h_start;
+    g.tiles.clear();
+    for (int ix = 0; ix < P; ++ix)
+        for (int iy = 0; iy < P; ++iy)
+            for (int iz = 0; iz < P; ++iz) {
+                const int c = (ix * P + iy) * P + iz;
+                const int s0 = hs[c], n = hs[c + 1] - s0;
+                for (int o = 0; o < n; o += kTileCap) {
+                    TileDesc t;
+                    t.start = s0 + o;
+                    t.count = std::min(kTileCap, n - o);
+                    t.ix = (int16_t)ix;
+                    t.iy = (int16_t)iy;
+                    t.z0 = t.z1 = (int16_t)iz;
+                    g.tiles.push_back(t);
+                }
+            }
+}
+
+void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self, PairPlan &plan,
+                int resident_warps) {
     const int P = home.P;
     const double cell = (double)box / P;
     const double R = (double)dmax;
@@ -394,22 +420,17 @@ void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dma
     plan.P = P;
     plan.cell = (float)cell;
     plan.rows.clear();
-    int kz_max = 0;
     for (int dx = -k; dx <= k; ++dx) {
         for (int dy = -k; dy <= k; ++dy) {
-            double mx = std::max(std::abs(dx) - 1, 0) * cell;
-            double my = std::max(std::abs(dy) - 1, 0) * cell;
-            double mxy2 = mx * mx + my * my;
+            const double mx = std::max(std::abs(dx) - 1, 0) * cell;
+            const double my = std::max(std::abs(dy) - 1, 0) * cell;
+            const double mxy2 = mx * mx + my * my;
             if (mxy2 >= Rm * Rm) continue;
-            int kz;
-            if (ani) {
-                kz = k;
-            } else {
-                double rem = std::sqrt(std::max(Rm * Rm - mxy2, 0.0));
-                kz = (int)std::ceil(rem / cell);  // max(|dz|-1,0)*cell < rem
-                kz = std::min(kz, k);
+            int kz = k;  // ani: cylinder |dz| < dmax
+            if (!ani) {  // iso: max(|dz|-1,0)*cell < sqrt(R^2 - mxy^2)
+                const double rem = std::sqrt(std::max(Rm * Rm - mxy2, 0.0));
+                kz = std::min(k, (int)std::ceil(rem / cell));
             }
-            kz_max = std::max(kz_max, kz);
             RowDesc r;
             r.dx = (int16_t)dx;
             r.dy = (int16_t)dy;
@@ -417,114 +438,23 @@ void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dma
             r.kind = 0;
             if (self) {
                 if (dx == 0 && dy == 0) {
-                    r.kind = 1;
+                    r.kind = 1;  // forward half of the home column
                     plan.rows.insert(plan.rows.begin(), r);
                     continue;
                 }
-                if (!(dx > 0 || (dx == 0 && dy > 0))) continue;
+                if (!(dx > 0 || (dx == 0 && dy > 0))) continue;  // half shell
             }
             plan.rows.push_back(r);
         }
     }
-    // tiles
-    plan.tiles.clear();
-    const std::vector<int> &hs = home.h_start;
-    // one cell per tile: the warp splits its 32 lanes into 32/H candidate
-    // streams, so small tiles keep the lanes busy without widening the
-    // candidate z-range
-    const int span_cap = 1;
-    for (int ix = 0; ix < P; ++ix) {
-        for (int iy = 0; iy < P; ++iy) {
-            const int col = (ix * P + iy) * P;
-            int cur_start = -1, cur_cnt = 0, z0 = 0, zlast = 0;
-            auto emit = [&](int start, int count, int za, int zb) {
-                TileDesc t;
-                t.start = start;
-                t.count = count;
-                t.ix = (int16_t)ix;
-                t.iy = (int16_t)iy;
-                t.z0 = (int16_t)za;
-                t.z1 = (int16_t)zb;
-                plan.tiles.push_back(t);
-            };
-            auto flush = [&]() {
-                if (cur_start >= 0 && cur_cnt > 0) emit(cur_start, cur_cnt, z0, zlast);
-                cur_start = -1;
-                cur_cnt = 0;
-            };
-            for (int iz = 0; iz < P; ++iz) {
-                const int s = hs[col + iz], c = hs[col + iz + 1] - s;
-                if (c == 0) continue;
-                if (cur_start >= 0 && (cur_cnt + c > tile_cap || iz - z0 + 1 > span_cap)) flush();
-                if (c > tile_cap) {  // heavy cell: slices of tile_cap points
-                    for (int o = 0; o < c; o += tile_cap) emit(s + o, std::min(tile_cap, c - o), iz, iz);
-                    continue;
-                }
-                if (cur_start < 0) {
-                    cur_start = s;
-                    z0 = iz;
-                }
-                cur_cnt += c;
-                zlast = iz;
-            }
-            flush();
-        }
-    }
-    // cost of (tile, row) = H * candidates in the row's ranges
-    const std::vector<int> &cs = cand ? cand->h_start : home.h_start;
-    auto row_cost = [&](const TileDesc &t, const RowDesc &rw) -> double {
-        int nx = t.ix + rw.dx, ny = t.iy + rw.dy;
-        if (bpc) {
-            nx = (nx % P + P) % P;
-            ny = (ny % P + P) % P;
-        } else if (nx < 0 || nx >= P || ny < 0 || ny >= P) {
-            return 0.0;
-        }
-        const int col = (nx * P + ny) * P;
-        int zlo = t.z0 - rw.kz, zhi = t.z1 + rw.kz;
-        if (rw.kind == 1) zlo = t.z0;
-        double n = 0;
-        if (bpc) {
-            for (int z = zlo; z <= zhi; ++z) {
-                int zz = (z % P + P) % P;
-                n += cs[col + zz + 1] - cs[col + zz];
-            }
-        } else {
-            zlo = std::max(zlo, 0);
-            zhi = std::min(zhi, P - 1);
-            if (zlo <= zhi) n = cs[col + zhi + 1] - cs[col + zlo];
-        }
-        return n * t.count;
-    };
-    double total = 0;
-    std::vector<std::vector<double>> rc(plan.tiles.size());
-    for (size_t ti = 0; ti < plan.tiles.size(); ++ti) {
-        rc[ti].resize(plan.rows.size());
-        for (size_t ri = 0; ri < plan.rows.size(); ++ri) {
-            rc[ti][ri] = row_cost(plan.tiles[ti], plan.rows[ri]);
-            total += rc[ti][ri];
-        }
-    }
-    // ~12 items per resident warp (LPT order below) keeps the tail short
-    const double target = std::max(total / (double)(sm_count * 32 * 12), 1024.0);
-    struct CI { WorkItem w; double c; };
-    std::vector<CI> items;
-    for (size_t ti = 0; ti < plan.tiles.size(); ++ti) {
-        int rb = 0;
-        double acc = 0;
-        for (size_t ri = 0; ri < plan.rows.size(); ++ri) {
-            acc += rc[ti][ri];
-            if (acc >= target || ri + 1 == plan.rows.size() || (int)ri + 1 - rb >= 32) {
-                if (acc > 0) items.push_back({{(int)ti, rb, (int)ri + 1, cat}, acc});
-                rb = (int)ri + 1;
-                acc = 0;
-            }
-        }
-    }
-    std::stable_sort(items.begin(), items.end(), [](const CI &a, const CI &b) { return a.c > b.c; });
-    plan.items.clear();
-    plan.items.reserve(items.size());
-    for (auto &c : items) plan.items.push_back(c.w);
+    // ~16 items per resident warp keeps the tail short; at most 32 rows each
+    const int64_t nt = (int64_t)home.tiles.size();
+    const int64_t nr = (int64_t)plan.rows.size();
+    const int64_t want = std::max<int64_t>(1, (int64_t)resident_warps * 16);
+    int rpi = (int)std::min<int64_t>(32, std::max<int64_t>(1, (nt * nr) / want));
+    plan.rows_per_item = rpi;
+    plan.n_chunks = (int)((nr + rpi - 1) / rpi);
+    plan.n_items = nt * plan.n_chunks;
 }
 
 // ---------------------------------------------------------------------------
@@ -556,16 +486,67 @@ static FastCuts make_cuts(const PairRule &rule, float box, float dmax) {
 }
 
 template <bool ANI, bool W, int HM>
-static pcf_status launch_one(pcf_ctx *ctx, const PairArgs &A, size_t smem, int n_items) {
+static pcf_status launch_one(pcf_ctx *ctx, const PairArgs &A, size_t smem, long long n_items) {
     auto kfn = k_pairs<ANI, W, HM>;
-    if (smem > 48 * 1024)
+    // attribute / occupancy queries cost microseconds each: do them once per
+    // (variant, shared-memory size)
+    static thread_local size_t attr_smem = 0;
+    static thread_local size_t occ_smem = ~(size_t)0;
+    static thread_local int occ_per_sm = 1;
+    if (smem > 48 * 1024 && smem > attr_smem) {
         PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    PCF_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
-    per_sm = std::max(1, per_sm);
-    const int want = (n_items + kWarps - 1) / kWarps;
-    const int grid = std::max(1, std::min(want, ctx->sm_count * per_sm));
+        attr_smem = smem;
+    }
+    if (occ_smem != smem) {
+        int per = 0;
+        PCF_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem));
+        occ_per_sm = std::max(1, per);
+        occ_smem = smem;
+    }
+    const int per_sm = occ_per_sm;
+    const long long want = (n_items + kWarps - 1) / kWarps;
+    const int grid = (int)std::max(1LL, std::min<long long>(want, (long long)ctx->sm_count * per_sm));
     kfn<<<grid, kThreads, smem, ctx->stream>>>(A);
+    return PCF_OK;
+}
+
+// Copies the stencil rows into the next staging slot (pinned host ->
+// device).  Waits only for the kernel that used that slot two launches ago.
+pcf_status stage_plan(pcf_ctx *ctx, const PairPlan &plan, PlanSlot **out) {
+    cudaStream_t st = ctx->stream;
+    ctx->slot ^= 1;
+    PlanSlot &sl = ctx->slots[ctx->slot];
+    if (!sl.done) PCF_CU(ctx, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    if (sl.used) PCF_CU(ctx, cudaEventSynchronize(sl.done));
+    const size_t rb = plan.rows.size() * sizeof(RowDesc);
+    if (sl.h_bytes < rb) {
+        if (sl.h_pinned) cudaFreeHost(sl.h_pinned);
+        sl.h_pinned = nullptr;
+        sl.h_bytes = 0;
+        const size_t want = std::max<size_t>(rb * 2, 1 << 16);
+        PCF_CU(ctx, cudaMallocHost(&sl.h_pinned, want));
+        sl.h_bytes = want;
+    }
+    PCF_CU(ctx, sl.d_rows.ensure(rb));
+    PCF_CU(ctx, sl.d_counter.ensure(64));
+    memcpy(sl.h_pinned, plan.rows.data(), rb);
+    PCF_CU(ctx, cudaMemcpyAsync(sl.d_rows.p, sl.h_pinned, rb, cudaMemcpyHostToDevice, st));
+    PCF_CU(ctx, cudaMemsetAsync(sl.d_counter.p, 0, 64, st));
+    sl.used = true;
+    *out = &sl;
+    return PCF_OK;
+}
+
+pcf_status profile_events(pcf_ctx *ctx, cudaEvent_t *a, cudaEvent_t *b) {
+    if (ctx->prof_used == ctx->prof_events.size()) {
+        cudaEvent_t e0, e1;
+        PCF_CU(ctx, cudaEventCreate(&e0));
+        PCF_CU(ctx, cudaEventCreate(&e1));
+        ctx->prof_events.push_back({e0, e1});
+    }
+    *a = ctx->prof_events[ctx->prof_used].first;
+    *b = ctx->prof_events[ctx->prof_used].second;
+    ++ctx->prof_used;
     return PCF_OK;
 }
 
@@ -575,36 +556,21 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
                         unsigned long long *d_count, double *d_wsum,
                         unsigned long long *d_stats) {
     cudaStream_t st = ctx->stream;
-    if (plan.items.empty()) return PCF_OK;
-    size_t tb = plan.tiles.size() * sizeof(TileDesc);
-    size_t rb = plan.rows.size() * sizeof(RowDesc);
-    size_t ib = plan.items.size() * sizeof(WorkItem);
-    PCF_CU(ctx, ctx->d_tiles.ensure(tb));
-    PCF_CU(ctx, ctx->d_rows.ensure(rb));
-    PCF_CU(ctx, ctx->d_items.ensure(ib));
-    PCF_CU(ctx, ctx->d_counter.ensure(sizeof(int) * 16));
-    pcf_status s = pcf_ensure_pinned(ctx, tb + rb + ib + 64);
-    if (s != PCF_OK) return s;
-    // the staging buffer may still feed a previous copy on this stream
-    PCF_CU(ctx, cudaStreamSynchronize(st));
-    char *hp = static_cast<char *>(ctx->h_pinned);
-    memcpy(hp, plan.tiles.data(), tb);
-    memcpy(hp + tb, plan.rows.data(), rb);
-    memcpy(hp + tb + rb, plan.items.data(), ib);
-    PCF_CU(ctx, cudaMemcpyAsync(ctx->d_tiles.p, hp, tb, cudaMemcpyHostToDevice, st));
-    PCF_CU(ctx, cudaMemcpyAsync(ctx->d_rows.p, hp + tb, rb, cudaMemcpyHostToDevice, st));
-    PCF_CU(ctx, cudaMemcpyAsync(ctx->d_items.p, hp + tb + rb, ib, cudaMemcpyHostToDevice, st));
-    PCF_CU(ctx, cudaMemsetAsync(ctx->d_counter.p, 0, sizeof(int), st));
-
+    if (plan.n_items == 0) return PCF_OK;
+    PlanSlot *sl = nullptr;
+    pcf_status ps = stage_plan(ctx, plan, &sl);
+    if (ps != PCF_OK) return ps;
     PairArgs A;
     A.hx = home.x(); A.hy = home.y(); A.hz = home.z(); A.hw = home.w();
     A.cx = cand.x(); A.cy = cand.y(); A.cz = cand.z(); A.cw = cand.w();
     A.cstart = cand.cell_start.as<int>();
-    A.tiles = ctx->d_tiles.as<TileDesc>();
-    A.rows = ctx->d_rows.as<RowDesc>();
-    A.items = ctx->d_items.as<WorkItem>();
-    A.n_items = (int)plan.items.size();
-    A.counter = ctx->d_counter.as<int>();
+    A.tiles = home.d_tiles.as<TileDesc>();
+    A.rows = sl->d_rows.as<RowDesc>();
+    A.n_rows = (int)plan.rows.size();
+    A.rows_per_item = plan.rows_per_item;
+    A.n_chunks = plan.n_chunks;
+    A.n_items = plan.n_items;
+    A.counter = sl->d_counter.as<unsigned long long>();
     A.P = plan.P;
     A.box = box;
     A.bpc = pl.bpc ? 1 : 0;
@@ -624,6 +590,12 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     else if (!pl.ani && lane_bytes <= 64 * 1024) { hm = H_LANE; smem = lane_bytes; }
     else { hm = H_WARP; smem = warp_bytes; }
     PCF_CU(ctx, cudaEventRecord(ctx->ev0, st));
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    if (ctx->profile) {
+        pcf_status q = profile_events(ctx, &pe0, &pe1);
+        if (q != PCF_OK) return q;
+        PCF_CU(ctx, cudaEventRecord(pe0, st));
+    }
     pcf_status r = PCF_OK;
 #define PCF_DISPATCH(ANI_)                                                                   \
     if (pl.weighted) {                                                                       \
@@ -640,6 +612,8 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     if (r != PCF_OK) return r;
     PCF_CU(ctx, cudaGetLastError());
     PCF_CU(ctx, cudaEventRecord(ctx->ev1, st));
+    if (pe1) PCF_CU(ctx, cudaEventRecord(pe1, st));
+    PCF_CU(ctx, cudaEventRecord(sl->done, st));
     ++ctx->launches;
     return PCF_OK;
 }

@@ -90,14 +90,6 @@ struct RowDesc {
     int16_t dx, dy, kz, kind;
 };
 
-// One unit of the persistent work queue.
-struct WorkItem {
-    int tile;       // index into the tile table
-    int row_begin;  // rows [row_begin, row_end) of the stencil
-    int row_end;
-    int cat;        // catalog slot (batched launches), else 0
-};
-
 // Device view of a gridded catalog.
 struct CatView {
     const float4 *pts;      // cell-ordered points
@@ -107,9 +99,23 @@ struct CatView {
 // ---------------------------------------------------------------------------
 // Host-side objects.
 // ---------------------------------------------------------------------------
+// Stream-ordered caching allocator of one context: blocks released by a
+// grid are reused by later allocations on the same stream, so building and
+// freeing grids per request costs no cudaMalloc / cudaFree (each of which
+// synchronises the device).
+struct MemPool {
+    std::multimap<size_t, void *> free_blocks;
+    size_t cached = 0;
+    cudaError_t get(size_t n, void **p, size_t *got);
+    void put(void *p, size_t n);
+    void release();
+    ~MemPool() { release(); }
+};
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    std::shared_ptr<MemPool> pool;  // null: plain cudaMalloc / cudaFree
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
@@ -126,6 +132,8 @@ struct CellGrid {
     size_t plane = 0;             // floats per plane
     DevBuf cell_start;            // int x (P^3 + 1)
     std::vector<int> h_start;     // host copy of cell_start
+    std::vector<TileDesc> tiles;  // home tiles: <= 32 points of one cell
+    DevBuf d_tiles;
     const float *x() const { return soa.as<float>(); }
     const float *y() const { return soa.as<float>() + plane; }
     const float *z() const { return soa.as<float>() + 2 * plane; }
@@ -136,6 +144,7 @@ struct CellGrid {
 constexpr int kSoaPad = 4;
 
 struct pcf_grid {
+    std::shared_ptr<MemPool> pool;
     int64_t n = 0;
     float box = 0.f;
     bool unit_weights = true;
@@ -143,14 +152,31 @@ struct pcf_grid {
     std::unique_ptr<CellGrid> cells;
 };
 
+// One of two plan staging slots: while the device runs the kernel of one
+// call, the host builds and stages the plan of the next into the other.
+struct PlanSlot {
+    void *h_pinned = nullptr;
+    size_t h_bytes = 0;
+    DevBuf d_rows, d_counter;
+    cudaEvent_t done = nullptr;  // recorded after the kernel that read this slot
+    bool used = false;
+};
+
 struct pcf_ctx {
+    std::shared_ptr<MemPool> pool = std::make_shared<MemPool>();
+    PlanSlot slots[2];
+    int slot = 0;
+    // optional kernel-time log (pcf_ctx_profile)
+    bool profile = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+    size_t prof_used = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int sm_count = 148;
     std::string last_error;
     // scratch reused across calls
-    DevBuf scratch_a, scratch_b, scratch_c, d_hist, d_items, d_tiles, d_rows, d_counter;
+    DevBuf scratch_a, scratch_b, scratch_c, d_hist;
     DevBuf d_flag;
     void *h_pinned = nullptr;
     size_t h_pinned_bytes = 0;
@@ -170,18 +196,24 @@ pcf_status pcf_fail(pcf_ctx *ctx, cudaError_t e, const char *what);
 pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P);
 int choose_partitions(int64_t n, float box, float dmax, int kind, bool bpc, int npoint_kind);
 
-// Stencil / tiles / work-list construction (host).
+// Stencil of one pair launch (host).  Work items are implicit: item i is
+// (tile i / n_chunks, rows [c*rows_per_item, ...) of chunk c = i % n_chunks).
 struct PairPlan {
     int P;
     float cell;
-    std::vector<TileDesc> tiles;
     std::vector<RowDesc> rows;
-    std::vector<WorkItem> items;
+    int rows_per_item = 1;
+    int n_chunks = 1;
+    int64_t n_items = 0;
 };
 
-// Builds the work plan of one pair launch.  self: XX half shell.
-void plan_pairs(const CellGrid &home, const CellGrid *cand, float box, float dmax, bool ani,
-                bool bpc, bool self, int tile_cap, int cat, PairPlan &plan, int sm_count);
+constexpr int kTileCap = 32;  // home points per warp item
+// Home tiles of a gridded catalog: each non-empty cell, sliced into runs
+// of at most kTileCap points.
+void build_tiles(CellGrid &g);
+// Builds the stencil and item shape of one pair launch.  self: XX half shell.
+void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self, PairPlan &plan,
+                int resident_warps);
 
 pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes);
 
@@ -197,5 +229,7 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
 pcf_status finalize_hist(pcf_ctx *ctx, const unsigned long long *d_count, const double *d_wsum,
                          bool weighted, double mult, int nb, double *d_out);
 PairRule make_pair_rule(int bins, float dmax, uint32_t flags, bool ani, bool bpc, bool cross);
+pcf_status stage_plan(pcf_ctx *ctx, const PairPlan &plan, PlanSlot **out);
+pcf_status profile_events(pcf_ctx *ctx, cudaEvent_t *a, cudaEvent_t *b);
 pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int kind, bool bpc,
                          int *P_out);

@@ -21,6 +21,12 @@ pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
 /* Kernels this context has launched since it was created. */
 int64_t pcf_ctx_launch_count(const pcf_ctx *ctx);
 
+/* Kernel-time log: while enabled, every counting kernel is bracketed by CUDA
+ * events on the context stream.  _read synchronises the stream, returns the
+ * summed kernel time and the number of logged launches, and clears the log. */
+pcf_status pcf_ctx_profile(pcf_ctx *ctx, int enable);
+pcf_status pcf_ctx_profile_read(pcf_ctx *ctx, double *total_ms, int64_t *launches);
+
 #ifdef __cplusplus
 }
 #endif
