@@ -223,7 +223,7 @@ def run_ours(args, rank, world, local_rank):
     smem_peak = ctx.microbench(1)
     achieved = 8.0 * k_pairs / (k_ms * 1e-3) / 1e12
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "pairs_c2_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "k_pairs_c2_traffic.json")
     if os.path.exists(prof):
         try:
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")

@@ -230,6 +230,8 @@ pcf_status finalize_hist(pcf_ctx *ctx, const unsigned long long *d_count, const 
                          bool weighted, double mult, int nb, double *d_out);
 PairRule make_pair_rule(int bins, float dmax, uint32_t flags, bool ani, bool bpc, bool cross);
 pcf_status stage_plan(pcf_ctx *ctx, const PairPlan &plan, PlanSlot **out);
+pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x, const pcf_grid *y, int bins,
+                                  float dmax, uint32_t flags, double *hist, pcf_stats *stats);
 pcf_status profile_events(pcf_ctx *ctx, cudaEvent_t *a, cudaEvent_t *b);
 pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int kind, bool bpc,
                          int *P_out);

@@ -1,0 +1,497 @@
+// triplets.cu -- isotropic triplet histograms DDD / RRR / DDR / DRR on the
+// CUDA cores.
+//
+// Reference kernels replaced: XXX3iso / XXY3iso (cuda/kernels/3iso_k.cuh:8,94)
+// and the periodic count123 / count123_mixed / XXX3iso_BPC / XXY3iso_BPC
+// (cuda/kernels/3isoBPC_k.cuh:8,98,191,940), which run one thread per cell
+// *triple* with a global FP64 atomic per triangle and spell out 64 image
+// combinations.  Here:
+//
+//  * A persistent CTA takes one anchor point i at a time.  It scans the
+//    anchor's neighbour cells (the pair stencil, periodic images by index
+//    wrap) and compacts into shared memory the X neighbours j > i (list J)
+//    and, for XXY, all Y neighbours (list K), each with its FP32 image
+//    displacement from i and its exact side bin (FP32 fast path + FP64
+//    recheck, as in the pair kernel).
+//  * It then runs the pairs of that list: XXX pairs (j < k) of J, XXY all of
+//    J x K.  The third side is |v_k - v_j| -- the consistent embedding of
+//    count123 (3isoBPC_k.cuh:56-75) -- tested and binned in FP32 with the
+//    same edge-window recheck.  Each unordered XXX triangle is seen once (i
+//    its lowest index), each unordered XX pair of an XXY triangle once.
+//  * Counts go to a shared u32 histogram U[b_ij][b_jk][b_ki] (one
+//    orientation per triangle); the finalize pass symmetrises it into the
+//    reference's ordered-triple histogram: XXX sums the 6 axis
+//    permutations, XXY the two orders of the XX pair (b_jk <-> b_ki).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "pcf_internal.cuh"
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kTThreads = 512;  // 16 warps, one CTA per SM
+constexpr int kTWarps = kTThreads / 32;
+constexpr float kMagic = 256.0f;
+constexpr int kFracBits = 15;
+constexpr unsigned kFracMask = (1u << kFracBits) - 1u;
+
+struct TripCuts {
+    float dsf, ds2;
+    float lo, hi;  // d2 window around dd (image-aware bound for periodic boxes)
+    unsigned w;    // edge window, 2^-15 units of r
+};
+
+struct Cat {
+    const float *x, *y, *z, *w;
+    const int *cstart;
+};
+
+struct TripArgs {
+    Cat X, Y;
+    int nX;
+    const RowDesc *rows;
+    int n_rows;
+    int P;
+    float cell;
+    float box;
+    int bpc;
+    PairRule rXX, rXY;  // side rules (X-X side, X-Y sides)
+    TripCuts fc;
+    int capJ, capK;          // shared-memory list capacities (entries)
+    float4 *gJ, *gK;         // per-CTA overflow lists in global memory
+    float *gwJ, *gwK;        // weights of the overflow lists
+    int gcap;                // entries per CTA in the overflow lists
+    unsigned long long *counter;
+    unsigned long long *g_count;  // bins^3 (unit weights)
+    double *g_wsum;               // bins^3 (weighted)
+    int hist_in_smem;
+    unsigned long long *g_stats;
+};
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ bool fix_safe(unsigned q, unsigned w) {
+    return ((q + w) & kFracMask) >= 2u * w;
+}
+
+// Exact FP64 side between two catalog points (minimum image when periodic),
+// returned as components.
+__device__ __forceinline__ void sep_exact(float ax, float ay, float az, float bx, float by,
+                                          float bz, int bpc, double L, double &dx, double &dy,
+                                          double &dz) {
+    dx = __dsub_rn((double)bx, (double)ax);
+    dy = __dsub_rn((double)by, (double)ay);
+    dz = __dsub_rn((double)bz, (double)az);
+    if (bpc) {
+        const double h = 0.5 * L;
+        if (dx > h) dx = __dsub_rn(dx, L); else if (dx < -h) dx = __dadd_rn(dx, L);
+        if (dy > h) dy = __dsub_rn(dy, L); else if (dy < -h) dy = __dadd_rn(dy, L);
+        if (dz > h) dz = __dsub_rn(dz, L); else if (dz < -h) dz = __dadd_rn(dz, L);
+    }
+}
+
+// Side bin of the anchor -> candidate pair in the canonical FP64 rule.
+__device__ __noinline__ int exact_side(float ax, float ay, float az, float bx, float by, float bz,
+                                       int bpc, float box, PairRule rule) {
+    double dx, dy, dz;
+    sep_exact(ax, ay, az, bx, by, bz, bpc, (double)box, dx, dy, dz);
+    return exact_slot<false>(dx, dy, dz, rule);
+}
+
+// Bin of side j-k in the consistent embedding anchored at i: v_jk = v_ik - v_ij.
+__device__ __noinline__ int exact_third(float ix, float iy, float iz, float jx, float jy, float jz,
+                                        float kx, float ky, float kz, int bpc, float box,
+                                        PairRule rule) {
+    double ax, ay, az, bx, by, bz;
+    sep_exact(ix, iy, iz, jx, jy, jz, bpc, (double)box, ax, ay, az);
+    sep_exact(ix, iy, iz, kx, ky, kz, bpc, (double)box, bx, by, bz);
+    return exact_slot<false>(__dsub_rn(bx, ax), __dsub_rn(by, ay), __dsub_rn(bz, az), rule);
+}
+
+// FP32 fast-path bin of a squared distance, or -1 (recheck needed), -2 (out).
+__device__ __forceinline__ int fast_bin(float d2, const TripCuts &c, int bins) {
+    if (!(d2 < c.hi)) return -2;
+    const float r = sqrt_approx(d2 * c.ds2);
+    const unsigned q = __float_as_uint(r + kMagic) & 0x7FFFFFu;
+    if (d2 < c.lo && fix_safe(q, c.w)) return min((int)(q >> kFracBits), bins - 1);
+    return -1;
+}
+
+// Appends the neighbours of anchor (hx,hy,hz) found in catalog C to a list.
+// only_after >= 0 keeps candidates with index > only_after (X list of XXX /
+// XXY).  Entries: {dx, dy, dz, bits(idx << 8 | bin)}.
+__device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, float hz, int hcell_ix,
+                           int hcell_iy, int hcell_iz, int only_after, const PairRule &rule,
+                           float4 *list, float *wlist, int cap, int *s_n, unsigned &n_rechk) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int P = A.P;
+    for (int r = 0; r < A.n_rows; ++r) {
+        const RowDesc rw = A.rows[r];
+        int nx = hcell_ix + rw.dx, ny = hcell_iy + rw.dy;
+        float sx = 0.f, sy = 0.f;
+        if (A.bpc) {
+            if (nx < 0) { nx += P; sx = -A.box; } else if (nx >= P) { nx -= P; sx = A.box; }
+            if (ny < 0) { ny += P; sy = -A.box; } else if (ny >= P) { ny -= P; sy = A.box; }
+        } else if (nx < 0 || nx >= P || ny < 0 || ny >= P) {
+            continue;
+        }
+        const int col = (nx * P + ny) * P;
+        const int zlo = hcell_iz - rw.kz, zhi = hcell_iz + rw.kz;
+        int ra[2], rb[2];
+        float rz[2] = {0.f, 0.f};
+        ra[0] = C.cstart[col + max(zlo, 0)];
+        rb[0] = C.cstart[col + min(zhi, P - 1) + 1];
+        ra[1] = rb[1] = 0;
+        if (A.bpc) {
+            if (zlo < 0) { ra[1] = C.cstart[col + zlo + P]; rb[1] = C.cstart[col + P]; rz[1] = -A.box; }
+            else if (zhi >= P) { ra[1] = C.cstart[col]; rb[1] = C.cstart[col + zhi - P + 1]; rz[1] = A.box; }
+        }
+        for (int sgi = 0; sgi < 2; ++sgi) {
+            int a = ra[sgi];
+            const int b = rb[sgi];
+            if (only_after >= 0) a = max(a, only_after + 1);
+            if (a >= b) continue;
+            const float ex = hx - sx, ey = hy - sy, ez = hz - rz[sgi];
+            // warps take 32-candidate chunks
+            for (int base = a + warp * 32; base < b; base += kTWarps * 32) {
+                const int c = base + lane;
+                int bin = -2;
+                float vx = 0.f, vy = 0.f, vz = 0.f;
+                if (c < b) {
+                    vx = C.x[c] - ex;
+                    vy = C.y[c] - ey;
+                    vz = C.z[c] - ez;
+                    const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
+                    bin = fast_bin(d2, A.fc, rule.bins);
+                    if (bin == -1) {
+                        ++n_rechk;
+                        bin = exact_side(hx, hy, hz, C.x[c], C.y[c], C.z[c], A.bpc, A.box, rule);
+                    }
+                }
+                const bool keep = bin >= 0;
+                const unsigned m = __ballot_sync(kFull, keep);
+                int off = 0;
+                if (lane == 0 && m) off = atomicAdd(s_n, __popc(m));
+                off = __shfl_sync(kFull, off, 0);
+                if (keep) {
+                    const int pos = off + __popc(m & ((1u << lane) - 1u));
+                    if (pos < cap) {
+                        list[pos] = make_float4(vx, vy, vz, __int_as_float((c << 8) | bin));
+                        if (wlist) wlist[pos] = C.w[c];
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <bool MIXED, bool WEIGHTED>
+__global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int bins = A.rXX.bins;
+    const int nb3 = bins * bins * bins;
+    unsigned *U = reinterpret_cast<unsigned *>(smem);
+    const size_t u_bytes = A.hist_in_smem ? (((size_t)nb3 * 4 + 15) & ~(size_t)15) : 0;
+    float4 *sJ = reinterpret_cast<float4 *>(smem + u_bytes);
+    float4 *sK = sJ + A.capJ;
+    float *swJ = reinterpret_cast<float *>(sK + (MIXED ? A.capK : 0));
+    float *swK = swJ + (WEIGHTED ? A.capJ : 0);
+    __shared__ int s_anchor, s_nJ, s_nK;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (A.hist_in_smem)
+        for (int k = tid; k < nb3; k += kTThreads) U[k] = 0u;
+    unsigned n_rechk = 0;
+    unsigned long long n_tri = 0;
+    __syncthreads();
+    float4 *gJ = A.gJ + (size_t)blockIdx.x * A.gcap;
+    float4 *gK = A.gK ? A.gK + (size_t)blockIdx.x * A.gcap : nullptr;
+    float *gwJ = A.gwJ ? A.gwJ + (size_t)blockIdx.x * A.gcap : nullptr;
+    float *gwK = A.gwK ? A.gwK + (size_t)blockIdx.x * A.gcap : nullptr;
+
+    for (;;) {
+        if (tid == 0) {
+            s_anchor = (int)atomicAdd(A.counter, 1ull);
+            s_nJ = 0;
+            s_nK = 0;
+        }
+        __syncthreads();
+        const int i = s_anchor;
+        if (i >= A.nX) break;
+        const float hx = A.X.x[i], hy = A.X.y[i], hz = A.X.z[i];
+        const float hw = WEIGHTED ? A.X.w[i] : 1.f;
+        const int P = A.P;
+        const int cix = min(max((int)__fdiv_rn(hx, A.cell), 0), P - 1);
+        const int ciy = min(max((int)__fdiv_rn(hy, A.cell), 0), P - 1);
+        const int ciz = min(max((int)__fdiv_rn(hz, A.cell), 0), P - 1);
+        // pass 1: lists into shared memory (sizes counted even past capacity)
+        build_list(A, A.X, hx, hy, hz, cix, ciy, ciz, i, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
+                   A.capJ, &s_nJ, n_rechk);
+        if (MIXED)
+            build_list(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK, WEIGHTED ? swK : nullptr,
+                       A.capK, &s_nK, n_rechk);
+        __syncthreads();
+        int nJ = s_nJ, nK = MIXED ? s_nK : nJ;
+        const float4 *LJ = sJ;
+        const float4 *LK = MIXED ? sK : sJ;
+        const float *WJ = swJ, *WK = MIXED ? swK : swJ;
+        if (nJ > A.capJ || (MIXED && nK > A.capK)) {
+            // overflow: rebuild the lists in this CTA's global scratch (L2)
+            __syncthreads();
+            if (tid == 0) { s_nJ = 0; s_nK = 0; }
+            __syncthreads();
+            build_list(A, A.X, hx, hy, hz, cix, ciy, ciz, i, A.rXX, gJ, WEIGHTED ? gwJ : nullptr,
+                       A.gcap, &s_nJ, n_rechk);
+            if (MIXED)
+                build_list(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, gK,
+                           WEIGHTED ? gwK : nullptr, A.gcap, &s_nK, n_rechk);
+            __threadfence_block();
+            __syncthreads();
+            nJ = min(s_nJ, A.gcap);
+            nK = MIXED ? min(s_nK, A.gcap) : nJ;
+            LJ = gJ;
+            LK = MIXED ? gK : gJ;
+            WJ = gwJ;
+            WK = MIXED ? gwK : gwJ;
+        }
+        // pass 2: pairs of neighbours.  Rows j are dealt to warps in the
+        // order 0, n-1, 1, n-2, ... (XXX rows shrink with j).
+        for (int rr = warp; rr < nJ; rr += kTWarps) {
+            const int half = rr >> 1;
+            const int jj = MIXED ? rr : ((rr & 1) ? nJ - 1 - half : half);
+            const float4 ej = LJ[jj];
+            const int bj = __float_as_int(ej.w) & 255;
+            const int jidx = (int)((unsigned)__float_as_int(ej.w) >> 8);
+            const double wij = WEIGHTED ? (double)hw * (double)WJ[jj] : 1.0;
+            const int ubase = bj * bins * bins;
+            const int k0 = MIXED ? 0 : jj + 1;
+            for (int kk = k0 + lane; kk < nK; kk += 32) {
+                const float4 ek = LK[kk];
+                const float dx = ek.x - ej.x, dy = ek.y - ej.y, dz = ek.z - ej.z;
+                const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                const PairRule &r3 = MIXED ? A.rXY : A.rXX;
+                int bjk = fast_bin(d2, A.fc, bins);
+                if (bjk == -1) {
+                    ++n_rechk;
+                    const int kidx = (int)((unsigned)__float_as_int(ek.w) >> 8);
+                    const Cat &CK = MIXED ? A.Y : A.X;
+                    bjk = exact_third(hx, hy, hz, A.X.x[jidx], A.X.y[jidx], A.X.z[jidx],
+                                      CK.x[kidx], CK.y[kidx], CK.z[kidx], A.bpc, A.box, r3);
+                }
+                if (bjk >= 0) {
+                    const int bk = __float_as_int(ek.w) & 255;
+                    const int slot = ubase + bjk * bins + bk;
+                    ++n_tri;
+                    if (WEIGHTED) {
+                        atomicAdd(A.g_wsum + slot, wij * (double)WK[kk]);
+                    } else if (A.hist_in_smem) {
+                        atomicAdd(U + slot, 1u);
+                    } else {
+                        atomicAdd(A.g_count + slot, 1ull);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (A.hist_in_smem) {
+        for (int k = tid; k < nb3; k += kTThreads)
+            if (U[k]) atomicAdd(A.g_count + k, (unsigned long long)U[k]);
+    }
+    unsigned long long rr = n_rechk;
+    for (int off = 16; off > 0; off >>= 1) {
+        rr += __shfl_down_sync(kFull, rr, off);
+        n_tri += __shfl_down_sync(kFull, n_tri, off);
+    }
+    if (lane == 0) {
+        if (rr) atomicAdd(A.g_stats + 0, rr);
+        if (n_tri) atomicAdd(A.g_stats + 2, n_tri);
+    }
+}
+
+// Ordered-triple histogram from the oriented counts U[b_ij][b_jk][b_ki].
+__global__ void k_trip_finalize(const unsigned long long *__restrict__ cnt,
+                                const double *__restrict__ ws, int weighted, int mixed, int bins,
+                                double *__restrict__ out) {
+    const int n3 = bins * bins * bins;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    const int a = t / (bins * bins), b = (t / bins) % bins, c = t % bins;
+    auto U = [&](int x, int y, int z) -> double {
+        const int s = (x * bins + y) * bins + z;
+        return weighted ? ws[s] : (double)cnt[s];
+    };
+    double v;
+    if (mixed) v = U(a, b, c) + U(a, c, b);
+    else v = U(a, b, c) + U(b, c, a) + U(c, a, b) + U(a, c, b) + U(c, b, a) + U(b, a, c);
+    out[t] = v;
+}
+
+}  // namespace
+
+extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid *x_,
+                                         const pcf_grid *y_, int bins, float dmax, uint32_t flags,
+                                         double *hist, pcf_stats *stats) {
+    if (!ctx || !x_ || !hist || bins < 1 || !(dmax > 0.f)) return PCF_ERR_INVALID_ARG;
+    if (kind == PCF_ANI) return pcf_count_triplets_ani(ctx, x_, y_, bins, dmax, flags, hist, stats);
+    if (kind != PCF_ISO) return PCF_ERR_INVALID_ARG;
+    if (bins > 255 || (int64_t)bins * bins * bins > (1 << 26)) return PCF_ERR_UNSUPPORTED;
+    cudaSetDevice(ctx->device);
+    pcf_grid *X = const_cast<pcf_grid *>(x_);
+    pcf_grid *Y = const_cast<pcf_grid *>(y_);
+    const bool bpc = (flags & PCF_BPC) != 0, mixed = Y != nullptr;
+    if (X->n >= (1 << 24) || (Y && Y->n >= (1 << 24))) return PCF_ERR_UNSUPPORTED;
+    int P = 0;
+    pcf_status s = prepare_grids(ctx, X, Y, dmax, PCF_ISO, bpc, &P);
+    if (s != PCF_OK) return s;
+    const CellGrid &gx = *X->cells;
+    const CellGrid &gy = mixed ? *Y->cells : gx;
+    PairPlan plan;
+    plan_pairs(gx, X->box, dmax, false, false, plan, ctx->sm_count * 24);
+
+    // side rules: X-X sides need d > 0; X-Y sides only with periodic boxes
+    // (3iso_k.cuh:158,160 vs 3isoBPC_k.cuh:165,170)
+    PairRule rXX = make_pair_rule(bins, dmax, flags & ~PCF_DS_EXACT, false, bpc, false);
+    PairRule rXY = rXX;
+    rXY.flags = bpc ? PCF_RULE_EXCL : 0u;
+    if (flags & PCF_RULE_CUSTOM) rXY.flags = rXX.flags;
+    TripArgs A;
+    A.X = {gx.x(), gx.y(), gx.z(), gx.w(), gx.cell_start.as<int>()};
+    A.Y = {gy.x(), gy.y(), gy.z(), gy.w(), gy.cell_start.as<int>()};
+    A.nX = (int)X->n;
+    A.n_rows = (int)plan.rows.size();
+    A.P = P;
+    A.cell = gx.cell;
+    A.box = X->box;
+    A.bpc = bpc ? 1 : 0;
+    A.rXX = rXX;
+    A.rXY = rXY;
+    {
+        // windows: the FP32 side |v_k - v_j| carries up to three roundings of
+        // coordinate differences (plus the image shift of the anchor when
+        // periodic); the bounds below keep a >= 8x margin
+        const double dd = rXX.dd;
+        const double rmax = (double)dmax * rXX.ds + 1.0;
+        const double Lx = bpc ? (double)X->box : (double)dmax;
+        const double e_d2 = dd * std::ldexp(1.0, -17) + (double)dmax * Lx * std::ldexp(1.0, -18);
+        const double wr = rmax * std::ldexp(1.0, -17) + rXX.ds * Lx * std::ldexp(1.0, -18);
+        A.fc.dsf = (float)rXX.ds;
+        A.fc.ds2 = A.fc.dsf * A.fc.dsf;
+        A.fc.lo = (float)(dd - e_d2);
+        A.fc.hi = (float)(dd + e_d2);
+        A.fc.w = std::min(8000u, (unsigned)std::ceil((wr + std::ldexp(1.0, -16)) * 32768.0) + 1u);
+    }
+    const bool weighted = !(X->unit_weights && (!mixed || Y->unit_weights));
+    const int n3 = bins * bins * bins;
+    const size_t u_bytes = ((size_t)n3 * 4 + 15) & ~(size_t)15;
+    const size_t smem_max = 227 * 1024 - 64;
+    A.hist_in_smem = (!weighted && u_bytes <= 150 * 1024) ? 1 : 0;
+    const size_t hist_b = A.hist_in_smem ? u_bytes : 0;
+    const size_t ent = 16 + (weighted ? 4 : 0);
+    const size_t room = smem_max - hist_b;
+    if (mixed) {
+        A.capJ = (int)(room / ent / 3);
+        A.capK = (int)(room / ent) - A.capJ;
+    } else {
+        A.capJ = (int)(room / ent);
+        A.capK = 0;
+    }
+    const size_t smem = hist_b + (size_t)(A.capJ + A.capK) * ent;
+    // overflow lists: bounded by the largest stencil population of any cell
+    auto max_stencil = [&](const CellGrid &g) -> int64_t {
+        const std::vector<int> &cs = g.h_start;
+        int64_t best = 0;
+        for (int ix = 0; ix < P; ++ix)
+            for (int iy = 0; iy < P; ++iy)
+                for (int iz = 0; iz < P; ++iz) {
+                    int64_t n = 0;
+                    for (const RowDesc &rw : plan.rows) {
+                        int nx = ix + rw.dx, ny = iy + rw.dy;
+                        if (bpc) { nx = (nx + P) % P; ny = (ny + P) % P; }
+                        else if (nx < 0 || nx >= P || ny < 0 || ny >= P) continue;
+                        const int col = (nx * P + ny) * P;
+                        const int zlo = iz - rw.kz, zhi = iz + rw.kz;
+                        const int lo = std::max(zlo, 0), hi = std::min(zhi, P - 1);
+                        if (lo <= hi) n += cs[col + hi + 1] - cs[col + lo];
+                        if (bpc && zlo < 0) n += cs[col + P] - cs[col + zlo + P];
+                        if (bpc && zhi >= P) n += cs[col + zhi - P + 1] - cs[col];
+                    }
+                    best = std::max(best, n);
+                }
+        return best;
+    };
+    const int64_t gmax = std::max<int64_t>(max_stencil(gx), mixed ? max_stencil(gy) : 0) + 32;
+    const int grid = ctx->sm_count;
+    A.gcap = (int)std::min<int64_t>(gmax, 1 << 24);
+    PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(float4) * (size_t)A.gcap * grid * (mixed ? 2 : 1) +
+                                      (weighted ? sizeof(float) * (size_t)A.gcap * grid * 2 : 0) + 256));
+    char *sc = ctx->scratch_c.as<char>();
+    A.gJ = reinterpret_cast<float4 *>(sc);
+    A.gK = mixed ? A.gJ + (size_t)A.gcap * grid : nullptr;
+    float *wbase = reinterpret_cast<float *>(sc + sizeof(float4) * (size_t)A.gcap * grid * (mixed ? 2 : 1));
+    A.gwJ = weighted ? wbase : nullptr;
+    A.gwK = weighted && mixed ? wbase + (size_t)A.gcap * grid : nullptr;
+
+    // rows + counter through the plan slot
+    PlanSlot *sl = nullptr;
+    s = stage_plan(ctx, plan, &sl);
+    if (s != PCF_OK) return s;
+    A.rows = sl->d_rows.as<RowDesc>();
+    A.counter = sl->d_counter.as<unsigned long long>();
+    // histogram scratch: [u64 n3][f64 n3][stats 8][f64 out n3]
+    PCF_CU(ctx, ctx->d_hist.ensure((size_t)n3 * 24 + 64));
+    char *hp = ctx->d_hist.as<char>();
+    A.g_count = reinterpret_cast<unsigned long long *>(hp);
+    A.g_wsum = reinterpret_cast<double *>(hp + (size_t)n3 * 8);
+    A.g_stats = reinterpret_cast<unsigned long long *>(hp + (size_t)n3 * 16);
+    double *d_out = reinterpret_cast<double *>(hp + (size_t)n3 * 16 + 64);
+    PCF_CU(ctx, cudaMemsetAsync(hp, 0, (size_t)n3 * 16 + 64, ctx->stream));
+
+    auto kfn = mixed ? (weighted ? k_triplets<true, true> : k_triplets<true, false>)
+                     : (weighted ? k_triplets<false, true> : k_triplets<false, false>);
+    PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    if (ctx->profile) {
+        s = profile_events(ctx, &pe0, &pe1);
+        if (s != PCF_OK) return s;
+        PCF_CU(ctx, cudaEventRecord(pe0, ctx->stream));
+    }
+    PCF_CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    kfn<<<grid, kTThreads, smem, ctx->stream>>>(A);
+    PCF_CU(ctx, cudaGetLastError());
+    PCF_CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    if (pe1) PCF_CU(ctx, cudaEventRecord(pe1, ctx->stream));
+    PCF_CU(ctx, cudaEventRecord(sl->done, ctx->stream));
+    ++ctx->launches;
+    const bool dev_out = (flags & PCF_DEVICE_OUT) != 0;
+    k_trip_finalize<<<(n3 + 255) / 256, 256, 0, ctx->stream>>>(A.g_count, A.g_wsum, weighted ? 1 : 0,
+                                                                mixed ? 1 : 0, bins,
+                                                                dev_out ? hist : d_out);
+    PCF_CU(ctx, cudaGetLastError());
+    ++ctx->launches;
+    if (!dev_out)
+        PCF_CU(ctx, cudaMemcpyAsync(hist, d_out, sizeof(double) * n3, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    if (stats || !dev_out) {
+        unsigned long long hs[4] = {0, 0, 0, 0};
+        PCF_CU(ctx, cudaMemcpyAsync(hs, A.g_stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+        PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        if (stats) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            stats->pairs = (double)hs[2];  // unordered triangles (XXY: per unordered XX pair)
+            stats->candidates = 0;
+            stats->rechecks = (double)hs[0];
+            stats->kernel_ms = ms;
+            stats->partitions = P;
+            stats->work_items = (int)X->n;
+        }
+    }
+    return PCF_OK;
+}

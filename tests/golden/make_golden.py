@@ -11,13 +11,14 @@ Writes:
                  reference files; checked here)
   golden_3iso.npz  int64 DDD, DDR, DRR, RRR (the .example values are integers)
 Usage: python tests/golden/make_golden.py [/path/to/reference]
+       python tests/golden/make_golden.py --fp64   (FP64-oracle histograms, see fp64_fixture)
 """
 import os
 import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = next((a for a in sys.argv[1:] if not a.startswith("--")), "/root/reference")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -42,5 +43,31 @@ def main():
     print({k: v.shape for k, v in cats.items()}, {k: int(v.sum()) for k, v in gold.items()})
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and "--fp64" not in sys.argv:
     main()
+
+
+def fp64_fixture():
+    """FP64-oracle histograms of the golden configuration (plain 3iso,
+    data.dat / rand0.dat, 32768 points, 30 bins, dmax 60, box 251 -- the
+    reference's auto box ceil(max+1)) for the full-size GPU parity test."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(OUT)))
+    import oracle
+    z = np.load(os.path.join(OUT, "catalogs.npz"))
+    one = lambda a: np.ascontiguousarray(
+        np.concatenate([a, np.ones((len(a), 1), np.float32)], 1).astype(np.float32))
+    D, R = one(z["data"]), one(z["rand0"])
+    kw = dict(box=251.0, bins=30, dmax=60.0)
+    res = {
+        "DDD": oracle.triplets_iso(D, **kw),
+        "RRR": oracle.triplets_iso(R, **kw),
+        "DDR": oracle.triplets_iso(D, R, **kw),
+        "DRR": oracle.triplets_iso(R, D, **kw),
+    }
+    np.savez_compressed(os.path.join(OUT, "golden_3iso_fp64.npz"),
+                        **{k: v.astype(np.int64) for k, v in res.items()})
+    print({k: int(v.sum()) for k, v in res.items()})
+
+
+if __name__ == "__main__" and "--fp64" in sys.argv:
+    fp64_fixture()
