@@ -78,6 +78,9 @@ _SIGS = {
     "pcf_autotune_partitions": (ctypes.c_int, [_vp, _i64, ctypes.c_float, ctypes.c_float,
                                                ctypes.c_int, ctypes.c_uint32]),
     "pcf_microbench": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "pcf_count_pairs_noalloc": (ctypes.c_int, [_vp, _i64, _vp, _i64, ctypes.c_float, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_float, ctypes.c_uint32, _vp,
+                                               _vp]),
     "pcf_ctx_launch_count": (_i64, [_vp]),
     "pcf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pcf_ctx_profile_read": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double),

@@ -135,7 +135,7 @@ __global__ void k_scatter(const float4 *__restrict__ pts, int64_t n, const int *
     if (i >= n) return;
     const float4 p = pts[i];
     const int64_t d = start[cid[i]] + rank[i];
-    out[d] = p;
+    if (out) out[d] = p;
     soa[d] = p.x;
     soa[plane + d] = p.y;
     soa[2 * plane + d] = p.z;
@@ -159,7 +159,53 @@ int scan_exclusive(const int *in, int *out, int64_t n, int *tmp, cudaStream_t st
     return launches;
 }
 
+__global__ void k_tile_counts(const int *__restrict__ start, int ncell, int *__restrict__ tc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > ncell) return;
+    tc[c] = c < ncell ? (start[c + 1] - start[c] + kTileCap - 1) / kTileCap : 0;
+}
+
+__global__ void k_tile_emit(const int *__restrict__ start, const int *__restrict__ toff, int P,
+                            TileDesc *__restrict__ tiles) {
+    const int ncell = P * P * P;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const int s0 = start[c], n = start[c + 1] - s0;
+    const int iz = c % P, iy = (c / P) % P, ix = c / (P * P);
+    int o = toff[c];
+    for (int k = 0; k < n; k += kTileCap, ++o) {
+        TileDesc t;
+        t.start = s0 + k;
+        t.count = min(kTileCap, n - k);
+        t.ix = (int16_t)ix;
+        t.iy = (int16_t)iy;
+        t.z0 = t.z1 = (int16_t)iz;
+        tiles[o] = t;
+    }
+}
+
 }  // namespace
+
+int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
+                      int *rank, int *counts, int *cell_start, int *scan_tmp, float4 *pts_out,
+                      float *soa, size_t plane, int *flags, cudaStream_t st) {
+    const int64_t ncell = (int64_t)P * P * P;
+    const int thr = 256;
+    const unsigned blocks = (unsigned)((n + thr - 1) / thr);
+    k_cell_ids<<<blocks, thr, 0, st>>>(raw, n, P, cell, box, cid, rank, counts, flags);
+    int launches = 1 + scan_exclusive(counts, cell_start, ncell + 1, scan_tmp, st);
+    k_scatter<<<blocks, thr, 0, st>>>(raw, n, cid, rank, cell_start, pts_out, soa, plane);
+    return launches + 1;
+}
+
+int launch_tile_build(const int *cell_start, int P, int *tile_counts, int *tile_offsets,
+                      int *scan_tmp, TileDesc *tiles, cudaStream_t st) {
+    const int ncell = P * P * P;
+    k_tile_counts<<<(ncell + 1 + 255) / 256, 256, 0, st>>>(cell_start, ncell, tile_counts);
+    int launches = 1 + scan_exclusive(tile_counts, tile_offsets, ncell + 1, scan_tmp, st);
+    k_tile_emit<<<(ncell + 255) / 256, 256, 0, st>>>(cell_start, tile_offsets, P, tiles);
+    return launches + 1;
+}
 
 pcf_status pcf_fail(pcf_ctx *ctx, cudaError_t e, const char *what) {
     if (ctx) {
@@ -207,17 +253,9 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     int *flags = ctx->d_flag.as<int>();
     PCF_CU(ctx, cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)(ncell + 1), st));
     PCF_CU(ctx, cudaMemsetAsync(flags, 0, sizeof(int), st));
-    const int thr = 256;
-    unsigned blocks = (unsigned)((n + thr - 1) / thr);
-    k_cell_ids<<<blocks, thr, 0, st>>>(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank,
-                                       counts, flags);
-    PCF_CU(ctx, cudaGetLastError());
-    ctx->launches += 2 + scan_exclusive(counts, cg->cell_start.as<int>(), ncell + 1,
-                                        ctx->scratch_c.as<int>(), st);
-    PCF_CU(ctx, cudaGetLastError());
-    k_scatter<<<blocks, thr, 0, st>>>(g->raw.as<float4>(), n, cid, rank,
-                                      cg->cell_start.as<int>(), cg->pts.as<float4>(),
-                                      cg->soa.as<float>(), cg->plane);
+    ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank, counts,
+                                       cg->cell_start.as<int>(), ctx->scratch_c.as<int>(),
+                                       cg->pts.as<float4>(), cg->soa.as<float>(), cg->plane, flags, st);
     PCF_CU(ctx, cudaGetLastError());
     cg->h_start.resize((size_t)(ncell + 1));
     int hflags = 0;

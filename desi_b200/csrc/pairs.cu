@@ -408,18 +408,14 @@ void build_tiles(CellGrid &g) {
             }
 }
 
-void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self, PairPlan &plan,
-                int resident_warps) {
-    const int P = home.P;
+void plan_rows(int P, float box, float dmax, bool ani, bool self, std::vector<RowDesc> &rows) {
     const double cell = (double)box / P;
     const double R = (double)dmax;
     // margin for points that sit a rounding step outside their cell
     const double margin = 1e-4 * cell + 8.0 * (double)box * 1.2e-7;
     const double Rm = R + margin;
     const int k = (int)std::ceil(Rm / cell);
-    plan.P = P;
-    plan.cell = (float)cell;
-    plan.rows.clear();
+    rows.clear();
     for (int dx = -k; dx <= k; ++dx) {
         for (int dy = -k; dy <= k; ++dy) {
             const double mx = std::max(std::abs(dx) - 1, 0) * cell;
@@ -439,14 +435,22 @@ void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self
             if (self) {
                 if (dx == 0 && dy == 0) {
                     r.kind = 1;  // forward half of the home column
-                    plan.rows.insert(plan.rows.begin(), r);
+                    rows.insert(rows.begin(), r);
                     continue;
                 }
                 if (!(dx > 0 || (dx == 0 && dy > 0))) continue;  // half shell
             }
-            plan.rows.push_back(r);
+            rows.push_back(r);
         }
     }
+}
+
+void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self, PairPlan &plan,
+                int resident_warps) {
+    const int P = home.P;
+    plan.P = P;
+    plan.cell = (float)((double)box / P);
+    plan_rows(P, box, dmax, ani, self, plan.rows);
     // ~16 items per resident warp keeps the tail short; at most 32 rows each
     const int64_t nt = (int64_t)home.tiles.size();
     const int64_t nr = (int64_t)plan.rows.size();
@@ -486,28 +490,108 @@ static FastCuts make_cuts(const PairRule &rule, float box, float dmax) {
 }
 
 template <bool ANI, bool W, int HM>
-static pcf_status launch_one(pcf_ctx *ctx, const PairArgs &A, size_t smem, long long n_items) {
+static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items, cudaStream_t st,
+                              int sm_count, int device) {
     auto kfn = k_pairs<ANI, W, HM>;
     // attribute / occupancy queries cost microseconds each: do them once per
-    // (variant, shared-memory size)
-    static thread_local size_t attr_smem = 0;
-    static thread_local size_t occ_smem = ~(size_t)0;
-    static thread_local int occ_per_sm = 1;
-    if (smem > 48 * 1024 && smem > attr_smem) {
-        PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_smem = smem;
+    // (device, variant, shared-memory size)
+    constexpr int kDev = 64;
+    static size_t attr_smem[kDev] = {};
+    static size_t occ_smem[kDev];
+    static int occ_per_sm[kDev];
+    static bool init = false;
+    if (!init) {
+        for (int d = 0; d < kDev; ++d) occ_smem[d] = ~(size_t)0;
+        init = true;
     }
-    if (occ_smem != smem) {
+    const int dv = (device >= 0 && device < kDev) ? device : 0;
+    cudaError_t e;
+    if (smem > 48 * 1024 && smem > attr_smem[dv]) {
+        e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_smem[dv] = smem;
+    }
+    if (occ_smem[dv] != smem) {
         int per = 0;
-        PCF_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem));
-        occ_per_sm = std::max(1, per);
-        occ_smem = smem;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem);
+        if (e != cudaSuccess) return e;
+        occ_per_sm[dv] = std::max(1, per);
+        occ_smem[dv] = smem;
     }
-    const int per_sm = occ_per_sm;
     const long long want = (n_items + kWarps - 1) / kWarps;
-    const int grid = (int)std::max(1LL, std::min<long long>(want, (long long)ctx->sm_count * per_sm));
-    kfn<<<grid, kThreads, smem, ctx->stream>>>(A);
-    return PCF_OK;
+    const int grid = (int)std::max(1LL, std::min<long long>(want, (long long)sm_count * occ_per_sm[dv]));
+    kfn<<<grid, kThreads, smem, st>>>(A);
+    return cudaGetLastError();
+}
+
+// Chooses the histogram mode of one launch and starts the kernel.
+static cudaError_t dispatch_pairs(const PairArgs &A, const PairLaunch &pl, cudaStream_t st,
+                                  int sm_count, int device) {
+    const int nb = pl.ani ? pl.rule.bins * pl.rule.bins : pl.rule.bins;
+    const size_t ebytes = pl.weighted ? 8 : 4;
+    const size_t lane_bytes = (size_t)nb * 32 * kWarps * ebytes;
+    const size_t warp_bytes = (size_t)nb * kWarps * ebytes;
+    int hm;
+    size_t smem;
+    if (pl.rule.bins > 255 || warp_bytes > 160 * 1024) { hm = H_GLOBAL; smem = 0; }
+    else if (!pl.ani && lane_bytes <= 64 * 1024) { hm = H_LANE; smem = lane_bytes; }
+    else { hm = H_WARP; smem = warp_bytes; }
+    const long long n = A.n_items;
+#define PCF_DISPATCH(ANI_)                                                                       \
+    if (pl.weighted) {                                                                           \
+        if (hm == H_LANE) return launch_one<ANI_, true, H_LANE>(A, smem, n, st, sm_count, device);   \
+        if (hm == H_WARP) return launch_one<ANI_, true, H_WARP>(A, smem, n, st, sm_count, device);   \
+        return launch_one<ANI_, true, H_GLOBAL>(A, smem, n, st, sm_count, device);                 \
+    } else {                                                                                     \
+        if (hm == H_LANE) return launch_one<ANI_, false, H_LANE>(A, smem, n, st, sm_count, device);  \
+        if (hm == H_WARP) return launch_one<ANI_, false, H_WARP>(A, smem, n, st, sm_count, device);  \
+        return launch_one<ANI_, false, H_GLOBAL>(A, smem, n, st, sm_count, device);                \
+    }
+    if (pl.ani) { PCF_DISPATCH(true) } else { PCF_DISPATCH(false) }
+#undef PCF_DISPATCH
+}
+
+static PairArgs make_args(const GridView &home, const GridView &cand, const TileDesc *tiles,
+                          const RowDesc *rows, int n_rows, int rows_per_item, int n_chunks,
+                          long long n_items, unsigned long long *counter, int P, float box,
+                          const PairLaunch &pl, unsigned long long *d_count, double *d_wsum,
+                          unsigned long long *d_stats) {
+    PairArgs A;
+    A.hx = home.x; A.hy = home.y; A.hz = home.z; A.hw = home.w;
+    A.cx = cand.x; A.cy = cand.y; A.cz = cand.z; A.cw = cand.w;
+    A.cstart = cand.cstart;
+    A.tiles = tiles;
+    A.rows = rows;
+    A.n_rows = n_rows;
+    A.rows_per_item = rows_per_item;
+    A.n_chunks = n_chunks;
+    A.n_items = n_items;
+    A.counter = counter;
+    A.P = P;
+    A.box = box;
+    A.bpc = pl.bpc ? 1 : 0;
+    A.rule = pl.rule;
+    A.fc = make_cuts(pl.rule, box, std::sqrt((float)pl.rule.dd));
+    A.g_count = d_count;
+    A.g_wsum = d_wsum;
+    A.g_stats = d_stats;
+    return A;
+}
+
+cudaError_t launch_pairs_view(const GridView &home, const GridView &cand, const TileDesc *tiles,
+                              int64_t n_tiles, const RowDesc *rows, int n_rows, int P, float box,
+                              const PairLaunch &pl, unsigned long long *counter,
+                              unsigned long long *d_count, double *d_wsum,
+                              unsigned long long *d_stats, cudaStream_t st, int sm_count,
+                              int device) {
+    const int64_t want = std::max<int64_t>(1, (int64_t)sm_count * 24 * 16);
+    const int rpi = (int)std::min<int64_t>(32, std::max<int64_t>(1, (n_tiles * n_rows) / want));
+    const int n_chunks = (n_rows + rpi - 1) / rpi;
+    const PairArgs A = make_args(home, cand, tiles, rows, n_rows, rpi, n_chunks,
+                                 (long long)n_tiles * n_chunks, counter, P, box, pl, d_count,
+                                 d_wsum, d_stats);
+    if (A.n_items == 0) return cudaSuccess;
+    return dispatch_pairs(A, pl, st, sm_count, device);
 }
 
 // Copies the stencil rows into the next staging slot (pinned host ->
@@ -560,35 +644,12 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     PlanSlot *sl = nullptr;
     pcf_status ps = stage_plan(ctx, plan, &sl);
     if (ps != PCF_OK) return ps;
-    PairArgs A;
-    A.hx = home.x(); A.hy = home.y(); A.hz = home.z(); A.hw = home.w();
-    A.cx = cand.x(); A.cy = cand.y(); A.cz = cand.z(); A.cw = cand.w();
-    A.cstart = cand.cell_start.as<int>();
-    A.tiles = home.d_tiles.as<TileDesc>();
-    A.rows = sl->d_rows.as<RowDesc>();
-    A.n_rows = (int)plan.rows.size();
-    A.rows_per_item = plan.rows_per_item;
-    A.n_chunks = plan.n_chunks;
-    A.n_items = plan.n_items;
-    A.counter = sl->d_counter.as<unsigned long long>();
-    A.P = plan.P;
-    A.box = box;
-    A.bpc = pl.bpc ? 1 : 0;
-    A.rule = pl.rule;
-    A.fc = make_cuts(pl.rule, box, std::sqrt((float)pl.rule.dd));
-    A.g_count = d_count;
-    A.g_wsum = d_wsum;
-    A.g_stats = d_stats;
-
-    const int nb = pl.ani ? pl.rule.bins * pl.rule.bins : pl.rule.bins;
-    const size_t ebytes = pl.weighted ? 8 : 4;
-    const size_t lane_bytes = (size_t)nb * 32 * kWarps * ebytes;
-    const size_t warp_bytes = (size_t)nb * kWarps * ebytes;
-    int hm;
-    size_t smem;
-    if (pl.rule.bins > 255 || warp_bytes > 160 * 1024) { hm = H_GLOBAL; smem = 0; }
-    else if (!pl.ani && lane_bytes <= 64 * 1024) { hm = H_LANE; smem = lane_bytes; }
-    else { hm = H_WARP; smem = warp_bytes; }
+    GridView hv{home.x(), home.y(), home.z(), home.w(), home.cell_start.as<int>()};
+    GridView cv{cand.x(), cand.y(), cand.z(), cand.w(), cand.cell_start.as<int>()};
+    const PairArgs A = make_args(hv, cv, home.d_tiles.as<TileDesc>(), sl->d_rows.as<RowDesc>(),
+                                 (int)plan.rows.size(), plan.rows_per_item, plan.n_chunks,
+                                 plan.n_items, sl->d_counter.as<unsigned long long>(), plan.P, box,
+                                 pl, d_count, d_wsum, d_stats);
     PCF_CU(ctx, cudaEventRecord(ctx->ev0, st));
     cudaEvent_t pe0 = nullptr, pe1 = nullptr;
     if (ctx->profile) {
@@ -596,26 +657,18 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
         if (q != PCF_OK) return q;
         PCF_CU(ctx, cudaEventRecord(pe0, st));
     }
-    pcf_status r = PCF_OK;
-#define PCF_DISPATCH(ANI_)                                                                   \
-    if (pl.weighted) {                                                                       \
-        if (hm == H_LANE) r = launch_one<ANI_, true, H_LANE>(ctx, A, smem, A.n_items);       \
-        else if (hm == H_WARP) r = launch_one<ANI_, true, H_WARP>(ctx, A, smem, A.n_items);  \
-        else r = launch_one<ANI_, true, H_GLOBAL>(ctx, A, smem, A.n_items);                  \
-    } else {                                                                                 \
-        if (hm == H_LANE) r = launch_one<ANI_, false, H_LANE>(ctx, A, smem, A.n_items);      \
-        else if (hm == H_WARP) r = launch_one<ANI_, false, H_WARP>(ctx, A, smem, A.n_items); \
-        else r = launch_one<ANI_, false, H_GLOBAL>(ctx, A, smem, A.n_items);                 \
-    }
-    if (pl.ani) { PCF_DISPATCH(true) } else { PCF_DISPATCH(false) }
-#undef PCF_DISPATCH
-    if (r != PCF_OK) return r;
-    PCF_CU(ctx, cudaGetLastError());
+    PCF_CU(ctx, dispatch_pairs(A, pl, st, ctx->sm_count, ctx->device));
     PCF_CU(ctx, cudaEventRecord(ctx->ev1, st));
     if (pe1) PCF_CU(ctx, cudaEventRecord(pe1, st));
     PCF_CU(ctx, cudaEventRecord(sl->done, st));
     ++ctx->launches;
     return PCF_OK;
+}
+
+cudaError_t launch_finalize(const unsigned long long *d_count, const double *d_wsum, bool weighted,
+                            double mult, int nb, double *d_out, cudaStream_t st) {
+    k_finalize<<<(nb + 255) / 256, 256, 0, st>>>(d_count, d_wsum, weighted ? 1 : 0, mult, nb, d_out);
+    return cudaGetLastError();
 }
 
 pcf_status finalize_hist(pcf_ctx *ctx, const unsigned long long *d_count, const double *d_wsum,

@@ -90,10 +90,11 @@ struct RowDesc {
     int16_t dx, dy, kz, kind;
 };
 
-// Device view of a gridded catalog.
-struct CatView {
-    const float4 *pts;      // cell-ordered points
-    const int *cell_start;  // P^3 + 1
+// Device view of a gridded catalog: cell-ordered coordinate planes and the
+// cell table (P^3 + 1 starts).
+struct GridView {
+    const float *x, *y, *z, *w;
+    const int *cstart;
 };
 
 // ---------------------------------------------------------------------------
@@ -211,6 +212,8 @@ constexpr int kTileCap = 32;  // home points per warp item
 // Home tiles of a gridded catalog: each non-empty cell, sliced into runs
 // of at most kTileCap points.
 void build_tiles(CellGrid &g);
+// Stencil rows (dx, dy, kz) of cells that can hold a pair within dmax.
+void plan_rows(int P, float box, float dmax, bool ani, bool self, std::vector<RowDesc> &rows);
 // Builds the stencil and item shape of one pair launch.  self: XX half shell.
 void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self, PairPlan &plan,
                 int resident_warps);
@@ -228,6 +231,25 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
                         unsigned long long *d_count, double *d_wsum, unsigned long long *d_stats);
 pcf_status finalize_hist(pcf_ctx *ctx, const unsigned long long *d_count, const double *d_wsum,
                          bool weighted, double mult, int nb, double *d_out);
+// The pair kernel on explicit buffers (no context): tiles / rows already on
+// the device, counter and accumulators zeroed by the caller.
+cudaError_t launch_pairs_view(const GridView &home, const GridView &cand, const TileDesc *tiles,
+                              int64_t n_tiles, const RowDesc *rows, int n_rows, int P, float box,
+                              const PairLaunch &pl, unsigned long long *counter,
+                              unsigned long long *d_count, double *d_wsum,
+                              unsigned long long *d_stats, cudaStream_t st, int sm_count,
+                              int device);
+cudaError_t launch_finalize(const unsigned long long *d_count, const double *d_wsum, bool weighted,
+                            double mult, int nb, double *d_out, cudaStream_t st);
+// Counting sort of n points into P^3 cells on explicit buffers; returns the
+// number of kernels launched (counts must be zeroed, P^3 + 1 entries).
+int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
+                      int *rank, int *counts, int *cell_start, int *scan_tmp, float4 *pts_out,
+                      float *soa, size_t plane, int *flags, cudaStream_t st);
+// Tile table on the device: per cell ceil(count / kTileCap) tiles; tile
+// offsets (P^3 + 1) give the total in offsets[P^3].
+int launch_tile_build(const int *cell_start, int P, int *tile_counts, int *tile_offsets,
+                      int *scan_tmp, TileDesc *tiles, cudaStream_t st);
 PairRule make_pair_rule(int bins, float dmax, uint32_t flags, bool ani, bool bpc, bool cross);
 pcf_status stage_plan(pcf_ctx *ctx, const PairPlan &plan, PlanSlot **out);
 pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x, const pcf_grid *y, int bins,
