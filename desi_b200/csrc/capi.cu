@@ -252,9 +252,11 @@ static pcf_status hist_scratch(pcf_ctx *ctx, int nb, unsigned long long **cnt, d
     return PCF_OK;
 }
 
-extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_,
-                                      const pcf_grid *b_, int bins, float dmax, uint32_t flags,
-                                      double *hist, pcf_stats *stats) {
+// One pair histogram; ds_override > 0 replaces the bin scale (the fine
+// histograms of the analytic path use (float)bins / dmax).
+static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, const pcf_grid *b_,
+                                   int bins, float dmax, uint32_t flags, double *hist,
+                                   pcf_stats *stats, double ds_override) {
     if (!ctx || !a_ || !hist || bins < 1 || !(dmax > 0.f) || (kind != PCF_ISO && kind != PCF_ANI))
         return PCF_ERR_INVALID_ARG;
     if (kind == PCF_ANI && (int64_t)bins * bins > (1 << 24)) return PCF_ERR_UNSUPPORTED;
@@ -278,6 +280,7 @@ extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_
     pl.self = !cross;
     pl.weighted = !(a->unit_weights && (!cross || b->unit_weights));
     pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, cross);
+    if (ds_override > 0) pl.rule.ds = ds_override;
     pl.mult = cross ? 1.0 : 2.0;
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
                      d_stats);
@@ -314,4 +317,15 @@ extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a_
         }
     }
     return PCF_OK;
+}
+
+extern "C" pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a, const pcf_grid *b,
+                                      int bins, float dmax, uint32_t flags, double *hist,
+                                      pcf_stats *stats) {
+    return count_pairs_impl(ctx, kind, a, b, bins, dmax, flags, hist, stats, 0.0);
+}
+
+pcf_status pcf_count_pairs_ds(pcf_ctx *ctx, const pcf_grid *a, int bins, float dmax, double ds,
+                              uint32_t flags, double *hist, pcf_stats *stats) {
+    return count_pairs_impl(ctx, PCF_ISO, a, nullptr, bins, dmax, flags, hist, stats, ds);
 }

@@ -252,6 +252,9 @@ int launch_tile_build(const int *cell_start, int P, int *tile_counts, int *tile_
                       int *scan_tmp, TileDesc *tiles, cudaStream_t st);
 PairRule make_pair_rule(int bins, float dmax, uint32_t flags, bool ani, bool bpc, bool cross);
 pcf_status stage_plan(pcf_ctx *ctx, const PairPlan &plan, PlanSlot **out);
+// XX iso pair histogram with an explicit bin scale (analytic path).
+pcf_status pcf_count_pairs_ds(pcf_ctx *ctx, const pcf_grid *a, int bins, float dmax, double ds,
+                              uint32_t flags, double *hist, pcf_stats *stats);
 pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x, const pcf_grid *y, int bins,
                                   float dmax, uint32_t flags, double *hist, pcf_stats *stats);
 pcf_status profile_events(pcf_ctx *ctx, cudaEvent_t *a, cudaEvent_t *b);

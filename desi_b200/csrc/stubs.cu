@@ -3,13 +3,6 @@
 #include "pcf_internal.cuh"
 
 extern "C" {
-pcf_status pcf_analytic_rr(pcf_ctx *, int, int64_t, float, float, int, double *) {
-    return PCF_ERR_UNSUPPORTED;
-}
-pcf_status pcf_analytic_3iso(pcf_ctx *, const pcf_grid *, int, float, int, int, int, double *,
-                             double *, double *, pcf_stats *) {
-    return PCF_ERR_UNSUPPORTED;
-}
 pcf_status pcf_batch_pairs(pcf_ctx *, int, const pcf_grid *, const pcf_grid *const *, int, int,
                            float, uint32_t, double *, double *, double *, pcf_stats *) {
     return PCF_ERR_UNSUPPORTED;

@@ -55,6 +55,9 @@ def _load():
     lib.orc_analytic_3iso.argtypes = [_fptr, ctypes.c_long, ctypes.c_float, ctypes.c_int,
                                       ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       _dptr, _dptr, _dptr, _dptr]
+    lib.orc_analytic_ff.argtypes = [_fptr, ctypes.c_long, ctypes.c_float, ctypes.c_int,
+                                    ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    _dptr, _dptr, _dptr]
     lib.orc_analytic_bin.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_float, ctypes.c_int, ctypes.c_double, _dptr,
                                      _dptr, _dptr]
@@ -169,6 +172,20 @@ def analytic_3iso(D, *, box: float, bins: int, dmax: float, ptt: int = 100,
     assert rc == 0
     s = (bins, bins, bins)
     return ddr.reshape(s), rrr.reshape(s), ff, ffr
+
+
+def analytic_ff(D, *, box: float, bins: int, dmax: float, ptt: int = 100, bn_ref: int = 200,
+                wrap: bool = True):
+    """(ff_av, ff_av_ref, alpha_ref) of the analytic 3iso path, without the
+    sub-grid refinement (use analytic_bin for single coarse bins)."""
+    D = _pts(D)
+    ff = np.zeros(bins, np.float64)
+    ffr = np.zeros(bins * bn_ref, np.float64)
+    a = np.zeros(1, np.float64)
+    rc = lib().orc_analytic_ff(_p(D), len(D), box, bins, dmax, ptt, bn_ref, int(wrap), _d(ff),
+                               _d(ffr), _d(a))
+    assert rc == 0
+    return ff, ffr, float(a[0])
 
 
 def analytic_bin(i, j, k, *, bins, dmax, bn_ref, alpha_ref, ff_ref):

@@ -437,8 +437,9 @@ static int all_corners(double ri, double rj, double rk, double h)
  * wrap: reproduce the reference's 32-bit coefficient overflow.
  * fine_dd / fine_dd_ref (optional, may be NULL): receive the fine DD histograms.
  */
-int orc_analytic_3iso(const opt *D, long n, float L, int bins, float dmax, int ptt, int bn_ref,
-                      int wrap, double *DDR, double *RRR, double *ff_av_out, double *ff_ref_out)
+static int analytic_3iso_impl(const opt *D, long n, float L, int bins, float dmax, int ptt,
+                              int bn_ref, int wrap, double *DDR, double *RRR, double *ff_av_out,
+                              double *ff_ref_out, int refine)
 {
     const long bn_ff = (long)ptt * bins;
     const long bn_ff_ref = (long)ptt * bn_ref * bins;
@@ -506,6 +507,13 @@ int orc_analytic_3iso(const opt *D, long n, float L, int bins, float dmax, int p
             }
         }
     }
+    if (refine < 0) {  /* caller wants ff, ff_ref and alpha_ref only */
+        if (ff_av_out) memcpy(ff_av_out, ff_av, sizeof(double) * bins);
+        if (ff_ref_out) memcpy(ff_ref_out, ff_ref, sizeof(double) * bn_ref * bins);
+        if (DDR) DDR[0] = alpha_ref;
+        free(dd_ff); free(dd_ref); free(rr_ff); free(rr_ref); free(ff_av); free(ff_ref);
+        return 0;
+    }
     /* make_histo_analitic (3isoBPC_k.cuh:2021) */
     const long b2 = (long)bins * bins;
     memset(DDR, 0, sizeof(double) * b2 * bins);
@@ -561,6 +569,21 @@ int orc_analytic_3iso(const opt *D, long n, float L, int bins, float dmax, int p
     if (ff_ref_out) memcpy(ff_ref_out, ff_ref, sizeof(double) * bn_ref * bins);
     free(dd_ff); free(dd_ref); free(rr_ff); free(rr_ref); free(ff_av); free(ff_ref);
     return 0;
+}
+
+int orc_analytic_3iso(const opt *D, long n, float L, int bins, float dmax, int ptt, int bn_ref,
+                      int wrap, double *DDR, double *RRR, double *ff_av_out, double *ff_ref_out)
+{
+    return analytic_3iso_impl(D, n, L, bins, dmax, ptt, bn_ref, wrap, DDR, RRR, ff_av_out,
+                              ff_ref_out, 1);
+}
+
+/* ff_av, ff_av_ref and alpha_ref only (no sub-grid refinement). */
+int orc_analytic_ff(const opt *D, long n, float L, int bins, float dmax, int ptt, int bn_ref,
+                    int wrap, double *ff_av_out, double *ff_ref_out, double *alpha_ref_out)
+{
+    return analytic_3iso_impl(D, n, L, bins, dmax, ptt, bn_ref, wrap, alpha_ref_out, NULL,
+                              ff_av_out, ff_ref_out, -1);
 }
 
 /* One partially covered coarse bin of make_histo_analitic, evaluated alone
