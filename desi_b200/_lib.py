@@ -18,7 +18,7 @@ PCF_RULE_CUSTOM = 1 << 2
 PCF_RULE_EXCL_ZERO = 1 << 3
 PCF_RULE_INCLUSIVE = 1 << 4
 PCF_DEVICE_OUT = 1 << 5
-PCF_NO_RECHECK = 1 << 6
+PCF_GRAPH = 1 << 7
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory",
           -4: "unsupported configuration", -5: "coordinate outside [0, box)",

@@ -13,8 +13,9 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import (PCF_ANI, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT, PCF_ISO,  # noqa: F401
-                   PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO, PCF_RULE_INCLUSIVE, PcfError, Stats)
+from ._lib import (PCF_ANI, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT, PCF_GRAPH,  # noqa: F401
+                   PCF_ISO, PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO, PCF_RULE_INCLUSIVE, PcfError,
+                   Stats)
 
 
 def _check(ctx, rc, where):
@@ -150,7 +151,7 @@ class Context:
 
     def batch_pairs(self, d: "Grid", rands, *, bins: int, dmax: float, ani: bool = False,
                     bpc: bool = False, flags: int = 0, want_dd: bool = True,
-                    stats: bool = False):
+                    stats: bool = False, graph: bool = False):
         nr = len(rands)
         nb = bins * bins if ani else bins
         arr = (ctypes.c_void_p * nr)(*[r.handle.value for r in rands])
@@ -158,7 +159,7 @@ class Context:
         rr = np.zeros(nr * nb, np.float64)
         dr = np.zeros(nr * nb, np.float64)
         st = Stats()
-        f = flags | (PCF_BPC if bpc else 0)
+        f = flags | (PCF_BPC if bpc else 0) | (PCF_GRAPH if graph else 0)
         rc = self._lib.pcf_batch_pairs(self.handle, PCF_ANI if ani else PCF_ISO, d.handle,
                                        ctypes.cast(arr, ctypes.c_void_p), nr, int(bins),
                                        float(dmax), f,

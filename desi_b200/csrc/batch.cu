@@ -1,0 +1,222 @@
+// batch.cu -- pcf_batch_pairs: one data catalog against many random
+// catalogs of any sizes in ONE persistent launch.
+//
+// Reference: the -rd mode of cuda/main.cu:157-192 with pcf_2iso /
+// pcf_2ani launching two kernels per random file on separate streams
+// (pcf2iso.cuh:96-104), all random files forced to the same size.  Here the
+// histograms DD, RR_i and DR_i are jobs of one work queue (items laid out
+// job after job, each warp flushing its private histogram when it crosses
+// into the next job), so small catalogs fill the gaps that large ones leave
+// and the whole batch is a single kernel.  With PCF_GRAPH the device side
+// of a batch (clears, kernel, finalize) is captured in a CUDA graph the
+// first time and replayed on later calls with the same grids.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+#include "pcf_internal.cuh"
+
+struct BatchGraph {
+    DevBuf plan;   // rows | jobs | mults
+    DevBuf accum;  // counts | sums | stats | counter | out
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int nslots = 0, nb = 0;
+    double *d_out = nullptr;
+    unsigned long long *d_stats = nullptr;
+    std::vector<double> mult;  // per slot: 2 for XX, 1 for XY
+    ~BatchGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_,
+                                      const pcf_grid *const *r_, int n_rand, int bins, float dmax,
+                                      uint32_t flags, double *dd, double *rr, double *dr,
+                                      pcf_stats *stats) {
+    if (!ctx || !d_ || bins < 1 || !(dmax > 0.f) || n_rand < 0 || (n_rand > 0 && !r_) ||
+        (kind != PCF_ISO && kind != PCF_ANI) || (!dd && !rr && !dr))
+        return PCF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0;
+    pcf_grid *D = const_cast<pcf_grid *>(d_);
+    std::vector<pcf_grid *> R((size_t)n_rand);
+    int64_t nmax = D->n;
+    for (int i = 0; i < n_rand; ++i) {
+        R[i] = const_cast<pcf_grid *>(r_[i]);
+        if (!R[i]) return PCF_ERR_INVALID_ARG;
+        if (R[i]->box != D->box) return PCF_ERR_MISMATCH;
+        nmax = std::max<int64_t>(nmax, R[i]->n);
+    }
+    const float box = D->box;
+    if (bpc && !(2.0 * (double)dmax < (double)box)) return PCF_ERR_UNSUPPORTED;
+    const int P = choose_partitions(nmax, box, dmax, kind, bpc, 0);
+    pcf_status s = grid_ensure_cells(ctx, D, P);
+    if (s != PCF_OK) return s;
+    for (auto *g : R) {
+        s = grid_ensure_cells(ctx, g, P);
+        if (s != PCF_OK) return s;
+    }
+    const int nb = ani ? bins * bins : bins;
+    bool weighted = !D->unit_weights;
+    for (auto *g : R) weighted = weighted || !g->unit_weights;
+
+    // cache key of the captured graph: grids (by cell buffers) and parameters
+    std::string key;
+    const bool use_graph = (flags & PCF_GRAPH) != 0;
+    if (use_graph) {
+        std::ostringstream os;
+        os << kind << ':' << bins << ':' << dmax << ':' << (flags & ~PCF_GRAPH) << ':' << (dd != nullptr)
+           << (rr != nullptr) << (dr != nullptr) << ':' << D->cells->pts.p;
+        for (auto *g : R) os << ',' << g->cells->pts.p;
+        key = os.str();
+    }
+    std::shared_ptr<BatchGraph> bg;
+    if (use_graph) {
+        auto it = ctx->graphs.find(key);
+        if (it != ctx->graphs.end()) bg = it->second;
+    }
+    cudaStream_t st = ctx->stream;
+    if (!bg) {
+        bg = std::make_shared<BatchGraph>();
+        bg->plan.pool = ctx->pool;
+        bg->accum.pool = ctx->pool;
+        std::vector<RowDesc> rows_self, rows_cross;
+        plan_rows(P, box, dmax, ani, true, rows_self);
+        plan_rows(P, box, dmax, ani, false, rows_cross);
+        struct J { pcf_grid *h, *c; bool self; double mult; };
+        std::vector<J> js;
+        if (dd) js.push_back({D, D, true, 2.0});
+        for (int i = 0; i < n_rand; ++i) {
+            if (rr) js.push_back({R[i], R[i], true, 2.0});
+            if (dr) js.push_back({D, R[i], false, 1.0});
+        }
+        const int nslots = (int)js.size();
+        int64_t total = 0;
+        for (auto &j : js) total += (int64_t)j.h->cells->tiles.size() * (j.self ? rows_self.size() : rows_cross.size());
+        const size_t rb_s = rows_self.size() * sizeof(RowDesc), rb_c = rows_cross.size() * sizeof(RowDesc);
+        const size_t off_c = (rb_s + 255) & ~(size_t)255;
+        const size_t off_j = (off_c + rb_c + 255) & ~(size_t)255;
+        const size_t off_m = (off_j + sizeof(PairJob) * nslots + 255) & ~(size_t)255;
+        const size_t plan_bytes = off_m + sizeof(double) * nslots;
+        PCF_CU(ctx, bg->plan.ensure(plan_bytes));
+        char *dp = bg->plan.as<char>();
+        std::vector<PairJob> jobs((size_t)nslots);
+        std::vector<double> mult((size_t)nslots);
+        long long item = 0;
+        const unsigned rXX = reference_pair_rule(ani, bpc, false), rXY = reference_pair_rule(ani, bpc, true);
+        for (int k = 0; k < nslots; ++k) {
+            const CellGrid &h = *js[k].h->cells, &c = *js[k].c->cells;
+            PairJob &j = jobs[k];
+            j.home = GridView{h.x(), h.y(), h.z(), h.w(), h.cell_start.as<int>()};
+            j.cand = GridView{c.x(), c.y(), c.z(), c.w(), c.cell_start.as<int>()};
+            j.tiles = h.d_tiles.as<TileDesc>();
+            j.rows = reinterpret_cast<const RowDesc *>(dp + (js[k].self ? 0 : off_c));
+            shape_job(j, (int64_t)h.tiles.size(), (int)(js[k].self ? rows_self.size() : rows_cross.size()),
+                      total, ctx->sm_count);
+            j.slot = k;
+            j.item_begin = item;
+            j.rule_flags = (flags & PCF_RULE_CUSTOM)
+                               ? (((flags & PCF_RULE_EXCL_ZERO) ? PCF_RULE_EXCL : 0u) |
+                                  ((flags & PCF_RULE_INCLUSIVE) ? PCF_RULE_LE : 0u))
+                               : (js[k].self ? rXX : rXY);
+            j.pad = 0;
+            item += (long long)h.tiles.size() * j.n_chunks;
+            mult[k] = js[k].mult;
+        }
+        std::vector<char> host(plan_bytes, 0);
+        memcpy(host.data(), rows_self.data(), rb_s);
+        memcpy(host.data() + off_c, rows_cross.data(), rb_c);
+        memcpy(host.data() + off_j, jobs.data(), sizeof(PairJob) * nslots);
+        memcpy(host.data() + off_m, mult.data(), sizeof(double) * nslots);
+        PCF_CU(ctx, cudaMemcpyAsync(dp, host.data(), plan_bytes, cudaMemcpyHostToDevice, st));
+        PCF_CU(ctx, cudaStreamSynchronize(st));  // host staging buffer goes out of scope
+        // accumulators: counts | sums | stats(64B) | counter(64B) | out
+        const size_t nacc = (size_t)nb * nslots;
+        PCF_CU(ctx, bg->accum.ensure(nacc * 24 + 256));
+        char *ap = bg->accum.as<char>();
+        unsigned long long *cnt = reinterpret_cast<unsigned long long *>(ap);
+        double *ws = reinterpret_cast<double *>(ap + nacc * 8);
+        unsigned long long *stt = reinterpret_cast<unsigned long long *>(ap + nacc * 16);
+        unsigned long long *counter = stt + 8;
+        double *out = reinterpret_cast<double *>(ap + nacc * 16 + 128);
+        bg->nslots = nslots;
+        bg->nb = nb;
+        bg->mult = mult;
+        bg->d_out = out;
+        bg->d_stats = stt;
+        PairLaunch pl;
+        pl.ani = ani;
+        pl.bpc = bpc;
+        pl.self = false;
+        pl.weighted = weighted;
+        pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
+        pl.mult = 1.0;
+        auto enqueue = [&]() -> cudaError_t {
+            cudaError_t e = cudaMemsetAsync(ap, 0, nacc * 16 + 128, st);
+            if (e != cudaSuccess) return e;
+            e = launch_pair_jobs(reinterpret_cast<const PairJob *>(dp + off_j), nslots, item, P, box, pl,
+                                 counter, cnt, ws, stt, st, ctx->sm_count, ctx->device);
+            if (e != cudaSuccess) return e;
+            return launch_finalize_slots(cnt, ws, weighted, reinterpret_cast<const double *>(dp + off_m),
+                                         nb, nslots, out, st);
+        };
+        if (use_graph) {
+            // make sure the kernel attributes are set outside the capture
+            PCF_CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = enqueue();
+            cudaGraph_t g = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(st, &g);
+            if (e != cudaSuccess) return pcf_fail(ctx, e, "batch capture");
+            if (e2 != cudaSuccess) return pcf_fail(ctx, e2, "cudaStreamEndCapture");
+            bg->graph = g;
+            PCF_CU(ctx, cudaGraphInstantiate(&bg->exec, g, 0));
+            ctx->graphs[key] = bg;
+        } else {
+            PCF_CU(ctx, cudaEventRecord(ctx->ev0, st));
+            PCF_CU(ctx, enqueue());
+            PCF_CU(ctx, cudaEventRecord(ctx->ev1, st));
+            ctx->launches += 2;
+        }
+    }
+    if (use_graph) {
+        PCF_CU(ctx, cudaEventRecord(ctx->ev0, st));
+        PCF_CU(ctx, cudaGraphLaunch(bg->exec, st));
+        PCF_CU(ctx, cudaEventRecord(ctx->ev1, st));
+        ctx->launches += 2;
+    }
+    // results
+    std::vector<double> host((size_t)bg->nb * bg->nslots);
+    unsigned long long hs[4] = {0, 0, 0, 0};
+    PCF_CU(ctx, cudaMemcpyAsync(host.data(), bg->d_out, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, st));
+    PCF_CU(ctx, cudaMemcpyAsync(hs, bg->d_stats, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    PCF_CU(ctx, cudaStreamSynchronize(st));
+    int k = 0;
+    if (dd) memcpy(dd, host.data() + (size_t)(k++) * nb, sizeof(double) * nb);
+    for (int i = 0; i < n_rand; ++i) {
+        if (rr) memcpy(rr + (size_t)i * nb, host.data() + (size_t)(k++) * nb, sizeof(double) * nb);
+        if (dr) memcpy(dr + (size_t)i * nb, host.data() + (size_t)(k++) * nb, sizeof(double) * nb);
+    }
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        double pairs = 0;
+        if (!weighted) {
+            for (int s2 = 0; s2 < bg->nslots; ++s2) {
+                double sm = 0;
+                for (int q = 0; q < nb; ++q) sm += host[(size_t)s2 * nb + q];
+                pairs += sm / bg->mult[s2];  // unordered XX pairs, XY pairs
+            }
+        }
+        stats->pairs = weighted ? (double)hs[2] : pairs;
+        stats->rechecks = (double)hs[0];
+        stats->candidates = (double)hs[1];
+        stats->kernel_ms = ms;
+        stats->partitions = P;
+        stats->work_items = bg->nslots;
+    }
+    if (!use_graph) bg.reset();
+    return PCF_OK;
+}

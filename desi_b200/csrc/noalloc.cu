@@ -116,6 +116,7 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
     double *d_ws = cv.take<double>((size_t)nbins);
     unsigned long long *d_stats = cv.take<unsigned long long>(8);
     int *d_flags = cv.take<int>(8);
+    PairJob *d_job = cv.take<PairJob>(1);
     if (cv.used > PCF_NOALLOC_SCRATCH_BYTES) return PCF_ERR_UNSUPPORTED;
 
     // everything that accumulates starts at zero (the array keeps the last
@@ -162,7 +163,7 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
     const GridView hv{A.soa, A.soa + A.plane, A.soa + 2 * A.plane, A.soa + 3 * A.plane, A.start};
     const GridView cvw{B.soa, B.soa + B.plane, B.soa + 2 * B.plane, B.soa + 3 * B.plane, B.start};
     e = launch_pairs_view(hv, cvw, tiles, h_tiles, d_rows, (int)rows.size(), P, box, pl, counter,
-                          d_cnt, d_ws, d_stats, st, sms, dev);
+                          d_cnt, d_ws, d_stats, d_job, st, sms, dev);
     if (e != cudaSuccess) return fail(e);
     e = launch_finalize(d_cnt, d_ws, pl.weighted, pl.mult, nbins, hist, st);
     if (e != cudaSuccess) return fail(e);

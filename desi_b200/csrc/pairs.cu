@@ -53,14 +53,8 @@ struct FastCuts {
 };
 
 struct PairArgs {
-    const float *hx, *hy, *hz, *hw;  // home catalog planes (cell order)
-    const float *cx, *cy, *cz, *cw;  // candidate catalog planes
-    const int *cstart;
-    const TileDesc *tiles;
-    const RowDesc *rows;
-    int n_rows;
-    int rows_per_item;
-    int n_chunks;
+    const PairJob *jobs;  // histograms of this launch, items laid out job after job
+    int n_jobs;
     long long n_items;
     unsigned long long *counter;
     int P;
@@ -129,6 +123,7 @@ struct Seg {
     float sx, sy, sz;  // image shift of the candidates
     float lo, hi;
     unsigned w;
+    unsigned rule_flags;
 };
 
 // Canonical FP64 decision for one pair (rare path): histogram slot or -1.
@@ -141,14 +136,51 @@ __device__ __noinline__ int slow_slot(float hx, float hy, float hz, float cx, fl
 }
 
 template <bool ANI, bool WEIGHTED, int HM>
-__device__ __forceinline__ void slow_pair(const PairArgs &A, const Home &h, const Seg &sg, int j,
-                                          const Sink<WEIGHTED, HM> &sink, unsigned &n_pairs) {
-    const int slot = slow_slot<ANI>(h.x, h.y, h.z, __ldg(A.cx + j), __ldg(A.cy + j),
-                                    __ldg(A.cz + j), sg.sx, sg.sy, sg.sz, A.rule);
+__device__ __forceinline__ void slow_pair(const PairArgs &A, const GridView &C, const Home &h,
+                                          const Seg &sg, int j, const Sink<WEIGHTED, HM> &sink,
+                                          unsigned &n_pairs) {
+    PairRule rule = A.rule;
+    rule.flags = sg.rule_flags;
+    const int slot = slow_slot<ANI>(h.x, h.y, h.z, __ldg(C.x + j), __ldg(C.y + j), __ldg(C.z + j),
+                                    sg.sx, sg.sy, sg.sz, rule);
     if (slot >= 0) {
-        sink.add(slot, h.w, WEIGHTED ? __ldg(A.cw + j) : 1.f, true);
+        sink.add(slot, h.w, WEIGHTED ? __ldg(C.w + j) : 1.f, true);
         if (WEIGHTED) ++n_pairs;
     }
+}
+
+// Adds this warp's histogram copy into histogram `slot` of the launch and
+// clears it (job change or end of the queue).
+template <bool WEIGHTED, int HM>
+__device__ __forceinline__ void flush_hist(typename std::conditional<WEIGHTED, double, unsigned>::type *mine,
+                                           int nb, int per_warp, int lane, const PairArgs &A,
+                                           int slot) {
+    typedef typename std::conditional<WEIGHTED, double, unsigned>::type HT;
+    if (HM == H_GLOBAL) return;
+    __syncwarp();
+    const size_t off = (size_t)slot * nb;
+    if (HM == H_LANE) {
+        for (int k = 0; k < nb; ++k) {
+            HT s = mine[k * 32 + lane];
+            mine[k * 32 + lane] = (HT)0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
+            if (lane == 0 && s != (HT)0) {
+                if (WEIGHTED) atomicAdd(A.g_wsum + off + k, (double)s);
+                else atomicAdd(A.g_count + off + k, (unsigned long long)s);
+            }
+        }
+    } else {
+        for (int k = lane; k < nb; k += 32) {
+            const HT s = mine[k];
+            mine[k] = (HT)0;
+            if (s != (HT)0) {
+                if (WEIGHTED) atomicAdd(A.g_wsum + off + k, (double)s);
+                else atomicAdd(A.g_count + off + k, (unsigned long long)s);
+            }
+        }
+    }
+    __syncwarp();
+    (void)per_warp;
 }
 
 // One candidate pair of elements (packed): distance test, fixed-point bin,
@@ -156,7 +188,8 @@ __device__ __forceinline__ void slow_pair(const PairArgs &A, const Home &h, cons
 // or at zero separation (frac(r) = 0 fails the window test) go to the FP64
 // rule, behind one warp-uniform branch.
 template <bool ANI, bool WEIGHTED, int HM>
-__device__ __forceinline__ void take2(const PairArgs &A, float2 DX, float2 DY, float2 DZ, bool v0,
+__device__ __forceinline__ void take2(const PairArgs &A, const GridView &C, float2 DX, float2 DY,
+                                      float2 DZ, bool v0,
                                       bool v1, int j, float2 Wt, const Home &h, const Seg &sg,
                                       const Sink<WEIGHTED, HM> &sink, unsigned &n_pairs,
                                       unsigned &n_rechk) {
@@ -209,11 +242,11 @@ __device__ __forceinline__ void take2(const PairArgs &A, float2 DX, float2 DY, f
     if (__any_sync(__activemask(), r0 || r1)) {
         if (r0) {
             ++n_rechk;
-            slow_pair<ANI, WEIGHTED, HM>(A, h, sg, j, sink, n_pairs);
+            slow_pair<ANI, WEIGHTED, HM>(A, C, h, sg, j, sink, n_pairs);
         }
         if (r1) {
             ++n_rechk;
-            slow_pair<ANI, WEIGHTED, HM>(A, h, sg, j + 1, sink, n_pairs);
+            slow_pair<ANI, WEIGHTED, HM>(A, C, h, sg, j + 1, sink, n_pairs);
         }
     }
 }
@@ -234,10 +267,15 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
     for (int k = lane; k < per_warp; k += 32) mine[k] = (HT)0;
     __syncwarp();
     Sink<WEIGHTED, HM> sink;
-    if (HM == H_GLOBAL) sink.base = WEIGHTED ? (void *)A.g_wsum : (void *)A.g_count;
-    else sink.base = HM == H_LANE ? (void *)(mine + lane) : (void *)mine;
+    if (HM != H_GLOBAL) sink.base = HM == H_LANE ? (void *)(mine + lane) : (void *)mine;
     unsigned n_pairs = 0, n_rechk = 0;
     unsigned long long n_cand = 0;
+    // current job (items of one warp arrive in increasing order), kept in
+    // shared memory to spare registers
+    __shared__ PairJob s_job[kWarps];
+    PairJob &J = s_job[warp];
+    int cj = -1, slot = 0;
+    long long job_end = -1;
 
     long long next = 0;
     if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);
@@ -245,11 +283,30 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
     while (next < A.n_items) {
         const long long it_idx = next;
         if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next item
-        const int tile = (int)(it_idx / A.n_chunks);
-        const int chunk = (int)(it_idx - (long long)tile * A.n_chunks);
-        const int row_begin = chunk * A.rows_per_item;
-        const int row_end = min(row_begin + A.rows_per_item, A.n_rows);
-        const TileDesc t = A.tiles[tile];
+        if (it_idx >= job_end) {  // entering another job: flush this one's histogram
+            if (cj >= 0) flush_hist<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
+            do {
+                ++cj;
+                job_end = cj + 1 < A.n_jobs ? A.jobs[cj + 1].item_begin : A.n_items;
+            } while (it_idx >= job_end);
+            {
+                static_assert(sizeof(PairJob) % 4 == 0, "PairJob words");
+                const int *src = reinterpret_cast<const int *>(A.jobs + cj);
+                int *dst = reinterpret_cast<int *>(&J);
+                for (int q = lane; q < (int)(sizeof(PairJob) / 4); q += 32) dst[q] = src[q];
+                __syncwarp();
+            }
+            slot = J.slot;
+            if (HM == H_GLOBAL)
+                sink.base = WEIGHTED ? (void *)(A.g_wsum + (size_t)slot * nb)
+                                     : (void *)(A.g_count + (size_t)slot * nb);
+        }
+        const long long loc = it_idx - J.item_begin;
+        const int tile = (int)(loc / J.n_chunks);
+        const int chunk = (int)(loc - (long long)tile * J.n_chunks);
+        const int row_begin = chunk * J.rows_per_item;
+        const int row_end = min(row_begin + J.rows_per_item, J.n_rows);
+        const TileDesc t = J.tiles[tile];
         const int H = t.count;                 // 1..32 home points
         const int S = 32 / H;                  // candidate streams per warp
         const int sidx = lane / H;             // this lane's stream
@@ -258,7 +315,7 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
         const int hidx = t.start + hl;
         Home h;
         if (valid) {
-            h.x = A.hx[hidx]; h.y = A.hy[hidx]; h.z = A.hz[hidx]; h.w = A.hw[hidx];
+            h.x = J.home.x[hidx]; h.y = J.home.y[hidx]; h.z = J.home.z[hidx]; h.w = J.home.w[hidx];
         } else {
             h.x = h.y = h.z = __int_as_float(0x7fc00000);  // NaN: never in range
             h.w = 0.f;
@@ -269,7 +326,7 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
         int ra0 = 0, rb0 = 0, ra1 = 0, rb1 = 0, rkind = 0;
         float rsx = 0.f, rsy = 0.f, rsz1 = 0.f;
         if (lane < nrows) {
-            const RowDesc rw = A.rows[row_begin + lane];
+            const RowDesc rw = J.rows[row_begin + lane];
             int nx = t.ix + rw.dx, ny = t.iy + rw.dy;
             const int P = A.P;
             bool ok = true;
@@ -283,17 +340,18 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
                 const int col = (nx * P + ny) * P;
                 const int zhi = t.z1 + rw.kz;
                 rkind = rw.kind;
+                const int *cs = J.cand.cstart;
                 if (rw.kind == 1) {  // forward half of the home column (XX): j > home index
                     ra0 = t.start;
-                    rb0 = A.cstart[col + min(zhi, P - 1) + 1];
-                    if (A.bpc && zhi >= P) { ra1 = A.cstart[col]; rb1 = A.cstart[col + zhi - P + 1]; rsz1 = A.box; }
+                    rb0 = cs[col + min(zhi, P - 1) + 1];
+                    if (A.bpc && zhi >= P) { ra1 = cs[col]; rb1 = cs[col + zhi - P + 1]; rsz1 = A.box; }
                 } else {
                     const int zlo = t.z0 - rw.kz;
-                    ra0 = A.cstart[col + max(zlo, 0)];
-                    rb0 = A.cstart[col + min(zhi, P - 1) + 1];
+                    ra0 = cs[col + max(zlo, 0)];
+                    rb0 = cs[col + min(zhi, P - 1) + 1];
                     if (A.bpc) {
-                        if (zlo < 0) { ra1 = A.cstart[col + zlo + P]; rb1 = A.cstart[col + P]; rsz1 = -A.box; }
-                        else if (zhi >= P) { ra1 = A.cstart[col]; rb1 = A.cstart[col + zhi - P + 1]; rsz1 = A.box; }
+                        if (zlo < 0) { ra1 = cs[col + zlo + P]; rb1 = cs[col + P]; rsz1 = -A.box; }
+                        else if (zhi >= P) { ra1 = cs[col]; rb1 = cs[col + zhi - P + 1]; rsz1 = A.box; }
                     }
                 }
             }
@@ -314,6 +372,7 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
                 sg.lo = A.fc.lo[sh];
                 sg.hi = A.fc.hi[sh];
                 sg.w = A.fc.w[sh];
+                sg.rule_flags = J.rule_flags;
                 const float2 NHX = make_float2(sg.sx - h.x, sg.sx - h.x);
                 const float2 NHY = make_float2(sg.sy - h.y, sg.sy - h.y);
                 const float2 NHZ = make_float2(sg.sz - h.z, sg.sz - h.z);
@@ -322,18 +381,19 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
                 const int a2 = a & ~1;
                 #pragma unroll 1
                 for (int p = a2 + 2 * sidx; p < b; p += 2 * S) {
-                    const float2 X = __ldg(reinterpret_cast<const float2 *>(A.cx + p));
-                    const float2 Y = __ldg(reinterpret_cast<const float2 *>(A.cy + p));
-                    const float2 Z = __ldg(reinterpret_cast<const float2 *>(A.cz + p));
+                    const float2 X = __ldg(reinterpret_cast<const float2 *>(J.cand.x + p));
+                    const float2 Y = __ldg(reinterpret_cast<const float2 *>(J.cand.y + p));
+                    const float2 Z = __ldg(reinterpret_cast<const float2 *>(J.cand.z + p));
                     float2 Wt = make_float2(1.f, 1.f);
-                    if (WEIGHTED) Wt = __ldg(reinterpret_cast<const float2 *>(A.cw + p));
+                    if (WEIGHTED) Wt = __ldg(reinterpret_cast<const float2 *>(J.cand.w + p));
                     // (x_j + shift) - x_home, rounded once: same value as the
                     // scalar (x_j - (x_home - shift)) up to the bound in make_cuts
                     const float2 DX = __fadd2_rn(X, NHX);
                     const float2 DY = __fadd2_rn(Y, NHY);
                     const float2 DZ = __fadd2_rn(Z, NHZ);
-                    take2<ANI, WEIGHTED, HM>(A, DX, DY, DZ, p > jmin, (p + 1 < b) && (p + 1 > jmin),
-                                             p, Wt, h, sg, sink, n_pairs, n_rechk);
+                    take2<ANI, WEIGHTED, HM>(A, J.cand, DX, DY, DZ, p > jmin,
+                                             (p + 1 < b) && (p + 1 > jmin), p, Wt, h, sg, sink,
+                                             n_pairs, n_rechk);
                 }
             }
         }
@@ -341,26 +401,7 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
     }
     // per-warp flush (no CTA barrier: warps leave as the queue drains)
     __syncwarp();
-    if (HM != H_GLOBAL) {
-        if (HM == H_LANE) {
-            for (int k = 0; k < nb; ++k) {
-                HT s = mine[k * 32 + lane];
-                for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(kFull, s, off);
-                if (lane == 0 && s != (HT)0) {
-                    if (WEIGHTED) atomicAdd(A.g_wsum + k, (double)s);
-                    else atomicAdd(A.g_count + k, (unsigned long long)s);
-                }
-            }
-        } else {
-            for (int k = lane; k < nb; k += 32) {
-                const HT s = mine[k];
-                if (s != (HT)0) {
-                    if (WEIGHTED) atomicAdd(A.g_wsum + k, (double)s);
-                    else atomicAdd(A.g_count + k, (unsigned long long)s);
-                }
-            }
-        }
-    }
+    if (cj >= 0) flush_hist<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
     unsigned long long rp = n_pairs, rr = n_rechk;
     for (int off = 16; off > 0; off >>= 1) {
         rr += __shfl_down_sync(kFull, rr, off);
@@ -371,6 +412,17 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
         if (n_cand) atomicAdd(A.g_stats + 1, n_cand);
         if (rp) atomicAdd(A.g_stats + 2, rp);
     }
+}
+
+// Several histograms: out[s*nb + k] = mult[s] * hist[s*nb + k].
+__global__ void k_finalize_slots(const unsigned long long *__restrict__ cnt,
+                                 const double *__restrict__ ws, int weighted,
+                                 const double *__restrict__ mult, int nb, int nslots,
+                                 double *__restrict__ out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * nslots) return;
+    const int s = (int)(t / nb);
+    out[t] = mult[s] * (weighted ? ws[t] : (double)cnt[t]);
 }
 
 // out[k] = mult * hist[k] (u64 counts or FP64 sums).
@@ -551,20 +603,13 @@ static cudaError_t dispatch_pairs(const PairArgs &A, const PairLaunch &pl, cudaS
 #undef PCF_DISPATCH
 }
 
-static PairArgs make_args(const GridView &home, const GridView &cand, const TileDesc *tiles,
-                          const RowDesc *rows, int n_rows, int rows_per_item, int n_chunks,
-                          long long n_items, unsigned long long *counter, int P, float box,
-                          const PairLaunch &pl, unsigned long long *d_count, double *d_wsum,
+static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
+                          unsigned long long *counter, int P, float box, const PairLaunch &pl,
+                          unsigned long long *d_count, double *d_wsum,
                           unsigned long long *d_stats) {
     PairArgs A;
-    A.hx = home.x; A.hy = home.y; A.hz = home.z; A.hw = home.w;
-    A.cx = cand.x; A.cy = cand.y; A.cz = cand.z; A.cw = cand.w;
-    A.cstart = cand.cstart;
-    A.tiles = tiles;
-    A.rows = rows;
-    A.n_rows = n_rows;
-    A.rows_per_item = rows_per_item;
-    A.n_chunks = n_chunks;
+    A.jobs = jobs;
+    A.n_jobs = n_jobs;
     A.n_items = n_items;
     A.counter = counter;
     A.P = P;
@@ -578,20 +623,47 @@ static PairArgs make_args(const GridView &home, const GridView &cand, const Tile
     return A;
 }
 
+cudaError_t launch_pair_jobs(const PairJob *d_jobs, int n_jobs, long long n_items, int P, float box,
+                             const PairLaunch &pl, unsigned long long *counter,
+                             unsigned long long *d_count, double *d_wsum,
+                             unsigned long long *d_stats, cudaStream_t st, int sm_count, int device) {
+    if (n_items == 0) return cudaSuccess;
+    const PairArgs A = make_args(d_jobs, n_jobs, n_items, counter, P, box, pl, d_count, d_wsum, d_stats);
+    return dispatch_pairs(A, pl, st, sm_count, device);
+}
+
+// Item shape of one job: rows per item so that the whole launch has ~16
+// items per resident warp.
+void shape_job(PairJob &j, int64_t n_tiles, int n_rows, int64_t total_tile_rows, int sm_count) {
+    const int64_t want = std::max<int64_t>(1, (int64_t)sm_count * 24 * 16);
+    const int rpi = (int)std::min<int64_t>(32, std::max<int64_t>(1, total_tile_rows / want));
+    j.n_rows = n_rows;
+    j.rows_per_item = rpi;
+    j.n_chunks = (n_rows + rpi - 1) / rpi;
+    (void)n_tiles;
+}
+
 cudaError_t launch_pairs_view(const GridView &home, const GridView &cand, const TileDesc *tiles,
                               int64_t n_tiles, const RowDesc *rows, int n_rows, int P, float box,
                               const PairLaunch &pl, unsigned long long *counter,
                               unsigned long long *d_count, double *d_wsum,
-                              unsigned long long *d_stats, cudaStream_t st, int sm_count,
-                              int device) {
-    const int64_t want = std::max<int64_t>(1, (int64_t)sm_count * 24 * 16);
-    const int rpi = (int)std::min<int64_t>(32, std::max<int64_t>(1, (n_tiles * n_rows) / want));
-    const int n_chunks = (n_rows + rpi - 1) / rpi;
-    const PairArgs A = make_args(home, cand, tiles, rows, n_rows, rpi, n_chunks,
-                                 (long long)n_tiles * n_chunks, counter, P, box, pl, d_count,
-                                 d_wsum, d_stats);
-    if (A.n_items == 0) return cudaSuccess;
-    return dispatch_pairs(A, pl, st, sm_count, device);
+                              unsigned long long *d_stats, PairJob *d_job, cudaStream_t st,
+                              int sm_count, int device) {
+    PairJob j;
+    j.home = home;
+    j.cand = cand;
+    j.tiles = tiles;
+    j.rows = rows;
+    j.slot = 0;
+    j.item_begin = 0;
+    j.rule_flags = pl.rule.flags;
+    j.pad = 0;
+    shape_job(j, n_tiles, n_rows, n_tiles * n_rows, sm_count);
+    const long long n_items = (long long)n_tiles * j.n_chunks;
+    cudaError_t e = cudaMemcpyAsync(d_job, &j, sizeof(PairJob), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    return launch_pair_jobs(d_job, 1, n_items, P, box, pl, counter, d_count, d_wsum, d_stats, st,
+                            sm_count, device);
 }
 
 // Copies the stencil rows into the next staging slot (pinned host ->
@@ -603,15 +675,16 @@ pcf_status stage_plan(pcf_ctx *ctx, const PairPlan &plan, PlanSlot **out) {
     if (!sl.done) PCF_CU(ctx, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
     if (sl.used) PCF_CU(ctx, cudaEventSynchronize(sl.done));
     const size_t rb = plan.rows.size() * sizeof(RowDesc);
-    if (sl.h_bytes < rb) {
+    const size_t jb = sizeof(PairJob) * 4;
+    if (sl.h_bytes < rb + jb + 256) {
         if (sl.h_pinned) cudaFreeHost(sl.h_pinned);
         sl.h_pinned = nullptr;
         sl.h_bytes = 0;
-        const size_t want = std::max<size_t>(rb * 2, 1 << 16);
+        const size_t want = std::max<size_t>((rb + jb) * 2 + 256, 1 << 16);
         PCF_CU(ctx, cudaMallocHost(&sl.h_pinned, want));
         sl.h_bytes = want;
     }
-    PCF_CU(ctx, sl.d_rows.ensure(rb));
+    PCF_CU(ctx, sl.d_rows.ensure(rb + jb + 256));
     PCF_CU(ctx, sl.d_counter.ensure(64));
     memcpy(sl.h_pinned, plan.rows.data(), rb);
     PCF_CU(ctx, cudaMemcpyAsync(sl.d_rows.p, sl.h_pinned, rb, cudaMemcpyHostToDevice, st));
@@ -644,12 +717,26 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     PlanSlot *sl = nullptr;
     pcf_status ps = stage_plan(ctx, plan, &sl);
     if (ps != PCF_OK) return ps;
-    GridView hv{home.x(), home.y(), home.z(), home.w(), home.cell_start.as<int>()};
-    GridView cv{cand.x(), cand.y(), cand.z(), cand.w(), cand.cell_start.as<int>()};
-    const PairArgs A = make_args(hv, cv, home.d_tiles.as<TileDesc>(), sl->d_rows.as<RowDesc>(),
-                                 (int)plan.rows.size(), plan.rows_per_item, plan.n_chunks,
-                                 plan.n_items, sl->d_counter.as<unsigned long long>(), plan.P, box,
-                                 pl, d_count, d_wsum, d_stats);
+    // the one job of this launch, staged behind the rows in the same slot
+    PairJob job;
+    job.home = GridView{home.x(), home.y(), home.z(), home.w(), home.cell_start.as<int>()};
+    job.cand = GridView{cand.x(), cand.y(), cand.z(), cand.w(), cand.cell_start.as<int>()};
+    job.tiles = home.d_tiles.as<TileDesc>();
+    job.rows = sl->d_rows.as<RowDesc>();
+    job.n_rows = (int)plan.rows.size();
+    job.rows_per_item = plan.rows_per_item;
+    job.n_chunks = plan.n_chunks;
+    job.slot = 0;
+    job.item_begin = 0;
+    job.rule_flags = pl.rule.flags;
+    job.pad = 0;
+    const size_t roff = (plan.rows.size() * sizeof(RowDesc) + 255) & ~(size_t)255;
+    char *hjob = static_cast<char *>(sl->h_pinned) + roff;
+    memcpy(hjob, &job, sizeof(PairJob));
+    PairJob *d_job = reinterpret_cast<PairJob *>(sl->d_rows.as<char>() + roff);
+    PCF_CU(ctx, cudaMemcpyAsync(d_job, hjob, sizeof(PairJob), cudaMemcpyHostToDevice, st));
+    const PairArgs A = make_args(d_job, 1, plan.n_items, sl->d_counter.as<unsigned long long>(),
+                                 plan.P, box, pl, d_count, d_wsum, d_stats);
     PCF_CU(ctx, cudaEventRecord(ctx->ev0, st));
     cudaEvent_t pe0 = nullptr, pe1 = nullptr;
     if (ctx->profile) {
@@ -663,6 +750,15 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     PCF_CU(ctx, cudaEventRecord(sl->done, st));
     ++ctx->launches;
     return PCF_OK;
+}
+
+cudaError_t launch_finalize_slots(const unsigned long long *d_count, const double *d_wsum,
+                                  bool weighted, const double *d_mult, int nb, int nslots,
+                                  double *d_out, cudaStream_t st) {
+    const long long n = (long long)nb * nslots;
+    k_finalize_slots<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_count, d_wsum, weighted ? 1 : 0,
+                                                                   d_mult, nb, nslots, d_out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const unsigned long long *d_count, const double *d_wsum, bool weighted,

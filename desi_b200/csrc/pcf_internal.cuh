@@ -182,6 +182,7 @@ struct pcf_ctx {
     void *h_pinned = nullptr;
     size_t h_pinned_bytes = 0;
     int64_t launches = 0;  // kernels launched by this context
+    std::map<std::string, std::shared_ptr<struct BatchGraph>> graphs;  // pcf_batch_pairs(PCF_GRAPH)
 };
 
 // ---------------------------------------------------------------------------
@@ -231,16 +232,38 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
                         unsigned long long *d_count, double *d_wsum, unsigned long long *d_stats);
 pcf_status finalize_hist(pcf_ctx *ctx, const unsigned long long *d_count, const double *d_wsum,
                          bool weighted, double mult, int nb, double *d_out);
-// The pair kernel on explicit buffers (no context): tiles / rows already on
-// the device, counter and accumulators zeroed by the caller.
+// One histogram of a pair launch: home / candidate catalogs, stencil rows,
+// and the implicit items [item_begin, item_begin + n_tiles * n_chunks).
+struct PairJob {
+    GridView home, cand;
+    const TileDesc *tiles;
+    const RowDesc *rows;
+    int n_rows, rows_per_item, n_chunks, slot;
+    long long item_begin;
+    unsigned rule_flags;  // exact-rule flags of this histogram (XX and XY differ)
+    int pad;
+};
+void shape_job(PairJob &j, int64_t n_tiles, int n_rows, int64_t total_tile_rows, int sm_count);
+// The pair kernel over a device job table (jobs ordered by item_begin);
+// counter and the n_jobs * nb accumulators zeroed by the caller.
+cudaError_t launch_pair_jobs(const PairJob *d_jobs, int n_jobs, long long n_items, int P, float box,
+                             const PairLaunch &pl, unsigned long long *counter,
+                             unsigned long long *d_count, double *d_wsum,
+                             unsigned long long *d_stats, cudaStream_t st, int sm_count, int device);
+// Single-job form on explicit buffers (no context); d_job: device room for
+// one PairJob.
 cudaError_t launch_pairs_view(const GridView &home, const GridView &cand, const TileDesc *tiles,
                               int64_t n_tiles, const RowDesc *rows, int n_rows, int P, float box,
                               const PairLaunch &pl, unsigned long long *counter,
                               unsigned long long *d_count, double *d_wsum,
-                              unsigned long long *d_stats, cudaStream_t st, int sm_count,
-                              int device);
+                              unsigned long long *d_stats, PairJob *d_job, cudaStream_t st,
+                              int sm_count, int device);
 cudaError_t launch_finalize(const unsigned long long *d_count, const double *d_wsum, bool weighted,
                             double mult, int nb, double *d_out, cudaStream_t st);
+cudaError_t launch_finalize_slots(const unsigned long long *d_count, const double *d_wsum,
+                                  bool weighted, const double *d_mult, int nb, int nslots,
+                                  double *d_out, cudaStream_t st);
+unsigned reference_pair_rule(bool ani, bool bpc, bool cross);
 // Counting sort of n points into P^3 cells on explicit buffers; returns the
 // number of kernels launched (counts must be zeroed, P^3 + 1 entries).
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,

@@ -3,10 +3,6 @@
 #include "pcf_internal.cuh"
 
 extern "C" {
-pcf_status pcf_batch_pairs(pcf_ctx *, int, const pcf_grid *, const pcf_grid *const *, int, int,
-                           float, uint32_t, double *, double *, double *, pcf_stats *) {
-    return PCF_ERR_UNSUPPORTED;
-}
 }
 
 pcf_status pcf_count_triplets_ani(pcf_ctx *, const pcf_grid *, const pcf_grid *, int, float,

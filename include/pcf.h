@@ -71,7 +71,9 @@ enum {
     PCF_RULE_INCLUSIVE = 1u << 4, /* d^2 <= dmax^2 instead of <                        */
     PCF_DEVICE_OUT = 1u << 5,  /* hist points to device memory; the call returns
                                   without synchronising the context stream           */
-    PCF_NO_RECHECK = 1u << 6   /* diagnostics only: skip the FP64 edge recheck         */
+    PCF_GRAPH = 1u << 7        /* pcf_batch_pairs: capture the launch in a CUDA graph the
+                                  first time and replay it on later calls with the same
+                                  grids and parameters                               */
 };
 
 /* Counters a counting call can report (any pointer argument may be NULL). */
