@@ -4,8 +4,3 @@
 
 extern "C" {
 }
-
-pcf_status pcf_count_triplets_ani(pcf_ctx *, const pcf_grid *, const pcf_grid *, int, float,
-                                  uint32_t, double *, pcf_stats *) {
-    return PCF_ERR_UNSUPPORTED;
-}

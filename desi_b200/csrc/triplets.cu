@@ -127,9 +127,29 @@ __device__ __forceinline__ int fast_bin(float d2, const TripCuts &c, int bins) {
 // Appends the neighbours of anchor (hx,hy,hz) found in catalog C to a list.
 // only_after >= 0 keeps candidates with index > only_after (X list of XXX /
 // XXY).  Entries: {dx, dy, dz, bits(idx << 8 | bin)}.
+// Angle bin of the anisotropic 3-point histograms for the side anchor->point:
+// t = (int)((1 + dz/d) * (float)(bins/2)) (3ani_k.cuh:79-91), dz signed, or
+// with periodic boxes dz = |z2-z1| - L*f (3aniBPC_k.cuh:18,34); -1 when >= bins.
+__device__ __noinline__ int exact_angle(float ax, float ay, float az, float bx, float by, float bz,
+                                        int bpc, float box, int bins, float ds_th) {
+    double dx, dy, dz;
+    sep_exact(ax, ay, az, bx, by, bz, bpc, (double)box, dx, dy, dz);
+    const double d = __dsqrt_rn(exact_d2(dx, dy, dz));
+    double dzr = dz;
+    if (bpc) {
+        const double raw = fabs(__dsub_rn((double)bz, (double)az));
+        dzr = raw > 0.5 * (double)box ? __dsub_rn(raw, (double)box) : raw;
+    }
+    const double c = __dadd_rn(1.0, __ddiv_rn(dzr, d));
+    const int t = (int)__dmul_rn(c, (double)ds_th);
+    return (t >= 0 && t < bins) ? t : -1;
+}
+
+template <bool ANG>
 __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, float hz, int hcell_ix,
                            int hcell_iy, int hcell_iz, int only_after, const PairRule &rule,
-                           float4 *list, float *wlist, int cap, int *s_n, unsigned &n_rechk) {
+                           float4 *list, float *wlist, int cap, int *s_n, unsigned &n_rechk,
+                           unsigned short *ang = nullptr) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int P = A.P;
     for (int r = 0; r < A.n_rows; ++r) {
@@ -175,6 +195,12 @@ __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, 
                         bin = exact_side(hx, hy, hz, C.x[c], C.y[c], C.z[c], A.bpc, A.box, rule);
                     }
                 }
+                int tang = 0;
+                if (ANG && bin >= 0) {
+                    tang = exact_angle(hx, hy, hz, C.x[c], C.y[c], C.z[c], A.bpc, A.box, rule.bins,
+                                       (float)rule.bins / 2.0f);
+                    if (tang < 0) bin = -2;  // the side can close no triangle
+                }
                 const bool keep = bin >= 0;
                 const unsigned m = __ballot_sync(kFull, keep);
                 int off = 0;
@@ -185,6 +211,7 @@ __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, 
                     if (pos < cap) {
                         list[pos] = make_float4(vx, vy, vz, __int_as_float((c << 8) | bin));
                         if (wlist) wlist[pos] = C.w[c];
+                        if (ANG) ang[pos] = (unsigned short)(bin | (tang << 8));
                     }
                 }
             }
@@ -231,11 +258,11 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
         const int ciy = min(max((int)__fdiv_rn(hy, A.cell), 0), P - 1);
         const int ciz = min(max((int)__fdiv_rn(hz, A.cell), 0), P - 1);
         // pass 1: lists into shared memory (sizes counted even past capacity)
-        build_list(A, A.X, hx, hy, hz, cix, ciy, ciz, i, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
-                   A.capJ, &s_nJ, n_rechk);
+        build_list<false>(A, A.X, hx, hy, hz, cix, ciy, ciz, i, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
+                          A.capJ, &s_nJ, n_rechk);
         if (MIXED)
-            build_list(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK, WEIGHTED ? swK : nullptr,
-                       A.capK, &s_nK, n_rechk);
+            build_list<false>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK,
+                              WEIGHTED ? swK : nullptr, A.capK, &s_nK, n_rechk);
         __syncthreads();
         int nJ = s_nJ, nK = MIXED ? s_nK : nJ;
         const float4 *LJ = sJ;
@@ -246,11 +273,11 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
             __syncthreads();
             if (tid == 0) { s_nJ = 0; s_nK = 0; }
             __syncthreads();
-            build_list(A, A.X, hx, hy, hz, cix, ciy, ciz, i, A.rXX, gJ, WEIGHTED ? gwJ : nullptr,
-                       A.gcap, &s_nJ, n_rechk);
+            build_list<false>(A, A.X, hx, hy, hz, cix, ciy, ciz, i, A.rXX, gJ,
+                              WEIGHTED ? gwJ : nullptr, A.gcap, &s_nJ, n_rechk);
             if (MIXED)
-                build_list(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, gK,
-                           WEIGHTED ? gwK : nullptr, A.gcap, &s_nK, n_rechk);
+                build_list<false>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, gK,
+                                  WEIGHTED ? gwK : nullptr, A.gcap, &s_nK, n_rechk);
             __threadfence_block();
             __syncthreads();
             nJ = min(s_nJ, A.gcap);
@@ -313,6 +340,105 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
         if (rr) atomicAdd(A.g_stats + 0, rr);
         if (n_tri) atomicAdd(A.g_stats + 2, n_tri);
     }
+}
+
+// Anisotropic triplets (3ani_k.cuh:8,109; 3aniBPC_k.cuh:210,959): ordered
+// triples anchored at point 1 = the anchor i; the lists hold every X (and
+// for XXY every Y) neighbour with its exact side bin and angle bin, and all
+// ordered (j, k), j != k, are counted into the bins^5 histogram
+// [b(d12)][b(d31)][b(d23)][t12][t31] in global memory.
+template <bool MIXED, bool WEIGHTED>
+__global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int bins = A.rXX.bins;
+    float4 *sJ = reinterpret_cast<float4 *>(smem);
+    float4 *sK = sJ + A.capJ;
+    unsigned short *aJ = reinterpret_cast<unsigned short *>(sK + (MIXED ? A.capK : 0));
+    unsigned short *aK = aJ + A.capJ;
+    float *swJ = reinterpret_cast<float *>(aK + (MIXED ? A.capK : 0) + 8);
+    float *swK = swJ + (WEIGHTED ? A.capJ : 0);
+    __shared__ int s_anchor, s_nJ, s_nK;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned n_rechk = 0;
+    unsigned long long n_tri = 0;
+    const long long B = bins, B2 = B * B, B3 = B2 * B, B4 = B3 * B;
+    for (;;) {
+        if (tid == 0) {
+            s_anchor = (int)atomicAdd(A.counter, 1ull);
+            s_nJ = 0;
+            s_nK = 0;
+        }
+        __syncthreads();
+        const int i = s_anchor;
+        if (i >= A.nX) break;
+        const float hx = A.X.x[i], hy = A.X.y[i], hz = A.X.z[i];
+        const float hw = WEIGHTED ? A.X.w[i] : 1.f;
+        const int P = A.P;
+        const int cix = min(max((int)__fdiv_rn(hx, A.cell), 0), P - 1);
+        const int ciy = min(max((int)__fdiv_rn(hy, A.cell), 0), P - 1);
+        const int ciz = min(max((int)__fdiv_rn(hz, A.cell), 0), P - 1);
+        build_list<true>(A, A.X, hx, hy, hz, cix, ciy, ciz, -1, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
+                         A.capJ, &s_nJ, n_rechk, aJ);
+        if (MIXED)
+            build_list<true>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK,
+                             WEIGHTED ? swK : nullptr, A.capK, &s_nK, n_rechk, aK);
+        __syncthreads();
+        const int nJ = s_nJ, nK = MIXED ? s_nK : s_nJ;
+        if (nJ > A.capJ || (MIXED && nK > A.capK)) {
+            // lists beyond shared memory: flagged for the host, anchor skipped
+            if (tid == 0) atomicAdd(A.g_stats + 3, 1ull);
+            __syncthreads();
+            continue;
+        }
+        const float4 *LK = MIXED ? sK : sJ;
+        const unsigned short *AK = MIXED ? aK : aJ;
+        const float *WK = MIXED ? swK : swJ;
+        for (int jj = warp; jj < nJ; jj += kTWarps) {
+            const float4 ej = sJ[jj];
+            const int jidx = (int)((unsigned)__float_as_int(ej.w) >> 8);
+            const unsigned short pj = aJ[jj];
+            const long long base = (long long)(pj & 255) * B4 + (long long)(pj >> 8) * B;
+            const double wij = WEIGHTED ? (double)hw * (double)swJ[jj] : 1.0;
+            for (int kk = lane; kk < nK; kk += 32) {
+                if (!MIXED && kk == jj) continue;
+                const float4 ek = LK[kk];
+                const float dx = ek.x - ej.x, dy = ek.y - ej.y, dz = ek.z - ej.z;
+                const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                const PairRule &r3 = MIXED ? A.rXY : A.rXX;
+                int c = fast_bin(d2, A.fc, bins);
+                if (c == -1) {
+                    ++n_rechk;
+                    const int kidx = (int)((unsigned)__float_as_int(ek.w) >> 8);
+                    const Cat &CK = MIXED ? A.Y : A.X;
+                    c = exact_third(hx, hy, hz, A.X.x[jidx], A.X.y[jidx], A.X.z[jidx], CK.x[kidx],
+                                    CK.y[kidx], CK.z[kidx], A.bpc, A.box, r3);
+                }
+                if (c >= 0) {
+                    const unsigned short pk = AK[kk];
+                    const long long slot = base + (long long)(pk & 255) * B3 + (long long)c * B2 + (pk >> 8);
+                    ++n_tri;
+                    if (WEIGHTED) atomicAdd(A.g_wsum + slot, wij * (double)WK[kk]);
+                    else atomicAdd(A.g_count + slot, 1ull);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    unsigned long long rr = n_rechk;
+    for (int off = 16; off > 0; off >>= 1) {
+        rr += __shfl_down_sync(kFull, rr, off);
+        n_tri += __shfl_down_sync(kFull, n_tri, off);
+    }
+    if (lane == 0) {
+        if (rr) atomicAdd(A.g_stats + 0, rr);
+        if (n_tri) atomicAdd(A.g_stats + 2, n_tri);
+    }
+}
+
+__global__ void k_to_double(const unsigned long long *__restrict__ c, const double *__restrict__ w,
+                            int weighted, long long n, double *__restrict__ out) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = weighted ? w[t] : (double)c[t];
 }
 
 // Ordered-triple histogram from the oriented counts U[b_ij][b_jk][b_ki].
@@ -492,6 +618,112 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
             stats->partitions = P;
             stats->work_items = (int)X->n;
         }
+    }
+    return PCF_OK;
+}
+
+// Anisotropic triplets (bins^5).  The histogram lives in global memory (u64
+// counts or FP64 sums); lists stay in shared memory (an anchor whose lists
+// do not fit makes the call fail with PCF_ERR_UNSUPPORTED).
+pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_grid *y_, int bins,
+                                  float dmax, uint32_t flags, double *hist, pcf_stats *stats) {
+    if (bins > 255 || (int64_t)bins * bins * bins * bins * bins > ((int64_t)1 << 31))
+        return PCF_ERR_UNSUPPORTED;
+    cudaSetDevice(ctx->device);
+    pcf_grid *X = const_cast<pcf_grid *>(x_);
+    pcf_grid *Y = const_cast<pcf_grid *>(y_);
+    const bool bpc = (flags & PCF_BPC) != 0, mixed = Y != nullptr;
+    if (X->n >= (1 << 24) || (Y && Y->n >= (1 << 24))) return PCF_ERR_UNSUPPORTED;
+    int P = 0;
+    pcf_status s = prepare_grids(ctx, X, Y, dmax, PCF_ISO, bpc, &P);
+    if (s != PCF_OK) return s;
+    const CellGrid &gx = *X->cells;
+    const CellGrid &gy = mixed ? *Y->cells : gx;
+    PairPlan plan;
+    plan_pairs(gx, X->box, dmax, false, false, plan, ctx->sm_count * 24);
+    PairRule rXX = make_pair_rule(bins, dmax, flags & ~PCF_DS_EXACT, false, bpc, false);
+    PairRule rXY = rXX;
+    rXY.flags = bpc ? PCF_RULE_EXCL : 0u;
+    if (flags & PCF_RULE_CUSTOM) rXY.flags = rXX.flags;
+    TripArgs A;
+    memset(&A, 0, sizeof(A));
+    A.X = {gx.x(), gx.y(), gx.z(), gx.w(), gx.cell_start.as<int>()};
+    A.Y = {gy.x(), gy.y(), gy.z(), gy.w(), gy.cell_start.as<int>()};
+    A.nX = (int)X->n;
+    A.n_rows = (int)plan.rows.size();
+    A.P = P;
+    A.cell = gx.cell;
+    A.box = X->box;
+    A.bpc = bpc ? 1 : 0;
+    A.rXX = rXX;
+    A.rXY = rXY;
+    {
+        const double dd = rXX.dd;
+        const double rmax = (double)dmax * rXX.ds + 1.0;
+        const double Lx = bpc ? (double)X->box : (double)dmax;
+        const double e_d2 = dd * std::ldexp(1.0, -17) + (double)dmax * Lx * std::ldexp(1.0, -18);
+        const double wr = rmax * std::ldexp(1.0, -17) + rXX.ds * Lx * std::ldexp(1.0, -18);
+        A.fc.dsf = (float)rXX.ds;
+        A.fc.ds2 = A.fc.dsf * A.fc.dsf;
+        A.fc.lo = (float)(dd - e_d2);
+        A.fc.hi = (float)(dd + e_d2);
+        A.fc.w = std::min(8000u, (unsigned)std::ceil((wr + std::ldexp(1.0, -16)) * 32768.0) + 1u);
+    }
+    const bool weighted = !(X->unit_weights && (!mixed || Y->unit_weights));
+    const size_t ent = 16 + 2 + (weighted ? 4 : 0);
+    const size_t room = 227 * 1024 - 256;
+    if (mixed) {
+        A.capJ = (int)(room / ent / 3);
+        A.capK = (int)(room / ent) - A.capJ - 8;
+    } else {
+        A.capJ = (int)(room / ent) - 8;
+        A.capK = 0;
+    }
+    const size_t smem = (size_t)(A.capJ + A.capK) * ent + 64;
+    const int64_t n5 = (int64_t)bins * bins * bins * bins * bins;
+    PlanSlot *sl = nullptr;
+    s = stage_plan(ctx, plan, &sl);
+    if (s != PCF_OK) return s;
+    A.rows = sl->d_rows.as<RowDesc>();
+    A.counter = sl->d_counter.as<unsigned long long>();
+    PCF_CU(ctx, ctx->d_hist.ensure((size_t)n5 * 16 + 128));
+    char *hp = ctx->d_hist.as<char>();
+    A.g_count = reinterpret_cast<unsigned long long *>(hp);
+    A.g_wsum = reinterpret_cast<double *>(hp);  // one of the two is used
+    A.g_stats = reinterpret_cast<unsigned long long *>(hp + (size_t)n5 * 8);
+    double *d_out = reinterpret_cast<double *>(hp + (size_t)n5 * 8 + 128);
+    PCF_CU(ctx, cudaMemsetAsync(hp, 0, (size_t)n5 * 8 + 128, ctx->stream));
+    auto kfn = mixed ? (weighted ? k_triplets_ani<true, true> : k_triplets_ani<true, false>)
+                     : (weighted ? k_triplets_ani<false, true> : k_triplets_ani<false, false>);
+    PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PCF_CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    kfn<<<ctx->sm_count, kTThreads, smem, ctx->stream>>>(A);
+    PCF_CU(ctx, cudaGetLastError());
+    PCF_CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    PCF_CU(ctx, cudaEventRecord(sl->done, ctx->stream));
+    k_to_double<<<(unsigned)((n5 + 255) / 256), 256, 0, ctx->stream>>>(A.g_count, A.g_wsum,
+                                                                       weighted ? 1 : 0, n5, d_out);
+    PCF_CU(ctx, cudaGetLastError());
+    ctx->launches += 2;
+    const bool dev_out = (flags & PCF_DEVICE_OUT) != 0;
+    unsigned long long hs[4] = {0, 0, 0, 0};
+    PCF_CU(ctx, cudaMemcpyAsync(hs, A.g_stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+    PCF_CU(ctx, cudaMemcpyAsync(hist, d_out, sizeof(double) * n5,
+                                dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hs[3]) {
+        ctx->last_error = "neighbour lists of the anisotropic triplet kernel exceed shared memory";
+        return PCF_ERR_UNSUPPORTED;
+    }
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->pairs = (double)hs[2];
+        stats->rechecks = (double)hs[0];
+        stats->candidates = 0;
+        stats->kernel_ms = ms;
+        stats->partitions = P;
+        stats->work_items = (int)X->n;
     }
     return PCF_OK;
 }

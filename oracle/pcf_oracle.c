@@ -308,10 +308,19 @@ int orc_triplets_iso(int bpc, int mixed, int prec, const opt *X, long nX, const 
 
 /* ----------------------------------------------------------------------- */
 /* Triplets (anisotropic, bins^5): a=b(d12), b=b(d31), c=b(d23),            */
+/* With periodic boundaries the reference folds the sign of dz:             */
+/* dz = |z2 - z1| - L*f (3aniBPC_k.cuh:18,34), f = 1 when the pair uses its */
+/* z image, i.e. +|dz| without a z wrap and -|dz_min| with one.             */
 /* t=(int)((1+dz12/d12)*bins/2), p=(int)((1+dz31/d31)*bins/2)               */
 /* (3ani_k.cuh:75-91), each dropped when >= bins.  Ordered triples are      */
 /* enumerated directly (no symmetry: the angles are anchored at point 1).   */
 /* ----------------------------------------------------------------------- */
+static inline double bpc_dz(float z1, float z2, double L)
+{
+    double d = fabs((double)z2 - (double)z1);
+    return d > 0.5 * L ? d - L : d;
+}
+
 static inline int ani_angle_bin(double dz, double d, int bins)
 {
     double c = 1.0 + dz / d;
@@ -349,7 +358,7 @@ int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, lo
                 const nbr_t *q = &N2[a];
                 if (q->idx == i) continue;
                 double d12 = sqrt((q->v[0] * q->v[0] + q->v[1] * q->v[1]) + q->v[2] * q->v[2]);
-                int t = ani_angle_bin(q->v[2], d12, bins);
+                int t = ani_angle_bin(bpc ? bpc_dz(p->z, X[q->idx].z, Ld) : q->v[2], d12, bins);
                 if (t < 0) continue;
                 double wij = (double)p->w * (double)X[q->idx].w;
                 for (long b = 0; b < n3; ++b) {
@@ -359,7 +368,7 @@ int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, lo
                     int c = side_bin(v, ddmax, mixed ? rXY : rXX, ds, bins);
                     if (c < 0) continue;
                     double d31 = sqrt((r->v[0] * r->v[0] + r->v[1] * r->v[1]) + r->v[2] * r->v[2]);
-                    int pp = ani_angle_bin(r->v[2], d31, bins);
+                    int pp = ani_angle_bin(bpc ? bpc_dz(p->z, Y[r->idx].z, Ld) : r->v[2], d31, bins);
                     if (pp < 0) continue;
                     double w = wij * (double)Y[r->idx].w;
                     long slot = (((q->bin * B + r->bin) * B + c) * B + t) * B + pp;

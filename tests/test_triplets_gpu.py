@@ -81,3 +81,18 @@ def test_golden_config_full_size(ctx, catalogs, golden_3iso):
         # sit in the neighbouring bin; totals of in-range triangles agree to 1e-6
         assert abs(v.sum() - g.sum()) <= 1e-6 * g.sum(), k
         assert np.abs(v - g).sum() <= 1e-5 * g.sum(), k
+
+
+@pytest.mark.parametrize("bpc", [False, True])
+@pytest.mark.parametrize("w", ["unit", "uniform"])
+def test_triplets_ani(ctx, bpc, w):
+    """bins^5 anisotropic triplets: ordered triples anchored at point 1."""
+    box, bins, dmax = 60.0, 6, 14.0
+    D = catalog.neyman_scott(700, box, seed=81, children=16, sigma=3.0, weights=w)
+    R = catalog.uniform(800, box, seed=82, weights=w)
+    gd, gr = ctx.grid(D, box), ctx.grid(R, box)
+    weighted = w != "unit"
+    _cmp(ctx.count_triplets(gd, bins=bins, dmax=dmax, ani=True, bpc=bpc),
+         oracle.triplets_ani(D, box=box, bins=bins, dmax=dmax, bpc=bpc), weighted)
+    _cmp(ctx.count_triplets(gd, gr, bins=bins, dmax=dmax, ani=True, bpc=bpc),
+         oracle.triplets_ani(D, R, box=box, bins=bins, dmax=dmax, bpc=bpc), weighted)
