@@ -34,6 +34,14 @@ class PcfError(RuntimeError):
         super().__init__(msg)
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [("refine", ctypes.c_int), ("hist_mode", ctypes.c_int), ("best_ms", ctypes.c_float),
+                ("default_ms", ctypes.c_float), ("tried", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("pairs", ctypes.c_double), ("candidates", ctypes.c_double),
                 ("rechecks", ctypes.c_double), ("kernel_ms", ctypes.c_float),
@@ -82,6 +90,13 @@ _SIGS = {
                                                ctypes.c_int, ctypes.c_float, ctypes.c_uint32, _vp,
                                                _vp]),
     "pcf_ctx_launch_count": (_i64, [_vp]),
+    "pcf_autotune_pairs": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_float,
+                                          ctypes.c_uint32, _vp]),
+    "pcf_tune_save": (ctypes.c_int, [_vp, ctypes.c_char_p]),
+    "pcf_tune_load": (ctypes.c_int, [_vp, ctypes.c_char_p]),
+    "pcf_tune_size": (ctypes.c_int, [_vp]),
+    "pcf_estimate": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _i64, _i64,
+                                    _vp]),
     "pcf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pcf_ctx_profile_read": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(_i64)]),

@@ -173,6 +173,38 @@ class Context:
         res = (dd, rr.reshape(shp), dr.reshape(shp))
         return (res, st.as_dict()) if stats else res
 
+    def estimate(self, hists, n_d: int = 0, n_r: int = 0) -> np.ndarray:
+        """Landy-Szalay: hists = (DD, DR, RR) or (DDD, DDR, DRR, RRR)."""
+        hs = [np.ascontiguousarray(h, np.float64) for h in hists]
+        shape = hs[0].shape
+        out = np.zeros(hs[0].size, np.float64)
+        p = [h.ctypes.data_as(ctypes.c_void_p) for h in hs] + [None] * (4 - len(hs))
+        npoint = 2 if len(hs) == 3 else 3
+        _check(self.handle, self._lib.pcf_estimate(self.handle, npoint, hs[0].size, *p, int(n_d),
+                                                   int(n_r), out.ctypes.data_as(ctypes.c_void_p)),
+               "pcf_estimate")
+        return out.reshape(shape)
+
+    def autotune_pairs(self, a: "Grid", b: "Grid | None" = None, *, bins: int, dmax: float,
+                       ani: bool = False, bpc: bool = False, flags: int = 0) -> dict:
+        """Time launch shapes on these catalogs; later counts of the class use the winner."""
+        r = _lib.TuneResult()
+        f = flags | (PCF_BPC if bpc else 0)
+        _check(self.handle, self._lib.pcf_autotune_pairs(
+            self.handle, PCF_ANI if ani else PCF_ISO, a.handle, b.handle if b is not None else None,
+            int(bins), float(dmax), f, ctypes.byref(r)), "pcf_autotune_pairs")
+        return r.as_dict()
+
+    def tune_save(self, path: str) -> None:
+        _check(self.handle, self._lib.pcf_tune_save(self.handle, path.encode()), "pcf_tune_save")
+
+    def tune_load(self, path: str) -> None:
+        _check(self.handle, self._lib.pcf_tune_load(self.handle, path.encode()), "pcf_tune_load")
+
+    @property
+    def tune_size(self) -> int:
+        return int(self._lib.pcf_tune_size(self.handle))
+
     def microbench(self, which: int) -> float:
         """0: FP32 FMA TFLOP/s; 1: conflict-free shared atomic Gop/s."""
         r = ctypes.c_double()

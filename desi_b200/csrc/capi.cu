@@ -211,7 +211,7 @@ PairRule make_pair_rule(int bins, float dmax, uint32_t flags, bool ani, bool bpc
 
 // Shared validation + re-gridding of the counting calls.
 pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int kind,
-                         bool bpc, int *P_out) {
+                         bool bpc, int *P_out, int refine) {
     if (b && b->box != a->box) return PCF_ERR_MISMATCH;
     const float box = a->box;
     if (bpc && !(2.0 * (double)dmax < (double)box)) {
@@ -219,7 +219,7 @@ pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int
         return PCF_ERR_UNSUPPORTED;
     }
     int64_t n = std::max<int64_t>(a->n, b ? b->n : 0);
-    int P = choose_partitions(n, box, dmax, kind, bpc, 0);
+    int P = choose_partitions(n, box, dmax, kind, bpc, refine);
     if (bpc) {
         double cell = (double)box / P;
         int k = (int)std::ceil(((double)dmax + 1e-4 * cell + 8.0 * box * 1.2e-7) / cell);
@@ -264,8 +264,17 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     pcf_grid *a = const_cast<pcf_grid *>(a_);
     pcf_grid *b = const_cast<pcf_grid *>(b_);
     const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0, cross = b != nullptr;
+    const bool weighted = !(a->unit_weights && (!cross || b->unit_weights));
+    TuneEntry te;
+    if (ctx->tune_override.refine > 0 || ctx->tune_override.hist_mode >= 0) {
+        te = ctx->tune_override;
+    } else if (!ctx->tune.empty()) {
+        auto it = ctx->tune.find(tune_key(kind, bpc, cross, weighted, bins,
+                                          std::max<int64_t>(a->n, cross ? b->n : 0), a->box, dmax));
+        if (it != ctx->tune.end()) te = it->second;
+    }
     int P = 0;
-    pcf_status s = prepare_grids(ctx, a, b, dmax, kind, bpc, &P);
+    pcf_status s = prepare_grids(ctx, a, b, dmax, kind, bpc, &P, te.refine);
     if (s != PCF_OK) return s;
     PairPlan plan;
     plan_pairs(*a->cells, a->box, dmax, ani, !cross, plan, ctx->sm_count * 24);
@@ -278,7 +287,8 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     pl.ani = ani;
     pl.bpc = bpc;
     pl.self = !cross;
-    pl.weighted = !(a->unit_weights && (!cross || b->unit_weights));
+    pl.weighted = weighted;
+    pl.hist_mode = te.hist_mode;
     pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, cross);
     if (ds_override > 0) pl.rule.ds = ds_override;
     pl.mult = cross ? 1.0 : 2.0;

@@ -588,6 +588,13 @@ static cudaError_t dispatch_pairs(const PairArgs &A, const PairLaunch &pl, cudaS
     if (pl.rule.bins > 255 || warp_bytes > 160 * 1024) { hm = H_GLOBAL; smem = 0; }
     else if (!pl.ani && lane_bytes <= 64 * 1024) { hm = H_LANE; smem = lane_bytes; }
     else { hm = H_WARP; smem = warp_bytes; }
+    // an autotuned scheme overrides the rule above when it is valid here
+    if (pl.hist_mode == H_GLOBAL) { hm = H_GLOBAL; smem = 0; }
+    else if (pl.hist_mode == H_WARP && pl.rule.bins <= 255 && warp_bytes <= 160 * 1024) {
+        hm = H_WARP; smem = warp_bytes;
+    } else if (pl.hist_mode == H_LANE && !pl.ani && pl.rule.bins <= 255 && lane_bytes <= 64 * 1024) {
+        hm = H_LANE; smem = lane_bytes;
+    }
     const long long n = A.n_items;
 #define PCF_DISPATCH(ANI_)                                                                       \
     if (pl.weighted) {                                                                           \

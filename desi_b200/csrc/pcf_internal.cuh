@@ -163,8 +163,17 @@ struct PlanSlot {
     bool used = false;
 };
 
+// Autotuned launch shape of one class of pair histograms.
+struct TuneEntry {
+    int refine = 0;      // cells per dmax (0: default rule)
+    int hist_mode = -1;  // histogram privatisation (-1: default rule)
+    float ms = 0.f;      // best kernel time seen while tuning
+};
+
 struct pcf_ctx {
     std::shared_ptr<MemPool> pool = std::make_shared<MemPool>();
+    std::map<std::string, TuneEntry> tune;
+    TuneEntry tune_override;  // set while the autotuner times a candidate
     PlanSlot slots[2];
     int slot = 0;
     // optional kernel-time log (pcf_ctx_profile)
@@ -225,8 +234,11 @@ pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes);
 struct PairLaunch {
     bool ani, weighted, bpc, self;
     PairRule rule;
-    double mult;  // 2 for XX (ordered-pair convention), 1 for XY
+    double mult;         // 2 for XX (ordered-pair convention), 1 for XY
+    int hist_mode = -1;  // 0 lane-private, 1 per-warp shared, 2 global; -1 automatic
 };
+std::string tune_key(int kind, bool bpc, bool cross, bool weighted, int bins, int64_t n, float box,
+                     float dmax);
 pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home,
                         const CellGrid &cand, float box, const PairLaunch &pl,
                         unsigned long long *d_count, double *d_wsum, unsigned long long *d_stats);
@@ -282,4 +294,4 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x, const pcf_gri
                                   float dmax, uint32_t flags, double *hist, pcf_stats *stats);
 pcf_status profile_events(pcf_ctx *ctx, cudaEvent_t *a, cudaEvent_t *b);
 pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int kind, bool bpc,
-                         int *P_out);
+                         int *P_out, int refine = 0);

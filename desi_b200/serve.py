@@ -1,0 +1,274 @@
+"""Continuous-batching request server for correlation-function histograms.
+
+Requests (2iso / 2ani / 3iso, optionally periodic) name catalogs registered
+with the server.  The server keeps ``slots`` workers, each with its own
+library context (its own CUDA stream and memory pool) and its own cache of
+gridded catalogs resident in HBM (LRU by bytes).  A request is admitted as
+soon as a slot is free *and* its HBM footprint fits the budget -- requests
+that arrive while others run start immediately on another slot, so their
+kernels overlap on the device (continuous batching, not a queue).  The
+library calls release the GIL (ctypes), so slots run concurrently.
+
+Every result is computed by the same kernels whether a request runs alone
+or in the mix; ``tests/test_serve.py`` checks that the histograms are
+identical both ways.  ``python -m desi_b200.serve`` runs a seeded stream of
+mixed requests with Poisson arrivals and prints latency p50/p99 and
+throughput as one JSON line.
+"""
+from __future__ import annotations
+
+import collections
+import json
+import math
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import api
+
+KINDS = ("2iso", "2ani", "3iso")
+
+
+@dataclass
+class Request:
+    kind: str
+    data: str
+    rand: str
+    bins: int
+    dmax: float
+    bpc: bool = False
+    arrival: float = 0.0  # seconds from stream start (run_stream)
+    rid: int = 0
+    future: Future = field(default_factory=Future, repr=False)
+    t_submit: float = 0.0
+    t_start: float = 0.0
+    t_end: float = 0.0
+    slot: int = -1
+
+
+def grid_bytes(n: int, partitions: int = 64) -> int:
+    """Device bytes of one gridded catalog: raw + cell-ordered AoS + SoA planes,
+    cell table and tiles (upper bound)."""
+    return n * (16 + 16 + 16) + 4 * (partitions ** 3 + 1) + 16 * n + (1 << 20)
+
+
+def request_bytes(req: Request, sizes: dict) -> int:
+    """HBM footprint of a running request: its two grids (if it has to build
+    them), histograms and scratch (triplet lists spill to per-SM scratch in
+    the worst case)."""
+    nb = req.bins ** (3 if req.kind == "3iso" else (2 if req.kind == "2ani" else 1))
+    fp = 3 * 24 * nb + (8 << 20) + grid_bytes(sizes[req.data]) + grid_bytes(sizes[req.rand])
+    if req.kind == "3iso":
+        fp += 2 * 148 * 16 * max(sizes[req.data], sizes[req.rand])
+    return fp
+
+
+class _Slot:
+    def __init__(self, server: "PcfServer", idx: int, device: int, cache_bytes: int):
+        self.server = server
+        self.idx = idx
+        self.ctx = api.Context(device)
+        self.cache = collections.OrderedDict()  # (catalog, box) -> (Grid, bytes)
+        self.cache_bytes = cache_bytes
+        self.used = 0
+        self.busy = False
+
+    def grid(self, name: str, keep=()) -> api.Grid:
+        """The catalog gridded on this slot's device, built on first use and
+        kept resident; least recently used grids (not in `keep`) are freed
+        when the slot's cache exceeds its byte budget."""
+        cat = self.server.catalogs[name]
+        key = (name, cat["box"])
+        if key in self.cache:
+            self.cache.move_to_end(key)
+            return self.cache[key][0]
+        g = self.ctx.grid(cat["points"], cat["box"])
+        b = grid_bytes(len(cat["points"]))
+        self.cache[key] = (g, b)
+        self.used += b
+        for k in list(self.cache.keys()):
+            if self.used <= self.cache_bytes:
+                break
+            if k == key or k[0] in keep:
+                continue
+            old, ob = self.cache.pop(k)
+            old.free()
+            self.used -= ob
+        return g
+
+    def run(self, req: Request) -> dict:
+        keep = (req.data, req.rand)
+        gd, gr = self.grid(req.data, keep), self.grid(req.rand, keep)
+        c = self.ctx
+        if req.kind == "3iso":
+            kw = dict(bins=req.bins, dmax=req.dmax, bpc=req.bpc)
+            out = {"DDD": c.count_triplets(gd, **kw), "RRR": c.count_triplets(gr, **kw),
+                   "DDR": c.count_triplets(gd, gr, **kw), "DRR": c.count_triplets(gr, gd, **kw)}
+            units = 0.0
+        else:
+            kw = dict(bins=req.bins, dmax=req.dmax, bpc=req.bpc, ani=req.kind == "2ani", stats=True)
+            (dd, s1), (rr, s2), (dr, s3) = (c.count_pairs(gd, None, **kw), c.count_pairs(gr, None, **kw),
+                                            c.count_pairs(gd, gr, **kw))
+            out = {"DD": dd, "RR": rr, "DR": dr}
+            units = s1["pairs"] + s2["pairs"] + s3["pairs"]
+        out["_units"] = units
+        return out
+
+
+class PcfServer:
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int | None = None,
+                 cache_bytes: int = 8 << 30):
+        """hbm_budget: bytes the running requests may hold at once (default:
+        half the free device memory); cache_bytes: resident grids per slot."""
+        if hbm_budget is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info(device)
+            hbm_budget = int(free * 0.5)
+        self.hbm_budget = hbm_budget
+        self.catalogs: dict = {}
+        self._lock = threading.Condition()
+        self._pending: collections.deque = collections.deque()
+        self._in_use = 0
+        self._stop = False
+        self.slots = [_Slot(self, i, device, cache_bytes) for i in range(slots)]
+        self._threads = [threading.Thread(target=self._worker, args=(s,), daemon=True)
+                         for s in self.slots]
+        for t in self._threads:
+            t.start()
+
+    # -- catalogs ----------------------------------------------------------
+    def register(self, name: str, points: np.ndarray, box: float) -> None:
+        self.catalogs[name] = {"points": api.as_points(points), "box": float(box)}
+
+    # -- requests ----------------------------------------------------------
+    def submit(self, req: Request) -> Future:
+        req.t_submit = time.perf_counter()
+        with self._lock:
+            self._pending.append(req)
+            self._lock.notify_all()
+        return req.future
+
+    def _admissible(self, req: Request) -> bool:
+        """Admit while the running requests' footprints plus this one fit the
+        budget (resident grid caches are bounded per slot by cache_bytes); a
+        request that alone exceeds the budget runs when nothing else does."""
+        sizes = {k: len(v["points"]) for k, v in self.catalogs.items()}
+        need = request_bytes(req, sizes)
+        return self._in_use + need <= self.hbm_budget or self._in_use == 0
+
+    def _worker(self, slot: _Slot) -> None:
+        while True:
+            with self._lock:
+                req = None
+                while req is None:
+                    if self._stop:
+                        return
+                    for i, r in enumerate(self._pending):  # first admissible, in order
+                        if self._admissible(r):
+                            req = r
+                            del self._pending[i]
+                            break
+                    if req is None:
+                        self._lock.wait(0.05)
+                sizes = {k: len(v["points"]) for k, v in self.catalogs.items()}
+                fp = request_bytes(req, sizes)
+                self._in_use += fp
+            req.slot = slot.idx
+            req.t_start = time.perf_counter()
+            try:
+                res = slot.run(req)
+                req.t_end = time.perf_counter()
+                req.future.set_result(res)
+            except Exception as e:  # reported to the caller, the slot keeps serving
+                req.t_end = time.perf_counter()
+                req.future.set_exception(e)
+            finally:
+                with self._lock:
+                    self._in_use -= fp
+                    self._lock.notify_all()
+
+    def close(self) -> None:
+        with self._lock:
+            self._stop = True
+            self._lock.notify_all()
+        for t in self._threads:
+            t.join(timeout=5)
+        for s in self.slots:
+            for g, _ in s.cache.values():
+                g.free()
+            s.ctx.close()
+
+    # -- a timed stream ----------------------------------------------------
+    def run_stream(self, reqs: list[Request]) -> dict:
+        """Submit requests at their arrival times; wait for all; report."""
+        t0 = time.perf_counter()
+        for r in sorted(reqs, key=lambda r: r.arrival):
+            delay = t0 + r.arrival - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            self.submit(r)
+        results = [r.future.result() for r in reqs]
+        t1 = time.perf_counter()
+        lat = np.array([(r.t_end - r.t_submit) * 1e3 for r in reqs])
+        units = sum(res["_units"] for res in results)
+        return {"requests": len(reqs), "wall_s": t1 - t0,
+                "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                               "p99": float(np.percentile(lat, 99)),
+                               "max": float(lat.max())},
+                "pairs_per_s": units / (t1 - t0), "results": results}
+
+
+def make_stream(n_requests: int, rate_hz: float, seed: int = 5000, n_max: int = 200_000,
+                n3_max: int = 8_192) -> tuple[dict, list[Request]]:
+    """Seeded stream of mixed requests (served-stream shape: kinds 2iso/2ani/3iso
+    uniform, N log-uniform, bins 20-50, dmax 40-120 with dmax < L/2, box
+    250/500/1000, clustered or uniform, unit weights, Poisson arrivals).  N is
+    capped by n_max (n3_max for 3iso) so the stream fits a short run."""
+    from . import catalog
+    rng = np.random.default_rng(seed)
+    cats, reqs = {}, []
+    t = 0.0
+    for i in range(n_requests):
+        kind = KINDS[rng.integers(0, 3)]
+        box = float(rng.choice([250.0, 500.0, 1000.0]))
+        cap = n3_max if kind == "3iso" else n_max
+        n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(cap)))))
+        bins = int(rng.integers(20, 51)) if kind != "3iso" else int(rng.integers(10, 21))
+        dmax = float(rng.uniform(40.0, min(120.0, 0.45 * box)))
+        if kind == "3iso":
+            dmax = min(dmax, 0.25 * box, 60.0)
+        clustered = bool(rng.integers(0, 2))
+        dname, rname = f"d{i}", f"r{i}"
+        gen = catalog.neyman_scott if clustered else catalog.uniform
+        cats[dname] = (gen(n, box, seed=seed + 2 * i), box)
+        cats[rname] = (catalog.uniform(n, box, seed=seed + 2 * i + 1), box)
+        t += rng.exponential(1.0 / rate_hz)
+        reqs.append(Request(kind, dname, rname, bins, dmax, bpc=bool(rng.integers(0, 2)),
+                            arrival=t, rid=i))
+    return cats, reqs
+
+
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--rate", type=float, default=40.0)
+    ap.add_argument("--slots", type=int, default=4)
+    a = ap.parse_args(argv)
+    cats, reqs = make_stream(a.requests, a.rate)
+    srv = PcfServer(slots=a.slots)
+    for k, (p, box) in cats.items():
+        srv.register(k, p, box)
+    try:
+        rep = srv.run_stream(reqs)
+    finally:
+        srv.close()
+    rep.pop("results")
+    print(json.dumps(dict(rep, slots=a.slots, rate_hz=a.rate)))
+
+
+if __name__ == "__main__":
+    main()

@@ -30,3 +30,34 @@ def test_batch_equals_per_call(ctx, ani, bpc, w, graph):
         for i, g in enumerate(grs):
             cmp(rr[i], ctx.count_pairs(g, None, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
             cmp(dr[i], ctx.count_pairs(gd, g, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
+
+
+def test_autotune_and_estimator(ctx, tmp_path):
+    import oracle
+    box, bins, dmax = 250.0, 30, 80.0
+    D = catalog.neyman_scott(6000, box, seed=111)
+    R = catalog.uniform(6000, box, seed=112)
+    gd, gr = ctx.grid(D, box), ctx.grid(R, box)
+    res = ctx.autotune_pairs(gd, gr, bins=bins, dmax=dmax, bpc=True)
+    assert res["tried"] >= 10 and res["best_ms"] <= res["default_ms"] + 1e-6
+    assert ctx.tune_size == 1
+    # counts with the tuned shape still match the oracle bit for bit
+    dr = ctx.count_pairs(gd, gr, bins=bins, dmax=dmax, bpc=True)
+    assert np.array_equal(dr, oracle.pairs(D, R, box=box, bins=bins, dmax=dmax, bpc=True))
+    p = str(tmp_path / "tune.txt")
+    ctx.tune_save(p)
+    from desi_b200 import api
+    c2 = api.Context(0)
+    c2.tune_load(p)
+    assert c2.tune_size == 1
+    # Landy-Szalay as the reference's script computes it
+    dd = ctx.count_pairs(gd, None, bins=bins, dmax=dmax, bpc=True)
+    rr = ctx.count_pairs(gr, None, bins=bins, dmax=dmax, bpc=True)
+    xi = c2.estimate((dd, dr, rr))
+    DD, DR, RR = (np.where(h == 0, 1e-11, h) for h in (dd, dr, rr))
+    np.testing.assert_allclose(xi, (DD - 2 * DR + RR) / RR, rtol=1e-14)
+    z = c2.estimate((dd, dr, rr), n_d=6000, n_r=6000)
+    n = 6000.0
+    want = (DD / (n * (n - 1)) - 2 * DR / (n * n) + RR / (n * (n - 1))) / (RR / (n * (n - 1)))
+    np.testing.assert_allclose(z, want, rtol=1e-12)
+    c2.close()
