@@ -113,6 +113,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Largest value of x over all ranks (the step time of the slowest GPU)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, units_per_step: float, steps: int, max_total_ms: float) -> float:
+    """Whole-job rate: every rank processed units_per_step per step."""
+    return world * units_per_step * steps / (max_total_ms * 1e-3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from desi_b200 import api
@@ -196,22 +211,14 @@ def run_ours(args, rank, world, local_rank):
     probe = []
     step_device(probe, with_stats=True)
     times, _, clocks, launches, kprof = timed(step_device, args.steps, args.warmup)
-    tot_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = max_over_ranks(sum(times), world, dev)
     pairs_step = sum(s["pairs"] for s in probe)
-    value = world * pairs_step * args.steps / (tot_ms * 1e-3)
+    value = replica_throughput(world, pairs_step, args.steps, tot_ms)
 
     # end to end through the public API from pinned host buffers
     e_times, e_stats, e_clocks, _, _ = timed(step_e2e, args.steps, max(1, args.warmup // 2))
-    e_tot = sum(e_times)
-    if world > 1:
-        t = torch.tensor([e_tot], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e_tot = float(t.item())
-    e2e_value = world * pairs_step * args.steps / (e_tot * 1e-3)
+    e_tot = max_over_ranks(sum(e_times), world, dev)
+    e2e_value = replica_throughput(world, pairs_step, args.steps, e_tot)
     h2d = (len(D) + len(R)) * 16
     d2h = 3 * W["bins"] * 8 + 3 * W["bins"] * W["bins"] * 8
 

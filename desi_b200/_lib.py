@@ -90,6 +90,9 @@ _SIGS = {
                                                ctypes.c_int, ctypes.c_float, ctypes.c_uint32, _vp,
                                                _vp]),
     "pcf_ctx_launch_count": (_i64, [_vp]),
+    "pcf_read_catalog": (ctypes.c_int, [ctypes.c_char_p, _i64, _vp, ctypes.POINTER(_i64),
+                                        ctypes.POINTER(ctypes.c_float)]),
+    "pcf_write_catalog_f4": (ctypes.c_int, [ctypes.c_char_p, _vp, _i64]),
     "pcf_autotune_pairs": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_float,
                                           ctypes.c_uint32, _vp]),
     "pcf_tune_save": (ctypes.c_int, [_vp, ctypes.c_char_p]),

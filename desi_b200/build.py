@@ -34,7 +34,8 @@ def _stale(target, sources):
 
 
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
-    cu = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    cu = sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + [
+        s for s in sorted(glob.glob(os.path.join(CSRC, "*.cpp"))) if not s.endswith("pcf_main.cpp")]
     hdr = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
     lib_src = [s for s in cu if not s.endswith("pcf_main.cu")]
     if force or _stale(LIB, lib_src + hdr):

@@ -30,6 +30,26 @@ def read_catalog(path: str, n: int | None = None) -> np.ndarray:
     return np.ascontiguousarray(pts)
 
 
+def load(path: str, n: int) -> tuple[np.ndarray, float]:
+    """First n points of a text or .f4 catalog through the library's parallel
+    reader; returns (points, reference automatic box)."""
+    import ctypes
+
+    from . import _lib
+    out = np.zeros((n, 4), np.float32)
+    got = ctypes.c_int64()
+    box = ctypes.c_float()
+    rc = _lib.lib().pcf_read_catalog(path.encode(), n, out.ctypes.data_as(ctypes.c_void_p),
+                                     ctypes.byref(got), ctypes.byref(box))
+    if rc != 0:
+        raise IOError(f"{path}: could not read {n} points (status {rc})")
+    return out, box.value
+
+
+def save_f4(path: str, pts: np.ndarray) -> None:
+    np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 4).tofile(path)
+
+
 def write_catalog(path: str, pts: np.ndarray) -> None:
     pts = np.asarray(pts, np.float32)
     with open(path, "w") as f:

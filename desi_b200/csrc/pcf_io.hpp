@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/pcf.h"
+#include "../../include/pcf_ingest.h"
 
 namespace pcfio {
 
@@ -22,23 +23,19 @@ namespace pcfio {
 inline bool open_catalog(const std::string &name, long n, std::vector<pcf_point> &out,
                          float &box_candidate, std::string *err = nullptr) {
     const std::string path = "../data/" + name;
-    std::ifstream f(path.c_str(), std::ios::in | std::ios::binary);
-    if (f.fail()) {
-        if (err) *err = "Failed to load the file in " + path;
-        return false;
-    }
-    out.resize((size_t)n);
-    double mx = 0;
-    for (long c = 0; c < n; ++c) {
-        pcf_point &p = out[(size_t)c];
-        if (!(f >> p.x >> p.y >> p.z >> p.w)) {
-            if (err) *err = path + ": fewer than " + std::to_string(n) + " rows";
+    {
+        std::ifstream probe(path.c_str(), std::ios::in | std::ios::binary);
+        if (probe.fail()) {
+            if (err) *err = "Failed to load the file in " + path;
             return false;
         }
-        float m = p.x > p.y ? (p.x > p.z ? p.x : p.z) : (p.y > p.z ? p.y : p.z);
-        if (m > mx) mx = m;
     }
-    box_candidate = (float)std::ceil(mx + 1);
+    out.resize((size_t)n);
+    int64_t got = 0;
+    if (pcf_read_catalog(path.c_str(), n, out.data(), &got, &box_candidate) != PCF_OK) {
+        if (err) *err = path + ": fewer than " + std::to_string(n) + " readable rows";
+        return false;
+    }
     return true;
 }
 
