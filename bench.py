@@ -270,8 +270,128 @@ def run_ours(args, rank, world, local_rank):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(pairs_step)
+    if not args.no_extras:
+        # the other north-star forms, measured beside the headline (not the metric)
+        out["triplets"] = run_triplets(ctx, torch, stream)
+        out["batched"] = run_batched(ctx, torch, stream)
+        if rank == 0:
+            out["served"] = run_served()
     ctx.close()
     return out
+
+
+def _timed_ms(torch, stream, fn, reps=1):
+    ts = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return min(ts), r
+
+
+def run_triplets(ctx, torch, stream):
+    """Periodic 3iso on 32768 clustered + 32768 uniform points (box 250, 30^3
+    bins, dmax 80, unit weights): DDD, RRR, DDR, DRR, and the analytic
+    DDR/RRR path.  Unit: one unordered in-range triangle (XXY: one
+    unordered XX pair with one Y point)."""
+    from desi_b200 import catalog
+    D = catalog.neyman_scott(32768, 250.0, seed=3001, weights="unit")
+    R = catalog.uniform(32768, 250.0, seed=3002, weights="unit")
+    gd, gr = ctx.grid(D, 250.0), ctx.grid(R, 250.0)
+    kw = dict(bins=30, dmax=80.0, bpc=True, stats=True)
+    res = {}
+
+    def four():
+        out = {}
+        for name, a, b in (("DDD", gd, None), ("RRR", gr, None), ("DDR", gd, gr), ("DRR", gr, gd)):
+            _, st = ctx.count_triplets(a, b, **kw)
+            out[name] = st
+        return out
+
+    four()  # warm-up
+    ms, sts = _timed_ms(torch, stream, four)
+    tri = sum(s["pairs"] for s in sts.values())
+    res.update({"workload": "3iso periodic, 32768 Neyman-Scott + 32768 uniform, box 250, 30^3 "
+                            "bins, dmax 80, unit weights: DDD, RRR, DDR, DRR",
+                "ms": ms, "triangles": tri, "value": tri / (ms * 1e-3), "unit": "triplets/s",
+                "per_histogram_ms": {k: v["kernel_ms"] for k, v in sts.items()}})
+    ams, _ = _timed_ms(torch, stream, lambda: ctx.analytic_3iso(gd, bins=30, dmax=80.0,
+                                                                 with_ddd=False))
+    res["analytic_ddr_rrr_ms"] = ams
+    gd.free()
+    gr.free()
+    return res
+
+
+def run_batched(ctx, torch, stream):
+    """One clustered data catalog (200k, box 1000) against 32 uniform random
+    catalogs of log-uniform sizes 50k-400k, weights U(0.5,1.5), 40 bins,
+    dmax 120, iso and ani: per-call loop vs one persistent launch vs the same
+    launch replayed from a CUDA graph.  Unit: in-range pairs."""
+    import math
+    from desi_b200 import catalog
+    rng = np.random.default_rng(4000)
+    D = catalog.neyman_scott(200_000, 1000.0, seed=4001, weights="uniform")
+    sizes = [int(round(math.exp(rng.uniform(math.log(5e4), math.log(4e5))))) for _ in range(32)]
+    Rs = [catalog.uniform(n, 1000.0, seed=4100 + i, weights="uniform") for i, n in enumerate(sizes)]
+    gd = ctx.grid(D, 1000.0)
+    grs = [ctx.grid(R, 1000.0) for R in Rs]
+    out = {"workload": "1 x 200k Neyman-Scott vs 32 uniform randoms (50k-400k, log-uniform), "
+                       "box 1000, w~U(0.5,1.5), 40 bins, dmax 120, iso + ani",
+           "random_sizes": sizes}
+    for ani in (False, True):
+        kw = dict(bins=40, dmax=120.0, ani=ani)
+
+        def per_call():
+            n = 0.0
+            n += ctx.count_pairs(gd, None, stats=True, **kw)[1]["pairs"]
+            for g in grs:
+                n += ctx.count_pairs(g, None, stats=True, **kw)[1]["pairs"]
+                n += ctx.count_pairs(gd, g, stats=True, **kw)[1]["pairs"]
+            return n
+
+        def batched(graph):
+            return lambda: ctx.batch_pairs(gd, grs, stats=True, graph=graph, **kw)[1]["pairs"]
+
+        per_call()
+        ms_plain, units = _timed_ms(torch, stream, per_call)
+        batched(False)()
+        ms_batch, u2 = _timed_ms(torch, stream, batched(False), reps=2)
+        batched(True)()  # capture
+        ms_graph, u3 = _timed_ms(torch, stream, batched(True), reps=2)
+        key = "ani" if ani else "iso"
+        out[key] = {"pairs": units, "plain_ms": ms_plain, "batched_ms": ms_batch,
+                    "graph_ms": ms_graph, "plain_pairs_per_s": units / (ms_plain * 1e-3),
+                    "batched_pairs_per_s": u2 / (ms_batch * 1e-3),
+                    "graph_pairs_per_s": u3 / (ms_graph * 1e-3)}
+    for g in grs:
+        g.free()
+    gd.free()
+    return out
+
+
+def run_served():
+    """A seeded stream of mixed 2iso / 2ani / 3iso requests with Poisson
+    arrivals (desi_b200.serve.make_stream) through the continuous-batching
+    server with 4 slots: latency p50 / p99 and pairs/s."""
+    from desi_b200 import serve
+    cats, reqs = serve.make_stream(40, rate_hz=30.0)
+    srv = serve.PcfServer(slots=4)
+    for k, (p, box) in cats.items():
+        srv.register(k, p, box)
+    try:
+        rep = srv.run_stream(reqs)
+    finally:
+        srv.close()
+    rep.pop("results")
+    rep["workload"] = ("40 requests, Poisson 30/s, kinds 2iso/2ani/3iso, N log-uniform 1k-200k "
+                       "(3iso <= 8192), bins 20-50, dmax 40-120, box 250/500/1000, 4 slots")
+    return rep
 
 
 def _ref_engines():
@@ -383,6 +503,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the triplet / batched / served measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
