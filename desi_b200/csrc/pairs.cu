@@ -99,8 +99,9 @@ struct Sink {
     void *base;  // shared: this warp's region (lane column folded in); global: g_count / g_wsum
     __device__ __forceinline__ void add(int slot, float wa, float wb, bool pred) const {
         if (HM == H_LANE) {
-            if (WEIGHTED) {  // lane-private column: plain add of 0 or w_a*w_b
-                double *h = static_cast<double *>(base) + slot * 32;
+            if (WEIGHTED) {  // lane-private column: unconditional add of 0 or w_a*w_b,
+                // so a lane without a pair (its slot undefined) adds 0 to slot 0
+                double *h = static_cast<double *>(base) + (pred ? slot : 0) * 32;
                 *h += pred ? (double)wa * (double)wb : 0.0;
             } else {
                 red_s_u32(static_cast<unsigned *>(base) + slot * 32, 1u, pred);
@@ -196,7 +197,6 @@ __device__ __forceinline__ void take2(const PairArgs &A, const GridView &C, floa
     const FastCuts &fc = A.fc;
     const float2 DS2 = make_float2(fc.ds2, fc.ds2);
     const float2 MG = make_float2(kMagic, kMagic);
-    const int B1 = A.rule.bins - 1;
     bool f0 = false, f1 = false;
     float m0, m1;  // largest squared component, for the recheck test
     if (!ANI) {
@@ -212,8 +212,9 @@ __device__ __forceinline__ void take2(const PairArgs &A, const GridView &C, floa
             const unsigned q1 = __float_as_uint(Q.y) & 0x7FFFFFu;
             f0 = v0 && (D2.x < sg.lo) && fix_safe(q0, sg.w);
             f1 = v1 && (D2.y < sg.lo) && fix_safe(q1, sg.w);
-            sink.add(min((int)(q0 >> kFracBits), B1), h.w, Wt.x, f0);
-            sink.add(min((int)(q1 >> kFracBits), B1), h.w, Wt.y, f1);
+            // f0 / f1 imply r < bins away from an edge, so q >> 15 <= bins - 1
+            sink.add((int)(q0 >> kFracBits), h.w, Wt.x, f0);
+            sink.add((int)(q1 >> kFracBits), h.w, Wt.y, f1);
         }
     } else {
         const float2 ZZ = __fmul2_rn(DZ, DZ);
@@ -230,8 +231,8 @@ __device__ __forceinline__ void take2(const PairArgs &A, const GridView &C, floa
             f0 = v0 && (m0 < sg.lo) && fix_safe(z0, sg.w) && fix_safe(p0, sg.w);
             f1 = v1 && (m1 < sg.lo) && fix_safe(z1, sg.w) && fix_safe(p1, sg.w);
             const int B = A.rule.bins;
-            sink.add(min((int)(z0 >> kFracBits), B1) * B + min((int)(p0 >> kFracBits), B1), h.w, Wt.x, f0);
-            sink.add(min((int)(z1 >> kFracBits), B1) * B + min((int)(p1 >> kFracBits), B1), h.w, Wt.y, f1);
+            sink.add((int)(z0 >> kFracBits) * B + (int)(p0 >> kFracBits), h.w, Wt.x, f0);
+            sink.add((int)(z1 >> kFracBits) * B + (int)(p1 >> kFracBits), h.w, Wt.y, f1);
         }
     }
     if (WEIGHTED) n_pairs += (unsigned)f0 + (unsigned)f1;
@@ -378,9 +379,8 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
                 const float2 NHZ = make_float2(sg.sz - h.z, sg.sz - h.z);
                 const int jmin = (kind == 1 && seg == 0) ? hidx : a - 1;
                 if (lane == 0) n_cand += (unsigned long long)(b - a) * (unsigned long long)H;
-                const int a2 = a & ~1;
-                #pragma unroll 1
-                for (int p = a2 + 2 * sidx; p < b; p += 2 * S) {
+                // one aligned pair of candidates (p, p+1); v0 / v1 say which are real
+                auto step = [&](int p, bool v0, bool v1) {
                     const float2 X = __ldg(reinterpret_cast<const float2 *>(J.cand.x + p));
                     const float2 Y = __ldg(reinterpret_cast<const float2 *>(J.cand.y + p));
                     const float2 Z = __ldg(reinterpret_cast<const float2 *>(J.cand.z + p));
@@ -391,10 +391,22 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
                     const float2 DX = __fadd2_rn(X, NHX);
                     const float2 DY = __fadd2_rn(Y, NHY);
                     const float2 DZ = __fadd2_rn(Z, NHZ);
-                    take2<ANI, WEIGHTED, HM>(A, J.cand, DX, DY, DZ, p > jmin,
-                                             (p + 1 < b) && (p + 1 > jmin), p, Wt, h, sg, sink,
+                    take2<ANI, WEIGHTED, HM>(A, J.cand, DX, DY, DZ, v0, v1, p, Wt, h, sg, sink,
                                              n_pairs, n_rechk);
-                }
+                };
+                // head: pairs that start before a, or that reach into the home
+                // tile of a forward row (j > home index per lane); body: pairs
+                // fully inside (a, b) past the tile, no checks; tail: the last
+                // pair when it ends at b
+                const int chk = (kind == 1 && seg == 0) ? t.start + H : a + 1;
+                const int a2 = a & ~1;
+                const int stride = 2 * S;
+                int p = a2 + 2 * sidx;
+                for (; p < b && p < chk; p += stride)
+                    step(p, p > jmin && p >= a, (p + 1 < b) && (p + 1 > jmin));
+                #pragma unroll 2
+                for (; p + 1 < b; p += stride) step(p, true, true);
+                if (p < b) step(p, true, false);
             }
         }
         next = __shfl_sync(kFull, next, 0);
