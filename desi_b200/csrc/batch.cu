@@ -154,6 +154,11 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         pl.weighted = weighted;
         pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
         pl.mult = 1.0;
+        {
+            std::vector<const pcf_grid *> gs(R.begin(), R.end());
+            gs.push_back(D);
+            set_weight_fix(pl, gs.data(), (int)gs.size());
+        }
         auto enqueue = [&]() -> cudaError_t {
             cudaError_t e = cudaMemsetAsync(ap, 0, nacc * 16 + 128, st);
             if (e != cudaSuccess) return e;

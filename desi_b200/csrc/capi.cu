@@ -292,6 +292,10 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, cross);
     if (ds_override > 0) pl.rule.ds = ds_override;
     pl.mult = cross ? 1.0 : 2.0;
+    {
+        const pcf_grid *gs[2] = {a, cross ? b : a};
+        set_weight_fix(pl, gs, 2);
+    }
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
                      d_stats);
     if (s != PCF_OK) return s;

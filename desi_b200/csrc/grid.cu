@@ -73,24 +73,44 @@ namespace {
 
 constexpr int kScanItems = 1024;  // per block (256 threads x 4)
 
+// flags[0] |= 1: a coordinate outside [0, box); |= 2: a weight != 1; |= 4: a
+// negative or non-finite weight.  flags[1] = max |w| (float bits), flags[2] =
+// ~(bits of the smallest nonzero |w|) -- both by atomicMax, after a warp
+// reduction, so a launch makes one atomic per warp, not per point.
 __global__ void k_cell_ids(const float4 *__restrict__ pts, int64_t n, int P, float cell, float box,
                            int *__restrict__ cid, int *__restrict__ rank,
                            int *__restrict__ counts, int *__restrict__ flags) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float4 p = pts[i];
-    bool ok = (p.x >= 0.f) && (p.x < box) && (p.y >= 0.f) && (p.y < box) && (p.z >= 0.f) &&
-              (p.z < box);
-    if (!ok) atomicOr(flags, 1);
-    if (p.w != 1.0f) atomicOr(flags, 2);
-    int ix = (int)__fdiv_rn(p.x, cell), iy = (int)__fdiv_rn(p.y, cell),
-        iz = (int)__fdiv_rn(p.z, cell);
-    ix = min(max(ix, 0), P - 1);
-    iy = min(max(iy, 0), P - 1);
-    iz = min(max(iz, 0), P - 1);
-    int c = (ix * P + iy) * P + iz;
-    cid[i] = c;
-    rank[i] = atomicAdd(&counts[c], 1);
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned f = 0u, wmax = 0u, wminc = 0u;
+    if (i < n) {
+        const float4 p = pts[i];
+        const bool ok = (p.x >= 0.f) && (p.x < box) && (p.y >= 0.f) && (p.y < box) && (p.z >= 0.f) &&
+                        (p.z < box);
+        if (!ok) f |= 1u;
+        if (p.w != 1.0f) f |= 2u;
+        if (!(p.w >= 0.f) || !(p.w < INFINITY)) {
+            f |= 4u;
+        } else {
+            wmax = __float_as_uint(p.w);
+            if (p.w > 0.f) wminc = ~__float_as_uint(p.w);
+        }
+        int ix = (int)__fdiv_rn(p.x, cell), iy = (int)__fdiv_rn(p.y, cell),
+            iz = (int)__fdiv_rn(p.z, cell);
+        ix = min(max(ix, 0), P - 1);
+        iy = min(max(iy, 0), P - 1);
+        iz = min(max(iz, 0), P - 1);
+        const int c = (ix * P + iy) * P + iz;
+        cid[i] = c;
+        rank[i] = atomicAdd(&counts[c], 1);
+    }
+    f = __reduce_or_sync(0xffffffffu, f);
+    wmax = __reduce_max_sync(0xffffffffu, wmax);
+    wminc = __reduce_max_sync(0xffffffffu, wminc);
+    if ((threadIdx.x & 31) == 0) {
+        if (f) atomicOr(flags, (int)f);
+        if (wmax) atomicMax(reinterpret_cast<unsigned *>(flags) + 1, wmax);
+        if (wminc) atomicMax(reinterpret_cast<unsigned *>(flags) + 2, wminc);
+    }
 }
 
 // Exclusive scan of one 1024-element chunk per block; the chunk total goes to
@@ -252,22 +272,28 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     int *counts = ctx->scratch_b.as<int>();
     int *flags = ctx->d_flag.as<int>();
     PCF_CU(ctx, cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)(ncell + 1), st));
-    PCF_CU(ctx, cudaMemsetAsync(flags, 0, sizeof(int), st));
+    PCF_CU(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * 3, st));
     ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank, counts,
                                        cg->cell_start.as<int>(), ctx->scratch_c.as<int>(),
                                        cg->pts.as<float4>(), cg->soa.as<float>(), cg->plane, flags, st);
     PCF_CU(ctx, cudaGetLastError());
     cg->h_start.resize((size_t)(ncell + 1));
-    int hflags = 0;
+    unsigned hf[3] = {0u, 0u, 0u};
     PCF_CU(ctx, cudaMemcpyAsync(cg->h_start.data(), cg->cell_start.p, sizeof(int) * (ncell + 1),
                                 cudaMemcpyDeviceToHost, st));
-    PCF_CU(ctx, cudaMemcpyAsync(&hflags, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PCF_CU(ctx, cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    const int hflags = (int)hf[0];
     PCF_CU(ctx, cudaStreamSynchronize(st));
     if (hflags & 1) {
         ctx->last_error = "a coordinate lies outside [0, box)";
         return PCF_ERR_OUT_OF_BOX;
     }
     g->unit_weights = (hflags & 2) == 0;
+    g->w_finite_nonneg = (hflags & 4) == 0;
+    std::memcpy(&g->w_absmax, &hf[1], sizeof(float));
+    const unsigned mn = ~hf[2];
+    if (hf[2]) std::memcpy(&g->w_absmin, &mn, sizeof(float));
+    else g->w_absmin = 0.f;
     build_tiles(*cg);
     cg->d_tiles.pool = g->pool;
     PCF_CU(ctx, cg->d_tiles.ensure(sizeof(TileDesc) * std::max<size_t>(1, cg->tiles.size())));

@@ -2,6 +2,8 @@
 // on the device the library runs on (the roofline denominators):
 //   PCF_MB_FP32_FMA      FP32 FMA throughput, TFLOP/s (2 flops per FMA)
 //   PCF_MB_SMEM_ATOMIC   conflict-free shared-memory u32 atomicAdd, Gop/s
+//   PCF_MB_SMEM_ATOMIC_F64 / _U64 / _F32   the same for f64 / u64 / f32 adds
+//                        (the weighted histograms' accumulator types)
 // Each runs ~10-50 ms, timed with CUDA events on the context stream.
 #include "pcf_internal.cuh"
 #include "../../include/pcf_bench.h"
@@ -22,18 +24,19 @@ __global__ void __launch_bounds__(256) k_fma(float *out, int iters, float a, flo
     if (s == 1234.5f) out[0] = s;  // keeps the chains live
 }
 
+template <typename T>
 __global__ void __launch_bounds__(256) k_smem_atomic(unsigned *out, int iters) {
-    __shared__ unsigned h[256 * 4];
-    for (int k = threadIdx.x; k < 256 * 4; k += 256) h[k] = 0;
+    __shared__ T h[256 * 4];
+    for (int k = threadIdx.x; k < 256 * 4; k += 256) h[k] = T(0);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned *mine = h + warp * 32 + lane;  // distinct bank per lane
+    T *mine = h + warp * 32 + lane;  // distinct address per lane, no conflicts between lanes
     for (int i = 0; i < iters; ++i) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k) atomicAdd(mine + ((k & 3) << 8), 1u);
+        for (int k = 0; k < 16; ++k) atomicAdd(mine + ((k & 3) << 8), T(1));
     }
     __syncthreads();
-    if (h[threadIdx.x] == 0xFFFFFFFFu) out[0] = 1;
+    if (h[threadIdx.x] == T(123456789)) out[0] = 1;
 }
 
 }  // namespace
@@ -51,9 +54,14 @@ extern "C" pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result) {
             const int iters = 2048;
             k_fma<<<blocks, threads, 0, ctx->stream>>>(ctx->d_flag.as<float>(), iters, 0.999f, 0.001f);
             ops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
-        } else if (which == PCF_MB_SMEM_ATOMIC) {
+        } else if (which >= PCF_MB_SMEM_ATOMIC && which <= PCF_MB_SMEM_ATOMIC_F32) {
             const int iters = 512;
-            k_smem_atomic<<<blocks, threads, 0, ctx->stream>>>(ctx->d_flag.as<unsigned>(), iters);
+            unsigned *o = ctx->d_flag.as<unsigned>();
+            if (which == PCF_MB_SMEM_ATOMIC) k_smem_atomic<unsigned><<<blocks, threads, 0, ctx->stream>>>(o, iters);
+            else if (which == PCF_MB_SMEM_ATOMIC_F64) k_smem_atomic<double><<<blocks, threads, 0, ctx->stream>>>(o, iters);
+            else if (which == PCF_MB_SMEM_ATOMIC_U64)
+                k_smem_atomic<unsigned long long><<<blocks, threads, 0, ctx->stream>>>(o, iters);
+            else k_smem_atomic<float><<<blocks, threads, 0, ctx->stream>>>(o, iters);
             ops = 16.0 * (double)iters * blocks * threads;
         } else {
             return PCF_ERR_INVALID_ARG;

@@ -40,7 +40,15 @@ constexpr float kMagic = 256.0f;  // r + 256 -> low mantissa bits = round(r * 2^
 constexpr int kFracBits = 15;
 constexpr unsigned kFracMask = (1u << kFracBits) - 1u;
 
-enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2 };
+enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3 };
+
+// H_WFIX (weighted, per-warp copy): each product w_a*w_b is rounded to an
+// integer v = round(w_a*w_b * 2^s) < 2^64 and added as four 16-bit limbs, each
+// with a 32-bit shared reduction (several times faster than a 64-bit one).
+// A limb counter absorbs kWfixBudget adds of < 2^16 before it could wrap, so a
+// warp flushes its copy after at most that many pair tests.
+constexpr int kWfixBudget = 65536;
+constexpr int kWfixChunk = kWfixBudget / 32;  // candidates per budget check (<= 32 homes each)
 
 // Fast-path cut constants for one range type (0: unshifted, 1: image-shifted).
 struct FastCuts {
@@ -65,6 +73,9 @@ struct PairArgs {
     unsigned long long *g_count;
     double *g_wsum;
     unsigned long long *g_stats;
+    float wscale;     // H_WFIX: 2^s, applied to the home weight
+    double wunscale;  // H_WFIX: 2^-s
+    int wlimbs;       // H_WFIX: limbs per bin (3: v < 2^48, 4: v < 2^64)
 };
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -97,8 +108,18 @@ __device__ __forceinline__ void red_s_f64(const void *p, double v, bool pred) {
 template <bool WEIGHTED, int HM>
 struct Sink {
     void *base;  // shared: this warp's region (lane column folded in); global: g_count / g_wsum
+    int plane;   // H_WFIX: u32 words between limb planes (bins of the histogram)
+    bool four;   // H_WFIX: the top limb is in use
     __device__ __forceinline__ void add(int slot, float wa, float wb, bool pred) const {
-        if (HM == H_LANE) {
+        if (HM == H_WFIX) {  // wa carries the 2^s scale; w_a*w_b is exact in FP64
+            const unsigned long long v = __double2ull_rn((double)wa * (double)wb);
+            unsigned *b = static_cast<unsigned *>(base) + slot;
+            const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+            red_s_u32(b, lo & 0xFFFFu, pred);
+            red_s_u32(b + plane, lo >> 16, pred);
+            red_s_u32(b + 2 * plane, hi & 0xFFFFu, pred);
+            red_s_u32(b + 3 * plane, hi >> 16, pred && four);
+        } else if (HM == H_LANE) {
             if (WEIGHTED) {  // lane-private column: unconditional add of 0 or w_a*w_b,
                 // so a lane without a pair (its slot undefined) adds 0 to slot 0
                 double *h = static_cast<double *>(base) + (pred ? slot : 0) * 32;
@@ -184,6 +205,37 @@ __device__ __forceinline__ void flush_hist(typename std::conditional<WEIGHTED, d
     (void)per_warp;
 }
 
+__device__ __forceinline__ void flush_wfix(unsigned *mine, int nb, int limbs, int lane,
+                                           const PairArgs &A, int slot);
+template <bool WEIGHTED, int HM, typename HT>
+__device__ __forceinline__ void flush_any(HT *mine, int nb, int per_warp, int lane, const PairArgs &A,
+                                          int slot) {
+    if (HM == H_WFIX) flush_wfix(reinterpret_cast<unsigned *>(mine), nb, A.wlimbs, lane, A, slot);
+    else flush_hist<WEIGHTED, HM>(reinterpret_cast<typename std::conditional<WEIGHTED, double, unsigned>::type *>(mine),
+                                  nb, per_warp, lane, A, slot);
+}
+
+// H_WFIX flush: limbs -> FP64 sum * 2^-s into histogram `slot`; clears the copy.
+__device__ __forceinline__ void flush_wfix(unsigned *mine, int nb, int limbs, int lane,
+                                           const PairArgs &A, int slot) {
+    __syncwarp();
+    const size_t off = (size_t)slot * nb;
+    for (int k = lane; k < nb; k += 32) {
+        const unsigned l0 = mine[k], l1 = mine[nb + k], l2 = mine[2 * nb + k];
+        const unsigned l3 = limbs == 4 ? mine[3 * nb + k] : 0u;
+        mine[k] = 0u;
+        mine[nb + k] = 0u;
+        mine[2 * nb + k] = 0u;
+        if (limbs == 4) mine[3 * nb + k] = 0u;
+        if (l0 | l1 | l2 | l3) {
+            // each term is exact; the sum of the four rounds once or twice
+            const double v = ((double)l3 * 0x1p48 + (double)l2 * 0x1p32) + ((double)l1 * 0x1p16 + (double)l0);
+            atomicAdd(A.g_wsum + off + k, v * A.wunscale);
+        }
+    }
+    __syncwarp();
+}
+
 // One candidate pair of elements (packed): distance test, fixed-point bin,
 // predicated accumulate.  Pairs within the edge window of a bin, near dmax,
 // or at zero separation (frac(r) = 0 fails the window test) go to the FP64
@@ -256,19 +308,24 @@ __device__ __forceinline__ void take2(const PairArgs &A, const GridView &C, floa
 #define PCF_PAIR_MINB 6
 #endif
 template <bool ANI, bool WEIGHTED, int HM>
-__global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArgs A) {
-    typedef typename std::conditional<WEIGHTED, double, unsigned>::type HT;
+// H_WFIX copies take 3-4x the shared memory of a u32 copy, which already
+// holds those launches to ~5 CTAs per SM: let them use the registers of 5.
+__global__ void __launch_bounds__(kThreads, HM == H_WFIX ? 5 : PCF_PAIR_MINB) k_pairs(const PairArgs A) {
+    typedef typename std::conditional<WEIGHTED && HM != H_WFIX, double, unsigned>::type HT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     HT *hist_all = reinterpret_cast<HT *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int bins = A.rule.bins;
     const int nb = ANI ? bins * bins : bins;
-    const int per_warp = HM == H_LANE ? nb * 32 : (HM == H_WARP ? nb : 0);
+    const int per_warp = HM == H_LANE ? nb * 32 : (HM == H_WARP ? nb : (HM == H_WFIX ? nb * A.wlimbs : 0));
     HT *mine = hist_all + warp * per_warp;
     for (int k = lane; k < per_warp; k += 32) mine[k] = (HT)0;
     __syncwarp();
     Sink<WEIGHTED, HM> sink;
     if (HM != H_GLOBAL) sink.base = HM == H_LANE ? (void *)(mine + lane) : (void *)mine;
+    sink.plane = nb;
+    sink.four = A.wlimbs == 4;
+    int wfix_since = 0;  // H_WFIX: pair tests since this warp's last flush
     unsigned n_pairs = 0, n_rechk = 0;
     unsigned long long n_cand = 0;
     // current job (items of one warp arrive in increasing order), kept in
@@ -285,7 +342,8 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
         const long long it_idx = next;
         if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next item
         if (it_idx >= job_end) {  // entering another job: flush this one's histogram
-            if (cj >= 0) flush_hist<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
+            if (cj >= 0) flush_any<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
+            wfix_since = 0;
             do {
                 ++cj;
                 job_end = cj + 1 < A.n_jobs ? A.jobs[cj + 1].item_begin : A.n_items;
@@ -317,6 +375,7 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
         Home h;
         if (valid) {
             h.x = J.home.x[hidx]; h.y = J.home.y[hidx]; h.z = J.home.z[hidx]; h.w = J.home.w[hidx];
+            if (HM == H_WFIX) h.w *= A.wscale;  // exact: a power of two, range checked by the host
         } else {
             h.x = h.y = h.z = __int_as_float(0x7fc00000);  // NaN: never in range
             h.w = 0.f;
@@ -401,19 +460,36 @@ __global__ void __launch_bounds__(kThreads, PCF_PAIR_MINB) k_pairs(const PairArg
                 const int chk = (kind == 1 && seg == 0) ? t.start + H : a + 1;
                 const int a2 = a & ~1;
                 const int stride = 2 * S;
-                int p = a2 + 2 * sidx;
-                for (; p < b && p < chk; p += stride)
-                    step(p, p > jmin && p >= a, (p + 1 < b) && (p + 1 > jmin));
-                #pragma unroll 2
-                for (; p + 1 < b; p += stride) step(p, true, true);
-                if (p < b) step(p, true, false);
+                // candidates [lo, hi) (lo even; hi even or b)
+                auto run = [&](int lo, int hi) {
+                    int p = lo + 2 * sidx;
+                    for (; p < hi && p < chk; p += stride)
+                        step(p, p > jmin && p >= a, (p + 1 < b) && (p + 1 > jmin));
+                    #pragma unroll 2
+                    for (; p + 1 < hi; p += stride) step(p, true, true);
+                    if (p < hi) step(p, true, false);
+                };
+                if (HM == H_WFIX) {  // flush before a limb counter could wrap
+                    for (int lo = a2; lo < b; lo += kWfixChunk) {
+                        const int hi = min(b, lo + kWfixChunk);
+                        const int tests = (hi - lo) * H;
+                        if (wfix_since + tests > kWfixBudget) {
+                            flush_any<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
+                            wfix_since = 0;
+                        }
+                        wfix_since += tests;
+                        run(lo, hi);
+                    }
+                } else {
+                    run(a2, b);
+                }
             }
         }
         next = __shfl_sync(kFull, next, 0);
     }
     // per-warp flush (no CTA barrier: warps leave as the queue drains)
     __syncwarp();
-    if (cj >= 0) flush_hist<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
+    if (cj >= 0) flush_any<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
     unsigned long long rp = n_pairs, rr = n_rechk;
     for (int off = 16; off > 0; off >>= 1) {
         rr += __shfl_down_sync(kFull, rr, off);
@@ -597,11 +673,17 @@ static cudaError_t dispatch_pairs(const PairArgs &A, const PairLaunch &pl, cudaS
     const size_t warp_bytes = (size_t)nb * kWarps * ebytes;
     int hm;
     size_t smem;
+    const bool wfix_ok = pl.weighted && pl.wlimbs >= 3 && pl.rule.bins <= 255;
+    const size_t wfix_bytes = (size_t)nb * 4 * pl.wlimbs * kWarps;
     if (pl.rule.bins > 255 || warp_bytes > 160 * 1024) { hm = H_GLOBAL; smem = 0; }
     else if (!pl.ani && lane_bytes <= 64 * 1024) { hm = H_LANE; smem = lane_bytes; }
     else { hm = H_WARP; smem = warp_bytes; }
+    if (hm == H_WARP && wfix_ok && wfix_bytes <= 160 * 1024) { hm = H_WFIX; smem = wfix_bytes; }
     // an autotuned scheme overrides the rule above when it is valid here
     if (pl.hist_mode == H_GLOBAL) { hm = H_GLOBAL; smem = 0; }
+    else if (pl.hist_mode == H_WFIX && wfix_ok && wfix_bytes <= 160 * 1024) {
+        hm = H_WFIX; smem = wfix_bytes;
+    }
     else if (pl.hist_mode == H_WARP && pl.rule.bins <= 255 && warp_bytes <= 160 * 1024) {
         hm = H_WARP; smem = warp_bytes;
     } else if (pl.hist_mode == H_LANE && !pl.ani && pl.rule.bins <= 255 && lane_bytes <= 64 * 1024) {
@@ -612,6 +694,7 @@ static cudaError_t dispatch_pairs(const PairArgs &A, const PairLaunch &pl, cudaS
     if (pl.weighted) {                                                                           \
         if (hm == H_LANE) return launch_one<ANI_, true, H_LANE>(A, smem, n, st, sm_count, device);   \
         if (hm == H_WARP) return launch_one<ANI_, true, H_WARP>(A, smem, n, st, sm_count, device);   \
+        if (hm == H_WFIX) return launch_one<ANI_, true, H_WFIX>(A, smem, n, st, sm_count, device);   \
         return launch_one<ANI_, true, H_GLOBAL>(A, smem, n, st, sm_count, device);                 \
     } else {                                                                                     \
         if (hm == H_LANE) return launch_one<ANI_, false, H_LANE>(A, smem, n, st, sm_count, device);  \
@@ -639,7 +722,41 @@ static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
     A.g_count = d_count;
     A.g_wsum = d_wsum;
     A.g_stats = d_stats;
+    A.wscale = pl.wscale;
+    A.wunscale = pl.wlimbs ? 1.0 / (double)pl.wscale : 0.0;
+    A.wlimbs = pl.wlimbs;
     return A;
+}
+
+// Scale of the fixed-point weighted histograms of a launch whose points come
+// from grids gs[0..n): s such that every nonzero product w_a*w_b is at least
+// 2^42 after scaling (rounding it costs at most 2^-43 of its value), with
+// the largest below 2^48 (three limbs) or 2^64 (four).  Weights must be
+// finite and >= 0, and each weight * 2^s a normal float.  Otherwise the
+// launch keeps FP64 shared atomics (wlimbs = 0).
+void set_weight_fix(PairLaunch &pl, const pcf_grid *const *gs, int n) {
+    pl.wscale = 0.f;
+    pl.wlimbs = 0;
+    if (!pl.weighted) return;
+    double wmin = 0.0, wmax = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const pcf_grid *g = gs[i];
+        if (!g->w_finite_nonneg) return;
+        wmax = std::max(wmax, (double)g->w_absmax);
+        if (g->w_absmin > 0.f) wmin = wmin > 0.0 ? std::min(wmin, (double)g->w_absmin) : (double)g->w_absmin;
+    }
+    if (!(wmin > 0.0)) return;
+    const double pmin = wmin * wmin, pmax = wmax * wmax;  // exact: 24-bit mantissas
+    const int s = 42 - (int)std::floor(std::log2(pmin));
+    if (s < -120 || s > 120) return;
+    const double top = std::ldexp(pmax, s);
+    int limbs;
+    if (top < std::ldexp(1.0, 48) - 1.0) limbs = 3;
+    else if (top < std::ldexp(1.0, 64) - 4096.0) limbs = 4;
+    else return;
+    if (std::ldexp(wmin, s) < std::ldexp(1.0, -125) || std::ldexp(wmax, s) >= std::ldexp(1.0, 126)) return;
+    pl.wscale = std::ldexp(1.0f, s);
+    pl.wlimbs = limbs;
 }
 
 cudaError_t launch_pair_jobs(const PairJob *d_jobs, int n_jobs, long long n_items, int P, float box,

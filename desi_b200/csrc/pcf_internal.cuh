@@ -149,6 +149,11 @@ struct pcf_grid {
     int64_t n = 0;
     float box = 0.f;
     bool unit_weights = true;
+    // weight range, for the fixed-point weighted histograms: max |w|, the
+    // smallest nonzero |w| (0 if every weight is 0), and whether every
+    // weight is finite and >= 0
+    float w_absmax = 1.f, w_absmin = 1.f;
+    bool w_finite_nonneg = true;
     DevBuf raw;                   // float4 x n, input order
     std::unique_ptr<CellGrid> cells;
 };
@@ -235,8 +240,12 @@ struct PairLaunch {
     bool ani, weighted, bpc, self;
     PairRule rule;
     double mult;         // 2 for XX (ordered-pair convention), 1 for XY
-    int hist_mode = -1;  // 0 lane-private, 1 per-warp shared, 2 global; -1 automatic
+    int hist_mode = -1;  // 0 lane-private, 1 per-warp shared, 2 global, 3 per-warp
+                         // fixed-point (weighted); -1 automatic
+    float wscale = 0.f;  // fixed-point weighted sums: 2^s (set_weight_fix)
+    int wlimbs = 0;      // 0: not available for this launch
 };
+void set_weight_fix(PairLaunch &pl, const pcf_grid *const *gs, int n);
 std::string tune_key(int kind, bool bpc, bool cross, bool weighted, int bins, int64_t n, float box,
                      float dmax);
 pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home,

@@ -12,10 +12,17 @@
 extern "C" {
 #endif
 
-enum { PCF_MB_FP32_FMA = 0, PCF_MB_SMEM_ATOMIC = 1 };
+enum {
+    PCF_MB_FP32_FMA = 0,
+    PCF_MB_SMEM_ATOMIC = 1,
+    PCF_MB_SMEM_ATOMIC_F64 = 2,
+    PCF_MB_SMEM_ATOMIC_U64 = 3,
+    PCF_MB_SMEM_ATOMIC_F32 = 4
+};
 
 /* PCF_MB_FP32_FMA: FP32 FMA throughput in TFLOP/s; PCF_MB_SMEM_ATOMIC:
- * conflict-free shared-memory 32-bit atomicAdd throughput in Gop/s. */
+ * conflict-free shared-memory 32-bit atomicAdd throughput in Gop/s; _F64,
+ * _U64, _F32: the same for 64-bit float, 64-bit integer and 32-bit float adds. */
 pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
 
 /* Kernels this context has launched since it was created. */

@@ -138,3 +138,53 @@ def test_grid_is_a_permutation_in_cell_order(ctx):
     idx = np.minimum((pts[:, :3] / cell).astype(np.int64), P - 1)
     cid = (idx[:, 0] * P + idx[:, 1]) * P + idx[:, 2]
     assert np.all(np.diff(cid) >= 0)
+
+
+def _weighted(pts, rng, kind):
+    out = pts.copy()
+    n = len(out)
+    if kind == "wide":      # log-uniform over three decades: four-limb fixed point
+        out[:, 3] = np.exp(rng.uniform(np.log(0.01), np.log(10.0), n)).astype(np.float32)
+    elif kind == "zeros":   # a third of the weights exactly zero
+        w = rng.uniform(0.5, 1.5, n).astype(np.float32)
+        w[rng.random(n) < 0.33] = 0.0
+        out[:, 3] = w
+    elif kind == "signed":  # negative weights: FP64 shared sums
+        out[:, 3] = rng.uniform(-1.0, 1.0, n).astype(np.float32)
+    return out
+
+
+@pytest.mark.parametrize("kind", ["wide", "zeros", "signed"])
+@pytest.mark.parametrize("ani,bins", [(True, 30), (False, 100)])
+def test_weighted_sum_paths(ctx, kind, ani, bins):
+    """Weighted histograms through the fixed-point limb sums (three or four
+    limbs, zero weights) and the FP64 fallback (negative weights), against
+    the FP64 oracle.  The signed case is compared on |oracle| + 1 to keep the
+    relative bound meaningful where positive and negative terms cancel."""
+    rng = np.random.default_rng(17)
+    box = 200.0
+    D = _weighted(catalog.neyman_scott(2500, box, seed=21), rng, kind)
+    R = _weighted(catalog.uniform(2600, box, seed=22), rng, kind)
+    gd, gr = ctx.grid(D, box), ctx.grid(R, box)
+    for bpc in (False, True):
+        for (a, b, A, B) in ((gd, None, D, None), (gd, gr, D, R)):
+            got = ctx.count_pairs(a, b, bins=bins, dmax=60.0, ani=ani, bpc=bpc)
+            want = oracle.pairs(A, B, box=box, bins=bins, dmax=60.0, ani=ani, bpc=bpc)
+            if kind == "signed":
+                assert np.all(np.abs(got - want) <= RTOL_W * (np.abs(want) + 1.0))
+            else:
+                _cmp(got, want, True)
+
+
+def test_weighted_dense_cells_flush_budget(ctx):
+    """Tight clusters: a warp runs far more than 65536 pair tests, so the
+    fixed-point copies flush mid-launch before a limb counter could wrap."""
+    rng = np.random.default_rng(5)
+    box = 100.0
+    D = catalog.neyman_scott(12000, box, seed=31, children=2000, sigma=1.0, weights="uniform")
+    g = ctx.grid(D, box)
+    for ani in (False, True):
+        got, st = ctx.count_pairs(g, None, bins=30, dmax=20.0, ani=ani, stats=True)
+        want = oracle.pairs(D, None, box=box, bins=30, dmax=20.0, ani=ani)
+        _cmp(got, want, True)
+        assert st["candidates"] > 64 * 65536
