@@ -103,7 +103,7 @@ class Context:
             outp = out.ctypes.data_as(ctypes.c_void_p)
         rc = self._lib.pcf_count_pairs(self.handle, PCF_ANI if ani else PCF_ISO, a.handle,
                                        b.handle if b is not None else None, int(bins),
-                                       float(dmax), f, outp, ctypes.byref(st))
+                                       float(dmax), f, outp, ctypes.byref(st) if stats else None)
         _check(self.handle, rc, "pcf_count_pairs")
         if out is not None and ani:
             out = out.reshape(bins, bins)

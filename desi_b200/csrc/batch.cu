@@ -69,8 +69,8 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     if (use_graph) {
         std::ostringstream os;
         os << kind << ':' << bins << ':' << dmax << ':' << (flags & ~PCF_GRAPH) << ':' << (dd != nullptr)
-           << (rr != nullptr) << (dr != nullptr) << ':' << D->cells->pts.p;
-        for (auto *g : R) os << ',' << g->cells->pts.p;
+           << (rr != nullptr) << (dr != nullptr) << ':' << D->cells->serial;
+        for (auto *g : R) os << ',' << g->cells->serial;
         key = os.str();
     }
     std::shared_ptr<BatchGraph> bg;
@@ -79,6 +79,18 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         if (it != ctx->graphs.end()) bg = it->second;
     }
     cudaStream_t st = ctx->stream;
+    PairLaunch pl;
+    pl.ani = ani;
+    pl.bpc = bpc;
+    pl.self = false;
+    pl.weighted = weighted;
+    pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
+    pl.mult = 1.0;
+    {
+        std::vector<const pcf_grid *> gs(R.begin(), R.end());
+        gs.push_back(D);
+        set_weight_fix(pl, gs.data(), (int)gs.size());
+    }
     if (!bg) {
         bg = std::make_shared<BatchGraph>();
         bg->plan.pool = ctx->pool;
@@ -110,8 +122,9 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         for (int k = 0; k < nslots; ++k) {
             const CellGrid &h = *js[k].h->cells, &c = *js[k].c->cells;
             PairJob &j = jobs[k];
-            j.home = GridView{h.x(), h.y(), h.z(), h.w(), h.cell_start.as<int>()};
-            j.cand = GridView{c.x(), c.y(), c.z(), c.w(), c.cell_start.as<int>()};
+            j.home = pair_view(h, pl.wfix);
+            j.cand = pair_view(c, pl.wfix);
+            j.wunscale = weight_unscale(js[k].h, js[k].c);
             j.tiles = h.d_tiles.as<TileDesc>();
             j.rows = reinterpret_cast<const RowDesc *>(dp + (js[k].self ? 0 : off_c));
             shape_job(j, (int64_t)h.tiles.size(), (int)(js[k].self ? rows_self.size() : rows_cross.size()),
@@ -147,18 +160,6 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         bg->mult = mult;
         bg->d_out = out;
         bg->d_stats = stt;
-        PairLaunch pl;
-        pl.ani = ani;
-        pl.bpc = bpc;
-        pl.self = false;
-        pl.weighted = weighted;
-        pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
-        pl.mult = 1.0;
-        {
-            std::vector<const pcf_grid *> gs(R.begin(), R.end());
-            gs.push_back(D);
-            set_weight_fix(pl, gs.data(), (int)gs.size());
-        }
         auto enqueue = [&]() -> cudaError_t {
             cudaError_t e = cudaMemsetAsync(ap, 0, nacc * 16 + 128, st);
             if (e != cudaSuccess) return e;

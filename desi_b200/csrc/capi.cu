@@ -128,6 +128,7 @@ pcf_status pcf_grid_build(pcf_ctx *ctx, const pcf_point *pts, int64_t n, float b
                                 is_device_ptr(pts) ? cudaMemcpyDeviceToDevice
                                                    : cudaMemcpyHostToDevice,
                                 ctx->stream));
+    g->user_P = partitions;
     int P = partitions > 0 ? partitions : choose_partitions(n, box, box / 8.f, PCF_ISO, false, 4);
     pcf_status s = grid_ensure_cells(ctx, g.get(), P);
     if (s != PCF_OK) return s;
@@ -219,7 +220,16 @@ pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int
         return PCF_ERR_UNSUPPORTED;
     }
     int64_t n = std::max<int64_t>(a->n, b ? b->n : 0);
-    int P = choose_partitions(n, box, dmax, kind, bpc, refine);
+    // partitions: the autotuner's candidate, else the caller's choice at
+    // grid build, else the tuned or default rule
+    int P = 0;
+    if (ctx->tune_override.refine <= 0) P = a->user_P > 0 ? a->user_P : (b ? b->user_P : 0);
+    if (P > 0 && bpc) {  // a periodic stencil must not wrap onto itself: else automatic
+        const double cell = (double)box / P;
+        const int k = (int)std::ceil(((double)dmax + 1e-4 * cell + 8.0 * box * 1.2e-7) / cell);
+        if (2 * k + 2 > P) P = 0;
+    }
+    if (P <= 0) P = choose_partitions(n, box, dmax, kind, bpc, refine);
     if (bpc) {
         double cell = (double)box / P;
         int k = (int)std::ceil(((double)dmax + 1e-4 * cell + 8.0 * box * 1.2e-7) / cell);
@@ -295,7 +305,9 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     {
         const pcf_grid *gs[2] = {a, cross ? b : a};
         set_weight_fix(pl, gs, 2);
+        pl.wunscale = weight_unscale(a, cross ? b : a);
     }
+    pl.count = stats != nullptr;
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
                      d_stats);
     if (s != PCF_OK) return s;

@@ -148,18 +148,49 @@ __global__ void k_scan_add(int *__restrict__ out, const int *__restrict__ offs, 
         if (i < n) out[i] += add;
 }
 
+// Biased exponents of the weight range (flags[1] = bits of max |w|, flags[2]
+// = ~bits of the smallest nonzero |w|) and whether the weights have exact
+// integer images q = w * 2^(150 - emin) below 2^32: every weight finite and
+// >= 0, the nonzero ones normal and within 8 binades of each other.
+__host__ __device__ inline bool weight_fix_range(unsigned f0, unsigned wmaxb, unsigned wminc, int *emin,
+                                                 int *emax) {
+    *emin = (int)((~wminc >> 23) & 0xFFu);
+    *emax = (int)((wmaxb >> 23) & 0xFFu);
+    return !(f0 & 4u) && wminc != 0u && *emin >= 1 && *emax - *emin <= 8;
+}
+
 __global__ void k_scatter(const float4 *__restrict__ pts, int64_t n, const int *__restrict__ cid,
                           const int *__restrict__ rank, const int *__restrict__ start,
-                          float4 *__restrict__ out, float *__restrict__ soa, size_t plane) {
+                          float4 *__restrict__ out, float *__restrict__ soa, size_t plane,
+                          float *__restrict__ pk, unsigned *__restrict__ qw,
+                          const int *__restrict__ flags) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pts[i];
     const int64_t d = start[cid[i]] + rank[i];
     if (out) out[d] = p;
-    soa[d] = p.x;
-    soa[plane + d] = p.y;
-    soa[2 * plane + d] = p.z;
-    soa[3 * plane + d] = p.w;
+    if (soa) {
+        soa[d] = p.x;
+        soa[plane + d] = p.y;
+        soa[2 * plane + d] = p.z;
+        soa[3 * plane + d] = p.w;
+    }
+    // pair-packed block d/2: (x0 x1 y0 y1)(z0 z1 w0 w1)
+    float *blk = pk + (d >> 1) * 8 + (d & 1);
+    blk[0] = p.x;
+    blk[2] = p.y;
+    blk[4] = p.z;
+    blk[6] = p.w;
+    if (qw) {
+        int emin, emax;
+        const unsigned *uf = reinterpret_cast<const unsigned *>(flags);
+        unsigned q = 0u;
+        if (weight_fix_range(uf[0], uf[1], uf[2], &emin, &emax)) {
+            const unsigned b = __float_as_uint(p.w) & 0x7FFFFFFFu;  // +0 and -0 give 0
+            if (b) q = ((b & 0x7FFFFFu) | 0x800000u) << ((int)(b >> 23) - emin);
+        }
+        qw[d] = q;
+    }
 }
 
 // Exclusive scan of n ints, in -> out, using tmp for the per-chunk sums
@@ -208,14 +239,29 @@ __global__ void k_tile_emit(const int *__restrict__ start, const int *__restrict
 
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
                       int *rank, int *counts, int *cell_start, int *scan_tmp, float4 *pts_out,
-                      float *soa, size_t plane, int *flags, cudaStream_t st) {
+                      float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
+                      cudaStream_t st) {
     const int64_t ncell = (int64_t)P * P * P;
     const int thr = 256;
     const unsigned blocks = (unsigned)((n + thr - 1) / thr);
     k_cell_ids<<<blocks, thr, 0, st>>>(raw, n, P, cell, box, cid, rank, counts, flags);
     int launches = 1 + scan_exclusive(counts, cell_start, ncell + 1, scan_tmp, st);
-    k_scatter<<<blocks, thr, 0, st>>>(raw, n, cid, rank, cell_start, pts_out, soa, plane);
+    k_scatter<<<blocks, thr, 0, st>>>(raw, n, cid, rank, cell_start, pts_out, soa, plane,
+                                      reinterpret_cast<float *>(pk), qw, flags);
     return launches + 1;
+}
+
+void set_weight_range(pcf_grid *g, const unsigned hf[3]) {
+    g->unit_weights = (hf[0] & 2u) == 0;
+    g->w_finite_nonneg = (hf[0] & 4u) == 0;
+    std::memcpy(&g->w_absmax, &hf[1], sizeof(float));
+    const unsigned mn = ~hf[2];
+    if (hf[2]) std::memcpy(&g->w_absmin, &mn, sizeof(float));
+    else g->w_absmin = 0.f;
+    int emin = 0, emax = 0;
+    g->wfix_ok = weight_fix_range(hf[0], hf[1], hf[2], &emin, &emax);
+    g->wshift = 150 - emin;
+    g->wqmax = g->wfix_ok ? (unsigned long long)((hf[1] & 0x7FFFFFu) | 0x800000u) << (emax - emin) : 0ull;
 }
 
 int launch_tile_build(const int *cell_start, int P, int *tile_counts, int *tile_offsets,
@@ -247,10 +293,23 @@ pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes) {
 }
 
 // Build (or rebuild) the cell structure of g for P cells per side.
+// A grid keeps the cell structures of the last few partition counts it was
+// counted at, so classes of histograms tuned to different partitions do not
+// rebuild (and synchronise) on every switch.
 pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     if (g->cells && g->cells->P == P) return PCF_OK;
     if (P < 1 || P > 320) return PCF_ERR_INVALID_ARG;
+    for (size_t i = 0; i < g->cell_cache.size(); ++i) {
+        if (g->cell_cache[i]->P != P) continue;
+        std::unique_ptr<CellGrid> hit = std::move(g->cell_cache[i]);
+        g->cell_cache.erase(g->cell_cache.begin() + (long)i);
+        if (g->cells) g->cell_cache.push_back(std::move(g->cells));
+        g->cells = std::move(hit);
+        return PCF_OK;
+    }
+    static uint64_t next_serial = 0;
     std::unique_ptr<CellGrid> cg(new CellGrid);
+    cg->serial = ++next_serial;
     cg->pts.pool = cg->soa.pool = cg->cell_start.pool = g->pool;
     cg->P = P;
     cg->cell = g->box / (float)P;
@@ -261,6 +320,11 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     cg->plane = ((size_t)n + kSoaPad + 3) & ~(size_t)3;
     PCF_CU(ctx, cg->soa.ensure(sizeof(float) * cg->plane * 4));
     PCF_CU(ctx, cudaMemsetAsync(cg->soa.p, 0, sizeof(float) * cg->plane * 4, ctx->stream));
+    cg->pk.pool = cg->qw.pool = g->pool;
+    PCF_CU(ctx, cg->pk.ensure(32 * pk_blocks(n)));
+    PCF_CU(ctx, cudaMemsetAsync(cg->pk.p, 0, 32 * pk_blocks(n), ctx->stream));
+    PCF_CU(ctx, cg->qw.ensure(sizeof(unsigned) * cg->plane));
+    PCF_CU(ctx, cudaMemsetAsync(cg->qw.p, 0, sizeof(unsigned) * cg->plane, ctx->stream));
     PCF_CU(ctx, cg->cell_start.ensure(sizeof(int) * (size_t)(ncell + 1)));
     // scratch: cid, rank (n each); counts (ncell + 1); scan tmp.
     PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(int) * (size_t)n * 2));
@@ -275,7 +339,8 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     PCF_CU(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * 3, st));
     ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank, counts,
                                        cg->cell_start.as<int>(), ctx->scratch_c.as<int>(),
-                                       cg->pts.as<float4>(), cg->soa.as<float>(), cg->plane, flags, st);
+                                       cg->pts.as<float4>(), cg->soa.as<float>(), cg->plane,
+                                       cg->pk.as<float4>(), cg->qw.as<unsigned>(), flags, st);
     PCF_CU(ctx, cudaGetLastError());
     cg->h_start.resize((size_t)(ncell + 1));
     unsigned hf[3] = {0u, 0u, 0u};
@@ -288,18 +353,17 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
         ctx->last_error = "a coordinate lies outside [0, box)";
         return PCF_ERR_OUT_OF_BOX;
     }
-    g->unit_weights = (hflags & 2) == 0;
-    g->w_finite_nonneg = (hflags & 4) == 0;
-    std::memcpy(&g->w_absmax, &hf[1], sizeof(float));
-    const unsigned mn = ~hf[2];
-    if (hf[2]) std::memcpy(&g->w_absmin, &mn, sizeof(float));
-    else g->w_absmin = 0.f;
+    set_weight_range(g, hf);
     build_tiles(*cg);
     cg->d_tiles.pool = g->pool;
     PCF_CU(ctx, cg->d_tiles.ensure(sizeof(TileDesc) * std::max<size_t>(1, cg->tiles.size())));
     if (!cg->tiles.empty())
         PCF_CU(ctx, cudaMemcpyAsync(cg->d_tiles.p, cg->tiles.data(),
                                     sizeof(TileDesc) * cg->tiles.size(), cudaMemcpyHostToDevice, st));
+    if (g->cells) {
+        g->cell_cache.push_back(std::move(g->cells));
+        if ((int)g->cell_cache.size() > kCellCache) g->cell_cache.erase(g->cell_cache.begin());
+    }
     g->cells = std::move(cg);
     return PCF_OK;
 }

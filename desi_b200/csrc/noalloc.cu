@@ -52,8 +52,7 @@ struct Carve {
 
 struct CatBufs {
     int *cid, *rank, *counts, *start;
-    float *soa;
-    size_t plane;
+    float4 *pk;  // pair-packed points (PairView)
 };
 
 pcf_status fail(cudaError_t e) {
@@ -100,8 +99,7 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
         c.rank = cv.take<int>((size_t)n);
         c.counts = cv.take<int>((size_t)ncell + 1);
         c.start = cv.take<int>((size_t)ncell + 1);
-        c.plane = ((size_t)n + kSoaPad + 3) & ~(size_t)3;
-        c.soa = cv.take<float>(c.plane * 4);
+        c.pk = cv.take<float4>(2 * pk_blocks(n));
         return c;
     };
     CatBufs A = carve_cat(na);
@@ -124,9 +122,8 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
     if ((e = cudaMemsetAsync(A.counts, 0, sizeof(int) * (ncell + 1), st)) != cudaSuccess) return fail(e);
     if (cross && (e = cudaMemsetAsync(B.counts, 0, sizeof(int) * (ncell + 1), st)) != cudaSuccess)
         return fail(e);
-    if ((e = cudaMemsetAsync(A.soa, 0, sizeof(float) * A.plane * 4, st)) != cudaSuccess) return fail(e);
-    if (cross && (e = cudaMemsetAsync(B.soa, 0, sizeof(float) * B.plane * 4, st)) != cudaSuccess)
-        return fail(e);
+    if ((e = cudaMemsetAsync(A.pk, 0, 32 * pk_blocks(na), st)) != cudaSuccess) return fail(e);
+    if (cross && (e = cudaMemsetAsync(B.pk, 0, 32 * pk_blocks(nb), st)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(counter, 0, 64, st)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * nbins, st)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(d_ws, 0, sizeof(double) * nbins, st)) != cudaSuccess) return fail(e);
@@ -135,10 +132,10 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
 
     const float cell = box / (float)P;
     launch_grid_build(reinterpret_cast<const float4 *>(a), na, P, cell, box, A.cid, A.rank, A.counts,
-                      A.start, scan_tmp, nullptr, A.soa, A.plane, d_flags, st);
+                      A.start, scan_tmp, nullptr, nullptr, 0, A.pk, nullptr, d_flags, st);
     if (cross)
         launch_grid_build(reinterpret_cast<const float4 *>(b), nb, P, cell, box, B.cid, B.rank,
-                          B.counts, B.start, scan_tmp, nullptr, B.soa, B.plane, d_flags, st);
+                          B.counts, B.start, scan_tmp, nullptr, nullptr, 0, B.pk, nullptr, d_flags, st);
     launch_tile_build(A.start, P, tile_counts, tile_offsets, scan_tmp, tiles, st);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
     if ((e = cudaMemcpyAsync(d_rows, rows.data(), sizeof(RowDesc) * rows.size(),
@@ -160,8 +157,8 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
     pl.weighted = (h_flags & 2) != 0;
     pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, cross);
     pl.mult = cross ? 1.0 : 2.0;
-    const GridView hv{A.soa, A.soa + A.plane, A.soa + 2 * A.plane, A.soa + 3 * A.plane, A.start};
-    const GridView cvw{B.soa, B.soa + B.plane, B.soa + 2 * B.plane, B.soa + 3 * B.plane, B.start};
+    const PairView hv{A.pk, nullptr, A.start};
+    const PairView cvw{B.pk, nullptr, B.start};
     e = launch_pairs_view(hv, cvw, tiles, h_tiles, d_rows, (int)rows.size(), P, box, pl, counter,
                           d_cnt, d_ws, d_stats, d_job, st, sms, dev);
     if (e != cudaSuccess) return fail(e);

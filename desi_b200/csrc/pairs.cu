@@ -8,21 +8,27 @@
 // image passes for periodic boxes; here:
 //
 //  * Work = (home tile, stencil rows) items in a persistent queue.  A home
-//    tile is <= 128 cell-ordered points of one (ix,iy) column; a stencil row
+//    tile is <= 32 cell-ordered points of one (ix,iy) column, one point per
+//    lane (a tile of H points runs 32/H candidate streams); a stencil row
 //    (dx,dy) names the neighbour column, whose cells z0-kz..z1+kz are one
 //    contiguous point range (or two when the periodic box wraps in z).  XX
 //    uses the half shell (each unordered pair once, histogram doubled at the
 //    end, matching the reference's ordered-pair convention).
 //  * Periodic boxes: the neighbour column index wraps and the home point is
 //    shifted by the image offset once per range, so no image passes.
-//  * Separations in FP32 (3 FADD + FMUL + 2 FFMA); the bin comes from
-//    r = d2*rsqrt(d2)*ds read out in 15-bit fixed point; any pair whose r is
-//    within a proven error window of a bin edge, or whose d2 is near dmax^2
-//    or 0, is re-evaluated with the canonical FP64 rule (pcf_internal.cuh),
-//    so bin membership equals the FP64 oracle's exactly.
-//  * Histograms: per-warp copies in shared memory (u32 counts for unit
-//    weights, FP64 sums otherwise), merged once per CTA into global u64 /
-//    FP64 and finalised to double (x2 for XX).
+//  * Candidates arrive two at a time as two 16-byte loads of the pair-packed
+//    layout (PairView); separations in packed FP32 (3 FADD2, FMUL2, 2 FFMA2
+//    per two pairs); the bin comes from r = sqrt.approx(d2*ds^2) read out in
+//    15-bit fixed point through r + 256.  A pair whose r is within a proven
+//    error window of a bin edge, or whose d2 is near dmax^2 or 0, is
+//    re-evaluated with the canonical FP64 rule (pcf_internal.cuh), so bin
+//    membership equals the FP64 oracle's exactly.
+//  * Histograms: u32 shared-memory copies per lane (iso) or per warp (ani),
+//    merged into global u64 counts / FP64 sums and finalised to double (x2
+//    for XX).  Weighted sums use exact integer weights: the 64-bit product
+//    q_a*q_b goes into three u32 limb counters (16 + 16 + 32 bits), flushed
+//    before any could wrap; FP64 shared atomics remain for weights without
+//    an exact integer image.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -39,16 +45,19 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr float kMagic = 256.0f;  // r + 256 -> low mantissa bits = round(r * 2^15)
 constexpr int kFracBits = 15;
 constexpr unsigned kFracMask = (1u << kFracBits) - 1u;
+// bits(256 + r) >> 15 = kBinBias + floor(r) for r in [0, 256) away from an edge
+constexpr unsigned kBinBias = 0x43800000u >> kFracBits;
 
-enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3 };
-
-// H_WFIX (weighted, per-warp copy): each product w_a*w_b is rounded to an
-// integer v = round(w_a*w_b * 2^s) < 2^64 and added as four 16-bit limbs, each
-// with a 32-bit shared reduction (several times faster than a 64-bit one).
-// A limb counter absorbs kWfixBudget adds of < 2^16 before it could wrap, so a
-// warp flushes its copy after at most that many pair tests.
-constexpr int kWfixBudget = 65536;
-constexpr int kWfixChunk = kWfixBudget / 32;  // candidates per budget check (<= 32 homes each)
+// Histogram privatisation.  H_LANE: a u32 (or FP64) column per lane (iso);
+// H_WARP: one copy per warp with shared atomics; H_GLOBAL: global atomics
+// (very wide histograms); H_WFIX: per-warp fixed-point limbs (weighted);
+// H_LFIX: per-lane fixed-point limbs (weighted iso).
+enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3, H_LFIX = 4 };
+constexpr int kLimbs = 3;
+#ifndef PCF_PAIR_GROUP
+#define PCF_PAIR_GROUP 4
+#endif
+constexpr int kGroup = PCF_PAIR_GROUP;  // candidate steps between recheck votes
 
 // Fast-path cut constants for one range type (0: unshifted, 1: image-shifted).
 struct FastCuts {
@@ -73,9 +82,10 @@ struct PairArgs {
     unsigned long long *g_count;
     double *g_wsum;
     unsigned long long *g_stats;
-    float wscale;     // H_WFIX: 2^s, applied to the home weight
-    double wunscale;  // H_WFIX: 2^-s
-    int wlimbs;       // H_WFIX: limbs per bin (3: v < 2^48, 4: v < 2^64)
+    int chunk;   // candidates per budget check (even)
+    int budget;  // adds one shared counter absorbs between flushes
+    int fast;    // 0: every pair in range takes the FP64 rule (bins > 255: r + 256
+                 // no longer has a fixed exponent)
 };
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -84,69 +94,83 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return r;
 }
 
-// Fixed-point readout of r in [0, 256): q = round(r * 2^15).  The bin
-// (q >> 15) is exact unless r is within w/2^15 of an integer.
-__device__ __forceinline__ bool fix_safe(unsigned q, unsigned w) {
-    return ((q + w) & kFracMask) >= 2u * w;
+// Fixed-point readout of r in [0, 256): u = bits(r + 256 + w/2^15), so the
+// low 15 bits are frac(r) + w in 2^-15 units.  The bin (u >> 15, biased) is
+// floor(r) unless r is within w/2^15 of an integer, which this rejects.
+__device__ __forceinline__ bool fix_safe(unsigned u, unsigned w2) {
+    return (u & kFracMask) >= w2;
 }
 
-// Predicated shared / global reductions (one instruction, no branch).
-__device__ __forceinline__ void red_s_u32(const void *p, unsigned v, bool pred) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q red.shared.add.u32 [%0], %1;\n\t}"
-                 :: "r"(a), "r"(v), "r"((unsigned)pred) : "memory");
+// Shared reductions on 32-bit shared-window addresses.  They are not
+// predicated: a lane without a pair adds 0 to a private dummy slot, which
+// keeps the candidate loop free of branches around memory operations.
+__device__ __forceinline__ void red_s_u32(unsigned a, unsigned v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(a), "r"(v));
 }
-__device__ __forceinline__ void red_s_f64(const void *p, double v, bool pred) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q red.shared.add.f64 [%0], %1;\n\t}"
-                 :: "r"(a), "d"(v), "r"((unsigned)pred) : "memory");
+__device__ __forceinline__ void red_s_f64(unsigned a, double v) {
+    asm volatile("red.shared.add.f64 [%0], %1;" :: "r"(a), "d"(v));
+}
+// The three limbs of one product into [a], [a + S], [a + 2S].
+template <int S>
+__device__ __forceinline__ void red_s_limbs(unsigned a, unsigned long long v) {
+    const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+    asm volatile("red.shared.add.u32 [%0], %1;\n\t"
+                 "red.shared.add.u32 [%0+%4], %2;\n\t"
+                 "red.shared.add.u32 [%0+%5], %3;"
+                 :: "r"(a), "r"(lo & 0xFFFFu), "r"(lo >> 16), "r"(hi), "n"(S), "n"(2 * S));
 }
 
-// Histogram sinks.  H_LANE: one u32 / f64 column per lane (iso, few bins),
-// no contention; H_WARP: one copy per warp with shared atomics; H_GLOBAL:
-// global atomics (very wide histograms).  add() is predicated on `pred`.
+// Weight carried per point: the exact integer q (fixed-point modes), the
+// float w (FP64 modes) or nothing (unit weights).
+template <bool WEIGHTED, int HM>
+struct WT {
+    typedef typename std::conditional<(HM == H_WFIX || HM == H_LFIX), unsigned, float>::type type;
+};
+
+// Histogram sink of one lane.  Slots arrive biased (see kBinBias); `base`
+// already subtracts bias * stride, so the address is base + sb * stride.
+// `dummy` is this lane's private slot for the adds of 0.
 template <bool WEIGHTED, int HM>
 struct Sink {
-    void *base;  // shared: this warp's region (lane column folded in); global: g_count / g_wsum
-    int plane;   // H_WFIX: u32 words between limb planes (bins of the histogram)
-    bool four;   // H_WFIX: the top limb is in use
-    __device__ __forceinline__ void add(int slot, float wa, float wb, bool pred) const {
-        if (HM == H_WFIX) {  // wa carries the 2^s scale; w_a*w_b is exact in FP64
-            const unsigned long long v = __double2ull_rn((double)wa * (double)wb);
-            unsigned *b = static_cast<unsigned *>(base) + slot;
-            const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-            red_s_u32(b, lo & 0xFFFFu, pred);
-            red_s_u32(b + plane, lo >> 16, pred);
-            red_s_u32(b + 2 * plane, hi & 0xFFFFu, pred);
-            red_s_u32(b + 3 * plane, hi >> 16, pred && four);
+    typedef typename WT<WEIGHTED, HM>::type W;
+    unsigned base;      // shared-window address (biased)
+    unsigned dummy;     // shared-window address of this lane's dummy slot
+    unsigned bias;
+    double *lane_col;   // H_LANE FP64: this lane's column (generic)
+    void *gbase;        // H_GLOBAL: this job's accumulator
+    __device__ __forceinline__ void add(unsigned sb, W wa, W wb, bool pred) const {
+        if (HM == H_LFIX) {
+            red_s_limbs<128>(pred ? base + sb * (kLimbs * 128u) : dummy,
+                             (unsigned long long)(pred ? wa : 0u) * wb);
+        } else if (HM == H_WFIX) {
+            red_s_limbs<4>(pred ? base + sb * (kLimbs * 4u) : dummy,
+                           (unsigned long long)(pred ? wa : 0u) * wb);
         } else if (HM == H_LANE) {
-            if (WEIGHTED) {  // lane-private column: unconditional add of 0 or w_a*w_b,
-                // so a lane without a pair (its slot undefined) adds 0 to slot 0
-                double *h = static_cast<double *>(base) + (pred ? slot : 0) * 32;
+            if (WEIGHTED) {  // lane-private FP64 column: add 0 to slot 0 when !pred
+                double *h = lane_col + (pred ? (int)(sb - bias) : 0) * 32;
                 *h += pred ? (double)wa * (double)wb : 0.0;
             } else {
-                red_s_u32(static_cast<unsigned *>(base) + slot * 32, 1u, pred);
+                red_s_u32(pred ? base + sb * 128u : dummy, (unsigned)pred);
             }
         } else if (HM == H_WARP) {
-            if (WEIGHTED) red_s_f64(static_cast<double *>(base) + slot, (double)wa * (double)wb, pred);
-            else red_s_u32(static_cast<unsigned *>(base) + slot, 1u, pred);
+            if (WEIGHTED) red_s_f64(pred ? base + sb * 8u : dummy, pred ? (double)wa * (double)wb : 0.0);
+            else red_s_u32(pred ? base + sb * 4u : dummy, (unsigned)pred);
         } else if (pred) {
-            if (WEIGHTED) atomicAdd(static_cast<double *>(base) + slot, (double)wa * (double)wb);
-            else atomicAdd(static_cast<unsigned long long *>(base) + slot, 1ull);
+            if (WEIGHTED) atomicAdd(static_cast<double *>(gbase) + (sb - bias), (double)wa * (double)wb);
+            else atomicAdd(static_cast<unsigned long long *>(gbase) + (sb - bias), 1ull);
         }
     }
 };
 
-struct Home {
-    float x, y, z, w;  // original coordinates
-};
-
-struct Seg {
-    float sx, sy, sz;  // image shift of the candidates
-    float lo, hi;
-    unsigned w;
-    unsigned rule_flags;
-};
+// Point j of a pair-packed view.
+__device__ __forceinline__ void load_point(const float4 *pk, int j, float &x, float &y, float &z, float &w) {
+    const float4 a = __ldg(pk + (j & ~1)), b = __ldg(pk + (j & ~1) + 1);
+    const bool o = j & 1;
+    x = o ? a.y : a.x;
+    y = o ? a.w : a.z;
+    z = o ? b.y : b.x;
+    w = o ? b.w : b.z;
+}
 
 // Canonical FP64 decision for one pair (rare path): histogram slot or -1.
 template <bool ANI>
@@ -157,183 +181,150 @@ __device__ __noinline__ int slow_slot(float hx, float hy, float hz, float cx, fl
     return exact_slot<ANI>(dx, dy, dz, rule);
 }
 
-template <bool ANI, bool WEIGHTED, int HM>
-__device__ __forceinline__ void slow_pair(const PairArgs &A, const GridView &C, const Home &h,
-                                          const Seg &sg, int j, const Sink<WEIGHTED, HM> &sink,
-                                          unsigned &n_pairs) {
-    PairRule rule = A.rule;
-    rule.flags = sg.rule_flags;
-    const int slot = slow_slot<ANI>(h.x, h.y, h.z, __ldg(C.x + j), __ldg(C.y + j), __ldg(C.z + j),
-                                    sg.sx, sg.sy, sg.sz, rule);
-    if (slot >= 0) {
-        sink.add(slot, h.w, WEIGHTED ? __ldg(C.w + j) : 1.f, true);
-        if (WEIGHTED) ++n_pairs;
-    }
+// Shared-memory words (of the copy's element type) of one warp's copy.
+// Per-warp copies end with 32 dummy slots, one per lane (never flushed).
+template <int HM>
+__host__ __device__ __forceinline__ int copy_words(int nb) {
+    return HM == H_LANE ? nb * 32 : HM == H_WARP ? nb + 32 : HM == H_WFIX ? (nb + 32) * kLimbs
+         : HM == H_LFIX ? nb * kLimbs * 32 : 0;
 }
 
-// Adds this warp's histogram copy into histogram `slot` of the launch and
-// clears it (job change or end of the queue).
+// Adds this warp's copy into histogram `slot` of the launch and clears it.
 template <bool WEIGHTED, int HM>
-__device__ __forceinline__ void flush_hist(typename std::conditional<WEIGHTED, double, unsigned>::type *mine,
-                                           int nb, int per_warp, int lane, const PairArgs &A,
-                                           int slot) {
-    typedef typename std::conditional<WEIGHTED, double, unsigned>::type HT;
+__device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, int slot, double unscale) {
     if (HM == H_GLOBAL) return;
     __syncwarp();
     const size_t off = (size_t)slot * nb;
-    if (HM == H_LANE) {
+    if (HM == H_LANE && !WEIGHTED) {
+        unsigned *mine = static_cast<unsigned *>(mine_v);
         for (int k = 0; k < nb; ++k) {
-            HT s = mine[k * 32 + lane];
-            mine[k * 32 + lane] = (HT)0;
+            unsigned long long s = mine[k * 32 + lane];
+            mine[k * 32 + lane] = 0u;
             for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
-            if (lane == 0 && s != (HT)0) {
-                if (WEIGHTED) atomicAdd(A.g_wsum + off + k, (double)s);
-                else atomicAdd(A.g_count + off + k, (unsigned long long)s);
-            }
+            if (lane == 0 && s) atomicAdd(A.g_count + off + k, s);
         }
-    } else {
+    } else if (HM == H_LANE) {
+        double *mine = static_cast<double *>(mine_v);
+        for (int k = 0; k < nb; ++k) {
+            double s = mine[k * 32 + lane];
+            mine[k * 32 + lane] = 0.0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
+            if (lane == 0 && s != 0.0) atomicAdd(A.g_wsum + off + k, s);
+        }
+    } else if (HM == H_WARP) {
         for (int k = lane; k < nb; k += 32) {
-            const HT s = mine[k];
-            mine[k] = (HT)0;
-            if (s != (HT)0) {
-                if (WEIGHTED) atomicAdd(A.g_wsum + off + k, (double)s);
-                else atomicAdd(A.g_count + off + k, (unsigned long long)s);
+            if (WEIGHTED) {
+                double *mine = static_cast<double *>(mine_v);
+                const double s = mine[k];
+                mine[k] = 0.0;
+                if (s != 0.0) atomicAdd(A.g_wsum + off + k, s);
+            } else {
+                unsigned *mine = static_cast<unsigned *>(mine_v);
+                const unsigned s = mine[k];
+                mine[k] = 0u;
+                if (s) atomicAdd(A.g_count + off + k, (unsigned long long)s);
             }
         }
-    }
-    __syncwarp();
-    (void)per_warp;
-}
-
-__device__ __forceinline__ void flush_wfix(unsigned *mine, int nb, int limbs, int lane,
-                                           const PairArgs &A, int slot);
-template <bool WEIGHTED, int HM, typename HT>
-__device__ __forceinline__ void flush_any(HT *mine, int nb, int per_warp, int lane, const PairArgs &A,
-                                          int slot) {
-    if (HM == H_WFIX) flush_wfix(reinterpret_cast<unsigned *>(mine), nb, A.wlimbs, lane, A, slot);
-    else flush_hist<WEIGHTED, HM>(reinterpret_cast<typename std::conditional<WEIGHTED, double, unsigned>::type *>(mine),
-                                  nb, per_warp, lane, A, slot);
-}
-
-// H_WFIX flush: limbs -> FP64 sum * 2^-s into histogram `slot`; clears the copy.
-__device__ __forceinline__ void flush_wfix(unsigned *mine, int nb, int limbs, int lane,
-                                           const PairArgs &A, int slot) {
-    __syncwarp();
-    const size_t off = (size_t)slot * nb;
-    for (int k = lane; k < nb; k += 32) {
-        const unsigned l0 = mine[k], l1 = mine[nb + k], l2 = mine[2 * nb + k];
-        const unsigned l3 = limbs == 4 ? mine[3 * nb + k] : 0u;
-        mine[k] = 0u;
-        mine[nb + k] = 0u;
-        mine[2 * nb + k] = 0u;
-        if (limbs == 4) mine[3 * nb + k] = 0u;
-        if (l0 | l1 | l2 | l3) {
-            // each term is exact; the sum of the four rounds once or twice
-            const double v = ((double)l3 * 0x1p48 + (double)l2 * 0x1p32) + ((double)l1 * 0x1p16 + (double)l0);
-            atomicAdd(A.g_wsum + off + k, v * A.wunscale);
+    } else if (HM == H_WFIX) {  // [bin][limb]
+        unsigned *mine = static_cast<unsigned *>(mine_v);
+        for (int k = lane; k < nb; k += 32) {
+            unsigned *c = mine + k * kLimbs;
+            const unsigned l0 = c[0], l1 = c[1], l2 = c[2];
+            c[0] = c[1] = c[2] = 0u;
+            if (l0 | l1 | l2) {  // each term exact; the sum rounds at most twice
+                const double v = (double)l2 * 0x1p32 + ((double)l1 * 0x1p16 + (double)l0);
+                atomicAdd(A.g_wsum + off + k, v * unscale);
+            }
+        }
+    } else if (HM == H_LFIX) {  // [bin][limb][lane]
+        unsigned *mine = static_cast<unsigned *>(mine_v);
+        for (int k = 0; k < nb; ++k) {
+            unsigned *c = mine + k * kLimbs * 32 + lane;
+            const unsigned l0 = c[0], l1 = c[32], l2 = c[64];
+            c[0] = c[32] = c[64] = 0u;
+            double v = (double)l2 * 0x1p32 + ((double)l1 * 0x1p16 + (double)l0);
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+            if (lane == 0 && v != 0.0) atomicAdd(A.g_wsum + off + k, v * unscale);
         }
     }
     __syncwarp();
-}
-
-// One candidate pair of elements (packed): distance test, fixed-point bin,
-// predicated accumulate.  Pairs within the edge window of a bin, near dmax,
-// or at zero separation (frac(r) = 0 fails the window test) go to the FP64
-// rule, behind one warp-uniform branch.
-template <bool ANI, bool WEIGHTED, int HM>
-__device__ __forceinline__ void take2(const PairArgs &A, const GridView &C, float2 DX, float2 DY,
-                                      float2 DZ, bool v0,
-                                      bool v1, int j, float2 Wt, const Home &h, const Seg &sg,
-                                      const Sink<WEIGHTED, HM> &sink, unsigned &n_pairs,
-                                      unsigned &n_rechk) {
-    const FastCuts &fc = A.fc;
-    const float2 DS2 = make_float2(fc.ds2, fc.ds2);
-    const float2 MG = make_float2(kMagic, kMagic);
-    bool f0 = false, f1 = false;
-    float m0, m1;  // largest squared component, for the recheck test
-    if (!ANI) {
-        float2 D2 = __fmul2_rn(DX, DX);
-        D2 = __ffma2_rn(DY, DY, D2);
-        D2 = __ffma2_rn(DZ, DZ, D2);
-        m0 = D2.x;
-        m1 = D2.y;
-        if (HM != H_GLOBAL) {
-            const float2 U = __fmul2_rn(D2, DS2);
-            const float2 Q = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)), MG);
-            const unsigned q0 = __float_as_uint(Q.x) & 0x7FFFFFu;
-            const unsigned q1 = __float_as_uint(Q.y) & 0x7FFFFFu;
-            f0 = v0 && (D2.x < sg.lo) && fix_safe(q0, sg.w);
-            f1 = v1 && (D2.y < sg.lo) && fix_safe(q1, sg.w);
-            // f0 / f1 imply r < bins away from an edge, so q >> 15 <= bins - 1
-            sink.add((int)(q0 >> kFracBits), h.w, Wt.x, f0);
-            sink.add((int)(q1 >> kFracBits), h.w, Wt.y, f1);
-        }
-    } else {
-        const float2 ZZ = __fmul2_rn(DZ, DZ);
-        const float2 PP = __ffma2_rn(DY, DY, __fmul2_rn(DX, DX));
-        m0 = fmaxf(ZZ.x, PP.x);
-        m1 = fmaxf(ZZ.y, PP.y);
-        if (HM != H_GLOBAL) {
-            const float2 RZ = __fmul2_rn(DZ, make_float2(fc.dsf, fc.dsf));
-            const float2 U = __fmul2_rn(PP, DS2);
-            const float2 QZ = __fadd2_rn(make_float2(fabsf(RZ.x), fabsf(RZ.y)), MG);
-            const float2 QP = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)), MG);
-            const unsigned z0 = __float_as_uint(QZ.x) & 0x7FFFFFu, z1 = __float_as_uint(QZ.y) & 0x7FFFFFu;
-            const unsigned p0 = __float_as_uint(QP.x) & 0x7FFFFFu, p1 = __float_as_uint(QP.y) & 0x7FFFFFu;
-            f0 = v0 && (m0 < sg.lo) && fix_safe(z0, sg.w) && fix_safe(p0, sg.w);
-            f1 = v1 && (m1 < sg.lo) && fix_safe(z1, sg.w) && fix_safe(p1, sg.w);
-            const int B = A.rule.bins;
-            sink.add((int)(z0 >> kFracBits) * B + (int)(p0 >> kFracBits), h.w, Wt.x, f0);
-            sink.add((int)(z1 >> kFracBits) * B + (int)(p1 >> kFracBits), h.w, Wt.y, f1);
-        }
-    }
-    if (WEIGHTED) n_pairs += (unsigned)f0 + (unsigned)f1;
-    const bool r0 = !f0 && v0 && m0 < sg.hi;
-    const bool r1 = !f1 && v1 && m1 < sg.hi;
-    // Lanes of different candidate streams leave the stream loop after
-    // different trip counts, so vote only among the lanes that are here.
-    if (__any_sync(__activemask(), r0 || r1)) {
-        if (r0) {
-            ++n_rechk;
-            slow_pair<ANI, WEIGHTED, HM>(A, C, h, sg, j, sink, n_pairs);
-        }
-        if (r1) {
-            ++n_rechk;
-            slow_pair<ANI, WEIGHTED, HM>(A, C, h, sg, j + 1, sink, n_pairs);
-        }
-    }
 }
 
 #ifndef PCF_PAIR_MINB
 #define PCF_PAIR_MINB 6
 #endif
-template <bool ANI, bool WEIGHTED, int HM>
-// H_WFIX copies take 3-4x the shared memory of a u32 copy, which already
-// holds those launches to ~5 CTAs per SM: let them use the registers of 5.
-__global__ void __launch_bounds__(kThreads, HM == H_WFIX ? 5 : PCF_PAIR_MINB) k_pairs(const PairArgs A) {
-    typedef typename std::conditional<WEIGHTED && HM != H_WFIX, double, unsigned>::type HT;
+template <int HM>
+struct MinBlocks {  // CTAs per SM the shared-memory footprint allows at 30 / 900 bins
+    static constexpr int value = HM == H_LFIX ? 4 : HM == H_WFIX ? 5 : PCF_PAIR_MINB;
+};
+
+// Candidate ranges of one stencil row for the current home tile: [a0, b0)
+// unshifted in z, [a1, b1) image-shifted by sz1 (periodic wrap in z); the
+// column's image shift is (sx, sy).  kind 1: forward half of the home column.
+struct RowRange {
+    int a0, b0, a1, b1;
+    float sx, sy, sz1;
+    int kind;
+};
+
+// Per-warp state kept in shared memory, so the candidate loop has the
+// registers to itself.
+struct WarpState {
+    PairJob job;
+    RowRange rows[32];
+    float4 home[32];                // this item's home point per lane (x, y, z, w)
+    unsigned long long n_cand;      // pair tests (statistics)
+    long long job_end;
+    int cj, slot;
+};
+
+// COUNT: also count the in-range pairs (weighted histograms, statistics on).
+template <bool ANI, bool WEIGHTED, int HM, bool COUNT>
+__global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const PairArgs A) {
+    constexpr bool FIX = HM == H_WFIX || HM == H_LFIX;
+    typedef typename WT<WEIGHTED, HM>::type W;
+    typedef typename std::conditional<WEIGHTED && !FIX, double, unsigned>::type HT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    HT *hist_all = reinterpret_cast<HT *>(smem_raw);
+    __shared__ WarpState s_ws[kWarps];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    WarpState &ws = s_ws[warp];
+    PairJob &J = ws.job;
     const int bins = A.rule.bins;
     const int nb = ANI ? bins * bins : bins;
-    const int per_warp = HM == H_LANE ? nb * 32 : (HM == H_WARP ? nb : (HM == H_WFIX ? nb * A.wlimbs : 0));
-    HT *mine = hist_all + warp * per_warp;
+    const int per_warp = copy_words<HM>(nb);
+    HT *mine = reinterpret_cast<HT *>(smem_raw) + warp * per_warp;
     for (int k = lane; k < per_warp; k += 32) mine[k] = (HT)0;
-    __syncwarp();
+    const unsigned bias = ANI ? kBinBias * (unsigned)(bins + 1) : kBinBias;
     Sink<WEIGHTED, HM> sink;
-    if (HM != H_GLOBAL) sink.base = HM == H_LANE ? (void *)(mine + lane) : (void *)mine;
-    sink.plane = nb;
-    sink.four = A.wlimbs == 4;
-    int wfix_since = 0;  // H_WFIX: pair tests since this warp's last flush
+    {
+        const unsigned ms = (unsigned)__cvta_generic_to_shared(mine);
+        sink.bias = bias;
+        sink.lane_col = reinterpret_cast<double *>(mine) + lane;
+        sink.gbase = nullptr;
+        switch (HM) {  // dummy: bin 0 of a lane-private column, else slot nb + lane
+        case H_LANE: sink.base = ms + lane * 4u - bias * 128u; sink.dummy = ms + lane * 4u; break;
+        case H_WARP:
+            sink.base = ms - bias * (unsigned)sizeof(HT);
+            sink.dummy = ms + (unsigned)(nb + lane) * (unsigned)sizeof(HT);
+            break;
+        case H_WFIX:
+            sink.base = ms - bias * (kLimbs * 4u);
+            sink.dummy = ms + (unsigned)(nb + lane) * (kLimbs * 4u);
+            break;
+        case H_LFIX: sink.base = ms + lane * 4u - bias * (kLimbs * 128u); sink.dummy = ms + lane * 4u; break;
+        default: sink.base = sink.dummy = 0u;
+        }
+    }
+    if (lane == 0) {
+        ws.n_cand = 0;
+        ws.job_end = -1;
+        ws.cj = -1;
+        ws.slot = 0;
+    }
+    __syncwarp();
+    int since = 0;  // adds per shared counter since this copy's last flush (bound)
     unsigned n_pairs = 0, n_rechk = 0;
-    unsigned long long n_cand = 0;
-    // current job (items of one warp arrive in increasing order), kept in
-    // shared memory to spare registers
-    __shared__ PairJob s_job[kWarps];
-    PairJob &J = s_job[warp];
-    int cj = -1, slot = 0;
-    long long job_end = -1;
+    const FastCuts &fc = A.fc;
 
     long long next = 0;
     if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);
@@ -341,155 +332,264 @@ __global__ void __launch_bounds__(kThreads, HM == H_WFIX ? 5 : PCF_PAIR_MINB) k_
     while (next < A.n_items) {
         const long long it_idx = next;
         if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next item
-        if (it_idx >= job_end) {  // entering another job: flush this one's histogram
-            if (cj >= 0) flush_any<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
-            wfix_since = 0;
+        if (it_idx >= ws.job_end) {  // entering another job: flush this one's histogram
+            if (ws.cj >= 0) flush_copy<WEIGHTED, HM>(mine, nb, lane, A, ws.slot, J.wunscale);
+            since = 0;
+            int cj = ws.cj;
+            long long job_end;
             do {
                 ++cj;
                 job_end = cj + 1 < A.n_jobs ? A.jobs[cj + 1].item_begin : A.n_items;
             } while (it_idx >= job_end);
-            {
-                static_assert(sizeof(PairJob) % 4 == 0, "PairJob words");
-                const int *src = reinterpret_cast<const int *>(A.jobs + cj);
-                int *dst = reinterpret_cast<int *>(&J);
-                for (int q = lane; q < (int)(sizeof(PairJob) / 4); q += 32) dst[q] = src[q];
-                __syncwarp();
+            __syncwarp();
+            static_assert(sizeof(PairJob) % 4 == 0, "PairJob words");
+            const int *src = reinterpret_cast<const int *>(A.jobs + cj);
+            int *dst = reinterpret_cast<int *>(&J);
+            for (int q = lane; q < (int)(sizeof(PairJob) / 4); q += 32) dst[q] = src[q];
+            if (lane == 0) {
+                ws.cj = cj;
+                ws.job_end = job_end;
             }
-            slot = J.slot;
-            if (HM == H_GLOBAL)
-                sink.base = WEIGHTED ? (void *)(A.g_wsum + (size_t)slot * nb)
-                                     : (void *)(A.g_count + (size_t)slot * nb);
+            __syncwarp();
+            if (lane == 0) ws.slot = J.slot;
+            if (HM == H_GLOBAL) {
+                sink.gbase = WEIGHTED ? (void *)(A.g_wsum + (size_t)J.slot * nb)
+                                      : (void *)(A.g_count + (size_t)J.slot * nb);
+            }
+            __syncwarp();
         }
         const long long loc = it_idx - J.item_begin;
         const int tile = (int)(loc / J.n_chunks);
         const int chunk = (int)(loc - (long long)tile * J.n_chunks);
         const int row_begin = chunk * J.rows_per_item;
-        const int row_end = min(row_begin + J.rows_per_item, J.n_rows);
+        const int nrows = min(row_begin + J.rows_per_item, J.n_rows) - row_begin;  // <= 32
         const TileDesc t = J.tiles[tile];
         const int H = t.count;                 // 1..32 home points
         const int S = 32 / H;                  // candidate streams per warp
         const int sidx = lane / H;             // this lane's stream
-        const int hl = lane - sidx * H;        // this lane's home point
-        const bool valid = sidx < S;
-        const int hidx = t.start + hl;
-        Home h;
-        if (valid) {
-            h.x = J.home.x[hidx]; h.y = J.home.y[hidx]; h.z = J.home.z[hidx]; h.w = J.home.w[hidx];
-            if (HM == H_WFIX) h.w *= A.wscale;  // exact: a power of two, range checked by the host
-        } else {
-            h.x = h.y = h.z = __int_as_float(0x7fc00000);  // NaN: never in range
-            h.w = 0.f;
+        const int hidx = t.start + (lane - sidx * H);
+        W hw = (W)0;
+        {
+            float4 h;
+            if (sidx < S) {
+                load_point(J.home.pk, hidx, h.x, h.y, h.z, h.w);
+                if (FIX) hw = (W)__ldg(J.home.qw + hidx);
+                else hw = (W)h.w;
+            } else {
+                h.x = h.y = h.z = __int_as_float(0x7fc00000);  // NaN: never in range
+                h.w = 0.f;
+            }
+            ws.home[lane] = h;
         }
         // Candidate ranges of all rows of the item, one row per lane, so the
         // dependent cell-table loads of different rows overlap.
-        const int nrows = row_end - row_begin;  // <= 32 (planner)
-        int ra0 = 0, rb0 = 0, ra1 = 0, rb1 = 0, rkind = 0;
-        float rsx = 0.f, rsy = 0.f, rsz1 = 0.f;
         if (lane < nrows) {
+            RowRange rr{0, 0, 0, 0, 0.f, 0.f, 0.f, 0};
             const RowDesc rw = J.rows[row_begin + lane];
             int nx = t.ix + rw.dx, ny = t.iy + rw.dy;
             const int P = A.P;
             bool ok = true;
             if (A.bpc) {
-                if (nx < 0) { nx += P; rsx = -A.box; } else if (nx >= P) { nx -= P; rsx = A.box; }
-                if (ny < 0) { ny += P; rsy = -A.box; } else if (ny >= P) { ny -= P; rsy = A.box; }
+                if (nx < 0) { nx += P; rr.sx = -A.box; } else if (nx >= P) { nx -= P; rr.sx = A.box; }
+                if (ny < 0) { ny += P; rr.sy = -A.box; } else if (ny >= P) { ny -= P; rr.sy = A.box; }
             } else if (nx < 0 || nx >= P || ny < 0 || ny >= P) {
                 ok = false;
             }
             if (ok) {
                 const int col = (nx * P + ny) * P;
                 const int zhi = t.z1 + rw.kz;
-                rkind = rw.kind;
+                rr.kind = rw.kind;
                 const int *cs = J.cand.cstart;
                 if (rw.kind == 1) {  // forward half of the home column (XX): j > home index
-                    ra0 = t.start;
-                    rb0 = cs[col + min(zhi, P - 1) + 1];
-                    if (A.bpc && zhi >= P) { ra1 = cs[col]; rb1 = cs[col + zhi - P + 1]; rsz1 = A.box; }
+                    rr.a0 = t.start;
+                    rr.b0 = cs[col + min(zhi, P - 1) + 1];
+                    if (A.bpc && zhi >= P) { rr.a1 = cs[col]; rr.b1 = cs[col + zhi - P + 1]; rr.sz1 = A.box; }
                 } else {
                     const int zlo = t.z0 - rw.kz;
-                    ra0 = cs[col + max(zlo, 0)];
-                    rb0 = cs[col + min(zhi, P - 1) + 1];
+                    rr.a0 = cs[col + max(zlo, 0)];
+                    rr.b0 = cs[col + min(zhi, P - 1) + 1];
                     if (A.bpc) {
-                        if (zlo < 0) { ra1 = cs[col + zlo + P]; rb1 = cs[col + P]; rsz1 = -A.box; }
-                        else if (zhi >= P) { ra1 = cs[col]; rb1 = cs[col + zhi - P + 1]; rsz1 = A.box; }
+                        if (zlo < 0) { rr.a1 = cs[col + zlo + P]; rr.b1 = cs[col + P]; rr.sz1 = -A.box; }
+                        else if (zhi >= P) { rr.a1 = cs[col]; rr.b1 = cs[col + zhi - P + 1]; rr.sz1 = A.box; }
                     }
                 }
             }
+            ws.rows[lane] = rr;
         }
+        __syncwarp();
+        const float4 *__restrict__ cpk = J.cand.pk;
+        const unsigned *__restrict__ cqw = J.cand.qw;
+        const int stride = 2 * S;
         for (int r = 0; r < nrows; ++r) {
-            const int a0 = __shfl_sync(kFull, ra0, r), b0 = __shfl_sync(kFull, rb0, r);
-            const int a1 = __shfl_sync(kFull, ra1, r), b1 = __shfl_sync(kFull, rb1, r);
-            const int kind = __shfl_sync(kFull, rkind, r);
-            const float sx = __shfl_sync(kFull, rsx, r), sy = __shfl_sync(kFull, rsy, r);
-            const float sz1 = __shfl_sync(kFull, rsz1, r);
             #pragma unroll 1
             for (int seg = 0; seg < 2; ++seg) {
-                const int a = seg ? a1 : a0, b = seg ? b1 : b0;
+                const RowRange &rg = ws.rows[r];
+                const int a = seg ? rg.a1 : rg.a0, b = seg ? rg.b1 : rg.b0;
                 if (a >= b) continue;
-                Seg sg;
-                sg.sx = sx; sg.sy = sy; sg.sz = seg ? sz1 : 0.f;
-                const int sh = (sg.sx != 0.f || sg.sy != 0.f || sg.sz != 0.f) ? 1 : 0;
-                sg.lo = A.fc.lo[sh];
-                sg.hi = A.fc.hi[sh];
-                sg.w = A.fc.w[sh];
-                sg.rule_flags = J.rule_flags;
-                const float2 NHX = make_float2(sg.sx - h.x, sg.sx - h.x);
-                const float2 NHY = make_float2(sg.sy - h.y, sg.sy - h.y);
-                const float2 NHZ = make_float2(sg.sz - h.z, sg.sz - h.z);
-                const int jmin = (kind == 1 && seg == 0) ? hidx : a - 1;
-                if (lane == 0) n_cand += (unsigned long long)(b - a) * (unsigned long long)H;
-                // one aligned pair of candidates (p, p+1); v0 / v1 say which are real
-                auto step = [&](int p, bool v0, bool v1) {
-                    const float2 X = __ldg(reinterpret_cast<const float2 *>(J.cand.x + p));
-                    const float2 Y = __ldg(reinterpret_cast<const float2 *>(J.cand.y + p));
-                    const float2 Z = __ldg(reinterpret_cast<const float2 *>(J.cand.z + p));
-                    float2 Wt = make_float2(1.f, 1.f);
-                    if (WEIGHTED) Wt = __ldg(reinterpret_cast<const float2 *>(J.cand.w + p));
-                    // (x_j + shift) - x_home, rounded once: same value as the
-                    // scalar (x_j - (x_home - shift)) up to the bound in make_cuts
-                    const float2 DX = __fadd2_rn(X, NHX);
-                    const float2 DY = __fadd2_rn(Y, NHY);
-                    const float2 DZ = __fadd2_rn(Z, NHZ);
-                    take2<ANI, WEIGHTED, HM>(A, J.cand, DX, DY, DZ, v0, v1, p, Wt, h, sg, sink,
-                                             n_pairs, n_rechk);
+                const float sx = rg.sx, sy = rg.sy, sz = seg ? rg.sz1 : 0.f;
+                const int sh = (sx != 0.f || sy != 0.f || sz != 0.f) ? 1 : 0;
+                const float lo = fc.lo[sh], hi = fc.hi[sh];
+                // r + 256 + w*2^-15: the window offset rides on the magic
+                // constant (exact: a multiple of the ulp at 256)
+                const unsigned w2 = 2u * fc.w[sh];
+                const float mgw = kMagic + (float)fc.w[sh] * 0x1p-15f;
+                // (x_j + shift) - x_home, rounded once: same value as the
+                // scalar (x_j - (x_home - shift)) up to the bound in make_cuts
+                const float4 h = ws.home[lane];
+                const float2 NHX = make_float2(sx - h.x, sx - h.x);
+                const float2 NHY = make_float2(sy - h.y, sy - h.y);
+                const float2 NHZ = make_float2(sz - h.z, sz - h.z);
+                const bool fwd = rg.kind == 1 && seg == 0;
+                const int jmin = fwd ? hidx : a - 1;
+                if (lane == 0) ws.n_cand += (unsigned long long)(b - a) * (unsigned long long)H;
+
+                // Rare path: the canonical rule for candidate j (reloads what
+                // the fast path does not keep in registers).
+                auto slow = [&](int j) {
+                    PairRule rule = A.rule;
+                    rule.flags = J.rule_flags;
+                    const RowRange &rq = ws.rows[r];
+                    const float4 hh = ws.home[lane];
+                    float cx, cy, cz, cw;
+                    load_point(cpk, j, cx, cy, cz, cw);
+                    const int s = slow_slot<ANI>(hh.x, hh.y, hh.z, cx, cy, cz, rq.sx, rq.sy,
+                                                 seg ? rq.sz1 : 0.f, rule);
+                    if (s >= 0) {
+                        W wj;
+                        if (FIX) wj = (W)__ldg(cqw + j);
+                        else wj = (W)cw;
+                        sink.add((unsigned)s + bias, hw, wj, true);
+                        if (COUNT) ++n_pairs;
+                    }
+                };
+                // One aligned pair of candidates (p, p+1); v0 / v1 say which are
+                // real.  Pure arithmetic: the histogram slots (biased), which
+                // pairs the fast path takes (f) and which need the FP64 rule (r).
+                struct Eval {
+                    unsigned sb0, sb1;
+                    W w0, w1;
+                    bool f0, f1, r0, r1;
+                };
+                auto eval = [&](int p, bool v0, bool v1) -> Eval {
+                    Eval e;
+                    const float4 qa = __ldg(cpk + p), qb = __ldg(cpk + p + 1);
+                    e.w0 = e.w1 = (W)1;
+                    if (FIX) {
+                        const uint2 q = __ldg(reinterpret_cast<const uint2 *>(cqw + p));
+                        e.w0 = (W)q.x;
+                        e.w1 = (W)q.y;
+                    } else if (WEIGHTED) {
+                        e.w0 = (W)qb.z;
+                        e.w1 = (W)qb.w;
+                    }
+                    const float2 DX = __fadd2_rn(make_float2(qa.x, qa.y), NHX);
+                    const float2 DY = __fadd2_rn(make_float2(qa.z, qa.w), NHY);
+                    const float2 DZ = __fadd2_rn(make_float2(qb.x, qb.y), NHZ);
+                    float m0, m1;  // the squared separation the dmax test reads
+                    if (!ANI) {
+                        float2 D2 = __fmul2_rn(DX, DX);
+                        D2 = __ffma2_rn(DY, DY, D2);
+                        D2 = __ffma2_rn(DZ, DZ, D2);
+                        m0 = D2.x;
+                        m1 = D2.y;
+                        const float2 U = __fmul2_rn(D2, make_float2(fc.ds2, fc.ds2));
+                        const float2 Q = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)),
+                                                    make_float2(mgw, mgw));
+                        const unsigned u0 = __float_as_uint(Q.x), u1 = __float_as_uint(Q.y);
+                        // f0 / f1 imply r < bins away from an edge: the slot is in range
+                        e.f0 = v0 && (m0 < lo) && fix_safe(u0, w2);
+                        e.f1 = v1 && (m1 < lo) && fix_safe(u1, w2);
+                        e.sb0 = u0 >> kFracBits;
+                        e.sb1 = u1 >> kFracBits;
+                    } else {
+                        const float2 ZZ = __fmul2_rn(DZ, DZ);
+                        const float2 PP = __ffma2_rn(DY, DY, __fmul2_rn(DX, DX));
+                        m0 = fmaxf(ZZ.x, PP.x);
+                        m1 = fmaxf(ZZ.y, PP.y);
+                        const float2 RZ = __fmul2_rn(DZ, make_float2(fc.dsf, fc.dsf));
+                        const float2 U = __fmul2_rn(PP, make_float2(fc.ds2, fc.ds2));
+                        const unsigned z0 = __float_as_uint(fabsf(RZ.x) + mgw);
+                        const unsigned z1 = __float_as_uint(fabsf(RZ.y) + mgw);
+                        const float2 QP = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)),
+                                                     make_float2(mgw, mgw));
+                        const unsigned p0 = __float_as_uint(QP.x), p1 = __float_as_uint(QP.y);
+                        e.f0 = v0 && (m0 < lo) && fix_safe(z0, w2) && fix_safe(p0, w2);
+                        e.f1 = v1 && (m1 < lo) && fix_safe(z1, w2) && fix_safe(p1, w2);
+                        const unsigned B = (unsigned)bins;
+                        e.sb0 = (z0 >> kFracBits) * B + (p0 >> kFracBits);
+                        e.sb1 = (z1 >> kFracBits) * B + (p1 >> kFracBits);
+                    }
+                    if (HM == H_GLOBAL) { e.f0 = e.f0 && A.fast; e.f1 = e.f1 && A.fast; }
+                    e.r0 = v0 && !e.f0 && m0 < hi;
+                    e.r1 = v1 && !e.f1 && m1 < hi;
+                    return e;
+                };
+                // Accumulates the fast-path pairs; true if either needs the FP64 rule.
+                auto core = [&](int p, bool v0, bool v1) -> bool {
+                    const Eval e = eval(p, v0, v1);
+                    sink.add(e.sb0, hw, e.w0, e.f0);
+                    sink.add(e.sb1, hw, e.w1, e.f1);
+                    if (COUNT) n_pairs += (unsigned)e.f0 + (unsigned)e.f1;
+                    return e.r0 || e.r1;
+                };
+                // Rechecks of `n` steps from p: the vote is rare, so the
+                // candidates are re-evaluated to find which need the FP64 rule.
+                // Lanes of different candidate streams leave the stream loop after
+                // different trip counts, so vote only among the lanes that are here.
+                auto settle = [&](bool any, int p, int n, bool v0, bool v1) {
+                    if (__any_sync(__activemask(), any)) {
+                        for (int k = 0; k < n; ++k) {
+                            const Eval e = eval(p + k * stride, v0, v1);
+                            if (e.r0) { ++n_rechk; slow(p + k * stride); }
+                            if (e.r1) { ++n_rechk; slow(p + k * stride + 1); }
+                        }
+                    }
                 };
                 // head: pairs that start before a, or that reach into the home
                 // tile of a forward row (j > home index per lane); body: pairs
                 // fully inside (a, b) past the tile, no checks; tail: the last
                 // pair when it ends at b
-                const int chk = (kind == 1 && seg == 0) ? t.start + H : a + 1;
-                const int a2 = a & ~1;
-                const int stride = 2 * S;
-                // candidates [lo, hi) (lo even; hi even or b)
-                auto run = [&](int lo, int hi) {
-                    int p = lo + 2 * sidx;
-                    for (; p < hi && p < chk; p += stride)
-                        step(p, p > jmin && p >= a, (p + 1 < b) && (p + 1 > jmin));
-                    #pragma unroll 2
-                    for (; p + 1 < hi; p += stride) step(p, true, true);
-                    if (p < hi) step(p, true, false);
-                };
-                if (HM == H_WFIX) {  // flush before a limb counter could wrap
-                    for (int lo = a2; lo < b; lo += kWfixChunk) {
-                        const int hi = min(b, lo + kWfixChunk);
-                        const int tests = (hi - lo) * H;
-                        if (wfix_since + tests > kWfixBudget) {
-                            flush_any<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
-                            wfix_since = 0;
-                        }
-                        wfix_since += tests;
-                        run(lo, hi);
+                const int chk = fwd ? t.start + H : a + 1;
+                auto run = [&](int lo_i, int hi_i) {  // candidates [lo_i, hi_i), lo_i even
+                    int p = lo_i + 2 * sidx;
+                    for (; p < hi_i && p < chk; p += stride) {
+                        const bool v0 = p > jmin, v1 = (p + 1 < b) && (p + 1 > jmin);
+                        settle(core(p, v0, v1), p, 1, v0, v1);
                     }
-                } else {
-                    run(a2, b);
+                    // body: kGroup steps per vote
+                    for (; p + (kGroup - 1) * stride + 1 < hi_i; p += kGroup * stride) {
+                        bool any = false;
+                        #pragma unroll
+                        for (int k = 0; k < kGroup; ++k) any |= core(p + k * stride, true, true);
+                        settle(any, p, kGroup, true, true);
+                    }
+                    for (; p + 1 < hi_i; p += stride) settle(core(p, true, true), p, 1, true, true);
+                    if (p < hi_i) settle(core(p, true, false), p, 1, true, false);
+                };
+                // flush before a shared counter could wrap: a chunk of c
+                // candidates adds at most c * H times to one per-warp counter
+                // and at most c / S + 2 times to one per-lane counter
+                for (int lo_i = a & ~1; lo_i < b; lo_i += A.chunk) {
+                    const int hi_i = min(b, lo_i + A.chunk);
+                    if (HM != H_GLOBAL) {
+                        const int c = hi_i - lo_i;
+                        const int adds = (HM == H_LANE || HM == H_LFIX) ? c / S + 2 : c * H;
+                        if (since + adds > A.budget) {
+                            flush_copy<WEIGHTED, HM>(mine, nb, lane, A, ws.slot, J.wunscale);
+                            since = 0;
+                        }
+                        since += adds;
+                    }
+                    run(lo_i, hi_i);
                 }
             }
         }
+        __syncwarp();  // the next item overwrites this item's rows and homes
         next = __shfl_sync(kFull, next, 0);
     }
     // per-warp flush (no CTA barrier: warps leave as the queue drains)
     __syncwarp();
-    if (cj >= 0) flush_any<WEIGHTED, HM>(mine, nb, per_warp, lane, A, slot);
+    if (ws.cj >= 0) flush_copy<WEIGHTED, HM>(mine, nb, lane, A, ws.slot, J.wunscale);
     unsigned long long rp = n_pairs, rr = n_rechk;
     for (int off = 16; off > 0; off >>= 1) {
         rr += __shfl_down_sync(kFull, rr, off);
@@ -497,8 +597,8 @@ __global__ void __launch_bounds__(kThreads, HM == H_WFIX ? 5 : PCF_PAIR_MINB) k_
     }
     if (lane == 0) {
         if (rr) atomicAdd(A.g_stats + 0, rr);
-        if (n_cand) atomicAdd(A.g_stats + 1, n_cand);
-        if (rp) atomicAdd(A.g_stats + 2, rp);
+        if (ws.n_cand) atomicAdd(A.g_stats + 1, ws.n_cand);
+        if (COUNT && rp) atomicAdd(A.g_stats + 2, rp);
     }
 }
 
@@ -629,10 +729,20 @@ static FastCuts make_cuts(const PairRule &rule, float box, float dmax) {
     return fc;
 }
 
-template <bool ANI, bool W, int HM>
+static int copy_words_host(int hm, int nb) {
+    switch (hm) {
+    case H_LANE: return copy_words<H_LANE>(nb);
+    case H_WARP: return copy_words<H_WARP>(nb);
+    case H_WFIX: return copy_words<H_WFIX>(nb);
+    case H_LFIX: return copy_words<H_LFIX>(nb);
+    }
+    return 0;
+}
+
+template <bool ANI, bool W, int HM, bool C = false>
 static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items, cudaStream_t st,
                               int sm_count, int device) {
-    auto kfn = k_pairs<ANI, W, HM>;
+    auto kfn = k_pairs<ANI, W, HM, C>;
     // attribute / occupancy queries cost microseconds each: do them once per
     // (device, variant, shared-memory size)
     constexpr int kDev = 64;
@@ -646,7 +756,8 @@ static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items,
     }
     const int dv = (device >= 0 && device < kDev) ? device : 0;
     cudaError_t e;
-    if (smem > 48 * 1024 && smem > attr_smem[dv]) {
+    // the opt-in limit covers static (per-warp state) + dynamic shared memory
+    if (smem > attr_smem[dv]) {
         e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_smem[dv] = smem;
@@ -665,44 +776,64 @@ static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items,
 }
 
 // Chooses the histogram mode of one launch and starts the kernel.
-static cudaError_t dispatch_pairs(const PairArgs &A, const PairLaunch &pl, cudaStream_t st,
+static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t st,
                                   int sm_count, int device) {
     const int nb = pl.ani ? pl.rule.bins * pl.rule.bins : pl.rule.bins;
     const size_t ebytes = pl.weighted ? 8 : 4;
-    const size_t lane_bytes = (size_t)nb * 32 * kWarps * ebytes;
-    const size_t warp_bytes = (size_t)nb * kWarps * ebytes;
+    auto bytes = [&](int hm) -> size_t {
+        const size_t e = (hm == H_WFIX || hm == H_LFIX) ? 4 : ebytes;
+        return (size_t)copy_words_host(hm, nb) * e * kWarps;
+    };
+    auto fits = [&](int hm) -> bool {
+        if (pl.rule.bins > 255) return hm == H_GLOBAL;
+        switch (hm) {
+        case H_LANE: return !pl.ani && bytes(hm) <= 64 * 1024;
+        case H_LFIX: return !pl.ani && pl.weighted && pl.wfix && bytes(hm) <= 64 * 1024;
+        case H_WFIX: return pl.weighted && pl.wfix && bytes(hm) <= 160 * 1024;
+        case H_WARP: return bytes(hm) <= 160 * 1024;
+        case H_GLOBAL: return true;
+        }
+        return false;
+    };
     int hm;
-    size_t smem;
-    const bool wfix_ok = pl.weighted && pl.wlimbs >= 3 && pl.rule.bins <= 255;
-    const size_t wfix_bytes = (size_t)nb * 4 * pl.wlimbs * kWarps;
-    if (pl.rule.bins > 255 || warp_bytes > 160 * 1024) { hm = H_GLOBAL; smem = 0; }
-    else if (!pl.ani && lane_bytes <= 64 * 1024) { hm = H_LANE; smem = lane_bytes; }
-    else { hm = H_WARP; smem = warp_bytes; }
-    if (hm == H_WARP && wfix_ok && wfix_bytes <= 160 * 1024) { hm = H_WFIX; smem = wfix_bytes; }
+    if (pl.rule.bins > 255 || !fits(H_WARP)) hm = H_GLOBAL;
+    else if (pl.weighted && fits(H_LFIX)) hm = H_LFIX;
+    else if (pl.weighted && fits(H_WFIX)) hm = H_WFIX;
+    else if (!pl.weighted && fits(H_LANE)) hm = H_LANE;
+    else hm = H_WARP;
     // an autotuned scheme overrides the rule above when it is valid here
-    if (pl.hist_mode == H_GLOBAL) { hm = H_GLOBAL; smem = 0; }
-    else if (pl.hist_mode == H_WFIX && wfix_ok && wfix_bytes <= 160 * 1024) {
-        hm = H_WFIX; smem = wfix_bytes;
-    }
-    else if (pl.hist_mode == H_WARP && pl.rule.bins <= 255 && warp_bytes <= 160 * 1024) {
-        hm = H_WARP; smem = warp_bytes;
-    } else if (pl.hist_mode == H_LANE && !pl.ani && pl.rule.bins <= 255 && lane_bytes <= 64 * 1024) {
-        hm = H_LANE; smem = lane_bytes;
+    if (pl.hist_mode >= 0 && pl.hist_mode <= H_LFIX && fits(pl.hist_mode)) hm = pl.hist_mode;
+    const size_t smem = hm == H_GLOBAL ? 0 : bytes(hm);
+    // budget: adds one shared counter absorbs between flushes; chunk:
+    // candidates per budget check (one chunk alone stays within the budget)
+    if (hm == H_WFIX || hm == H_LFIX) {
+        A.budget = pl.wbudget;
+        A.chunk = std::max(2, (pl.wbudget / 32) & ~1);
+    } else {
+        A.budget = 1 << 30;  // u32 counters: flushed long before 2^32
+        A.chunk = 1 << 22;
     }
     const long long n = A.n_items;
+#define PCF_DISPATCH_W(ANI_, C_)                                                                   \
+    {                                                                                              \
+        if (!ANI_ && hm == H_LANE) return launch_one<false, true, H_LANE, C_>(A, smem, n, st, sm_count, device); \
+        if (hm == H_WARP) return launch_one<ANI_, true, H_WARP, C_>(A, smem, n, st, sm_count, device);   \
+        if (hm == H_WFIX) return launch_one<ANI_, true, H_WFIX, C_>(A, smem, n, st, sm_count, device);   \
+        if (!ANI_ && hm == H_LFIX) return launch_one<false, true, H_LFIX, C_>(A, smem, n, st, sm_count, device); \
+        return launch_one<ANI_, true, H_GLOBAL, C_>(A, smem, n, st, sm_count, device);                 \
+    }
 #define PCF_DISPATCH(ANI_)                                                                       \
     if (pl.weighted) {                                                                           \
-        if (hm == H_LANE) return launch_one<ANI_, true, H_LANE>(A, smem, n, st, sm_count, device);   \
-        if (hm == H_WARP) return launch_one<ANI_, true, H_WARP>(A, smem, n, st, sm_count, device);   \
-        if (hm == H_WFIX) return launch_one<ANI_, true, H_WFIX>(A, smem, n, st, sm_count, device);   \
-        return launch_one<ANI_, true, H_GLOBAL>(A, smem, n, st, sm_count, device);                 \
+        if (pl.count) PCF_DISPATCH_W(ANI_, true)                                                 \
+        else PCF_DISPATCH_W(ANI_, false)                                                         \
     } else {                                                                                     \
-        if (hm == H_LANE) return launch_one<ANI_, false, H_LANE>(A, smem, n, st, sm_count, device);  \
+        if (!ANI_ && hm == H_LANE) return launch_one<false, false, H_LANE>(A, smem, n, st, sm_count, device);  \
         if (hm == H_WARP) return launch_one<ANI_, false, H_WARP>(A, smem, n, st, sm_count, device);  \
         return launch_one<ANI_, false, H_GLOBAL>(A, smem, n, st, sm_count, device);                \
     }
     if (pl.ani) { PCF_DISPATCH(true) } else { PCF_DISPATCH(false) }
 #undef PCF_DISPATCH
+#undef PCF_DISPATCH_W
 }
 
 static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
@@ -722,41 +853,42 @@ static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
     A.g_count = d_count;
     A.g_wsum = d_wsum;
     A.g_stats = d_stats;
-    A.wscale = pl.wscale;
-    A.wunscale = pl.wlimbs ? 1.0 / (double)pl.wscale : 0.0;
-    A.wlimbs = pl.wlimbs;
+    A.chunk = 1 << 22;
+    A.budget = 1 << 30;
+    A.fast = pl.rule.bins <= 255 ? 1 : 0;
     return A;
 }
 
-// Scale of the fixed-point weighted histograms of a launch whose points come
-// from grids gs[0..n): s such that every nonzero product w_a*w_b is at least
-// 2^42 after scaling (rounding it costs at most 2^-43 of its value), with
-// the largest below 2^48 (three limbs) or 2^64 (four).  Weights must be
-// finite and >= 0, and each weight * 2^s a normal float.  Otherwise the
-// launch keeps FP64 shared atomics (wlimbs = 0).
+// Fixed-point weighted histograms: every grid has exact integer weights q <
+// 2^32 (set_weight_range), so a product q_a*q_b is exact in 64 bits and
+// splits into limbs l0 = bits 0-15, l1 = bits 16-31, l2 = bits 32-63.  A u32
+// counter absorbs 65536 adds of l0 or l1, and floor((2^32-1) / max l2) adds
+// of l2: the smaller is the flush budget.  Launches whose largest product
+// would leave a budget under 4096 keep FP64 shared atomics.
 void set_weight_fix(PairLaunch &pl, const pcf_grid *const *gs, int n) {
-    pl.wscale = 0.f;
-    pl.wlimbs = 0;
+    pl.wfix = false;
+    pl.wbudget = 0;
     if (!pl.weighted) return;
-    double wmin = 0.0, wmax = 0.0;
+    unsigned long long qmax = 0;
     for (int i = 0; i < n; ++i) {
-        const pcf_grid *g = gs[i];
-        if (!g->w_finite_nonneg) return;
-        wmax = std::max(wmax, (double)g->w_absmax);
-        if (g->w_absmin > 0.f) wmin = wmin > 0.0 ? std::min(wmin, (double)g->w_absmin) : (double)g->w_absmin;
+        if (!gs[i]->wfix_ok) return;
+        qmax = std::max(qmax, gs[i]->wqmax);
     }
-    if (!(wmin > 0.0)) return;
-    const double pmin = wmin * wmin, pmax = wmax * wmax;  // exact: 24-bit mantissas
-    const int s = 42 - (int)std::floor(std::log2(pmin));
-    if (s < -120 || s > 120) return;
-    const double top = std::ldexp(pmax, s);
-    int limbs;
-    if (top < std::ldexp(1.0, 48) - 1.0) limbs = 3;
-    else if (top < std::ldexp(1.0, 64) - 4096.0) limbs = 4;
-    else return;
-    if (std::ldexp(wmin, s) < std::ldexp(1.0, -125) || std::ldexp(wmax, s) >= std::ldexp(1.0, 126)) return;
-    pl.wscale = std::ldexp(1.0f, s);
-    pl.wlimbs = limbs;
+    const unsigned __int128 top = (unsigned __int128)qmax * qmax;
+    const unsigned long long hi = (unsigned long long)(top >> 32);
+    const unsigned long long budget = hi ? std::min<unsigned long long>(65536, 0xFFFFFFFFull / hi) : 65536;
+    if (budget < 4096) return;
+    pl.wfix = true;
+    pl.wbudget = (int)budget;
+}
+
+double weight_unscale(const pcf_grid *home, const pcf_grid *cand) {
+    return std::ldexp(1.0, -(home->wshift + cand->wshift));
+}
+
+PairView pair_view(const CellGrid &g, bool with_q) {
+    return PairView{g.pk.as<float4>(), with_q ? g.qw.as<unsigned>() : nullptr,
+                    g.cell_start.as<int>()};
 }
 
 cudaError_t launch_pair_jobs(const PairJob *d_jobs, int n_jobs, long long n_items, int P, float box,
@@ -779,7 +911,7 @@ void shape_job(PairJob &j, int64_t n_tiles, int n_rows, int64_t total_tile_rows,
     (void)n_tiles;
 }
 
-cudaError_t launch_pairs_view(const GridView &home, const GridView &cand, const TileDesc *tiles,
+cudaError_t launch_pairs_view(const PairView &home, const PairView &cand, const TileDesc *tiles,
                               int64_t n_tiles, const RowDesc *rows, int n_rows, int P, float box,
                               const PairLaunch &pl, unsigned long long *counter,
                               unsigned long long *d_count, double *d_wsum,
@@ -794,6 +926,7 @@ cudaError_t launch_pairs_view(const GridView &home, const GridView &cand, const 
     j.item_begin = 0;
     j.rule_flags = pl.rule.flags;
     j.pad = 0;
+    j.wunscale = 0.0;
     shape_job(j, n_tiles, n_rows, n_tiles * n_rows, sm_count);
     const long long n_items = (long long)n_tiles * j.n_chunks;
     cudaError_t e = cudaMemcpyAsync(d_job, &j, sizeof(PairJob), cudaMemcpyHostToDevice, st);
@@ -855,8 +988,8 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     if (ps != PCF_OK) return ps;
     // the one job of this launch, staged behind the rows in the same slot
     PairJob job;
-    job.home = GridView{home.x(), home.y(), home.z(), home.w(), home.cell_start.as<int>()};
-    job.cand = GridView{cand.x(), cand.y(), cand.z(), cand.w(), cand.cell_start.as<int>()};
+    job.home = pair_view(home, pl.wfix);
+    job.cand = pair_view(cand, pl.wfix);
     job.tiles = home.d_tiles.as<TileDesc>();
     job.rows = sl->d_rows.as<RowDesc>();
     job.n_rows = (int)plan.rows.size();
@@ -866,6 +999,7 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     job.item_begin = 0;
     job.rule_flags = pl.rule.flags;
     job.pad = 0;
+    job.wunscale = pl.wunscale;
     const size_t roff = (plan.rows.size() * sizeof(RowDesc) + 255) & ~(size_t)255;
     char *hjob = static_cast<char *>(sl->h_pinned) + roff;
     memcpy(hjob, &job, sizeof(PairJob));

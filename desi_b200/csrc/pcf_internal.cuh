@@ -97,6 +97,18 @@ struct GridView {
     const int *cstart;
 };
 
+// The pair kernel's view of a gridded catalog.  Points are pair-packed: the
+// cell-ordered points 2k and 2k+1 form one 32-byte block of two float4,
+//   pk[2k] = (x_2k, x_2k+1, y_2k, y_2k+1),  pk[2k+1] = (z_2k, z_2k+1, w_2k, w_2k+1),
+// so two candidates arrive in two 16-byte loads already laid out for the
+// packed f32x2 arithmetic.  qw holds the exact integer weights
+// q = w * 2^wshift of a grid whose weights allow it (null otherwise).
+struct PairView {
+    const float4 *pk;
+    const unsigned *qw;
+    const int *cstart;
+};
+
 // ---------------------------------------------------------------------------
 // Host-side objects.
 // ---------------------------------------------------------------------------
@@ -127,10 +139,13 @@ struct DevBuf {
 
 struct CellGrid {
     int P = 0;
+    uint64_t serial = 0;          // unique per build (keys captured graphs)
     float cell = 0.f;             // box / P
     DevBuf pts;                   // float4 x n, cell order
     DevBuf soa;                   // x | y | z | w planes, n + kSoaPad floats each
     size_t plane = 0;             // floats per plane
+    DevBuf pk;                    // pair-packed blocks (PairView), pk_blocks(n) x 32 B
+    DevBuf qw;                    // exact integer weights (u32 x (n + kSoaPad)), when wfix_ok
     DevBuf cell_start;            // int x (P^3 + 1)
     std::vector<int> h_start;     // host copy of cell_start
     std::vector<TileDesc> tiles;  // home tiles: <= 32 points of one cell
@@ -143,6 +158,8 @@ struct CellGrid {
 // SoA planes are padded so that a float2 load at the last even index stays
 // inside the allocation, and each plane starts 16-byte aligned.
 constexpr int kSoaPad = 4;
+// Pair-packed blocks of a catalog of n points (one spare block past the end).
+inline size_t pk_blocks(int64_t n) { return (size_t)(n / 2) + 2; }
 
 struct pcf_grid {
     std::shared_ptr<MemPool> pool;
@@ -154,9 +171,18 @@ struct pcf_grid {
     // weight is finite and >= 0
     float w_absmax = 1.f, w_absmin = 1.f;
     bool w_finite_nonneg = true;
+    // exact integer weights q = w * 2^wshift (q < 2^32) exist when every
+    // weight is finite, >= 0, and the nonzero ones are normal floats within
+    // 8 binades of each other; wqmax = the largest q
+    bool wfix_ok = false;
+    int wshift = 0;
+    unsigned long long wqmax = 0;
     DevBuf raw;                   // float4 x n, input order
-    std::unique_ptr<CellGrid> cells;
+    int user_P = 0;               // partitions fixed by the caller at build (0: automatic)
+    std::unique_ptr<CellGrid> cells;                    // the current cell structure
+    std::vector<std::unique_ptr<CellGrid>> cell_cache;  // earlier ones, most recent last
 };
+constexpr int kCellCache = 2;  // cell structures kept besides the current one
 
 // One of two plan staging slots: while the device runs the kernel of one
 // call, the host builds and stages the plan of the next into the other.
@@ -241,11 +267,18 @@ struct PairLaunch {
     PairRule rule;
     double mult;         // 2 for XX (ordered-pair convention), 1 for XY
     int hist_mode = -1;  // 0 lane-private, 1 per-warp shared, 2 global, 3 per-warp
-                         // fixed-point (weighted); -1 automatic
-    float wscale = 0.f;  // fixed-point weighted sums: 2^s (set_weight_fix)
-    int wlimbs = 0;      // 0: not available for this launch
+                         // fixed-point (weighted), 4 lane-private fixed-point
+                         // (weighted iso); -1 automatic
+    bool wfix = false;   // exact integer weight products available (set_weight_fix)
+    int wbudget = 0;     // limb adds between flushes of a fixed-point copy
+    double wunscale = 0.0;  // single-job launches: weight_unscale(home, cand)
+    bool count = true;   // weighted launches: count in-range pairs (statistics)
 };
+// Enables the fixed-point weighted histograms when every grid of the launch
+// has exact integer weights and any product fits the three-limb budget.
 void set_weight_fix(PairLaunch &pl, const pcf_grid *const *gs, int n);
+// 2^-(wshift_home + wshift_cand): converts a fixed-point sum back to w*w units.
+double weight_unscale(const pcf_grid *home, const pcf_grid *cand);
 std::string tune_key(int kind, bool bpc, bool cross, bool weighted, int bins, int64_t n, float box,
                      float dmax);
 pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home,
@@ -256,14 +289,16 @@ pcf_status finalize_hist(pcf_ctx *ctx, const unsigned long long *d_count, const 
 // One histogram of a pair launch: home / candidate catalogs, stencil rows,
 // and the implicit items [item_begin, item_begin + n_tiles * n_chunks).
 struct PairJob {
-    GridView home, cand;
+    PairView home, cand;
     const TileDesc *tiles;
     const RowDesc *rows;
     int n_rows, rows_per_item, n_chunks, slot;
     long long item_begin;
     unsigned rule_flags;  // exact-rule flags of this histogram (XX and XY differ)
     int pad;
+    double wunscale;      // fixed-point launches: weight_unscale(home, cand)
 };
+PairView pair_view(const CellGrid &g, bool with_q);
 void shape_job(PairJob &j, int64_t n_tiles, int n_rows, int64_t total_tile_rows, int sm_count);
 // The pair kernel over a device job table (jobs ordered by item_begin);
 // counter and the n_jobs * nb accumulators zeroed by the caller.
@@ -273,7 +308,7 @@ cudaError_t launch_pair_jobs(const PairJob *d_jobs, int n_jobs, long long n_item
                              unsigned long long *d_stats, cudaStream_t st, int sm_count, int device);
 // Single-job form on explicit buffers (no context); d_job: device room for
 // one PairJob.
-cudaError_t launch_pairs_view(const GridView &home, const GridView &cand, const TileDesc *tiles,
+cudaError_t launch_pairs_view(const PairView &home, const PairView &cand, const TileDesc *tiles,
                               int64_t n_tiles, const RowDesc *rows, int n_rows, int P, float box,
                               const PairLaunch &pl, unsigned long long *counter,
                               unsigned long long *d_count, double *d_wsum,
@@ -287,9 +322,15 @@ cudaError_t launch_finalize_slots(const unsigned long long *d_count, const doubl
 unsigned reference_pair_rule(bool ani, bool bpc, bool cross);
 // Counting sort of n points into P^3 cells on explicit buffers; returns the
 // number of kernels launched (counts must be zeroed, P^3 + 1 entries).
+// pts_out, soa and qw may be null; pk (pk_blocks(n) blocks, zeroed by the
+// caller) is always written, qw only when the weights allow exact integers.
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
                       int *rank, int *counts, int *cell_start, int *scan_tmp, float4 *pts_out,
-                      float *soa, size_t plane, int *flags, cudaStream_t st);
+                      float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
+                      cudaStream_t st);
+// Host side of the weight scan (flags[0..2] as written by the grid build):
+// fills g's weight-range fields, including the integer-weight scale.
+void set_weight_range(pcf_grid *g, const unsigned flags[3]);
 // Tile table on the device: per cell ceil(count / kTileCap) tiles; tile
 // offsets (P^3 + 1) give the total in offsets[P^3].
 int launch_tile_build(const int *cell_start, int P, int *tile_counts, int *tile_offsets,

@@ -31,15 +31,17 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
     out.pool = ctx->pool;
     PCF_CU(ctx, out.ensure(sizeof(double) * nb));
     const int refines[] = {0, 3, 4, 5, 6, 8};
-    const int modes[] = {-1, 0, 1, 3};  // 3: fixed-point weighted sums (weighted only)
+    const int modes[] = {-1, 0, 1, 3, 4};  // 3, 4: fixed-point weighted sums (weighted only)
     TuneEntry best;
     best.ms = 1e30f;
     float default_ms = 0.f;
     int tried = 0;
     ctx->tune.erase(key);
     for (int r : refines) {
+        // partitions fixed by the caller: tune the histogram scheme only
+        if ((a->user_P > 0 || (b && b->user_P > 0)) && r != 0) continue;
         for (int m : modes) {
-            if ((m == 0 && ani) || (m == 3 && !weighted)) continue;
+            if (((m == 0 || m == 4) && ani) || ((m == 3 || m == 4) && !weighted)) continue;
             ctx->tune_override.refine = r;
             ctx->tune_override.hist_mode = m;
             float ms = 1e30f;
