@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <sstream>
 
 #include "pcf_internal.cuh"
@@ -26,6 +27,7 @@ struct BatchGraph {
     double *d_out = nullptr;
     unsigned long long *d_stats = nullptr;
     std::vector<double> mult;  // per slot: 2 for XX, 1 for XY
+    std::vector<std::shared_ptr<CellGrid>> keep;  // cell structures the jobs read
     ~BatchGraph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -52,12 +54,33 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     }
     const float box = D->box;
     if (bpc && !(2.0 * (double)dmax < (double)box)) return PCF_ERR_UNSUPPORTED;
-    const int P = choose_partitions(nmax, box, dmax, kind, bpc, 0);
-    pcf_status s = grid_ensure_cells(ctx, D, P);
-    if (s != PCF_OK) return s;
-    for (auto *g : R) {
-        s = grid_ensure_cells(ctx, g, P);
-        if (s != PCF_OK) return s;
+    // The jobs: DD, then RR_i and DR_i per random catalog.  Each job gets the
+    // partition count a single call would use for its catalogs (small
+    // catalogs get coarser cells), and holds the cell structures at that
+    // count (a grid keeps several).
+    struct J {
+        pcf_grid *h, *c;
+        bool self;
+        double mult;
+        int P;
+        std::shared_ptr<CellGrid> hc, cc;
+    };
+    std::vector<J> js;
+    auto add_job = [&](pcf_grid *h, pcf_grid *c, bool self, double mult) {
+        const int64_t n = std::max<int64_t>(h->n, c->n);
+        js.push_back({h, c, self, mult, choose_partitions(n, box, dmax, kind, bpc, 0), nullptr, nullptr});
+    };
+    if (dd) add_job(D, D, true, 2.0);
+    for (int i = 0; i < n_rand; ++i) {
+        if (rr) add_job(R[i], R[i], true, 2.0);
+        if (dr) add_job(D, R[i], false, 1.0);
+    }
+    pcf_status s = PCF_OK;
+    for (auto &j : js) {
+        if ((s = grid_ensure_cells(ctx, j.h, j.P)) != PCF_OK) return s;
+        j.hc = j.h->cells;
+        if ((s = grid_ensure_cells(ctx, j.c, j.P)) != PCF_OK) return s;
+        j.cc = j.c->cells;
     }
     const int nb = ani ? bins * bins : bins;
     bool weighted = !D->unit_weights;
@@ -69,8 +92,8 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     if (use_graph) {
         std::ostringstream os;
         os << kind << ':' << bins << ':' << dmax << ':' << (flags & ~PCF_GRAPH) << ':' << (dd != nullptr)
-           << (rr != nullptr) << (dr != nullptr) << ':' << D->cells->serial;
-        for (auto *g : R) os << ',' << g->cells->serial;
+           << (rr != nullptr) << (dr != nullptr);
+        for (auto &j : js) os << ',' << j.hc->serial << '/' << j.cc->serial;
         key = os.str();
     }
     std::shared_ptr<BatchGraph> bg;
@@ -95,22 +118,30 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         bg = std::make_shared<BatchGraph>();
         bg->plan.pool = ctx->pool;
         bg->accum.pool = ctx->pool;
-        std::vector<RowDesc> rows_self, rows_cross;
-        plan_rows(P, box, dmax, ani, true, rows_self);
-        plan_rows(P, box, dmax, ani, false, rows_cross);
-        struct J { pcf_grid *h, *c; bool self; double mult; };
-        std::vector<J> js;
-        if (dd) js.push_back({D, D, true, 2.0});
-        for (int i = 0; i < n_rand; ++i) {
-            if (rr) js.push_back({R[i], R[i], true, 2.0});
-            if (dr) js.push_back({D, R[i], false, 1.0});
+        // stencil rows per distinct partition count: [P] -> (self, cross)
+        std::map<int, std::pair<std::vector<RowDesc>, std::vector<RowDesc>>> rows;
+        for (auto &j : js) {
+            if (rows.count(j.P)) continue;
+            auto &rp = rows[j.P];
+            plan_rows(j.P, box, dmax, ani, true, rp.first);
+            plan_rows(j.P, box, dmax, ani, false, rp.second);
         }
         const int nslots = (int)js.size();
         int64_t total = 0;
-        for (auto &j : js) total += (int64_t)j.h->cells->tiles.size() * (j.self ? rows_self.size() : rows_cross.size());
-        const size_t rb_s = rows_self.size() * sizeof(RowDesc), rb_c = rows_cross.size() * sizeof(RowDesc);
-        const size_t off_c = (rb_s + 255) & ~(size_t)255;
-        const size_t off_j = (off_c + rb_c + 255) & ~(size_t)255;
+        for (auto &j : js) {
+            const auto &rp = rows[j.P];
+            total += (int64_t)j.hc->tiles.size() * (int64_t)(j.self ? rp.first.size() : rp.second.size());
+        }
+        // plan buffer: row tables | jobs | mults
+        std::map<int, std::pair<size_t, size_t>> roff;  // [P] -> (self, cross) byte offsets
+        size_t off = 0;
+        for (auto &kv : rows) {
+            const size_t a = off;
+            off = (off + kv.second.first.size() * sizeof(RowDesc) + 255) & ~(size_t)255;
+            roff[kv.first] = {a, off};
+            off = (off + kv.second.second.size() * sizeof(RowDesc) + 255) & ~(size_t)255;
+        }
+        const size_t off_j = off;
         const size_t off_m = (off_j + sizeof(PairJob) * nslots + 255) & ~(size_t)255;
         const size_t plan_bytes = off_m + sizeof(double) * nslots;
         PCF_CU(ctx, bg->plan.ensure(plan_bytes));
@@ -120,14 +151,15 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         long long item = 0;
         const unsigned rXX = reference_pair_rule(ani, bpc, false), rXY = reference_pair_rule(ani, bpc, true);
         for (int k = 0; k < nslots; ++k) {
-            const CellGrid &h = *js[k].h->cells, &c = *js[k].c->cells;
+            const CellGrid &h = *js[k].hc, &c = *js[k].cc;
+            const auto &rp = rows[js[k].P];
             PairJob &j = jobs[k];
             j.home = pair_view(h, pl.wfix);
             j.cand = pair_view(c, pl.wfix);
             j.wunscale = weight_unscale(js[k].h, js[k].c);
             j.tiles = h.d_tiles.as<TileDesc>();
-            j.rows = reinterpret_cast<const RowDesc *>(dp + (js[k].self ? 0 : off_c));
-            shape_job(j, (int64_t)h.tiles.size(), (int)(js[k].self ? rows_self.size() : rows_cross.size()),
+            j.rows = reinterpret_cast<const RowDesc *>(dp + (js[k].self ? roff[js[k].P].first : roff[js[k].P].second));
+            shape_job(j, (int64_t)h.tiles.size(), (int)(js[k].self ? rp.first.size() : rp.second.size()),
                       total, ctx->sm_count);
             j.slot = k;
             j.item_begin = item;
@@ -135,13 +167,19 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
                                ? (((flags & PCF_RULE_EXCL_ZERO) ? PCF_RULE_EXCL : 0u) |
                                   ((flags & PCF_RULE_INCLUSIVE) ? PCF_RULE_LE : 0u))
                                : (js[k].self ? rXX : rXY);
-            j.pad = 0;
+            j.P = js[k].P;
             item += (long long)h.tiles.size() * j.n_chunks;
             mult[k] = js[k].mult;
+            bg->keep.push_back(js[k].hc);
+            bg->keep.push_back(js[k].cc);
         }
         std::vector<char> host(plan_bytes, 0);
-        memcpy(host.data(), rows_self.data(), rb_s);
-        memcpy(host.data() + off_c, rows_cross.data(), rb_c);
+        for (auto &kv : rows) {
+            memcpy(host.data() + roff[kv.first].first, kv.second.first.data(),
+                   kv.second.first.size() * sizeof(RowDesc));
+            memcpy(host.data() + roff[kv.first].second, kv.second.second.data(),
+                   kv.second.second.size() * sizeof(RowDesc));
+        }
         memcpy(host.data() + off_j, jobs.data(), sizeof(PairJob) * nslots);
         memcpy(host.data() + off_m, mult.data(), sizeof(double) * nslots);
         PCF_CU(ctx, cudaMemcpyAsync(dp, host.data(), plan_bytes, cudaMemcpyHostToDevice, st));
@@ -163,7 +201,7 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         auto enqueue = [&]() -> cudaError_t {
             cudaError_t e = cudaMemsetAsync(ap, 0, nacc * 16 + 128, st);
             if (e != cudaSuccess) return e;
-            e = launch_pair_jobs(reinterpret_cast<const PairJob *>(dp + off_j), nslots, item, P, box, pl,
+            e = launch_pair_jobs(reinterpret_cast<const PairJob *>(dp + off_j), nslots, item, js[0].P, box, pl,
                                  counter, cnt, ws, stt, st, ctx->sm_count, ctx->device);
             if (e != cudaSuccess) return e;
             return launch_finalize_slots(cnt, ws, weighted, reinterpret_cast<const double *>(dp + off_m),
@@ -220,7 +258,7 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         stats->rechecks = (double)hs[0];
         stats->candidates = (double)hs[1];
         stats->kernel_ms = ms;
-        stats->partitions = P;
+        stats->partitions = js.empty() ? 0 : js[0].P;  // the DD job's (or first job's)
         stats->work_items = bg->nslots;
     }
     if (!use_graph) bg.reset();

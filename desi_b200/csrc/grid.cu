@@ -301,14 +301,14 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     if (P < 1 || P > 320) return PCF_ERR_INVALID_ARG;
     for (size_t i = 0; i < g->cell_cache.size(); ++i) {
         if (g->cell_cache[i]->P != P) continue;
-        std::unique_ptr<CellGrid> hit = std::move(g->cell_cache[i]);
+        std::shared_ptr<CellGrid> hit = std::move(g->cell_cache[i]);
         g->cell_cache.erase(g->cell_cache.begin() + (long)i);
         if (g->cells) g->cell_cache.push_back(std::move(g->cells));
         g->cells = std::move(hit);
         return PCF_OK;
     }
     static uint64_t next_serial = 0;
-    std::unique_ptr<CellGrid> cg(new CellGrid);
+    std::shared_ptr<CellGrid> cg(new CellGrid);
     cg->serial = ++next_serial;
     cg->pts.pool = cg->soa.pool = cg->cell_start.pool = g->pool;
     cg->P = P;

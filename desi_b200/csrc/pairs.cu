@@ -58,6 +58,7 @@ constexpr int kLimbs = 3;
 #define PCF_PAIR_GROUP 4
 #endif
 constexpr int kGroup = PCF_PAIR_GROUP;  // candidate steps between recheck votes
+constexpr int kChunkMax = 8;            // work items per ticket, at most
 
 // Fast-path cut constants for one range type (0: unshifted, 1: image-shifted).
 struct FastCuts {
@@ -73,8 +74,10 @@ struct PairArgs {
     const PairJob *jobs;  // histograms of this launch, items laid out job after job
     int n_jobs;
     long long n_items;
-    unsigned long long *counter;
-    int P;
+    unsigned long long *counter;  // work tickets handed out so far
+    long long n_chunked;          // items [0, n_chunked) go out `kchunk` per ticket,
+    long long t_chunked;          // in t_chunked tickets; later tickets: one item each
+    int kchunk;
     float box;
     int bpc;
     PairRule rule;
@@ -326,12 +329,27 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
     unsigned n_pairs = 0, n_rechk = 0;
     const FastCuts &fc = A.fc;
 
-    long long next = 0;
-    if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);
-    next = __shfl_sync(kFull, next, 0);
-    while (next < A.n_items) {
-        const long long it_idx = next;
-        if (lane == 0) next = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next item
+    // Work queue of tickets: while a queue holds many items per warp, a
+    // ticket is a run of `kchunk` consecutive items (a warp then changes job,
+    // and flushes its histogram copy, less often); the last two rounds go out
+    // one item per ticket so the tail stays short.
+    auto ticket_items = [&](long long t, long long &ib, long long &ie) {
+        if (t < A.t_chunked) {
+            ib = t * A.kchunk;
+            ie = min(ib + A.kchunk, A.n_chunked);
+        } else {
+            ib = A.n_chunked + (t - A.t_chunked);
+            ie = ib + 1;
+        }
+        ie = min(ie, A.n_items);
+    };
+    long long tk = 0, ib, ie;
+    if (lane == 0) tk = (long long)atomicAdd(A.counter, 1ull);
+    tk = __shfl_sync(kFull, tk, 0);
+    ticket_items(tk, ib, ie);
+    while (ib < A.n_items) {
+      if (lane == 0) tk = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next ticket
+      for (long long it_idx = ib; it_idx < ie; ++it_idx) {
         if (it_idx >= ws.job_end) {  // entering another job: flush this one's histogram
             if (ws.cj >= 0) flush_copy<WEIGHTED, HM>(mine, nb, lane, A, ws.slot, J.wunscale);
             since = 0;
@@ -387,7 +405,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
             RowRange rr{0, 0, 0, 0, 0.f, 0.f, 0.f, 0};
             const RowDesc rw = J.rows[row_begin + lane];
             int nx = t.ix + rw.dx, ny = t.iy + rw.dy;
-            const int P = A.P;
+            const int P = J.P;
             bool ok = true;
             if (A.bpc) {
                 if (nx < 0) { nx += P; rr.sx = -A.box; } else if (nx >= P) { nx -= P; rr.sx = A.box; }
@@ -585,7 +603,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
             }
         }
         __syncwarp();  // the next item overwrites this item's rows and homes
-        next = __shfl_sync(kFull, next, 0);
+      }
+      tk = __shfl_sync(kFull, tk, 0);
+      ticket_items(tk, ib, ie);
     }
     // per-warp flush (no CTA barrier: warps leave as the queue drains)
     __syncwarp();
@@ -771,7 +791,13 @@ static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items,
     }
     const long long want = (n_items + kWarps - 1) / kWarps;
     const int grid = (int)std::max(1LL, std::min<long long>(want, (long long)sm_count * occ_per_sm[dv]));
-    kfn<<<grid, kThreads, smem, st>>>(A);
+    // runs of k items per ticket while a queue holds >= 32 runs per warp
+    PairArgs B = A;
+    const long long warps = (long long)grid * kWarps;
+    B.kchunk = (int)std::max(1LL, std::min<long long>(kChunkMax, n_items / (warps * 32)));
+    B.n_chunked = B.kchunk > 1 ? std::max(0LL, n_items - 2 * warps) : 0;
+    B.t_chunked = (B.n_chunked + B.kchunk - 1) / B.kchunk;
+    kfn<<<grid, kThreads, smem, st>>>(B);
     return cudaGetLastError();
 }
 
@@ -845,7 +871,7 @@ static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
     A.n_jobs = n_jobs;
     A.n_items = n_items;
     A.counter = counter;
-    A.P = P;
+    (void)P;  // partitions travel per job (PairJob::P)
     A.box = box;
     A.bpc = pl.bpc ? 1 : 0;
     A.rule = pl.rule;
@@ -925,7 +951,7 @@ cudaError_t launch_pairs_view(const PairView &home, const PairView &cand, const 
     j.slot = 0;
     j.item_begin = 0;
     j.rule_flags = pl.rule.flags;
-    j.pad = 0;
+    j.P = P;
     j.wunscale = 0.0;
     shape_job(j, n_tiles, n_rows, n_tiles * n_rows, sm_count);
     const long long n_items = (long long)n_tiles * j.n_chunks;
@@ -998,7 +1024,7 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     job.slot = 0;
     job.item_begin = 0;
     job.rule_flags = pl.rule.flags;
-    job.pad = 0;
+    job.P = plan.P;
     job.wunscale = pl.wunscale;
     const size_t roff = (plan.rows.size() * sizeof(RowDesc) + 255) & ~(size_t)255;
     char *hjob = static_cast<char *>(sl->h_pinned) + roff;

@@ -179,8 +179,9 @@ struct pcf_grid {
     unsigned long long wqmax = 0;
     DevBuf raw;                   // float4 x n, input order
     int user_P = 0;               // partitions fixed by the caller at build (0: automatic)
-    std::unique_ptr<CellGrid> cells;                    // the current cell structure
-    std::vector<std::unique_ptr<CellGrid>> cell_cache;  // earlier ones, most recent last
+    // cell structures are shared: a captured batch graph keeps the ones it reads alive
+    std::shared_ptr<CellGrid> cells;                    // the current cell structure
+    std::vector<std::shared_ptr<CellGrid>> cell_cache;  // earlier ones, most recent last
 };
 constexpr int kCellCache = 2;  // cell structures kept besides the current one
 
@@ -295,7 +296,7 @@ struct PairJob {
     int n_rows, rows_per_item, n_chunks, slot;
     long long item_begin;
     unsigned rule_flags;  // exact-rule flags of this histogram (XX and XY differ)
-    int pad;
+    int P;                // cells per side of both grids of this job
     double wunscale;      // fixed-point launches: weight_unscale(home, cand)
 };
 PairView pair_view(const CellGrid &g, bool with_q);
