@@ -37,6 +37,7 @@ constexpr int kTWarps = kTThreads / 32;
 constexpr float kMagic = 256.0f;
 constexpr int kFracBits = 15;
 constexpr unsigned kFracMask = (1u << kFracBits) - 1u;
+constexpr unsigned kBinBias = 0x43800000u >> kFracBits;  // bits(256 + r) >> 15 = this + floor(r)
 
 struct TripCuts {
     float dsf, ds2;
@@ -225,7 +226,8 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
     const int bins = A.rXX.bins;
     const int nb3 = bins * bins * bins;
     unsigned *U = reinterpret_cast<unsigned *>(smem);
-    const size_t u_bytes = A.hist_in_smem ? (((size_t)nb3 * 4 + 15) & ~(size_t)15) : 0;
+    // histogram + 32 dummy slots (see the unit-weight pass 2)
+    const size_t u_bytes = A.hist_in_smem ? (((size_t)(nb3 + 32) * 4 + 15) & ~(size_t)15) : 0;
     float4 *sJ = reinterpret_cast<float4 *>(smem + u_bytes);
     float4 *sK = sJ + A.capJ;
     float *swJ = reinterpret_cast<float *>(sK + (MIXED ? A.capK : 0));
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
     __shared__ int s_anchor, s_nJ, s_nK;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (A.hist_in_smem)
-        for (int k = tid; k < nb3; k += kTThreads) U[k] = 0u;
+        for (int k = tid; k < nb3 + 32; k += kTThreads) U[k] = 0u;
     unsigned n_rechk = 0;
     unsigned long long n_tri = 0;
     __syncthreads();
@@ -289,6 +291,96 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
         }
         // pass 2: pairs of neighbours.  Rows j are dealt to warps in the
         // order 0, n-1, 1, n-2, ... (XXX rows shrink with j).
+        if (!WEIGHTED && A.hist_in_smem) {
+            // Unit weights, shared histogram: two k per lane per step in packed
+            // FP32, unpredicated shared reductions (a lane without a triangle
+            // adds 0 to its dummy slot past the histogram), one recheck vote
+            // per group of steps.
+            const PairRule &r3 = MIXED ? A.rXY : A.rXX;
+            const unsigned Us = (unsigned)__cvta_generic_to_shared(U);
+            const unsigned dummy = Us + (unsigned)(nb3 + lane) * 4u;
+            const float lo = A.fc.lo, hi = A.fc.hi;
+            const unsigned w2 = 2u * A.fc.w;
+            const float mgw = kMagic + (float)A.fc.w * 0x1p-15f;
+            const float2 DS2 = make_float2(A.fc.ds2, A.fc.ds2);
+            for (int rr = warp; rr < nJ; rr += kTWarps) {
+                const int half = rr >> 1;
+                const int jj = MIXED ? rr : ((rr & 1) ? nJ - 1 - half : half);
+                const float4 ej = LJ[jj];
+                const int bj = __float_as_int(ej.w) & 255;
+                const int jidx = (int)((unsigned)__float_as_int(ej.w) >> 8);
+                // slot = bj*bins^2 + b_jk*bins + b_k, with bits(r+256..) >> 15 = kBinBias + b_jk
+                const unsigned base_j = Us + 4u * (unsigned)(bj * bins * bins - (int)kBinBias * bins);
+                const float2 NJX = make_float2(-ej.x, -ej.x), NJY = make_float2(-ej.y, -ej.y),
+                             NJZ = make_float2(-ej.z, -ej.z);
+                struct Ev {
+                    unsigned a0, a1;
+                    bool f0, f1, r0, r1;
+                };
+                // k0 and (if v1) k0 + 32
+                auto eval = [&](int k0, bool v1) -> Ev {
+                    const float4 e0 = LK[k0];
+                    const float4 e1 = LK[v1 ? k0 + 32 : k0];
+                    const float2 DX = __fadd2_rn(make_float2(e0.x, e1.x), NJX);
+                    const float2 DY = __fadd2_rn(make_float2(e0.y, e1.y), NJY);
+                    const float2 DZ = __fadd2_rn(make_float2(e0.z, e1.z), NJZ);
+                    float2 D2 = __fmul2_rn(DX, DX);
+                    D2 = __ffma2_rn(DY, DY, D2);
+                    D2 = __ffma2_rn(DZ, DZ, D2);
+                    const float2 UU = __fmul2_rn(D2, DS2);
+                    const float2 Q = __fadd2_rn(make_float2(sqrt_approx(UU.x), sqrt_approx(UU.y)),
+                                                make_float2(mgw, mgw));
+                    const unsigned u0 = __float_as_uint(Q.x), u1 = __float_as_uint(Q.y);
+                    Ev e;
+                    e.f0 = (D2.x < lo) && (u0 & kFracMask) >= w2;
+                    e.f1 = v1 && (D2.y < lo) && (u1 & kFracMask) >= w2;
+                    e.r0 = !e.f0 && D2.x < hi;
+                    e.r1 = v1 && !e.f1 && D2.y < hi;
+                    e.a0 = base_j + 4u * ((u0 >> kFracBits) * (unsigned)bins + (unsigned)(__float_as_int(e0.w) & 255));
+                    e.a1 = base_j + 4u * ((u1 >> kFracBits) * (unsigned)bins + (unsigned)(__float_as_int(e1.w) & 255));
+                    return e;
+                };
+                auto core = [&](int k0, bool v1) -> bool {
+                    const Ev e = eval(k0, v1);
+                    asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(e.f0 ? e.a0 : dummy), "r"((unsigned)e.f0));
+                    asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(e.f1 ? e.a1 : dummy), "r"((unsigned)e.f1));
+                    n_tri += (unsigned)e.f0 + (unsigned)e.f1;
+                    return e.r0 || e.r1;
+                };
+                // third side by the canonical FP64 rule
+                auto slow = [&](int kk) {
+                    ++n_rechk;
+                    const float4 ek = LK[kk];
+                    const int kidx = (int)((unsigned)__float_as_int(ek.w) >> 8);
+                    const Cat &CK = MIXED ? A.Y : A.X;
+                    const int bjk = exact_third(hx, hy, hz, A.X.x[jidx], A.X.y[jidx], A.X.z[jidx],
+                                                CK.x[kidx], CK.y[kidx], CK.z[kidx], A.bpc, A.box, r3);
+                    if (bjk >= 0) {
+                        atomicAdd(U + bj * bins * bins + bjk * bins + (__float_as_int(ek.w) & 255), 1u);
+                        ++n_tri;
+                    }
+                };
+                auto settle = [&](bool any, int k0, int nsteps, bool v1) {
+                    if (__any_sync(__activemask(), any)) {
+                        for (int q = 0; q < nsteps; ++q) {
+                            const Ev e = eval(k0 + 64 * q, v1);
+                            if (e.r0) slow(k0 + 64 * q);
+                            if (e.r1) slow(k0 + 64 * q + 32);
+                        }
+                    }
+                };
+                int kk = (MIXED ? 0 : jj + 1) + lane;
+                constexpr int G = 4;
+                for (; kk + 64 * (G - 1) + 32 < nK; kk += 64 * G) {
+                    bool any = false;
+                    #pragma unroll
+                    for (int q = 0; q < G; ++q) any |= core(kk + 64 * q, true);
+                    settle(any, kk, G, true);
+                }
+                for (; kk + 32 < nK; kk += 64) settle(core(kk, true), kk, 1, true);
+                if (kk < nK) settle(core(kk, false), kk, 1, false);
+            }
+        } else {
         for (int rr = warp; rr < nJ; rr += kTWarps) {
             const int half = rr >> 1;
             const int jj = MIXED ? rr : ((rr & 1) ? nJ - 1 - half : half);
@@ -324,6 +416,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                     }
                 }
             }
+        }
         }
         __syncthreads();
     }
@@ -515,7 +608,8 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
     }
     const bool weighted = !(X->unit_weights && (!mixed || Y->unit_weights));
     const int n3 = bins * bins * bins;
-    const size_t u_bytes = ((size_t)n3 * 4 + 15) & ~(size_t)15;
+    // histogram + 32 dummy slots (the adds of 0 of lanes without a triangle)
+    const size_t u_bytes = ((size_t)(n3 + 32) * 4 + 15) & ~(size_t)15;
     const size_t smem_max = 227 * 1024 - 64;
     A.hist_in_smem = (!weighted && u_bytes <= 150 * 1024) ? 1 : 0;
     const size_t hist_b = A.hist_in_smem ? u_bytes : 0;
