@@ -100,9 +100,12 @@ void *pcf_ctx_stream(pcf_ctx *ctx);
 /*
  * Grid a catalog.  pts may be host or device memory (n points, 16 bytes
  * each).  Every coordinate must lie in [0, box).  partitions = cells per box
- * side, or 0 to let the library choose; the counting calls re-grid to the
- * cell size their dmax wants, so partitions only sets the initial grid (the
- * reference's -p).  The points are copied; the caller keeps pts.
+ * side (the reference's -p), or 0 to let the library choose.  Pair and
+ * triplet counts use the caller's partitions when periodic stencils allow
+ * them (2*ceil(dmax/cell) + 2 <= partitions), otherwise the count the
+ * library picks for dmax (or the autotuner's, pcf_tune.h); a grid keeps the
+ * cell structures of its last few partition counts.  Results do not depend
+ * on the partitions.  The points are copied; the caller keeps pts.
  */
 pcf_status pcf_grid_build(pcf_ctx *ctx, const pcf_point *pts, int64_t n, float box,
                           int partitions, pcf_grid **out);
@@ -118,7 +121,9 @@ pcf_status pcf_grid_download(pcf_ctx *ctx, const pcf_grid *g, pcf_point *pts_out
  * One pair histogram.  b == NULL: XX (DD or RR) over a, ordered pairs as the
  * reference counts them (each unordered pair twice).  b != NULL: XY (DR),
  * every (a, b) pair once.  kind PCF_ISO: bins doubles; PCF_ANI: bins*bins
- * doubles indexed [bin(|dz|)][bin(r_perp)].  hist is overwritten.
+ * doubles indexed [bin(|dz|)][bin(r_perp)].  hist is overwritten.  stats
+ * may be NULL; when given, the call waits for the result and weighted
+ * histograms also count their in-range pairs (a little extra kernel work).
  */
 pcf_status pcf_count_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a, const pcf_grid *b,
                            int bins, float dmax, uint32_t flags, double *hist,

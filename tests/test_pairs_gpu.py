@@ -143,7 +143,7 @@ def test_grid_is_a_permutation_in_cell_order(ctx):
 def _weighted(pts, rng, kind):
     out = pts.copy()
     n = len(out)
-    if kind == "wide":      # log-uniform over three decades: four-limb fixed point
+    if kind == "wide":      # log-uniform over three decades: no exact integer image, FP64 sums
         out[:, 3] = np.exp(rng.uniform(np.log(0.01), np.log(10.0), n)).astype(np.float32)
     elif kind == "zeros":   # a third of the weights exactly zero
         w = rng.uniform(0.5, 1.5, n).astype(np.float32)
@@ -157,9 +157,9 @@ def _weighted(pts, rng, kind):
 @pytest.mark.parametrize("kind", ["wide", "zeros", "signed"])
 @pytest.mark.parametrize("ani,bins", [(True, 30), (False, 100)])
 def test_weighted_sum_paths(ctx, kind, ani, bins):
-    """Weighted histograms through the fixed-point limb sums (three or four
-    limbs, zero weights) and the FP64 fallback (negative weights), against
-    the FP64 oracle.  The signed case is compared on |oracle| + 1 to keep the
+    """Weighted histograms through the fixed-point limb sums (zero weights)
+    and the FP64 fallback (weights over three decades, negative weights),
+    against the FP64 oracle.  The signed case is compared on |oracle| + 1 to keep the
     relative bound meaningful where positive and negative terms cancel."""
     rng = np.random.default_rng(17)
     box = 200.0
@@ -188,3 +188,43 @@ def test_weighted_dense_cells_flush_budget(ctx):
         want = oracle.pairs(D, None, box=box, bins=30, dmax=20.0, ani=ani)
         _cmp(got, want, True)
         assert st["candidates"] > 64 * 65536
+
+
+def _tune_key(ani, bpc, cross, weighted, bins, n, box, dmax):
+    """The library's tuning-table key of a pair-histogram class (tune.cu)."""
+    import math
+    nbar = n * 4.18879 * dmax ** 3 / box ** 3
+    bucket = int(math.floor(2.0 * math.log2(nbar + 1.0) + 0.5))
+    return (f"{'ani' if ani else 'iso'}{'-bpc' if bpc else ''}{'-xy' if cross else '-xx'}"
+            f"{'-w' if weighted else '-u'}-b{bins}-n{bucket}")
+
+
+@pytest.mark.parametrize("w", ["unit", "uniform"])
+@pytest.mark.parametrize("ani", [False, True])
+def test_every_histogram_scheme(tmp_path, w, ani):
+    """Each shared-memory privatisation scheme (lane-private, per-warp, global,
+    per-warp and lane-private fixed-point limbs), forced through a loaded
+    tuning table, gives the oracle's histogram: bit-exact for unit weights,
+    within 1e-12 for weights."""
+    from desi_b200 import api
+    box, bins, dmax, n = 250.0, 30, 80.0, 2500
+    D = catalog.neyman_scott(n, box, seed=41, weights=w)
+    R = catalog.uniform(n + 77, box, seed=42, weights=w)
+    weighted = w != "unit"
+    want = {cross: oracle.pairs(D, R if cross else None, box=box, bins=bins, dmax=dmax, ani=ani,
+                                bpc=True) for cross in (False, True)}
+    for mode in (0, 1, 2, 3, 4):
+        path = str(tmp_path / f"tune{mode}.txt")
+        with open(path, "w") as f:
+            for cross in (False, True):
+                key = _tune_key(ani, True, cross, weighted, bins, n + 77 if cross else n, box, dmax)
+                f.write(f"{key} 0 {mode} 1.0\n")
+        c = api.Context(0)
+        try:
+            c.tune_load(path)
+            gd, gr = c.grid(D, box), c.grid(R, box)
+            for cross in (False, True):
+                got = c.count_pairs(gd, gr if cross else None, bins=bins, dmax=dmax, ani=ani, bpc=True)
+                _cmp(got.ravel(), want[cross].ravel(), weighted)
+        finally:
+            c.close()
