@@ -131,7 +131,7 @@ def replica_throughput(world: int, units_per_step: float, steps: int, max_total_
     return world * units_per_step * steps / (max_total_ms * 1e-3)
 
 
-def tune_step(ctx, D, R, candidates=(8, 9, 10, 12, 14)):
+def tune_step(ctx, D, R, candidates=(8, 9, 10, 12, 14, 16)):
     """Untimed: the partition count of the step (one for all six histograms,
     so the grids are built once per step) and, per histogram class, the
     privatisation scheme (the library's autotuner).  Returns (P, schemes)."""

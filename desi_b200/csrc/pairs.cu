@@ -647,25 +647,38 @@ __global__ void k_finalize(const unsigned long long *__restrict__ cnt, const dou
 // ---------------------------------------------------------------------------
 // Host planning.
 // ---------------------------------------------------------------------------
+// Home tiles: up to kTileCap consecutive points of one (ix, iy) column,
+// spanning at most two adjacent cells [z0, z1], so a warp's lanes stay busy
+// when cells hold fewer than 32 points.  Two cells keep a periodic stencil
+// within the box: the counts require 2k + 2 <= P for k neighbour cells per
+// side, and a row covers z0 - k .. z1 + k.
 void build_tiles(CellGrid &g) {
     const int P = g.P;
     const std::vector<int> &hs = g.h_start;
     g.tiles.clear();
     for (int ix = 0; ix < P; ++ix)
-        for (int iy = 0; iy < P; ++iy)
-            for (int iz = 0; iz < P; ++iz) {
-                const int c = (ix * P + iy) * P + iz;
-                const int s0 = hs[c], n = hs[c + 1] - s0;
-                for (int o = 0; o < n; o += kTileCap) {
-                    TileDesc t;
-                    t.start = s0 + o;
-                    t.count = std::min(kTileCap, n - o);
-                    t.ix = (int16_t)ix;
-                    t.iy = (int16_t)iy;
-                    t.z0 = t.z1 = (int16_t)iz;
-                    g.tiles.push_back(t);
-                }
+        for (int iy = 0; iy < P; ++iy) {
+            const int col = (ix * P + iy) * P;
+            int iz = 0;
+            int p = hs[col];
+            const int end = hs[col + P];
+            while (p < end) {
+                while (hs[col + iz + 1] <= p) ++iz;  // cell of point p
+                const int limit = hs[col + std::min(iz + 2, P)];
+                const int n = std::min(kTileCap, limit - p);
+                int z1 = iz;
+                while (hs[col + z1 + 1] < p + n) ++z1;  // cell of the tile's last point
+                TileDesc t;
+                t.start = p;
+                t.count = n;
+                t.ix = (int16_t)ix;
+                t.iy = (int16_t)iy;
+                t.z0 = (int16_t)iz;
+                t.z1 = (int16_t)z1;
+                g.tiles.push_back(t);
+                p += n;
             }
+        }
 }
 
 void plan_rows(int P, float box, float dmax, bool ani, bool self, std::vector<RowDesc> &rows) {

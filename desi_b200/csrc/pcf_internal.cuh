@@ -148,7 +148,7 @@ struct CellGrid {
     DevBuf qw;                    // exact integer weights (u32 x (n + kSoaPad)), when wfix_ok
     DevBuf cell_start;            // int x (P^3 + 1)
     std::vector<int> h_start;     // host copy of cell_start
-    std::vector<TileDesc> tiles;  // home tiles: <= 32 points of one cell
+    std::vector<TileDesc> tiles;  // home tiles: <= 32 points of one column, <= 2 cells
     DevBuf d_tiles;
     const float *x() const { return soa.as<float>(); }
     const float *y() const { return soa.as<float>() + plane; }
@@ -251,8 +251,8 @@ struct PairPlan {
 };
 
 constexpr int kTileCap = 32;  // home points per warp item
-// Home tiles of a gridded catalog: each non-empty cell, sliced into runs
-// of at most kTileCap points.
+// Home tiles of a gridded catalog: runs of at most kTileCap consecutive
+// points of one column within two adjacent cells (pairs.cu).
 void build_tiles(CellGrid &g);
 // Stencil rows (dx, dy, kz) of cells that can hold a pair within dmax.
 void plan_rows(int P, float box, float dmax, bool ani, bool self, std::vector<RowDesc> &rows);
