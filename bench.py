@@ -8,9 +8,11 @@ parents x 64 Gaussian children, sigma 5, wrapped) plus 32768 uniform
 randoms in a box of side 250, weights U(0.5, 1.5), 30 bins per axis,
 dmax = 80.  The step grids both catalogs on the device (counting sort) and
 runs the six histograms through the library's C ABI.  Before the timed
-region the bench picks the step's partition count and, per histogram class,
-the histogram privatisation scheme (the library's autotuner); statistics are
-off inside the timed region (no per-call host synchronisation).
+region the bench picks the step's partition count, whether each catalog
+pair's isotropic and anisotropic histograms come from one pass over the
+candidate pairs (kind "both") or two, and per histogram class the
+privatisation scheme (the library's autotuner); statistics are off inside the
+timed region (no per-call host synchronisation).
 
   value  pairs/s with the catalogs already in HBM (unit: one in-range
          unordered XX pair or one XY pair; the reference counts XX pairs
@@ -133,30 +135,36 @@ def replica_throughput(world: int, units_per_step: float, steps: int, max_total_
 
 def tune_step(ctx, D, R, candidates=(8, 9, 10, 12, 14, 16)):
     """Untimed: the partition count of the step (one for all six histograms,
-    so the grids are built once per step) and, per histogram class, the
-    privatisation scheme (the library's autotuner).  Returns (P, schemes)."""
+    so the grids are built once per step), whether the isotropic and
+    anisotropic histograms of a catalog pair come from one pass (kind
+    "both") or two, and per histogram class the privatisation scheme (the
+    library's autotuner).  Returns (P, fused, schemes)."""
     W = WORKLOAD
     best = None
     for P in candidates:
         gd, gr = ctx.grid(D, W["box"], partitions=P), ctx.grid(R, W["box"], partitions=P)
-        tot, modes = 0.0, {}
-        for ani in (False, True):
-            for name, (a, b) in (("DD", (gd, None)), ("RR", (gr, None)), ("DR", (gd, gr))):
-                r = ctx.autotune_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True)
-                tot += r["best_ms"]
-                modes[name + ("ani" if ani else "iso")] = r["hist_mode"]
+        for fused in (False, True):
+            kinds = ("both",) if fused else (False, True)
+            tot, modes = 0.0, {}
+            for ani in kinds:
+                for name, (a, b) in (("DD", (gd, None)), ("RR", (gr, None)), ("DR", (gd, gr))):
+                    r = ctx.autotune_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True)
+                    tot += r["best_ms"]
+                    tag = "both" if ani == "both" else ("ani" if ani else "iso")
+                    modes[name + tag] = r["hist_mode"]
+            if best is None or tot < best[0]:
+                best = (tot, P, fused, modes)
         gd.free()
         gr.free()
-        if best is None or tot < best[0]:
-            best = (tot, P, modes)
     # the tuning table keeps the last candidate's schemes: tune again at the winner
-    gd, gr = ctx.grid(D, W["box"], partitions=best[1]), ctx.grid(R, W["box"], partitions=best[1])
-    for ani in (False, True):
+    _, P, fused, modes = best
+    gd, gr = ctx.grid(D, W["box"], partitions=P), ctx.grid(R, W["box"], partitions=P)
+    for ani in (("both",) if fused else (False, True)):
         for a, b in ((gd, None), (gr, None), (gd, gr)):
             ctx.autotune_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True)
     gd.free()
     gr.free()
-    return best[1], best[2]
+    return P, fused, modes
 
 
 def run_ours(args, rank, world, local_rank):
@@ -169,10 +177,11 @@ def run_ours(args, rank, world, local_rank):
     D, R = catalogs()
     ctx = api.Context(local_rank)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
-    P, tuned = tune_step(ctx, D, R)
+    P, fused, tuned = tune_step(ctx, D, R)
+    kinds = ("both",) if fused else (False, True)
     Dt = torch.from_numpy(D).to(dev)
     Rt = torch.from_numpy(R).to(dev)
-    outs = torch.zeros((6, W["bins"] * W["bins"]), dtype=torch.float64, device=dev)
+    outs = torch.zeros((6, W["bins"] + W["bins"] * W["bins"]), dtype=torch.float64, device=dev)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     # pinned host copies for the end-to-end path
     Dh = torch.from_numpy(D).pin_memory()
@@ -184,7 +193,7 @@ def run_ours(args, rank, world, local_rank):
         gd = ctx.grid(None, W["box"], partitions=P, device_ptr=Dt.data_ptr(), n=len(D))
         gr = ctx.grid(None, W["box"], partitions=P, device_ptr=Rt.data_ptr(), n=len(R))
         k = 0
-        for ani in (False, True):
+        for ani in kinds:
             for a, b in ((gd, None), (gr, None), (gd, gr)):
                 r = ctx.count_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True,
                                     stats=with_stats, out_device_ptr=outs[k].data_ptr())
@@ -198,7 +207,7 @@ def run_ours(args, rank, world, local_rank):
         gd = ctx.grid(Dh.numpy(), W["box"], partitions=P)
         gr = ctx.grid(Rh.numpy(), W["box"], partitions=P)
         hists = []
-        for ani in (False, True):
+        for ani in kinds:
             for a, b in ((gd, None), (gr, None), (gd, gr)):
                 hists.append(ctx.count_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True))
         gd.free()
@@ -287,7 +296,8 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Neyman-Scott data + uniform randoms; no dataset ships with "
                 "the workload)",
-        "config": dict(W, partitions=P, schemes=tuned, parallelism=f"replicas x{world}",
+        "config": dict(W, partitions=P, kinds_in_one_pass=fused, schemes=tuned,
+                       parallelism=f"replicas x{world}",
                        l2="flushed between steps (512 MB write)",
                        pairs_per_step=pairs_step),
         "latency_ms": {"p50": statistics.median(times),

@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpcf.so")
 
-PCF_ISO, PCF_ANI = 0, 1
+PCF_ISO, PCF_ANI, PCF_BOTH = 0, 1, 2
 PCF_BPC = 1 << 0
 PCF_DS_EXACT = 1 << 1
 PCF_RULE_CUSTOM = 1 << 2

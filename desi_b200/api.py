@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import (PCF_ANI, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT, PCF_GRAPH,  # noqa: F401
+from ._lib import (PCF_ANI, PCF_BOTH, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT, PCF_GRAPH,  # noqa: F401
                    PCF_ISO, PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO, PCF_RULE_INCLUSIVE, PcfError,
                    Stats)
 
@@ -89,9 +89,15 @@ class Context:
 
     # -- counting ------------------------------------------------------------
     def count_pairs(self, a: "Grid", b: "Grid | None" = None, *, bins: int, dmax: float,
-                    ani: bool = False, bpc: bool = False, flags: int = 0,
+                    ani: "bool | str" = False, bpc: bool = False, flags: int = 0,
                     stats: bool = False, out_device_ptr: int | None = None):
-        nb = bins * bins if ani else bins
+        """One pair histogram (DD / RR with b None, else DR).  ani=False:
+        isotropic [bins]; True: anisotropic [bins, bins]; "both": the two from
+        one pass, returned as (iso, ani) (a device output then holds bins +
+        bins^2 doubles, isotropic first)."""
+        both = ani == "both"
+        kind = PCF_BOTH if both else (PCF_ANI if ani else PCF_ISO)
+        nb = bins + bins * bins if both else (bins * bins if ani else bins)
         f = flags | (PCF_BPC if bpc else 0)
         st = Stats()
         if out_device_ptr is not None:
@@ -101,11 +107,13 @@ class Context:
         else:
             out = np.zeros(nb, np.float64)
             outp = out.ctypes.data_as(ctypes.c_void_p)
-        rc = self._lib.pcf_count_pairs(self.handle, PCF_ANI if ani else PCF_ISO, a.handle,
+        rc = self._lib.pcf_count_pairs(self.handle, kind, a.handle,
                                        b.handle if b is not None else None, int(bins),
                                        float(dmax), f, outp, ctypes.byref(st) if stats else None)
         _check(self.handle, rc, "pcf_count_pairs")
-        if out is not None and ani:
+        if out is not None and both:
+            out = (out[:bins], out[bins:].reshape(bins, bins))
+        elif out is not None and ani:
             out = out.reshape(bins, bins)
         return (out, st.as_dict()) if stats else out
 
@@ -149,24 +157,33 @@ class Context:
         res = (ddd.reshape(s) if ddd is not None else None, ddr.reshape(s), rrr.reshape(s))
         return (res, st.as_dict()) if stats else res
 
-    def batch_pairs(self, d: "Grid", rands, *, bins: int, dmax: float, ani: bool = False,
+    def batch_pairs(self, d: "Grid", rands, *, bins: int, dmax: float, ani: "bool | str" = False,
                     bpc: bool = False, flags: int = 0, want_dd: bool = True,
                     stats: bool = False, graph: bool = False):
+        """DD, RR_i and DR_i of one data grid against random grids in one
+        launch.  ani as for count_pairs ("both": each result an (iso, ani) pair)."""
         nr = len(rands)
-        nb = bins * bins if ani else bins
+        both = ani == "both"
+        kind = PCF_BOTH if both else (PCF_ANI if ani else PCF_ISO)
+        nb = bins + bins * bins if both else (bins * bins if ani else bins)
         arr = (ctypes.c_void_p * nr)(*[r.handle.value for r in rands])
         dd = np.zeros(nb, np.float64) if want_dd else None
         rr = np.zeros(nr * nb, np.float64)
         dr = np.zeros(nr * nb, np.float64)
         st = Stats()
         f = flags | (PCF_BPC if bpc else 0) | (PCF_GRAPH if graph else 0)
-        rc = self._lib.pcf_batch_pairs(self.handle, PCF_ANI if ani else PCF_ISO, d.handle,
+        rc = self._lib.pcf_batch_pairs(self.handle, kind, d.handle,
                                        ctypes.cast(arr, ctypes.c_void_p), nr, int(bins),
                                        float(dmax), f,
                                        dd.ctypes.data_as(ctypes.c_void_p) if dd is not None else None,
                                        rr.ctypes.data_as(ctypes.c_void_p),
                                        dr.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st))
         _check(self.handle, rc, "pcf_batch_pairs")
+        if both:
+            rr, dr = rr.reshape(nr, nb), dr.reshape(nr, nb)
+            split = lambda h: (h[..., :bins], h[..., bins:].reshape(h.shape[:-1] + (bins, bins)))
+            res = (split(dd) if dd is not None else None, split(rr), split(dr))
+            return (res, st.as_dict()) if stats else res
         shp = (nr, bins, bins) if ani else (nr, bins)
         if dd is not None and ani:
             dd = dd.reshape(bins, bins)
@@ -191,7 +208,8 @@ class Context:
         r = _lib.TuneResult()
         f = flags | (PCF_BPC if bpc else 0)
         _check(self.handle, self._lib.pcf_autotune_pairs(
-            self.handle, PCF_ANI if ani else PCF_ISO, a.handle, b.handle if b is not None else None,
+            self.handle, PCF_BOTH if ani == "both" else (PCF_ANI if ani else PCF_ISO), a.handle,
+            b.handle if b is not None else None,
             int(bins), float(dmax), f, ctypes.byref(r)), "pcf_autotune_pairs")
         return r.as_dict()
 

@@ -39,10 +39,10 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
                                       uint32_t flags, double *dd, double *rr, double *dr,
                                       pcf_stats *stats) {
     if (!ctx || !d_ || bins < 1 || !(dmax > 0.f) || n_rand < 0 || (n_rand > 0 && !r_) ||
-        (kind != PCF_ISO && kind != PCF_ANI) || (!dd && !rr && !dr))
+        (kind != PCF_ISO && kind != PCF_ANI && kind != PCF_BOTH) || (!dd && !rr && !dr))
         return PCF_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0;
+    const bool ani = kind != PCF_ISO, both = kind == PCF_BOTH, bpc = (flags & PCF_BPC) != 0;
     pcf_grid *D = const_cast<pcf_grid *>(d_);
     std::vector<pcf_grid *> R((size_t)n_rand);
     int64_t nmax = D->n;
@@ -82,7 +82,7 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         if ((s = grid_ensure_cells(ctx, j.c, j.P)) != PCF_OK) return s;
         j.cc = j.c->cells;
     }
-    const int nb = ani ? bins * bins : bins;
+    const int nb = both ? bins + bins * bins : ani ? bins * bins : bins;
     bool weighted = !D->unit_weights;
     for (auto *g : R) weighted = weighted || !g->unit_weights;
 
@@ -104,10 +104,11 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     cudaStream_t st = ctx->stream;
     PairLaunch pl;
     pl.ani = ani;
+    pl.both = both;
     pl.bpc = bpc;
     pl.self = false;
     pl.weighted = weighted;
-    pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
+    pl.rule = make_pair_rule(bins, dmax, flags, ani && !both, bpc, false);
     pl.mult = 1.0;
     {
         std::vector<const pcf_grid *> gs(R.begin(), R.end());
@@ -149,7 +150,11 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         std::vector<PairJob> jobs((size_t)nslots);
         std::vector<double> mult((size_t)nslots);
         long long item = 0;
-        const unsigned rXX = reference_pair_rule(ani, bpc, false), rXY = reference_pair_rule(ani, bpc, true);
+        // exact-rule flags per job: rule_flags for the first (or only) kind,
+        // rule_flags2 for the anisotropic histogram of a both-kinds launch
+        const bool first_ani = ani && !both;
+        const unsigned rXX = reference_pair_rule(first_ani, bpc, false), rXY = reference_pair_rule(first_ani, bpc, true);
+        const unsigned aXX = reference_pair_rule(true, bpc, false), aXY = reference_pair_rule(true, bpc, true);
         for (int k = 0; k < nslots; ++k) {
             const CellGrid &h = *js[k].hc, &c = *js[k].cc;
             const auto &rp = rows[js[k].P];
@@ -163,10 +168,11 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
                       total, ctx->sm_count);
             j.slot = k;
             j.item_begin = item;
-            j.rule_flags = (flags & PCF_RULE_CUSTOM)
-                               ? (((flags & PCF_RULE_EXCL_ZERO) ? PCF_RULE_EXCL : 0u) |
-                                  ((flags & PCF_RULE_INCLUSIVE) ? PCF_RULE_LE : 0u))
-                               : (js[k].self ? rXX : rXY);
+            const unsigned custom = ((flags & PCF_RULE_EXCL_ZERO) ? PCF_RULE_EXCL : 0u) |
+                                    ((flags & PCF_RULE_INCLUSIVE) ? PCF_RULE_LE : 0u);
+            j.rule_flags = (flags & PCF_RULE_CUSTOM) ? custom : (js[k].self ? rXX : rXY);
+            j.rule_flags2 = (flags & PCF_RULE_CUSTOM) ? custom : (js[k].self ? aXX : aXY);
+            j.pad = 0;
             j.P = js[k].P;
             item += (long long)h.tiles.size() * j.n_chunks;
             mult[k] = js[k].mult;

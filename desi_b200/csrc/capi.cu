@@ -267,13 +267,16 @@ static pcf_status hist_scratch(pcf_ctx *ctx, int nb, unsigned long long **cnt, d
 static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, const pcf_grid *b_,
                                    int bins, float dmax, uint32_t flags, double *hist,
                                    pcf_stats *stats, double ds_override) {
-    if (!ctx || !a_ || !hist || bins < 1 || !(dmax > 0.f) || (kind != PCF_ISO && kind != PCF_ANI))
+    if (!ctx || !a_ || !hist || bins < 1 || !(dmax > 0.f) ||
+        (kind != PCF_ISO && kind != PCF_ANI && kind != PCF_BOTH))
         return PCF_ERR_INVALID_ARG;
-    if (kind == PCF_ANI && (int64_t)bins * bins > (1 << 24)) return PCF_ERR_UNSUPPORTED;
+    if (kind != PCF_ISO && (int64_t)bins * bins > (1 << 24)) return PCF_ERR_UNSUPPORTED;
+    if (kind == PCF_BOTH && ds_override > 0) return PCF_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     pcf_grid *a = const_cast<pcf_grid *>(a_);
     pcf_grid *b = const_cast<pcf_grid *>(b_);
-    const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0, cross = b != nullptr;
+    const bool ani = kind != PCF_ISO, both = kind == PCF_BOTH;
+    const bool bpc = (flags & PCF_BPC) != 0, cross = b != nullptr;
     const bool weighted = !(a->unit_weights && (!cross || b->unit_weights));
     TuneEntry te;
     if (ctx->tune_override.refine > 0 || ctx->tune_override.hist_mode >= 0) {
@@ -288,18 +291,20 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     if (s != PCF_OK) return s;
     PairPlan plan;
     plan_pairs(*a->cells, a->box, dmax, ani, !cross, plan, ctx->sm_count * 24);
-    const int nb = ani ? bins * bins : bins;
+    const int nb = both ? bins + bins * bins : ani ? bins * bins : bins;
     unsigned long long *d_cnt, *d_stats;
     double *d_ws, *d_out;
     s = hist_scratch(ctx, nb, &d_cnt, &d_ws, &d_stats, &d_out);
     if (s != PCF_OK) return s;
     PairLaunch pl;
     pl.ani = ani;
+    pl.both = both;
     pl.bpc = bpc;
     pl.self = !cross;
     pl.weighted = weighted;
     pl.hist_mode = te.hist_mode;
-    pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, cross);
+    pl.rule = make_pair_rule(bins, dmax, flags, ani && !both, bpc, cross);
+    if (both) pl.flags2 = make_pair_rule(bins, dmax, flags, true, bpc, cross).flags;
     if (ds_override > 0) pl.rule.ds = ds_override;
     pl.mult = cross ? 1.0 : 2.0;
     {

@@ -192,12 +192,12 @@ __host__ __device__ __forceinline__ int copy_words(int nb) {
          : HM == H_LFIX ? nb * kLimbs * 32 : 0;
 }
 
-// Adds this warp's copy into histogram `slot` of the launch and clears it.
+// Adds this warp's copy (nb bins) into the launch's accumulators at `off`
+// and clears it.
 template <bool WEIGHTED, int HM>
-__device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, int slot, double unscale) {
+__device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, size_t off, double unscale) {
     if (HM == H_GLOBAL) return;
     __syncwarp();
-    const size_t off = (size_t)slot * nb;
     if (HM == H_LANE && !WEIGHTED) {
         unsigned *mine = static_cast<unsigned *>(mine_v);
         for (int k = 0; k < nb; ++k) {
@@ -256,10 +256,47 @@ __device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, in
 #ifndef PCF_PAIR_MINB
 #define PCF_PAIR_MINB 6
 #endif
-template <int HM>
-struct MinBlocks {  // CTAs per SM the shared-memory footprint allows at 30 / 900 bins
-    static constexpr int value = HM == H_LFIX ? 4 : HM == H_WFIX ? 5 : PCF_PAIR_MINB;
+// CTAs per SM the shared-memory footprint allows at 30 / 900 bins (the
+// register cap of the launch bounds follows from it)
+template <int KIND, int HM>
+struct MinBlocks {
+    static constexpr int value = KIND == 2 ? (HM == H_WFIX ? 4 : 5)
+                               : HM == H_LFIX ? 4 : HM == H_WFIX ? 5 : PCF_PAIR_MINB;
 };
+
+// Kinds of one launch: the isotropic histogram, the anisotropic one, or both
+// from one pass over the candidates (the anisotropic stencil covers the
+// isotropic one).
+enum { K_ISO = 0, K_ANI = 1, K_BOTH = 2 };
+// Scheme of the isotropic copy of a K_BOTH launch, given the anisotropic one:
+// lane-private counts, else per-warp copies of the same element type.
+template <bool WEIGHTED, int HM>
+struct IsoScheme {
+    static constexpr int value = HM == H_WARP ? (WEIGHTED ? H_WARP : H_LANE) : HM;
+};
+
+// Sets up one lane's sink over a copy at shared address ms (see Sink).
+template <bool WEIGHTED, int HM>
+__device__ __forceinline__ void setup_sink(Sink<WEIGHTED, HM> &sk, unsigned ms, void *mine, int lane,
+                                           unsigned bias, int nb) {
+    typedef typename std::conditional<WEIGHTED && !(HM == H_WFIX || HM == H_LFIX), double, unsigned>::type HT;
+    sk.bias = bias;
+    sk.lane_col = reinterpret_cast<double *>(mine) + lane;
+    sk.gbase = nullptr;
+    switch (HM) {  // dummy: bin 0 of a lane-private column, else slot nb + lane
+    case H_LANE: sk.base = ms + lane * 4u - bias * 128u; sk.dummy = ms + lane * 4u; break;
+    case H_WARP:
+        sk.base = ms - bias * (unsigned)sizeof(HT);
+        sk.dummy = ms + (unsigned)(nb + lane) * (unsigned)sizeof(HT);
+        break;
+    case H_WFIX:
+        sk.base = ms - bias * (kLimbs * 4u);
+        sk.dummy = ms + (unsigned)(nb + lane) * (kLimbs * 4u);
+        break;
+    case H_LFIX: sk.base = ms + lane * 4u - bias * (kLimbs * 128u); sk.dummy = ms + lane * 4u; break;
+    default: sk.base = sk.dummy = 0u;
+    }
+}
 
 // Candidate ranges of one stencil row for the current home tile: [a0, b0)
 // unshifted in z, [a1, b1) image-shifted by sz1 (periodic wrap in z); the
@@ -282,9 +319,12 @@ struct WarpState {
 };
 
 // COUNT: also count the in-range pairs (weighted histograms, statistics on).
-template <bool ANI, bool WEIGHTED, int HM, bool COUNT>
-__global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const PairArgs A) {
+// HM is the scheme of the anisotropic copy for K_ANI / K_BOTH launches.
+template <int KIND, bool WEIGHTED, int HM, bool COUNT>
+__global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(const PairArgs A) {
     constexpr bool FIX = HM == H_WFIX || HM == H_LFIX;
+    constexpr bool DO_I = KIND != K_ANI, DO_A = KIND != K_ISO;
+    constexpr int HMI = KIND == K_BOTH ? IsoScheme<WEIGHTED, HM>::value : HM;
     typedef typename WT<WEIGHTED, HM>::type W;
     typedef typename std::conditional<WEIGHTED && !FIX, double, unsigned>::type HT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -293,31 +333,23 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
     WarpState &ws = s_ws[warp];
     PairJob &J = ws.job;
     const int bins = A.rule.bins;
-    const int nb = ANI ? bins * bins : bins;
-    const int per_warp = copy_words<HM>(nb);
-    HT *mine = reinterpret_cast<HT *>(smem_raw) + warp * per_warp;
-    for (int k = lane; k < per_warp; k += 32) mine[k] = (HT)0;
-    const unsigned bias = ANI ? kBinBias * (unsigned)(bins + 1) : kBinBias;
-    Sink<WEIGHTED, HM> sink;
-    {
-        const unsigned ms = (unsigned)__cvta_generic_to_shared(mine);
-        sink.bias = bias;
-        sink.lane_col = reinterpret_cast<double *>(mine) + lane;
-        sink.gbase = nullptr;
-        switch (HM) {  // dummy: bin 0 of a lane-private column, else slot nb + lane
-        case H_LANE: sink.base = ms + lane * 4u - bias * 128u; sink.dummy = ms + lane * 4u; break;
-        case H_WARP:
-            sink.base = ms - bias * (unsigned)sizeof(HT);
-            sink.dummy = ms + (unsigned)(nb + lane) * (unsigned)sizeof(HT);
-            break;
-        case H_WFIX:
-            sink.base = ms - bias * (kLimbs * 4u);
-            sink.dummy = ms + (unsigned)(nb + lane) * (kLimbs * 4u);
-            break;
-        case H_LFIX: sink.base = ms + lane * 4u - bias * (kLimbs * 128u); sink.dummy = ms + lane * 4u; break;
-        default: sink.base = sink.dummy = 0u;
-        }
-    }
+    const int nbi = bins, nba = bins * bins;
+    const int nbt = (DO_I ? nbi : 0) + (DO_A ? nba : 0);  // accumulators per job slot
+    const int wi = DO_I ? copy_words<HMI>(nbi) : 0, wa = DO_A ? copy_words<HM>(nba) : 0;
+    HT *mine_i = reinterpret_cast<HT *>(smem_raw) + warp * (wi + wa);
+    HT *mine_a = mine_i + wi;
+    for (int k = lane; k < wi + wa; k += 32) mine_i[k] = (HT)0;
+    const unsigned bias_i = kBinBias, bias_a = kBinBias * (unsigned)(bins + 1);
+    Sink<WEIGHTED, HMI> sink_i;
+    Sink<WEIGHTED, HM> sink_a;
+    if (DO_I) setup_sink<WEIGHTED, HMI>(sink_i, (unsigned)__cvta_generic_to_shared(mine_i), mine_i, lane, bias_i, nbi);
+    if (DO_A) setup_sink<WEIGHTED, HM>(sink_a, (unsigned)__cvta_generic_to_shared(mine_a), mine_a, lane, bias_a, nba);
+    // flushes both copies of this warp into job slot `slot`
+    auto flush = [&](int slot, double unscale) {
+        const size_t off = (size_t)slot * nbt;
+        if (DO_I) flush_copy<WEIGHTED, HMI>(mine_i, nbi, lane, A, off, unscale);
+        if (DO_A) flush_copy<WEIGHTED, HM>(mine_a, nba, lane, A, off + (DO_I ? nbi : 0), unscale);
+    };
     if (lane == 0) {
         ws.n_cand = 0;
         ws.job_end = -1;
@@ -351,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
       if (lane == 0) tk = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next ticket
       for (long long it_idx = ib; it_idx < ie; ++it_idx) {
         if (it_idx >= ws.job_end) {  // entering another job: flush this one's histogram
-            if (ws.cj >= 0) flush_copy<WEIGHTED, HM>(mine, nb, lane, A, ws.slot, J.wunscale);
+            if (ws.cj >= 0) flush(ws.slot, J.wunscale);
             since = 0;
             int cj = ws.cj;
             long long job_end;
@@ -371,8 +403,11 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
             __syncwarp();
             if (lane == 0) ws.slot = J.slot;
             if (HM == H_GLOBAL) {
-                sink.gbase = WEIGHTED ? (void *)(A.g_wsum + (size_t)J.slot * nb)
-                                      : (void *)(A.g_count + (size_t)J.slot * nb);
+                const size_t off = (size_t)J.slot * nbt;
+                void *g = WEIGHTED ? (void *)(A.g_wsum + off) : (void *)(A.g_count + off);
+                sink_i.gbase = g;
+                sink_a.gbase = WEIGHTED ? (void *)(A.g_wsum + off + (DO_I ? nbi : 0))
+                                        : (void *)(A.g_count + off + (DO_I ? nbi : 0));
             }
             __syncwarp();
         }
@@ -462,31 +497,44 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
                 if (lane == 0) ws.n_cand += (unsigned long long)(b - a) * (unsigned long long)H;
 
                 // Rare path: the canonical rule for candidate j (reloads what
-                // the fast path does not keep in registers).
-                auto slow = [&](int j) {
-                    PairRule rule = A.rule;
-                    rule.flags = J.rule_flags;
+                // the fast path does not keep in registers), for the kinds
+                // whose fast path did not take it.
+                auto slow = [&](int j, bool do_i, bool do_a) {
                     const RowRange &rq = ws.rows[r];
                     const float4 hh = ws.home[lane];
                     float cx, cy, cz, cw;
                     load_point(cpk, j, cx, cy, cz, cw);
-                    const int s = slow_slot<ANI>(hh.x, hh.y, hh.z, cx, cy, cz, rq.sx, rq.sy,
-                                                 seg ? rq.sz1 : 0.f, rule);
-                    if (s >= 0) {
-                        W wj;
-                        if (FIX) wj = (W)__ldg(cqw + j);
-                        else wj = (W)cw;
-                        sink.add((unsigned)s + bias, hw, wj, true);
-                        if (COUNT) ++n_pairs;
+                    W wj;
+                    if (FIX) wj = (W)__ldg(cqw + j);
+                    else wj = (W)cw;
+                    PairRule rule = A.rule;
+                    if (DO_I && do_i) {
+                        rule.flags = J.rule_flags;
+                        const int s = slow_slot<false>(hh.x, hh.y, hh.z, cx, cy, cz, rq.sx, rq.sy,
+                                                       seg ? rq.sz1 : 0.f, rule);
+                        if (s >= 0) {
+                            sink_i.add((unsigned)s + bias_i, hw, wj, true);
+                            if (COUNT) ++n_pairs;
+                        }
+                    }
+                    if (DO_A && do_a) {
+                        rule.flags = KIND == K_BOTH ? J.rule_flags2 : J.rule_flags;
+                        const int s = slow_slot<true>(hh.x, hh.y, hh.z, cx, cy, cz, rq.sx, rq.sy,
+                                                      seg ? rq.sz1 : 0.f, rule);
+                        if (s >= 0) {
+                            sink_a.add((unsigned)s + bias_a, hw, wj, true);
+                            if (COUNT) ++n_pairs;
+                        }
                     }
                 };
                 // One aligned pair of candidates (p, p+1); v0 / v1 say which are
-                // real.  Pure arithmetic: the histogram slots (biased), which
-                // pairs the fast path takes (f) and which need the FP64 rule (r).
+                // real.  Pure arithmetic: per kind the histogram slots (biased),
+                // which pairs the fast path takes (f) and which need the FP64
+                // rule (r).
                 struct Eval {
-                    unsigned sb0, sb1;
+                    unsigned si0, si1, sa0, sa1;
                     W w0, w1;
-                    bool f0, f1, r0, r1;
+                    bool fi0, fi1, fa0, fa1, ri0, ri1, ra0, ra1;
                 };
                 auto eval = [&](int p, bool v0, bool v1) -> Eval {
                     Eval e;
@@ -503,27 +551,27 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
                     const float2 DX = __fadd2_rn(make_float2(qa.x, qa.y), NHX);
                     const float2 DY = __fadd2_rn(make_float2(qa.z, qa.w), NHY);
                     const float2 DZ = __fadd2_rn(make_float2(qb.x, qb.y), NHZ);
-                    float m0, m1;  // the squared separation the dmax test reads
-                    if (!ANI) {
-                        float2 D2 = __fmul2_rn(DX, DX);
-                        D2 = __ffma2_rn(DY, DY, D2);
-                        D2 = __ffma2_rn(DZ, DZ, D2);
-                        m0 = D2.x;
-                        m1 = D2.y;
+                    const float2 PP = __ffma2_rn(DY, DY, __fmul2_rn(DX, DX));
+                    e.si0 = e.si1 = e.sa0 = e.sa1 = 0u;
+                    e.fi0 = e.fi1 = e.fa0 = e.fa1 = e.ri0 = e.ri1 = e.ra0 = e.ra1 = false;
+                    if (DO_I) {  // d2 = (dx^2 + dy^2) + dz^2 with fused adds
+                        const float2 D2 = __ffma2_rn(DZ, DZ, PP);
                         const float2 U = __fmul2_rn(D2, make_float2(fc.ds2, fc.ds2));
                         const float2 Q = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)),
                                                     make_float2(mgw, mgw));
                         const unsigned u0 = __float_as_uint(Q.x), u1 = __float_as_uint(Q.y);
-                        // f0 / f1 imply r < bins away from an edge: the slot is in range
-                        e.f0 = v0 && (m0 < lo) && fix_safe(u0, w2);
-                        e.f1 = v1 && (m1 < lo) && fix_safe(u1, w2);
-                        e.sb0 = u0 >> kFracBits;
-                        e.sb1 = u1 >> kFracBits;
-                    } else {
+                        // f implies r < bins away from an edge: the slot is in range
+                        e.fi0 = v0 && (D2.x < lo) && fix_safe(u0, w2);
+                        e.fi1 = v1 && (D2.y < lo) && fix_safe(u1, w2);
+                        if (HM == H_GLOBAL) { e.fi0 = e.fi0 && A.fast; e.fi1 = e.fi1 && A.fast; }
+                        e.si0 = u0 >> kFracBits;
+                        e.si1 = u1 >> kFracBits;
+                        e.ri0 = v0 && !e.fi0 && D2.x < hi;
+                        e.ri1 = v1 && !e.fi1 && D2.y < hi;
+                    }
+                    if (DO_A) {
                         const float2 ZZ = __fmul2_rn(DZ, DZ);
-                        const float2 PP = __ffma2_rn(DY, DY, __fmul2_rn(DX, DX));
-                        m0 = fmaxf(ZZ.x, PP.x);
-                        m1 = fmaxf(ZZ.y, PP.y);
+                        const float m0 = fmaxf(ZZ.x, PP.x), m1 = fmaxf(ZZ.y, PP.y);
                         const float2 RZ = __fmul2_rn(DZ, make_float2(fc.dsf, fc.dsf));
                         const float2 U = __fmul2_rn(PP, make_float2(fc.ds2, fc.ds2));
                         const unsigned z0 = __float_as_uint(fabsf(RZ.x) + mgw);
@@ -531,24 +579,31 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
                         const float2 QP = __fadd2_rn(make_float2(sqrt_approx(U.x), sqrt_approx(U.y)),
                                                      make_float2(mgw, mgw));
                         const unsigned p0 = __float_as_uint(QP.x), p1 = __float_as_uint(QP.y);
-                        e.f0 = v0 && (m0 < lo) && fix_safe(z0, w2) && fix_safe(p0, w2);
-                        e.f1 = v1 && (m1 < lo) && fix_safe(z1, w2) && fix_safe(p1, w2);
+                        e.fa0 = v0 && (m0 < lo) && fix_safe(z0, w2) && fix_safe(p0, w2);
+                        e.fa1 = v1 && (m1 < lo) && fix_safe(z1, w2) && fix_safe(p1, w2);
+                        if (HM == H_GLOBAL) { e.fa0 = e.fa0 && A.fast; e.fa1 = e.fa1 && A.fast; }
                         const unsigned B = (unsigned)bins;
-                        e.sb0 = (z0 >> kFracBits) * B + (p0 >> kFracBits);
-                        e.sb1 = (z1 >> kFracBits) * B + (p1 >> kFracBits);
+                        e.sa0 = (z0 >> kFracBits) * B + (p0 >> kFracBits);
+                        e.sa1 = (z1 >> kFracBits) * B + (p1 >> kFracBits);
+                        e.ra0 = v0 && !e.fa0 && m0 < hi;
+                        e.ra1 = v1 && !e.fa1 && m1 < hi;
                     }
-                    if (HM == H_GLOBAL) { e.f0 = e.f0 && A.fast; e.f1 = e.f1 && A.fast; }
-                    e.r0 = v0 && !e.f0 && m0 < hi;
-                    e.r1 = v1 && !e.f1 && m1 < hi;
                     return e;
                 };
-                // Accumulates the fast-path pairs; true if either needs the FP64 rule.
+                // Accumulates the fast-path pairs; true if any needs the FP64 rule.
                 auto core = [&](int p, bool v0, bool v1) -> bool {
                     const Eval e = eval(p, v0, v1);
-                    sink.add(e.sb0, hw, e.w0, e.f0);
-                    sink.add(e.sb1, hw, e.w1, e.f1);
-                    if (COUNT) n_pairs += (unsigned)e.f0 + (unsigned)e.f1;
-                    return e.r0 || e.r1;
+                    if (DO_I) {
+                        sink_i.add(e.si0, hw, e.w0, e.fi0);
+                        sink_i.add(e.si1, hw, e.w1, e.fi1);
+                        if (COUNT) n_pairs += (unsigned)e.fi0 + (unsigned)e.fi1;
+                    }
+                    if (DO_A) {
+                        sink_a.add(e.sa0, hw, e.w0, e.fa0);
+                        sink_a.add(e.sa1, hw, e.w1, e.fa1);
+                        if (COUNT) n_pairs += (unsigned)e.fa0 + (unsigned)e.fa1;
+                    }
+                    return e.ri0 || e.ri1 || e.ra0 || e.ra1;
                 };
                 // Rechecks of `n` steps from p: the vote is rare, so the
                 // candidates are re-evaluated to find which need the FP64 rule.
@@ -558,8 +613,8 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
                     if (__any_sync(__activemask(), any)) {
                         for (int k = 0; k < n; ++k) {
                             const Eval e = eval(p + k * stride, v0, v1);
-                            if (e.r0) { ++n_rechk; slow(p + k * stride); }
-                            if (e.r1) { ++n_rechk; slow(p + k * stride + 1); }
+                            if (e.ri0 || e.ra0) { ++n_rechk; slow(p + k * stride, e.ri0, e.ra0); }
+                            if (e.ri1 || e.ra1) { ++n_rechk; slow(p + k * stride + 1, e.ri1, e.ra1); }
                         }
                     }
                 };
@@ -593,7 +648,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
                         const int c = hi_i - lo_i;
                         const int adds = (HM == H_LANE || HM == H_LFIX) ? c / S + 2 : c * H;
                         if (since + adds > A.budget) {
-                            flush_copy<WEIGHTED, HM>(mine, nb, lane, A, ws.slot, J.wunscale);
+                            flush(ws.slot, J.wunscale);
                             since = 0;
                         }
                         since += adds;
@@ -609,7 +664,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<HM>::value) k_pairs(const 
     }
     // per-warp flush (no CTA barrier: warps leave as the queue drains)
     __syncwarp();
-    if (ws.cj >= 0) flush_copy<WEIGHTED, HM>(mine, nb, lane, A, ws.slot, J.wunscale);
+    if (ws.cj >= 0) flush(ws.slot, J.wunscale);
     unsigned long long rp = n_pairs, rr = n_rechk;
     for (int off = 16; off > 0; off >>= 1) {
         rr += __shfl_down_sync(kFull, rr, off);
@@ -772,10 +827,10 @@ static int copy_words_host(int hm, int nb) {
     return 0;
 }
 
-template <bool ANI, bool W, int HM, bool C = false>
+template <int KIND, bool W, int HM, bool C>
 static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items, cudaStream_t st,
                               int sm_count, int device) {
-    auto kfn = k_pairs<ANI, W, HM, C>;
+    auto kfn = k_pairs<KIND, W, HM, C>;
     // attribute / occupancy queries cost microseconds each: do them once per
     // (device, variant, shared-memory size)
     constexpr int kDev = 64;
@@ -814,17 +869,22 @@ static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items,
     return cudaGetLastError();
 }
 
-// Chooses the histogram mode of one launch and starts the kernel.
+// Chooses the histogram mode of one launch and starts the kernel.  For a
+// both-kinds launch the mode is the anisotropic copy's; the isotropic copy
+// takes the matching scheme (IsoScheme).
 static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t st,
                                   int sm_count, int device) {
-    const int nb = pl.ani ? pl.rule.bins * pl.rule.bins : pl.rule.bins;
+    const int bins = pl.rule.bins;
+    const int nb = pl.ani ? bins * bins : bins;
     const size_t ebytes = pl.weighted ? 8 : 4;
     auto bytes = [&](int hm) -> size_t {
         const size_t e = (hm == H_WFIX || hm == H_LFIX) ? 4 : ebytes;
-        return (size_t)copy_words_host(hm, nb) * e * kWarps;
+        size_t w = (size_t)copy_words_host(hm, nb);
+        if (pl.both) w += (size_t)copy_words_host(hm == H_WARP && !pl.weighted ? H_LANE : hm, bins);
+        return w * e * kWarps;
     };
     auto fits = [&](int hm) -> bool {
-        if (pl.rule.bins > 255) return hm == H_GLOBAL;
+        if (bins > 255) return hm == H_GLOBAL;
         switch (hm) {
         case H_LANE: return !pl.ani && bytes(hm) <= 64 * 1024;
         case H_LFIX: return !pl.ani && pl.weighted && pl.wfix && bytes(hm) <= 64 * 1024;
@@ -835,7 +895,7 @@ static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t
         return false;
     };
     int hm;
-    if (pl.rule.bins > 255 || !fits(H_WARP)) hm = H_GLOBAL;
+    if (bins > 255 || !fits(H_WARP)) hm = H_GLOBAL;
     else if (pl.weighted && fits(H_LFIX)) hm = H_LFIX;
     else if (pl.weighted && fits(H_WFIX)) hm = H_WFIX;
     else if (!pl.weighted && fits(H_LANE)) hm = H_LANE;
@@ -853,26 +913,34 @@ static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t
         A.chunk = 1 << 22;
     }
     const long long n = A.n_items;
-#define PCF_DISPATCH_W(ANI_, C_)                                                                   \
-    {                                                                                              \
-        if (!ANI_ && hm == H_LANE) return launch_one<false, true, H_LANE, C_>(A, smem, n, st, sm_count, device); \
-        if (hm == H_WARP) return launch_one<ANI_, true, H_WARP, C_>(A, smem, n, st, sm_count, device);   \
-        if (hm == H_WFIX) return launch_one<ANI_, true, H_WFIX, C_>(A, smem, n, st, sm_count, device);   \
-        if (!ANI_ && hm == H_LFIX) return launch_one<false, true, H_LFIX, C_>(A, smem, n, st, sm_count, device); \
-        return launch_one<ANI_, true, H_GLOBAL, C_>(A, smem, n, st, sm_count, device);                 \
+    const bool C = pl.weighted && pl.count;
+#define PCF_LAUNCH(K_, W_, H_)                                                                     \
+    return C ? launch_one<K_, W_, H_, true>(A, smem, n, st, sm_count, device)                      \
+             : launch_one<K_, W_, H_, false>(A, smem, n, st, sm_count, device)
+    if (!pl.ani) {
+        if (pl.weighted) {
+            if (hm == H_LANE) PCF_LAUNCH(K_ISO, true, H_LANE);
+            if (hm == H_WARP) PCF_LAUNCH(K_ISO, true, H_WARP);
+            if (hm == H_WFIX) PCF_LAUNCH(K_ISO, true, H_WFIX);
+            if (hm == H_LFIX) PCF_LAUNCH(K_ISO, true, H_LFIX);
+            PCF_LAUNCH(K_ISO, true, H_GLOBAL);
+        }
+        if (hm == H_LANE) return launch_one<K_ISO, false, H_LANE, false>(A, smem, n, st, sm_count, device);
+        if (hm == H_WARP) return launch_one<K_ISO, false, H_WARP, false>(A, smem, n, st, sm_count, device);
+        return launch_one<K_ISO, false, H_GLOBAL, false>(A, smem, n, st, sm_count, device);
     }
-#define PCF_DISPATCH(ANI_)                                                                       \
-    if (pl.weighted) {                                                                           \
-        if (pl.count) PCF_DISPATCH_W(ANI_, true)                                                 \
-        else PCF_DISPATCH_W(ANI_, false)                                                         \
-    } else {                                                                                     \
-        if (!ANI_ && hm == H_LANE) return launch_one<false, false, H_LANE>(A, smem, n, st, sm_count, device);  \
-        if (hm == H_WARP) return launch_one<ANI_, false, H_WARP>(A, smem, n, st, sm_count, device);  \
-        return launch_one<ANI_, false, H_GLOBAL>(A, smem, n, st, sm_count, device);                \
-    }
-    if (pl.ani) { PCF_DISPATCH(true) } else { PCF_DISPATCH(false) }
-#undef PCF_DISPATCH
-#undef PCF_DISPATCH_W
+#define PCF_DISPATCH_A(K_)                                                                         \
+    if (pl.weighted) {                                                                             \
+        if (hm == H_WARP) PCF_LAUNCH(K_, true, H_WARP);                                            \
+        if (hm == H_WFIX) PCF_LAUNCH(K_, true, H_WFIX);                                            \
+        PCF_LAUNCH(K_, true, H_GLOBAL);                                                            \
+    }                                                                                              \
+    if (hm == H_WARP) return launch_one<K_, false, H_WARP, false>(A, smem, n, st, sm_count, device); \
+    return launch_one<K_, false, H_GLOBAL, false>(A, smem, n, st, sm_count, device);
+    if (pl.both) { PCF_DISPATCH_A(K_BOTH) }
+    PCF_DISPATCH_A(K_ANI)
+#undef PCF_DISPATCH_A
+#undef PCF_LAUNCH
 }
 
 static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
@@ -964,6 +1032,8 @@ cudaError_t launch_pairs_view(const PairView &home, const PairView &cand, const 
     j.slot = 0;
     j.item_begin = 0;
     j.rule_flags = pl.rule.flags;
+    j.rule_flags2 = pl.flags2;
+    j.pad = 0;
     j.P = P;
     j.wunscale = 0.0;
     shape_job(j, n_tiles, n_rows, n_tiles * n_rows, sm_count);
@@ -1037,6 +1107,8 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     job.slot = 0;
     job.item_begin = 0;
     job.rule_flags = pl.rule.flags;
+    job.rule_flags2 = pl.flags2;
+    job.pad = 0;
     job.P = plan.P;
     job.wunscale = pl.wunscale;
     const size_t roff = (plan.rows.size() * sizeof(RowDesc) + 255) & ~(size_t)255;

@@ -265,6 +265,9 @@ pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes);
 // One pair-kernel launch (pairs.cu).
 struct PairLaunch {
     bool ani, weighted, bpc, self;
+    bool both = false;   // isotropic and anisotropic histograms in one pass (ani set too);
+                         // a job slot then holds bins + bins^2 accumulators, iso first
+    unsigned flags2 = 0; // both: the anisotropic rule's flags (rule.flags: isotropic)
     PairRule rule;
     double mult;         // 2 for XX (ordered-pair convention), 1 for XY
     int hist_mode = -1;  // 0 lane-private, 1 per-warp shared, 2 global, 3 per-warp
@@ -297,6 +300,8 @@ struct PairJob {
     long long item_begin;
     unsigned rule_flags;  // exact-rule flags of this histogram (XX and XY differ)
     int P;                // cells per side of both grids of this job
+    unsigned rule_flags2; // both-kinds launches: the anisotropic histogram's flags
+    int pad;
     double wunscale;      // fixed-point launches: weight_unscale(home, cand)
 };
 PairView pair_view(const CellGrid &g, bool with_q);

@@ -13,7 +13,8 @@ std::string tune_key(int kind, bool bpc, bool cross, bool weighted, int bins, in
     const double nbar = (double)n * 4.18879 * (double)dmax * dmax * dmax / ((double)box * box * box);
     const int bucket = (int)std::lround(2.0 * std::log2(nbar + 1.0));
     std::ostringstream os;
-    os << (kind == PCF_ANI ? "ani" : "iso") << (bpc ? "-bpc" : "") << (cross ? "-xy" : "-xx")
+    os << (kind == PCF_BOTH ? "both" : kind == PCF_ANI ? "ani" : "iso") << (bpc ? "-bpc" : "")
+       << (cross ? "-xy" : "-xx")
        << (weighted ? "-w" : "-u") << "-b" << bins << "-n" << bucket;
     return os.str();
 }
@@ -22,11 +23,11 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
                                          const pcf_grid *b, int bins, float dmax, uint32_t flags,
                                          pcf_tune_result *res) {
     if (!ctx || !a || bins < 1 || !(dmax > 0.f)) return PCF_ERR_INVALID_ARG;
-    const bool ani = kind == PCF_ANI, cross = b != nullptr;
+    const bool ani = kind != PCF_ISO, cross = b != nullptr;
     const bool weighted = !(a->unit_weights && (!cross || b->unit_weights));
     const std::string key = tune_key(kind, (flags & PCF_BPC) != 0, cross, weighted, bins,
                                      std::max<int64_t>(a->n, cross ? b->n : 0), a->box, dmax);
-    const int nb = ani ? bins * bins : bins;
+    const int nb = kind == PCF_BOTH ? bins + bins * bins : ani ? bins * bins : bins;
     DevBuf out;
     out.pool = ctx->pool;
     PCF_CU(ctx, out.ensure(sizeof(double) * nb));

@@ -57,8 +57,10 @@ typedef enum pcf_status {
     PCF_ERR_MISMATCH = -8      /* grids of different box or partitions               */
 } pcf_status;
 
-/* Histogram kinds. */
-enum { PCF_ISO = 0, PCF_ANI = 1 };
+/* Histogram kinds.  PCF_BOTH (pair counts only): the isotropic and the
+ * anisotropic histogram from one pass over the candidate pairs, written as
+ * bins doubles (isotropic) followed by bins*bins doubles (anisotropic). */
+enum { PCF_ISO = 0, PCF_ANI = 1, PCF_BOTH = 2 };
 
 /* Flags for the counting calls. */
 enum {
@@ -121,7 +123,8 @@ pcf_status pcf_grid_download(pcf_ctx *ctx, const pcf_grid *g, pcf_point *pts_out
  * One pair histogram.  b == NULL: XX (DD or RR) over a, ordered pairs as the
  * reference counts them (each unordered pair twice).  b != NULL: XY (DR),
  * every (a, b) pair once.  kind PCF_ISO: bins doubles; PCF_ANI: bins*bins
- * doubles indexed [bin(|dz|)][bin(r_perp)].  hist is overwritten.  stats
+ * doubles indexed [bin(|dz|)][bin(r_perp)]; PCF_BOTH: the two, isotropic
+ * first (stats count the pairs of both).  hist is overwritten.  stats
  * may be NULL; when given, the call waits for the result and weighted
  * histograms also count their in-range pairs (a little extra kernel work).
  */
@@ -159,8 +162,9 @@ pcf_status pcf_analytic_3iso(pcf_ctx *ctx, const pcf_grid *d, int bins, float dm
 /*
  * One data catalog against n_rand random catalogs of any sizes, all in one
  * persistent launch over a (tile, neighbour rows, catalog) work queue.
- * Writes, per random catalog i: rr[i*nb .. ] and dr[i*nb ..] (nb = bins or
- * bins^2), and dd (nb) once.  Any of dd / rr / dr may be NULL to skip it.
+ * Writes, per random catalog i: rr[i*nb .. ] and dr[i*nb ..] (nb = bins,
+ * bins^2, or bins + bins^2 for PCF_BOTH), and dd (nb) once.  Any of dd / rr
+ * / dr may be NULL to skip it.
  */
 pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d, const pcf_grid *const *r,
                            int n_rand, int bins, float dmax, uint32_t flags, double *dd,

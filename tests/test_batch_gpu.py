@@ -9,7 +9,7 @@ from desi_b200 import catalog
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("ani", [False, True])
+@pytest.mark.parametrize("ani", [False, True, "both"])
 @pytest.mark.parametrize("bpc", [False, True])
 @pytest.mark.parametrize("w", ["unit", "uniform"])
 @pytest.mark.parametrize("graph", [False, True])
@@ -24,12 +24,14 @@ def test_batch_equals_per_call(ctx, ani, bpc, w, graph):
     for _ in range(reps):  # graph: captured on the first call, replayed after
         (dd, rr, dr), st = ctx.batch_pairs(gd, grs, bins=bins, dmax=dmax, ani=ani, bpc=bpc,
                                            graph=graph, stats=True)
-        cmp = (lambda a, b: np.testing.assert_allclose(a, b, rtol=1e-12, atol=0)) if w != "unit" \
+        cmp1 = (lambda a, b: np.testing.assert_allclose(a, b, rtol=1e-12, atol=0)) if w != "unit" \
             else (lambda a, b: np.testing.assert_array_equal(a, b))
+        cmp = (lambda a, b: [cmp1(x, y) for x, y in zip(a, b)]) if ani == "both" else cmp1
+        at = (lambda h, i: (h[0][i], h[1][i])) if ani == "both" else (lambda h, i: h[i])
         cmp(dd, ctx.count_pairs(gd, None, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
         for i, g in enumerate(grs):
-            cmp(rr[i], ctx.count_pairs(g, None, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
-            cmp(dr[i], ctx.count_pairs(gd, g, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
+            cmp(at(rr, i), ctx.count_pairs(g, None, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
+            cmp(at(dr, i), ctx.count_pairs(gd, g, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
 
 
 def test_autotune_and_estimator(ctx, tmp_path):

@@ -195,12 +195,13 @@ def _tune_key(ani, bpc, cross, weighted, bins, n, box, dmax):
     import math
     nbar = n * 4.18879 * dmax ** 3 / box ** 3
     bucket = int(math.floor(2.0 * math.log2(nbar + 1.0) + 0.5))
-    return (f"{'ani' if ani else 'iso'}{'-bpc' if bpc else ''}{'-xy' if cross else '-xx'}"
+    kind = "both" if ani == "both" else ("ani" if ani else "iso")
+    return (f"{kind}{'-bpc' if bpc else ''}{'-xy' if cross else '-xx'}"
             f"{'-w' if weighted else '-u'}-b{bins}-n{bucket}")
 
 
 @pytest.mark.parametrize("w", ["unit", "uniform"])
-@pytest.mark.parametrize("ani", [False, True])
+@pytest.mark.parametrize("ani", [False, True, "both"])
 def test_every_histogram_scheme(tmp_path, w, ani):
     """Each shared-memory privatisation scheme (lane-private, per-warp, global,
     per-warp and lane-private fixed-point limbs), forced through a loaded
@@ -211,8 +212,14 @@ def test_every_histogram_scheme(tmp_path, w, ani):
     D = catalog.neyman_scott(n, box, seed=41, weights=w)
     R = catalog.uniform(n + 77, box, seed=42, weights=w)
     weighted = w != "unit"
-    want = {cross: oracle.pairs(D, R if cross else None, box=box, bins=bins, dmax=dmax, ani=ani,
-                                bpc=True) for cross in (False, True)}
+    def ref(cross):
+        kw = dict(box=box, bins=bins, dmax=dmax, bpc=True)
+        B = R if cross else None
+        if ani == "both":
+            return np.concatenate([oracle.pairs(D, B, ani=False, **kw).ravel(),
+                                   oracle.pairs(D, B, ani=True, **kw).ravel()])
+        return oracle.pairs(D, B, ani=ani, **kw)
+    want = {cross: ref(cross) for cross in (False, True)}
     for mode in (0, 1, 2, 3, 4):
         path = str(tmp_path / f"tune{mode}.txt")
         with open(path, "w") as f:
@@ -225,6 +232,36 @@ def test_every_histogram_scheme(tmp_path, w, ani):
             gd, gr = c.grid(D, box), c.grid(R, box)
             for cross in (False, True):
                 got = c.count_pairs(gd, gr if cross else None, bins=bins, dmax=dmax, ani=ani, bpc=True)
+                if ani == "both":
+                    got = np.concatenate([got[0].ravel(), got[1].ravel()])
                 _cmp(got.ravel(), want[cross].ravel(), weighted)
         finally:
             c.close()
+
+
+@pytest.mark.parametrize("w", ["unit", "uniform", "signed"])
+@pytest.mark.parametrize("bpc", [False, True])
+def test_both_kinds_one_pass(ctx, w, bpc):
+    """ani="both": the isotropic and anisotropic histograms from one pass over
+    the candidates equal the two single-kind calls (bit-exact for unit
+    weights, 1e-12 for weights; the FP64 fallback for signed weights) and the
+    oracle."""
+    rng = np.random.default_rng(23)
+    box, bins, dmax = 250.0, 30, 80.0
+    D = catalog.neyman_scott(2600, box, seed=51, weights="uniform" if w != "unit" else "unit")
+    R = catalog.uniform(2700, box, seed=52, weights="uniform" if w != "unit" else "unit")
+    if w == "signed":
+        D = _weighted(D, rng, "signed")
+        R = _weighted(R, rng, "signed")
+    gd, gr = ctx.grid(D, box), ctx.grid(R, box)
+    for (a, b, A, B) in ((gd, None, D, None), (gr, None, R, None), (gd, gr, D, R)):
+        iso, ani = ctx.count_pairs(a, b, bins=bins, dmax=dmax, ani="both", bpc=bpc)
+        for got, is_ani in ((iso, False), (ani, True)):
+            single = ctx.count_pairs(a, b, bins=bins, dmax=dmax, ani=is_ani, bpc=bpc)
+            want = oracle.pairs(A, B, box=box, bins=bins, dmax=dmax, ani=is_ani, bpc=bpc)
+            if w == "signed":
+                assert np.all(np.abs(got - want) <= RTOL_W * (np.abs(want) + 1.0))
+                assert np.all(np.abs(got - single) <= RTOL_W * (np.abs(single) + 1.0))
+            else:
+                _cmp(got, want, w != "unit")
+                _cmp(got, single, w != "unit")
