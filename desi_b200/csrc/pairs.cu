@@ -54,10 +54,15 @@ constexpr unsigned kBinBias = 0x43800000u >> kFracBits;
 // H_LFIX: per-lane fixed-point limbs (weighted iso).
 enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3, H_LFIX = 4 };
 constexpr int kLimbs = 3;
-#ifndef PCF_PAIR_GROUP
-#define PCF_PAIR_GROUP 4
+// Candidate steps between recheck votes, per kind: the anisotropic (and
+// both-kinds) kernels carry more live state per step and schedule better
+// with shorter groups.
+#ifndef PCF_GROUP_ISO
+#define PCF_GROUP_ISO 4
 #endif
-constexpr int kGroup = PCF_PAIR_GROUP;  // candidate steps between recheck votes
+#ifndef PCF_GROUP_ANI
+#define PCF_GROUP_ANI 2
+#endif
 constexpr int kChunkMax = 8;            // work items per ticket, at most
 
 // Fast-path cut constants for one range type (0: unshifted, 1: image-shifted).
@@ -324,6 +329,7 @@ template <int KIND, bool WEIGHTED, int HM, bool COUNT>
 __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(const PairArgs A) {
     constexpr bool FIX = HM == H_WFIX || HM == H_LFIX;
     constexpr bool DO_I = KIND != K_ANI, DO_A = KIND != K_ISO;
+    constexpr int kGroup = KIND == K_ISO ? PCF_GROUP_ISO : PCF_GROUP_ANI;
     constexpr int HMI = KIND == K_BOTH ? IsoScheme<WEIGHTED, HM>::value : HM;
     typedef typename WT<WEIGHTED, HM>::type W;
     typedef typename std::conditional<WEIGHTED && !FIX, double, unsigned>::type HT;
@@ -536,14 +542,26 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
                     W w0, w1;
                     bool fi0, fi1, fa0, fa1, ri0, ri1, ra0, ra1;
                 };
-                auto eval = [&](int p, bool v0, bool v1) -> Eval {
+                // The loads of one step (two candidates).
+                struct Raw {
+                    float4 qa, qb;
+                    uint2 q;
+                };
+                auto load = [&](int p) -> Raw {
+                    Raw w;
+                    w.qa = __ldg(cpk + p);
+                    w.qb = __ldg(cpk + p + 1);
+                    if (FIX) w.q = __ldg(reinterpret_cast<const uint2 *>(cqw + p));
+                    else w.q = make_uint2(0u, 0u);
+                    return w;
+                };
+                auto eval_raw = [&](const Raw &w, bool v0, bool v1) -> Eval {
                     Eval e;
-                    const float4 qa = __ldg(cpk + p), qb = __ldg(cpk + p + 1);
+                    const float4 qa = w.qa, qb = w.qb;
                     e.w0 = e.w1 = (W)1;
                     if (FIX) {
-                        const uint2 q = __ldg(reinterpret_cast<const uint2 *>(cqw + p));
-                        e.w0 = (W)q.x;
-                        e.w1 = (W)q.y;
+                        e.w0 = (W)w.q.x;
+                        e.w1 = (W)w.q.y;
                     } else if (WEIGHTED) {
                         e.w0 = (W)qb.z;
                         e.w1 = (W)qb.w;
@@ -590,9 +608,10 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
                     }
                     return e;
                 };
+                auto eval = [&](int p, bool v0, bool v1) -> Eval { return eval_raw(load(p), v0, v1); };
                 // Accumulates the fast-path pairs; true if any needs the FP64 rule.
-                auto core = [&](int p, bool v0, bool v1) -> bool {
-                    const Eval e = eval(p, v0, v1);
+                auto core_raw = [&](const Raw &w, bool v0, bool v1) -> bool {
+                    const Eval e = eval_raw(w, v0, v1);
                     if (DO_I) {
                         sink_i.add(e.si0, hw, e.w0, e.fi0);
                         sink_i.add(e.si1, hw, e.w1, e.fi1);
@@ -605,6 +624,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
                     }
                     return e.ri0 || e.ri1 || e.ra0 || e.ra1;
                 };
+                auto core = [&](int p, bool v0, bool v1) -> bool { return core_raw(load(p), v0, v1); };
                 // Rechecks of `n` steps from p: the vote is rare, so the
                 // candidates are re-evaluated to find which need the FP64 rule.
                 // Lanes of different candidate streams leave the stream loop after
