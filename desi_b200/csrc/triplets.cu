@@ -38,6 +38,9 @@ constexpr float kMagic = 256.0f;
 constexpr int kFracBits = 15;
 constexpr unsigned kFracMask = (1u << kFracBits) - 1u;
 constexpr unsigned kBinBias = 0x43800000u >> kFracBits;  // bits(256 + r) >> 15 = this + floor(r)
+#ifndef PCF_TRIP_GROUP
+#define PCF_TRIP_GROUP 2  // third-side steps between recheck votes
+#endif
 
 struct TripCuts {
     float dsf, ds2;
@@ -370,7 +373,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                     }
                 };
                 int kk = (MIXED ? 0 : jj + 1) + lane;
-                constexpr int G = 4;
+                constexpr int G = PCF_TRIP_GROUP;
                 for (; kk + 64 * (G - 1) + 32 < nK; kk += 64 * G) {
                     bool any = false;
                     #pragma unroll
