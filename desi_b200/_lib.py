@@ -103,6 +103,8 @@ _SIGS = {
     "pcf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pcf_ctx_profile_read": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(_i64)]),
+    "pcf_ctx_profile_read_grid": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
 }
 
 

@@ -242,6 +242,17 @@ class Context:
                                                            ctypes.byref(n)), "pcf_ctx_profile_read")
         return ms.value, n.value
 
+    def profile_read_grid(self):
+        """(summed grid-build kernel ms, builds, points gridded) since
+        profile(); clears that log."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        pts = ctypes.c_int64()
+        _check(self.handle, self._lib.pcf_ctx_profile_read_grid(self.handle, ctypes.byref(ms),
+                                                                ctypes.byref(n), ctypes.byref(pts)),
+               "pcf_ctx_profile_read_grid")
+        return ms.value, n.value, pts.value
+
     @property
     def launches(self) -> int:
         return int(self._lib.pcf_ctx_launch_count(self.handle))

@@ -68,6 +68,10 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
+    for (auto &e : ctx->prof_grid_events) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
     cudaEventDestroy(ctx->ev0);
     cudaEventDestroy(ctx->ev1);
     cudaStreamDestroy(ctx->stream);
@@ -83,6 +87,27 @@ pcf_status pcf_ctx_profile(pcf_ctx *ctx, int enable) {
     if (!ctx) return PCF_ERR_INVALID_ARG;
     ctx->profile = enable != 0;
     ctx->prof_used = 0;
+    ctx->prof_grid_used = 0;
+    ctx->prof_grid_points = 0;
+    return PCF_OK;
+}
+
+pcf_status pcf_ctx_profile_read_grid(pcf_ctx *ctx, double *total_ms, int64_t *builds, int64_t *points) {
+    if (!ctx) return PCF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    double tot = 0;
+    for (size_t i = 0; i < ctx->prof_grid_used; ++i) {
+        float ms = 0.f;
+        PCF_CU(ctx, cudaEventElapsedTime(&ms, ctx->prof_grid_events[i].first,
+                                         ctx->prof_grid_events[i].second));
+        tot += ms;
+    }
+    if (total_ms) *total_ms = tot;
+    if (builds) *builds = (int64_t)ctx->prof_grid_used;
+    if (points) *points = ctx->prof_grid_points;
+    ctx->prof_grid_used = 0;
+    ctx->prof_grid_points = 0;
     return PCF_OK;
 }
 
@@ -167,10 +192,25 @@ pcf_status pcf_grid_download(pcf_ctx *ctx, const pcf_grid *g, pcf_point *pts_out
                              int32_t *cell_start_out) {
     if (!ctx || !g || !g->cells) return PCF_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    if (pts_out)
-        PCF_CU(ctx, cudaMemcpyAsync(pts_out, g->cells->pts.p, sizeof(float4) * (size_t)g->n,
-                                    cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<float> planes;
+    if (pts_out) {  // the cell-ordered SoA planes, interleaved on the host
+        const CellGrid &c = *g->cells;
+        planes.resize(4 * (size_t)g->n);
+        for (int k = 0; k < 4; ++k)
+            PCF_CU(ctx, cudaMemcpyAsync(planes.data() + (size_t)k * g->n, c.soa.as<float>() + k * c.plane,
+                                        sizeof(float) * (size_t)g->n, cudaMemcpyDeviceToHost, ctx->stream));
+    }
     PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (pts_out) {
+        float *o = reinterpret_cast<float *>(pts_out);
+        const size_t n = (size_t)g->n;
+        for (size_t i = 0; i < n; ++i) {
+            o[4 * i] = planes[i];
+            o[4 * i + 1] = planes[n + i];
+            o[4 * i + 2] = planes[2 * n + i];
+            o[4 * i + 3] = planes[3 * n + i];
+        }
+    }
     if (cell_start_out)
         memcpy(cell_start_out, g->cells->h_start.data(), sizeof(int) * g->cells->h_start.size());
     return PCF_OK;

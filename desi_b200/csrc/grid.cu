@@ -6,7 +6,9 @@
 // HBM-bound passes over the points --
 //   1. cell id + per-cell count (atomic), with out-of-box / weight checks,
 //   2. exclusive scan of the counts into the dense cell table,
-//   3. scatter of the float4 points into cell order.
+//   3. the destination of every point (a 4-byte scattered write),
+//   4. a gather in destination order that writes the cell-ordered copies
+//      (SoA planes, pair-packed blocks, integer weights) coalesced.
 // Cell id = (ix*P + iy)*P + iz with ix = (int)(x / cell), the reference's
 // binning (create_grid.cuh:131-133) clamped to [0, P-1].
 #include <algorithm>
@@ -159,28 +161,39 @@ __host__ __device__ inline bool weight_fix_range(unsigned f0, unsigned wmaxb, un
     return !(f0 & 4u) && wminc != 0u && *emin >= 1 && *emax - *emin <= 8;
 }
 
-__global__ void k_scatter(const float4 *__restrict__ pts, int64_t n, const int *__restrict__ cid,
-                          const int *__restrict__ rank, const int *__restrict__ start,
-                          float4 *__restrict__ out, float *__restrict__ soa, size_t plane,
-                          float *__restrict__ pk, unsigned *__restrict__ qw,
-                          const int *__restrict__ flags) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// Destination of every point: perm[start[cid] + rank] = i (one scattered
+// 4-byte write per point).
+__global__ void k_perm(int64_t n, const int *__restrict__ cid, const int *__restrict__ rank,
+                       const int *__restrict__ start, int *__restrict__ perm) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 p = pts[i];
-    const int64_t d = start[cid[i]] + rank[i];
-    if (out) out[d] = p;
+    perm[start[cid[i]] + rank[i]] = (int)i;
+}
+
+// Cell-ordered copies, one thread per destination d: a random 16-byte read
+// of the source point, then coalesced writes of the SoA planes, the integer
+// weight and the pair-packed blocks (an even lane writes block d/2 with its
+// odd neighbour's values).
+__global__ void k_gather(const float4 *__restrict__ pts, int64_t n, const int *__restrict__ perm,
+                         float *__restrict__ soa, size_t plane, float4 *__restrict__ pk,
+                         unsigned *__restrict__ qw, const int *__restrict__ flags) {
+    const int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (d < n) p = pts[perm[d]];
+    const float nx = __shfl_down_sync(0xffffffffu, p.x, 1), ny = __shfl_down_sync(0xffffffffu, p.y, 1);
+    const float nz = __shfl_down_sync(0xffffffffu, p.z, 1), nw = __shfl_down_sync(0xffffffffu, p.w, 1);
+    if (d >= n) return;
     if (soa) {
         soa[d] = p.x;
         soa[plane + d] = p.y;
         soa[2 * plane + d] = p.z;
         soa[3 * plane + d] = p.w;
     }
-    // pair-packed block d/2: (x0 x1 y0 y1)(z0 z1 w0 w1)
-    float *blk = pk + (d >> 1) * 8 + (d & 1);
-    blk[0] = p.x;
-    blk[2] = p.y;
-    blk[4] = p.z;
-    blk[6] = p.w;
+    if (!(d & 1)) {  // block d/2: (x_d x_d+1 y_d y_d+1)(z_d z_d+1 w_d w_d+1); d+1 >= n gives 0
+        const bool has = d + 1 < n;
+        pk[d] = make_float4(p.x, has ? nx : 0.f, p.y, has ? ny : 0.f);
+        pk[d + 1] = make_float4(p.z, has ? nz : 0.f, p.w, has ? nw : 0.f);
+    }
     if (qw) {
         int emin, emax;
         const unsigned *uf = reinterpret_cast<const unsigned *>(flags);
@@ -238,17 +251,16 @@ __global__ void k_tile_emit(const int *__restrict__ start, const int *__restrict
 }  // namespace
 
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
-                      int *rank, int *counts, int *cell_start, int *scan_tmp, float4 *pts_out,
-                      float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
-                      cudaStream_t st) {
+                      int *rank, int *perm, int *counts, int *cell_start, int *scan_tmp, float *soa,
+                      size_t plane, float4 *pk, unsigned *qw, int *flags, cudaStream_t st) {
     const int64_t ncell = (int64_t)P * P * P;
     const int thr = 256;
     const unsigned blocks = (unsigned)((n + thr - 1) / thr);
     k_cell_ids<<<blocks, thr, 0, st>>>(raw, n, P, cell, box, cid, rank, counts, flags);
     int launches = 1 + scan_exclusive(counts, cell_start, ncell + 1, scan_tmp, st);
-    k_scatter<<<blocks, thr, 0, st>>>(raw, n, cid, rank, cell_start, pts_out, soa, plane,
-                                      reinterpret_cast<float *>(pk), qw, flags);
-    return launches + 1;
+    k_perm<<<blocks, thr, 0, st>>>(n, cid, rank, cell_start, perm);
+    k_gather<<<blocks, thr, 0, st>>>(raw, n, perm, soa, plane, pk, qw, flags);
+    return launches + 2;
 }
 
 void set_weight_range(pcf_grid *g, const unsigned hf[3]) {
@@ -310,13 +322,12 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     static uint64_t next_serial = 0;
     std::shared_ptr<CellGrid> cg(new CellGrid);
     cg->serial = ++next_serial;
-    cg->pts.pool = cg->soa.pool = cg->cell_start.pool = g->pool;
+    cg->soa.pool = cg->cell_start.pool = g->pool;
     cg->P = P;
     cg->cell = g->box / (float)P;
     const int64_t n = g->n;
     const int64_t ncell = (int64_t)P * P * P;
     cudaStream_t st = ctx->stream;
-    PCF_CU(ctx, cg->pts.ensure(sizeof(float4) * (size_t)n));
     cg->plane = ((size_t)n + kSoaPad + 3) & ~(size_t)3;
     PCF_CU(ctx, cg->soa.ensure(sizeof(float) * cg->plane * 4));
     PCF_CU(ctx, cudaMemsetAsync(cg->soa.p, 0, sizeof(float) * cg->plane * 4, ctx->stream));
@@ -327,21 +338,37 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     PCF_CU(ctx, cudaMemsetAsync(cg->qw.p, 0, sizeof(unsigned) * cg->plane, ctx->stream));
     PCF_CU(ctx, cg->cell_start.ensure(sizeof(int) * (size_t)(ncell + 1)));
     // scratch: cid, rank (n each); counts (ncell + 1); scan tmp.
-    PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(int) * (size_t)n * 2));
+    PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(int) * (size_t)n * 3));
     PCF_CU(ctx, ctx->scratch_b.ensure(sizeof(int) * (size_t)(ncell + 1)));
     PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(int) * (size_t)((ncell + 1) / 256 + 256)));
     PCF_CU(ctx, ctx->d_flag.ensure(sizeof(int) * 4));
     int *cid = ctx->scratch_a.as<int>();
     int *rank = cid + n;
+    int *perm = rank + n;
     int *counts = ctx->scratch_b.as<int>();
     int *flags = ctx->d_flag.as<int>();
     PCF_CU(ctx, cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)(ncell + 1), st));
     PCF_CU(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * 3, st));
-    ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank, counts,
-                                       cg->cell_start.as<int>(), ctx->scratch_c.as<int>(),
-                                       cg->pts.as<float4>(), cg->soa.as<float>(), cg->plane,
-                                       cg->pk.as<float4>(), cg->qw.as<unsigned>(), flags, st);
+    cudaEvent_t pg0 = nullptr, pg1 = nullptr;  // kernel-time log of grid builds
+    if (ctx->profile) {
+        if (ctx->prof_grid_used == ctx->prof_grid_events.size()) {
+            cudaEvent_t e0, e1;
+            PCF_CU(ctx, cudaEventCreate(&e0));
+            PCF_CU(ctx, cudaEventCreate(&e1));
+            ctx->prof_grid_events.push_back({e0, e1});
+        }
+        pg0 = ctx->prof_grid_events[ctx->prof_grid_used].first;
+        pg1 = ctx->prof_grid_events[ctx->prof_grid_used].second;
+        ++ctx->prof_grid_used;
+        ctx->prof_grid_points += n;
+        PCF_CU(ctx, cudaEventRecord(pg0, st));
+    }
+    ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank, perm,
+                                       counts, cg->cell_start.as<int>(), ctx->scratch_c.as<int>(),
+                                       cg->soa.as<float>(), cg->plane, cg->pk.as<float4>(),
+                                       cg->qw.as<unsigned>(), flags, st);
     PCF_CU(ctx, cudaGetLastError());
+    if (pg1) PCF_CU(ctx, cudaEventRecord(pg1, st));
     cg->h_start.resize((size_t)(ncell + 1));
     unsigned hf[3] = {0u, 0u, 0u};
     PCF_CU(ctx, cudaMemcpyAsync(cg->h_start.data(), cg->cell_start.p, sizeof(int) * (ncell + 1),

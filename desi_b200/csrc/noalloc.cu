@@ -51,7 +51,7 @@ struct Carve {
 };
 
 struct CatBufs {
-    int *cid, *rank, *counts, *start;
+    int *cid, *rank, *perm, *counts, *start;
     float4 *pk;  // pair-packed points (PairView)
 };
 
@@ -97,6 +97,7 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
         CatBufs c;
         c.cid = cv.take<int>((size_t)n);
         c.rank = cv.take<int>((size_t)n);
+        c.perm = cv.take<int>((size_t)n);
         c.counts = cv.take<int>((size_t)ncell + 1);
         c.start = cv.take<int>((size_t)ncell + 1);
         c.pk = cv.take<float4>(2 * pk_blocks(n));
@@ -131,11 +132,11 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
     if ((e = cudaMemsetAsync(d_flags, 0, 32, st)) != cudaSuccess) return fail(e);
 
     const float cell = box / (float)P;
-    launch_grid_build(reinterpret_cast<const float4 *>(a), na, P, cell, box, A.cid, A.rank, A.counts,
-                      A.start, scan_tmp, nullptr, nullptr, 0, A.pk, nullptr, d_flags, st);
+    launch_grid_build(reinterpret_cast<const float4 *>(a), na, P, cell, box, A.cid, A.rank, A.perm,
+                      A.counts, A.start, scan_tmp, nullptr, 0, A.pk, nullptr, d_flags, st);
     if (cross)
         launch_grid_build(reinterpret_cast<const float4 *>(b), nb, P, cell, box, B.cid, B.rank,
-                          B.counts, B.start, scan_tmp, nullptr, nullptr, 0, B.pk, nullptr, d_flags, st);
+                          B.perm, B.counts, B.start, scan_tmp, nullptr, 0, B.pk, nullptr, d_flags, st);
     launch_tile_build(A.start, P, tile_counts, tile_offsets, scan_tmp, tiles, st);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
     if ((e = cudaMemcpyAsync(d_rows, rows.data(), sizeof(RowDesc) * rows.size(),

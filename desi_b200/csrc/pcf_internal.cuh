@@ -141,7 +141,6 @@ struct CellGrid {
     int P = 0;
     uint64_t serial = 0;          // unique per build (keys captured graphs)
     float cell = 0.f;             // box / P
-    DevBuf pts;                   // float4 x n, cell order
     DevBuf soa;                   // x | y | z | w planes, n + kSoaPad floats each
     size_t plane = 0;             // floats per plane
     DevBuf pk;                    // pair-packed blocks (PairView), pk_blocks(n) x 32 B
@@ -212,6 +211,10 @@ struct pcf_ctx {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
+    // the same for grid builds (counting sort + scatter kernels)
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_grid_events;
+    size_t prof_grid_used = 0;
+    int64_t prof_grid_points = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -328,12 +331,12 @@ cudaError_t launch_finalize_slots(const unsigned long long *d_count, const doubl
 unsigned reference_pair_rule(bool ani, bool bpc, bool cross);
 // Counting sort of n points into P^3 cells on explicit buffers; returns the
 // number of kernels launched (counts must be zeroed, P^3 + 1 entries).
-// pts_out, soa and qw may be null; pk (pk_blocks(n) blocks, zeroed by the
-// caller) is always written, qw only when the weights allow exact integers.
+// soa and qw may be null; pk (pk_blocks(n) blocks, zeroed by the caller) is
+// always written, qw only when the weights allow exact integers.  cid, rank
+// and perm: n ints of scratch each.
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
-                      int *rank, int *counts, int *cell_start, int *scan_tmp, float4 *pts_out,
-                      float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
-                      cudaStream_t st);
+                      int *rank, int *perm, int *counts, int *cell_start, int *scan_tmp, float *soa,
+                      size_t plane, float4 *pk, unsigned *qw, int *flags, cudaStream_t st);
 // Host side of the weight scan (flags[0..2] as written by the grid build):
 // fills g's weight-range fields, including the integer-weight scale.
 void set_weight_range(pcf_grid *g, const unsigned flags[3]);

@@ -50,8 +50,8 @@ class Request:
 
 
 def grid_bytes(n: int, partitions: int = 64) -> int:
-    """Device bytes of one gridded catalog: raw + cell-ordered AoS + SoA planes,
-    cell table and tiles (upper bound)."""
+    """Device bytes of one gridded catalog: raw copy, cell-ordered SoA planes,
+    pair-packed copy and integer weights, cell table and tiles (upper bound)."""
     return n * (16 + 16 + 16) + 4 * (partitions ** 3 + 1) + 16 * n + (1 << 20)
 
 

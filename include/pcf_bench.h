@@ -33,6 +33,11 @@ int64_t pcf_ctx_launch_count(const pcf_ctx *ctx);
  * summed kernel time and the number of logged launches, and clears the log. */
 pcf_status pcf_ctx_profile(pcf_ctx *ctx, int enable);
 pcf_status pcf_ctx_profile_read(pcf_ctx *ctx, double *total_ms, int64_t *launches);
+/* The same log for grid builds (the counting-sort and scatter kernels of
+ * each cell structure built while enabled): summed kernel time, number of
+ * builds and points gridded; clears that log. */
+pcf_status pcf_ctx_profile_read_grid(pcf_ctx *ctx, double *total_ms, int64_t *builds,
+                                     int64_t *points);
 
 #ifdef __cplusplus
 }
