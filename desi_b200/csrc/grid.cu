@@ -105,13 +105,27 @@ __global__ void k_cell_ids(const float4 *__restrict__ pts, int64_t n, int P, flo
         cid[i] = c;
         rank[i] = atomicAdd(&counts[c], 1);
     }
+    // one update of the three flag words per block, and only when it changes
+    // them: every block targets the same three addresses, which would
+    // otherwise serialise millions of atomics in L2
     f = __reduce_or_sync(0xffffffffu, f);
     wmax = __reduce_max_sync(0xffffffffu, wmax);
     wminc = __reduce_max_sync(0xffffffffu, wminc);
+    __shared__ unsigned s_f, s_max, s_minc;
+    if (threadIdx.x == 0) s_f = s_max = s_minc = 0u;
+    __syncthreads();
     if ((threadIdx.x & 31) == 0) {
-        if (f) atomicOr(flags, (int)f);
-        if (wmax) atomicMax(reinterpret_cast<unsigned *>(flags) + 1, wmax);
-        if (wminc) atomicMax(reinterpret_cast<unsigned *>(flags) + 2, wminc);
+        if (f) atomicOr(&s_f, f);
+        if (wmax) atomicMax(&s_max, wmax);
+        if (wminc) atomicMax(&s_minc, wminc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned *uf = reinterpret_cast<unsigned *>(flags);
+        const volatile unsigned *vf = uf;
+        if (s_f && (vf[0] & s_f) != s_f) atomicOr(uf, s_f);
+        if (s_max > vf[1]) atomicMax(uf + 1, s_max);
+        if (s_minc > vf[2]) atomicMax(uf + 2, s_minc);
     }
 }
 

@@ -8,8 +8,9 @@
 // image passes for periodic boxes; here:
 //
 //  * Work = (home tile, stencil rows) items in a persistent queue.  A home
-//    tile is <= 32 cell-ordered points of one (ix,iy) column, one point per
-//    lane (a tile of H points runs 32/H candidate streams); a stencil row
+//    tile is <= 32 consecutive cell-ordered points of one (ix,iy) column
+//    within two cells, one point per lane (a tile of H points runs 32/H
+//    candidate streams); a stencil row
 //    (dx,dy) names the neighbour column, whose cells z0-kz..z1+kz are one
 //    contiguous point range (or two when the periodic box wraps in z).  XX
 //    uses the half shell (each unordered pair once, histogram doubled at the
@@ -29,6 +30,8 @@
 //    q_a*q_b goes into three u32 limb counters (16 + 16 + 32 bits), flushed
 //    before any could wrap; FP64 shared atomics remain for weights without
 //    an exact integer image.
+//  * A launch produces the isotropic histogram, the anisotropic one, or both
+//    from one pass over the candidates (PCF_BOTH).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
