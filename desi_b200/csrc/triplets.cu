@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
     float4 *sK = sJ + A.capJ;
     float *swJ = reinterpret_cast<float *>(sK + (MIXED ? A.capK : 0));
     float *swK = swJ + (WEIGHTED ? A.capJ : 0);
-    __shared__ int s_anchor, s_nJ, s_nK;
+    __shared__ int s_anchor, s_nJ, s_nK, s_unit;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (A.hist_in_smem)
         for (int k = tid; k < nb3 + 32; k += kTThreads) U[k] = 0u;
@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
             s_anchor = (int)atomicAdd(A.counter, 1ull);
             s_nJ = 0;
             s_nK = 0;
+            s_unit = 0;
         }
         __syncthreads();
         const int i = s_anchor;
@@ -306,9 +307,19 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
             const unsigned w2 = 2u * A.fc.w;
             const float mgw = kMagic + (float)A.fc.w * 0x1p-15f;
             const float2 DS2 = make_float2(A.fc.ds2, A.fc.ds2);
-            for (int rr = warp; rr < nJ; rr += kTWarps) {
-                const int half = rr >> 1;
-                const int jj = MIXED ? rr : ((rr & 1) ? nJ - 1 - half : half);
+            // Work units handed out dynamically (a shared counter), so warps
+            // finish together: XXX rows j in order (largest first), XXY rows
+            // split into `segs` segments of the K list when rows are few.
+            const int segs = (MIXED && nJ < 8 * kTWarps) ? 4 : 1;
+            const int units = nJ * segs;
+            for (;;) {
+                int u = 0;
+                if (lane == 0) u = atomicAdd(&s_unit, 1);
+                u = __shfl_sync(kFull, u, 0);
+                if (u >= units) break;
+                const int jj = u / segs, sg = u - jj * segs;
+                const int kbeg = MIXED ? (int)((long long)nK * sg / segs) : jj + 1;
+                const int kend = MIXED ? (int)((long long)nK * (sg + 1) / segs) : nK;
                 const float4 ej = LJ[jj];
                 const int bj = __float_as_int(ej.w) & 255;
                 const int jidx = (int)((unsigned)__float_as_int(ej.w) >> 8);
@@ -372,16 +383,16 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                         }
                     }
                 };
-                int kk = (MIXED ? 0 : jj + 1) + lane;
+                int kk = kbeg + lane;
                 constexpr int G = PCF_TRIP_GROUP;
-                for (; kk + 64 * (G - 1) + 32 < nK; kk += 64 * G) {
+                for (; kk + 64 * (G - 1) + 32 < kend; kk += 64 * G) {
                     bool any = false;
                     #pragma unroll
                     for (int q = 0; q < G; ++q) any |= core(kk + 64 * q, true);
                     settle(any, kk, G, true);
                 }
-                for (; kk + 32 < nK; kk += 64) settle(core(kk, true), kk, 1, true);
-                if (kk < nK) settle(core(kk, false), kk, 1, false);
+                for (; kk + 32 < kend; kk += 64) settle(core(kk, true), kk, 1, true);
+                if (kk < kend) settle(core(kk, false), kk, 1, false);
             }
         } else {
         for (int rr = warp; rr < nJ; rr += kTWarps) {
