@@ -296,6 +296,9 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
         // pass 2: pairs of neighbours.  Rows j are dealt to warps in the
         // order 0, n-1, 1, n-2, ... (XXX rows shrink with j).
         if (!WEIGHTED && A.hist_in_smem) {
+            // the lists' address space is fixed per instantiation, so the
+            // shared-memory case (all but overflowing anchors) uses shared loads
+            auto pass2 = [&](const float4 *__restrict__ LJx, const float4 *__restrict__ LKx) {
             // Unit weights, shared histogram: two k per lane per step in packed
             // FP32, unpredicated shared reductions (a lane without a triangle
             // adds 0 to its dummy slot past the histogram), one recheck vote
@@ -320,7 +323,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                 const int jj = u / segs, sg = u - jj * segs;
                 const int kbeg = MIXED ? (int)((long long)nK * sg / segs) : jj + 1;
                 const int kend = MIXED ? (int)((long long)nK * (sg + 1) / segs) : nK;
-                const float4 ej = LJ[jj];
+                const float4 ej = LJx[jj];
                 const int bj = __float_as_int(ej.w) & 255;
                 const int jidx = (int)((unsigned)__float_as_int(ej.w) >> 8);
                 // slot = bj*bins^2 + b_jk*bins + b_k, with bits(r+256..) >> 15 = kBinBias + b_jk
@@ -333,8 +336,8 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                 };
                 // k0 and (if v1) k0 + 32
                 auto eval = [&](int k0, bool v1) -> Ev {
-                    const float4 e0 = LK[k0];
-                    const float4 e1 = LK[v1 ? k0 + 32 : k0];
+                    const float4 e0 = LKx[k0];
+                    const float4 e1 = LKx[v1 ? k0 + 32 : k0];
                     const float2 DX = __fadd2_rn(make_float2(e0.x, e1.x), NJX);
                     const float2 DY = __fadd2_rn(make_float2(e0.y, e1.y), NJY);
                     const float2 DZ = __fadd2_rn(make_float2(e0.z, e1.z), NJZ);
@@ -364,7 +367,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                 // third side by the canonical FP64 rule
                 auto slow = [&](int kk) {
                     ++n_rechk;
-                    const float4 ek = LK[kk];
+                    const float4 ek = LKx[kk];
                     const int kidx = (int)((unsigned)__float_as_int(ek.w) >> 8);
                     const Cat &CK = MIXED ? A.Y : A.X;
                     const int bjk = exact_third(hx, hy, hz, A.X.x[jidx], A.X.y[jidx], A.X.z[jidx],
@@ -394,6 +397,9 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                 for (; kk + 32 < kend; kk += 64) settle(core(kk, true), kk, 1, true);
                 if (kk < kend) settle(core(kk, false), kk, 1, false);
             }
+            };
+            if (LJ == sJ) pass2(sJ, MIXED ? sK : sJ);
+            else pass2(gJ, MIXED ? gK : gJ);
         } else {
         for (int rr = warp; rr < nJ; rr += kTWarps) {
             const int half = rr >> 1;
