@@ -153,7 +153,7 @@ template <bool ANG>
 __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, float hz, int hcell_ix,
                            int hcell_iy, int hcell_iz, int only_after, const PairRule &rule,
                            float4 *list, float *wlist, int cap, int *s_n, unsigned &n_rechk,
-                           unsigned short *ang = nullptr) {
+                           unsigned short *ang = nullptr, int step = 1) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int P = A.P;
     for (int r = 0; r < A.n_rows; ++r) {
@@ -212,8 +212,8 @@ __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, 
                 off = __shfl_sync(kFull, off, 0);
                 if (keep) {
                     const int pos = off + __popc(m & ((1u << lane) - 1u));
-                    if (pos < cap) {
-                        list[pos] = make_float4(vx, vy, vz, __int_as_float((c << 8) | bin));
+                    if (pos < cap) {  // step -1: the list grows downwards from `list`
+                        list[step * pos] = make_float4(vx, vy, vz, __int_as_float((c << 8) | bin));
                         if (wlist) wlist[pos] = C.w[c];
                         if (ANG) ang[pos] = (unsigned short)(bin | (tang << 8));
                     }
@@ -263,18 +263,27 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
         const int cix = min(max((int)__fdiv_rn(hx, A.cell), 0), P - 1);
         const int ciy = min(max((int)__fdiv_rn(hy, A.cell), 0), P - 1);
         const int ciz = min(max((int)__fdiv_rn(hz, A.cell), 0), P - 1);
-        // pass 1: lists into shared memory (sizes counted even past capacity)
+        // pass 1: lists into shared memory (sizes counted even past capacity).
+        // Pooled (XXY, unit weights, shared histogram): one buffer of capJ
+        // entries, J from the front and K from the back, so the anchor
+        // overflows only when both together exceed it.
+        const bool pool = MIXED && !WEIGHTED && A.hist_in_smem;
         build_list<false>(A, A.X, hx, hy, hz, cix, ciy, ciz, i, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
                           A.capJ, &s_nJ, n_rechk);
+        int capK = A.capK;
+        if (pool) {
+            __syncthreads();
+            capK = max(0, A.capJ - s_nJ);
+        }
         if (MIXED)
-            build_list<false>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK,
-                              WEIGHTED ? swK : nullptr, A.capK, &s_nK, n_rechk);
+            build_list<false>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, pool ? sJ + A.capJ - 1 : sK,
+                              WEIGHTED ? swK : nullptr, capK, &s_nK, n_rechk, nullptr, pool ? -1 : 1);
         __syncthreads();
         int nJ = s_nJ, nK = MIXED ? s_nK : nJ;
         const float4 *LJ = sJ;
         const float4 *LK = MIXED ? sK : sJ;
         const float *WJ = swJ, *WK = MIXED ? swK : swJ;
-        if (nJ > A.capJ || (MIXED && nK > A.capK)) {
+        if (nJ > A.capJ || (MIXED && nK > capK)) {
             // overflow: rebuild the lists in this CTA's global scratch (L2)
             __syncthreads();
             if (tid == 0) { s_nJ = 0; s_nK = 0; }
@@ -298,7 +307,8 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
         if (!WEIGHTED && A.hist_in_smem) {
             // the lists' address space is fixed per instantiation, so the
             // shared-memory case (all but overflowing anchors) uses shared loads
-            auto pass2 = [&](const float4 *__restrict__ LJx, const float4 *__restrict__ LKx) {
+            // LKx[kstep * k] is K entry k (kstep -1: the pooled, downward K list)
+            auto pass2 = [&](const float4 *__restrict__ LJx, const float4 *__restrict__ LKx, int kstep) {
             // Unit weights, shared histogram: two k per lane per step in packed
             // FP32, unpredicated shared reductions (a lane without a triangle
             // adds 0 to its dummy slot past the histogram), one recheck vote
@@ -336,8 +346,8 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                 };
                 // k0 and (if v1) k0 + 32
                 auto eval = [&](int k0, bool v1) -> Ev {
-                    const float4 e0 = LKx[k0];
-                    const float4 e1 = LKx[v1 ? k0 + 32 : k0];
+                    const float4 e0 = LKx[kstep * k0];
+                    const float4 e1 = LKx[kstep * (v1 ? k0 + 32 : k0)];
                     const float2 DX = __fadd2_rn(make_float2(e0.x, e1.x), NJX);
                     const float2 DY = __fadd2_rn(make_float2(e0.y, e1.y), NJY);
                     const float2 DZ = __fadd2_rn(make_float2(e0.z, e1.z), NJZ);
@@ -367,7 +377,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                 // third side by the canonical FP64 rule
                 auto slow = [&](int kk) {
                     ++n_rechk;
-                    const float4 ek = LKx[kk];
+                    const float4 ek = LKx[kstep * kk];
                     const int kidx = (int)((unsigned)__float_as_int(ek.w) >> 8);
                     const Cat &CK = MIXED ? A.Y : A.X;
                     const int bjk = exact_third(hx, hy, hz, A.X.x[jidx], A.X.y[jidx], A.X.z[jidx],
@@ -398,8 +408,12 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                 if (kk < kend) settle(core(kk, false), kk, 1, false);
             }
             };
-            if (LJ == sJ) pass2(sJ, MIXED ? sK : sJ);
-            else pass2(gJ, MIXED ? gK : gJ);
+            if (LJ == sJ) {
+                if (pool) pass2(sJ, sJ + A.capJ - 1, -1);
+                else pass2(sJ, MIXED ? sK : sJ, 1);
+            } else {
+                pass2(gJ, MIXED ? gK : gJ, 1);
+            }
         } else {
         for (int rr = warp; rr < nJ; rr += kTWarps) {
             const int half = rr >> 1;
@@ -635,10 +649,10 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
     const size_t hist_b = A.hist_in_smem ? u_bytes : 0;
     const size_t ent = 16 + (weighted ? 4 : 0);
     const size_t room = smem_max - hist_b;
-    if (mixed) {
+    if (mixed && !(A.hist_in_smem && !weighted)) {
         A.capJ = (int)(room / ent / 3);
         A.capK = (int)(room / ent) - A.capJ;
-    } else {
+    } else {  // XXX, or XXY with one pooled buffer (J up, K down; see k_triplets)
         A.capJ = (int)(room / ent);
         A.capK = 0;
     }
