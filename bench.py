@@ -389,14 +389,14 @@ def _timed_ms(torch, stream, fn, reps=1):
     return min(ts), r
 
 
-def run_triplets(ctx, torch, stream):
-    """Periodic 3iso on 32768 clustered + 32768 uniform points (box 250, 30^3
-    bins, dmax 80, unit weights): DDD, RRR, DDR, DRR, and the analytic
-    DDR/RRR path.  Unit: one unordered in-range triangle (XXY: one
-    unordered XX pair with one Y point)."""
+def run_triplets(ctx, torch, stream, n=32768):
+    """Periodic 3iso on n clustered + n uniform points (box 250, 30^3 bins,
+    dmax 80, unit weights; n = 32768 in the bench line): DDD, RRR, DDR, DRR,
+    and the analytic DDR/RRR path.  Unit: one unordered in-range triangle
+    (XXY: one unordered XX pair with one Y point)."""
     from desi_b200 import catalog
-    D = catalog.neyman_scott(32768, 250.0, seed=3001, weights="unit")
-    R = catalog.uniform(32768, 250.0, seed=3002, weights="unit")
+    D = catalog.neyman_scott(n, 250.0, seed=3001, weights="unit")
+    R = catalog.uniform(n, 250.0, seed=3002, weights="unit")
     gd, gr = ctx.grid(D, 250.0), ctx.grid(R, 250.0)
     kw = dict(bins=30, dmax=80.0, bpc=True, stats=True)
     res = {}
@@ -411,7 +411,7 @@ def run_triplets(ctx, torch, stream):
     four()  # warm-up
     ms, sts = _timed_ms(torch, stream, four)
     tri = sum(s["pairs"] for s in sts.values())
-    res.update({"workload": "3iso periodic, 32768 Neyman-Scott + 32768 uniform, box 250, 30^3 "
+    res.update({"workload": f"3iso periodic, {n} Neyman-Scott + {n} uniform, box 250, 30^3 "
                             "bins, dmax 80, unit weights: DDD, RRR, DDR, DRR",
                 "ms": ms, "triangles": tri, "value": tri / (ms * 1e-3), "unit": "triplets/s",
                 "per_histogram_ms": {k: v["kernel_ms"] for k, v in sts.items()}})
@@ -615,7 +615,18 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the triplet / batched / served measurements")
+    ap.add_argument("--triplets-only", type=int, default=0, metavar="N",
+                    help="run only the 3iso section on N + N points and print its result "
+                         "(a small case for profiling; not the bench line)")
     args = ap.parse_args()
+    if args.triplets_only:
+        import torch
+        from desi_b200 import api
+        ctx = api.Context(0)
+        stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+        print(json.dumps(run_triplets(ctx, torch, stream, n=args.triplets_only)))
+        ctx.close()
+        return
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world = int(os.environ.get("WORLD_SIZE", "1"))
