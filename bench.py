@@ -179,6 +179,10 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     P, fused, tuned = tune_step(ctx, D, R)
     kinds = ("both",) if fused else (False, True)
+    # a both-kinds call tuned to the library's default rule (-1) runs as two
+    # single-kind launches when the isotropic histogram alone gets
+    # lane-private copies (this workload's 30 exact-weight bins)
+    one_pass = [k[:2] for k, m in tuned.items() if k.endswith("both") and m >= 0]
     Dt = torch.from_numpy(D).to(dev)
     Rt = torch.from_numpy(R).to(dev)
     outs = torch.zeros((6, W["bins"] + W["bins"] * W["bins"]), dtype=torch.float64, device=dev)
@@ -309,7 +313,7 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Neyman-Scott data + uniform randoms; no dataset ships with "
                 "the workload)",
-        "config": dict(W, partitions=P, kinds_in_one_pass=fused, schemes=tuned,
+        "config": dict(W, partitions=P, kinds_in_one_pass=one_pass, schemes=tuned,
                        parallelism=f"replicas x{world}",
                        l2="flushed between steps (512 MB write)",
                        pairs_per_step=pairs_step),

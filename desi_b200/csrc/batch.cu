@@ -34,6 +34,47 @@ struct BatchGraph {
     }
 };
 
+// Both kinds as two single-kind batches, interleaved into the both-kinds
+// layout: per histogram bins isotropic doubles, then bins^2 anisotropic.
+// (One pass over the candidates for both kinds is slower: the measurements
+// sit beside count_pairs_impl in capi.cu.)
+static pcf_status batch_both_split(pcf_ctx *ctx, const pcf_grid *d, const pcf_grid *const *r,
+                                   int n_rand, int bins, float dmax, uint32_t flags, double *dd,
+                                   double *rr, double *dr, pcf_stats *stats) {
+    const size_t b1 = (size_t)bins, b2 = (size_t)bins * bins, nb = b1 + b2, nr = (size_t)n_rand;
+    std::vector<double> h[2][3];  // [kind][dd, rr, dr]
+    pcf_stats st[2] = {};
+    for (int k = 0; k < 2; ++k) {
+        const size_t w = k ? b2 : b1;
+        if (dd) h[k][0].resize(w);
+        if (rr) h[k][1].resize(w * nr);
+        if (dr) h[k][2].resize(w * nr);
+        auto ptr = [&](int i, bool want) { return want ? h[k][i].data() : nullptr; };
+        const pcf_status s = pcf_batch_pairs(ctx, k ? PCF_ANI : PCF_ISO, d, r, n_rand, bins, dmax, flags,
+                                             ptr(0, dd != nullptr), ptr(1, rr != nullptr),
+                                             ptr(2, dr != nullptr), stats ? &st[k] : nullptr);
+        if (s != PCF_OK) return s;
+    }
+    auto put = [&](double *out, int i, size_t j) {
+        memcpy(out + j * nb, h[0][i].data() + j * b1, sizeof(double) * b1);
+        memcpy(out + j * nb + b1, h[1][i].data() + j * b2, sizeof(double) * b2);
+    };
+    if (dd) put(dd, 0, 0);
+    for (size_t j = 0; j < nr; ++j) {
+        if (rr) put(rr, 1, j);
+        if (dr) put(dr, 2, j);
+    }
+    if (stats) {
+        stats->pairs = st[0].pairs + st[1].pairs;
+        stats->candidates = st[0].candidates + st[1].candidates;
+        stats->rechecks = st[0].rechecks + st[1].rechecks;
+        stats->kernel_ms = st[0].kernel_ms + st[1].kernel_ms;
+        stats->partitions = st[1].partitions;
+        stats->work_items = st[0].work_items + st[1].work_items;
+    }
+    return PCF_OK;
+}
+
 extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_,
                                       const pcf_grid *const *r_, int n_rand, int bins, float dmax,
                                       uint32_t flags, double *dd, double *rr, double *dr,
@@ -41,8 +82,9 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     if (!ctx || !d_ || bins < 1 || !(dmax > 0.f) || n_rand < 0 || (n_rand > 0 && !r_) ||
         (kind != PCF_ISO && kind != PCF_ANI && kind != PCF_BOTH) || (!dd && !rr && !dr))
         return PCF_ERR_INVALID_ARG;
+    if (kind == PCF_BOTH) return batch_both_split(ctx, d_, r_, n_rand, bins, dmax, flags, dd, rr, dr, stats);
     cudaSetDevice(ctx->device);
-    const bool ani = kind != PCF_ISO, both = kind == PCF_BOTH, bpc = (flags & PCF_BPC) != 0;
+    const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0;
     pcf_grid *D = const_cast<pcf_grid *>(d_);
     std::vector<pcf_grid *> R((size_t)n_rand);
     int64_t nmax = D->n;
@@ -82,7 +124,7 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         if ((s = grid_ensure_cells(ctx, j.c, j.P)) != PCF_OK) return s;
         j.cc = j.c->cells;
     }
-    const int nb = both ? bins + bins * bins : ani ? bins * bins : bins;
+    const int nb = ani ? bins * bins : bins;
     bool weighted = !D->unit_weights;
     for (auto *g : R) weighted = weighted || !g->unit_weights;
 
@@ -104,11 +146,10 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     cudaStream_t st = ctx->stream;
     PairLaunch pl;
     pl.ani = ani;
-    pl.both = both;
     pl.bpc = bpc;
     pl.self = false;
     pl.weighted = weighted;
-    pl.rule = make_pair_rule(bins, dmax, flags, ani && !both, bpc, false);
+    pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
     pl.mult = 1.0;
     {
         std::vector<const pcf_grid *> gs(R.begin(), R.end());
@@ -150,11 +191,8 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         std::vector<PairJob> jobs((size_t)nslots);
         std::vector<double> mult((size_t)nslots);
         long long item = 0;
-        // exact-rule flags per job: rule_flags for the first (or only) kind,
-        // rule_flags2 for the anisotropic histogram of a both-kinds launch
-        const bool first_ani = ani && !both;
-        const unsigned rXX = reference_pair_rule(first_ani, bpc, false), rXY = reference_pair_rule(first_ani, bpc, true);
-        const unsigned aXX = reference_pair_rule(true, bpc, false), aXY = reference_pair_rule(true, bpc, true);
+        // exact-rule flags per job
+        const unsigned rXX = reference_pair_rule(ani, bpc, false), rXY = reference_pair_rule(ani, bpc, true);
         for (int k = 0; k < nslots; ++k) {
             const CellGrid &h = *js[k].hc, &c = *js[k].cc;
             const auto &rp = rows[js[k].P];
@@ -171,7 +209,7 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
             const unsigned custom = ((flags & PCF_RULE_EXCL_ZERO) ? PCF_RULE_EXCL : 0u) |
                                     ((flags & PCF_RULE_INCLUSIVE) ? PCF_RULE_LE : 0u);
             j.rule_flags = (flags & PCF_RULE_CUSTOM) ? custom : (js[k].self ? rXX : rXY);
-            j.rule_flags2 = (flags & PCF_RULE_CUSTOM) ? custom : (js[k].self ? aXX : aXY);
+            j.rule_flags2 = 0;  // single-kind jobs
             j.pad = 0;
             j.P = js[k].P;
             item += (long long)h.tiles.size() * j.n_chunks;

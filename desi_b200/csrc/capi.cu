@@ -326,6 +326,32 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
                                           std::max<int64_t>(a->n, cross ? b->n : 0), a->box, dmax));
         if (it != ctx->tune.end()) te = it->second;
     }
+    // Both kinds run as the two single-kind launches written into one layout
+    // unless the autotuner found one pass faster for this call class (a
+    // tuned or forced scheme).  One pass saves the isotropic launch's
+    // candidate tests, but its isotropic copy takes the anisotropic copy's
+    // per-warp scheme, where lanes contend for few hot bins, and its extra
+    // shared memory can cost resident CTAs.  Measured (200k x 32 randoms,
+    // dmax 120, one batch each): exact weights, 40 bins: one pass 273 ms vs
+    // 74 + 146 ms; 48 bins: 500 vs 68 + 267 ms; signed weights (per-warp FP64
+    // copies either way), 40 bins: 381 vs 133 + 216 ms.
+    if (both && te.hist_mode < 0) {
+        pcf_stats si{}, sa{};
+        pcf_status s = count_pairs_impl(ctx, PCF_ISO, a_, b_, bins, dmax, flags, hist,
+                                        stats ? &si : nullptr, 0.0);
+        if (s == PCF_OK)
+            s = count_pairs_impl(ctx, PCF_ANI, a_, b_, bins, dmax, flags, hist + bins,
+                                 stats ? &sa : nullptr, 0.0);
+        if (s == PCF_OK && stats) {
+            stats->pairs = si.pairs + sa.pairs;
+            stats->candidates = si.candidates + sa.candidates;
+            stats->rechecks = si.rechecks + sa.rechecks;
+            stats->kernel_ms = si.kernel_ms + sa.kernel_ms;
+            stats->partitions = sa.partitions;
+            stats->work_items = (int)std::min<int64_t>((int64_t)si.work_items + sa.work_items, INT32_MAX);
+        }
+        return s;
+    }
     int P = 0;
     pcf_status s = prepare_grids(ctx, a, b, dmax, kind, bpc, &P, te.refine);
     if (s != PCF_OK) return s;

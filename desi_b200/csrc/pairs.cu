@@ -892,40 +892,50 @@ static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items,
     return cudaGetLastError();
 }
 
-// Chooses the histogram mode of one launch and starts the kernel.  For a
-// both-kinds launch the mode is the anisotropic copy's; the isotropic copy
-// takes the matching scheme (IsoScheme).
-static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t st,
-                                  int sm_count, int device) {
+// Shared-memory bytes per CTA of histogram scheme hm for launch pl (both
+// kinds: the anisotropic copy plus the isotropic one).
+static size_t scheme_bytes(const PairLaunch &pl, int hm) {
     const int bins = pl.rule.bins;
     const int nb = pl.ani ? bins * bins : bins;
-    const size_t ebytes = pl.weighted ? 8 : 4;
-    auto bytes = [&](int hm) -> size_t {
-        const size_t e = (hm == H_WFIX || hm == H_LFIX) ? 4 : ebytes;
-        size_t w = (size_t)copy_words_host(hm, nb);
-        if (pl.both) w += (size_t)copy_words_host(hm == H_WARP && !pl.weighted ? H_LANE : hm, bins);
-        return w * e * kWarps;
-    };
-    auto fits = [&](int hm) -> bool {
-        if (bins > 255) return hm == H_GLOBAL;
-        switch (hm) {
-        case H_LANE: return !pl.ani && bytes(hm) <= 64 * 1024;
-        case H_LFIX: return !pl.ani && pl.weighted && pl.wfix && bytes(hm) <= 64 * 1024;
-        case H_WFIX: return pl.weighted && pl.wfix && bytes(hm) <= 160 * 1024;
-        case H_WARP: return bytes(hm) <= 160 * 1024;
-        case H_GLOBAL: return true;
-        }
-        return false;
-    };
+    const size_t e = (hm == H_WFIX || hm == H_LFIX) ? 4 : (pl.weighted ? 8 : 4);
+    size_t w = (size_t)copy_words_host(hm, nb);
+    if (pl.both) w += (size_t)copy_words_host(hm == H_WARP && !pl.weighted ? H_LANE : hm, bins);
+    return w * e * kWarps;
+}
+
+static bool scheme_fits(const PairLaunch &pl, int hm) {
+    if (pl.rule.bins > 255) return hm == H_GLOBAL;
+    switch (hm) {
+    case H_LANE: return !pl.ani && scheme_bytes(pl, hm) <= 64 * 1024;
+    case H_LFIX: return !pl.ani && pl.weighted && pl.wfix && scheme_bytes(pl, hm) <= 64 * 1024;
+    case H_WFIX: return pl.weighted && pl.wfix && scheme_bytes(pl, hm) <= 160 * 1024;
+    case H_WARP: return scheme_bytes(pl, hm) <= 160 * 1024;
+    case H_GLOBAL: return true;
+    }
+    return false;
+}
+
+// The histogram scheme of one launch: lane-private copies where they fit
+// (isotropic), else one copy per warp, else global atomics; an autotuned
+// scheme overrides the rule when it is valid for the launch.  For a
+// both-kinds launch the scheme is the anisotropic copy's; the isotropic copy
+// takes the matching scheme (IsoScheme).
+static int pair_scheme(const PairLaunch &pl) {
     int hm;
-    if (bins > 255 || !fits(H_WARP)) hm = H_GLOBAL;
-    else if (pl.weighted && fits(H_LFIX)) hm = H_LFIX;
-    else if (pl.weighted && fits(H_WFIX)) hm = H_WFIX;
-    else if (!pl.weighted && fits(H_LANE)) hm = H_LANE;
+    if (pl.rule.bins > 255 || !scheme_fits(pl, H_WARP)) hm = H_GLOBAL;
+    else if (pl.weighted && scheme_fits(pl, H_LFIX)) hm = H_LFIX;
+    else if (pl.weighted && scheme_fits(pl, H_WFIX)) hm = H_WFIX;
+    else if (!pl.weighted && scheme_fits(pl, H_LANE)) hm = H_LANE;
     else hm = H_WARP;
-    // an autotuned scheme overrides the rule above when it is valid here
-    if (pl.hist_mode >= 0 && pl.hist_mode <= H_LFIX && fits(pl.hist_mode)) hm = pl.hist_mode;
-    const size_t smem = hm == H_GLOBAL ? 0 : bytes(hm);
+    if (pl.hist_mode >= 0 && pl.hist_mode <= H_LFIX && scheme_fits(pl, pl.hist_mode)) hm = pl.hist_mode;
+    return hm;
+}
+
+// Chooses the histogram mode of one launch and starts the kernel.
+static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t st,
+                                  int sm_count, int device) {
+    const int hm = pair_scheme(pl);
+    const size_t smem = hm == H_GLOBAL ? 0 : scheme_bytes(pl, hm);
     // budget: adds one shared counter absorbs between flushes; chunk:
     // candidates per budget check (one chunk alone stays within the budget)
     if (hm == H_WFIX || hm == H_LFIX) {

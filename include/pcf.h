@@ -58,8 +58,10 @@ typedef enum pcf_status {
 } pcf_status;
 
 /* Histogram kinds.  PCF_BOTH (pair counts only): the isotropic and the
- * anisotropic histogram from one pass over the candidate pairs, written as
- * bins doubles (isotropic) followed by bins*bins doubles (anisotropic). */
+ * anisotropic histogram in one call, written as bins doubles (isotropic)
+ * followed by bins*bins doubles (anisotropic).  The call runs the two
+ * single-kind launches, or one pass over the candidate pairs for both kinds
+ * where pcf_autotune_pairs found that faster for the call's class. */
 enum { PCF_ISO = 0, PCF_ANI = 1, PCF_BOTH = 2 };
 
 /* Flags for the counting calls. */

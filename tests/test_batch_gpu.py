@@ -34,6 +34,34 @@ def test_batch_equals_per_call(ctx, ani, bpc, w, graph):
             cmp(at(dr, i), ctx.count_pairs(gd, g, bins=bins, dmax=dmax, ani=ani, bpc=bpc))
 
 
+@pytest.mark.parametrize("w", ["uniform", "signed"])
+def test_batch_both_kinds(ctx, w):
+    """ani="both" in a batch equals the single-kind per-call histograms, for
+    exact (fixed-point) and signed (FP64) weights.  The batch runs as two
+    single-kind batches (work_items: one per job slot of each)."""
+    box, bins, dmax = 300.0, 16, 40.0
+    rng = np.random.default_rng(80)
+    def wts(P):
+        if w == "signed":
+            P = P.copy()
+            P[:, 3] = rng.uniform(-1.0, 1.0, len(P)).astype(np.float32)
+        return P
+    D = wts(catalog.neyman_scott(3000, box, seed=81, weights="uniform"))
+    Rs = [wts(catalog.uniform(n, box, seed=82 + i, weights="uniform")) for i, n in enumerate([2500, 400, 5000])]
+    gd = ctx.grid(D, box)
+    grs = [ctx.grid(R, box) for R in Rs]
+    (dd, rr, dr), st = ctx.batch_pairs(gd, grs, bins=bins, dmax=dmax, ani="both", bpc=True, stats=True)
+    slots = 1 + 2 * len(grs)
+    assert st["work_items"] == 2 * slots
+    def cmp(a, b):
+        assert np.all(np.abs(a - b) <= 1e-12 * (np.abs(b) + (1.0 if w == "signed" else 0.0)))
+    for k, is_ani in enumerate((False, True)):
+        cmp(dd[k], ctx.count_pairs(gd, None, bins=bins, dmax=dmax, ani=is_ani, bpc=True))
+        for i, g in enumerate(grs):
+            cmp(rr[k][i], ctx.count_pairs(g, None, bins=bins, dmax=dmax, ani=is_ani, bpc=True))
+            cmp(dr[k][i], ctx.count_pairs(gd, g, bins=bins, dmax=dmax, ani=is_ani, bpc=True))
+
+
 def test_autotune_and_estimator(ctx, tmp_path):
     import oracle
     box, bins, dmax = 250.0, 30, 80.0

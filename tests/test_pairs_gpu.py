@@ -241,13 +241,15 @@ def test_every_histogram_scheme(tmp_path, w, ani):
 
 @pytest.mark.parametrize("w", ["unit", "uniform", "signed"])
 @pytest.mark.parametrize("bpc", [False, True])
-def test_both_kinds_one_pass(ctx, w, bpc):
-    """ani="both": the isotropic and anisotropic histograms from one pass over
-    the candidates equal the two single-kind calls (bit-exact for unit
-    weights, 1e-12 for weights; the FP64 fallback for signed weights) and the
-    oracle."""
+@pytest.mark.parametrize("bins", [30, 48])
+def test_both_kinds(ctx, w, bpc, bins):
+    """ani="both": the isotropic and anisotropic histograms equal the two
+    single-kind calls (bit-exact for unit weights, 1e-12 for weights; the FP64
+    fallback for signed weights) and the oracle.  Untuned, the call runs the
+    two single-kind launches; the one-pass kernel (a tuned scheme) is covered
+    by test_every_histogram_scheme."""
     rng = np.random.default_rng(23)
-    box, bins, dmax = 250.0, 30, 80.0
+    box, dmax = 250.0, 80.0
     D = catalog.neyman_scott(2600, box, seed=51, weights="uniform" if w != "unit" else "unit")
     R = catalog.uniform(2700, box, seed=52, weights="uniform" if w != "unit" else "unit")
     if w == "signed":
