@@ -156,12 +156,19 @@ def tune_step(ctx, D, R, candidates=(8, 9, 10, 12, 14, 16)):
                 best = (tot, P, fused, modes)
         gd.free()
         gr.free()
-    # the tuning table keeps the last candidate's schemes: tune again at the winner
+    # the tuning table keeps the last candidate's schemes: tune again at the
+    # winner.  A both-kinds call tuned to the default rule (-1) runs the two
+    # single-kind launches, so it needs their entries too; if every one of
+    # the three chose that, the step is the single-kind form.
     _, P, fused, modes = best
+    if fused and all(m < 0 for m in modes.values()):
+        fused = False
     gd, gr = ctx.grid(D, W["box"], partitions=P), ctx.grid(R, W["box"], partitions=P)
-    for ani in (("both",) if fused else (False, True)):
-        for a, b in ((gd, None), (gr, None), (gd, gr)):
-            ctx.autotune_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True)
+    modes = {}
+    for ani in ((False, True, "both") if fused else (False, True)):
+        for name, (a, b) in (("DD", (gd, None)), ("RR", (gr, None)), ("DR", (gd, gr))):
+            r = ctx.autotune_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True)
+            modes[name + ("both" if ani == "both" else ("ani" if ani else "iso"))] = r["hist_mode"]
     gd.free()
     gr.free()
     return P, fused, modes

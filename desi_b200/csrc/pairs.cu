@@ -193,10 +193,14 @@ __device__ __noinline__ int slow_slot(float hx, float hy, float hz, float cx, fl
 }
 
 // Shared-memory words (of the copy's element type) of one warp's copy.
-// Per-warp copies end with 32 dummy slots, one per lane (never flushed).
+// Per-warp copies end with a dummy region (never flushed) where each lane
+// has its own word: 32 words, or for fixed-point limbs 32 + 2, lane l's
+// three limbs at words l, l+1, l+2 of the region (one limb per reduction
+// instruction, so the lanes of one instruction never share a word; the adds
+// there are of 0).
 template <int HM>
 __host__ __device__ __forceinline__ int copy_words(int nb) {
-    return HM == H_LANE ? nb * 32 : HM == H_WARP ? nb + 32 : HM == H_WFIX ? (nb + 32) * kLimbs
+    return HM == H_LANE ? nb * 32 : HM == H_WARP ? nb + 32 : HM == H_WFIX ? nb * kLimbs + 32 + kLimbs - 1
          : HM == H_LFIX ? nb * kLimbs * 32 : 0;
 }
 
@@ -299,7 +303,7 @@ __device__ __forceinline__ void setup_sink(Sink<WEIGHTED, HM> &sk, unsigned ms, 
         break;
     case H_WFIX:
         sk.base = ms - bias * (kLimbs * 4u);
-        sk.dummy = ms + (unsigned)(nb + lane) * (kLimbs * 4u);
+        sk.dummy = ms + (unsigned)(nb * kLimbs + lane) * 4u;
         break;
     case H_LFIX: sk.base = ms + lane * 4u - bias * (kLimbs * 128u); sk.dummy = ms + lane * 4u; break;
     default: sk.base = sk.dummy = 0u;
