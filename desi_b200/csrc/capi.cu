@@ -378,7 +378,7 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
         set_weight_fix(pl, gs, 2);
         pl.wunscale = weight_unscale(a, cross ? b : a);
     }
-    pl.count = stats != nullptr;
+    pl.count = stats != nullptr && !ctx->tune_timing;
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
                      d_stats);
     if (s != PCF_OK) return s;

@@ -205,6 +205,8 @@ struct pcf_ctx {
     std::shared_ptr<MemPool> pool = std::make_shared<MemPool>();
     std::map<std::string, TuneEntry> tune;
     TuneEntry tune_override;  // set while the autotuner times a candidate
+    bool tune_timing = false; // autotuner: statistics carry kernel time only (no pair
+                              // counting), so candidates run the kernels a plain call runs
     PlanSlot slots[2];
     int slot = 0;
     // optional kernel-time log (pcf_ctx_profile)

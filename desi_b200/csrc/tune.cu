@@ -38,6 +38,7 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
     float default_ms = 0.f;
     int tried = 0;
     ctx->tune.erase(key);
+    ctx->tune_timing = true;
     for (int r : refines) {
         // partitions fixed by the caller: tune the histogram scheme only
         if ((a->user_P > 0 || (b && b->user_P > 0)) && r != 0) continue;
@@ -50,9 +51,10 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
                 pcf_stats st{};
                 pcf_status s = pcf_count_pairs(ctx, kind, a, b, bins, dmax, flags | PCF_DEVICE_OUT,
                                                out.as<double>(), &st);
+                if (s == PCF_ERR_UNSUPPORTED) { ms = 1e30f; break; }
                 if (s != PCF_OK) {
                     ctx->tune_override = TuneEntry();
-                    if (s == PCF_ERR_UNSUPPORTED) { ms = 1e30f; break; }
+                    ctx->tune_timing = false;
                     return s;
                 }
                 ms = std::min(ms, st.kernel_ms);
@@ -67,6 +69,7 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
         }
     }
     ctx->tune_override = TuneEntry();
+    ctx->tune_timing = false;
     ctx->tune[key] = best;
     if (res) {
         res->refine = best.refine;
