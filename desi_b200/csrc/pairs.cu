@@ -54,8 +54,11 @@ constexpr unsigned kBinBias = 0x43800000u >> kFracBits;
 // Histogram privatisation.  H_LANE: a u32 (or FP64) column per lane (iso);
 // H_WARP: one copy per warp with shared atomics; H_GLOBAL: global atomics
 // (very wide histograms); H_WFIX: per-warp fixed-point limbs (weighted);
-// H_LFIX: per-lane fixed-point limbs (weighted iso).
-enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3, H_LFIX = 4 };
+// H_LFIX: per-lane fixed-point limbs (weighted iso); H_WFIX4: per-warp
+// fixed-point limbs in four sub-copies, lane l adding to copy l % 4 (the
+// isotropic copy of a weighted both-kinds launch: its few bins would
+// otherwise take the reductions of all 32 lanes).
+enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3, H_LFIX = 4, H_WFIX4 = 5 };
 constexpr int kLimbs = 3;
 // Candidate steps between recheck votes, per kind: the anisotropic (and
 // both-kinds) kernels carry more live state per step and schedule better
@@ -135,7 +138,7 @@ __device__ __forceinline__ void red_s_limbs(unsigned a, unsigned long long v) {
 // float w (FP64 modes) or nothing (unit weights).
 template <bool WEIGHTED, int HM>
 struct WT {
-    typedef typename std::conditional<(HM == H_WFIX || HM == H_LFIX), unsigned, float>::type type;
+    typedef typename std::conditional<(HM == H_WFIX || HM == H_LFIX || HM == H_WFIX4), unsigned, float>::type type;
 };
 
 // Histogram sink of one lane.  Slots arrive biased (see kBinBias); `base`
@@ -153,7 +156,7 @@ struct Sink {
         if (HM == H_LFIX) {
             red_s_limbs<128>(pred ? base + sb * (kLimbs * 128u) : dummy,
                              (unsigned long long)(pred ? wa : 0u) * wb);
-        } else if (HM == H_WFIX) {
+        } else if (HM == H_WFIX || HM == H_WFIX4) {
             red_s_limbs<4>(pred ? base + sb * (kLimbs * 4u) : dummy,
                            (unsigned long long)(pred ? wa : 0u) * wb);
         } else if (HM == H_LANE) {
@@ -201,7 +204,7 @@ __device__ __noinline__ int slow_slot(float hx, float hy, float hz, float cx, fl
 template <int HM>
 __host__ __device__ __forceinline__ int copy_words(int nb) {
     return HM == H_LANE ? nb * 32 : HM == H_WARP ? nb + 32 : HM == H_WFIX ? nb * kLimbs + 32 + kLimbs - 1
-         : HM == H_LFIX ? nb * kLimbs * 32 : 0;
+         : HM == H_WFIX4 ? 4 * nb * kLimbs + 32 + kLimbs - 1 : HM == H_LFIX ? nb * kLimbs * 32 : 0;
 }
 
 // Adds this warp's copy (nb bins) into the launch's accumulators at `off`
@@ -251,6 +254,23 @@ __device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, si
                 atomicAdd(A.g_wsum + off + k, v * unscale);
             }
         }
+    } else if (HM == H_WFIX4) {  // [copy][bin][limb]: limbs summed exactly over the copies
+        unsigned *mine = static_cast<unsigned *>(mine_v);
+        for (int k = lane; k < nb; k += 32) {
+            unsigned long long s0 = 0, s1 = 0, s2 = 0;
+            #pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                unsigned *c = mine + (q * nb + k) * kLimbs;
+                s0 += c[0];
+                s1 += c[1];
+                s2 += c[2];
+                c[0] = c[1] = c[2] = 0u;
+            }
+            if (s0 | s1 | s2) {  // each term exact (< 2^53); the sum rounds at most twice
+                const double v = (double)s2 * 0x1p32 + ((double)s1 * 0x1p16 + (double)s0);
+                atomicAdd(A.g_wsum + off + k, v * unscale);
+            }
+        }
     } else if (HM == H_LFIX) {  // [bin][limb][lane]
         unsigned *mine = static_cast<unsigned *>(mine_v);
         for (int k = 0; k < nb; ++k) {
@@ -281,17 +301,21 @@ struct MinBlocks {
 // isotropic one).
 enum { K_ISO = 0, K_ANI = 1, K_BOTH = 2 };
 // Scheme of the isotropic copy of a K_BOTH launch, given the anisotropic one:
-// lane-private counts, else per-warp copies of the same element type.
+// lane-private counts, four per-warp fixed-point sub-copies, else per-warp
+// copies of the same element type.
+__host__ __device__ constexpr int iso_scheme(bool weighted, int hm) {
+    return hm == H_WARP ? (weighted ? H_WARP : H_LANE) : hm == H_WFIX ? H_WFIX4 : hm;
+}
 template <bool WEIGHTED, int HM>
 struct IsoScheme {
-    static constexpr int value = HM == H_WARP ? (WEIGHTED ? H_WARP : H_LANE) : HM;
+    static constexpr int value = iso_scheme(WEIGHTED, HM);
 };
 
 // Sets up one lane's sink over a copy at shared address ms (see Sink).
 template <bool WEIGHTED, int HM>
 __device__ __forceinline__ void setup_sink(Sink<WEIGHTED, HM> &sk, unsigned ms, void *mine, int lane,
                                            unsigned bias, int nb) {
-    typedef typename std::conditional<WEIGHTED && !(HM == H_WFIX || HM == H_LFIX), double, unsigned>::type HT;
+    typedef typename std::conditional<WEIGHTED && !(HM == H_WFIX || HM == H_LFIX || HM == H_WFIX4), double, unsigned>::type HT;
     sk.bias = bias;
     sk.lane_col = reinterpret_cast<double *>(mine) + lane;
     sk.gbase = nullptr;
@@ -304,6 +328,10 @@ __device__ __forceinline__ void setup_sink(Sink<WEIGHTED, HM> &sk, unsigned ms, 
     case H_WFIX:
         sk.base = ms - bias * (kLimbs * 4u);
         sk.dummy = ms + (unsigned)(nb * kLimbs + lane) * 4u;
+        break;
+    case H_WFIX4:
+        sk.base = ms + (unsigned)((lane & 3) * nb * kLimbs) * 4u - bias * (kLimbs * 4u);
+        sk.dummy = ms + (unsigned)(4 * nb * kLimbs + lane) * 4u;
         break;
     case H_LFIX: sk.base = ms + lane * 4u - bias * (kLimbs * 128u); sk.dummy = ms + lane * 4u; break;
     default: sk.base = sk.dummy = 0u;
@@ -850,6 +878,7 @@ static int copy_words_host(int hm, int nb) {
     case H_WARP: return copy_words<H_WARP>(nb);
     case H_WFIX: return copy_words<H_WFIX>(nb);
     case H_LFIX: return copy_words<H_LFIX>(nb);
+    case H_WFIX4: return copy_words<H_WFIX4>(nb);
     }
     return 0;
 }
@@ -903,7 +932,7 @@ static size_t scheme_bytes(const PairLaunch &pl, int hm) {
     const int nb = pl.ani ? bins * bins : bins;
     const size_t e = (hm == H_WFIX || hm == H_LFIX) ? 4 : (pl.weighted ? 8 : 4);
     size_t w = (size_t)copy_words_host(hm, nb);
-    if (pl.both) w += (size_t)copy_words_host(hm == H_WARP && !pl.weighted ? H_LANE : hm, bins);
+    if (pl.both) w += (size_t)copy_words_host(iso_scheme(pl.weighted, hm), bins);
     return w * e * kWarps;
 }
 
