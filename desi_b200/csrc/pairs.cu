@@ -365,6 +365,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
     constexpr bool FIX = HM == H_WFIX || HM == H_LFIX;
     constexpr bool DO_I = KIND != K_ANI, DO_A = KIND != K_ISO;
     constexpr int kGroup = KIND == K_ISO ? PCF_GROUP_ISO : PCF_GROUP_ANI;
+    constexpr bool kPrefetch = KIND == K_BOTH && HM == H_WFIX;  // measured: helps only here
     constexpr int HMI = KIND == K_BOTH ? IsoScheme<WEIGHTED, HM>::value : HM;
     typedef typename WT<WEIGHTED, HM>::type W;
     typedef typename std::conditional<WEIGHTED && !FIX, double, unsigned>::type HT;
@@ -684,12 +685,40 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
                         const bool v0 = p > jmin, v1 = (p + 1 < b) && (p + 1 > jmin);
                         settle(core(p, v0, v1), p, 1, v0, v1);
                     }
-                    // body: kGroup steps per vote
-                    for (; p + (kGroup - 1) * stride + 1 < hi_i; p += kGroup * stride) {
-                        bool any = false;
+                    // body: kGroup steps per vote.  In the fixed-point
+                    // both-kinds pass (register room at four CTAs per SM) the
+                    // next group's candidates are loaded before this group is
+                    // evaluated, so their latency overlaps this group's
+                    // arithmetic and the vote; the single-kind fixed-point
+                    // kernels ran 4-6% slower that way.
+                    if (!kPrefetch) {
+                        for (; p + (kGroup - 1) * stride + 1 < hi_i; p += kGroup * stride) {
+                            bool any = false;
+                            #pragma unroll
+                            for (int k = 0; k < kGroup; ++k) any |= core(p + k * stride, true, true);
+                            settle(any, p, kGroup, true, true);
+                        }
+                    } else if (p + (kGroup - 1) * stride + 1 < hi_i) {
+                        Raw nx[kGroup];
                         #pragma unroll
-                        for (int k = 0; k < kGroup; ++k) any |= core(p + k * stride, true, true);
-                        settle(any, p, kGroup, true, true);
+                        for (int k = 0; k < kGroup; ++k) nx[k] = load(p + k * stride);
+                        for (;;) {
+                            Raw cur[kGroup];
+                            #pragma unroll
+                            for (int k = 0; k < kGroup; ++k) cur[k] = nx[k];
+                            const int pn = p + kGroup * stride;
+                            const bool more = pn + (kGroup - 1) * stride + 1 < hi_i;
+                            if (more) {
+                                #pragma unroll
+                                for (int k = 0; k < kGroup; ++k) nx[k] = load(pn + k * stride);
+                            }
+                            bool any = false;
+                            #pragma unroll
+                            for (int k = 0; k < kGroup; ++k) any |= core_raw(cur[k], true, true);
+                            settle(any, p, kGroup, true, true);
+                            p = pn;
+                            if (!more) break;
+                        }
                     }
                     for (; p + 1 < hi_i; p += stride) settle(core(p, true, true), p, 1, true, true);
                     if (p < hi_i) settle(core(p, true, false), p, 1, true, false);
