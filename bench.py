@@ -133,7 +133,7 @@ def replica_throughput(world: int, units_per_step: float, steps: int, max_total_
     return world * units_per_step * steps / (max_total_ms * 1e-3)
 
 
-def tune_step(ctx, D, R, candidates=(8, 9, 10, 12, 14, 16)):
+def tune_step(ctx, D, R, candidates=(8, 9, 10, 11, 12, 13, 14, 16)):
     """Untimed: the partition count of the step (one for all six histograms,
     so the grids are built once per step), whether the isotropic and
     anisotropic histograms of a catalog pair come from one pass (kind
