@@ -483,30 +483,44 @@ def run_batched(ctx, torch, stream):
 
 def run_served(n_requests=40, load=0.7):
     """A seeded stream of mixed 2iso / 2ani / 3iso requests through the
-    continuous-batching server with 4 slots (desi_b200.serve).  First the
-    requests run closed-loop (all submitted at once) to measure capacity in
-    requests/s; then the same requests arrive as a Poisson stream at `load`
-    times that capacity: latency p50 / p99 and pairs/s of that pass."""
+    continuous-batching server with 4 slots (desi_b200.serve).  One server
+    serves every pass of the same requests, its resident grids dropped
+    before each (every request grids its catalogs from host memory; the
+    slots' memory pools stay warm, as in a long-running server): a discarded
+    warm-up pass, three closed-loop passes (all submitted at once) whose
+    median measures capacity in requests/s, and three passes with Poisson
+    arrivals at `load` times that capacity.  Reported: the Poisson pass with
+    the median p99 (latency p50 / p99, pairs/s), and every pass's figures
+    (single passes are occasionally slowed by host-side stalls of ~0.3-1 s)."""
     from desi_b200 import serve
 
+    cats, _ = serve.make_stream(n_requests, rate_hz=1.0)
+    srv = serve.PcfServer(slots=4)
+    for k, (p, box) in cats.items():
+        srv.register(k, p, box)
+
     def one_pass(rate_hz):
-        cats, reqs = serve.make_stream(n_requests, rate_hz=rate_hz or 1.0)
+        _, reqs = serve.make_stream(n_requests, rate_hz=rate_hz or 1.0)
         if rate_hz is None:
             for r in reqs:
                 r.arrival = 0.0
-        srv = serve.PcfServer(slots=4)
-        for k, (p, box) in cats.items():
-            srv.register(k, p, box)
-        try:
-            rep = srv.run_stream(reqs)
-        finally:
-            srv.close()
+        srv.drop_grids()
+        rep = srv.run_stream(reqs)
         rep.pop("results")
         return rep
 
-    closed = one_pass(None)
-    capacity = n_requests / closed["wall_s"]
-    rep = one_pass(load * capacity)
+    try:
+        one_pass(None)  # warm-up, discarded: pool allocations, first kernel launches
+        walls = sorted(one_pass(None)["wall_s"] for _ in range(3))
+        capacity = n_requests / walls[1]
+        reps = sorted((one_pass(load * capacity) for _ in range(3)),
+                      key=lambda r: r["latency_ms"]["p99"])
+        rep = dict(reps[1])
+        rep["passes"] = [{"p50_ms": r["latency_ms"]["p50"], "p99_ms": r["latency_ms"]["p99"],
+                          "wall_s": r["wall_s"]} for r in reps]
+        rep["closed_loop_wall_s"] = walls
+    finally:
+        srv.close()
     rep["capacity_req_per_s"] = capacity
     rep["rate_hz"] = load * capacity
     rep["workload"] = (f"{n_requests} requests, Poisson at {load:.0%} of the closed-loop capacity, "

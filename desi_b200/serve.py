@@ -190,6 +190,16 @@ class PcfServer:
                     self._in_use -= fp
                     self._lock.notify_all()
 
+    def drop_grids(self) -> None:
+        """Frees every slot's resident grids (their device memory returns to
+        the slot's pool, so rebuilding them allocates nothing).  Call while
+        no request runs."""
+        for s in self.slots:
+            for g, _ in s.cache.values():
+                g.free()
+            s.cache.clear()
+            s.used = 0
+
     def close(self) -> None:
         with self._lock:
             self._stop = True

@@ -61,3 +61,20 @@ def test_admission_by_footprint_serialises_but_completes():
             assert s1 >= e0  # never two at once
     finally:
         srv.close()
+
+
+def test_dropped_grids_rebuild_to_the_same_result():
+    """drop_grids frees the resident grids; the next pass grids the catalogs
+    again (from the slots' pools) and returns identical histograms."""
+    srv = _server(2)
+    try:
+        first = srv.run_stream(_requests()[:5])["results"]
+        assert any(s.cache for s in srv.slots)
+        srv.drop_grids()
+        assert all(not s.cache and s.used == 0 for s in srv.slots)
+        again = srv.run_stream(_requests()[:5])["results"]
+    finally:
+        srv.close()
+    for a, b in zip(first, again):
+        for k in a:
+            assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
