@@ -267,3 +267,39 @@ def test_both_kinds(ctx, w, bpc, bins):
             else:
                 _cmp(got, want, w != "unit")
                 _cmp(got, single, w != "unit")
+
+
+@pytest.mark.parametrize("w", ["uniform", "signed"])
+@pytest.mark.parametrize("bins", [30, 48])
+def test_both_kinds_forced_one_pass(tmp_path, w, bins):
+    """A both-kinds call tuned to one pass (exact weights: per-warp limbs with
+    the isotropic copy in four sub-copies and the next candidate group loaded
+    ahead; signed weights: per-warp FP64 sums) equals the two single-kind
+    calls and the oracle (1e-12; the signed sums with an absolute floor)."""
+    from desi_b200 import api
+    rng = np.random.default_rng(29)
+    box, dmax, n = 250.0, 80.0, 2400
+    D = catalog.neyman_scott(n, box, seed=61, weights="uniform")
+    R = catalog.uniform(n + 90, box, seed=62, weights="uniform")
+    if w == "signed":
+        D, R = _weighted(D, rng, "signed"), _weighted(R, rng, "signed")
+    mode = 3 if w == "uniform" else 1
+    path = str(tmp_path / "tune.txt")
+    with open(path, "w") as f:
+        for cross in (False, True):
+            f.write(f"{_tune_key('both', True, cross, True, bins, n + 90 if cross else n, box, dmax)} 0 {mode} 1.0\n")
+    c = api.Context(0)
+    try:
+        c.tune_load(path)
+        gd, gr = c.grid(D, box), c.grid(R, box)
+        for (a, b, A, B) in ((gd, None, D, None), (gd, gr, D, R)):
+            (iso, ani), st = c.count_pairs(a, b, bins=bins, dmax=dmax, ani="both", bpc=True, stats=True)
+            assert st["work_items"] > 0
+            for got, is_ani in ((iso, False), (ani, True)):
+                single = c.count_pairs(a, b, bins=bins, dmax=dmax, ani=is_ani, bpc=True)
+                want = oracle.pairs(A, B, box=box, bins=bins, dmax=dmax, ani=is_ani, bpc=True)
+                floor = 1.0 if w == "signed" else 0.0
+                assert np.all(np.abs(got - want) <= RTOL_W * (np.abs(want) + floor))
+                assert np.all(np.abs(got - single) <= RTOL_W * (np.abs(single) + floor))
+    finally:
+        c.close()
