@@ -490,8 +490,7 @@ def run_served(n_requests=40, load=0.7):
     warm-up pass, three closed-loop passes (all submitted at once) whose
     median measures capacity in requests/s, and three passes with Poisson
     arrivals at `load` times that capacity.  Reported: the Poisson pass with
-    the median p99 (latency p50 / p99, pairs/s), and every pass's figures
-    (single passes are occasionally slowed by host-side stalls of ~0.3-1 s)."""
+    the median p99 (latency p50 / p99, pairs/s), and every pass's figures."""
     from desi_b200 import serve
 
     cats, _ = serve.make_stream(n_requests, rate_hz=1.0)

@@ -6,8 +6,11 @@ library context (its own CUDA stream and memory pool) and its own cache of
 gridded catalogs resident in HBM (LRU by bytes).  A request is admitted as
 soon as a slot is free *and* its HBM footprint fits the budget -- requests
 that arrive while others run start immediately on another slot, so their
-kernels overlap on the device (continuous batching, not a queue).  The
-library calls release the GIL (ctypes), so slots run concurrently.
+kernels overlap on the device (continuous batching, not a queue).  When
+several requests wait, a free slot takes the one with the least expected
+work (in-range pairs at uniform density), unless one has waited longer than
+``max_wait_s``.  The library calls release the GIL (ctypes), so slots run
+concurrently.
 
 Every result is computed by the same kernels whether a request runs alone
 or in the mix; ``tests/test_serve.py`` checks that the histograms are
@@ -53,6 +56,19 @@ def grid_bytes(n: int, partitions: int = 64) -> int:
     """Device bytes of one gridded catalog: raw copy, cell-ordered SoA planes,
     pair-packed copy and integer weights, cell table and tiles (upper bound)."""
     return n * (16 + 16 + 16) + 4 * (partitions ** 3 + 1) + 16 * n + (1 << 20)
+
+
+def request_work(req: Request, sizes: dict, boxes: dict) -> float:
+    """Expected candidate work of a request (its scheduling cost): in-range
+    pairs of DD + RR + DR at uniform density, times the expected neighbours
+    of a point for 3iso (triangles per pair)."""
+    nd, nr = sizes[req.data], sizes[req.rand]
+    box = boxes[req.data]
+    frac = (2.0 if req.kind == "2ani" else 4.0 / 3.0) * math.pi * req.dmax ** 3 / box ** 3
+    pairs = 0.5 * (nd * nd + nr * nr) * frac + nd * nr * frac
+    if req.kind == "3iso":
+        pairs *= max(nd, nr) * 4.0 / 3.0 * math.pi * req.dmax ** 3 / box ** 3
+    return pairs
 
 
 def request_bytes(req: Request, sizes: dict) -> int:
@@ -120,9 +136,12 @@ class _Slot:
 
 class PcfServer:
     def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int | None = None,
-                 cache_bytes: int = 8 << 30):
+                 cache_bytes: int = 8 << 30, max_wait_s: float = 0.05):
         """hbm_budget: bytes the running requests may hold at once (default:
-        half the free device memory); cache_bytes: resident grids per slot."""
+        half the free device memory); cache_bytes: resident grids per slot;
+        max_wait_s: a pending request older than this runs before shorter
+        ones (bounds the wait that shortest-first scheduling adds)."""
+        self.max_wait_s = max_wait_s
         if hbm_budget is None:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
@@ -141,7 +160,12 @@ class PcfServer:
 
     # -- catalogs ----------------------------------------------------------
     def register(self, name: str, points: np.ndarray, box: float) -> None:
-        self.catalogs[name] = {"points": api.as_points(points), "box": float(box)}
+        """Keeps the catalog in page-locked host memory, so a slot's grid
+        build copies it by DMA without staging it through the CPU."""
+        import torch
+        pts = api.as_points(points)
+        pinned = torch.from_numpy(pts).pin_memory()
+        self.catalogs[name] = {"points": pinned.numpy(), "box": float(box), "_pinned": pinned}
 
     # -- requests ----------------------------------------------------------
     def submit(self, req: Request) -> Future:
@@ -159,6 +183,31 @@ class PcfServer:
         need = request_bytes(req, sizes)
         return self._in_use + need <= self.hbm_budget or self._in_use == 0
 
+    def _pick(self) -> Request | None:
+        """Removes and returns the next request to run: among the admissible
+        pending requests, one that has waited longer than max_wait_s (the
+        oldest), else the one with the least expected work, so small
+        requests do not queue behind large ones (shortest job first with an
+        age bound).  Caller holds the lock."""
+        now = time.perf_counter()
+        best, best_i, best_cost = None, -1, None
+        sizes = boxes = None
+        for i, r in enumerate(self._pending):
+            if not self._admissible(r):
+                continue
+            if now - r.t_submit > self.max_wait_s:
+                best, best_i = r, i
+                break
+            if sizes is None:
+                sizes = {k: len(v["points"]) for k, v in self.catalogs.items()}
+                boxes = {k: v["box"] for k, v in self.catalogs.items()}
+            cost = request_work(r, sizes, boxes)
+            if best_cost is None or cost < best_cost:
+                best, best_i, best_cost = r, i, cost
+        if best is not None:
+            del self._pending[best_i]
+        return best
+
     def _worker(self, slot: _Slot) -> None:
         while True:
             with self._lock:
@@ -166,11 +215,7 @@ class PcfServer:
                 while req is None:
                     if self._stop:
                         return
-                    for i, r in enumerate(self._pending):  # first admissible, in order
-                        if self._admissible(r):
-                            req = r
-                            del self._pending[i]
-                            break
+                    req = self._pick()
                     if req is None:
                         self._lock.wait(0.05)
                 sizes = {k: len(v["points"]) for k, v in self.catalogs.items()}

@@ -78,3 +78,4 @@ def test_dropped_grids_rebuild_to_the_same_result():
     for a, b in zip(first, again):
         for k in a:
             assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+
