@@ -50,6 +50,10 @@ pcf_status pcf_ctx_create(int device, pcf_ctx **out) {
         return PCF_ERR_CUDA;
     }
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (pcf_ensure_pinned(c, (size_t)2 << 20) != PCF_OK) {  // result staging (grows on demand)
+        pcf_ctx_destroy(c);
+        return PCF_ERR_NO_MEMORY;
+    }
     *out = c;
     return PCF_OK;
 }
@@ -385,22 +389,26 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     const bool dev_out = (flags & PCF_DEVICE_OUT) != 0;
     s = finalize_hist(ctx, d_cnt, d_ws, pl.weighted, pl.mult, nb, dev_out ? hist : d_out);
     if (s != PCF_OK) return s;
-    if (!dev_out)
-        PCF_CU(ctx, cudaMemcpyAsync(hist, d_out, sizeof(double) * nb, cudaMemcpyDeviceToHost,
-                                    ctx->stream));
     if (stats || !dev_out) {
-        unsigned long long hs[4] = {0, 0, 0, 0};
-        PCF_CU(ctx, cudaMemcpyAsync(hs, d_stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
-        std::vector<unsigned long long> cnt;
-        if (stats && !pl.weighted) {  // unit weights: pairs = sum of the counts
-            cnt.resize(nb);
-            PCF_CU(ctx, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(unsigned long long) * nb,
-                                        cudaMemcpyDeviceToHost, ctx->stream));
-        }
+        // results come back through the context's page-locked buffer: copies
+        // into pageable memory go through the driver's staging, where the
+        // request server's concurrent slots were seen to stall one another
+        const size_t hb = dev_out ? 0 : sizeof(double) * nb;
+        const size_t cb = (stats && !pl.weighted) ? sizeof(unsigned long long) * nb : 0;
+        s = pcf_ensure_pinned(ctx, hb + cb + 64);
+        if (s != PCF_OK) return s;
+        char *hp = static_cast<char *>(ctx->h_pinned);
+        if (hb) PCF_CU(ctx, cudaMemcpyAsync(hp, d_out, hb, cudaMemcpyDeviceToHost, ctx->stream));
+        if (cb) PCF_CU(ctx, cudaMemcpyAsync(hp + hb, d_cnt, cb, cudaMemcpyDeviceToHost, ctx->stream));
+        PCF_CU(ctx, cudaMemcpyAsync(hp + hb + cb, d_stats, 32, cudaMemcpyDeviceToHost, ctx->stream));
         PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
-        if (!cnt.empty()) {
+        if (hb) memcpy(hist, hp, hb);
+        unsigned long long hs[4];
+        memcpy(hs, hp + hb + cb, sizeof(hs));
+        if (cb) {  // unit weights: pairs = sum of the counts
+            const unsigned long long *cnt = reinterpret_cast<const unsigned long long *>(hp + hb);
             hs[2] = 0;
-            for (auto c : cnt) hs[2] += c;
+            for (int q = 0; q < nb; ++q) hs[2] += cnt[q];
         }
         if (stats) {
             float ms = 0.f;

@@ -19,9 +19,12 @@
 
 #include "pcf_internal.cuh"
 
+// The smallest cached block that holds n bytes is reused if it is at most
+// 8n + 1 MB: a cudaMalloc can stall other threads' work on the device (the
+// request server's slots), so a moderately oversized block beats a new one.
 cudaError_t MemPool::get(size_t n, void **p, size_t *got) {
     auto it = free_blocks.lower_bound(n);
-    if (it != free_blocks.end() && it->first <= 2 * n + 4096) {
+    if (it != free_blocks.end() && it->first <= 8 * n + (1u << 20)) {
         *p = it->second;
         *got = it->first;
         cached -= it->first;
@@ -307,9 +310,14 @@ pcf_status pcf_fail(pcf_ctx *ctx, cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? PCF_ERR_NO_MEMORY : PCF_ERR_CUDA;
 }
 
+// The context's page-locked staging buffer, grown to at least `bytes`.  A
+// copy queued from it may still be in flight: growing waits for the stream.
 pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes) {
     if (ctx->h_pinned_bytes >= bytes) return PCF_OK;
-    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->h_pinned) {
+        PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        cudaFreeHost(ctx->h_pinned);
+    }
     ctx->h_pinned = nullptr;
     ctx->h_pinned_bytes = 0;
     size_t want = std::max<size_t>(bytes, 1 << 20);
@@ -383,13 +391,20 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
                                        cg->qw.as<unsigned>(), flags, st);
     PCF_CU(ctx, cudaGetLastError());
     if (pg1) PCF_CU(ctx, cudaEventRecord(pg1, st));
-    cg->h_start.resize((size_t)(ncell + 1));
-    unsigned hf[3] = {0u, 0u, 0u};
-    PCF_CU(ctx, cudaMemcpyAsync(cg->h_start.data(), cg->cell_start.p, sizeof(int) * (ncell + 1),
-                                cudaMemcpyDeviceToHost, st));
-    PCF_CU(ctx, cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
-    const int hflags = (int)hf[0];
+    // cell table and flags come back through the context's page-locked
+    // buffer (pageable copies go through the driver's staging, where
+    // concurrent contexts were seen to stall one another)
+    const size_t sb = sizeof(int) * (size_t)(ncell + 1);
+    pcf_status ps = pcf_ensure_pinned(ctx, sb + 64);
+    if (ps != PCF_OK) return ps;
+    char *hp = static_cast<char *>(ctx->h_pinned);
+    PCF_CU(ctx, cudaMemcpyAsync(hp, cg->cell_start.p, sb, cudaMemcpyDeviceToHost, st));
+    PCF_CU(ctx, cudaMemcpyAsync(hp + sb, flags, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     PCF_CU(ctx, cudaStreamSynchronize(st));
+    cg->h_start.assign(reinterpret_cast<const int *>(hp), reinterpret_cast<const int *>(hp) + ncell + 1);
+    unsigned hf[3];
+    memcpy(hf, hp + sb, sizeof(hf));
+    const int hflags = (int)hf[0];
     if (hflags & 1) {
         ctx->last_error = "a coordinate lies outside [0, box)";
         return PCF_ERR_OUT_OF_BOX;
@@ -398,9 +413,14 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     build_tiles(*cg);
     cg->d_tiles.pool = g->pool;
     PCF_CU(ctx, cg->d_tiles.ensure(sizeof(TileDesc) * std::max<size_t>(1, cg->tiles.size())));
-    if (!cg->tiles.empty())
-        PCF_CU(ctx, cudaMemcpyAsync(cg->d_tiles.p, cg->tiles.data(),
-                                    sizeof(TileDesc) * cg->tiles.size(), cudaMemcpyHostToDevice, st));
+    if (!cg->tiles.empty()) {
+        // staged in the page-locked buffer: every later host write to it
+        // follows a synchronisation of this stream
+        const size_t tb = sizeof(TileDesc) * cg->tiles.size();
+        if ((ps = pcf_ensure_pinned(ctx, tb)) != PCF_OK) return ps;
+        memcpy(ctx->h_pinned, cg->tiles.data(), tb);
+        PCF_CU(ctx, cudaMemcpyAsync(cg->d_tiles.p, ctx->h_pinned, tb, cudaMemcpyHostToDevice, st));
+    }
     if (g->cells) {
         g->cell_cache.push_back(std::move(g->cells));
         if ((int)g->cell_cache.size() > kCellCache) g->cell_cache.erase(g->cell_cache.begin());

@@ -729,13 +729,17 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
                                                                 dev_out ? hist : d_out);
     PCF_CU(ctx, cudaGetLastError());
     ++ctx->launches;
-    if (!dev_out)
-        PCF_CU(ctx, cudaMemcpyAsync(hist, d_out, sizeof(double) * n3, cudaMemcpyDeviceToHost,
-                                    ctx->stream));
-    if (stats || !dev_out) {
-        unsigned long long hs[4] = {0, 0, 0, 0};
-        PCF_CU(ctx, cudaMemcpyAsync(hs, A.g_stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+    if (stats || !dev_out) {  // through the context's page-locked buffer (see count_pairs_impl)
+        const size_t hb = dev_out ? 0 : sizeof(double) * n3;
+        s = pcf_ensure_pinned(ctx, hb + 64);
+        if (s != PCF_OK) return s;
+        char *hp = static_cast<char *>(ctx->h_pinned);
+        if (hb) PCF_CU(ctx, cudaMemcpyAsync(hp, d_out, hb, cudaMemcpyDeviceToHost, ctx->stream));
+        PCF_CU(ctx, cudaMemcpyAsync(hp + hb, A.g_stats, 32, cudaMemcpyDeviceToHost, ctx->stream));
         PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        if (hb) memcpy(hist, hp, hb);
+        unsigned long long hs[4];
+        memcpy(hs, hp + hb, sizeof(hs));
         if (stats) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
