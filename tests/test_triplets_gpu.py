@@ -96,3 +96,16 @@ def test_triplets_ani(ctx, bpc, w):
          oracle.triplets_ani(D, box=box, bins=bins, dmax=dmax, bpc=bpc), weighted)
     _cmp(ctx.count_triplets(gd, gr, bins=bins, dmax=dmax, ani=True, bpc=bpc),
          oracle.triplets_ani(D, R, box=box, bins=bins, dmax=dmax, bpc=bpc), weighted)
+
+
+def test_wide_histogram_through_grown_staging(ctx):
+    """A 70^3 histogram (2.7 MB of doubles) is larger than a context's initial
+    page-locked staging buffer: the buffer grows and the result still equals
+    the oracle, and a pair histogram on the same context afterwards too."""
+    box, bins, dmax = 100.0, 70, 30.0
+    D = catalog.neyman_scott(700, box, seed=31)
+    gd = ctx.grid(D, box)
+    got = ctx.count_triplets(gd, bins=bins, dmax=dmax, bpc=True)
+    _cmp(got, oracle.triplets_iso(D, box=box, bins=bins, dmax=dmax, bpc=True), False)
+    got2 = ctx.count_pairs(gd, None, bins=30, dmax=dmax, bpc=True)
+    assert np.array_equal(got2, oracle.pairs(D, None, box=box, bins=30, dmax=dmax, bpc=True))
