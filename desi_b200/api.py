@@ -92,8 +92,9 @@ class Context:
                     ani: "bool | str" = False, bpc: bool = False, flags: int = 0,
                     stats: bool = False, out_device_ptr: int | None = None):
         """One pair histogram (DD / RR with b None, else DR).  ani=False:
-        isotropic [bins]; True: anisotropic [bins, bins]; "both": the two from
-        one pass, returned as (iso, ani) (a device output then holds bins +
+        isotropic [bins]; True: anisotropic [bins, bins]; "both": the two in
+        one call (one pass over the candidates where the autotuner found that
+        faster), returned as (iso, ani) (a device output then holds bins +
         bins^2 doubles, isotropic first)."""
         both = ani == "both"
         kind = PCF_BOTH if both else (PCF_ANI if ani else PCF_ISO)

@@ -303,3 +303,34 @@ def test_both_kinds_forced_one_pass(tmp_path, w, bins):
                 assert np.all(np.abs(got - single) <= RTOL_W * (np.abs(single) + floor))
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("tuned", [False, True])
+def test_both_kinds_device_output(ctx, tmp_path, tuned):
+    """ani="both" into a device buffer (bins + bins^2 doubles, isotropic
+    first) equals the host-output call within 1e-12, as two launches
+    (untuned) and as one pass (a tuned scheme)."""
+    import torch
+    from desi_b200 import api
+    box, bins, dmax, n = 250.0, 30, 80.0, 2200
+    D = catalog.neyman_scott(n, box, seed=71, weights="uniform")
+    R = catalog.uniform(n + 40, box, seed=72, weights="uniform")
+    c = api.Context(0)
+    try:
+        if tuned:
+            path = str(tmp_path / "tune.txt")
+            with open(path, "w") as f:
+                for cross in (False, True):
+                    f.write(f"{_tune_key('both', True, cross, True, bins, n + 40 if cross else n, box, dmax)} 0 3 1.0\n")
+            c.tune_load(path)
+        gd, gr = c.grid(D, box), c.grid(R, box)
+        for b in (None, gr):
+            iso, ani = c.count_pairs(gd, b, bins=bins, dmax=dmax, ani="both", bpc=True)
+            out = torch.full((bins + bins * bins,), -1.0, dtype=torch.float64, device="cuda")
+            c.count_pairs(gd, b, bins=bins, dmax=dmax, ani="both", bpc=True, out_device_ptr=out.data_ptr())
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            _cmp(got[:bins], iso, True)  # FP64 sums: atomic order varies, 1e-12
+            _cmp(got[bins:], ani.ravel(), True)
+    finally:
+        c.close()
