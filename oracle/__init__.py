@@ -25,6 +25,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(HERE, "liboracle.so")
 
 FP64, REF32_NOFMA, REF32_FMA_A, REF32_FMA_B, REF32_FMA_C = 0, 1, 2, 3, 4
+# the reference's CPU periodic engines (cpp/2PCF{isotropic,anisotropic}/BPC),
+# FP32 throughout; see cpu_bpc_slot in pcf_oracle.c
+REF32_CPU_BPC = 5
+_METHODS = {"auto": 0, "brute": 1, "cells": 2}
 RULE_EXCL_ZERO, RULE_INCLUSIVE = 1, 2
 
 _dptr = ctypes.POINTER(ctypes.c_double)
@@ -44,6 +48,7 @@ def _load():
                               ctypes.c_int, ctypes.c_double, ctypes.c_int,
                               _fptr, ctypes.c_long, _fptr, ctypes.c_long, ctypes.c_float,
                               ctypes.c_int, ctypes.c_float, _dptr]
+    lib.orc_pairs_m.argtypes = lib.orc_pairs.argtypes + [ctypes.c_int]
     lib.orc_triplets_iso.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _fptr,
                                      ctypes.c_long, _fptr, ctypes.c_long, ctypes.c_float,
                                      ctypes.c_int, ctypes.c_float, _dptr]
@@ -61,6 +66,8 @@ def _load():
     lib.orc_analytic_bin.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_float, ctypes.c_int, ctypes.c_double, _dptr,
                                      _dptr, _dptr]
+    lib.orc_ff_average_ref.argtypes = [_dptr, _dptr, ctypes.c_int, ctypes.c_float,
+                                       ctypes.c_int, ctypes.c_int, _dptr]
     lib.orc_ds.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_int]
     lib.orc_ds.restype = ctypes.c_double
     return lib
@@ -96,21 +103,27 @@ def ds(bins: int, dmax: float, exact: bool = False) -> float:
 
 def pairs(A, B=None, *, box: float, bins: int, dmax: float, ani: bool = False,
           bpc: bool = False, rule: int | None = None, ds_exact: bool = False,
-          ds_value: float = 0.0, prec: int = FP64) -> np.ndarray:
+          ds_value: float = 0.0, prec: int = FP64, method: str = "auto") -> np.ndarray:
     """Pair histogram.  ``B is None`` -> XX over A (ordered pairs), else XY.
 
     ``rule`` defaults to the reference CUDA rule for the variant (see
-    :func:`reference_rule`).
+    :func:`reference_rule`).  ``method``: "brute" tests every pair, "cells"
+    only pairs of adjacent cells of side >= dmax (same histogram), "auto"
+    picks "cells" for large inputs.  Weighted sums are compensated, so they
+    carry about one rounding of the total whatever the order of additions.
     """
     A = _pts(A)
     self_ = B is None
     Bp = A if self_ else _pts(B)
     if rule is None:
-        rule = reference_rule(ani=ani, bpc=bpc, cross=not self_)
+        # the CPU periodic engines count direct pairs with <= (2PCF.h:199)
+        rule = (RULE_INCLUSIVE if prec == REF32_CPU_BPC
+                else reference_rule(ani=ani, bpc=bpc, cross=not self_))
     nb = bins * bins if ani else bins
     out = np.zeros(nb, np.float64)
-    rc = lib().orc_pairs(int(ani), int(bpc), int(self_), rule, int(ds_exact), float(ds_value),
-                         prec, _p(A), len(A), _p(Bp), len(Bp), box, bins, dmax, _d(out))
+    rc = lib().orc_pairs_m(int(ani), int(bpc), int(self_), rule, int(ds_exact), float(ds_value),
+                           prec, _p(A), len(A), _p(Bp), len(Bp), box, bins, dmax, _d(out),
+                           _METHODS[method])
     assert rc == 0
     return out.reshape(bins, bins) if ani else out
 
@@ -188,6 +201,18 @@ def analytic_ff(D, *, box: float, bins: int, dmax: float, ptt: int = 100, bn_ref
     return ff, ffr, float(a[0])
 
 
+def ff_average_ref(dd_ref, rr_ref, *, bins, dmax, ptt=100, bn_ref=200):
+    """make_ff_av_ref of the analytic 3iso path (3isoBPC_k.cuh:2001) on given
+    fine DD and RR histograms (ptt * bn_ref * bins bins): bn_ref * bins
+    averaged correction factors."""
+    dd = np.ascontiguousarray(dd_ref, np.float64)
+    rr = np.ascontiguousarray(rr_ref, np.float64)
+    assert dd.size == rr.size == ptt * bn_ref * bins
+    out = np.zeros(bn_ref * bins, np.float64)
+    lib().orc_ff_average_ref(_d(dd), _d(rr), bins, dmax, ptt, bn_ref, _d(out))
+    return out
+
+
 def analytic_bin(i, j, k, *, bins, dmax, bn_ref, alpha_ref, ff_ref):
     ffr = np.ascontiguousarray(ff_ref, np.float64)
     r = ctypes.c_double()
@@ -230,6 +255,68 @@ class RefEngine:
         out = np.zeros(bins * bins if self.is2d else bins, np.float64)
         self.lib.ref_xy(_p(A), _p(B), len(A), box, size_node, dmax, bins, _d(out))
         return out.reshape(bins, bins) if self.is2d else out
+
+
+class RefAnalyticRR:
+    """The reference's CPU periodic 2-point engine with the analytic RR
+    (cpp/2PCFisotropic/BPC_analitic/2PCF.h), compiled in place."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "_ref", "libref_2iso_analytic.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.lib.ref_dd_rr_analytic.argtypes = [_fptr, ctypes.c_int, ctypes.c_float,
+                                                ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                                _dptr, _dptr]
+
+    def set_threads(self, t: int) -> None:
+        self.lib.ref_set_threads(int(t))
+
+    def dd_rr(self, A, *, box, size_node, bins, dmax):
+        A = _pts(A)
+        dd = np.zeros(bins, np.float64)
+        rr = np.zeros(bins, np.float64)
+        self.lib.ref_dd_rr_analytic(_p(A), len(A), box, size_node, dmax, bins, _d(dd), _d(rr))
+        return dd, rr
+
+
+class Ref3IsoBPC:
+    """The reference's CPU periodic 3-point engine NODE3P
+    (cpp/3PCFisotropic/BPC/3PCFiso.h), compiled in place: DDD of one
+    catalog and the analytic path's averaged correction factors."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "_ref", "libref_3iso_bpc.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.lib.ref3_xxx.argtypes = [_fptr, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_float, ctypes.c_int, _dptr]
+        self.lib.ref3_analytic_ff.argtypes = [_fptr, ctypes.c_int, ctypes.c_float,
+                                              ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                              ctypes.c_char_p, _dptr, _dptr, _dptr]
+
+    def set_threads(self, t: int) -> None:
+        self.lib.ref_set_threads(int(t))
+
+    def xxx(self, A, *, box, size_node, bins, dmax):
+        A = _pts(A)
+        out = np.zeros(bins ** 3, np.float64)
+        self.lib.ref3_xxx(_p(A), len(A), box, size_node, dmax, bins, _d(out))
+        return out.reshape(bins, bins, bins)
+
+    def analytic_ff(self, A, *, box, size_node, bins, dmax, workdir):
+        """(ff_av, ff_av_ref, fine DD of ff_av_ref at 100*200*bins bins); the
+        engine writes them as text files into workdir."""
+        A = _pts(A)
+        ff = np.zeros(bins, np.float64)
+        ffr = np.zeros(200 * bins, np.float64)
+        dd = np.zeros(100 * 200 * bins, np.float64)
+        rc = self.lib.ref3_analytic_ff(_p(A), len(A), box, size_node, dmax, bins,
+                                       os.fsencode(workdir), _d(ff), _d(ffr), _d(dd))
+        assert rc == 0
+        return ff, ffr, dd
 
 
 def available_ref_engines():

@@ -45,7 +45,8 @@ enum {
     ORC_REF32_NOFMA = 1,   /* FP32 d2, ((dx*dx + dy*dy) + dz*dz), no contraction */
     ORC_REF32_FMA_A = 2,   /* FP32 d2 = fma(dz,dz, fma(dy,dy, dx*dx))            */
     ORC_REF32_FMA_B = 3,   /* FP32 d2 = fma(dz,dz, fma(dx,dx, dy*dy))            */
-    ORC_REF32_FMA_C = 4    /* FP32 d2 = fma(dx,dx, fma(dy,dy, dz*dz))            */
+    ORC_REF32_FMA_C = 4,   /* FP32 d2 = fma(dx,dx, fma(dy,dy, dz*dz))            */
+    ORC_REF32_CPU_BPC = 5  /* the reference's CPU periodic engines, see cpu_bpc_slot */
 };
 #define RULE_EXCL_ZERO 1u  /* require d2 > 0 (every component for 2ani)          */
 #define RULE_INCLUSIVE 2u  /* d2 <= dd_max instead of d2 < dd_max                */
@@ -136,46 +137,218 @@ static inline int pair_slot(const opt *p, const opt *q, int ani, int bpc, double
 }
 
 /*
+ * The reference's CPU periodic engines, restated for pinning
+ * (cpp/2PCFisotropic/BPC/2PCF.h:151-335, :338-495, :498-700 and
+ * cpp/2PCFanisotropic/BPC/2PCFani.h:152-700).  p is the point the engine's
+ * outer loop holds (x = elements[i].x), q the inner one.  All in FP32:
+ *   direct pass   d = p - q per axis; iso: dis = (dx*dx + dy*dy) + dz*dz,
+ *                 counted when dis <= dd_max (2PCF.h:199,232,274,316) under
+ *                 RULE_INCLUSIVE, else dis < dd_max (the fine DD of the
+ *                 3-point engine, 3PCFiso.h:1760);
+ *   image pass    a wrapped axis uses fabs(d) - L (2PCF.h:358), counted when
+ *                 dis < dd_max (2PCF.h:362).  With dmax < L/2 a pair lands in
+ *                 the pass that wraps exactly the axes with |d| > L/2.
+ *   ani           dz2 = dz*dz, r2 = dx*dx + dy*dy, both < dd_max in every
+ *                 pass (2PCFani.h:207,238,492);
+ *   bin           (int)(sqrt((double)dis) * ds), ds floored to 1e-6 in both
+ *                 engines (2PCF.h:74, 2PCFani.h:72); no d > 0 test and no
+ *                 bin cap (a bin >= bins is dropped here; the engine would
+ *                 write past its histogram);
+ *   weight        the product is formed in FP32 before the FP64 sum:
+ *                 2*w1*w2 for XX (2PCF.h:200), w1*w2 for XY.
+ * Returns the slot or -1; *wprod receives the FP32 weight product.
+ */
+static inline int cpu_bpc_slot(const opt *p, const opt *q, int ani, int self, float L,
+                               float ddf, double ds, int bins, unsigned rule, double *wprod)
+{
+    float d[3] = {p->x - q->x, p->y - q->y, p->z - q->z};
+    int wrapped = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (fabsf(d[k]) > 0.5f * L) { d[k] = fabsf(d[k]) - L; wrapped = 1; }
+    }
+    int slot;
+    if (!ani) {
+        float a = d[0] * d[0], b = d[1] * d[1], c = d[2] * d[2];
+        float s = a + b;
+        double dis = (double)(s + c);
+        const int incl = !wrapped && (rule & RULE_INCLUSIVE);
+        if (incl ? !(dis <= (double)ddf) : !(dis < (double)ddf)) return -1;
+        int bn = (int)(sqrt(dis) * ds);
+        if (bn < 0 || bn >= bins) return -1;
+        slot = bn;
+    } else {
+        float z2 = d[2] * d[2];
+        float a = d[0] * d[0], b = d[1] * d[1];
+        float r2 = a + b;
+        if (!(z2 < ddf && r2 < ddf)) return -1;
+        int bz = (int)(sqrt((double)z2) * ds), bp = (int)(sqrt((double)r2) * ds);
+        if (bz < 0 || bz >= bins || bp < 0 || bp >= bins) return -1;
+        slot = bz * bins + bp;
+    }
+    float w = self ? (2.0f * p->w) * q->w : p->w * q->w;
+    *wprod = (double)w;
+    return slot;
+}
+
+/* Neumaier (compensated) summation: s + c carries the sum of every term with
+ * an error of about one rounding of the total, so the order of the additions
+ * (threads, cells) does not show in the result.  Every term added here (an
+ * FP32 x FP32 product, times 2) is exact in FP64. */
+static inline void nsum_add(double *s, double *c, double x)
+{
+    double t = *s + x;
+    if (fabs(*s) >= fabs(x)) *c += (*s - t) + x;
+    else *c += (x - t) + *s;
+    *s = t;
+}
+
+/* Cells of side >= dmax * 1.001 over the box: every pair within reach of the
+ * rule (|d| per axis < dmax, or <= for the inclusive rule, after the minimum
+ * image) lies in the same or an adjacent cell.  Returns the cells per side,
+ * 0 when the box holds fewer than 3 (no pruning possible). */
+static int prune_cells(float L, float dmax)
+{
+    double c = (double)L / ((double)dmax * 1.001);
+    int P = (int)c;
+    if (P > 256) P = 256;
+    return P >= 3 ? P : 0;
+}
+
+static inline int cell_of(float x, int P, float L)
+{
+    int c = (int)((double)x * (double)P / (double)L);
+    return c < 0 ? 0 : (c >= P ? P - 1 : c);
+}
+
+/*
  * Pair histogram.  self != 0: XX over catalog A, ordered pairs i != j
  * (each unordered pair adds 2*w_i*w_j, as the reference launches both
  * orders); self == 0: XY, every A x B pair once.
  * ds <= 0 selects orc_ds(bins, dmax, ds_exact); ds > 0 is used as given.
  * out has bins (iso) or bins*bins (ani) doubles and is overwritten.
+ * method: 0 automatic, 1 every pair (brute force), 2 cell-pruned (only pairs
+ * of the same or adjacent cells of side >= dmax are tested; falls back to
+ * brute force when the box holds fewer than 3 such cells).  Both visit every
+ * pair the rule can accept, so they give the same histogram.
  */
-int orc_pairs(int ani, int bpc, int self, unsigned rule, int ds_exact, double ds_in, int prec,
-              const opt *A, long nA, const opt *B, long nB, float L, int bins, float dmax,
-              double *out)
+int orc_pairs_m(int ani, int bpc, int self, unsigned rule, int ds_exact, double ds_in, int prec,
+                const opt *A, long nA, const opt *B, long nB, float L, int bins, float dmax,
+                double *out, int method)
 {
     const int nb = ani ? bins * bins : bins;
     const double ds = ds_in > 0 ? ds_in : orc_ds(bins, dmax, ds_exact);
     const float ddf = dmax * dmax;
     const double ddmax = (double)ddf;
     const double Ld = (double)L;
+    const int cpu = prec == ORC_REF32_CPU_BPC;
     if (self) { B = A; nB = nA; }
     memset(out, 0, sizeof(double) * (size_t)nb);
+    int P = 0;
+    if (method == 2 || (method == 0 && (double)nA * (double)nB > 2e8)) P = prune_cells(L, dmax);
     int nt = omp_get_max_threads();
-    double *priv = (double *)calloc((size_t)nt * nb, sizeof(double));
+    double *priv = (double *)calloc((size_t)nt * nb * 2, sizeof(double));
     if (!priv) return -1;
+    /* cell-ordered index of B (pruned method) */
+    long *bstart = NULL, *border = NULL;
+    if (P) {
+        long ncell = (long)P * P * P;
+        bstart = (long *)calloc((size_t)ncell + 1, sizeof(long));
+        border = (long *)malloc(sizeof(long) * (size_t)(nB > 0 ? nB : 1));
+        long *fill = (long *)calloc((size_t)ncell, sizeof(long));
+        if (!bstart || !border || !fill) return -1;
+        for (long j = 0; j < nB; ++j) {
+            long c = ((long)cell_of(B[j].x, P, L) * P + cell_of(B[j].y, P, L)) * P +
+                     cell_of(B[j].z, P, L);
+            ++bstart[c + 1];
+        }
+        for (long c = 0; c < ncell; ++c) bstart[c + 1] += bstart[c];
+        for (long j = 0; j < nB; ++j) {
+            long c = ((long)cell_of(B[j].x, P, L) * P + cell_of(B[j].y, P, L)) * P +
+                     cell_of(B[j].z, P, L);
+            border[bstart[c] + fill[c]++] = j;
+        }
+        free(fill);
+    }
 #pragma omp parallel
     {
-        double *h = priv + (size_t)omp_get_thread_num() * nb;
+        double *h = priv + (size_t)omp_get_thread_num() * nb * 2;
+        double *hc = h + nb;
+        /* one pair (i, j): adds its weight to its slot */
+#define ORC_PAIR(pi, pj, wmul)                                                              \
+        do {                                                                                \
+            double wq = 0.0;                                                                \
+            int s_;                                                                         \
+            if (cpu) s_ = cpu_bpc_slot(pi, pj, ani, self, L, ddf, ds, bins, rule, &wq);           \
+            else {                                                                          \
+                s_ = pair_slot(pi, pj, ani, bpc, Ld, prec, rule, ddmax, ds, bins);          \
+                wq = (wmul) * ((double)(pi)->w * (double)(pj)->w);                          \
+            }                                                                               \
+            if (s_ >= 0) nsum_add(&h[s_], &hc[s_], wq);                                     \
+        } while (0)
+        if (!P) {
 #pragma omp for schedule(dynamic, 16)
-        for (long i = 0; i < nA; ++i) {
-            const opt *p = &A[i];
-            long j0 = self ? i + 1 : 0;
-            for (long j = j0; j < nB; ++j) {
-                int s = pair_slot(p, &B[j], ani, bpc, Ld, prec, rule, ddmax, ds, bins);
-                if (s >= 0) {
-                    double w = (double)p->w * (double)B[j].w;
-                    h[s] += self ? 2.0 * w : w;
+            for (long i = 0; i < nA; ++i) {
+                const opt *p = &A[i];
+                long j0 = self ? i + 1 : 0;
+                for (long j = j0; j < nB; ++j) ORC_PAIR(p, &B[j], self ? 2.0 : 1.0);
+            }
+        } else {
+            /* ordered pairs: for XX each unordered pair is met twice, from
+             * either end, and adds w_i*w_j each time (the emulated CPU rule
+             * forms 2*w1*w2 itself, so it takes half of that) */
+#pragma omp for schedule(dynamic, 64)
+            for (long i = 0; i < nA; ++i) {
+                const opt *p = &A[i];
+                int cx = cell_of(p->x, P, L), cy = cell_of(p->y, P, L), cz = cell_of(p->z, P, L);
+                for (int ox = -1; ox <= 1; ++ox) {
+                    int nx = cx + ox;
+                    if (nx < 0 || nx >= P) { if (!bpc) continue; nx = (nx + P) % P; }
+                    for (int oy = -1; oy <= 1; ++oy) {
+                        int ny = cy + oy;
+                        if (ny < 0 || ny >= P) { if (!bpc) continue; ny = (ny + P) % P; }
+                        for (int oz = -1; oz <= 1; ++oz) {
+                            int nz = cz + oz;
+                            if (nz < 0 || nz >= P) { if (!bpc) continue; nz = (nz + P) % P; }
+                            long c = ((long)nx * P + ny) * P + nz;
+                            for (long t = bstart[c]; t < bstart[c + 1]; ++t) {
+                                long j = border[t];
+                                if (self && j == i) continue;
+                                if (cpu && self) {
+                                    /* the engine meets each unordered pair once, with the
+                                     * lower cell-order point as p; use the lower index */
+                                    if (j < i) continue;
+                                    ORC_PAIR(p, &B[j], 1.0);
+                                } else {
+                                    ORC_PAIR(p, &B[j], 1.0);
+                                }
+                            }
+                        }
+                    }
                 }
             }
         }
+#undef ORC_PAIR
     }
-    for (int t = 0; t < nt; ++t)
-        for (int k = 0; k < nb; ++k) out[k] += priv[(size_t)t * nb + k];
+    for (int k = 0; k < nb; ++k) {
+        double s = 0.0, c = 0.0;
+        for (int t = 0; t < nt; ++t) {
+            nsum_add(&s, &c, priv[(size_t)t * nb * 2 + k]);
+            nsum_add(&s, &c, priv[(size_t)t * nb * 2 + nb + k]);
+        }
+        out[k] = s + c;
+    }
     free(priv);
+    free(bstart);
+    free(border);
     return 0;
+}
+
+int orc_pairs(int ani, int bpc, int self, unsigned rule, int ds_exact, double ds_in, int prec,
+              const opt *A, long nA, const opt *B, long nB, float L, int bins, float dmax,
+              double *out)
+{
+    return orc_pairs_m(ani, bpc, self, rule, ds_exact, ds_in, prec, A, nA, B, nB, L, bins, dmax,
+                       out, 0);
 }
 
 /* ----------------------------------------------------------------------- */
@@ -446,6 +619,29 @@ static int all_corners(double ri, double rj, double rk, double h)
  * wrap: reproduce the reference's 32-bit coefficient overflow.
  * fine_dd / fine_dd_ref (optional, may be NULL): receive the fine DD histograms.
  */
+/* make_ff_av_ref (3isoBPC_k.cuh:2001; the same average as the CPU engine's
+ * cpp/3PCFisotropic/BPC/3PCFiso.h:1584-1604): per coarse bin i and
+ * sub-bin j, the mean over the ptt fine bins k of
+ * (r_i + r_j + r_k) * (DD/RR - 1).  ff_ref: bn_ref * bins, added to. */
+void orc_ff_average_ref(const double *dd_ref, const double *rr_ref, int bins, float dmax, int ptt,
+                        int bn_ref, double *ff_ref)
+{
+    for (int i = 0; i < bins; ++i) {
+        for (int j = 0; j < bn_ref; ++j) {
+            for (int k = 0; k < ptt; ++k) {
+                double drr = dmax / (double)bins;
+                double drr_ref = drr / bn_ref;
+                double dr_ptt_ref = dmax / (double)((long)ptt * bn_ref * bins);
+                double ri = i * drr, rj = j * drr_ref, rk = (k + 0.5) * dr_ptt_ref;
+                long i_ = (long)i * bn_ref, j_ = (long)j * ptt;
+                long s = i_ * ptt + j_ + k;
+                double f = (ri + rj + rk) * ((dd_ref[s] / rr_ref[s]) - 1) / (double)ptt;
+                ff_ref[i_ + j] += f;
+            }
+        }
+    }
+}
+
 static int analytic_3iso_impl(const opt *D, long n, float L, int bins, float dmax, int ptt,
                               int bn_ref, int wrap, double *DDR, double *RRR, double *ff_av_out,
                               double *ff_ref_out, int refine)
@@ -501,21 +697,7 @@ static int analytic_3iso_impl(const opt *D, long n, float L, int bins, float dma
             ff_av[i] += v;
         }
     }
-    /* make_ff_av_ref (3isoBPC_k.cuh:2001) */
-    for (int i = 0; i < bins; ++i) {
-        for (int j = 0; j < bn_ref; ++j) {
-            for (int k = 0; k < ptt; ++k) {
-                double drr = dmax / (double)bins;
-                double drr_ref = drr / bn_ref;
-                double dr_ptt_ref = dmax / (double)((long)ptt * bn_ref * bins);
-                double ri = i * drr, rj = j * drr_ref, rk = (k + 0.5) * dr_ptt_ref;
-                long i_ = (long)i * bn_ref, j_ = (long)j * ptt;
-                long s = i_ * ptt + j_ + k;
-                double f = (ri + rj + rk) * ((dd_ref[s] / rr_ref[s]) - 1) / (double)ptt;
-                ff_ref[i_ + j] += f;
-            }
-        }
-    }
+    orc_ff_average_ref(dd_ref, rr_ref, bins, dmax, ptt, bn_ref, ff_ref);
     if (refine < 0) {  /* caller wants ff, ff_ref and alpha_ref only */
         if (ff_av_out) memcpy(ff_av_out, ff_av, sizeof(double) * bins);
         if (ff_ref_out) memcpy(ff_ref_out, ff_ref, sizeof(double) * bn_ref * bins);

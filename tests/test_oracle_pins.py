@@ -103,3 +103,195 @@ def test_fp64_vs_fp32_differ_only_near_edges(catalogs):
         frac = r64[diff] - np.floor(r64[diff])
         near = np.minimum(frac, 1 - frac) < 1e-5 * bins
         assert near.all()
+
+
+# ---------------------------------------------------------------------------
+# Periodic (BPC), weighted and analytic rules against the reference's CPU
+# engines, compiled in place by oracle/Makefile.
+# ---------------------------------------------------------------------------
+
+def _cat(kind, n, seed, weights="unit", box=250.0):
+    from desi_b200 import catalog
+    f = catalog.neyman_scott if kind == "clustered" else catalog.uniform
+    return f(n, box, seed=seed, weights=weights)
+
+
+@pytest.mark.parametrize("bins,dmax,sn", [(30, 80.0, 20.0), (20, 100.0, 25.0), (17, 33.3, 9.0)])
+@pytest.mark.parametrize("kind", ["2iso_bpc", "2ani_bpc"])
+def test_ref_cpu_bpc_bitexact(catalogs, kind, bins, dmax, sn):
+    """The oracle's emulation of the periodic CPU engines (FP32 distances,
+    <= for direct and < for image pairs, FP32 weight products) equals
+    cpp/2PCF{isotropic,anisotropic}/BPC bit for bit."""
+    D, R = catalogs["data_1K"], catalogs["rand0_1K"]
+    e = _ref(kind)
+    ani = kind.startswith("2ani")
+    kw = dict(box=L1K, bins=bins, dmax=dmax, ani=ani, bpc=True, prec=oracle.REF32_CPU_BPC)
+    assert np.array_equal(e.xx(D, box=L1K, size_node=sn, bins=bins, dmax=dmax),
+                          oracle.pairs(D, **kw))
+    assert np.array_equal(e.xy(D, R, box=L1K, size_node=sn, bins=bins, dmax=dmax),
+                          oracle.pairs(D, R, **kw))
+
+
+@pytest.mark.parametrize("kind", ["2iso_bpc", "2ani_bpc"])
+def test_ref_cpu_bpc_weighted(kind):
+    """Weighted clustered catalogs (w ~ U(0.5, 1.5)) at 8192 points: the
+    compensated oracle sums match the engines' FP64 sums to 1e-12."""
+    e = _ref(kind)
+    e.set_threads(os.cpu_count() or 4)
+    D = _cat("clustered", 8192, 11, "uniform")
+    R = _cat("uniform", 8192, 12, "uniform")
+    sn = 2.176 * 250.0 / 8192 ** (1 / 3)
+    kw = dict(box=250.0, bins=30, dmax=80.0, ani=kind.startswith("2ani"), bpc=True,
+              prec=oracle.REF32_CPU_BPC)
+    for got, want in ((e.xx(D, box=250.0, size_node=sn, bins=30, dmax=80.0), oracle.pairs(D, **kw)),
+                      (e.xy(D, R, box=250.0, size_node=sn, bins=30, dmax=80.0),
+                       oracle.pairs(D, R, **kw))):
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=0)
+        assert want.sum() > 0
+
+
+def test_fp64_vs_cpu_bpc_differ_only_near_edges():
+    """Every pair that the canonical FP64 rule and the emulated CPU periodic
+    engine bin differently lies within FP32 rounding of a bin edge or of
+    dmax (minimum image per axis)."""
+    D = _cat("clustered", 900, 21)
+    bins, dmax, L = 30, 80.0, 250.0
+    ds = oracle.ds(bins, dmax)
+    p = D[:, :3].astype(np.float64)
+    i, j = np.triu_indices(len(D), 1)
+    d = p[j] - p[i]
+    d = np.where(d > L / 2, d - L, np.where(d < -L / 2, d + L, d))
+    d2 = (d[:, 0] ** 2 + d[:, 1] ** 2) + d[:, 2] ** 2
+    f = (D[i, :3] - D[j, :3]).astype(np.float32)
+    wrapped = np.abs(f) > np.float32(L / 2)
+    f = np.where(wrapped, np.abs(f) - np.float32(L), f).astype(np.float32)
+    d2f = ((f[:, 0] * f[:, 0] + f[:, 1] * f[:, 1]) + f[:, 2] * f[:, 2]).astype(np.float64)
+    dd = float(np.float32(dmax) * np.float32(dmax))
+    in64 = (d2 > 0) & (d2 < dd)
+    in32 = np.where(wrapped.any(1), d2f < dd, d2f <= dd)
+    b64 = np.where(in64, np.floor(np.sqrt(d2) * ds), -1)
+    b32 = np.where(in32, np.floor(np.sqrt(d2f) * ds), -1)
+    diff = b64 != b32
+    r = np.sqrt(d2[diff]) * ds
+    near_edge = np.minimum(r - np.floor(r), np.ceil(r) - r) < 1e-5 * bins
+    near_dmax = np.abs(np.sqrt(d2[diff]) - dmax) < 1e-4
+    zero = d2[diff] == 0
+    assert (near_edge | near_dmax | zero).all()
+    # and the histograms differ only by those pairs
+    h64 = oracle.pairs(D, box=L, bins=bins, dmax=dmax, bpc=True, rule=oracle.RULE_EXCL_ZERO)
+    h32 = oracle.pairs(D, box=L, bins=bins, dmax=dmax, bpc=True, prec=oracle.REF32_CPU_BPC)
+    # (each such XX pair moves 2 counts out of one bin and at most into another)
+    assert np.abs(h64 - h32).sum() <= 4 * diff.sum()
+
+
+def test_oracle_cells_equal_brute():
+    """The cell-pruned oracle (used for the large parity cases) gives the
+    brute-force histogram: counts bit for bit, weighted sums to 1e-15."""
+    box = 1000.0
+    D = _cat("clustered", 12000, 31, "uniform", box=box)
+    R = _cat("uniform", 15000, 32, "uniform", box=box)
+    for ani in (False, True):
+        for bpc in (False, True):
+            for B in (None, R):
+                kw = dict(box=box, bins=40, dmax=120.0, ani=ani, bpc=bpc)
+                a = oracle.pairs(D, B, method="brute", **kw)
+                b = oracle.pairs(D, B, method="cells", **kw)
+                np.testing.assert_allclose(b, a, rtol=1e-15, atol=0)
+                Du = D.copy(); Du[:, 3] = 1
+                Bu = None if B is None else B.copy()
+                if Bu is not None:
+                    Bu[:, 3] = 1
+                assert np.array_equal(oracle.pairs(Du, Bu, method="brute", **kw),
+                                      oracle.pairs(Du, Bu, method="cells", **kw))
+
+
+def _ref_analytic():
+    try:
+        return oracle.RefAnalyticRR()
+    except FileNotFoundError:
+        pytest.skip("oracle/_ref/libref_2iso_analytic.so not built")
+
+
+def _ref_3iso():
+    try:
+        return oracle.Ref3IsoBPC()
+    except FileNotFoundError:
+        pytest.skip("oracle/_ref/libref_3iso_bpc.so not built")
+
+
+def _cpu_rr(n, L, dmax, nbins, dr_f32):
+    """The CPU engines' analytic RR (cpp/2PCFisotropic/BPC_analitic/2PCF.h:333-355,
+    cpp/3PCFisotropic/BPC/3PCFiso.h:1794-1812): beta = n/L * (float)(n/L) / L
+    in FP64, alpha = 4 pi beta dr^3 / 3, RR[a] = alpha ((a+1)^3 - a^3), with
+    dr = d_max/bn in FP32 (2-point engine) or in FP64 (3-point engine)."""
+    f32 = np.float32
+    dr = np.float64(f32(dmax) / f32(nbins)) if dr_f32 else np.float64(f32(dmax)) / nbins
+    beta = n / np.float64(L)
+    beta *= np.float64(f32(n) / f32(L))
+    beta /= np.float64(L)
+    alph = 4 * (2 * np.arccos(0.0)) * beta / 3
+    alph *= dr * dr * dr
+    r2 = np.arange(nbins, dtype=np.float64)
+    r1 = r2 + 1
+    return alph * ((r1 * r1 * r1) - (r2 * r2 * r2))
+
+
+@pytest.mark.parametrize("bins,dmax", [(30, 80.0), (20, 100.0), (17, 33.3)])
+def test_ref_analytic_rr(bins, dmax):
+    """cpp/2PCFisotropic/BPC_analitic: its periodic DD equals the oracle's CPU
+    emulation bit for bit, its RR the restated CPU formula, and the oracle's
+    analytic RR (the CUDA path's constants, pcf2isoBPC.cuh:199-202, which
+    round N^2/L^3 to FP32) agrees with it to the FP32 rounding of beta."""
+    e = _ref_analytic()
+    D = _cat("uniform", 4096, 5)
+    sn = 2.276 * 250.0 / 4096 ** (1 / 3)
+    dd, rr = e.dd_rr(D, box=250.0, size_node=sn, bins=bins, dmax=dmax)
+    assert np.array_equal(dd, oracle.pairs(D, box=250.0, bins=bins, dmax=dmax, bpc=True,
+                                           prec=oracle.REF32_CPU_BPC))
+    np.testing.assert_allclose(rr, _cpu_rr(len(D), 250.0, dmax, bins, True), rtol=1e-15, atol=0)
+    a = oracle.analytic_rr(bins, len(D), 250.0, dmax, wrap=False)
+    np.testing.assert_allclose(a, rr, rtol=1.2e-7, atol=0)
+
+
+@pytest.mark.parametrize("n,dmax,kind,seed", [(2048, 60.0, "uniform", 7),
+                                              (4096, 80.0, "clustered", 7),
+                                              (8192, 50.0, "clustered", 8)])
+def test_ref_3iso_bpc_ddd_bitexact(n, dmax, kind, seed):
+    """cpp/3PCFisotropic/BPC (NODE3P, its own node-image passes, FP32
+    distances, float symmetrisation) gives the oracle's FP64 periodic DDD
+    (consistent embedding) bit for bit on these catalogs.  (Larger or denser
+    catalogs hold pairs within FP32 rounding of a bin edge, which move every
+    triangle they belong to between adjacent cells, totals unchanged.)"""
+    e = _ref_3iso()
+    e.set_threads(os.cpu_count() or 4)
+    D = _cat(kind, n, seed)
+    sn = 2.17 * 250.0 / n ** (1 / 3)
+    h = e.xxx(D, box=250.0, size_node=sn, bins=30, dmax=dmax)
+    o = oracle.triplets_iso(D, box=250.0, bins=30, dmax=dmax, bpc=True)
+    assert o.sum() > 0
+    assert np.array_equal(h, o)
+
+
+def test_ref_3iso_analytic_ff_ref(tmp_path):
+    """The analytic 3iso path of cpp/3PCFisotropic/BPC (make_histo_analitic,
+    3PCFiso.h:1484): its fine DD (600 000 bins) equals the oracle's FP32
+    emulation bit for bit, and the oracle's make_ff_av_ref on that DD and the
+    engine's RR reproduces the engine's ff_av_ref.dat (written with 12
+    significant digits).  (The engine's RRR/DDR refinement loop is commented
+    out, 3PCFiso.h:1623-1710, so the CUDA kernels are the only reference for
+    the refined histograms.)"""
+    e = _ref_3iso()
+    e.set_threads(os.cpu_count() or 4)
+    D = _cat("uniform", 2048, 9)
+    bins, dmax = 30, 80.0
+    sn = 2.17 * 250.0 / 2048 ** (1 / 3)
+    ff, ffr, dd = e.analytic_ff(D, box=250.0, size_node=sn, bins=bins, dmax=dmax,
+                                workdir=str(tmp_path))
+    nref = 100 * 200 * bins
+    dsf = float(np.float32(np.float32(nref) / np.float32(dmax)))
+    emu = oracle.pairs(D, box=250.0, bins=nref, dmax=dmax, bpc=True, prec=oracle.REF32_CPU_BPC,
+                       rule=0, ds_value=dsf)
+    assert np.array_equal(emu, dd)
+    got = oracle.ff_average_ref(dd, _cpu_rr(len(D), 250.0, dmax, nref, False), bins=bins,
+                                dmax=dmax)
+    np.testing.assert_allclose(got, ffr, rtol=1e-10, atol=1e-10)
