@@ -174,6 +174,67 @@ def tune_step(ctx, D, R, candidates=(8, 9, 10, 11, 12, 13, 14, 16)):
     return P, fused, modes
 
 
+HISTS = (("DD", 0), ("RR", 1), ("DR", 2))
+
+
+def step_calls(ctx, gd, gr, kinds, out_ptrs, with_stats=False):
+    """The counting calls of one headline step, each histogram written to
+    the device buffer out_ptrs[k] (no host synchronisation unless
+    with_stats).  Returns the calls' statistics when with_stats."""
+    W = WORKLOAD
+    k, st = 0, []
+    for ani in kinds:
+        for a, b in ((gd, None), (gr, None), (gd, gr)):
+            r = ctx.count_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True,
+                                stats=with_stats, out_device_ptr=out_ptrs[k])
+            if with_stats:
+                st.append(r[1])
+            k += 1
+    return st
+
+
+def step_results(outs, kinds):
+    """The six histograms of one step as host arrays, from the step's
+    device buffers (one row per call; a both-kinds call holds the isotropic
+    bins, then the anisotropic ones)."""
+    W = WORKLOAD
+    b1, b2 = W["bins"], W["bins"] * W["bins"]
+    rows = outs.cpu().numpy()
+    res = {}
+    for name, k in HISTS:
+        if kinds == ("both",):
+            res[name + "iso"] = rows[k][:b1]
+            res[name + "ani"] = rows[k][b1:b1 + b2].reshape(b1, b1)
+        else:
+            res[name + "iso"] = rows[k][:b1]
+            res[name + "ani"] = rows[3 + k][:b2].reshape(b1, b1)
+    return res
+
+
+def oracle_step(D, R):
+    """The checker: the six histograms of the step from the FP64 oracle
+    (oracle/pcf_oracle.c), computed on the host outside any timed region."""
+    import oracle
+    W = WORKLOAD
+    want = {}
+    for ani in (False, True):
+        for name, (A, B) in (("DD", (D, None)), ("RR", (R, None)), ("DR", (D, R))):
+            want[name + ("ani" if ani else "iso")] = oracle.pairs(
+                A, B, box=W["box"], bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True)
+    return want
+
+
+def mismatches(got, want, rtol=1e-12):
+    """Bins per histogram that differ from the oracle: unit weights
+    exactly, weighted sums by more than rtol relative (a single pair binned
+    differently moves a bin by ~1 in ~1e5, far above rtol)."""
+    out = {}
+    for k, w in want.items():
+        g = np.asarray(got[k], np.float64).reshape(w.shape)
+        out[k] = int((np.abs(g - w) > rtol * np.abs(w)).sum())
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from desi_b200 import api
@@ -199,18 +260,13 @@ def run_ours(args, rank, world, local_rank):
     Rh = torch.from_numpy(R).pin_memory()
     torch.cuda.synchronize()
 
+    out_ptrs = [outs[k].data_ptr() for k in range(6)]
+
     def step_device(collect, with_stats=False):
         # asynchronous: histograms stay in HBM, no per-call host sync
         gd = ctx.grid(None, W["box"], partitions=P, device_ptr=Dt.data_ptr(), n=len(D))
         gr = ctx.grid(None, W["box"], partitions=P, device_ptr=Rt.data_ptr(), n=len(R))
-        k = 0
-        for ani in kinds:
-            for a, b in ((gd, None), (gr, None), (gd, gr)):
-                r = ctx.count_pairs(a, b, bins=W["bins"], dmax=W["dmax"], ani=ani, bpc=True,
-                                    stats=with_stats, out_device_ptr=outs[k].data_ptr())
-                if with_stats:
-                    collect.append(r[1])
-                k += 1
+        collect.extend(step_calls(ctx, gd, gr, kinds, out_ptrs, with_stats))
         gd.free()
         gr.free()
 
@@ -275,6 +331,10 @@ def run_ours(args, rank, world, local_rank):
     step_device(probe, with_stats=True)
     times, _, clocks, launches, kprof = timed(step_device, args.steps, args.warmup)
     tot_ms = max_over_ranks(sum(times), world, dev)
+    # parity of the last timed step's histograms against the FP64 oracle
+    # (host, after the timed region)
+    ctx.synchronize()
+    got = step_results(outs, kinds)
     pairs_step = sum(s["pairs"] for s in probe)
     value = replica_throughput(world, pairs_step, args.steps, tot_ms)
 
@@ -334,6 +394,16 @@ def run_ours(args, rank, world, local_rank):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(pairs_step)
+    if not args.no_parity:
+        t0 = time.perf_counter()
+        mm = mismatches(got, oracle_step(D, R))
+        out["mismatches"] = mm
+        out["parity"] = {"checked": "the last timed step's six histograms",
+                         "oracle": "FP64 restatement of the reference rules (oracle/pcf_oracle.c), "
+                                   "host, outside the timed region",
+                         "rtol": 1e-12, "bins_compared": int(sum(v.size for v in got.values())),
+                         "mismatched_bins": int(sum(mm.values())),
+                         "oracle_s": round(time.perf_counter() - t0, 2)}
     if not args.no_extras:
         # the other north-star forms, measured beside the headline (not the metric)
         out["grid_build"] = run_grid_build(ctx, torch)
@@ -640,6 +710,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the check of the timed step against the FP64 oracle")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the triplet / batched / served measurements")
     ap.add_argument("--triplets-only", type=int, default=0, metavar="N",

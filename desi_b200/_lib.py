@@ -19,6 +19,8 @@ PCF_RULE_EXCL_ZERO = 1 << 3
 PCF_RULE_INCLUSIVE = 1 << 4
 PCF_DEVICE_OUT = 1 << 5
 PCF_GRAPH = 1 << 7
+PCF_ERR_TIMEOUT = -6
+PCF_OPT_TRIP_FLUSH_BUDGET, PCF_OPT_ABORT_HOST_CHECK = 1, 2
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory",
           -4: "unsupported configuration", -5: "coordinate outside [0, box)",
@@ -100,6 +102,9 @@ _SIGS = {
     "pcf_tune_size": (ctypes.c_int, [_vp]),
     "pcf_estimate": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _i64, _i64,
                                     _vp]),
+    "pcf_ctx_abort": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pcf_ctx_synchronize": (ctypes.c_int, [_vp]),
+    "pcf_ctx_set_option": (ctypes.c_int, [_vp, ctypes.c_int, _i64]),
     "pcf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pcf_ctx_profile_read": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(_i64)]),

@@ -13,9 +13,10 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import (PCF_ANI, PCF_BOTH, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT, PCF_GRAPH,  # noqa: F401
-                   PCF_ISO, PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO, PCF_RULE_INCLUSIVE, PcfError,
-                   Stats)
+from ._lib import (PCF_ANI, PCF_BOTH, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT,  # noqa: F401
+                   PCF_ERR_TIMEOUT, PCF_GRAPH, PCF_ISO, PCF_OPT_ABORT_HOST_CHECK,
+                   PCF_OPT_TRIP_FLUSH_BUDGET, PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO,
+                   PCF_RULE_INCLUSIVE, PcfError, Stats)
 
 
 def _check(ctx, rc, where):
@@ -52,6 +53,24 @@ class Context:
     @property
     def stream(self) -> int:
         return int(self._lib.pcf_ctx_stream(self.handle) or 0)
+
+    # -- failure handling ------------------------------------------------------
+    def abort(self, on: bool = True) -> None:
+        """Ask this context's running and future kernels to stop taking work
+        (calls then raise PcfError(PCF_ERR_TIMEOUT)); abort(False) clears the
+        request.  Safe to call from another thread while a call runs."""
+        _check(self.handle, self._lib.pcf_ctx_abort(self.handle, int(bool(on))), "pcf_ctx_abort")
+
+    def synchronize(self) -> None:
+        """Wait for the context stream; raises PcfError(PCF_ERR_TIMEOUT) if a
+        kernel gave up its queue since the last abort(False)."""
+        _check(self.handle, self._lib.pcf_ctx_synchronize(self.handle), "pcf_ctx_synchronize")
+
+    def set_option(self, option: int, value: int) -> None:
+        """pcf_ctx_set_option (include/pcf_bench.h): PCF_OPT_TRIP_FLUSH_BUDGET,
+        PCF_OPT_ABORT_HOST_CHECK."""
+        _check(self.handle, self._lib.pcf_ctx_set_option(self.handle, int(option), int(value)),
+               "pcf_ctx_set_option")
 
     def close(self):
         if self.handle:

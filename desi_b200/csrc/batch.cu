@@ -83,6 +83,7 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         (kind != PCF_ISO && kind != PCF_ANI && kind != PCF_BOTH) || (!dd && !rr && !dr))
         return PCF_ERR_INVALID_ARG;
     if (kind == PCF_BOTH) return batch_both_split(ctx, d_, r_, n_rand, bins, dmax, flags, dd, rr, dr, stats);
+    if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
     cudaSetDevice(ctx->device);
     const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0;
     pcf_grid *D = const_cast<pcf_grid *>(d_);
@@ -151,6 +152,8 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     pl.weighted = weighted;
     pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
     pl.mult = 1.0;
+    pl.ctrl = ctx->d_ctrl;
+    pl.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
     {
         std::vector<const pcf_grid *> gs(R.begin(), R.end());
         gs.push_back(D);
@@ -281,6 +284,8 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     PCF_CU(ctx, cudaMemcpyAsync(host.data(), bg->d_out, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, st));
     PCF_CU(ctx, cudaMemcpyAsync(hs, bg->d_stats, sizeof(hs), cudaMemcpyDeviceToHost, st));
     PCF_CU(ctx, cudaStreamSynchronize(st));
+    s = ctx_queue_status(ctx);
+    if (s != PCF_OK) return s;
     int k = 0;
     if (dd) memcpy(dd, host.data() + (size_t)(k++) * nb, sizeof(double) * nb);
     for (int i = 0; i < n_rand; ++i) {

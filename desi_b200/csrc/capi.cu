@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "pcf_internal.cuh"
 #include "../../include/pcf_bench.h"
@@ -50,6 +52,16 @@ pcf_status pcf_ctx_create(int device, pcf_ctx **out) {
         return PCF_ERR_CUDA;
     }
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    void *ctrl = nullptr;
+    if (cudaHostAlloc(&ctrl, 64, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->d_ctrl), ctrl, 0) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctrl) cudaFreeHost(ctrl);
+        pcf_ctx_destroy(c);
+        return PCF_ERR_NO_MEMORY;
+    }
+    c->h_ctrl = static_cast<unsigned *>(ctrl);
+    memset(ctrl, 0, 64);
     if (pcf_ensure_pinned(c, (size_t)2 << 20) != PCF_OK) {  // result staging (grows on demand)
         pcf_ctx_destroy(c);
         return PCF_ERR_NO_MEMORY;
@@ -64,6 +76,7 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);
     ctx->pool->release();
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
     for (auto &sl : ctx->slots) {
         if (sl.h_pinned) cudaFreeHost(sl.h_pinned);
         if (sl.done) cudaEventDestroy(sl.done);
@@ -84,6 +97,39 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
 }
 
 void *pcf_ctx_stream(pcf_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+pcf_status pcf_ctx_abort(pcf_ctx *ctx, int on) {
+    if (!ctx || !ctx->h_ctrl) return PCF_ERR_INVALID_ARG;
+    volatile unsigned *w = ctx->h_ctrl;
+    if (on) {
+        w[0] = 1u;
+    } else {
+        w[0] = 0u;
+        w[1] = 0u;
+    }
+    return PCF_OK;
+}
+
+pcf_status pcf_ctx_synchronize(pcf_ctx *ctx) {
+    if (!ctx) return PCF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return ctx_queue_status(ctx);
+}
+
+pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value) {
+    if (!ctx) return PCF_ERR_INVALID_ARG;
+    switch (option) {
+    case PCF_OPT_TRIP_FLUSH_BUDGET:
+        if (value < 1 || value > ((int64_t)1 << 31)) return PCF_ERR_INVALID_ARG;
+        ctx->trip_flush_budget = (unsigned long long)value;
+        return PCF_OK;
+    case PCF_OPT_ABORT_HOST_CHECK:
+        ctx->abort_host_check = value != 0;
+        return PCF_OK;
+    }
+    return PCF_ERR_INVALID_ARG;
+}
 
 int64_t pcf_ctx_launch_count(const pcf_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
@@ -130,6 +176,40 @@ pcf_status pcf_ctx_profile_read(pcf_ctx *ctx, double *total_ms, int64_t *n) {
     ctx->prof_used = 0;
     return PCF_OK;
 }
+
+}  // extern "C"
+
+pcf_status ctx_abort_requested(pcf_ctx *ctx) {
+    const volatile unsigned *w = ctx->h_ctrl;
+    if (ctx->abort_host_check && w && w[0]) {
+        ctx->last_error = "abort requested (pcf_ctx_abort)";
+        return PCF_ERR_TIMEOUT;
+    }
+    return PCF_OK;
+}
+
+pcf_status ctx_queue_status(pcf_ctx *ctx) {
+    const volatile unsigned *w = ctx->h_ctrl;
+    if (w && w[1]) {
+        ctx->last_error = (w[1] & 2u) ? "a persistent kernel reached its iteration cap"
+                                      : "a persistent kernel stopped on the abort request";
+        return PCF_ERR_TIMEOUT;
+    }
+    return PCF_OK;
+}
+
+cudaError_t ensure_smem_limit(const void *fn, int device, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> limit;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &cur = limit[{fn, device}];
+    if (bytes <= cur) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
+extern "C" {
 
 static bool is_device_ptr(const void *p) {
     cudaPointerAttributes a;
@@ -316,6 +396,7 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
         return PCF_ERR_INVALID_ARG;
     if (kind != PCF_ISO && (int64_t)bins * bins > (1 << 24)) return PCF_ERR_UNSUPPORTED;
     if (kind == PCF_BOTH && ds_override > 0) return PCF_ERR_INVALID_ARG;
+    if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
     cudaSetDevice(ctx->device);
     pcf_grid *a = const_cast<pcf_grid *>(a_);
     pcf_grid *b = const_cast<pcf_grid *>(b_);
@@ -383,6 +464,8 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
         pl.wunscale = weight_unscale(a, cross ? b : a);
     }
     pl.count = stats != nullptr && !ctx->tune_timing;
+    pl.ctrl = ctx->d_ctrl;
+    pl.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
                      d_stats);
     if (s != PCF_OK) return s;
@@ -402,6 +485,8 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
         if (cb) PCF_CU(ctx, cudaMemcpyAsync(hp + hb, d_cnt, cb, cudaMemcpyDeviceToHost, ctx->stream));
         PCF_CU(ctx, cudaMemcpyAsync(hp + hb + cb, d_stats, 32, cudaMemcpyDeviceToHost, ctx->stream));
         PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        s = ctx_queue_status(ctx);
+        if (s != PCF_OK) return s;
         if (hb) memcpy(hist, hp, hb);
         unsigned long long hs[4];
         memcpy(hs, hp + hb + cb, sizeof(hs));

@@ -12,6 +12,7 @@
 // Cell id = (ix*P + iy)*P + iz with ix = (int)(x / cell), the reference's
 // binning (create_grid.cuh:131-133) clamped to [0, P-1].
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <cmath>
 #include <cstdlib>
@@ -341,7 +342,7 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
         g->cells = std::move(hit);
         return PCF_OK;
     }
-    static uint64_t next_serial = 0;
+    static std::atomic<uint64_t> next_serial{0};  // contexts on several host threads build grids
     std::shared_ptr<CellGrid> cg(new CellGrid);
     cg->serial = ++next_serial;
     cg->soa.pool = cg->cell_start.pool = g->pool;

@@ -1,7 +1,9 @@
 // legacy.cu -- the reference's C++ entry points (include/pcf_legacy.h) on
-// top of the C ABI: gather each catalog from the caller's device arrays,
-// grid it, count, and write the reference's files.
+// top of the C ABI: grid each catalog straight from the caller's device
+// arrays, count, and write the reference's files.
 #include <chrono>
+#include <cmath>
+#include <cstring>
 #include <iostream>
 #include <vector>
 
@@ -11,40 +13,80 @@
 
 namespace {
 
-// Points of the nodes [node_off, node_off + nnodes) of a device DNode array
-// (their start/end index the device point array), copied to the host.
-bool gather(const DNode *dnode, const PointW3D *pts, int node_off, int nnodes,
-            std::vector<pcf_point> &out) {
-    out.clear();
+// The points of nodes [node_off, node_off + nnodes) of a device DNode array
+// form one contiguous range [lo, hi) of the device point array (the nodes'
+// start / end index it, cuda/main.cu:300-317).  Only the node table is read
+// back; the points stay on the device.
+bool node_range(const DNode *dnode, int node_off, int nnodes, int &lo, int &hi) {
+    lo = hi = 0;
     if (nnodes <= 0) return true;
     std::vector<DNode> h((size_t)nnodes);
     if (cudaMemcpy(h.data(), dnode + node_off, sizeof(DNode) * nnodes, cudaMemcpyDeviceToHost) != cudaSuccess)
         return false;
-    int lo = h[0].start, hi = h[0].end;
+    lo = h[0].start;
+    hi = h[0].end;
     for (const DNode &n : h) {
         lo = std::min(lo, n.start);
         hi = std::max(hi, n.end);
     }
-    out.resize((size_t)(hi - lo));
-    return cudaMemcpy(out.data(), pts + lo, sizeof(PointW3D) * (hi - lo), cudaMemcpyDeviceToHost) ==
-           cudaSuccess;
+    return true;
 }
 
-float auto_box(const std::vector<pcf_point> &a, const std::vector<std::vector<pcf_point>> &r) {
-    double mx = 0;
-    auto scan = [&](const std::vector<pcf_point> &v) {
-        for (const pcf_point &p : v) mx = std::max(mx, (double)std::max(p.x, std::max(p.y, p.z)));
+// Largest coordinate of n device points (all >= 0, so their float bits
+// order like unsigned integers).
+__global__ void k_max_coord(const PointW3D *__restrict__ p, int n, unsigned *out) {
+    unsigned m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = max(m, max(__float_as_uint(fmaxf(p[i].x, 0.f)),
+                       max(__float_as_uint(fmaxf(p[i].y, 0.f)), __float_as_uint(fmaxf(p[i].z, 0.f)))));
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// A device catalog: the point range of its nodes.
+struct DevCat {
+    const PointW3D *p = nullptr;
+    int n = 0;
+};
+
+bool device_catalog(const DNode *dnode, const PointW3D *pts, int node_off, int nnodes, DevCat &c) {
+    int lo, hi;
+    if (!node_range(dnode, node_off, nnodes, lo, hi)) return false;
+    c.p = pts + lo;
+    c.n = hi - lo;
+    return true;
+}
+
+// Box of the non-periodic entry points, which receive none: ceil(max + 1)
+// over every catalog, as the reference sizes it from its files
+// (cuda/create_grid.cuh:75).
+bool auto_box(const DevCat &a, const std::vector<DevCat> &r, float &box) {
+    unsigned *d = nullptr;
+    if (cudaMalloc(&d, sizeof(unsigned)) != cudaSuccess) return false;
+    cudaMemset(d, 0, sizeof(unsigned));
+    auto scan = [&](const DevCat &c) {
+        if (c.n > 0) k_max_coord<<<std::min(1024, (c.n + 255) / 256), 256>>>(c.p, c.n, d);
     };
     scan(a);
-    for (auto &v : r) scan(v);
-    return (float)std::ceil(mx + 1);
+    for (const DevCat &c : r) scan(c);
+    unsigned h = 0;
+    const bool ok = cudaMemcpy(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost) == cudaSuccess;
+    cudaFree(d);
+    float mx;
+    memcpy(&mx, &h, sizeof(mx));
+    box = (float)std::ceil((double)mx + 1.0);
+    return ok;
 }
 
 struct Session {
     pcf_ctx *ctx = nullptr;
     bool ok = true;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
-    Session() { check(pcf_ctx_create(0, &ctx), "pcf_ctx_create"); }
+    Session() {
+        int dev = 0;  // the caller's current device, which holds its arrays
+        if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+        check(pcf_ctx_create(dev, &ctx), "pcf_ctx_create");
+    }
     ~Session() {
         if (ctx) pcf_ctx_destroy(ctx);
         if (ok)
@@ -65,24 +107,25 @@ struct Session {
 void two_point(std::string *names, DNode *dD, PointW3D *pD, int nD, DNode *dR, PointW3D *pR,
                int *nR, int *accR, int nrand, int bn, float box, float dmax, bool ani, bool bpc) {
     Session S;
-    std::vector<pcf_point> D;
-    std::vector<std::vector<pcf_point>> R((size_t)std::max(nrand, 0));
-    if (!gather(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "gather"); return; }
+    DevCat D;
+    std::vector<DevCat> R((size_t)std::max(nrand, 0));
+    if (!device_catalog(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "node table"); return; }
     for (int i = 0; i < nrand; ++i)
-        if (!gather(dR, pR, accR[i], nR[i], R[i])) { S.check(PCF_ERR_CUDA, "gather"); return; }
-    if (!bpc) box = auto_box(D, R);
+        if (!device_catalog(dR, pR, accR[i], nR[i], R[i])) { S.check(PCF_ERR_CUDA, "node table"); return; }
+    if (!bpc && !auto_box(D, R, box)) { S.check(PCF_ERR_CUDA, "box"); return; }
     const int kind = ani ? PCF_ANI : PCF_ISO;
     const uint32_t f = bpc ? (PCF_BPC | (ani ? 0u : (uint32_t)PCF_DS_EXACT)) : 0u;
     const std::string tag = std::string(ani ? "ani_" : "iso_") + (bpc ? "BPC_" : "");
     std::vector<double> h(ani ? (size_t)bn * bn : (size_t)bn);
     auto save = [&](const std::string &n) { ani ? pcfio::save2d(n, bn, h.data()) : pcfio::save1d(n, bn, h.data()); };
     pcf_grid *gD = nullptr;
-    if (!S.check(pcf_grid_build(S.ctx, D.data(), (int64_t)D.size(), box, 0, &gD), "grid")) return;
+    auto pts = [](const DevCat &c) { return reinterpret_cast<const pcf_point *>(c.p); };
+    if (!S.check(pcf_grid_build(S.ctx, pts(D), D.n, box, 0, &gD), "grid")) return;
     if (S.check(pcf_count_pairs(S.ctx, kind, gD, nullptr, bn, dmax, f, h.data(), nullptr), "DD"))
         save("DD" + tag + names[0]);
     for (int i = 0; i < nrand && S.ok; ++i) {
         pcf_grid *gR = nullptr;
-        if (!S.check(pcf_grid_build(S.ctx, R[i].data(), (int64_t)R[i].size(), box, 0, &gR), "grid")) break;
+        if (!S.check(pcf_grid_build(S.ctx, pts(R[i]), R[i].n, box, 0, &gR), "grid")) break;
         if (S.check(pcf_count_pairs(S.ctx, kind, gR, nullptr, bn, dmax, f, h.data(), nullptr), "RR"))
             save("RR" + tag + names[i + 1]);
         if (S.check(pcf_count_pairs(S.ctx, kind, gD, gR, bn, dmax, f, h.data(), nullptr), "DR"))
@@ -96,12 +139,12 @@ void two_point(std::string *names, DNode *dD, PointW3D *pD, int nD, DNode *dR, P
 void three_point(std::string *names, DNode *dD, PointW3D *pD, int nD, DNode *dR, PointW3D *pR,
                  int *nR, int *accR, int nrand, int bn, float box, float dmax, bool ani, bool bpc) {
     Session S;
-    std::vector<pcf_point> D;
-    std::vector<std::vector<pcf_point>> R((size_t)std::max(nrand, 0));
-    if (!gather(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "gather"); return; }
+    DevCat D;
+    std::vector<DevCat> R((size_t)std::max(nrand, 0));
+    if (!device_catalog(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "node table"); return; }
     for (int i = 0; i < nrand; ++i)
-        if (!gather(dR, pR, accR[i], nR[i], R[i])) { S.check(PCF_ERR_CUDA, "gather"); return; }
-    if (!bpc) box = auto_box(D, R);
+        if (!device_catalog(dR, pR, accR[i], nR[i], R[i])) { S.check(PCF_ERR_CUDA, "node table"); return; }
+    if (!bpc && !auto_box(D, R, box)) { S.check(PCF_ERR_CUDA, "box"); return; }
     const int kind = ani ? PCF_ANI : PCF_ISO;
     const uint32_t f = bpc ? PCF_BPC : 0u;
     const std::string tag = std::string(ani ? "ani_" : "iso_") + (bpc ? "BPC_" : "");
@@ -109,12 +152,13 @@ void three_point(std::string *names, DNode *dD, PointW3D *pD, int nD, DNode *dR,
     std::vector<double> h(nb);
     auto save = [&](const std::string &n) { ani ? pcfio::save5d(n, bn, h.data()) : pcfio::save3d(n, bn, h.data()); };
     pcf_grid *gD = nullptr;
-    if (!S.check(pcf_grid_build(S.ctx, D.data(), (int64_t)D.size(), box, 0, &gD), "grid")) return;
+    auto pts = [](const DevCat &c) { return reinterpret_cast<const pcf_point *>(c.p); };
+    if (!S.check(pcf_grid_build(S.ctx, pts(D), D.n, box, 0, &gD), "grid")) return;
     if (S.check(pcf_count_triplets(S.ctx, kind, gD, nullptr, bn, dmax, f, h.data(), nullptr), "DDD"))
         save("DDD" + tag + names[0]);
     for (int i = 0; i < nrand && S.ok; ++i) {
         pcf_grid *gR = nullptr;
-        if (!S.check(pcf_grid_build(S.ctx, R[i].data(), (int64_t)R[i].size(), box, 0, &gR), "grid")) break;
+        if (!S.check(pcf_grid_build(S.ctx, pts(R[i]), R[i].n, box, 0, &gR), "grid")) break;
         if (S.check(pcf_count_triplets(S.ctx, kind, gR, nullptr, bn, dmax, f, h.data(), nullptr), "RRR"))
             save("RRR" + tag + names[i + 1]);
         if (S.check(pcf_count_triplets(S.ctx, kind, gD, gR, bn, dmax, f, h.data(), nullptr), "DDR"))
@@ -164,10 +208,12 @@ void pcf_3aniBPC(std::string *n, DNode *dD, PointW3D *pD, int nD, DNode *dR, Poi
 void pcf_2iso_BPCanalytic(std::string name, DNode *dD, PointW3D *pD, int nD, int bn, int np, float,
                           float box, float dmax) {
     Session S;
-    std::vector<pcf_point> D;
-    if (!gather(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "gather"); return; }
+    DevCat D;
+    if (!device_catalog(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "node table"); return; }
     pcf_grid *g = nullptr;
-    if (!S.check(pcf_grid_build(S.ctx, D.data(), (int64_t)D.size(), box, 0, &g), "grid")) return;
+    if (!S.check(pcf_grid_build(S.ctx, reinterpret_cast<const pcf_point *>(D.p), D.n, box, 0, &g),
+                 "grid"))
+        return;
     std::vector<double> h((size_t)bn);
     if (S.check(pcf_count_pairs(S.ctx, PCF_ISO, g, nullptr, bn, dmax, PCF_BPC | PCF_DS_EXACT, h.data(), nullptr), "DD"))
         pcfio::save1d("DDiso_BPCanalytic_" + name, bn, h.data());
@@ -181,10 +227,12 @@ void pcf_2iso_BPCanalytic(std::string name, DNode *dD, PointW3D *pD, int nD, int
 void pcf_3isoBPC_analytic(std::string name, DNode *dD, PointW3D *pD, int nD, int bn, int, float,
                           float box, float dmax) {
     Session S;
-    std::vector<pcf_point> D;
-    if (!gather(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "gather"); return; }
+    DevCat D;
+    if (!device_catalog(dD, pD, 0, nD, D)) { S.check(PCF_ERR_CUDA, "node table"); return; }
     pcf_grid *g = nullptr;
-    if (!S.check(pcf_grid_build(S.ctx, D.data(), (int64_t)D.size(), box, 0, &g), "grid")) return;
+    if (!S.check(pcf_grid_build(S.ctx, reinterpret_cast<const pcf_point *>(D.p), D.n, box, 0, &g),
+                 "grid"))
+        return;
     const size_t n3 = (size_t)bn * bn * bn;
     std::vector<double> ddd(n3), ddr(n3), rrr(n3);
     if (S.check(pcf_analytic_3iso(S.ctx, g, bn, dmax, 0, 0, 1, ddd.data(), ddr.data(), rrr.data(), nullptr),

@@ -87,6 +87,8 @@ extern "C" pcf_status pcf_count_pairs_noalloc(const pcf_point *a, int64_t na, co
         if (2 * k + 2 > P) return PCF_ERR_UNSUPPORTED;
     }
     const int64_t ncell = (int64_t)P * P * P;
+    // the same bound as pcf_count_pairs (bins^2 accumulators at most 2^24)
+    if (ani && (int64_t)bins * bins > (1 << 24)) return PCF_ERR_UNSUPPORTED;
     const int nbins = ani ? bins * bins : bins;
     std::vector<RowDesc> rows;
     plan_rows(P, box, dmax, ani, !cross, rows);

@@ -35,6 +35,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <type_traits>
 
@@ -100,6 +102,9 @@ struct PairArgs {
     int budget;  // adds one shared counter absorbs between flushes
     int fast;    // 0: every pair in range takes the FP64 rule (bins > 255: r + 256
                  // no longer has a fixed exponent)
+    const unsigned *ctrl;  // abort request polled at every ticket (null: none)
+    unsigned *status;      // where a warp that gives up records why (null: none)
+    long long max_tickets; // iteration cap: tickets one warp may take
 };
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -423,8 +428,13 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
     if (lane == 0) tk = (long long)atomicAdd(A.counter, 1ull);
     tk = __shfl_sync(kFull, tk, 0);
     ticket_items(tk, ib, ie);
+    long long taken = 1;  // tickets this warp has taken (iteration cap)
+    unsigned stop = 0;    // abort request, read with each ticket
     while (ib < A.n_items) {
-      if (lane == 0) tk = (long long)atomicAdd(A.counter, 1ull);  // prefetch the next ticket
+      if (lane == 0) {  // prefetch the next ticket (and the abort word with it)
+          tk = (long long)atomicAdd(A.counter, 1ull);
+          if (A.ctrl) stop = ctrl_load(A.ctrl);
+      }
       for (long long it_idx = ib; it_idx < ie; ++it_idx) {
         if (it_idx >= ws.job_end) {  // entering another job: flush this one's histogram
             if (ws.cj >= 0) flush(ws.slot, J.wunscale);
@@ -747,6 +757,14 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
       }
       tk = __shfl_sync(kFull, tk, 0);
       ticket_items(tk, ib, ie);
+      // give up the queue on an abort request or past the iteration cap
+      // (the histogram copy is still flushed below; the host discards it)
+      stop = __shfl_sync(kFull, stop, 0) ? PCF_GAVE_UP_ABORT : 0u;
+      if (++taken > A.max_tickets) stop |= PCF_GAVE_UP_CAP;
+      if (stop) {
+          if (lane == 0 && A.status) ctrl_store(A.status, stop);
+          break;
+      }
     }
     // per-warp flush (no CTA barrier: warps leave as the queue drains)
     __syncwarp();
@@ -918,40 +936,40 @@ template <int KIND, bool W, int HM, bool C>
 static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items, cudaStream_t st,
                               int sm_count, int device) {
     auto kfn = k_pairs<KIND, W, HM, C>;
-    // attribute / occupancy queries cost microseconds each: do them once per
-    // (device, variant, shared-memory size)
-    constexpr int kDev = 64;
-    static size_t attr_smem[kDev] = {};
-    static size_t occ_smem[kDev];
-    static int occ_per_sm[kDev];
-    static bool init = false;
-    if (!init) {
-        for (int d = 0; d < kDev; ++d) occ_smem[d] = ~(size_t)0;
-        init = true;
-    }
-    const int dv = (device >= 0 && device < kDev) ? device : 0;
-    cudaError_t e;
-    // the opt-in limit covers static (per-warp state) + dynamic shared memory
-    if (smem > attr_smem[dv]) {
-        e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_smem[dv] = smem;
-    }
-    if (occ_smem[dv] != smem) {
-        int per = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem);
-        if (e != cudaSuccess) return e;
-        occ_per_sm[dv] = std::max(1, per);
-        occ_smem[dv] = smem;
+    // occupancy queries cost microseconds: cached per (device, shared-memory
+    // size) and instantiation, under a lock (several host threads launch)
+    struct Occ {
+        std::mutex mu;
+        std::map<std::pair<int, size_t>, int> per_sm;
+    };
+    static Occ occ;
+    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(kfn), device, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lk(occ.mu);
+        auto it = occ.per_sm.find({device, smem});
+        if (it != occ.per_sm.end()) {
+            per_sm = it->second;
+        } else {
+            int per = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem);
+            if (e != cudaSuccess) return e;
+            per_sm = std::max(1, per);
+            occ.per_sm[{device, smem}] = per_sm;
+        }
     }
     const long long want = (n_items + kWarps - 1) / kWarps;
-    const int grid = (int)std::max(1LL, std::min<long long>(want, (long long)sm_count * occ_per_sm[dv]));
+    const int grid = (int)std::max(1LL, std::min<long long>(want, (long long)sm_count * per_sm));
     // runs of k items per ticket while a queue holds >= 32 runs per warp
     PairArgs B = A;
     const long long warps = (long long)grid * kWarps;
     B.kchunk = (int)std::max(1LL, std::min<long long>(kChunkMax, n_items / (warps * 32)));
     B.n_chunked = B.kchunk > 1 ? std::max(0LL, n_items - 2 * warps) : 0;
     B.t_chunked = (B.n_chunked + B.kchunk - 1) / B.kchunk;
+    // a warp can take at most every ticket of the queue plus the one that
+    // finds it empty
+    B.max_tickets = B.t_chunked + (n_items - B.n_chunked) + 2;
     kfn<<<grid, kThreads, smem, st>>>(B);
     return cudaGetLastError();
 }
@@ -1060,6 +1078,9 @@ static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
     A.chunk = 1 << 22;
     A.budget = 1 << 30;
     A.fast = pl.rule.bins <= 255 ? 1 : 0;
+    A.ctrl = pl.ctrl;
+    A.status = pl.status;
+    A.max_tickets = n_items + 2;  // refined per launch shape in launch_one
     return A;
 }
 

@@ -71,6 +71,21 @@ __device__ __forceinline__ int exact_slot(double dx, double dy, double dz, const
     return bz * r.bins + bp;
 }
 
+// Queue control words in mapped host memory (pcf_ctx::h_ctrl): system-scope
+// loads and stores, so a request the host writes during a launch is seen by
+// the running kernel, and the kernel's record reaches the host.
+__device__ __forceinline__ unsigned ctrl_load(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.relaxed.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void ctrl_store(unsigned *p, unsigned v) {
+    asm volatile("st.relaxed.sys.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+// Status bits a kernel records when it gives up its queue.
+#define PCF_GAVE_UP_ABORT 1u
+#define PCF_GAVE_UP_CAP 2u
+
 // ---------------------------------------------------------------------------
 // Device-side layout.
 // ---------------------------------------------------------------------------
@@ -228,6 +243,15 @@ struct pcf_ctx {
     void *h_pinned = nullptr;
     size_t h_pinned_bytes = 0;
     int64_t launches = 0;  // kernels launched by this context
+    // Queue control in mapped host memory: ctrl[0] is the abort request (set
+    // by any host thread, polled by the persistent kernels at every work
+    // item), ctrl[1] records that a kernel gave up its queue (bit 0: abort
+    // request, bit 1: iteration cap).  d_ctrl is the device's view of it.
+    unsigned *h_ctrl = nullptr;
+    unsigned *d_ctrl = nullptr;
+    bool abort_host_check = true;  // refuse calls while the request is set
+    // adds a triplet kernel's shared u32 histogram absorbs between flushes
+    unsigned long long trip_flush_budget = 1ull << 31;
     std::map<std::string, std::shared_ptr<struct BatchGraph>> graphs;  // pcf_batch_pairs(PCF_GRAPH)
 };
 
@@ -235,6 +259,11 @@ struct pcf_ctx {
 // Internal host API (implemented in grid.cu / pairs.cu / triplets.cu ...).
 // ---------------------------------------------------------------------------
 pcf_status pcf_fail(pcf_ctx *ctx, cudaError_t e, const char *what);
+// Raises kernel `fn`'s dynamic shared-memory limit on `device` to at least
+// `bytes`.  Thread-safe (the request server drives one library from several
+// host threads) and monotone: the limit is never lowered, so a launch that
+// fits the limit one thread set stays valid while another thread raises it.
+cudaError_t ensure_smem_limit(const void *fn, int device, size_t bytes);
 #define PCF_CU(ctx, call)                                   \
     do {                                                    \
         cudaError_t _e = (call);                            \
@@ -266,6 +295,10 @@ void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self
                 int resident_warps);
 
 pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes);
+// PCF_ERR_TIMEOUT if an abort is requested (before a call launches) or if a
+// kernel gave up its queue (after the call's work is complete), else PCF_OK.
+pcf_status ctx_abort_requested(pcf_ctx *ctx);
+pcf_status ctx_queue_status(pcf_ctx *ctx);
 
 // One pair-kernel launch (pairs.cu).
 struct PairLaunch {
@@ -282,6 +315,10 @@ struct PairLaunch {
     int wbudget = 0;     // limb adds between flushes of a fixed-point copy
     double wunscale = 0.0;  // single-job launches: weight_unscale(home, cand)
     bool count = true;   // weighted launches: count in-range pairs (statistics)
+    // queue control (pcf_ctx_abort): the abort word the kernel polls at every
+    // ticket and the status word it sets when it gives up; null: no polling
+    const unsigned *ctrl = nullptr;
+    unsigned *status = nullptr;
 };
 // Enables the fixed-point weighted histograms when every grid of the launch
 // has exact integer weights and any product fits the three-limb budget.

@@ -6,14 +6,17 @@
 //
 // Same flags, defaults, paths (../data/<name> in, ../results/<name> out),
 // file names and text formats as the reference; the histograms come from
-// libpcf.so (include/pcf.h).  Differences, all documented in the design
-// notes: library errors print a message and exit(1) instead of crashing;
-// 3-point names are not accumulated across random files
-// (pcf3iso.cuh:127); the 3ani histograms are written in full (bins^5,
-// save_histogram5D) rather than their first bins^3 values; -p is accepted
-// but the library picks its own cell size for each dmax.
+// libpcf.so (include/pcf.h).  Differences: library errors print a message
+// and exit(1) instead of crashing; 3-point names are not accumulated across
+// random files (pcf3iso.cuh:127); the 3ani histograms are written in full
+// (bins^5, save_histogram5D) rather than their first bins^3 values; -p sets
+// the cells per box side, which the library uses when a periodic stencil
+// fits them (2*ceil(dmax/cell) + 2 <= P) and otherwise replaces with its own
+// choice (results do not depend on it); -rd counts RR and DR of every random
+// catalog of the directory in one persistent launch (pcf_batch_pairs).
 #include <dirent.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -151,6 +154,20 @@ int main(int argc, char **argv) {
             CHECK(pcf_analytic_rr(ctx, bn, np, size_box, dmax, 1, h.data()));
             save("RR" + sfx + tag + data_name);
             save("DR" + sfx + tag + data_name);  // the reference writes RR as DR (pcf2isoBPC.cuh:265)
+        } else if (gR.size() > 1) {
+            // -rd: every random catalog of the directory in one persistent
+            // launch (the reference launches two kernels per file,
+            // cuda/pcf2iso.cuh:96-104)
+            const size_t nb = h.size(), nr = gR.size();
+            std::vector<double> rr(nb * nr), dr(nb * nr);
+            CHECK(pcf_batch_pairs(ctx, kind, gD, gR.data(), (int)nr, bn, dmax, f, nullptr, rr.data(),
+                                  dr.data(), nullptr));
+            for (size_t i = 0; i < nr; ++i) {
+                std::copy(rr.begin() + i * nb, rr.begin() + (i + 1) * nb, h.begin());
+                save("RR" + sfx + tag + rand_labels[i]);
+                std::copy(dr.begin() + i * nb, dr.begin() + (i + 1) * nb, h.begin());
+                save("DR" + sfx + tag + rand_labels[i]);
+            }
         } else {
             for (size_t i = 0; i < gR.size(); ++i) {
                 CHECK(pcf_count_pairs(ctx, kind, gR[i], nullptr, bn, dmax, f, h.data(), nullptr));

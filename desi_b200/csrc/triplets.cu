@@ -73,6 +73,11 @@ struct TripArgs {
     double *g_wsum;               // bins^3 (weighted)
     int hist_in_smem;
     unsigned long long *g_stats;
+    // adds the shared u32 histogram absorbs between flushes into g_count
+    // (a counter then never wraps: one slot gets at most that many adds)
+    unsigned long long flush_budget;
+    const unsigned *ctrl;  // abort request, polled with every anchor (null: none)
+    unsigned *status;      // where a CTA that gives up records why (null: none)
 };
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -236,11 +241,28 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
     float *swJ = reinterpret_cast<float *>(sK + (MIXED ? A.capK : 0));
     float *swK = swJ + (WEIGHTED ? A.capJ : 0);
     __shared__ int s_anchor, s_nJ, s_nK, s_unit;
+    __shared__ unsigned s_stop;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (A.hist_in_smem)
         for (int k = tid; k < nb3 + 32; k += kTThreads) U[k] = 0u;
     unsigned n_rechk = 0;
     unsigned long long n_tri = 0;
+    // pair tests since the shared histogram's last flush: each adds at most
+    // once, so no u32 slot can pass this count
+    unsigned long long since = 0;
+    long long taken = 0;  // anchors this CTA took (iteration cap: nX + 1)
+    // adds U into the global u64 histogram and clears it (whole CTA)
+    auto flush_u = [&]() {
+        __syncthreads();
+        for (int k = tid; k < nb3; k += kTThreads) {
+            const unsigned v = U[k];
+            if (v) {
+                atomicAdd(A.g_count + k, (unsigned long long)v);
+                U[k] = 0u;
+            }
+        }
+        __syncthreads();
+    };
     __syncthreads();
     float4 *gJ = A.gJ + (size_t)blockIdx.x * A.gcap;
     float4 *gK = A.gK ? A.gK + (size_t)blockIdx.x * A.gcap : nullptr;
@@ -253,10 +275,14 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
             s_nJ = 0;
             s_nK = 0;
             s_unit = 0;
+            unsigned stop = (A.ctrl && ctrl_load(A.ctrl)) ? PCF_GAVE_UP_ABORT : 0u;
+            if (++taken > (long long)A.nX + 1) stop |= PCF_GAVE_UP_CAP;
+            if (stop && A.status) ctrl_store(A.status, stop);
+            s_stop = stop;
         }
         __syncthreads();
         const int i = s_anchor;
-        if (i >= A.nX) break;
+        if (i >= A.nX || s_stop) break;
         const float hx = A.X.x[i], hy = A.X.y[i], hz = A.X.z[i];
         const float hw = WEIGHTED ? A.X.w[i] : 1.f;
         const int P = A.P;
@@ -302,9 +328,34 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
             WJ = gwJ;
             WK = MIXED ? gwK : gwJ;
         }
+        // K entry k is LK[kstepK * k]: the pooled K list grows downwards from
+        // the end of the shared buffer
+        int kstepK = 1;
+        if (pool && LJ == sJ) {
+            LK = sJ + A.capJ - 1;
+            kstepK = -1;
+        }
+        // Flush budget of the shared histogram: this anchor adds at most
+        // `tests` times.  Flush first if the total could pass the budget; an
+        // anchor whose tests alone exceed it counts into global memory.
+        bool smem_hist = !WEIGHTED && A.hist_in_smem;
+        if (smem_hist) {
+            const unsigned long long tests =
+                MIXED ? (unsigned long long)nJ * (unsigned long long)nK
+                      : (unsigned long long)nJ * (unsigned long long)(nJ > 0 ? nJ - 1 : 0) / 2;
+            if (tests > A.flush_budget) {
+                smem_hist = false;
+            } else {
+                if (since + tests > A.flush_budget) {
+                    flush_u();
+                    since = 0;
+                }
+                since += tests;
+            }
+        }
         // pass 2: pairs of neighbours.  Rows j are dealt to warps in the
         // order 0, n-1, 1, n-2, ... (XXX rows shrink with j).
-        if (!WEIGHTED && A.hist_in_smem) {
+        if (smem_hist) {
             // the lists' address space is fixed per instantiation, so the
             // shared-memory case (all but overflowing anchors) uses shared loads
             // LKx[kstep * k] is K entry k (kstep -1: the pooled, downward K list)
@@ -425,7 +476,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
             const int ubase = bj * bins * bins;
             const int k0 = MIXED ? 0 : jj + 1;
             for (int kk = k0 + lane; kk < nK; kk += 32) {
-                const float4 ek = LK[kk];
+                const float4 ek = LK[kstepK * kk];
                 const float dx = ek.x - ej.x, dy = ek.y - ej.y, dz = ek.z - ej.z;
                 const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                 const PairRule &r3 = MIXED ? A.rXY : A.rXX;
@@ -443,9 +494,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
                     ++n_tri;
                     if (WEIGHTED) {
                         atomicAdd(A.g_wsum + slot, wij * (double)WK[kk]);
-                    } else if (A.hist_in_smem) {
-                        atomicAdd(U + slot, 1u);
-                    } else {
+                    } else {  // (the shared histogram took the anchor above if it could)
                         atomicAdd(A.g_count + slot, 1ull);
                     }
                 }
@@ -485,19 +534,25 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
     float *swJ = reinterpret_cast<float *>(aK + (MIXED ? A.capK : 0) + 8);
     float *swK = swJ + (WEIGHTED ? A.capJ : 0);
     __shared__ int s_anchor, s_nJ, s_nK;
+    __shared__ unsigned s_stop;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned n_rechk = 0;
     unsigned long long n_tri = 0;
+    long long taken = 0;
     const long long B = bins, B2 = B * B, B3 = B2 * B, B4 = B3 * B;
     for (;;) {
         if (tid == 0) {
             s_anchor = (int)atomicAdd(A.counter, 1ull);
             s_nJ = 0;
             s_nK = 0;
+            unsigned stop = (A.ctrl && ctrl_load(A.ctrl)) ? PCF_GAVE_UP_ABORT : 0u;
+            if (++taken > (long long)A.nX + 1) stop |= PCF_GAVE_UP_CAP;
+            if (stop && A.status) ctrl_store(A.status, stop);
+            s_stop = stop;
         }
         __syncthreads();
         const int i = s_anchor;
-        if (i >= A.nX) break;
+        if (i >= A.nX || s_stop) break;
         const float hx = A.X.x[i], hy = A.X.y[i], hz = A.X.z[i];
         const float hw = WEIGHTED ? A.X.w[i] : 1.f;
         const int P = A.P;
@@ -600,6 +655,7 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
     pcf_grid *Y = const_cast<pcf_grid *>(y_);
     const bool bpc = (flags & PCF_BPC) != 0, mixed = Y != nullptr;
     if (X->n >= (1 << 24) || (Y && Y->n >= (1 << 24))) return PCF_ERR_UNSUPPORTED;
+    if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
     int P = 0;
     pcf_status s = prepare_grids(ctx, X, Y, dmax, PCF_ISO, bpc, &P);
     if (s != PCF_OK) return s;
@@ -625,6 +681,9 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
     A.bpc = bpc ? 1 : 0;
     A.rXX = rXX;
     A.rXY = rXY;
+    A.flush_budget = ctx->trip_flush_budget;
+    A.ctrl = ctx->d_ctrl;
+    A.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
     {
         // windows: the FP32 side |v_k - v_j| carries up to three roundings of
         // coordinate differences (plus the image shift of the anchor when
@@ -709,7 +768,7 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
 
     auto kfn = mixed ? (weighted ? k_triplets<true, true> : k_triplets<true, false>)
                      : (weighted ? k_triplets<false, true> : k_triplets<false, false>);
-    PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PCF_CU(ctx, ensure_smem_limit(reinterpret_cast<const void *>(kfn), ctx->device, smem));
     cudaEvent_t pe0 = nullptr, pe1 = nullptr;
     if (ctx->profile) {
         s = profile_events(ctx, &pe0, &pe1);
@@ -737,6 +796,8 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
         if (hb) PCF_CU(ctx, cudaMemcpyAsync(hp, d_out, hb, cudaMemcpyDeviceToHost, ctx->stream));
         PCF_CU(ctx, cudaMemcpyAsync(hp + hb, A.g_stats, 32, cudaMemcpyDeviceToHost, ctx->stream));
         PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        s = ctx_queue_status(ctx);
+        if (s != PCF_OK) return s;
         if (hb) memcpy(hist, hp, hb);
         unsigned long long hs[4];
         memcpy(hs, hp + hb, sizeof(hs));
@@ -766,6 +827,7 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     pcf_grid *Y = const_cast<pcf_grid *>(y_);
     const bool bpc = (flags & PCF_BPC) != 0, mixed = Y != nullptr;
     if (X->n >= (1 << 24) || (Y && Y->n >= (1 << 24))) return PCF_ERR_UNSUPPORTED;
+    if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
     int P = 0;
     pcf_status s = prepare_grids(ctx, X, Y, dmax, PCF_ISO, bpc, &P);
     if (s != PCF_OK) return s;
@@ -789,6 +851,8 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     A.bpc = bpc ? 1 : 0;
     A.rXX = rXX;
     A.rXY = rXY;
+    A.ctrl = ctx->d_ctrl;
+    A.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
     {
         const double dd = rXX.dd;
         const double rmax = (double)dmax * rXX.ds + 1.0;
@@ -827,7 +891,7 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     PCF_CU(ctx, cudaMemsetAsync(hp, 0, (size_t)n5 * 8 + 128, ctx->stream));
     auto kfn = mixed ? (weighted ? k_triplets_ani<true, true> : k_triplets_ani<true, false>)
                      : (weighted ? k_triplets_ani<false, true> : k_triplets_ani<false, false>);
-    PCF_CU(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PCF_CU(ctx, ensure_smem_limit(reinterpret_cast<const void *>(kfn), ctx->device, smem));
     PCF_CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     kfn<<<ctx->sm_count, kTThreads, smem, ctx->stream>>>(A);
     PCF_CU(ctx, cudaGetLastError());
@@ -843,6 +907,8 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     PCF_CU(ctx, cudaMemcpyAsync(hist, d_out, sizeof(double) * n5,
                                 dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
     PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    s = ctx_queue_status(ctx);
+    if (s != PCF_OK) return s;
     if (hs[3]) {
         ctx->last_error = "neighbour lists of the anisotropic triplet kernel exceed shared memory";
         return PCF_ERR_UNSUPPORTED;

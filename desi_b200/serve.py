@@ -12,6 +12,16 @@ work (in-range pairs at uniform density), unless one has waited longer than
 ``max_wait_s``.  The library calls release the GIL (ctypes), so slots run
 concurrently.
 
+Failure handling (no device fault involved): a request may carry a
+deadline and may be cancelled; a watchdog thread drops pending requests past
+their deadline and, for a running one, asks its slot's context to abort
+(pcf_ctx_abort: the persistent kernels stop at their next work item and the
+call returns PCF_ERR_TIMEOUT), then fails the request's future with
+DeadlineExceeded or RequestCancelled.  A slot whose request outlives
+``stuck_after_s`` is aborted the same way; if it still has not returned
+after a grace period, the slot is retired (its request fails with
+SlotStuck) and the other slots keep serving.
+
 Every result is computed by the same kernels whether a request runs alone
 or in the mix; ``tests/test_serve.py`` checks that the histograms are
 identical both ways.  ``python -m desi_b200.serve`` runs a seeded stream of
@@ -35,6 +45,18 @@ from . import api
 KINDS = ("2iso", "2ani", "3iso")
 
 
+class RequestCancelled(Exception):
+    """The request was cancelled (PcfServer.cancel) before it completed."""
+
+
+class DeadlineExceeded(Exception):
+    """The request did not complete within its deadline."""
+
+
+class SlotStuck(Exception):
+    """The slot running the request stopped responding and was retired."""
+
+
 @dataclass
 class Request:
     kind: str
@@ -45,11 +67,15 @@ class Request:
     bpc: bool = False
     arrival: float = 0.0  # seconds from stream start (run_stream)
     rid: int = 0
+    deadline_s: float | None = None  # from submission; None: no deadline
     future: Future = field(default_factory=Future, repr=False)
     t_submit: float = 0.0
     t_start: float = 0.0
     t_end: float = 0.0
     slot: int = -1
+    # why the request is being stopped (an exception class), set under the
+    # server lock by cancel() or the watchdog
+    stop_reason: type | None = field(default=None, repr=False)
 
 
 def grid_bytes(n: int, partitions: int = 64) -> int:
@@ -91,6 +117,12 @@ class _Slot:
         self.cache_bytes = cache_bytes
         self.used = 0
         self.busy = False
+        self.current: Request | None = None  # the running request
+        self.aborted = False                 # abort requested for the current request
+        self.retired = False                 # declared stuck: takes no more requests
+
+    def abort(self, on: bool = True) -> None:
+        self.ctx.abort(on)
 
     def grid(self, name: str, keep=()) -> api.Grid:
         """The catalog gridded on this slot's device, built on first use and
@@ -136,12 +168,21 @@ class _Slot:
 
 class PcfServer:
     def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int | None = None,
-                 cache_bytes: int = 8 << 30, max_wait_s: float = 0.05):
+                 cache_bytes: int = 8 << 30, max_wait_s: float = 0.05,
+                 stuck_after_s: float | None = None, stuck_grace_s: float = 2.0,
+                 watchdog_s: float = 0.01, slot_factory=None):
         """hbm_budget: bytes the running requests may hold at once (default:
         half the free device memory); cache_bytes: resident grids per slot;
         max_wait_s: a pending request older than this runs before shorter
-        ones (bounds the wait that shortest-first scheduling adds)."""
+        ones (bounds the wait that shortest-first scheduling adds);
+        stuck_after_s: a request running longer than this has its slot
+        aborted, and a slot that has not returned stuck_grace_s later is
+        retired (None: no limit); watchdog_s: the watchdog's period;
+        slot_factory(server, index): builds a slot (tests pass host-only
+        stand-ins; default: a library context on `device`)."""
         self.max_wait_s = max_wait_s
+        self.stuck_after_s = stuck_after_s
+        self.stuck_grace_s = stuck_grace_s
         if hbm_budget is None:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
@@ -152,11 +193,15 @@ class PcfServer:
         self._pending: collections.deque = collections.deque()
         self._in_use = 0
         self._stop = False
-        self.slots = [_Slot(self, i, device, cache_bytes) for i in range(slots)]
+        make = slot_factory or (lambda srv, i: _Slot(srv, i, device, cache_bytes))
+        self.slots = [make(self, i) for i in range(slots)]
         self._threads = [threading.Thread(target=self._worker, args=(s,), daemon=True)
                          for s in self.slots]
         for t in self._threads:
             t.start()
+        self._watchdog_s = watchdog_s
+        self._watch = threading.Thread(target=self._watchdog, daemon=True)
+        self._watch.start()
 
     # -- catalogs ----------------------------------------------------------
     def register(self, name: str, points: np.ndarray, box: float) -> None:
@@ -174,6 +219,69 @@ class PcfServer:
             self._pending.append(req)
             self._lock.notify_all()
         return req.future
+
+    def cancel(self, req: Request) -> bool:
+        """Cancels a pending or running request; its future raises
+        RequestCancelled.  Returns False if it had already completed."""
+        with self._lock:
+            if req.future.done():
+                return False
+            if req in self._pending:
+                self._pending.remove(req)
+                self._finish(req, exc=RequestCancelled(f"request {req.rid}"))
+                return True
+            req.stop_reason = RequestCancelled
+            self._abort_slot_of(req)
+            return True
+
+    # -- failure handling (caller holds the lock) ---------------------------
+    def _finish(self, req: Request, result=None, exc: BaseException | None = None) -> None:
+        if req.future.done():
+            return
+        req.t_end = req.t_end or time.perf_counter()
+        if exc is not None:
+            req.future.set_exception(exc)
+        else:
+            req.future.set_result(result)
+
+    def _abort_slot_of(self, req: Request) -> None:
+        for sl in self.slots:
+            if sl.current is req and not sl.aborted:
+                sl.aborted = True
+                try:
+                    sl.abort(True)
+                except Exception:  # pragma: no cover - the slot is failing anyway
+                    pass
+
+    def _watchdog(self) -> None:
+        """Deadlines of pending and running requests, stuck slots."""
+        while True:
+            time.sleep(self._watchdog_s)
+            with self._lock:
+                if self._stop:
+                    return
+                now = time.perf_counter()
+                for r in list(self._pending):
+                    if r.deadline_s is not None and now > r.t_submit + r.deadline_s:
+                        self._pending.remove(r)
+                        self._finish(r, exc=DeadlineExceeded(f"request {r.rid} (pending)"))
+                for sl in self.slots:
+                    r = sl.current
+                    if r is None or sl.retired:
+                        continue
+                    if r.deadline_s is not None and now > r.t_submit + r.deadline_s \
+                            and r.stop_reason is None:
+                        r.stop_reason = DeadlineExceeded
+                        self._abort_slot_of(r)
+                    if self.stuck_after_s is not None and now - r.t_start > self.stuck_after_s:
+                        if r.stop_reason is None:
+                            r.stop_reason = SlotStuck
+                        self._abort_slot_of(r)
+                        if now - r.t_start > self.stuck_after_s + self.stuck_grace_s:
+                            # the slot did not come back from the abort: retire it
+                            sl.retired = True
+                            self._finish(r, exc=SlotStuck(f"slot {sl.idx}, request {r.rid}"))
+                            self._lock.notify_all()
 
     def _admissible(self, req: Request) -> bool:
         """Admit while the running requests' footprints plus this one fit the
@@ -213,7 +321,7 @@ class PcfServer:
             with self._lock:
                 req = None
                 while req is None:
-                    if self._stop:
+                    if self._stop or slot.retired:
                         return
                     req = self._pick()
                     if req is None:
@@ -221,19 +329,35 @@ class PcfServer:
                 sizes = {k: len(v["points"]) for k, v in self.catalogs.items()}
                 fp = request_bytes(req, sizes)
                 self._in_use += fp
-            req.slot = slot.idx
-            req.t_start = time.perf_counter()
+                req.slot = slot.idx
+                req.t_start = time.perf_counter()
+                slot.current = req
+            res, err = None, None
             try:
                 res = slot.run(req)
-                req.t_end = time.perf_counter()
-                req.future.set_result(res)
             except Exception as e:  # reported to the caller, the slot keeps serving
+                err = e
+            with self._lock:
                 req.t_end = time.perf_counter()
-                req.future.set_exception(e)
-            finally:
-                with self._lock:
-                    self._in_use -= fp
-                    self._lock.notify_all()
+                slot.current = None
+                if req.stop_reason is not None:
+                    # stopped by cancel(), a deadline or the stuck-slot watchdog:
+                    # whatever the call returned, the request failed for that reason
+                    self._finish(req, exc=req.stop_reason(f"request {req.rid}"))
+                elif err is not None:
+                    self._finish(req, exc=err)
+                else:
+                    self._finish(req, result=res)
+                if slot.aborted:
+                    slot.aborted = False
+                    try:
+                        slot.abort(False)  # clear the request before the next call
+                    except Exception:  # pragma: no cover
+                        slot.retired = True
+                self._in_use -= fp
+                self._lock.notify_all()
+                if slot.retired:
+                    return
 
     def drop_grids(self) -> None:
         """Frees every slot's resident grids (their device memory returns to
@@ -251,10 +375,14 @@ class PcfServer:
             self._lock.notify_all()
         for t in self._threads:
             t.join(timeout=5)
-        for s in self.slots:
-            for g, _ in s.cache.values():
+        self._watch.join(timeout=5)
+        for s, t in zip(self.slots, self._threads):
+            if t.is_alive():  # a retired slot still inside a call: leave its context
+                continue
+            for g, _ in getattr(s, "cache", {}).values():
                 g.free()
-            s.ctx.close()
+            if hasattr(s, "ctx"):
+                s.ctx.close()
 
     # -- a timed stream ----------------------------------------------------
     def run_stream(self, reqs: list[Request]) -> dict:
@@ -269,11 +397,15 @@ class PcfServer:
         t1 = time.perf_counter()
         lat = np.array([(r.t_end - r.t_submit) * 1e3 for r in reqs])
         units = sum(res["_units"] for res in results)
+        # how much the requests' device spans overlapped (continuous batching)
+        spans = sorted((r.t_start, r.t_end) for r in reqs)
+        overlap = sum(1 for (s0, e0), (s1, _) in zip(spans, spans[1:]) if s1 < e0)
         return {"requests": len(reqs), "wall_s": t1 - t0,
                 "latency_ms": {"p50": float(np.percentile(lat, 50)),
                                "p99": float(np.percentile(lat, 99)),
                                "max": float(lat.max())},
-                "pairs_per_s": units / (t1 - t0), "results": results}
+                "pairs_per_s": units / (t1 - t0), "overlapping_starts": overlap,
+                "results": results}
 
 
 def make_stream(n_requests: int, rate_hz: float, seed: int = 5000, n_max: int = 200_000,

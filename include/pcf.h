@@ -52,7 +52,8 @@ typedef enum pcf_status {
     PCF_ERR_NO_MEMORY = -3,    /* device or host allocation failed                   */
     PCF_ERR_UNSUPPORTED = -4,  /* e.g. periodic boundaries with dmax >= box/2        */
     PCF_ERR_OUT_OF_BOX = -5,   /* a coordinate outside [0, box)                      */
-    PCF_ERR_TIMEOUT = -6,      /* a bounded device wait gave up                      */
+    PCF_ERR_TIMEOUT = -6,      /* a persistent kernel gave up its work queue: abort
+                                  requested (pcf_ctx_abort) or iteration cap reached */
     PCF_ERR_IO = -7,           /* catalog / histogram file error                     */
     PCF_ERR_MISMATCH = -8      /* grids of different box or partitions               */
 } pcf_status;
@@ -100,6 +101,24 @@ pcf_status pcf_ctx_create(int device, pcf_ctx **out);
 pcf_status pcf_ctx_destroy(pcf_ctx *ctx);
 /* The CUDA stream (cudaStream_t) the context enqueues on. */
 void *pcf_ctx_stream(pcf_ctx *ctx);
+
+/*
+ * Failure handling without a device fault.  pcf_ctx_abort(ctx, 1) asks the
+ * context's persistent kernels (the pair, triplet and batched work queues)
+ * to stop taking work at their next work item; any host thread may call it
+ * while another thread's call runs (the request lives in mapped host memory
+ * that the kernels poll).  While it is set, counting calls return
+ * PCF_ERR_TIMEOUT without launching, and a call whose kernels gave up
+ * returns PCF_ERR_TIMEOUT once its work is complete (partial histograms are
+ * not returned).  Every queue also stops at an iteration cap (more tickets
+ * than the queue holds) with the same status.  pcf_ctx_abort(ctx, 0) clears
+ * the request and the record of kernels that gave up.
+ */
+pcf_status pcf_ctx_abort(pcf_ctx *ctx, int on);
+/* Waits for the context stream; PCF_ERR_TIMEOUT if a kernel of the context
+ * gave up its queue since the last clear (device-output calls report it
+ * here, as they return before their kernels finish). */
+pcf_status pcf_ctx_synchronize(pcf_ctx *ctx);
 
 /*
  * Grid a catalog.  pts may be host or device memory (n points, 16 bytes

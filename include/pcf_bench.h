@@ -25,6 +25,19 @@ enum {
  * _U64, _F32: the same for 64-bit float, 64-bit integer and 32-bit float adds. */
 pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
 
+/* Context options for tests and tuning.
+ *   PCF_OPT_TRIP_FLUSH_BUDGET  adds the isotropic triplet kernel's per-CTA
+ *                              u32 histogram absorbs between flushes into the
+ *                              u64 global histogram (1 .. 2^31, default 2^31;
+ *                              a counter can therefore never wrap).  A small
+ *                              budget forces many flushes (a test of them).
+ *   PCF_OPT_ABORT_HOST_CHECK   0: calls launch even while an abort is
+ *                              requested, so the kernels' own polling is what
+ *                              stops them (a test of it); 1 (default): they
+ *                              return PCF_ERR_TIMEOUT without launching. */
+enum { PCF_OPT_TRIP_FLUSH_BUDGET = 1, PCF_OPT_ABORT_HOST_CHECK = 2 };
+pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value);
+
 /* Kernels this context has launched since it was created. */
 int64_t pcf_ctx_launch_count(const pcf_ctx *ctx);
 

@@ -2,10 +2,12 @@
  * pcf_noalloc.h -- a pair-histogram entry point of libpcf.so that allocates
  * no device memory.  It has no counterpart in the reference.
  *
- * Some callers cannot call cudaMalloc: code running inside a CUDA graph
- * being captured elsewhere, plug-in hosts that own the device memory budget
- * and forbid allocations from libraries, and processes whose allocator is
- * already at its limit.  pcf_count_pairs_noalloc serves them: its scratch
+ * Some callers cannot call cudaMalloc: plug-in hosts that own the device
+ * memory budget and forbid allocations from the libraries they load (a
+ * cudaMalloc there fails, or fragments a pool the host manages itself), and
+ * processes whose allocator is already at its limit, where a library that
+ * allocates per call would fail midway.  pcf_count_pairs_noalloc serves
+ * them: its scratch
  * (the cell-sorted copies of both catalogs, the cell and tile tables, the
  * stencil rows and the histogram accumulators) lives in one fixed array of
  * PCF_NOALLOC_SCRATCH_BYTES in the library's device image, which every GPU
@@ -34,8 +36,9 @@ extern "C" {
  *   hist        device pointer to the output histogram (overwritten)
  *   stream      cudaStream_t to run on (NULL: the legacy default stream)
  * Returns PCF_ERR_UNSUPPORTED when the inputs need more scratch than
- * PCF_NOALLOC_SCRATCH_BYTES.  The call synchronises `stream` once (to size
- * the work queue); hist is complete when `stream` reaches the end of the
+ * PCF_NOALLOC_SCRATCH_BYTES, or an anisotropic histogram has more than 2^24
+ * bins.  The call waits for `stream` once (it reads the tile count back to
+ * size the work queue); hist is complete when `stream` reaches the end of the
  * call's work.  The first call on a device looks up the scratch array's
  * device address; make that first call before any stream capture.  All calls
  * share the one array: calls that overlap on the GPU (other streams, other

@@ -293,9 +293,9 @@ int orc_pairs_m(int ani, int bpc, int self, unsigned rule, int ds_exact, double 
                 for (long j = j0; j < nB; ++j) ORC_PAIR(p, &B[j], self ? 2.0 : 1.0);
             }
         } else {
-            /* ordered pairs: for XX each unordered pair is met twice, from
-             * either end, and adds w_i*w_j each time (the emulated CPU rule
-             * forms 2*w1*w2 itself, so it takes half of that) */
+            /* XX: each unordered pair once, from its lower index, adding
+             * 2*w_i*w_j as the brute-force loop does (the rule is symmetric
+             * in the two points; the emulated CPU rule forms 2*w1*w2 itself) */
 #pragma omp for schedule(dynamic, 64)
             for (long i = 0; i < nA; ++i) {
                 const opt *p = &A[i];
@@ -312,15 +312,8 @@ int orc_pairs_m(int ani, int bpc, int self, unsigned rule, int ds_exact, double 
                             long c = ((long)nx * P + ny) * P + nz;
                             for (long t = bstart[c]; t < bstart[c + 1]; ++t) {
                                 long j = border[t];
-                                if (self && j == i) continue;
-                                if (cpu && self) {
-                                    /* the engine meets each unordered pair once, with the
-                                     * lower cell-order point as p; use the lower index */
-                                    if (j < i) continue;
-                                    ORC_PAIR(p, &B[j], 1.0);
-                                } else {
-                                    ORC_PAIR(p, &B[j], 1.0);
-                                }
+                                if (self && j <= i) continue;
+                                ORC_PAIR(p, &B[j], self ? 2.0 : 1.0);
                             }
                         }
                     }

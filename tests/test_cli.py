@@ -81,9 +81,19 @@ def test_cli_2iso_2ani_plain_bpc_rd(layout):
     assert np.array_equal(_read(res / "DRiso_r.dat"), oracle.pairs(D, R, box=box, bins=20, dmax=30.0))
     _run(["2ani", "-n", str(n), "-f", "d.dat", "-rd", "rands/", "-b", "12", "-d", "30", "-bpc",
           "-s", str(box)], layout / "cuda")
+    # -rd: both random files through one batched launch
+    kw = dict(box=box, bins=12, dmax=30.0, ani=True, bpc=True)
     got = _read(res / "RRani_BPC_rb.dat").reshape(12, 12)
-    assert np.array_equal(got, oracle.pairs(R2, box=box, bins=12, dmax=30.0, ani=True, bpc=True))
-    assert (res / "DRani_BPC_ra.dat").exists()
+    assert np.array_equal(got, oracle.pairs(R2, **kw))
+    assert np.array_equal(_read(res / "DRani_BPC_ra.dat").reshape(12, 12), oracle.pairs(D, R, **kw))
+    assert np.array_equal(_read(res / "DRani_BPC_rb.dat").reshape(12, 12), oracle.pairs(D, R2, **kw))
+    assert np.array_equal(_read(res / "RRani_BPC_ra.dat").reshape(12, 12), oracle.pairs(R, **kw))
+    _run(["2iso", "-n", str(n), "-f", "d.dat", "-rd", "rands/", "-b", "20", "-d", "30", "-s", str(box)],
+         layout / "cuda")
+    for lab, RR in (("ra", R), ("rb", R2)):
+        assert np.array_equal(_read(res / f"RRiso_{lab}.dat"), oracle.pairs(RR, box=box, bins=20, dmax=30.0))
+        assert np.array_equal(_read(res / f"DRiso_{lab}.dat"),
+                              oracle.pairs(D, RR, box=box, bins=20, dmax=30.0))
     # text layout of the 2-D writer: bins lines of bins values each
     lines = open(res / "DDani_BPC_d.dat").read().split("\n")
     assert len(lines[0].split()) == 12
@@ -108,6 +118,27 @@ def test_cli_3iso_and_file_format(layout):
     assert text.count("\n") == 8 * 8 + 8 * 2
     got = _read(res / "DDRiso_r.dat").reshape(8, 8, 8)
     assert np.array_equal(got, oracle.triplets_iso(D, R, box=box, bins=8, dmax=20.0))
+
+
+@pytest.mark.gpu
+def test_cli_3ani_writes_every_bin(layout):
+    """PCF.out 3ani writes the full bins^5 histogram (the reference's writer
+    stops at bins^3 values, cuda/pcf3ani.cuh:123): bins^4 lines of bins
+    values, in [b12][b31][b23][t12][t31] order, equal to the oracle."""
+    D, R, _ = _cats(layout, n=300)
+    box, bins = 100.0, 4
+    _run(["3ani", "-n", "300", "-f", "d.dat", "-r", "r.dat", "-b", str(bins), "-d", "25",
+          "-s", str(box)], layout / "cuda")
+    res = layout / "results"
+    text = open(res / "DDDani_d.dat").read()
+    rows = [ln for ln in text.split("\n") if ln.strip()]
+    assert len(rows) == bins ** 4 and all(len(r.split()) == bins for r in rows)
+    got = np.array(text.split(), dtype=np.float64).reshape((bins,) * 5)
+    want = oracle.triplets_ani(D, box=box, bins=bins, dmax=25.0)
+    assert want.sum() > 0
+    assert np.array_equal(got, want)
+    got = _read(res / "DDRani_r.dat").reshape((bins,) * 5)
+    assert np.array_equal(got, oracle.triplets_ani(D, R, box=box, bins=bins, dmax=25.0))
 
 
 @pytest.mark.gpu
