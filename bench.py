@@ -410,7 +410,7 @@ def run_ours(args, rank, world, local_rank):
         out["triplets"] = run_triplets(ctx, torch, stream)
         out["batched"] = run_batched(ctx, torch, stream)
         if rank == 0:
-            out["served"] = run_served()
+            out["served"] = run_served(args.served_requests)
     ctx.close()
     return out
 
@@ -489,19 +489,75 @@ def run_triplets(ctx, torch, stream, n=32768):
             out[name] = st
         return out
 
-    four()  # warm-up
-    ms, sts = _timed_ms(torch, stream, four)
+    sts = four()  # warm-up and the per-histogram counters
     tri = sum(s["pairs"] for s in sts.values())
+    dout = torch.zeros((4, 30 ** 3), dtype=torch.float64, device=torch.device("cuda", ctx.device))
+    akw = dict(bins=30, dmax=80.0, bpc=True)
+
+    def four_async():
+        # device outputs, no host wait between calls (the plain form at its best)
+        for k, (a, b) in enumerate(((gd, None), (gr, None), (gd, gr), (gr, gd))):
+            ctx.count_triplets(a, b, out_device_ptr=dout[k].data_ptr(), **akw)
+        ctx.synchronize()
+
+    four_async()
+    ms, _ = _timed_ms(torch, stream, four_async)
     res.update({"workload": f"3iso periodic, {n} Neyman-Scott + {n} uniform, box 250, 30^3 "
                             "bins, dmax 80, unit weights: DDD, RRR, DDR, DRR",
                 "ms": ms, "triangles": tri, "value": tri / (ms * 1e-3), "unit": "triplets/s",
                 "per_histogram_ms": {k: v["kernel_ms"] for k, v in sts.items()}})
+    # the same four histograms as the jobs of one persistent launch
+    batched = lambda: ctx.batch_triplets(gd, [gr], **kw)[1]  # noqa: E731
+    batched()
+    bms, bst = _timed_ms(torch, stream, batched)
+    res["batched"] = {"ms": bms, "triangles": bst["pairs"], "value": bst["pairs"] / (bms * 1e-3),
+                      "vs_per_call": ms / bms}
     ams, _ = _timed_ms(torch, stream, lambda: ctx.analytic_3iso(gd, bins=30, dmax=80.0,
                                                                  with_ddd=False))
     res["analytic_ddr_rrr_ms"] = ams
     gd.free()
     gr.free()
+    res["random_directory"] = run_triplets_rd(ctx, torch, stream)
     return res
+
+
+def run_triplets_rd(ctx, torch, stream, n_rand=8):
+    """The -rd form of 3iso: one clustered data catalog (32768, box 250)
+    against n_rand uniform random catalogs of log-uniform sizes 4k-32k,
+    periodic, 20^3 bins, dmax 40, unit weights: DDD, RRR_i, DDR_i, DRR_i per
+    call (the reference's per-file loop) vs one batched launch."""
+    import math
+    from desi_b200 import catalog
+    rng = np.random.default_rng(3100)
+    D = catalog.neyman_scott(32768, 250.0, seed=3101, weights="unit")
+    sizes = [int(round(math.exp(rng.uniform(math.log(4096), math.log(32768))))) for _ in range(n_rand)]
+    Rs = [catalog.uniform(s, 250.0, seed=3200 + i, weights="unit") for i, s in enumerate(sizes)]
+    gd = ctx.grid(D, 250.0)
+    grs = [ctx.grid(R, 250.0) for R in Rs]
+    kw = dict(bins=20, dmax=40.0, bpc=True)
+    calls = [(gd, None)] + [c for g in grs for c in ((g, None), (gd, g), (g, gd))]
+    out = torch.zeros((len(calls), 20 ** 3), dtype=torch.float64, device=torch.device("cuda", ctx.device))
+
+    def per_call():
+        # device outputs, no host wait between calls (the plain form at its best)
+        for k, (x, y) in enumerate(calls):
+            ctx.count_triplets(x, y, out_device_ptr=out[k].data_ptr(), **kw)
+        ctx.synchronize()
+
+    batched = lambda: ctx.batch_triplets(gd, grs, stats=True, **kw)[1]["pairs"]  # noqa: E731
+    per_call()
+    btri = batched()
+    pms, _ = _timed_ms(torch, stream, per_call, reps=2)
+    bms, btri = _timed_ms(torch, stream, batched, reps=2)
+    ptri = btri
+    for g in grs:
+        g.free()
+    gd.free()
+    return {"workload": f"1 x 32768 Neyman-Scott vs {n_rand} uniform randoms (4k-32k, log-uniform), "
+                        "box 250, periodic, 20^3 bins, dmax 40: DDD + RRR/DDR/DRR per random",
+            "random_sizes": sizes, "triangles": btri, "per_call_ms": pms, "batched_ms": bms,
+            "per_call_triplets_per_s": ptri / (pms * 1e-3),
+            "batched_triplets_per_s": btri / (bms * 1e-3), "batched_vs_per_call": pms / bms}
 
 
 def run_batched(ctx, torch, stream):
@@ -520,22 +576,24 @@ def run_batched(ctx, torch, stream):
     out = {"workload": "1 x 200k Neyman-Scott vs 32 uniform randoms (50k-400k, log-uniform), "
                        "box 1000, w~U(0.5,1.5), 40 bins, dmax 120, iso + ani",
            "random_sizes": sizes}
+    calls = [(gd, None)] + [c for g in grs for c in ((g, None), (gd, g))]
     for ani in (False, True):
         kw = dict(bins=40, dmax=120.0, ani=ani)
+        nb = 40 * 40 if ani else 40
+        out = torch.zeros((len(calls), nb), dtype=torch.float64, device=torch.device("cuda", ctx.device))
 
         def per_call():
-            n = 0.0
-            n += ctx.count_pairs(gd, None, stats=True, **kw)[1]["pairs"]
-            for g in grs:
-                n += ctx.count_pairs(g, None, stats=True, **kw)[1]["pairs"]
-                n += ctx.count_pairs(gd, g, stats=True, **kw)[1]["pairs"]
-            return n
+            # device outputs, no host wait between calls (the plain form at its best)
+            for k, (a, b) in enumerate(calls):
+                ctx.count_pairs(a, b, out_device_ptr=out[k].data_ptr(), **kw)
+            ctx.synchronize()
 
         def batched(graph):
             return lambda: ctx.batch_pairs(gd, grs, stats=True, graph=graph, **kw)[1]["pairs"]
 
         per_call()
-        ms_plain, units = _timed_ms(torch, stream, per_call)
+        ms_plain, _ = _timed_ms(torch, stream, per_call)
+        units = batched(False)()
         batched(False)()
         ms_batch, u2 = _timed_ms(torch, stream, batched(False), reps=2)
         batched(True)()  # capture
@@ -551,50 +609,64 @@ def run_batched(ctx, torch, stream):
     return out
 
 
-def run_served(n_requests=40, load=0.7):
-    """A seeded stream of mixed 2iso / 2ani / 3iso requests through the
-    continuous-batching server with 4 slots (desi_b200.serve).  One server
-    serves every pass of the same requests, its resident grids dropped
-    before each (every request grids its catalogs from host memory; the
-    slots' memory pools stay warm, as in a long-running server): a discarded
-    warm-up pass, three closed-loop passes (all submitted at once) whose
-    median measures capacity in requests/s, and three passes with Poisson
-    arrivals at `load` times that capacity.  Reported: the Poisson pass with
-    the median p99 (latency p50 / p99, pairs/s), and every pass's figures."""
+def run_served(n_requests=300, load=0.7):
+    """The served stream: a seeded mix of 2iso / 2ani / 3iso requests (N
+    log-uniform 1k-1M, 3iso 1k-65k; bins 20-50; dmax 40-120; box
+    250/500/1000, 3iso in the 1000 box; clustered or uniform; periodic or
+    not) through the continuous-batching server with 4 slots, every request
+    gridding its catalogs from page-locked host memory (resident grids
+    dropped before each pass).  Passes over the same requests: a warm-up on
+    the first 40 (discarded), one closed-loop pass (all submitted at once)
+    that measures capacity in requests/s, one pass with Poisson arrivals at
+    `load` times that capacity (latency p50 / p99 over all requests), and
+    the plain per-call form -- the same requests one at a time, each
+    submitted when the previous one completed.  Reported: pairs/s and
+    triplets/s of the served and plain forms (same requests, same kernels)."""
     from desi_b200 import serve
 
-    cats, _ = serve.make_stream(n_requests, rate_hz=1.0)
+    cats, _ = serve.make_stream_mixed(n_requests, rate_hz=1.0)
     srv = serve.PcfServer(slots=4)
     for k, (p, box) in cats.items():
         srv.register(k, p, box)
+    del cats
 
-    def one_pass(rate_hz):
-        _, reqs = serve.make_stream(n_requests, rate_hz=rate_hz or 1.0)
+    def _requests(rate_hz):
+        _, reqs = serve.make_stream_mixed(n_requests, rate_hz=rate_hz or 1.0, catalogs=False)
         if rate_hz is None:
             for r in reqs:
                 r.arrival = 0.0
-        srv.drop_grids()
-        rep = srv.run_stream(reqs)
-        rep.pop("results")
-        return rep
+        return reqs
 
     try:
-        one_pass(None)  # warm-up, discarded: pool allocations, first kernel launches
-        walls = sorted(one_pass(None)["wall_s"] for _ in range(3))
-        capacity = n_requests / walls[1]
-        reps = sorted((one_pass(load * capacity) for _ in range(3)),
-                      key=lambda r: r["latency_ms"]["p99"])
-        rep = dict(reps[1])
-        rep["passes"] = [{"p50_ms": r["latency_ms"]["p50"], "p99_ms": r["latency_ms"]["p99"],
-                          "wall_s": r["wall_s"]} for r in reps]
-        rep["closed_loop_wall_s"] = walls
+        warm = _requests(None)[:40]
+        srv.drop_grids()
+        srv.run_stream(warm)
+        srv.drop_grids()
+        closed = srv.run_stream(_requests(None))
+        closed.pop("results")
+        capacity = n_requests / closed["wall_s"]
+        srv.drop_grids()
+        rep = srv.run_stream(_requests(load * capacity))
+        rep.pop("results")
+        srv.drop_grids()
+        plain = srv.run_serial(_requests(None))
+        plain.pop("results")
     finally:
         srv.close()
+    rep["closed_loop"] = {k: closed[k] for k in ("wall_s", "pairs_per_s", "triplets_per_s",
+                                                 "overlapping_starts")}
+    rep["plain_per_call"] = {k: plain[k] for k in ("wall_s", "pairs_per_s", "triplets_per_s",
+                                                   "latency_ms")}
+    rep["served_vs_plain"] = {
+        "pairs_per_s": closed["pairs_per_s"] / plain["pairs_per_s"] if plain["pairs_per_s"] else None,
+        "triplets_per_s": (closed["triplets_per_s"] / plain["triplets_per_s"]
+                           if plain["triplets_per_s"] else None),
+        "note": "closed-loop served pass vs the same requests one at a time"}
     rep["capacity_req_per_s"] = capacity
     rep["rate_hz"] = load * capacity
-    rep["workload"] = (f"{n_requests} requests, Poisson at {load:.0%} of the closed-loop capacity, "
-                       "kinds 2iso/2ani/3iso, N log-uniform 1k-200k (3iso <= 8192), bins 20-50, "
-                       "dmax 40-120, box 250/500/1000, 4 slots")
+    rep["workload"] = (f"{n_requests} requests, Poisson at {load:.0%} of the closed-loop capacity; "
+                       "kinds 2iso/2ani/3iso; N log-uniform 1k-1M (3iso 1k-65k, box 1000); "
+                       "bins 20-50; dmax 40-120; box 250/500/1000; 4 slots")
     return rep
 
 
@@ -710,6 +782,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--served-requests", type=int, default=300,
+                    help="requests of the served stream (the workload's own count: 300)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of the timed step against the FP64 oracle")
     ap.add_argument("--no-extras", action="store_true",

@@ -85,6 +85,9 @@ _SIGS = {
     "pcf_batch_pairs": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_float, ctypes.c_uint32, _vp, _vp, _vp,
                                        ctypes.POINTER(Stats)]),
+    "pcf_batch_triplets": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                          ctypes.c_uint32, _vp, _vp, _vp, _vp,
+                                          ctypes.POINTER(Stats)]),
     "pcf_autotune_partitions": (ctypes.c_int, [_vp, _i64, ctypes.c_float, ctypes.c_float,
                                                ctypes.c_int, ctypes.c_uint32]),
     "pcf_microbench": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),

@@ -139,17 +139,25 @@ class Context:
 
     def count_triplets(self, x: "Grid", y: "Grid | None" = None, *, bins: int, dmax: float,
                        ani: bool = False, bpc: bool = False, flags: int = 0,
-                       stats: bool = False):
+                       stats: bool = False, out_device_ptr: int | None = None):
+        """One triplet histogram (XXX with y None, else XXY); out_device_ptr:
+        write it to device memory without waiting for it (isotropic only)."""
         nb = bins ** 5 if ani else bins ** 3
-        out = np.zeros(nb, np.float64)
         st = Stats()
         f = flags | (PCF_BPC if bpc else 0)
+        if out_device_ptr is not None:
+            f |= PCF_DEVICE_OUT
+            out, outp = None, ctypes.c_void_p(out_device_ptr)
+        else:
+            out = np.zeros(nb, np.float64)
+            outp = out.ctypes.data_as(ctypes.c_void_p)
         rc = self._lib.pcf_count_triplets(self.handle, PCF_ANI if ani else PCF_ISO, x.handle,
                                           y.handle if y is not None else None, int(bins),
-                                          float(dmax), f,
-                                          out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st))
+                                          float(dmax), f, outp,
+                                          ctypes.byref(st) if stats else None)
         _check(self.handle, rc, "pcf_count_triplets")
-        out = out.reshape((bins,) * (5 if ani else 3))
+        if out is not None:
+            out = out.reshape((bins,) * (5 if ani else 3))
         return (out, st.as_dict()) if stats else out
 
     def analytic_rr(self, bins: int, n: int, box: float, dmax: float, wrap: bool = True):
@@ -208,6 +216,28 @@ class Context:
         if dd is not None and ani:
             dd = dd.reshape(bins, bins)
         res = (dd, rr.reshape(shp), dr.reshape(shp))
+        return (res, st.as_dict()) if stats else res
+
+    def batch_triplets(self, d: "Grid", rands, *, bins: int, dmax: float, bpc: bool = False,
+                       flags: int = 0, stats: bool = False):
+        """DDD, and RRR_i, DDR_i, DRR_i per random grid, in one persistent
+        launch (pcf_batch_triplets): (ddd, rrr, ddr, drr), the last three
+        with a leading random-catalog axis."""
+        nr = len(rands)
+        n3 = bins ** 3
+        arr = (ctypes.c_void_p * max(nr, 1))(*[r.handle.value for r in rands])
+        ddd = np.zeros(n3, np.float64)
+        rrr, ddr, drr = (np.zeros(max(nr, 1) * n3, np.float64) for _ in range(3))
+        st = Stats()
+        f = flags | (PCF_BPC if bpc else 0)
+        p = lambda x: x.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        rc = self._lib.pcf_batch_triplets(self.handle, d.handle, ctypes.cast(arr, ctypes.c_void_p),
+                                          nr, int(bins), float(dmax), f, p(ddd), p(rrr), p(ddr),
+                                          p(drr), ctypes.byref(st))
+        _check(self.handle, rc, "pcf_batch_triplets")
+        shp = (nr, bins, bins, bins)
+        res = (ddd.reshape(bins, bins, bins), rrr[:nr * n3].reshape(shp), ddr[:nr * n3].reshape(shp),
+               drr[:nr * n3].reshape(shp))
         return (res, st.as_dict()) if stats else res
 
     def estimate(self, hists, n_d: int = 0, n_r: int = 0) -> np.ndarray:

@@ -12,8 +12,9 @@
 // (bins^5, save_histogram5D) rather than their first bins^3 values; -p sets
 // the cells per box side, which the library uses when a periodic stencil
 // fits them (2*ceil(dmax/cell) + 2 <= P) and otherwise replaces with its own
-// choice (results do not depend on it); -rd counts RR and DR of every random
-// catalog of the directory in one persistent launch (pcf_batch_pairs).
+// choice (results do not depend on it); -rd counts RR and DR (3iso: DDD,
+// RRR, DDR, DRR) of every random catalog of the directory in one persistent
+// launch (pcf_batch_pairs, pcf_batch_triplets).
 #include <dirent.h>
 
 #include <algorithm>
@@ -190,6 +191,20 @@ int main(int argc, char **argv) {
             pcfio::save3d("DDR" + sfx + tag + data_name, bn, ddr.data());
             pcfio::save3d("DRR" + sfx + tag + data_name, bn, ddr.data());  // pcf3isoBPC.cuh:340
             pcfio::save3d("RRR" + sfx + tag + data_name, bn, rrr.data());
+        } else if (!ani && gR.size() > 1) {
+            // -rd: DDD, and RRR / DDR / DRR of every random catalog, in one
+            // persistent launch (the reference launches per file,
+            // cuda/pcf3iso.cuh:101-112)
+            const size_t nr = gR.size();
+            std::vector<double> rrr(b3 * nr), ddr(b3 * nr), drr(b3 * nr);
+            CHECK(pcf_batch_triplets(ctx, gD, gR.data(), (int)nr, bn, dmax, f, h.data(), rrr.data(),
+                                     ddr.data(), drr.data(), nullptr));
+            save("DDD" + sfx + tag + data_name);
+            for (size_t i = 0; i < nr; ++i) {
+                pcfio::save3d("RRR" + sfx + tag + rand_labels[i], bn, rrr.data() + i * b3);
+                pcfio::save3d("DDR" + sfx + tag + rand_labels[i], bn, ddr.data() + i * b3);
+                pcfio::save3d("DRR" + sfx + tag + rand_labels[i], bn, drr.data() + i * b3);
+            }
         } else {
             CHECK(pcf_count_triplets(ctx, kind, gD, nullptr, bn, dmax, f, h.data(), nullptr));
             save("DDD" + sfx + tag + data_name);

@@ -25,6 +25,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <vector>
 #include <type_traits>
 
 #include "pcf_internal.cuh"
@@ -78,6 +80,10 @@ struct TripArgs {
     unsigned long long flush_budget;
     const unsigned *ctrl;  // abort request, polled with every anchor (null: none)
     unsigned *status;      // where a CTA that gives up records why (null: none)
+    // batched launches (k_triplets_batch): this job's anchors are the
+    // queue's [anchor_begin, anchor_begin + nX); mixed: XXY
+    long long anchor_begin;
+    int mixed;
 };
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -228,61 +234,52 @@ __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, 
     }
 }
 
+// Adds the shared histogram U (nb3 u32) into the u64 histogram g and clears
+// it (whole CTA).
+__device__ __forceinline__ void flush_hist(unsigned *U, int nb3, unsigned long long *g) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nb3; k += kTThreads) {
+        const unsigned v = U[k];
+        if (v) {
+            atomicAdd(g + k, (unsigned long long)v);
+            U[k] = 0u;
+        }
+    }
+    __syncthreads();
+}
+
+// Per-CTA state of the anchor loop.
+struct TripCta {
+    unsigned *U;                      // shared histogram (hist_in_smem)
+    unsigned char *lists;             // shared neighbour lists
+    int *s_nJ, *s_nK, *s_unit;        // shared counters
+    unsigned n_rechk;
+    unsigned long long n_tri;
+    unsigned long long since;         // pair tests since U's last flush
+};
+
+// All triangles of anchor i of job A: pass 1 builds the anchor's
+// neighbour lists in shared memory (or, past their capacity, in this CTA's
+// global scratch), pass 2 counts the neighbour pairs.
 template <bool MIXED, bool WEIGHTED>
-__global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void tri_anchor(const TripArgs &A, int i, TripCta &C) {
     const int bins = A.rXX.bins;
     const int nb3 = bins * bins * bins;
-    unsigned *U = reinterpret_cast<unsigned *>(smem);
-    // histogram + 32 dummy slots (see the unit-weight pass 2)
-    const size_t u_bytes = A.hist_in_smem ? (((size_t)(nb3 + 32) * 4 + 15) & ~(size_t)15) : 0;
-    float4 *sJ = reinterpret_cast<float4 *>(smem + u_bytes);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned *U = C.U;
+    int &s_nJ = *C.s_nJ, &s_nK = *C.s_nK, &s_unit = *C.s_unit;
+    unsigned &n_rechk = C.n_rechk;
+    unsigned long long &n_tri = C.n_tri;
+    unsigned long long &since = C.since;
+    float4 *sJ = reinterpret_cast<float4 *>(C.lists);
     float4 *sK = sJ + A.capJ;
     float *swJ = reinterpret_cast<float *>(sK + (MIXED ? A.capK : 0));
     float *swK = swJ + (WEIGHTED ? A.capJ : 0);
-    __shared__ int s_anchor, s_nJ, s_nK, s_unit;
-    __shared__ unsigned s_stop;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (A.hist_in_smem)
-        for (int k = tid; k < nb3 + 32; k += kTThreads) U[k] = 0u;
-    unsigned n_rechk = 0;
-    unsigned long long n_tri = 0;
-    // pair tests since the shared histogram's last flush: each adds at most
-    // once, so no u32 slot can pass this count
-    unsigned long long since = 0;
-    long long taken = 0;  // anchors this CTA took (iteration cap: nX + 1)
-    // adds U into the global u64 histogram and clears it (whole CTA)
-    auto flush_u = [&]() {
-        __syncthreads();
-        for (int k = tid; k < nb3; k += kTThreads) {
-            const unsigned v = U[k];
-            if (v) {
-                atomicAdd(A.g_count + k, (unsigned long long)v);
-                U[k] = 0u;
-            }
-        }
-        __syncthreads();
-    };
-    __syncthreads();
     float4 *gJ = A.gJ + (size_t)blockIdx.x * A.gcap;
     float4 *gK = A.gK ? A.gK + (size_t)blockIdx.x * A.gcap : nullptr;
     float *gwJ = A.gwJ ? A.gwJ + (size_t)blockIdx.x * A.gcap : nullptr;
     float *gwK = A.gwK ? A.gwK + (size_t)blockIdx.x * A.gcap : nullptr;
-
-    for (;;) {
-        if (tid == 0) {
-            s_anchor = (int)atomicAdd(A.counter, 1ull);
-            s_nJ = 0;
-            s_nK = 0;
-            s_unit = 0;
-            unsigned stop = (A.ctrl && ctrl_load(A.ctrl)) ? PCF_GAVE_UP_ABORT : 0u;
-            if (++taken > (long long)A.nX + 1) stop |= PCF_GAVE_UP_CAP;
-            if (stop && A.status) ctrl_store(A.status, stop);
-            s_stop = stop;
-        }
-        __syncthreads();
-        const int i = s_anchor;
-        if (i >= A.nX || s_stop) break;
+    auto flush_u = [&]() { flush_hist(U, nb3, A.g_count); };
         const float hx = A.X.x[i], hy = A.X.y[i], hz = A.X.z[i];
         const float hw = WEIGHTED ? A.X.w[i] : 1.f;
         const int P = A.P;
@@ -501,20 +498,128 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
             }
         }
         }
+}
+
+template <bool MIXED, bool WEIGHTED>
+__global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int bins = A.rXX.bins;
+    const int nb3 = bins * bins * bins;
+    // histogram + 32 dummy slots (see the unit-weight pass 2)
+    const size_t u_bytes = A.hist_in_smem ? (((size_t)(nb3 + 32) * 4 + 15) & ~(size_t)15) : 0;
+    __shared__ int s_anchor, s_nJ, s_nK, s_unit;
+    __shared__ unsigned s_stop;
+    const int tid = threadIdx.x, lane = tid & 31;
+    TripCta C{reinterpret_cast<unsigned *>(smem), smem + u_bytes, &s_nJ, &s_nK, &s_unit, 0u, 0ull, 0ull};
+    if (A.hist_in_smem)
+        for (int k = tid; k < nb3 + 32; k += kTThreads) C.U[k] = 0u;
+    long long taken = 0;  // anchors this CTA took (iteration cap: nX + 1)
+    __syncthreads();
+    for (;;) {
+        if (tid == 0) {
+            s_anchor = (int)atomicAdd(A.counter, 1ull);
+            s_nJ = 0;
+            s_nK = 0;
+            s_unit = 0;
+            unsigned stop = (A.ctrl && ctrl_load(A.ctrl)) ? PCF_GAVE_UP_ABORT : 0u;
+            if (++taken > (long long)A.nX + 1) stop |= PCF_GAVE_UP_CAP;
+            if (stop && A.status) ctrl_store(A.status, stop);
+            s_stop = stop;
+        }
+        __syncthreads();
+        const int i = s_anchor;
+        if (i >= A.nX || s_stop) break;
+        tri_anchor<MIXED, WEIGHTED>(A, i, C);
         __syncthreads();
     }
     if (A.hist_in_smem) {
         for (int k = tid; k < nb3; k += kTThreads)
-            if (U[k]) atomicAdd(A.g_count + k, (unsigned long long)U[k]);
+            if (C.U[k]) atomicAdd(A.g_count + k, (unsigned long long)C.U[k]);
     }
-    unsigned long long rr = n_rechk;
+    unsigned long long rr = C.n_rechk, nt = C.n_tri;
     for (int off = 16; off > 0; off >>= 1) {
         rr += __shfl_down_sync(kFull, rr, off);
-        n_tri += __shfl_down_sync(kFull, n_tri, off);
+        nt += __shfl_down_sync(kFull, nt, off);
     }
     if (lane == 0) {
         if (rr) atomicAdd(A.g_stats + 0, rr);
-        if (n_tri) atomicAdd(A.g_stats + 2, n_tri);
+        if (nt) atomicAdd(A.g_stats + 2, nt);
+    }
+}
+
+// Several isotropic triplet histograms in one persistent launch: the jobs'
+// anchors form one queue (job after job); a CTA that crosses into another
+// job flushes its shared histogram into the previous job's histogram and
+// loads the next job's arguments.  Jobs mix XXX and XXY.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(kTThreads, 1) k_triplets_batch(const TripArgs *__restrict__ jobs,
+                                                                  int n_jobs, long long n_anchors,
+                                                                  unsigned long long *counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ TripArgs s_job;
+    __shared__ long long s_anchor;
+    __shared__ int s_cur, s_nJ, s_nK, s_unit;
+    __shared__ unsigned s_stop;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int bins = jobs[0].rXX.bins;
+    const int nb3 = bins * bins * bins;
+    const bool in_smem = jobs[0].hist_in_smem != 0;
+    const size_t u_bytes = in_smem ? (((size_t)(nb3 + 32) * 4 + 15) & ~(size_t)15) : 0;
+    TripCta C{reinterpret_cast<unsigned *>(smem), smem + u_bytes, &s_nJ, &s_nK, &s_unit, 0u, 0ull, 0ull};
+    if (in_smem)
+        for (int k = tid; k < nb3 + 32; k += kTThreads) C.U[k] = 0u;
+    if (tid == 0) s_cur = -1;
+    long long taken = 0;
+    __syncthreads();
+    for (;;) {
+        if (tid == 0) {
+            s_anchor = (long long)atomicAdd(counter, 1ull);
+            s_nJ = 0;
+            s_nK = 0;
+            s_unit = 0;
+            const TripArgs &j0 = jobs[0];
+            unsigned stop = (j0.ctrl && ctrl_load(j0.ctrl)) ? PCF_GAVE_UP_ABORT : 0u;
+            if (++taken > n_anchors + 1) stop |= PCF_GAVE_UP_CAP;
+            if (stop && j0.status) ctrl_store(j0.status, stop);
+            s_stop = stop;
+        }
+        __syncthreads();
+        const long long g = s_anchor;
+        if (g >= n_anchors || s_stop) break;
+        // the job of anchor g (a CTA's anchors only move forward in the queue)
+        int cur = s_cur;
+        if (cur < 0 || g >= s_job.anchor_begin + s_job.nX) {
+            int j = cur < 0 ? 0 : cur;
+            while (j + 1 < n_jobs && g >= jobs[j + 1].anchor_begin) ++j;
+            if (cur >= 0 && in_smem && C.since) {
+                flush_hist(C.U, nb3, s_job.g_count);
+                C.since = 0;
+            }
+            __syncthreads();
+            static_assert(sizeof(TripArgs) % 4 == 0, "TripArgs words");
+            const int *src = reinterpret_cast<const int *>(jobs + j);
+            int *dst = reinterpret_cast<int *>(&s_job);
+            for (int q = tid; q < (int)(sizeof(TripArgs) / 4); q += kTThreads) dst[q] = src[q];
+            if (tid == 0) s_cur = j;
+            __syncthreads();
+        }
+        const int i = (int)(g - s_job.anchor_begin);
+        if (s_job.mixed) tri_anchor<true, WEIGHTED>(s_job, i, C);
+        else tri_anchor<false, WEIGHTED>(s_job, i, C);
+        __syncthreads();
+    }
+    if (in_smem && s_cur >= 0) {
+        for (int k = tid; k < nb3; k += kTThreads)
+            if (C.U[k]) atomicAdd(s_job.g_count + k, (unsigned long long)C.U[k]);
+    }
+    unsigned long long rr = C.n_rechk, nt = C.n_tri;
+    for (int off = 16; off > 0; off >>= 1) {
+        rr += __shfl_down_sync(kFull, rr, off);
+        nt += __shfl_down_sync(kFull, nt, off);
+    }
+    if (lane == 0) {
+        if (rr) atomicAdd(jobs[0].g_stats + 0, rr);
+        if (nt) atomicAdd(jobs[0].g_stats + 2, nt);
     }
 }
 
@@ -643,6 +748,108 @@ __global__ void k_trip_finalize(const unsigned long long *__restrict__ cnt,
 
 }  // namespace
 
+// Largest stencil population of any cell of g: bounds an anchor's lists.
+static int64_t max_stencil(const CellGrid &g, int P, const std::vector<RowDesc> &rows, bool bpc) {
+    const std::vector<int> &cs = g.h_start;
+    int64_t best = 0;
+    for (int ix = 0; ix < P; ++ix)
+        for (int iy = 0; iy < P; ++iy)
+            for (int iz = 0; iz < P; ++iz) {
+                int64_t n = 0;
+                for (const RowDesc &rw : rows) {
+                    int nx = ix + rw.dx, ny = iy + rw.dy;
+                    if (bpc) { nx = (nx + P) % P; ny = (ny + P) % P; }
+                    else if (nx < 0 || nx >= P || ny < 0 || ny >= P) continue;
+                    const int col = (nx * P + ny) * P;
+                    const int zlo = iz - rw.kz, zhi = iz + rw.kz;
+                    const int lo = std::max(zlo, 0), hi = std::min(zhi, P - 1);
+                    if (lo <= hi) n += cs[col + hi + 1] - cs[col + lo];
+                    if (bpc && zlo < 0) n += cs[col + P] - cs[col + zlo + P];
+                    if (bpc && zhi >= P) n += cs[col + zhi - P + 1] - cs[col];
+                }
+                best = std::max(best, n);
+            }
+    return best;
+}
+
+// Arguments of one isotropic triplet histogram over the cell structures of
+// x (and y for XXY) at P partitions: catalogs, side rules, FP32 windows and
+// the shared-memory layout (smem: dynamic bytes).  The buffers (rows,
+// counter, histograms, overflow lists) are the caller's.
+static void trip_setup(pcf_ctx *ctx, const pcf_grid *X, const pcf_grid *Y, int P, int n_rows, int bins,
+                       float dmax, uint32_t flags, bool weighted, TripArgs &A, size_t &smem) {
+    const bool bpc = (flags & PCF_BPC) != 0, mixed = Y != nullptr;
+    const CellGrid &gx = *X->cells;
+    const CellGrid &gy = mixed ? *Y->cells : gx;
+    // side rules: X-X sides need d > 0; X-Y sides only with periodic boxes
+    // (3iso_k.cuh:158,160 vs 3isoBPC_k.cuh:165,170)
+    PairRule rXX = make_pair_rule(bins, dmax, flags & ~PCF_DS_EXACT, false, bpc, false);
+    PairRule rXY = rXX;
+    rXY.flags = bpc ? PCF_RULE_EXCL : 0u;
+    if (flags & PCF_RULE_CUSTOM) rXY.flags = rXX.flags;
+    memset(&A, 0, sizeof(A));
+    A.X = {gx.x(), gx.y(), gx.z(), gx.w(), gx.cell_start.as<int>()};
+    A.Y = {gy.x(), gy.y(), gy.z(), gy.w(), gy.cell_start.as<int>()};
+    A.nX = (int)X->n;
+    A.n_rows = n_rows;
+    A.P = P;
+    A.cell = gx.cell;
+    A.box = X->box;
+    A.bpc = bpc ? 1 : 0;
+    A.rXX = rXX;
+    A.rXY = rXY;
+    A.flush_budget = ctx->trip_flush_budget;
+    A.ctrl = ctx->d_ctrl;
+    A.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
+    A.mixed = mixed ? 1 : 0;
+    {
+        // windows: the FP32 side |v_k - v_j| carries up to three roundings of
+        // coordinate differences (plus the image shift of the anchor when
+        // periodic); the bounds below keep a >= 8x margin
+        const double dd = rXX.dd;
+        const double rmax = (double)dmax * rXX.ds + 1.0;
+        const double Lx = bpc ? (double)X->box : (double)dmax;
+        const double e_d2 = dd * std::ldexp(1.0, -17) + (double)dmax * Lx * std::ldexp(1.0, -18);
+        const double wr = rmax * std::ldexp(1.0, -17) + rXX.ds * Lx * std::ldexp(1.0, -18);
+        A.fc.dsf = (float)rXX.ds;
+        A.fc.ds2 = A.fc.dsf * A.fc.dsf;
+        A.fc.lo = (float)(dd - e_d2);
+        A.fc.hi = (float)(dd + e_d2);
+        A.fc.w = std::min(8000u, (unsigned)std::ceil((wr + std::ldexp(1.0, -16)) * 32768.0) + 1u);
+    }
+    const int n3 = bins * bins * bins;
+    // histogram + 32 dummy slots (the adds of 0 of lanes without a triangle)
+    const size_t u_bytes = ((size_t)(n3 + 32) * 4 + 15) & ~(size_t)15;
+    const size_t smem_max = 227 * 1024 - 64 - sizeof(TripArgs);
+    A.hist_in_smem = (!weighted && u_bytes <= 150 * 1024) ? 1 : 0;
+    const size_t hist_b = A.hist_in_smem ? u_bytes : 0;
+    const size_t ent = 16 + (weighted ? 4 : 0);
+    const size_t room = smem_max - hist_b;
+    if (mixed && !(A.hist_in_smem && !weighted)) {
+        A.capJ = (int)(room / ent / 3);
+        A.capK = (int)(room / ent) - A.capJ;
+    } else {  // XXX, or XXY with one pooled buffer (J up, K down; see tri_anchor)
+        A.capJ = (int)(room / ent);
+        A.capK = 0;
+    }
+    smem = hist_b + (size_t)(A.capJ + A.capK) * ent;
+}
+
+// Per-CTA overflow lists for lists of up to gcap entries (J, K and weights).
+static pcf_status trip_overflow(pcf_ctx *ctx, int64_t gmax, bool mixed, bool weighted, int grid,
+                                TripArgs &A) {
+    A.gcap = (int)std::min<int64_t>(gmax, 1 << 24);
+    PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(float4) * (size_t)A.gcap * grid * (mixed ? 2 : 1) +
+                                      (weighted ? sizeof(float) * (size_t)A.gcap * grid * 2 : 0) + 256));
+    char *sc = ctx->scratch_c.as<char>();
+    A.gJ = reinterpret_cast<float4 *>(sc);
+    A.gK = mixed ? A.gJ + (size_t)A.gcap * grid : nullptr;
+    float *wbase = reinterpret_cast<float *>(sc + sizeof(float4) * (size_t)A.gcap * grid * (mixed ? 2 : 1));
+    A.gwJ = weighted ? wbase : nullptr;
+    A.gwK = weighted && mixed ? wbase + (size_t)A.gcap * grid : nullptr;
+    return PCF_OK;
+}
+
 extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid *x_,
                                          const pcf_grid *y_, int bins, float dmax, uint32_t flags,
                                          double *hist, pcf_stats *stats) {
@@ -663,94 +870,17 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
     const CellGrid &gy = mixed ? *Y->cells : gx;
     PairPlan plan;
     plan_pairs(gx, X->box, dmax, false, false, plan, ctx->sm_count * 24);
-
-    // side rules: X-X sides need d > 0; X-Y sides only with periodic boxes
-    // (3iso_k.cuh:158,160 vs 3isoBPC_k.cuh:165,170)
-    PairRule rXX = make_pair_rule(bins, dmax, flags & ~PCF_DS_EXACT, false, bpc, false);
-    PairRule rXY = rXX;
-    rXY.flags = bpc ? PCF_RULE_EXCL : 0u;
-    if (flags & PCF_RULE_CUSTOM) rXY.flags = rXX.flags;
-    TripArgs A;
-    A.X = {gx.x(), gx.y(), gx.z(), gx.w(), gx.cell_start.as<int>()};
-    A.Y = {gy.x(), gy.y(), gy.z(), gy.w(), gy.cell_start.as<int>()};
-    A.nX = (int)X->n;
-    A.n_rows = (int)plan.rows.size();
-    A.P = P;
-    A.cell = gx.cell;
-    A.box = X->box;
-    A.bpc = bpc ? 1 : 0;
-    A.rXX = rXX;
-    A.rXY = rXY;
-    A.flush_budget = ctx->trip_flush_budget;
-    A.ctrl = ctx->d_ctrl;
-    A.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
-    {
-        // windows: the FP32 side |v_k - v_j| carries up to three roundings of
-        // coordinate differences (plus the image shift of the anchor when
-        // periodic); the bounds below keep a >= 8x margin
-        const double dd = rXX.dd;
-        const double rmax = (double)dmax * rXX.ds + 1.0;
-        const double Lx = bpc ? (double)X->box : (double)dmax;
-        const double e_d2 = dd * std::ldexp(1.0, -17) + (double)dmax * Lx * std::ldexp(1.0, -18);
-        const double wr = rmax * std::ldexp(1.0, -17) + rXX.ds * Lx * std::ldexp(1.0, -18);
-        A.fc.dsf = (float)rXX.ds;
-        A.fc.ds2 = A.fc.dsf * A.fc.dsf;
-        A.fc.lo = (float)(dd - e_d2);
-        A.fc.hi = (float)(dd + e_d2);
-        A.fc.w = std::min(8000u, (unsigned)std::ceil((wr + std::ldexp(1.0, -16)) * 32768.0) + 1u);
-    }
     const bool weighted = !(X->unit_weights && (!mixed || Y->unit_weights));
+    TripArgs A;
+    size_t smem = 0;
+    trip_setup(ctx, X, Y, P, (int)plan.rows.size(), bins, dmax, flags, weighted, A, smem);
     const int n3 = bins * bins * bins;
-    // histogram + 32 dummy slots (the adds of 0 of lanes without a triangle)
-    const size_t u_bytes = ((size_t)(n3 + 32) * 4 + 15) & ~(size_t)15;
-    const size_t smem_max = 227 * 1024 - 64;
-    A.hist_in_smem = (!weighted && u_bytes <= 150 * 1024) ? 1 : 0;
-    const size_t hist_b = A.hist_in_smem ? u_bytes : 0;
-    const size_t ent = 16 + (weighted ? 4 : 0);
-    const size_t room = smem_max - hist_b;
-    if (mixed && !(A.hist_in_smem && !weighted)) {
-        A.capJ = (int)(room / ent / 3);
-        A.capK = (int)(room / ent) - A.capJ;
-    } else {  // XXX, or XXY with one pooled buffer (J up, K down; see k_triplets)
-        A.capJ = (int)(room / ent);
-        A.capK = 0;
-    }
-    const size_t smem = hist_b + (size_t)(A.capJ + A.capK) * ent;
     // overflow lists: bounded by the largest stencil population of any cell
-    auto max_stencil = [&](const CellGrid &g) -> int64_t {
-        const std::vector<int> &cs = g.h_start;
-        int64_t best = 0;
-        for (int ix = 0; ix < P; ++ix)
-            for (int iy = 0; iy < P; ++iy)
-                for (int iz = 0; iz < P; ++iz) {
-                    int64_t n = 0;
-                    for (const RowDesc &rw : plan.rows) {
-                        int nx = ix + rw.dx, ny = iy + rw.dy;
-                        if (bpc) { nx = (nx + P) % P; ny = (ny + P) % P; }
-                        else if (nx < 0 || nx >= P || ny < 0 || ny >= P) continue;
-                        const int col = (nx * P + ny) * P;
-                        const int zlo = iz - rw.kz, zhi = iz + rw.kz;
-                        const int lo = std::max(zlo, 0), hi = std::min(zhi, P - 1);
-                        if (lo <= hi) n += cs[col + hi + 1] - cs[col + lo];
-                        if (bpc && zlo < 0) n += cs[col + P] - cs[col + zlo + P];
-                        if (bpc && zhi >= P) n += cs[col + zhi - P + 1] - cs[col];
-                    }
-                    best = std::max(best, n);
-                }
-        return best;
-    };
-    const int64_t gmax = std::max<int64_t>(max_stencil(gx), mixed ? max_stencil(gy) : 0) + 32;
+    const int64_t gmax = std::max<int64_t>(max_stencil(gx, P, plan.rows, bpc),
+                                           mixed ? max_stencil(gy, P, plan.rows, bpc) : 0) + 32;
     const int grid = ctx->sm_count;
-    A.gcap = (int)std::min<int64_t>(gmax, 1 << 24);
-    PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(float4) * (size_t)A.gcap * grid * (mixed ? 2 : 1) +
-                                      (weighted ? sizeof(float) * (size_t)A.gcap * grid * 2 : 0) + 256));
-    char *sc = ctx->scratch_c.as<char>();
-    A.gJ = reinterpret_cast<float4 *>(sc);
-    A.gK = mixed ? A.gJ + (size_t)A.gcap * grid : nullptr;
-    float *wbase = reinterpret_cast<float *>(sc + sizeof(float4) * (size_t)A.gcap * grid * (mixed ? 2 : 1));
-    A.gwJ = weighted ? wbase : nullptr;
-    A.gwK = weighted && mixed ? wbase + (size_t)A.gcap * grid : nullptr;
-
+    s = trip_overflow(ctx, gmax, mixed, weighted, grid, A);
+    if (s != PCF_OK) return s;
     // rows + counter through the plan slot
     PlanSlot *sl = nullptr;
     s = stage_plan(ctx, plan, &sl);
@@ -811,6 +941,155 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
             stats->partitions = P;
             stats->work_items = (int)X->n;
         }
+    }
+    return PCF_OK;
+}
+
+// One data catalog against n_rand random catalogs: DDD once, RRR_i, DDR_i
+// and DRR_i per random catalog, as the jobs of one persistent launch
+// (k_triplets_batch).  All grids take one partition count (the one a call
+// on the largest catalog would use; results do not depend on it).
+extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const pcf_grid *const *r_,
+                                         int n_rand, int bins, float dmax, uint32_t flags, double *ddd,
+                                         double *rrr, double *ddr, double *drr, pcf_stats *stats) {
+    if (!ctx || !d_ || bins < 1 || !(dmax > 0.f) || n_rand < 0 || (n_rand > 0 && !r_) ||
+        (!ddd && !rrr && !ddr && !drr))
+        return PCF_ERR_INVALID_ARG;
+    if (bins > 255 || (int64_t)bins * bins * bins > (1 << 26)) return PCF_ERR_UNSUPPORTED;
+    if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
+    cudaSetDevice(ctx->device);
+    const bool bpc = (flags & PCF_BPC) != 0;
+    pcf_grid *D = const_cast<pcf_grid *>(d_);
+    std::vector<pcf_grid *> R((size_t)n_rand);
+    pcf_grid *big = D;
+    bool weighted = !D->unit_weights;
+    for (int i = 0; i < n_rand; ++i) {
+        R[i] = const_cast<pcf_grid *>(r_[i]);
+        if (!R[i]) return PCF_ERR_INVALID_ARG;
+        if (R[i]->box != D->box) return PCF_ERR_MISMATCH;
+        if (R[i]->n >= (1 << 24)) return PCF_ERR_UNSUPPORTED;
+        if (R[i]->n > big->n) big = R[i];
+        weighted = weighted || !R[i]->unit_weights;
+    }
+    if (D->n >= (1 << 24)) return PCF_ERR_UNSUPPORTED;
+    int P = 0;
+    pcf_status s = prepare_grids(ctx, big, nullptr, dmax, PCF_ISO, bpc, &P);
+    if (s != PCF_OK) return s;
+    if ((s = grid_ensure_cells(ctx, D, P)) != PCF_OK) return s;
+    for (pcf_grid *g : R)
+        if ((s = grid_ensure_cells(ctx, g, P)) != PCF_OK) return s;
+    PairPlan plan;
+    plan_pairs(*D->cells, D->box, dmax, false, false, plan, ctx->sm_count * 24);
+    const int n3 = bins * bins * bins;
+
+    // jobs: (X, Y) in output order
+    struct Job { pcf_grid *x, *y; double *out; };
+    std::vector<Job> jobs;
+    if (ddd) jobs.push_back({D, nullptr, ddd});
+    for (int i = 0; i < n_rand; ++i) {
+        if (rrr) jobs.push_back({R[i], nullptr, rrr + (size_t)i * n3});
+        if (ddr) jobs.push_back({D, R[i], ddr + (size_t)i * n3});
+        if (drr) jobs.push_back({R[i], D, drr + (size_t)i * n3});
+    }
+    const int nj = (int)jobs.size();
+    std::vector<TripArgs> args((size_t)nj);
+    size_t smem = 0;
+    long long anchors = 0;
+    bool any_mixed = false;
+    int64_t gmax = 0;
+    std::map<const pcf_grid *, int64_t> stencil;  // per grid
+    auto stencil_of = [&](const pcf_grid *g) {
+        auto it = stencil.find(g);
+        if (it != stencil.end()) return it->second;
+        return stencil[g] = max_stencil(*g->cells, P, plan.rows, bpc);
+    };
+    for (int k = 0; k < nj; ++k) {
+        size_t sm = 0;
+        trip_setup(ctx, jobs[k].x, jobs[k].y, P, (int)plan.rows.size(), bins, dmax, flags, weighted,
+                   args[k], sm);
+        smem = std::max(smem, sm);
+        args[k].anchor_begin = anchors;
+        anchors += jobs[k].x->n;
+        any_mixed = any_mixed || jobs[k].y;
+        gmax = std::max<int64_t>(gmax, stencil_of(jobs[k].x));
+        if (jobs[k].y) gmax = std::max<int64_t>(gmax, stencil_of(jobs[k].y));
+    }
+    const int grid = ctx->sm_count;
+    TripArgs ov;
+    s = trip_overflow(ctx, gmax + 32, any_mixed, weighted, grid, ov);
+    if (s != PCF_OK) return s;
+
+    // rows + counter through the plan slot; histograms per job
+    PlanSlot *sl = nullptr;
+    s = stage_plan(ctx, plan, &sl);
+    if (s != PCF_OK) return s;
+    const size_t nh = (size_t)nj * n3;
+    PCF_CU(ctx, ctx->d_hist.ensure(nh * 24 + 64));
+    char *hp = ctx->d_hist.as<char>();
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(hp);
+    double *wsum = reinterpret_cast<double *>(hp + nh * 8);
+    unsigned long long *gstats = reinterpret_cast<unsigned long long *>(hp + nh * 16);
+    double *d_out = reinterpret_cast<double *>(hp + nh * 16 + 64);
+    PCF_CU(ctx, cudaMemsetAsync(hp, 0, nh * 16 + 64, ctx->stream));
+    for (int k = 0; k < nj; ++k) {
+        TripArgs &A = args[k];
+        A.gcap = ov.gcap;
+        A.gJ = ov.gJ;
+        A.gK = ov.gK;
+        A.gwJ = ov.gwJ;
+        A.gwK = ov.gwK;
+        A.rows = sl->d_rows.as<RowDesc>();
+        A.counter = sl->d_counter.as<unsigned long long>();
+        A.g_count = cnt + (size_t)k * n3;
+        A.g_wsum = wsum + (size_t)k * n3;
+        A.g_stats = gstats;
+    }
+    DevBuf d_jobs;
+    d_jobs.pool = ctx->pool;
+    PCF_CU(ctx, d_jobs.ensure(sizeof(TripArgs) * nj));
+    PCF_CU(ctx, cudaMemcpyAsync(d_jobs.p, args.data(), sizeof(TripArgs) * nj, cudaMemcpyHostToDevice,
+                                ctx->stream));
+    auto kfn = weighted ? k_triplets_batch<true> : k_triplets_batch<false>;
+    PCF_CU(ctx, ensure_smem_limit(reinterpret_cast<const void *>(kfn), ctx->device, smem));
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    if (ctx->profile) {
+        s = profile_events(ctx, &pe0, &pe1);
+        if (s != PCF_OK) return s;
+        PCF_CU(ctx, cudaEventRecord(pe0, ctx->stream));
+    }
+    PCF_CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    kfn<<<grid, kTThreads, smem, ctx->stream>>>(d_jobs.as<TripArgs>(), nj, anchors,
+                                                sl->d_counter.as<unsigned long long>());
+    PCF_CU(ctx, cudaGetLastError());
+    PCF_CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    if (pe1) PCF_CU(ctx, cudaEventRecord(pe1, ctx->stream));
+    PCF_CU(ctx, cudaEventRecord(sl->done, ctx->stream));
+    ++ctx->launches;
+    for (int k = 0; k < nj; ++k) {
+        k_trip_finalize<<<(n3 + 255) / 256, 256, 0, ctx->stream>>>(
+            cnt + (size_t)k * n3, wsum + (size_t)k * n3, weighted ? 1 : 0, jobs[k].y ? 1 : 0, bins,
+            d_out + (size_t)k * n3);
+        PCF_CU(ctx, cudaGetLastError());
+        ++ctx->launches;
+    }
+    std::vector<double> host(nh);
+    unsigned long long hs[4] = {0, 0, 0, 0};
+    PCF_CU(ctx, cudaMemcpyAsync(host.data(), d_out, sizeof(double) * nh, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+    PCF_CU(ctx, cudaMemcpyAsync(hs, gstats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+    PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    s = ctx_queue_status(ctx);
+    if (s != PCF_OK) return s;
+    for (int k = 0; k < nj; ++k) memcpy(jobs[k].out, host.data() + (size_t)k * n3, sizeof(double) * n3);
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->pairs = (double)hs[2];
+        stats->candidates = 0;
+        stats->rechecks = (double)hs[0];
+        stats->kernel_ms = ms;
+        stats->partitions = P;
+        stats->work_items = (int)std::min<long long>(anchors, INT32_MAX);
     }
     return PCF_OK;
 }

@@ -152,9 +152,12 @@ class _Slot:
         gd, gr = self.grid(req.data, keep), self.grid(req.rand, keep)
         c = self.ctx
         if req.kind == "3iso":
-            kw = dict(bins=req.bins, dmax=req.dmax, bpc=req.bpc)
-            out = {"DDD": c.count_triplets(gd, **kw), "RRR": c.count_triplets(gr, **kw),
-                   "DDR": c.count_triplets(gd, gr, **kw), "DRR": c.count_triplets(gr, gd, **kw)}
+            kw = dict(bins=req.bins, dmax=req.dmax, bpc=req.bpc, stats=True)
+            out, tri = {}, 0.0
+            for name, x, y in (("DDD", gd, None), ("RRR", gr, None), ("DDR", gd, gr), ("DRR", gr, gd)):
+                out[name], st = c.count_triplets(x, y, **kw)
+                tri += st["pairs"]  # in-range unordered triangles (XXY: per XX pair)
+            out["_triangles"] = tri
             units = 0.0
         else:
             kw = dict(bins=req.bins, dmax=req.dmax, bpc=req.bpc, ani=req.kind == "2ani", stats=True)
@@ -395,25 +398,83 @@ class PcfServer:
             self.submit(r)
         results = [r.future.result() for r in reqs]
         t1 = time.perf_counter()
+        return self._report(reqs, results, t1 - t0)
+
+    def run_serial(self, reqs: list[Request]) -> dict:
+        """The plain per-call form of the same requests: one at a time, in
+        arrival order, each submitted when the previous one has completed
+        (no overlap on the device)."""
+        t0 = time.perf_counter()
+        results = []
+        for r in sorted(reqs, key=lambda r: r.arrival):
+            results.append(self.submit(r).result())
+        t1 = time.perf_counter()
+        order = sorted(reqs, key=lambda r: r.arrival)
+        return self._report(order, results, t1 - t0)
+
+    @staticmethod
+    def _report(reqs, results, wall) -> dict:
         lat = np.array([(r.t_end - r.t_submit) * 1e3 for r in reqs])
-        units = sum(res["_units"] for res in results)
+        units = sum(res.get("_units", 0.0) for res in results)
+        tri = sum(res.get("_triangles", 0.0) for res in results)
+        busy = {}
+        for r in reqs:
+            busy[r.kind] = busy.get(r.kind, 0.0) + (r.t_end - r.t_start)
         # how much the requests' device spans overlapped (continuous batching)
         spans = sorted((r.t_start, r.t_end) for r in reqs)
         overlap = sum(1 for (s0, e0), (s1, _) in zip(spans, spans[1:]) if s1 < e0)
-        return {"requests": len(reqs), "wall_s": t1 - t0,
+        return {"requests": len(reqs), "wall_s": wall,
                 "latency_ms": {"p50": float(np.percentile(lat, 50)),
                                "p99": float(np.percentile(lat, 99)),
                                "max": float(lat.max())},
-                "pairs_per_s": units / (t1 - t0), "overlapping_starts": overlap,
+                "pairs": units, "triangles": tri,
+                "pairs_per_s": units / wall, "triplets_per_s": tri / wall,
+                "overlapping_starts": overlap, "slot_seconds_by_kind": busy,
                 "results": results}
+
+
+def make_stream_mixed(n_requests: int, rate_hz: float, seed: int = 6000, n_max: int = 1_000_000,
+                      n3_max: int = 65_536, box3: float = 1000.0,
+                      catalogs: bool = True) -> tuple[dict, list[Request]]:
+    """The served-stream workload: Poisson arrivals of mixed requests, kinds
+    2iso / 2ani / 3iso uniform, N log-uniform in [1e3, n_max] (3iso:
+    [1e3, n3_max]), bins uniform in 20..50, dmax uniform in [40, 120], box
+    250 / 500 / 1000 (dmax < L/2 holds for all), data clustered or uniform
+    by a seeded draw, unit weights, periodic or not by a seeded draw.  3iso
+    requests take the box of side box3 (1000): their cost grows as
+    N * (N dmax^3 / L^3)^2, and in the smaller boxes one 65k-point request
+    alone would take minutes.  catalogs=False returns the same requests
+    (other rate) without generating the catalogs again."""
+    from . import catalog
+    rng = np.random.default_rng(seed)
+    cats, reqs = {}, []
+    t = 0.0
+    for i in range(n_requests):
+        kind = KINDS[rng.integers(0, 3)]
+        cap = n3_max if kind == "3iso" else n_max
+        n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(cap)))))
+        box = box3 if kind == "3iso" else float(rng.choice([250.0, 500.0, 1000.0]))
+        bins = int(rng.integers(20, 51))
+        dmax = float(rng.uniform(40.0, 120.0))
+        clustered = bool(rng.integers(0, 2))
+        bpc = bool(rng.integers(0, 2))
+        dname, rname = f"d{i}", f"r{i}"
+        if catalogs:
+            gen = catalog.neyman_scott if clustered else catalog.uniform
+            cats[dname] = (gen(n, box, seed=seed + 2 * i), box)
+            cats[rname] = (catalog.uniform(n, box, seed=seed + 2 * i + 1), box)
+        t += rng.exponential(1.0 / rate_hz)
+        reqs.append(Request(kind, dname, rname, bins, dmax, bpc=bpc, arrival=t, rid=i))
+    return cats, reqs
 
 
 def make_stream(n_requests: int, rate_hz: float, seed: int = 5000, n_max: int = 200_000,
                 n3_max: int = 8_192) -> tuple[dict, list[Request]]:
-    """Seeded stream of mixed requests (served-stream shape: kinds 2iso/2ani/3iso
-    uniform, N log-uniform, bins 20-50, dmax 40-120 with dmax < L/2, box
-    250/500/1000, clustered or uniform, unit weights, Poisson arrivals).  N is
-    capped by n_max (n3_max for 3iso) so the stream fits a short run."""
+    """A lighter seeded stream of mixed requests (kinds 2iso/2ani/3iso
+    uniform, N log-uniform, bins 20-50 (3iso 10-20), dmax 40-120 with
+    dmax < L/2 (3iso <= min(L/4, 60)), box 250/500/1000, clustered or
+    uniform, unit weights, Poisson arrivals), N capped by n_max (n3_max for
+    3iso): the request server's quick demonstration."""
     from . import catalog
     rng = np.random.default_rng(seed)
     cats, reqs = {}, []

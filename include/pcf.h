@@ -191,6 +191,18 @@ pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d, const pcf_
                            int n_rand, int bins, float dmax, uint32_t flags, double *dd,
                            double *rr, double *dr, pcf_stats *stats);
 
+/*
+ * The 3-point analogue of pcf_batch_pairs: one data catalog against n_rand
+ * random catalogs, every isotropic triplet histogram in one persistent
+ * launch over an (anchor, histogram) work queue.  Writes ddd (bins^3) once
+ * and, per random catalog i, rrr / ddr / drr at [i*bins^3 ..]; any of them
+ * may be NULL to skip it.  Replaces the per-file loop of pcf_3iso /
+ * pcf_3isoBPC over the -rd random directory (cuda/pcf3iso.cuh:101-112).
+ */
+pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d, const pcf_grid *const *r,
+                              int n_rand, int bins, float dmax, uint32_t flags, double *ddd,
+                              double *rrr, double *ddr, double *drr, pcf_stats *stats);
+
 /* Cells per side the library would pick for (n, box, dmax, kind). */
 int pcf_autotune_partitions(pcf_ctx *ctx, int64_t n, float box, float dmax, int kind,
                             uint32_t flags);

@@ -121,6 +121,24 @@ def test_cli_3iso_and_file_format(layout):
 
 
 @pytest.mark.gpu
+def test_cli_3iso_rd_batched(layout):
+    """PCF.out 3iso -rd: DDD and every random file's RRR / DDR / DRR from one
+    batched launch, each equal to the oracle."""
+    D, R, R2 = _cats(layout, n=700)
+    box = 100.0
+    _run(["3iso", "-n", "700", "-f", "d.dat", "-rd", "rands/", "-b", "8", "-d", "20", "-bpc",
+          "-s", str(box)], layout / "cuda")
+    res = layout / "results"
+    kw = dict(box=box, bins=8, dmax=20.0, bpc=True)
+    rd = lambda name: _read(res / name).reshape(8, 8, 8)  # noqa: E731
+    assert np.array_equal(rd("DDDiso_BPC_d.dat"), oracle.triplets_iso(D, **kw))
+    for lab, RR in (("ra", R), ("rb", R2)):
+        assert np.array_equal(rd(f"RRRiso_BPC_{lab}.dat"), oracle.triplets_iso(RR, **kw))
+        assert np.array_equal(rd(f"DDRiso_BPC_{lab}.dat"), oracle.triplets_iso(D, RR, **kw))
+        assert np.array_equal(rd(f"DRRiso_BPC_{lab}.dat"), oracle.triplets_iso(RR, D, **kw))
+
+
+@pytest.mark.gpu
 def test_cli_3ani_writes_every_bin(layout):
     """PCF.out 3ani writes the full bins^5 histogram (the reference's writer
     stops at bins^3 values, cuda/pcf3ani.cuh:123): bins^4 lines of bins
