@@ -245,6 +245,8 @@ def run_ours(args, rank, world, local_rank):
     D, R = catalogs()
     ctx = api.Context(local_rank)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    if args.pair_variant:
+        ctx.set_option(api.PCF_OPT_PAIR_VARIANT, args.pair_variant)
     P, fused, tuned = tune_step(ctx, D, R)
     kinds = ("both",) if fused else (False, True)
     # a both-kinds call tuned to the library's default rule (-1) runs as two
@@ -381,6 +383,7 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded Neyman-Scott data + uniform randoms; no dataset ships with "
                 "the workload)",
         "config": dict(W, partitions=P, kinds_in_one_pass=one_pass, schemes=tuned,
+                       pair_kernel_variant=args.pair_variant,
                        parallelism=f"replicas x{world}",
                        l2="flushed between steps (512 MB write)",
                        pairs_per_step=pairs_step),
@@ -782,6 +785,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--pair-variant", type=int, default=0, choices=[0, 1, 2],
+                    help="one-pass pair kernel variant (A/B of shared-memory staging; "
+                         "include/pcf_bench.h PCF_OPT_PAIR_VARIANT)")
     ap.add_argument("--served-requests", type=int, default=300,
                     help="requests of the served stream (the workload's own count: 300)")
     ap.add_argument("--no-parity", action="store_true",

@@ -20,7 +20,7 @@ PCF_RULE_INCLUSIVE = 1 << 4
 PCF_DEVICE_OUT = 1 << 5
 PCF_GRAPH = 1 << 7
 PCF_ERR_TIMEOUT = -6
-PCF_OPT_TRIP_FLUSH_BUDGET, PCF_OPT_ABORT_HOST_CHECK = 1, 2
+PCF_OPT_TRIP_FLUSH_BUDGET, PCF_OPT_ABORT_HOST_CHECK, PCF_OPT_PAIR_VARIANT = 1, 2, 3
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory",
           -4: "unsupported configuration", -5: "coordinate outside [0, box)",
@@ -38,7 +38,7 @@ class PcfError(RuntimeError):
 
 class TuneResult(ctypes.Structure):
     _fields_ = [("refine", ctypes.c_int), ("hist_mode", ctypes.c_int), ("best_ms", ctypes.c_float),
-                ("default_ms", ctypes.c_float), ("tried", ctypes.c_int)]
+                ("default_ms", ctypes.c_float), ("tried", ctypes.c_int), ("tile", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from ._lib import (PCF_ANI, PCF_BOTH, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT,  # noqa: F401
                    PCF_ERR_TIMEOUT, PCF_GRAPH, PCF_ISO, PCF_OPT_ABORT_HOST_CHECK,
-                   PCF_OPT_TRIP_FLUSH_BUDGET, PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO,
+                   PCF_OPT_PAIR_VARIANT, PCF_OPT_TRIP_FLUSH_BUDGET, PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO,
                    PCF_RULE_INCLUSIVE, PcfError, Stats)
 
 

@@ -127,6 +127,10 @@ pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value) {
     case PCF_OPT_ABORT_HOST_CHECK:
         ctx->abort_host_check = value != 0;
         return PCF_OK;
+    case PCF_OPT_PAIR_VARIANT:
+        if (value < 0 || value > 2) return PCF_ERR_INVALID_ARG;
+        ctx->pair_variant = (int)value;
+        return PCF_OK;
     }
     return PCF_ERR_INVALID_ARG;
 }
@@ -404,7 +408,7 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     const bool bpc = (flags & PCF_BPC) != 0, cross = b != nullptr;
     const bool weighted = !(a->unit_weights && (!cross || b->unit_weights));
     TuneEntry te;
-    if (ctx->tune_override.refine > 0 || ctx->tune_override.hist_mode >= 0) {
+    if (ctx->tune_override.refine > 0 || ctx->tune_override.hist_mode >= 0 || ctx->tune_override.tile) {
         te = ctx->tune_override;
     } else if (!ctx->tune.empty()) {
         auto it = ctx->tune.find(tune_key(kind, bpc, cross, weighted, bins,
@@ -440,8 +444,13 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     int P = 0;
     pcf_status s = prepare_grids(ctx, a, b, dmax, kind, bpc, &P, te.refine);
     if (s != PCF_OK) return s;
+    const int tile_cap = te.tile == 16 ? 16 : kTileCap;
+    if (tile_cap == 16) {
+        s = ensure_half_tiles(ctx, *a->cells);
+        if (s != PCF_OK) return s;
+    }
     PairPlan plan;
-    plan_pairs(*a->cells, a->box, dmax, ani, !cross, plan, ctx->sm_count * 24);
+    plan_pairs(*a->cells, a->box, dmax, ani, !cross, plan, ctx->sm_count * 24, tile_cap);
     const int nb = both ? bins + bins * bins : ani ? bins * bins : bins;
     unsigned long long *d_cnt, *d_stats;
     double *d_ws, *d_out;
@@ -466,6 +475,8 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     pl.count = stats != nullptr && !ctx->tune_timing;
     pl.ctrl = ctx->d_ctrl;
     pl.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
+    pl.variant = ctx->pair_variant;
+    pl.tile_cap = tile_cap;
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
                      d_stats);
     if (s != PCF_OK) return s;

@@ -411,7 +411,7 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
         return PCF_ERR_OUT_OF_BOX;
     }
     set_weight_range(g, hf);
-    build_tiles(*cg);
+    build_tiles(*cg, kTileCap, cg->tiles);
     cg->d_tiles.pool = g->pool;
     PCF_CU(ctx, cg->d_tiles.ensure(sizeof(TileDesc) * std::max<size_t>(1, cg->tiles.size())));
     if (!cg->tiles.empty()) {
@@ -463,4 +463,23 @@ int choose_partitions(int64_t n, float box, float dmax, int kind, bool bpc, int 
     }
     (void)kind;
     return P;
+}
+
+pcf_status ensure_half_tiles(pcf_ctx *ctx, CellGrid &g) {
+    if (g.have_half) return PCF_OK;
+    build_tiles(g, 16, g.tiles_half);
+    g.d_tiles_half.pool = g.d_tiles.pool;
+    PCF_CU(ctx, g.d_tiles_half.ensure(sizeof(TileDesc) * std::max<size_t>(1, g.tiles_half.size())));
+    if (!g.tiles_half.empty()) {
+        // the page-locked buffer may still feed an earlier copy: wait first
+        PCF_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        const size_t tb = sizeof(TileDesc) * g.tiles_half.size();
+        pcf_status ps = pcf_ensure_pinned(ctx, tb);
+        if (ps != PCF_OK) return ps;
+        memcpy(ctx->h_pinned, g.tiles_half.data(), tb);
+        PCF_CU(ctx, cudaMemcpyAsync(g.d_tiles_half.p, ctx->h_pinned, tb, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+    }
+    g.have_half = true;
+    return PCF_OK;
 }

@@ -60,7 +60,16 @@ constexpr unsigned kBinBias = 0x43800000u >> kFracBits;
 // fixed-point limbs in four sub-copies, lane l adding to copy l % 4 (the
 // isotropic copy of a weighted both-kinds launch: its few bins would
 // otherwise take the reductions of all 32 lanes).
-enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3, H_LFIX = 4, H_WFIX4 = 5 };
+enum { H_LANE = 0, H_WARP = 1, H_GLOBAL = 2, H_WFIX = 3, H_LFIX = 4, H_WFIX4 = 5, H_WFIX2 = 6 };
+// Variants of the weighted one-pass both-kinds kernel (the isotropic copy
+// and the candidate loads), selected by PCF_OPT_PAIR_VARIANT for the A/B of
+// shared-memory staging: 0 four isotropic sub-copies, candidates by __ldg
+// (the default); 1 two sub-copies (frees 720 B per warp), __ldg; 2 two
+// sub-copies, candidates of full tiles staged into shared memory by
+// cp.async, in double-buffered windows of 16, in the space the two freed
+// sub-copies left (so the CTA count per SM stays at four).
+constexpr int kStageCands = 16;
+constexpr int kStageBytes = 2 * (kStageCands * 16 + kStageCands * 4);  // per warp
 constexpr int kLimbs = 3;
 // Candidate steps between recheck votes, per kind: the anisotropic (and
 // both-kinds) kernels carry more live state per step and schedule better
@@ -143,7 +152,8 @@ __device__ __forceinline__ void red_s_limbs(unsigned a, unsigned long long v) {
 // float w (FP64 modes) or nothing (unit weights).
 template <bool WEIGHTED, int HM>
 struct WT {
-    typedef typename std::conditional<(HM == H_WFIX || HM == H_LFIX || HM == H_WFIX4), unsigned, float>::type type;
+    typedef typename std::conditional<(HM == H_WFIX || HM == H_LFIX || HM == H_WFIX4 || HM == H_WFIX2),
+                                      unsigned, float>::type type;
 };
 
 // Histogram sink of one lane.  Slots arrive biased (see kBinBias); `base`
@@ -161,7 +171,7 @@ struct Sink {
         if (HM == H_LFIX) {
             red_s_limbs<128>(pred ? base + sb * (kLimbs * 128u) : dummy,
                              (unsigned long long)(pred ? wa : 0u) * wb);
-        } else if (HM == H_WFIX || HM == H_WFIX4) {
+        } else if (HM == H_WFIX || HM == H_WFIX4 || HM == H_WFIX2) {
             red_s_limbs<4>(pred ? base + sb * (kLimbs * 4u) : dummy,
                            (unsigned long long)(pred ? wa : 0u) * wb);
         } else if (HM == H_LANE) {
@@ -209,7 +219,8 @@ __device__ __noinline__ int slow_slot(float hx, float hy, float hz, float cx, fl
 template <int HM>
 __host__ __device__ __forceinline__ int copy_words(int nb) {
     return HM == H_LANE ? nb * 32 : HM == H_WARP ? nb + 32 : HM == H_WFIX ? nb * kLimbs + 32 + kLimbs - 1
-         : HM == H_WFIX4 ? 4 * nb * kLimbs + 32 + kLimbs - 1 : HM == H_LFIX ? nb * kLimbs * 32 : 0;
+         : HM == H_WFIX4 ? 4 * nb * kLimbs + 32 + kLimbs - 1 : HM == H_WFIX2 ? 2 * nb * kLimbs + 32 + kLimbs - 1
+         : HM == H_LFIX ? nb * kLimbs * 32 : 0;
 }
 
 // Adds this warp's copy (nb bins) into the launch's accumulators at `off`
@@ -259,12 +270,13 @@ __device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, si
                 atomicAdd(A.g_wsum + off + k, v * unscale);
             }
         }
-    } else if (HM == H_WFIX4) {  // [copy][bin][limb]: limbs summed exactly over the copies
+    } else if (HM == H_WFIX4 || HM == H_WFIX2) {  // [copy][bin][limb]: limbs summed exactly over the copies
+        constexpr int NSUB = HM == H_WFIX4 ? 4 : 2;
         unsigned *mine = static_cast<unsigned *>(mine_v);
         for (int k = lane; k < nb; k += 32) {
             unsigned long long s0 = 0, s1 = 0, s2 = 0;
             #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < NSUB; ++q) {
                 unsigned *c = mine + (q * nb + k) * kLimbs;
                 s0 += c[0];
                 s1 += c[1];
@@ -308,19 +320,20 @@ enum { K_ISO = 0, K_ANI = 1, K_BOTH = 2 };
 // Scheme of the isotropic copy of a K_BOTH launch, given the anisotropic one:
 // lane-private counts, four per-warp fixed-point sub-copies, else per-warp
 // copies of the same element type.
-__host__ __device__ constexpr int iso_scheme(bool weighted, int hm) {
-    return hm == H_WARP ? (weighted ? H_WARP : H_LANE) : hm == H_WFIX ? H_WFIX4 : hm;
+__host__ __device__ constexpr int iso_scheme(bool weighted, int hm, int var = 0) {
+    return hm == H_WARP ? (weighted ? H_WARP : H_LANE) : hm == H_WFIX ? (var ? H_WFIX2 : H_WFIX4) : hm;
 }
-template <bool WEIGHTED, int HM>
+template <bool WEIGHTED, int HM, int VAR>
 struct IsoScheme {
-    static constexpr int value = iso_scheme(WEIGHTED, HM);
+    static constexpr int value = iso_scheme(WEIGHTED, HM, VAR);
 };
 
 // Sets up one lane's sink over a copy at shared address ms (see Sink).
 template <bool WEIGHTED, int HM>
 __device__ __forceinline__ void setup_sink(Sink<WEIGHTED, HM> &sk, unsigned ms, void *mine, int lane,
                                            unsigned bias, int nb) {
-    typedef typename std::conditional<WEIGHTED && !(HM == H_WFIX || HM == H_LFIX || HM == H_WFIX4), double, unsigned>::type HT;
+    typedef typename std::conditional<WEIGHTED && !(HM == H_WFIX || HM == H_LFIX || HM == H_WFIX4 || HM == H_WFIX2),
+                                      double, unsigned>::type HT;
     sk.bias = bias;
     sk.lane_col = reinterpret_cast<double *>(mine) + lane;
     sk.gbase = nullptr;
@@ -337,6 +350,10 @@ __device__ __forceinline__ void setup_sink(Sink<WEIGHTED, HM> &sk, unsigned ms, 
     case H_WFIX4:
         sk.base = ms + (unsigned)((lane & 3) * nb * kLimbs) * 4u - bias * (kLimbs * 4u);
         sk.dummy = ms + (unsigned)(4 * nb * kLimbs + lane) * 4u;
+        break;
+    case H_WFIX2:
+        sk.base = ms + (unsigned)((lane & 1) * nb * kLimbs) * 4u - bias * (kLimbs * 4u);
+        sk.dummy = ms + (unsigned)(2 * nb * kLimbs + lane) * 4u;
         break;
     case H_LFIX: sk.base = ms + lane * 4u - bias * (kLimbs * 128u); sk.dummy = ms + lane * 4u; break;
     default: sk.base = sk.dummy = 0u;
@@ -365,15 +382,16 @@ struct WarpState {
 
 // COUNT: also count the in-range pairs (weighted histograms, statistics on).
 // HM is the scheme of the anisotropic copy for K_ANI / K_BOTH launches.
-template <int KIND, bool WEIGHTED, int HM, bool COUNT>
+template <int KIND, bool WEIGHTED, int HM, bool COUNT, int VAR = 0>
 __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(const PairArgs A) {
     constexpr bool FIX = HM == H_WFIX || HM == H_LFIX;
     constexpr bool DO_I = KIND != K_ANI, DO_A = KIND != K_ISO;
     constexpr bool kPrefetch = KIND == K_BOTH && HM == H_WFIX;  // measured: helps only here
+    constexpr bool kStage = VAR == 2;  // candidates of full tiles through shared memory
     // with the next step's loads in flight, a vote per step ran 1.4% faster
     // than one per two steps (periodic 2iso+2ani step, A/B on one box)
     constexpr int kGroup = kPrefetch ? 1 : KIND == K_ISO ? PCF_GROUP_ISO : PCF_GROUP_ANI;
-    constexpr int HMI = KIND == K_BOTH ? IsoScheme<WEIGHTED, HM>::value : HM;
+    constexpr int HMI = KIND == K_BOTH ? IsoScheme<WEIGHTED, HM, VAR>::value : HM;
     typedef typename WT<WEIGHTED, HM>::type W;
     typedef typename std::conditional<WEIGHTED && !FIX, double, unsigned>::type HT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -387,6 +405,16 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
     const int wi = DO_I ? copy_words<HMI>(nbi) : 0, wa = DO_A ? copy_words<HM>(nba) : 0;
     HT *mine_i = reinterpret_cast<HT *>(smem_raw) + warp * (wi + wa);
     HT *mine_a = mine_i + wi;
+    // staging windows (kStage): two of kStageCands candidates per warp after
+    // every warp's copies: pair-packed blocks, then their integer weights
+    float4 *stg_f4 = nullptr;
+    unsigned *stg_q = nullptr;
+    if (kStage) {
+        unsigned char *sb = smem_raw + (((size_t)kWarps * (wi + wa) * sizeof(HT) + 15) & ~(size_t)15) +
+                            (size_t)warp * kStageBytes;
+        stg_f4 = reinterpret_cast<float4 *>(sb);
+        stg_q = reinterpret_cast<unsigned *>(sb + 2 * kStageCands * 16);
+    }
     for (int k = lane; k < wi + wa; k += 32) mine_i[k] = (HT)0;
     const unsigned bias_i = kBinBias, bias_a = kBinBias * (unsigned)(bins + 1);
     Sink<WEIGHTED, HMI> sink_i;
@@ -710,6 +738,53 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
                             for (int k = 0; k < kGroup; ++k) any |= core(p + k * stride, true, true);
                             settle(any, p, kGroup, true, true);
                         }
+                    } else if (kStage && H == 32) {
+                        // the steps p + 1 < hi_i, in windows of kStageCands
+                        // candidates copied into this warp's shared buffers by
+                        // cp.async (double-buffered; all lanes walk the same
+                        // candidates, so reads broadcast)
+                        const int nst = p + 1 < hi_i ? (hi_i - p) / 2 : 0;
+                        const int nwin = (nst + kStageCands / 2 - 1) / (kStageCands / 2);
+                        const int p0 = p;
+                        auto stage = [&](int w) {
+                            const int q = p0 + kStageCands * w;
+                            float4 *dst = stg_f4 + (w & 1) * kStageCands;
+                            if (lane < kStageCands) {
+                                // float4 q + lane belongs to the block of point q + (lane & ~1)
+                                const bool in = q + (lane & ~1) < hi_i;
+                                const unsigned d = (unsigned)__cvta_generic_to_shared(dst + lane);
+                                asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;"
+                                             :: "r"(d), "l"(cpk + q + lane), "r"(in ? 16 : 0));
+                            } else if (FIX && lane < kStageCands + kStageCands / 2) {
+                                const int t = 2 * (lane - kStageCands);
+                                const bool in = q + t < hi_i;
+                                const unsigned d = (unsigned)__cvta_generic_to_shared(
+                                    stg_q + (w & 1) * kStageCands + t);
+                                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                                             :: "r"(d), "l"(cqw + q + t), "r"(in ? 8 : 0));
+                            }
+                            asm volatile("cp.async.commit_group;" ::: "memory");
+                        };
+                        if (nwin > 0) stage(0);
+                        if (nwin > 1) stage(1);
+                        for (int w = 0; w < nwin; ++w) {
+                            if (w + 1 < nwin) asm volatile("cp.async.wait_group 1;" ::: "memory");
+                            else asm volatile("cp.async.wait_group 0;" ::: "memory");
+                            __syncwarp();
+                            const int ns = min(kStageCands / 2, nst - (kStageCands / 2) * w);
+                            const float4 *sf = stg_f4 + (w & 1) * kStageCands;
+                            const uint2 *sq = reinterpret_cast<const uint2 *>(stg_q + (w & 1) * kStageCands);
+                            for (int s = 0; s < ns; ++s) {
+                                Raw r;
+                                r.qa = sf[2 * s];
+                                r.qb = sf[2 * s + 1];
+                                r.q = FIX ? sq[s] : make_uint2(0u, 0u);
+                                settle(core_raw(r, true, true), p0 + kStageCands * w + 2 * s, 1, true, true);
+                            }
+                            __syncwarp();  // every lane has read this buffer
+                            if (w + 2 < nwin) stage(w + 2);
+                        }
+                        p = p0 + 2 * nst;
                     } else if (p + (kGroup - 1) * stride + 1 < hi_i) {
                         Raw nx[kGroup];
                         #pragma unroll
@@ -811,10 +886,10 @@ __global__ void k_finalize(const unsigned long long *__restrict__ cnt, const dou
 // when cells hold fewer than 32 points.  Two cells keep a periodic stencil
 // within the box: the counts require 2k + 2 <= P for k neighbour cells per
 // side, and a row covers z0 - k .. z1 + k.
-void build_tiles(CellGrid &g) {
+void build_tiles(const CellGrid &g, int cap, std::vector<TileDesc> &out) {
     const int P = g.P;
     const std::vector<int> &hs = g.h_start;
-    g.tiles.clear();
+    out.clear();
     for (int ix = 0; ix < P; ++ix)
         for (int iy = 0; iy < P; ++iy) {
             const int col = (ix * P + iy) * P;
@@ -824,7 +899,7 @@ void build_tiles(CellGrid &g) {
             while (p < end) {
                 while (hs[col + iz + 1] <= p) ++iz;  // cell of point p
                 const int limit = hs[col + std::min(iz + 2, P)];
-                const int n = std::min(kTileCap, limit - p);
+                const int n = std::min(cap, limit - p);
                 int z1 = iz;
                 while (hs[col + z1 + 1] < p + n) ++z1;  // cell of the tile's last point
                 TileDesc t;
@@ -834,7 +909,7 @@ void build_tiles(CellGrid &g) {
                 t.iy = (int16_t)iy;
                 t.z0 = (int16_t)iz;
                 t.z1 = (int16_t)z1;
-                g.tiles.push_back(t);
+                out.push_back(t);
                 p += n;
             }
         }
@@ -878,13 +953,13 @@ void plan_rows(int P, float box, float dmax, bool ani, bool self, std::vector<Ro
 }
 
 void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self, PairPlan &plan,
-                int resident_warps) {
+                int resident_warps, int tile_cap) {
     const int P = home.P;
     plan.P = P;
     plan.cell = (float)((double)box / P);
     plan_rows(P, box, dmax, ani, self, plan.rows);
     // ~16 items per resident warp keeps the tail short; at most 32 rows each
-    const int64_t nt = (int64_t)home.tiles.size();
+    const int64_t nt = (int64_t)home.tiles_for(tile_cap).size();
     const int64_t nr = (int64_t)plan.rows.size();
     const int64_t want = std::max<int64_t>(1, (int64_t)resident_warps * 16);
     int rpi = (int)std::min<int64_t>(32, std::max<int64_t>(1, (nt * nr) / want));
@@ -928,14 +1003,21 @@ static int copy_words_host(int hm, int nb) {
     case H_WFIX: return copy_words<H_WFIX>(nb);
     case H_LFIX: return copy_words<H_LFIX>(nb);
     case H_WFIX4: return copy_words<H_WFIX4>(nb);
+    case H_WFIX2: return copy_words<H_WFIX2>(nb);
     }
     return 0;
 }
 
-template <int KIND, bool W, int HM, bool C>
+// The one-pass variant of a launch (PCF_OPT_PAIR_VARIANT): only the weighted
+// both-kinds kernel with per-warp fixed-point copies has variants.
+static int pair_variant(const PairLaunch &pl, int hm) {
+    return (pl.both && pl.weighted && hm == H_WFIX && !pl.count) ? pl.variant : 0;
+}
+
+template <int KIND, bool W, int HM, bool C, int VAR = 0>
 static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items, cudaStream_t st,
                               int sm_count, int device) {
-    auto kfn = k_pairs<KIND, W, HM, C>;
+    auto kfn = k_pairs<KIND, W, HM, C, VAR>;
     // occupancy queries cost microseconds: cached per (device, shared-memory
     // size) and instantiation, under a lock (several host threads launch)
     struct Occ {
@@ -980,9 +1062,12 @@ static size_t scheme_bytes(const PairLaunch &pl, int hm) {
     const int bins = pl.rule.bins;
     const int nb = pl.ani ? bins * bins : bins;
     const size_t e = (hm == H_WFIX || hm == H_LFIX) ? 4 : (pl.weighted ? 8 : 4);
+    const int var = pair_variant(pl, hm);
     size_t w = (size_t)copy_words_host(hm, nb);
-    if (pl.both) w += (size_t)copy_words_host(iso_scheme(pl.weighted, hm), bins);
-    return w * e * kWarps;
+    if (pl.both) w += (size_t)copy_words_host(iso_scheme(pl.weighted, hm, var), bins);
+    size_t b = w * e * kWarps;
+    if (var == 2) b = ((b + 15) & ~(size_t)15) + (size_t)kWarps * kStageBytes;
+    return b;
 }
 
 static bool scheme_fits(const PairLaunch &pl, int hm) {
@@ -1044,6 +1129,9 @@ static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t
         if (hm == H_WARP) return launch_one<K_ISO, false, H_WARP, false>(A, smem, n, st, sm_count, device);
         return launch_one<K_ISO, false, H_GLOBAL, false>(A, smem, n, st, sm_count, device);
     }
+    const int var = pair_variant(pl, hm);
+    if (pl.both && var == 1) return launch_one<K_BOTH, true, H_WFIX, false, 1>(A, smem, n, st, sm_count, device);
+    if (pl.both && var == 2) return launch_one<K_BOTH, true, H_WFIX, false, 2>(A, smem, n, st, sm_count, device);
 #define PCF_DISPATCH_A(K_)                                                                         \
     if (pl.weighted) {                                                                             \
         if (hm == H_WARP) PCF_LAUNCH(K_, true, H_WARP);                                            \
@@ -1217,7 +1305,7 @@ pcf_status launch_pairs(pcf_ctx *ctx, const PairPlan &plan, const CellGrid &home
     PairJob job;
     job.home = pair_view(home, pl.wfix);
     job.cand = pair_view(cand, pl.wfix);
-    job.tiles = home.d_tiles.as<TileDesc>();
+    job.tiles = home.d_tiles_for(pl.tile_cap);
     job.rows = sl->d_rows.as<RowDesc>();
     job.n_rows = (int)plan.rows.size();
     job.rows_per_item = plan.rows_per_item;

@@ -152,6 +152,8 @@ struct DevBuf {
     template <class T> T *as() const { return static_cast<T *>(p); }
 };
 
+constexpr int kTileCap = 32;  // home points per warp item
+
 struct CellGrid {
     int P = 0;
     uint64_t serial = 0;          // unique per build (keys captured graphs)
@@ -164,6 +166,15 @@ struct CellGrid {
     std::vector<int> h_start;     // host copy of cell_start
     std::vector<TileDesc> tiles;  // home tiles: <= 32 points of one column, <= 2 cells
     DevBuf d_tiles;
+    // the same with at most 16 points per tile (an autotuner candidate),
+    // built on first use
+    std::vector<TileDesc> tiles_half;
+    DevBuf d_tiles_half;
+    bool have_half = false;
+    const std::vector<TileDesc> &tiles_for(int cap) const { return cap == 16 ? tiles_half : tiles; }
+    const TileDesc *d_tiles_for(int cap) const {
+        return (cap == 16 ? d_tiles_half : d_tiles).as<TileDesc>();
+    }
     const float *x() const { return soa.as<float>(); }
     const float *y() const { return soa.as<float>() + plane; }
     const float *z() const { return soa.as<float>() + 2 * plane; }
@@ -214,6 +225,7 @@ struct TuneEntry {
     int refine = 0;      // cells per dmax (0: default rule)
     int hist_mode = -1;  // histogram privatisation (-1: default rule)
     float ms = 0.f;      // best kernel time seen while tuning
+    int tile = 0;        // home points per tile: 0 or 32 (kTileCap), or 16
 };
 
 struct pcf_ctx {
@@ -252,6 +264,7 @@ struct pcf_ctx {
     bool abort_host_check = true;  // refuse calls while the request is set
     // adds a triplet kernel's shared u32 histogram absorbs between flushes
     unsigned long long trip_flush_budget = 1ull << 31;
+    int pair_variant = 0;  // PCF_OPT_PAIR_VARIANT
     std::map<std::string, std::shared_ptr<struct BatchGraph>> graphs;  // pcf_batch_pairs(PCF_GRAPH)
 };
 
@@ -284,15 +297,16 @@ struct PairPlan {
     int64_t n_items = 0;
 };
 
-constexpr int kTileCap = 32;  // home points per warp item
-// Home tiles of a gridded catalog: runs of at most kTileCap consecutive
-// points of one column within two adjacent cells (pairs.cu).
-void build_tiles(CellGrid &g);
+// Home tiles of a gridded catalog: runs of at most `cap` (<= kTileCap)
+// consecutive points of one column within two adjacent cells (pairs.cu).
+void build_tiles(const CellGrid &g, int cap, std::vector<TileDesc> &out);
+// The 16-point tile table of a cell structure, built and uploaded on first use.
+pcf_status ensure_half_tiles(pcf_ctx *ctx, CellGrid &g);
 // Stencil rows (dx, dy, kz) of cells that can hold a pair within dmax.
 void plan_rows(int P, float box, float dmax, bool ani, bool self, std::vector<RowDesc> &rows);
 // Builds the stencil and item shape of one pair launch.  self: XX half shell.
 void plan_pairs(const CellGrid &home, float box, float dmax, bool ani, bool self, PairPlan &plan,
-                int resident_warps);
+                int resident_warps, int tile_cap = kTileCap);
 
 pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes);
 // PCF_ERR_TIMEOUT if an abort is requested (before a call launches) or if a
@@ -319,6 +333,8 @@ struct PairLaunch {
     // ticket and the status word it sets when it gives up; null: no polling
     const unsigned *ctrl = nullptr;
     unsigned *status = nullptr;
+    int variant = 0;     // one-pass kernel variant (PCF_OPT_PAIR_VARIANT; pairs.cu)
+    int tile_cap = kTileCap;  // home points per tile (32, or 16 when tuned so)
 };
 // Enables the fixed-point weighted histograms when every grid of the launch
 // has exact integer weights and any product fits the three-limb budget.

@@ -68,12 +68,33 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
             }
         }
     }
+    // home tiles of 16 points instead of 32 at the best shape (twice the
+    // candidate streams per warp, half the home points per item)
+    if (best.ms < 1e30f) {
+        ctx->tune_override.refine = best.refine;
+        ctx->tune_override.hist_mode = best.hist_mode;
+        ctx->tune_override.tile = 16;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+            pcf_stats st{};
+            pcf_status s = pcf_count_pairs(ctx, kind, a, b, bins, dmax, flags | PCF_DEVICE_OUT,
+                                           out.as<double>(), &st);
+            if (s != PCF_OK) { ms = 1e30f; break; }
+            ms = std::min(ms, st.kernel_ms);
+        }
+        ++tried;
+        if (ms < best.ms) {
+            best.ms = ms;
+            best.tile = 16;
+        }
+    }
     ctx->tune_override = TuneEntry();
     ctx->tune_timing = false;
     ctx->tune[key] = best;
     if (res) {
         res->refine = best.refine;
         res->hist_mode = best.hist_mode;
+        res->tile = best.tile ? best.tile : kTileCap;
         res->best_ms = best.ms;
         res->default_ms = default_ms;
         res->tried = tried;
@@ -86,7 +107,8 @@ extern "C" pcf_status pcf_tune_save(const pcf_ctx *ctx, const char *path) {
     std::ofstream f(path);
     if (!f) return PCF_ERR_IO;
     for (const auto &kv : ctx->tune)
-        f << kv.first << ' ' << kv.second.refine << ' ' << kv.second.hist_mode << ' ' << kv.second.ms << '\n';
+        f << kv.first << ' ' << kv.second.refine << ' ' << kv.second.hist_mode << ' ' << kv.second.ms
+          << ' ' << (kv.second.tile ? kv.second.tile : kTileCap) << '\n';
     return f ? PCF_OK : PCF_ERR_IO;
 }
 
@@ -94,9 +116,16 @@ extern "C" pcf_status pcf_tune_load(pcf_ctx *ctx, const char *path) {
     if (!ctx || !path) return PCF_ERR_INVALID_ARG;
     std::ifstream f(path);
     if (!f) return PCF_ERR_IO;
-    std::string key;
-    TuneEntry e;
-    while (f >> key >> e.refine >> e.hist_mode >> e.ms) ctx->tune[key] = e;
+    std::string line;
+    while (std::getline(f, line)) {  // "key refine hist_mode ms [tile]"
+        std::istringstream is(line);
+        std::string key;
+        TuneEntry e;
+        if (!(is >> key >> e.refine >> e.hist_mode >> e.ms)) continue;
+        int tile = 0;
+        if (is >> tile) e.tile = tile == 16 ? 16 : 0;
+        ctx->tune[key] = e;
+    }
     return PCF_OK;
 }
 

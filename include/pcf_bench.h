@@ -34,8 +34,15 @@ pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
  *   PCF_OPT_ABORT_HOST_CHECK   0: calls launch even while an abort is
  *                              requested, so the kernels' own polling is what
  *                              stops them (a test of it); 1 (default): they
- *                              return PCF_ERR_TIMEOUT without launching. */
-enum { PCF_OPT_TRIP_FLUSH_BUDGET = 1, PCF_OPT_ABORT_HOST_CHECK = 2 };
+ *                              return PCF_ERR_TIMEOUT without launching.
+ *   PCF_OPT_PAIR_VARIANT       the weighted one-pass (PCF_BOTH) pair kernel:
+ *                              0 (default) four isotropic sub-copies,
+ *                              candidates through the L1 path; 1 two
+ *                              sub-copies; 2 two sub-copies and candidates
+ *                              staged into shared memory by cp.async (the
+ *                              measured A/B of staging).  Results are the
+ *                              same in every variant. */
+enum { PCF_OPT_TRIP_FLUSH_BUDGET = 1, PCF_OPT_ABORT_HOST_CHECK = 2, PCF_OPT_PAIR_VARIANT = 3 };
 pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value);
 
 /* Kernels this context has launched since it was created. */

@@ -3,11 +3,16 @@
  * which hard-codes 35 partitions per side and one thread per cell pair).
  *
  * The launch shape of a pair histogram is the cell size (cells per dmax,
- * "refine") and the histogram privatisation scheme (0: one column per lane,
- * 1: one copy per warp with shared atomics, 2: global atomics).  The best
- * shape depends on the kind, the bins and the point density, so the tuner
- * times candidates on the caller's own catalogs and records the winner for
- * the class (kind, periodic, XX/XY, weighted, bins, expected neighbours per
+ * "refine": the default rule, 3, 4, 5, 6 or 8), the histogram privatisation
+ * scheme (-1: the library's rule; 0: a u32 column per lane; 1: one copy per
+ * warp with shared atomics; 3: per-warp fixed-point limbs of the exact
+ * weight products; 4: lane-private fixed-point limbs (isotropic); for
+ * PCF_BOTH a scheme >= 0 means one pass over the candidates for both kinds)
+ * and the home-tile size (32 or 16 points per warp item).  The best shape
+ * depends on the kind, the bins and the point density, so the tuner times
+ * candidates on the caller's own catalogs (every refine x scheme at 32-point
+ * tiles, then 16-point tiles at the winner) and records the winner for the
+ * class (kind, periodic, XX/XY, weighted, bins, expected neighbours per
  * point in half-octave buckets).  Later counting calls of that class in the
  * same context use it.  The table can be saved and loaded as text.
  */
@@ -26,13 +31,15 @@ typedef struct pcf_tune_result {
     float best_ms;    /* kernel time of the winner                  */
     float default_ms; /* kernel time of the default shape           */
     int tried;        /* candidates timed                           */
+    int tile;         /* chosen home points per tile (32 or 16)     */
 } pcf_tune_result;
 
 /* Times the candidates for one pair histogram (arguments as pcf_count_pairs)
  * and stores the winner in the context's table. */
 pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a, const pcf_grid *b,
                               int bins, float dmax, uint32_t flags, pcf_tune_result *res);
-/* Text form: one line "key refine hist_mode ms" per class. */
+/* Text form: one line "key refine hist_mode ms tile" per class (tile may be
+ * omitted: 32). */
 pcf_status pcf_tune_save(const pcf_ctx *ctx, const char *path);
 pcf_status pcf_tune_load(pcf_ctx *ctx, const char *path);
 /* Number of classes in the table. */

@@ -72,9 +72,12 @@ def test_headline_step_tuned(headline_catalogs):
         np.testing.assert_allclose(got[k], want[k], rtol=1e-12, atol=0)
 
 
-def test_headline_step_forced_one_pass(headline_catalogs, tmp_path):
-    """Both kinds in one pass with per-warp fixed-point limbs (scheme 3) and
-    the isotropic copy in four sub-copies, at the headline size, P = 12."""
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_headline_step_forced_one_pass(headline_catalogs, tmp_path, variant):
+    """Both kinds in one pass with per-warp fixed-point limbs (scheme 3) at
+    the headline size, P = 12, in each kernel variant: the isotropic copy in
+    four sub-copies (0), in two (1), and two with the candidates staged into
+    shared memory by cp.async (2)."""
     D, R, want = headline_catalogs
     W = bench.WORKLOAD
     path = str(tmp_path / "tune.txt")
@@ -85,6 +88,7 @@ def test_headline_step_forced_one_pass(headline_catalogs, tmp_path):
     ctx = api.Context(0)
     try:
         ctx.tune_load(path)
+        ctx.set_option(api.PCF_OPT_PAIR_VARIANT, variant)
         got = _run_step(ctx, D, R, 12, ("both",))
     finally:
         ctx.close()

@@ -334,3 +334,62 @@ def test_both_kinds_device_output(ctx, tmp_path, tuned):
             _cmp(got[bins:], ani.ravel(), True)
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("bpc", [False, True])
+def test_one_pass_variants(tmp_path, variant, bpc):
+    """The weighted one-pass kernel's variants (two isotropic sub-copies;
+    plus candidates staged into shared memory) give the oracle's histograms
+    within 1e-12, on catalogs dense enough for full 32-point tiles and on
+    sparse ones (partial tiles take the unstaged path)."""
+    from desi_b200 import api
+    box, dmax, bins = 250.0, 80.0, 30
+    for n in (2600, 9000):
+        D = catalog.neyman_scott(n, box, seed=63, weights="uniform")
+        R = catalog.uniform(n + 77, box, seed=64, weights="uniform")
+        path = str(tmp_path / f"tune{n}.txt")
+        with open(path, "w") as f:
+            for cross in (False, True):
+                f.write(f"{_tune_key('both', bpc, cross, True, bins, n + 77 if cross else n, box, dmax)} 0 3 1.0\n")
+        c = api.Context(0)
+        try:
+            c.tune_load(path)
+            c.set_option(api.PCF_OPT_PAIR_VARIANT, variant)
+            gd, gr = c.grid(D, box), c.grid(R, box)
+            for (a, b, A, B) in ((gd, None, D, None), (gd, gr, D, R)):
+                iso, ani = c.count_pairs(a, b, bins=bins, dmax=dmax, ani="both", bpc=bpc)
+                for got, is_ani in ((iso, False), (ani, True)):
+                    want = oracle.pairs(A, B, box=box, bins=bins, dmax=dmax, ani=is_ani, bpc=bpc)
+                    _cmp(got, want, True)
+        finally:
+            c.close()
+
+
+@pytest.mark.parametrize("ani", [False, True, "both"])
+@pytest.mark.parametrize("w", ["unit", "uniform"])
+def test_half_tiles(tmp_path, ani, w):
+    """Home tiles of 16 points (an autotuner candidate, forced through a
+    loaded tuning table with the tile column) give the oracle's histograms."""
+    from desi_b200 import api
+    box, dmax, bins, n = 250.0, 80.0, 30, 3000
+    D = catalog.neyman_scott(n, box, seed=65, weights=w)
+    R = catalog.uniform(n + 50, box, seed=66, weights=w)
+    path = str(tmp_path / "tune.txt")
+    mode = 3 if (ani == "both" and w != "unit") else -1
+    with open(path, "w") as f:
+        for cross in (False, True):
+            key = _tune_key(ani, True, cross, w != "unit", bins, n + 50 if cross else n, box, dmax)
+            f.write(f"{key} 0 {mode} 1.0 16\n")
+    c = api.Context(0)
+    try:
+        c.tune_load(path)
+        gd, gr = c.grid(D, box), c.grid(R, box)
+        for (a, b, A, B) in ((gd, None, D, None), (gd, gr, D, R)):
+            got = c.count_pairs(a, b, bins=bins, dmax=dmax, ani=ani, bpc=True)
+            kinds = ((got[0], False), (got[1], True)) if ani == "both" else ((got, ani),)
+            for g, is_ani in kinds:
+                want = oracle.pairs(A, B, box=box, bins=bins, dmax=dmax, ani=is_ani, bpc=True)
+                _cmp(g, want, w != "unit")
+    finally:
+        c.close()
