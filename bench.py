@@ -709,12 +709,18 @@ def cpu_baseline(pairs_step=None, steps=1):
         for _ in range(steps):
             _cpu_step(eng, D, R, threads)
         dt = (time.perf_counter() - t0) / steps
+        # as shipped: the engines hard-code num_threads(2) (2PCF.h:163,320)
+        t0 = time.perf_counter()
+        _cpu_step(eng, D, R, 2)
+        dt2 = time.perf_counter() - t0
         return {"value": pairs_step / dt, "unit": "pairs/s", "cores": threads,
                 "kind": "reference",
                 "sample": "the full step (6 histograms, 32768+32768 points) through the "
-                          "reference engines cpp/2PCF{isotropic,anisotropic}/BPC, "
+                          "reference engines cpp/2PCF{isotropic,anisotropic}/BPC (g++ -O3 -fopenmp), "
                           f"{steps} step(s), {dt:.3f} s per step",
-                "seconds_per_step": dt}
+                "seconds_per_step": dt,
+                "as_shipped_2_threads": {"value": pairs_step / dt2, "seconds_per_step": dt2},
+                "triplets": cpu_triplet_baseline(threads)}
     # fallback: the oracle port (brute force) on a bounded sample
     import oracle
     n = 8192
@@ -736,6 +742,31 @@ def cpu_baseline(pairs_step=None, steps=1):
             cnt += h.sum() / (2 if B is None else 1)
     return {"value": 2 * cnt / dt, "unit": "pairs/s", "cores": threads, "kind": "port",
             "sample": f"oracle brute force on the first {n} points of each catalog"}
+
+
+def cpu_triplet_baseline(threads, n=8192):
+    """The reference's periodic 3-point CPU engine (cpp/3PCFisotropic/BPC,
+    NODE3P::make_histoXXX, compiled in place) on DDD of an n-point
+    Neyman-Scott catalog (box 250, 30^3 bins, dmax 80), all host threads.  The
+    GPU's triplet workload has 32768 points per catalog; at fixed box the
+    work grows as N^3 (N anchors x (N dmax^3/L^3)^2 neighbour pairs), 64x from
+    8192 to 32768, so the full-size CPU run is not timed."""
+    import oracle
+    try:
+        e = oracle.Ref3IsoBPC()
+    except FileNotFoundError:
+        return None
+    from desi_b200 import catalog
+    D = catalog.neyman_scott(n, 250.0, seed=3001, weights="unit")
+    e.set_threads(threads)
+    t0 = time.perf_counter()
+    h = e.xxx(D, box=250.0, size_node=2.17 * 250.0 / n ** (1.0 / 3.0), bins=30, dmax=80.0)
+    dt = time.perf_counter() - t0
+    tri = float(h.sum()) / 6.0  # ordered triples -> unordered triangles
+    return {"value": tri / dt, "unit": "triplets/s", "cores": threads, "kind": "reference",
+            "sample": f"DDD of {n} Neyman-Scott points (box 250, 30^3 bins, dmax 80), periodic, "
+                      f"{dt:.2f} s; work scales as N^3 at fixed box",
+            "seconds": dt}
 
 
 def run_reference(args, rank, world):
