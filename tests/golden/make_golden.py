@@ -10,15 +10,17 @@ Writes:
   catalogs.npz   float32 xyz of each catalog (weights are all 1 in the
                  reference files; checked here)
   golden_3iso.npz  int64 DDD, DDR, DRR, RRR (the .example values are integers)
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/reference
        python tests/golden/make_golden.py --fp64   (FP64-oracle histograms, see fp64_fixture)
+The reference root comes from the argument or, failing that, the
+PCF_REFERENCE_ROOT environment variable.
 """
 import os
 import sys
 
 import numpy as np
 
-REF = next((a for a in sys.argv[1:] if not a.startswith("--")), "/root/reference")
+REF = next((a for a in sys.argv[1:] if not a.startswith("--")), os.environ.get("PCF_REFERENCE_ROOT"))
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -44,6 +46,8 @@ def main():
 
 
 if __name__ == "__main__" and "--fp64" not in sys.argv:
+    if not REF:
+        sys.exit("usage: make_golden.py /path/to/reference (or set PCF_REFERENCE_ROOT)")
     main()
 
 
