@@ -583,12 +583,12 @@ def run_batched(ctx, torch, stream):
     for ani in (False, True):
         kw = dict(bins=40, dmax=120.0, ani=ani)
         nb = 40 * 40 if ani else 40
-        out = torch.zeros((len(calls), nb), dtype=torch.float64, device=torch.device("cuda", ctx.device))
+        dbuf = torch.zeros((len(calls), nb), dtype=torch.float64, device=torch.device("cuda", ctx.device))
 
         def per_call():
             # device outputs, no host wait between calls (the plain form at its best)
             for k, (a, b) in enumerate(calls):
-                ctx.count_pairs(a, b, out_device_ptr=out[k].data_ptr(), **kw)
+                ctx.count_pairs(a, b, out_device_ptr=dbuf[k].data_ptr(), **kw)
             ctx.synchronize()
 
         def batched(graph):
