@@ -152,8 +152,8 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     pl.weighted = weighted;
     pl.rule = make_pair_rule(bins, dmax, flags, ani, bpc, false);
     pl.mult = 1.0;
-    pl.ctrl = ctx->d_ctrl;
-    pl.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
+    pl.ctrl = ctx->d_abort;
+    pl.status = ctx->d_status;
     {
         std::vector<const pcf_grid *> gs(R.begin(), R.end());
         gs.push_back(D);

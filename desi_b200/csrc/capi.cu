@@ -53,8 +53,12 @@ pcf_status pcf_ctx_create(int device, pcf_ctx **out) {
     }
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
     void *ctrl = nullptr;
+    void *dstatus = nullptr;
     if (cudaHostAlloc(&ctrl, 64, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
-        cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->d_ctrl), ctrl, 0) != cudaSuccess) {
+        cudaHostGetDevicePointer(&dstatus, ctrl, 0) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void **>(&c->d_abort), 256) != cudaSuccess ||
+        cudaMemset(c->d_abort, 0, 256) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->ctrl_stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         if (ctrl) cudaFreeHost(ctrl);
         pcf_ctx_destroy(c);
@@ -62,6 +66,8 @@ pcf_status pcf_ctx_create(int device, pcf_ctx **out) {
     }
     c->h_ctrl = static_cast<unsigned *>(ctrl);
     memset(ctrl, 0, 64);
+    c->h_ctrl[3] = 1u;
+    c->d_status = static_cast<unsigned *>(dstatus) + 1;
     if (pcf_ensure_pinned(c, (size_t)2 << 20) != PCF_OK) {  // result staging (grows on demand)
         pcf_ctx_destroy(c);
         return PCF_ERR_NO_MEMORY;
@@ -77,6 +83,8 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
     ctx->pool->release();
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
+    if (ctx->d_abort) cudaFree(ctx->d_abort);
+    if (ctx->ctrl_stream) cudaStreamDestroy(ctx->ctrl_stream);
     for (auto &sl : ctx->slots) {
         if (sl.h_pinned) cudaFreeHost(sl.h_pinned);
         if (sl.done) cudaEventDestroy(sl.done);
@@ -99,14 +107,20 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
 void *pcf_ctx_stream(pcf_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 pcf_status pcf_ctx_abort(pcf_ctx *ctx, int on) {
-    if (!ctx || !ctx->h_ctrl) return PCF_ERR_INVALID_ARG;
+    if (!ctx || !ctx->h_ctrl || !ctx->d_abort) return PCF_ERR_INVALID_ARG;
     volatile unsigned *w = ctx->h_ctrl;
-    if (on) {
-        w[0] = 1u;
-    } else {
-        w[0] = 0u;
-        w[1] = 0u;
+    w[0] = on ? 1u : 0u;
+    // the request reaches the device by a copy on the control stream, which
+    // runs beside a launch in flight on the context stream
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMemcpyAsync(ctx->d_abort, ctx->h_ctrl + (on ? 3 : 2), sizeof(unsigned),
+                                    cudaMemcpyHostToDevice, ctx->ctrl_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->ctrl_stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return PCF_ERR_CUDA;
     }
+    if (!on) w[1] = 0u;
     return PCF_OK;
 }
 
@@ -473,8 +487,8 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
         pl.wunscale = weight_unscale(a, cross ? b : a);
     }
     pl.count = stats != nullptr && !ctx->tune_timing;
-    pl.ctrl = ctx->d_ctrl;
-    pl.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
+    pl.ctrl = ctx->d_abort;
+    pl.status = ctx->d_status;
     pl.variant = ctx->pair_variant;
     pl.tile_cap = tile_cap;
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,

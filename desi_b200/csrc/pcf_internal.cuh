@@ -71,12 +71,13 @@ __device__ __forceinline__ int exact_slot(double dx, double dy, double dz, const
     return bz * r.bins + bp;
 }
 
-// Queue control words in mapped host memory (pcf_ctx::h_ctrl): system-scope
-// loads and stores, so a request the host writes during a launch is seen by
-// the running kernel, and the kernel's record reaches the host.
+// Queue control.  The abort request is a word in device memory (the host
+// sets it by a copy on a stream of its own, which runs beside the kernels),
+// read by the persistent kernels at every work ticket through L2; the
+// record of a kernel giving up is written, rarely, to mapped host memory.
 __device__ __forceinline__ unsigned ctrl_load(const unsigned *p) {
     unsigned v;
-    asm volatile("ld.relaxed.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
 }
 __device__ __forceinline__ void ctrl_store(unsigned *p, unsigned v) {
@@ -255,12 +256,17 @@ struct pcf_ctx {
     void *h_pinned = nullptr;
     size_t h_pinned_bytes = 0;
     int64_t launches = 0;  // kernels launched by this context
-    // Queue control in mapped host memory: ctrl[0] is the abort request (set
-    // by any host thread, polled by the persistent kernels at every work
-    // item), ctrl[1] records that a kernel gave up its queue (bit 0: abort
-    // request, bit 1: iteration cap).  d_ctrl is the device's view of it.
+    // Queue control.  d_abort: the abort request in device memory, polled by
+    // the persistent kernels at every work item and set by pcf_ctx_abort
+    // through ctrl_stream (any host thread).  h_ctrl, mapped page-locked host
+    // memory: [0] the host's copy of the request, [1] the record of a kernel
+    // that gave up its queue (bit 0: abort request, bit 1: iteration cap),
+    // written by the kernel through d_status; [2] = 0 and [3] = 1, the
+    // sources of the request copies.
+    unsigned *d_abort = nullptr;
     unsigned *h_ctrl = nullptr;
-    unsigned *d_ctrl = nullptr;
+    unsigned *d_status = nullptr;
+    cudaStream_t ctrl_stream = nullptr;
     bool abort_host_check = true;  // refuse calls while the request is set
     // adds a triplet kernel's shared u32 histogram absorbs between flushes
     unsigned long long trip_flush_budget = 1ull << 31;

@@ -261,8 +261,12 @@ struct TripCta {
 // All triangles of anchor i of job A: pass 1 builds the anchor's
 // neighbour lists in shared memory (or, past their capacity, in this CTA's
 // global scratch), pass 2 counts the neighbour pairs.
-template <bool MIXED, bool WEIGHTED>
-__device__ __forceinline__ void tri_anchor(const TripArgs &A, int i, TripCta &C) {
+// COPY: work from a private copy of the job's arguments (the batched kernel,
+// whose arguments sit in shared memory, where every use would be a load
+// that the anchor's shared-memory stores keep the compiler from hoisting).
+template <bool MIXED, bool WEIGHTED, bool COPY = false>
+__device__ __forceinline__ void tri_anchor(const TripArgs &Ain, int i, TripCta &C) {
+    typename std::conditional<COPY, const TripArgs, const TripArgs &>::type A = Ain;
     const int bins = A.rXX.bins;
     const int nb3 = bins * bins * bins;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -604,8 +608,8 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_batch(const TripArgs 
             __syncthreads();
         }
         const int i = (int)(g - s_job.anchor_begin);
-        if (s_job.mixed) tri_anchor<true, WEIGHTED>(s_job, i, C);
-        else tri_anchor<false, WEIGHTED>(s_job, i, C);
+        if (s_job.mixed) tri_anchor<true, WEIGHTED, true>(s_job, i, C);
+        else tri_anchor<false, WEIGHTED, true>(s_job, i, C);
         __syncthreads();
     }
     if (in_smem && s_cur >= 0) {
@@ -799,8 +803,8 @@ static void trip_setup(pcf_ctx *ctx, const pcf_grid *X, const pcf_grid *Y, int P
     A.rXX = rXX;
     A.rXY = rXY;
     A.flush_budget = ctx->trip_flush_budget;
-    A.ctrl = ctx->d_ctrl;
-    A.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
+    A.ctrl = ctx->d_abort;
+    A.status = ctx->d_status;
     A.mixed = mixed ? 1 : 0;
     {
         // windows: the FP32 side |v_k - v_j| carries up to three roundings of
@@ -1130,8 +1134,8 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     A.bpc = bpc ? 1 : 0;
     A.rXX = rXX;
     A.rXY = rXY;
-    A.ctrl = ctx->d_ctrl;
-    A.status = ctx->d_ctrl ? ctx->d_ctrl + 1 : nullptr;
+    A.ctrl = ctx->d_abort;
+    A.status = ctx->d_status;
     {
         const double dd = rXX.dd;
         const double rmax = (double)dmax * rXX.ds + 1.0;

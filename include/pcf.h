@@ -106,8 +106,10 @@ void *pcf_ctx_stream(pcf_ctx *ctx);
  * Failure handling without a device fault.  pcf_ctx_abort(ctx, 1) asks the
  * context's persistent kernels (the pair, triplet and batched work queues)
  * to stop taking work at their next work item; any host thread may call it
- * while another thread's call runs (the request lives in mapped host memory
- * that the kernels poll).  While it is set, counting calls return
+ * while another thread's call runs (the request is copied, on a stream of the
+ * context's own that runs beside the launch in flight, into a device word
+ * that the kernels poll; the call returns when the copy has landed).  While
+ * it is set, counting calls return
  * PCF_ERR_TIMEOUT without launching, and a call whose kernels gave up
  * returns PCF_ERR_TIMEOUT once its work is complete (partial histograms are
  * not returned).  Every queue also stops at an iteration cap (more tickets
