@@ -613,18 +613,19 @@ def run_batched(ctx, torch, stream):
 
 
 def run_served(n_requests=300, load=0.7):
-    """The served stream: a seeded mix of 2iso / 2ani / 3iso requests (N
-    log-uniform 1k-1M, 3iso 1k-65k; bins 20-50; dmax 40-120; box
-    250/500/1000, 3iso in the 1000 box; clustered or uniform; periodic or
-    not) through the continuous-batching server with 4 slots, every request
-    gridding its catalogs from page-locked host memory (resident grids
-    dropped before each pass).  Passes over the same requests: a warm-up on
-    the first 40 (discarded), one closed-loop pass (all submitted at once)
-    that measures capacity in requests/s, one pass with Poisson arrivals at
-    `load` times that capacity (latency p50 / p99 over all requests), and
-    the plain per-call form -- the same requests one at a time, each
-    submitted when the previous one completed.  Reported: pairs/s and
-    triplets/s of the served and plain forms (same requests, same kernels)."""
+    """The served stream: a seeded mix of 2iso / 2ani / 3iso requests over a
+    shared pool of catalog pairs (N log-uniform 1k-1M, 3iso 1k-65k; bins
+    20-50; dmax 40-120; box 250/500/1000, 3iso in the 1000 box; clustered
+    or uniform; periodic or not) through the continuous-batching server with
+    4 slots, catalogs in page-locked host memory, grids kept resident within
+    a pass (dropped before each pass).  Passes over the same requests: a
+    warm-up on the first 40 (discarded), one closed-loop pass (all submitted
+    at once) that measures capacity in requests/s, one pass with Poisson
+    arrivals at `load` times that capacity (latency p50 / p99 over all
+    requests), and the plain per-call form -- the same requests one at a
+    time, each submitted when the previous one completed and gridding its
+    catalogs from host memory.  Reported: pairs/s and triplets/s of the
+    served and plain forms (same requests, same kernels)."""
     from desi_b200 import serve
 
     cats, _ = serve.make_stream_mixed(n_requests, rate_hz=1.0)
@@ -668,8 +669,9 @@ def run_served(n_requests=300, load=0.7):
     rep["capacity_req_per_s"] = capacity
     rep["rate_hz"] = load * capacity
     rep["workload"] = (f"{n_requests} requests, Poisson at {load:.0%} of the closed-loop capacity; "
-                       "kinds 2iso/2ani/3iso; N log-uniform 1k-1M (3iso 1k-65k, box 1000); "
-                       "bins 20-50; dmax 40-120; box 250/500/1000; 4 slots")
+                       "kinds 2iso/2ani/3iso over a pool of catalog pairs (n_requests/4 per "
+                       "pool); N log-uniform 1k-1M (3iso 1k-65k, box 1000); bins 20-50; "
+                       "dmax 40-120; box 250/500/1000; 4 slots; resident grids reused")
     return rep
 
 

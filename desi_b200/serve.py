@@ -403,11 +403,13 @@ class PcfServer:
     def run_serial(self, reqs: list[Request]) -> dict:
         """The plain per-call form of the same requests: one at a time, in
         arrival order, each submitted when the previous one has completed
-        (no overlap on the device)."""
+        (no overlap on the device), and each gridding its catalogs from host
+        memory (no resident grids kept between requests)."""
         t0 = time.perf_counter()
         results = []
         for r in sorted(reqs, key=lambda r: r.arrival):
             results.append(self.submit(r).result())
+            self.drop_grids()
         t1 = time.perf_counter()
         order = sorted(reqs, key=lambda r: r.arrival)
         return self._report(order, results, t1 - t0)
@@ -434,37 +436,49 @@ class PcfServer:
 
 
 def make_stream_mixed(n_requests: int, rate_hz: float, seed: int = 6000, n_max: int = 1_000_000,
-                      n3_max: int = 65_536, box3: float = 1000.0,
+                      n3_max: int = 65_536, box3: float = 1000.0, pool: int | None = None,
                       catalogs: bool = True) -> tuple[dict, list[Request]]:
     """The served-stream workload: Poisson arrivals of mixed requests, kinds
-    2iso / 2ani / 3iso uniform, N log-uniform in [1e3, n_max] (3iso:
-    [1e3, n3_max]), bins uniform in 20..50, dmax uniform in [40, 120], box
-    250 / 500 / 1000 (dmax < L/2 holds for all), data clustered or uniform
-    by a seeded draw, unit weights, periodic or not by a seeded draw.  3iso
-    requests take the box of side box3 (1000): their cost grows as
-    N * (N dmax^3 / L^3)^2, and in the smaller boxes one 65k-point request
-    alone would take minutes.  catalogs=False returns the same requests
+    2iso / 2ani / 3iso uniform, bins uniform in 20..50, dmax uniform in
+    [40, 120], periodic or not by a seeded draw, over a seeded pool of
+    catalog pairs (data clustered or uniform by a seeded draw, uniform
+    randoms of the same size and box, unit weights) that the requests share,
+    as requests of a survey share its catalogs: N log-uniform in [1e3, n_max],
+    box 250 / 500 / 1000 (dmax < L/2 holds for all) for the 2-point pool;
+    N in [1e3, n3_max], box3 (1000) for the 3iso pool, because a 3iso
+    request costs N * (N dmax^3 / L^3)^2 and in the smaller boxes one
+    65k-point request alone would take minutes.  pool: catalog pairs per
+    pool (default n_requests / 4).  catalogs=False returns the same requests
     (other rate) without generating the catalogs again."""
     from . import catalog
     rng = np.random.default_rng(seed)
-    cats, reqs = {}, []
+    npool = pool or max(4, n_requests // 4)
+    cats = {}
+    specs = {}
+    for tag, cap in (("p", n_max), ("t", n3_max)):
+        for j in range(npool):
+            n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(cap)))))
+            box = box3 if tag == "t" else float(rng.choice([250.0, 500.0, 1000.0]))
+            clustered = bool(rng.integers(0, 2))
+            specs[(tag, j)] = (n, box, clustered)
+    if catalogs:
+        for (tag, j), (n, box, clustered) in specs.items():
+            s0 = seed + 10 * j + (5 if tag == "t" else 0)
+            gen = catalog.neyman_scott if clustered else catalog.uniform
+            cats[f"{tag}d{j}"] = (gen(n, box, seed=s0), box)
+            cats[f"{tag}r{j}"] = (catalog.uniform(n, box, seed=s0 + 1), box)
+    reqs = []
     t = 0.0
     for i in range(n_requests):
         kind = KINDS[rng.integers(0, 3)]
-        cap = n3_max if kind == "3iso" else n_max
-        n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(cap)))))
-        box = box3 if kind == "3iso" else float(rng.choice([250.0, 500.0, 1000.0]))
+        tag = "t" if kind == "3iso" else "p"
+        j = int(rng.integers(0, npool))
         bins = int(rng.integers(20, 51))
         dmax = float(rng.uniform(40.0, 120.0))
-        clustered = bool(rng.integers(0, 2))
         bpc = bool(rng.integers(0, 2))
-        dname, rname = f"d{i}", f"r{i}"
-        if catalogs:
-            gen = catalog.neyman_scott if clustered else catalog.uniform
-            cats[dname] = (gen(n, box, seed=seed + 2 * i), box)
-            cats[rname] = (catalog.uniform(n, box, seed=seed + 2 * i + 1), box)
         t += rng.exponential(1.0 / rate_hz)
-        reqs.append(Request(kind, dname, rname, bins, dmax, bpc=bpc, arrival=t, rid=i))
+        reqs.append(Request(kind, f"{tag}d{j}", f"{tag}r{j}", bins, dmax, bpc=bpc, arrival=t,
+                            rid=i))
     return cats, reqs
 
 

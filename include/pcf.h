@@ -195,8 +195,9 @@ pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d, const pcf_
 
 /*
  * The 3-point analogue of pcf_batch_pairs: one data catalog against n_rand
- * random catalogs, every isotropic triplet histogram in one persistent
- * launch over an (anchor, histogram) work queue.  Writes ddd (bins^3) once
+ * random catalogs, the isotropic triplet histograms in two persistent
+ * launches (DDD and every RRR_i; every DDR_i and DRR_i), each over one
+ * (anchor, histogram) work queue.  Writes ddd (bins^3) once
  * and, per random catalog i, rrr / ddr / drr at [i*bins^3 ..]; any of them
  * may be NULL to skip it.  Replaces the per-file loop of pcf_3iso /
  * pcf_3isoBPC over the -rd random directory (cuda/pcf3iso.cuh:101-112).
