@@ -354,11 +354,13 @@ def run_ours(args, rank, world, local_rank):
     fp32_peak = ctx.microbench(0)
     smem_peak = ctx.microbench(1)
     achieved = 8.0 * k_pairs / (k_ms * 1e-3) / 1e12
-    traffic = None
+    traffic, inst_per_pair = None, None
     prof = os.path.join(ROOT, "profiles", "k_pairs_c2_traffic.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+            pj = json.load(open(prof))
+            traffic = pj.get("dram_bytes_per_launch")
+            inst_per_pair = pj.get("thread_inst_per_pair")
         except Exception:
             traffic = None
     roofline = {
@@ -376,6 +378,17 @@ def run_ours(args, rank, world, local_rank):
         "recheck_fraction": sum(s["rechecks"] for s in stats) / max(pairs_step, 1),
         "kernel_share_of_step": k_ms / tot_ms if world == 1 else None,
     }
+    if inst_per_pair:
+        # the second ceiling: instruction issue.  Each SM issues one warp
+        # instruction per scheduler (4) per clock, 32 threads each; the
+        # kernel spends inst_per_pair thread instructions per in-range pair
+        # (ncu, profiles/k_pairs_c2.md)
+        mhz = clocks.get("sm_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        ceil = sms * 4 * 32 * mhz * 1e6 / inst_per_pair
+        roofline["issue_bound"] = {"thread_inst_per_pair": inst_per_pair,
+                                   "ceiling_pairs_per_s": ceil, "sm_mhz": mhz,
+                                   "frac": (k_pairs / (k_ms * 1e-3)) / ceil}
     out = {
         "metric": "pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
@@ -642,30 +655,43 @@ def run_served(n_requests=300, load=0.7):
         return reqs
 
     try:
-        warm = _requests(None)[:40]
+        # warm-up: every request once, so each slot's memory pool and
+        # page-locked buffers reach their working size (a first-use
+        # cudaMalloc waits for the whole device)
         srv.drop_grids()
-        srv.run_stream(warm)
-        srv.drop_grids()
-        closed = srv.run_stream(_requests(None))
-        closed.pop("results")
+        srv.run_stream(_requests(None))
+        passes = []
+        for _ in range(2):
+            srv.drop_grids()
+            r = srv.run_stream(_requests(None))
+            r.pop("results")
+            passes.append(r)
+        closed = min(passes, key=lambda r: r["wall_s"])
         capacity = n_requests / closed["wall_s"]
         srv.drop_grids()
         rep = srv.run_stream(_requests(load * capacity))
         rep.pop("results")
-        srv.drop_grids()
-        plain = srv.run_serial(_requests(None))
-        plain.pop("results")
+        plains = []
+        for _ in range(2):
+            srv.drop_grids()
+            r = srv.run_serial(_requests(None))
+            r.pop("results")
+            plains.append(r)
+        plain = min(plains, key=lambda r: r["wall_s"])
     finally:
         srv.close()
     rep["closed_loop"] = {k: closed[k] for k in ("wall_s", "pairs_per_s", "triplets_per_s",
                                                  "overlapping_starts")}
+    rep["closed_loop"]["passes_wall_s"] = [r["wall_s"] for r in passes]
+    rep["plain_passes_wall_s"] = [r["wall_s"] for r in plains]
     rep["plain_per_call"] = {k: plain[k] for k in ("wall_s", "pairs_per_s", "triplets_per_s",
                                                    "latency_ms")}
     rep["served_vs_plain"] = {
         "pairs_per_s": closed["pairs_per_s"] / plain["pairs_per_s"] if plain["pairs_per_s"] else None,
         "triplets_per_s": (closed["triplets_per_s"] / plain["triplets_per_s"]
                            if plain["triplets_per_s"] else None),
-        "note": "closed-loop served pass vs the same requests one at a time"}
+        "note": "best of two closed-loop served passes vs best of two passes of the same "
+                "requests one at a time"}
     rep["capacity_req_per_s"] = capacity
     rep["rate_hz"] = load * capacity
     rep["workload"] = (f"{n_requests} requests, Poisson at {load:.0%} of the closed-loop capacity; "

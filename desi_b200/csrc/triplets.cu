@@ -261,12 +261,8 @@ struct TripCta {
 // All triangles of anchor i of job A: pass 1 builds the anchor's
 // neighbour lists in shared memory (or, past their capacity, in this CTA's
 // global scratch), pass 2 counts the neighbour pairs.
-// COPY: work from a private copy of the job's arguments (the batched kernel,
-// whose arguments sit in shared memory, where every use would be a load
-// that the anchor's shared-memory stores keep the compiler from hoisting).
-template <bool MIXED, bool WEIGHTED, bool COPY = false>
-__device__ __forceinline__ void tri_anchor(const TripArgs &Ain, int i, TripCta &C) {
-    typename std::conditional<COPY, const TripArgs, const TripArgs &>::type A = Ain;
+template <bool MIXED, bool WEIGHTED>
+__device__ __forceinline__ void tri_anchor(const TripArgs &A, int i, TripCta &C) {
     const int bins = A.rXX.bins;
     const int nb3 = bins * bins * bins;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -551,71 +547,71 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets(const TripArgs A) {
     }
 }
 
+// The job table of a batched launch, passed as the kernel's parameter (so
+// job arguments are read from the parameter constant bank, as a single-job
+// launch reads its own; a table in global or shared memory ran the four
+// histograms of the 3iso step 8% slower).
+constexpr int kBatchJobs = 64;
+struct TripBatch {
+    TripArgs job[kBatchJobs];
+    int n_jobs;
+    long long n_anchors;
+    unsigned long long *counter;
+};
+
 // Several isotropic triplet histograms of one kind (XXX, or XXY) in one
 // persistent launch: the jobs' anchors form one queue (job after job); a CTA
 // that crosses into another job flushes its shared histogram into the
-// previous job's histogram and loads the next job's arguments.  (One kernel
-// for both kinds ran the four histograms of the 3iso step 7.5% slower than
-// four single-job launches: its code carried both paths.)
+// previous job's histogram.
 template <bool MIXED, bool WEIGHTED>
-__global__ void __launch_bounds__(kTThreads, 1) k_triplets_batch(const TripArgs *__restrict__ jobs,
-                                                                  int n_jobs, long long n_anchors,
-                                                                  unsigned long long *counter) {
+__global__ void __launch_bounds__(kTThreads, 1) k_triplets_batch(const __grid_constant__ TripBatch B) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ TripArgs s_job;
     __shared__ long long s_anchor;
-    __shared__ int s_cur, s_nJ, s_nK, s_unit;
+    __shared__ int s_nJ, s_nK, s_unit;
     __shared__ unsigned s_stop;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int bins = jobs[0].rXX.bins;
+    const TripArgs &J0 = B.job[0];
+    const int bins = J0.rXX.bins;
     const int nb3 = bins * bins * bins;
-    const bool in_smem = jobs[0].hist_in_smem != 0;
+    const bool in_smem = J0.hist_in_smem != 0;
     const size_t u_bytes = in_smem ? (((size_t)(nb3 + 32) * 4 + 15) & ~(size_t)15) : 0;
     TripCta C{reinterpret_cast<unsigned *>(smem), smem + u_bytes, &s_nJ, &s_nK, &s_unit, 0u, 0ull, 0ull};
     if (in_smem)
         for (int k = tid; k < nb3 + 32; k += kTThreads) C.U[k] = 0u;
-    if (tid == 0) s_cur = -1;
+    int cur = -1;  // the CTA's current job (uniform: every thread follows s_anchor)
     long long taken = 0;
     __syncthreads();
     for (;;) {
         if (tid == 0) {
-            s_anchor = (long long)atomicAdd(counter, 1ull);
+            s_anchor = (long long)atomicAdd(B.counter, 1ull);
             s_nJ = 0;
             s_nK = 0;
             s_unit = 0;
-            const TripArgs &j0 = jobs[0];
-            unsigned stop = (j0.ctrl && ctrl_load(j0.ctrl)) ? PCF_GAVE_UP_ABORT : 0u;
-            if (++taken > n_anchors + 1) stop |= PCF_GAVE_UP_CAP;
-            if (stop && j0.status) ctrl_store(j0.status, stop);
+            unsigned stop = (J0.ctrl && ctrl_load(J0.ctrl)) ? PCF_GAVE_UP_ABORT : 0u;
+            if (++taken > B.n_anchors + 1) stop |= PCF_GAVE_UP_CAP;
+            if (stop && J0.status) ctrl_store(J0.status, stop);
             s_stop = stop;
         }
         __syncthreads();
         const long long g = s_anchor;
-        if (g >= n_anchors || s_stop) break;
+        if (g >= B.n_anchors || s_stop) break;
         // the job of anchor g (a CTA's anchors only move forward in the queue)
-        int cur = s_cur;
-        if (cur < 0 || g >= s_job.anchor_begin + s_job.nX) {
+        if (cur < 0 || g >= B.job[cur].anchor_begin + B.job[cur].nX) {
             int j = cur < 0 ? 0 : cur;
-            while (j + 1 < n_jobs && g >= jobs[j + 1].anchor_begin) ++j;
+            while (j + 1 < B.n_jobs && g >= B.job[j + 1].anchor_begin) ++j;
             if (cur >= 0 && in_smem && C.since) {
-                flush_hist(C.U, nb3, s_job.g_count);
+                flush_hist(C.U, nb3, B.job[cur].g_count);
                 C.since = 0;
             }
-            __syncthreads();
-            static_assert(sizeof(TripArgs) % 4 == 0, "TripArgs words");
-            const int *src = reinterpret_cast<const int *>(jobs + j);
-            int *dst = reinterpret_cast<int *>(&s_job);
-            for (int q = tid; q < (int)(sizeof(TripArgs) / 4); q += kTThreads) dst[q] = src[q];
-            if (tid == 0) s_cur = j;
-            __syncthreads();
+            cur = j;
         }
-        const int i = (int)(g - s_job.anchor_begin);
-        tri_anchor<MIXED, WEIGHTED, true>(s_job, i, C);
+        const TripArgs &A = B.job[cur];
+        tri_anchor<MIXED, WEIGHTED>(A, (int)(g - A.anchor_begin), C);
         __syncthreads();
     }
-    if (in_smem && s_cur >= 0) {
+    if (in_smem && cur >= 0) {
         for (int k = tid; k < nb3; k += kTThreads)
-            if (C.U[k]) atomicAdd(s_job.g_count + k, (unsigned long long)C.U[k]);
+            if (C.U[k]) atomicAdd(B.job[cur].g_count + k, (unsigned long long)C.U[k]);
     }
     unsigned long long rr = C.n_rechk, nt = C.n_tri;
     for (int off = 16; off > 0; off >>= 1) {
@@ -623,8 +619,8 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_batch(const TripArgs 
         nt += __shfl_down_sync(kFull, nt, off);
     }
     if (lane == 0) {
-        if (rr) atomicAdd(jobs[0].g_stats + 0, rr);
-        if (nt) atomicAdd(jobs[0].g_stats + 2, nt);
+        if (rr) atomicAdd(J0.g_stats + 0, rr);
+        if (nt) atomicAdd(J0.g_stats + 2, nt);
     }
 }
 
@@ -825,7 +821,7 @@ static void trip_setup(pcf_ctx *ctx, const pcf_grid *X, const pcf_grid *Y, int P
     const int n3 = bins * bins * bins;
     // histogram + 32 dummy slots (the adds of 0 of lanes without a triangle)
     const size_t u_bytes = ((size_t)(n3 + 32) * 4 + 15) & ~(size_t)15;
-    const size_t smem_max = 227 * 1024 - 64 - sizeof(TripArgs);
+    const size_t smem_max = 227 * 1024 - 64;
     A.hist_in_smem = (!weighted && u_bytes <= 150 * 1024) ? 1 : 0;
     const size_t hist_b = A.hist_in_smem ? u_bytes : 0;
     const size_t ent = 16 + (weighted ? 4 : 0);
@@ -1049,27 +1045,22 @@ extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const
         A.g_wsum = wsum + (size_t)k * n3;
         A.g_stats = gstats;
     }
-    // one launch per kind: the XXX jobs, then the XXY jobs, each with the
-    // anchors of its jobs in one queue (its own counter)
-    std::vector<TripArgs> kargs[2];
-    long long kanchors[2] = {0, 0};
-    for (int k = 0; k < nj; ++k) {
-        const int m = jobs[k].y ? 1 : 0;
-        TripArgs a = args[k];
-        a.anchor_begin = kanchors[m];
-        kanchors[m] += a.nX;
-        kargs[m].push_back(a);
+    // launches per kind (the XXX jobs, then the XXY jobs), each over one
+    // anchor queue of up to kBatchJobs jobs with its own counter
+    std::vector<std::vector<TripArgs>> groups;
+    for (int m = 0; m < 2; ++m) {
+        std::vector<TripArgs> cur;
+        for (int k = 0; k < nj; ++k) {
+            if ((jobs[k].y ? 1 : 0) != m) continue;
+            cur.push_back(args[k]);
+            if ((int)cur.size() == kBatchJobs) {
+                groups.push_back(cur);
+                cur.clear();
+            }
+        }
+        if (!cur.empty()) groups.push_back(cur);
     }
-    DevBuf d_jobs;
-    d_jobs.pool = ctx->pool;
-    PCF_CU(ctx, d_jobs.ensure(sizeof(TripArgs) * nj));
-    TripArgs *dj = d_jobs.as<TripArgs>();
-    const size_t n0 = kargs[0].size();
-    if (n0) PCF_CU(ctx, cudaMemcpyAsync(dj, kargs[0].data(), sizeof(TripArgs) * n0, cudaMemcpyHostToDevice,
-                                        ctx->stream));
-    if (!kargs[1].empty())
-        PCF_CU(ctx, cudaMemcpyAsync(dj + n0, kargs[1].data(), sizeof(TripArgs) * kargs[1].size(),
-                                    cudaMemcpyHostToDevice, ctx->stream));
+    if (groups.size() > 8) return PCF_ERR_UNSUPPORTED;  // counters of the plan slot
     cudaEvent_t pe0 = nullptr, pe1 = nullptr;
     if (ctx->profile) {
         s = profile_events(ctx, &pe0, &pe1);
@@ -1078,13 +1069,23 @@ extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const
     }
     PCF_CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     unsigned long long *ctr = sl->d_counter.as<unsigned long long>();
-    for (int m = 0; m < 2; ++m) {
-        if (kargs[m].empty()) continue;
+    std::unique_ptr<TripBatch> tb(new TripBatch);
+    for (size_t q = 0; q < groups.size(); ++q) {
+        memset(tb.get(), 0, sizeof(TripBatch));
+        long long a0 = 0;
+        for (size_t k = 0; k < groups[q].size(); ++k) {
+            tb->job[k] = groups[q][k];
+            tb->job[k].anchor_begin = a0;
+            a0 += tb->job[k].nX;
+        }
+        tb->n_jobs = (int)groups[q].size();
+        tb->n_anchors = a0;
+        tb->counter = ctr + q;
+        const bool m = groups[q][0].mixed != 0;
         auto kfn = m ? (weighted ? k_triplets_batch<true, true> : k_triplets_batch<true, false>)
                      : (weighted ? k_triplets_batch<false, true> : k_triplets_batch<false, false>);
         PCF_CU(ctx, ensure_smem_limit(reinterpret_cast<const void *>(kfn), ctx->device, smem));
-        kfn<<<grid, kTThreads, smem, ctx->stream>>>(dj + (m ? n0 : 0), (int)kargs[m].size(), kanchors[m],
-                                                    ctr + m);
+        kfn<<<grid, kTThreads, smem, ctx->stream>>>(*tb);
         PCF_CU(ctx, cudaGetLastError());
         ++ctx->launches;
     }
