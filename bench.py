@@ -632,12 +632,12 @@ def run_served(n_requests=300, load=0.7):
     or uniform; periodic or not) through the continuous-batching server with
     4 slots, catalogs in page-locked host memory, grids kept resident within
     a pass (dropped before each pass).  Passes over the same requests: a
-    warm-up on the first 40 (discarded), one closed-loop pass (all submitted
-    at once) that measures capacity in requests/s, one pass with Poisson
+    warm-up pass (discarded), two closed-loop passes (all submitted at once)
+    whose better measures capacity in requests/s, one pass with Poisson
     arrivals at `load` times that capacity (latency p50 / p99 over all
-    requests), and the plain per-call form -- the same requests one at a
-    time, each submitted when the previous one completed and gridding its
-    catalogs from host memory.  Reported: pairs/s and triplets/s of the
+    requests), and two passes of the plain per-call form -- the same
+    requests one at a time, each submitted when the previous one completed
+    and gridding its catalogs from host memory.  Reported: pairs/s and triplets/s of the
     served and plain forms (same requests, same kernels)."""
     from desi_b200 import serve
 
