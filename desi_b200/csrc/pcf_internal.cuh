@@ -172,6 +172,9 @@ struct CellGrid {
     std::vector<TileDesc> tiles_half;
     DevBuf d_tiles_half;
     bool have_half = false;
+    // largest stencil population of a cell per (dmax, periodic), memoised
+    // for the triplet launches (a host pass over every cell and row)
+    mutable std::vector<std::pair<std::pair<float, bool>, int64_t>> stencil_memo;
     const std::vector<TileDesc> &tiles_for(int cap) const { return cap == 16 ? tiles_half : tiles; }
     const TileDesc *d_tiles_for(int cap) const {
         return (cap == 16 ? d_tiles_half : d_tiles).as<TileDesc>();

@@ -749,8 +749,18 @@ __global__ void k_trip_finalize(const unsigned long long *__restrict__ cnt,
 
 }  // namespace
 
-// Largest stencil population of any cell of g: bounds an anchor's lists.
-static int64_t max_stencil(const CellGrid &g, int P, const std::vector<RowDesc> &rows, bool bpc) {
+// Largest stencil population of any cell of g: bounds an anchor's lists
+// (memoised per cell structure, dmax and periodicity: the rows are fixed by
+// them and the structure's P).
+static int64_t max_stencil_scan(const CellGrid &g, int P, const std::vector<RowDesc> &rows, bool bpc);
+static int64_t max_stencil(const CellGrid &g, float dmax, const std::vector<RowDesc> &rows, bool bpc) {
+    for (const auto &m : g.stencil_memo)
+        if (m.first.first == dmax && m.first.second == bpc) return m.second;
+    const int64_t v = max_stencil_scan(g, g.P, rows, bpc);
+    g.stencil_memo.push_back({{dmax, bpc}, v});
+    return v;
+}
+static int64_t max_stencil_scan(const CellGrid &g, int P, const std::vector<RowDesc> &rows, bool bpc) {
     const std::vector<int> &cs = g.h_start;
     int64_t best = 0;
     for (int ix = 0; ix < P; ++ix)
@@ -877,8 +887,8 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
     trip_setup(ctx, X, Y, P, (int)plan.rows.size(), bins, dmax, flags, weighted, A, smem);
     const int n3 = bins * bins * bins;
     // overflow lists: bounded by the largest stencil population of any cell
-    const int64_t gmax = std::max<int64_t>(max_stencil(gx, P, plan.rows, bpc),
-                                           mixed ? max_stencil(gy, P, plan.rows, bpc) : 0) + 32;
+    const int64_t gmax = std::max<int64_t>(max_stencil(gx, dmax, plan.rows, bpc),
+                                           mixed ? max_stencil(gy, dmax, plan.rows, bpc) : 0) + 32;
     const int grid = ctx->sm_count;
     s = trip_overflow(ctx, gmax, mixed, weighted, grid, A);
     if (s != PCF_OK) return s;
@@ -1002,7 +1012,7 @@ extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const
     auto stencil_of = [&](const pcf_grid *g) {
         auto it = stencil.find(g);
         if (it != stencil.end()) return it->second;
-        return stencil[g] = max_stencil(*g->cells, P, plan.rows, bpc);
+        return stencil[g] = max_stencil(*g->cells, dmax, plan.rows, bpc);
     };
     for (int k = 0; k < nj; ++k) {
         size_t sm = 0;
