@@ -22,6 +22,7 @@
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <new>
 #include <string>
 #include <vector>
 #include <omp.h>
@@ -252,8 +253,17 @@ int ref3_analytic_ff(const float *pts, int n, float L, float size_node, float dm
         double ***xxx = new3(bins), ***xxy = new3(bins);
         {
             Quiet q;
-            NODE3P eng(bins, n, L, size_node, dmax, d, g.n);
-            eng.make_histo_analitic(xxy, xxx, eng.meshData());
+            // NODE3P never sets its member ll (size_box^2, 3PCFiso.h:52), which
+            // the fine DD's image passes read to prune node pairs
+            // (3PCFiso.h:1925-2039): built on the stack it holds whatever the
+            // stack held, and the fine DD changes from call to call.  Built in
+            // zero-filled storage, ll = 0 and the prune keeps every node pair,
+            // so each pair is decided by its own distance test.
+            alignas(NODE3P) unsigned char buf[sizeof(NODE3P)];
+            memset(buf, 0, sizeof(buf));
+            NODE3P *eng = new (buf) NODE3P(bins, n, L, size_node, dmax, d, g.n);
+            eng->make_histo_analitic(xxy, xxx, eng->meshData());
+            eng->~NODE3P();
         }
         free3(xxx, bins);
         free3(xxy, bins);

@@ -274,12 +274,16 @@ def test_ref_3iso_bpc_ddd_bitexact(n, dmax, kind, seed):
 
 def test_ref_3iso_analytic_ff_ref(tmp_path):
     """The analytic 3iso path of cpp/3PCFisotropic/BPC (make_histo_analitic,
-    3PCFiso.h:1484): its fine DD (600 000 bins) equals the oracle's FP32
-    emulation bit for bit, and the oracle's make_ff_av_ref on that DD and the
-    engine's RR reproduces the engine's ff_av_ref.dat (written with 12
-    significant digits).  (The engine's RRR/DDR refinement loop is commented
-    out, 3PCFiso.h:1623-1710, so the CUDA kernels are the only reference for
-    the refined histograms.)"""
+    3PCFiso.h:1484): the oracle's make_ff_av_ref on the engine's own fine DD
+    (600 000 bins) and RR reproduces the engine's ff_av_ref.dat (written
+    with 12 significant digits).  The fine DD itself agrees with the oracle's
+    FP32 emulation up to the engine's own fault: its Z-only image pass reads
+    dis_nod, which that loop never sets (3PCFiso.h:1794; the value left by an
+    earlier loop or the stack), and so now and then skips a node pair's image
+    pass, dropping a few dozen pairs.  So the engine never has more pairs
+    than the emulation in any bin and misses at most 0.1% of them.  (Its
+    RRR/DDR refinement loop is commented out, 3PCFiso.h:1623-1710, so the
+    CUDA kernels are the only reference for the refined histograms.)"""
     e = _ref_3iso()
     e.set_threads(os.cpu_count() or 4)
     D = _cat("uniform", 2048, 9)
@@ -291,7 +295,8 @@ def test_ref_3iso_analytic_ff_ref(tmp_path):
     dsf = float(np.float32(np.float32(nref) / np.float32(dmax)))
     emu = oracle.pairs(D, box=250.0, bins=nref, dmax=dmax, bpc=True, prec=oracle.REF32_CPU_BPC,
                        rule=0, ds_value=dsf)
-    assert np.array_equal(emu, dd)
+    assert np.all(dd <= emu)
+    assert emu.sum() - dd.sum() <= 1e-3 * emu.sum()
     got = oracle.ff_average_ref(dd, _cpu_rr(len(D), 250.0, dmax, nref, False), bins=bins,
                                 dmax=dmax)
     np.testing.assert_allclose(got, ffr, rtol=1e-10, atol=1e-10)
