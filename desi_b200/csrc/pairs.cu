@@ -172,8 +172,11 @@ struct Sink {
             red_s_limbs<128>(pred ? base + sb * (kLimbs * 128u) : dummy,
                              (unsigned long long)(pred ? wa : 0u) * wb);
         } else if (HM == H_WFIX || HM == H_WFIX4 || HM == H_WFIX2) {
-            red_s_limbs<4>(pred ? base + sb * (kLimbs * 4u) : dummy,
-                           (unsigned long long)(pred ? wa : 0u) * wb);
+            // per-warp copies end in a dummy region that is never read, so a
+            // lane without a pair adds its real product there: the product
+            // and its limbs are then the same for both copies of a
+            // both-kinds pass and computed once
+            red_s_limbs<4>(pred ? base + sb * (kLimbs * 4u) : dummy, (unsigned long long)wa * wb);
         } else if (HM == H_LANE) {
             if (WEIGHTED) {  // lane-private FP64 column: add 0 to slot 0 when !pred
                 double *h = lane_col + (pred ? (int)(sb - bias) : 0) * 32;
