@@ -48,6 +48,31 @@ def test_same_result_alone_and_in_the_mix():
         assert a.keys() == b.keys()
         for k in a:
             assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+    # the mix really ran requests at the same time on the device
+    assert rep["overlapping_starts"] > 0
+
+
+def test_mix_equals_the_oracle():
+    """The histograms of requests served in the mix equal the FP64 oracle
+    (unit weights: bit for bit), for the 2-point and 3-point kinds."""
+    import oracle
+    reqs = _requests()
+    mix = _server(4)
+    try:
+        cats = {k: v["points"] for k, v in mix.catalogs.items()}
+        rep = mix.run_stream(reqs)
+    finally:
+        mix.close()
+    for r, res in zip(reqs, rep["results"]):
+        D, R = cats[r.data], cats[r.rand]
+        kw = dict(box=200.0, bins=r.bins, dmax=r.dmax, bpc=r.bpc)
+        if r.kind == "3iso":
+            assert np.array_equal(res["DDD"], oracle.triplets_iso(D, **kw))
+            assert np.array_equal(res["DDR"], oracle.triplets_iso(D, R, **kw))
+        else:
+            ani = r.kind == "2ani"
+            assert np.array_equal(res["DD"], oracle.pairs(D, ani=ani, **kw))
+            assert np.array_equal(res["DR"], oracle.pairs(D, R, ani=ani, **kw))
 
 
 def test_admission_by_footprint_serialises_but_completes():
