@@ -2,15 +2,23 @@
 //
 // Replaces the host grid builder of the reference (open_files/make_nodos/add
 // in cuda/create_grid.cuh:35-139 and the flattening in cuda/main.cu:248-329,
-// an O(sum len^2) reallocation per insert followed by a serial copy): three
-// HBM-bound passes over the points --
-//   1. cell id + per-cell count (atomic), with out-of-box / weight checks,
-//   2. exclusive scan of the counts into the dense cell table,
-//   3. the destination of every point (a 4-byte scattered write),
-//   4. a gather in destination order that writes the cell-ordered copies
-//      (SoA planes, pair-packed blocks, integer weights) coalesced.
+// an O(sum len^2) reallocation per insert followed by a serial copy).
 // Cell id = (ix*P + iy)*P + iz with ix = (int)(x / cell), the reference's
 // binning (create_grid.cuh:131-133) clamped to [0, P-1].
+//
+// The build for catalogs of up to ~75M points is bucketed (runs of cells),
+// three streaming passes with shared-memory histograms and no per-point
+// global atomic:
+//   1. per CTA, a histogram of its slice of the input over the buckets, with
+//      the out-of-box / weight checks;
+//   2. a scan of the CTA x bucket matrix, then a scatter of the points into
+//      bucket order (each CTA into its own exact ranges);
+//   3. per bucket, a counting sort by cell in shared memory that writes the
+//      bucket's cell table and the cell-ordered copies (SoA planes,
+//      pair-packed blocks, integer weights) coalesced.
+// Larger catalogs take the per-point build: cell id + per-cell count
+// (atomic), a scan, the destination of every point (a scattered write) and a
+// gather in destination order.
 #include <algorithm>
 #include <atomic>
 #include <map>
@@ -79,39 +87,65 @@ namespace {
 
 constexpr int kScanItems = 1024;  // per block (256 threads x 4)
 
+// (int)(x / cell) with the division correctly rounded, as the reference's
+// host code computes it.  x * (1/cell) is within 2^-23 (relative) of the
+// exact quotient, i.e. within 6.2e-5 for quotients below 512 (P <= 320), and
+// the rounded quotient within half an ulp (3.1e-5) of it; so when the
+// product lies more than 2.4e-4 from every integer both truncate alike, and
+// only the rare quotients near a cell face take the division.  Negative,
+// infinite and NaN coordinates all take the division.
+__device__ __forceinline__ int cell_axis(float x, float cell, float rcell) {
+    const float q = x * rcell;
+    const int k = (int)q;
+    const float fr = q - (float)k;
+    if (fr > 2.4e-4f && fr < 1.0f - 2.4e-4f) return k;
+    return (int)__fdiv_rn(x, cell);
+}
+
+// Cell of a point: ix = (int)(x / cell) clamped to [0, P-1] per axis, the
+// reference's binning (create_grid.cuh:131-133).  Every pass of both builds
+// computes it with this one function, so a point's cell never differs
+// between passes.
+__device__ __forceinline__ int cell_of_point(const float4 &p, int P, float cell) {
+    const float rcell = 1.0f / cell;
+    int ix = cell_axis(p.x, cell, rcell), iy = cell_axis(p.y, cell, rcell), iz = cell_axis(p.z, cell, rcell);
+    ix = min(max(ix, 0), P - 1);
+    iy = min(max(iy, 0), P - 1);
+    iz = min(max(iz, 0), P - 1);
+    return (ix * P + iy) * P + iz;
+}
+
+// c / Q for c < K * Q with K <= 2^14: the float estimate is within 0.003 of
+// the quotient, so one correction step makes it exact.
+__device__ __forceinline__ int div_q(int c, int Q, float rq) {
+    int k = (int)((float)c * rq);
+    const int r = c - k * Q;
+    k += (r >= Q) - (r < 0);
+    return k;
+}
+
 // flags[0] |= 1: a coordinate outside [0, box); |= 2: a weight != 1; |= 4: a
 // negative or non-finite weight.  flags[1] = max |w| (float bits), flags[2] =
-// ~(bits of the smallest nonzero |w|) -- both by atomicMax, after a warp
-// reduction, so a launch makes one atomic per warp, not per point.
-__global__ void k_cell_ids(const float4 *__restrict__ pts, int64_t n, int P, float cell, float box,
-                           int *__restrict__ cid, int *__restrict__ rank,
-                           int *__restrict__ counts, int *__restrict__ flags) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned f = 0u, wmax = 0u, wminc = 0u;
-    if (i < n) {
-        const float4 p = pts[i];
-        const bool ok = (p.x >= 0.f) && (p.x < box) && (p.y >= 0.f) && (p.y < box) && (p.z >= 0.f) &&
-                        (p.z < box);
-        if (!ok) f |= 1u;
-        if (p.w != 1.0f) f |= 2u;
-        if (!(p.w >= 0.f) || !(p.w < INFINITY)) {
-            f |= 4u;
-        } else {
-            wmax = __float_as_uint(p.w);
-            if (p.w > 0.f) wminc = ~__float_as_uint(p.w);
-        }
-        int ix = (int)__fdiv_rn(p.x, cell), iy = (int)__fdiv_rn(p.y, cell),
-            iz = (int)__fdiv_rn(p.z, cell);
-        ix = min(max(ix, 0), P - 1);
-        iy = min(max(iy, 0), P - 1);
-        iz = min(max(iz, 0), P - 1);
-        const int c = (ix * P + iy) * P + iz;
-        cid[i] = c;
-        rank[i] = atomicAdd(&counts[c], 1);
+// ~(bits of the smallest nonzero |w|).
+__device__ __forceinline__ void point_flags(const float4 &p, float box, unsigned &f, unsigned &wmax,
+                                            unsigned &wminc) {
+    const bool ok = (p.x >= 0.f) && (p.x < box) && (p.y >= 0.f) && (p.y < box) && (p.z >= 0.f) &&
+                    (p.z < box);
+    if (!ok) f |= 1u;
+    if (p.w != 1.0f) f |= 2u;
+    if (!(p.w >= 0.f) || !(p.w < INFINITY)) {
+        f |= 4u;
+    } else {
+        wmax = max(wmax, __float_as_uint(p.w));
+        if (p.w > 0.f) wminc = max(wminc, ~__float_as_uint(p.w));
     }
-    // one update of the three flag words per block, and only when it changes
-    // them: every block targets the same three addresses, which would
-    // otherwise serialise millions of atomics in L2
+}
+
+// One update of the three flag words per block (after a warp reduction), and
+// only when it changes them: every block targets the same three addresses,
+// which would otherwise serialise millions of atomics in L2.  Called by every
+// thread of the block.
+__device__ __forceinline__ void flush_flags(unsigned f, unsigned wmax, unsigned wminc, int *flags) {
     f = __reduce_or_sync(0xffffffffu, f);
     wmax = __reduce_max_sync(0xffffffffu, wmax);
     wminc = __reduce_max_sync(0xffffffffu, wminc);
@@ -131,6 +165,21 @@ __global__ void k_cell_ids(const float4 *__restrict__ pts, int64_t n, int P, flo
         if (s_max > vf[1]) atomicMax(uf + 1, s_max);
         if (s_minc > vf[2]) atomicMax(uf + 2, s_minc);
     }
+}
+
+__global__ void k_cell_ids(const float4 *__restrict__ pts, int64_t n, int P, float cell, float box,
+                           int *__restrict__ cid, int *__restrict__ rank,
+                           int *__restrict__ counts, int *__restrict__ flags) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned f = 0u, wmax = 0u, wminc = 0u;
+    if (i < n) {
+        const float4 p = pts[i];
+        point_flags(p, box, f, wmax, wminc);
+        const int c = cell_of_point(p, P, cell);
+        cid[i] = c;
+        rank[i] = atomicAdd(&counts[c], 1);
+    }
+    flush_flags(f, wmax, wminc, flags);
 }
 
 // Exclusive scan of one 1024-element chunk per block; the chunk total goes to
@@ -266,6 +315,248 @@ __global__ void k_tile_emit(const int *__restrict__ start, const int *__restrict
     }
 }
 
+// ---- bucketed build -------------------------------------------------------
+// Buckets are runs of Q consecutive cells.  The count pass gives every CTA a
+// shared histogram of its own contiguous slice of the input; one scan of the
+// CTA x bucket matrix (bucket-major) then hands each CTA a private, exact
+// write range per bucket, so the scatter pass places points with shared
+// atomics only (no per-point global atomic: those run at ~1e11/s on this
+// part, a third of a millisecond for 33.5M points).  Each CTA's range in a
+// bucket fills front to back, so the partially written sectors sit at the
+// ranges' fronts in L2 and reach DRAM whole.  The sort pass then takes one
+// bucket per CTA: a shared counting sort by cell, the cell table of the
+// bucket's cells, and the cell-ordered copies written coalesced.
+constexpr int kBktThreads = 1024;      // count and scatter CTAs, one per SM
+constexpr int kBktTarget = 6144;       // mean points per bucket
+constexpr int kBktCap = 12288;         // most points a bucket sorts in shared memory
+constexpr int kBktMaxCells = 4096;     // cells per bucket (the sort's counters)
+constexpr int kBktMaxBuckets = 12288;  // buckets (the count and scatter histograms)
+constexpr int kSortThreads = 1024;
+constexpr int kBktUnroll = 8;          // loads in flight per thread in every pass
+constexpr size_t kSortSmem = (size_t)kBktCap * sizeof(float4) + (size_t)kBktMaxCells * sizeof(int);
+
+__device__ __forceinline__ unsigned weight_q(float w, int emin) {
+    const unsigned b = __float_as_uint(w) & 0x7FFFFFFFu;  // +0 and -0 give 0
+    return b ? ((b & 0x7FFFFFu) | 0x800000u) << ((int)(b >> 23) - emin) : 0u;
+}
+
+// This point's half of pair block d/2 (components d & 1 of its two float4s).
+__device__ __forceinline__ void pk_put(float4 *pk, int64_t d, const float4 &p) {
+    const int h = (int)(d & 1);
+    float *a = reinterpret_cast<float *>(pk + (d - h));
+    float *b = a + 4;
+    a[h] = p.x;
+    a[2 + h] = p.y;
+    b[h] = p.z;
+    b[2 + h] = p.w;
+}
+
+__global__ void __launch_bounds__(kBktThreads) k_bkt_count(const float4 *__restrict__ pts, int64_t n,
+                                                           int64_t span, int P, float cell, float box,
+                                                           int Q, float rq, int K, int *__restrict__ M,
+                                                           int *__restrict__ flags) {
+    extern __shared__ int hist[];
+    for (int k = threadIdx.x; k < K; k += blockDim.x) hist[k] = 0;
+    __syncthreads();
+    const int64_t i0 = (int64_t)blockIdx.x * span, i1 = min(n, i0 + span);
+    const int64_t T = blockDim.x;
+    unsigned f = 0u, wmax = 0u, wminc = 0u;
+    int64_t i = i0 + threadIdx.x;
+    for (; i + (kBktUnroll - 1) * T < i1; i += kBktUnroll * T) {  // kBktUnroll loads in flight per thread
+        float4 p[kBktUnroll];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) p[u] = pts[i + u * T];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) {
+            point_flags(p[u], box, f, wmax, wminc);
+            atomicAdd(&hist[div_q(cell_of_point(p[u], P, cell), Q, rq)], 1);
+        }
+    }
+    for (; i < i1; i += T) {
+        const float4 p = pts[i];
+        point_flags(p, box, f, wmax, wminc);
+        atomicAdd(&hist[div_q(cell_of_point(p, P, cell), Q, rq)], 1);
+    }
+    flush_flags(f, wmax, wminc, flags);  // ends with the block's histogram complete
+    const int64_t G = gridDim.x;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) M[k * G + blockIdx.x] = hist[k];
+}
+
+__global__ void __launch_bounds__(kBktThreads) k_bkt_scatter(const float4 *__restrict__ pts, int64_t n,
+                                                             int64_t span, int P, float cell, int Q,
+                                                             float rq, int K, const int *__restrict__ base,
+                                                             float4 *__restrict__ S) {
+    extern __shared__ int cur[];
+    const int64_t G = gridDim.x;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) cur[k] = base[k * G + blockIdx.x];
+    __syncthreads();
+    const int64_t i0 = (int64_t)blockIdx.x * span, i1 = min(n, i0 + span);
+    const int64_t T = blockDim.x;
+    int64_t i = i0 + threadIdx.x;
+    for (; i + (kBktUnroll - 1) * T < i1; i += kBktUnroll * T) {
+        float4 p[kBktUnroll];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) p[u] = pts[i + u * T];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) S[atomicAdd(&cur[div_q(cell_of_point(p[u], P, cell), Q, rq)], 1)] = p[u];
+    }
+    for (; i < i1; i += T) {
+        const float4 p = pts[i];
+        S[atomicAdd(&cur[div_q(cell_of_point(p, P, cell), Q, rq)], 1)] = p;
+    }
+}
+
+// Exclusive scan of a[0..q) in place, q <= 4 * blockDim.x, blockDim.x a
+// multiple of 32 and at most 1024.  Called by every thread of the block.
+__device__ void block_excl_scan4(int *a, int q, int *wsum) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    int v[4], s = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int i = 4 * t + u;
+        v[u] = i < q ? a[i] : 0;
+        s += v[u];
+    }
+    int x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        const int ws = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+        int z = ws;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += y;
+        }
+        wsum[lane] = z - ws;
+    }
+    __syncthreads();
+    int e = wsum[w] + x - s;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int i = 4 * t + u;
+        if (i < q) a[i] = e;
+        e += v[u];
+    }
+    __syncthreads();
+}
+
+// One bucket per CTA: count its points per cell, write the bucket's part of
+// the cell table, place the points in cell order in shared memory and write
+// the copies coalesced.  A bucket above kBktCap points (a very dense region)
+// takes the same counting sort with the copies written point by point.
+__global__ void __launch_bounds__(kSortThreads) k_bkt_sort(
+    const float4 *__restrict__ S, const int *__restrict__ base, int G, int K, int n, int P, float cell,
+    int Q, int ncell, int *__restrict__ cell_start, float *__restrict__ soa, size_t plane,
+    float4 *__restrict__ pk, unsigned *__restrict__ qw, const int *__restrict__ flags) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float4 *ord = reinterpret_cast<float4 *>(smem);
+    int *cnt = reinterpret_cast<int *>(smem + (size_t)kBktCap * sizeof(float4));
+    __shared__ int wsum[32];
+    const int k = blockIdx.x;
+    const int b0 = base[(int64_t)k * G];
+    const int b1 = k + 1 < K ? base[(int64_t)(k + 1) * G] : n;
+    const int m = b1 - b0;
+    const int c0 = k * Q, q = min(Q, ncell - c0);
+    for (int i = threadIdx.x; i < q; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    const int T = blockDim.x;
+    for (int j = threadIdx.x; j < m; j += kBktUnroll * T) {
+        float4 p[kBktUnroll];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u)
+            if (j + u * T < m) p[u] = S[b0 + j + u * T];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) {
+            if (j + u * T >= m) break;
+            const int lc = cell_of_point(p[u], P, cell) - c0;
+            if ((unsigned)lc < (unsigned)q) atomicAdd(&cnt[lc], 1);
+        }
+    }
+    __syncthreads();
+    block_excl_scan4(cnt, q, wsum);
+    for (int i = threadIdx.x; i < q; i += blockDim.x) cell_start[c0 + i] = b0 + cnt[i];
+    if (k == K - 1 && threadIdx.x == 0) cell_start[ncell] = n;
+    __syncthreads();  // the counters become placement cursors below
+    int emin, emax;
+    const unsigned *uf = reinterpret_cast<const unsigned *>(flags);
+    const bool fix = weight_fix_range(uf[0], uf[1], uf[2], &emin, &emax);
+    if (m <= kBktCap) {
+        for (int j = threadIdx.x; j < m; j += kBktUnroll * T) {  // second read of the bucket: L2
+            float4 p[kBktUnroll];
+#pragma unroll
+            for (int u = 0; u < kBktUnroll; ++u)
+                if (j + u * T < m) p[u] = S[b0 + j + u * T];
+#pragma unroll
+            for (int u = 0; u < kBktUnroll; ++u) {
+                if (j + u * T >= m) break;
+                const int lc = cell_of_point(p[u], P, cell) - c0;
+                if ((unsigned)lc < (unsigned)q) ord[atomicAdd(&cnt[lc], 1)] = p[u];
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < m; t += T) {
+            const float4 p = ord[t];
+            const int64_t d = (int64_t)b0 + t;
+            if (soa) {
+                soa[d] = p.x;
+                soa[plane + d] = p.y;
+                soa[2 * plane + d] = p.z;
+                soa[3 * plane + d] = p.w;
+            }
+            if (qw) qw[d] = fix ? weight_q(p.w, emin) : 0u;
+            if (!(d & 1)) {
+                if (t + 1 < m) {  // block d/2 lies inside the bucket
+                    const float4 o = ord[t + 1];
+                    pk[d] = make_float4(p.x, o.x, p.y, o.y);
+                    pk[d + 1] = make_float4(p.z, o.z, p.w, o.w);
+                } else if (d + 1 >= n) {  // the catalog's last point, without a partner
+                    pk[d] = make_float4(p.x, 0.f, p.y, 0.f);
+                    pk[d + 1] = make_float4(p.z, 0.f, p.w, 0.f);
+                } else {
+                    pk_put(pk, d, p);  // the partner opens the next bucket
+                }
+            } else if (t == 0) {
+                pk_put(pk, d, p);  // the partner closes an earlier bucket
+            }
+        }
+    } else {
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            const float4 p = S[b0 + j];
+            const int lc = cell_of_point(p, P, cell) - c0;
+            if ((unsigned)lc >= (unsigned)q) continue;
+            const int64_t d = (int64_t)b0 + atomicAdd(&cnt[lc], 1);
+            if (soa) {
+                soa[d] = p.x;
+                soa[plane + d] = p.y;
+                soa[2 * plane + d] = p.z;
+                soa[3 * plane + d] = p.w;
+            }
+            if (qw) qw[d] = fix ? weight_q(p.w, emin) : 0u;
+            pk_put(pk, d, p);  // the partner slot of an odd n's last block is zeroed beforehand
+        }
+    }
+}
+
+// Zero the padding past the catalog: the SoA planes' and integer weights'
+// entries n .. plane - 1 and the pair blocks from the one holding point n
+// (an odd n leaves that block's second half empty).
+__global__ void k_tails(float *__restrict__ soa, size_t plane, int64_t n, float4 *__restrict__ pk,
+                        int64_t pk_from, int64_t pk_to, unsigned *__restrict__ qw) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < (int64_t)plane - n) {
+        if (soa)
+            for (int a = 0; a < 4; ++a) soa[a * plane + n + t] = 0.f;
+        if (qw) qw[n + t] = 0u;
+    }
+    if (pk_from + t < pk_to) pk[pk_from + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 }  // namespace
 
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
@@ -279,6 +570,58 @@ int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box
     k_perm<<<blocks, thr, 0, st>>>(n, cid, rank, cell_start, perm);
     k_gather<<<blocks, thr, 0, st>>>(raw, n, perm, soa, plane, pk, qw, flags);
     return launches + 2;
+}
+
+bool grid_bucket_plan(int64_t n, int P, int G, int *Q, int *K) {
+    const int64_t ncell = (int64_t)P * P * P;
+    if (n < 1 || n > ((int64_t)1 << 30)) return false;
+    // mean bucket near kBktTarget points, at least two buckets per CTA of the
+    // count pass where the cells allow (a small catalog still fills the GPU
+    // in the sort pass), at most kBktMaxCells cells per bucket
+    int64_t k = std::max<int64_t>((n + kBktTarget - 1) / kBktTarget, 2 * (int64_t)G);
+    k = std::max<int64_t>(k, (ncell + kBktMaxCells - 1) / kBktMaxCells);
+    k = std::max<int64_t>(1, std::min<int64_t>(k, ncell));
+    const int64_t q = (ncell + k - 1) / k;
+    k = (ncell + q - 1) / q;
+    if (k > kBktMaxBuckets || q > kBktMaxCells) return false;
+    *Q = (int)q;
+    *K = (int)k;
+    return true;
+}
+
+size_t grid_bucket_scratch_ints(int G, int K) { return (size_t)G * K + 1; }
+
+cudaError_t grid_bucket_attrs(int device, int K) {
+    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(k_bkt_count), device,
+                                      sizeof(int) * (size_t)K);
+    if (e == cudaSuccess)
+        e = ensure_smem_limit(reinterpret_cast<const void *>(k_bkt_scatter), device, sizeof(int) * (size_t)K);
+    if (e == cudaSuccess)
+        e = ensure_smem_limit(reinterpret_cast<const void *>(k_bkt_sort), device, kSortSmem);
+    return e;
+}
+
+int launch_grid_build_buckets(const float4 *raw, int64_t n, int P, float cell, float box, int G, int Q,
+                              int K, int *M, int *Mx, int *scan_tmp, float4 *S, int *cell_start,
+                              float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
+                              cudaStream_t st) {
+    const int ncell = P * P * P;
+    const int64_t span = (n + G - 1) / G;
+    const size_t hs = sizeof(int) * (size_t)K;
+    const float rq = 1.0f / (float)Q;
+    k_bkt_count<<<G, kBktThreads, hs, st>>>(raw, n, span, P, cell, box, Q, rq, K, M, flags);
+    int launches = 1 + scan_exclusive(M, Mx, (int64_t)G * K, scan_tmp, st);
+    k_bkt_scatter<<<G, kBktThreads, hs, st>>>(raw, n, span, P, cell, Q, rq, K, Mx, S);
+    k_bkt_sort<<<K, kSortThreads, kSortSmem, st>>>(S, Mx, G, K, (int)n, P, cell, Q, ncell, cell_start, soa,
+                                                  plane, pk, qw, flags);
+    return launches + 2;
+}
+
+int launch_grid_tails(float *soa, size_t plane, int64_t n, float4 *pk, unsigned *qw, cudaStream_t st) {
+    const int64_t from = 2 * (n / 2), to = 2 * (int64_t)pk_blocks(n);
+    const int64_t m = std::max<int64_t>((int64_t)plane - n, to - from);
+    k_tails<<<(unsigned)((m + 127) / 128), 128, 0, st>>>(soa, plane, n, pk, from, to, qw);
+    return 1;
 }
 
 void set_weight_range(pcf_grid *g, const unsigned hf[3]) {
@@ -353,24 +696,30 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     cudaStream_t st = ctx->stream;
     cg->plane = ((size_t)n + kSoaPad + 3) & ~(size_t)3;
     PCF_CU(ctx, cg->soa.ensure(sizeof(float) * cg->plane * 4));
-    PCF_CU(ctx, cudaMemsetAsync(cg->soa.p, 0, sizeof(float) * cg->plane * 4, ctx->stream));
     cg->pk.pool = cg->qw.pool = g->pool;
     PCF_CU(ctx, cg->pk.ensure(32 * pk_blocks(n)));
-    PCF_CU(ctx, cudaMemsetAsync(cg->pk.p, 0, 32 * pk_blocks(n), ctx->stream));
     PCF_CU(ctx, cg->qw.ensure(sizeof(unsigned) * cg->plane));
-    PCF_CU(ctx, cudaMemsetAsync(cg->qw.p, 0, sizeof(unsigned) * cg->plane, ctx->stream));
     PCF_CU(ctx, cg->cell_start.ensure(sizeof(int) * (size_t)(ncell + 1)));
-    // scratch: cid, rank (n each); counts (ncell + 1); scan tmp.
-    PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(int) * (size_t)n * 3));
-    PCF_CU(ctx, ctx->scratch_b.ensure(sizeof(int) * (size_t)(ncell + 1)));
-    PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(int) * (size_t)((ncell + 1) / 256 + 256)));
+    int Q = 0, K = 0;
+    const int G = ctx->sm_count;
+    const bool buckets = grid_bucket_plan(n, P, G, &Q, &K);
+    const size_t mat = buckets ? grid_bucket_scratch_ints(G, K) : 0;
+    if (buckets) {
+        // scratch: the bucketed copy of the catalog (n float4); the CTA x
+        // bucket counts and their scan; scan tmp.
+        PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(float4) * (size_t)n));
+        PCF_CU(ctx, ctx->scratch_b.ensure(sizeof(int) * 2 * mat));
+        PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(int) * (mat / 256 + 256)));
+        PCF_CU(ctx, grid_bucket_attrs(ctx->device, K));
+    } else {
+        // scratch: cid, rank, perm (n each); counts (ncell + 1); scan tmp.
+        PCF_CU(ctx, ctx->scratch_a.ensure(sizeof(int) * (size_t)n * 3));
+        PCF_CU(ctx, ctx->scratch_b.ensure(sizeof(int) * (size_t)(ncell + 1)));
+        PCF_CU(ctx, ctx->scratch_c.ensure(sizeof(int) * (size_t)((ncell + 1) / 256 + 256)));
+    }
     PCF_CU(ctx, ctx->d_flag.ensure(sizeof(int) * 4));
-    int *cid = ctx->scratch_a.as<int>();
-    int *rank = cid + n;
-    int *perm = rank + n;
-    int *counts = ctx->scratch_b.as<int>();
     int *flags = ctx->d_flag.as<int>();
-    PCF_CU(ctx, cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)(ncell + 1), st));
+    if (!buckets) PCF_CU(ctx, cudaMemsetAsync(ctx->scratch_b.p, 0, sizeof(int) * (size_t)(ncell + 1), st));
     PCF_CU(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * 3, st));
     cudaEvent_t pg0 = nullptr, pg1 = nullptr;  // kernel-time log of grid builds
     if (ctx->profile) {
@@ -386,10 +735,21 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
         ctx->prof_grid_points += n;
         PCF_CU(ctx, cudaEventRecord(pg0, st));
     }
-    ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, rank, perm,
-                                       counts, cg->cell_start.as<int>(), ctx->scratch_c.as<int>(),
-                                       cg->soa.as<float>(), cg->plane, cg->pk.as<float4>(),
-                                       cg->qw.as<unsigned>(), flags, st);
+    ctx->launches += launch_grid_tails(cg->soa.as<float>(), cg->plane, n, cg->pk.as<float4>(),
+                                       cg->qw.as<unsigned>(), st);
+    if (buckets) {
+        int *M = ctx->scratch_b.as<int>();
+        ctx->launches += launch_grid_build_buckets(
+            g->raw.as<float4>(), n, P, cg->cell, g->box, G, Q, K, M, M + mat, ctx->scratch_c.as<int>(),
+            ctx->scratch_a.as<float4>(), cg->cell_start.as<int>(), cg->soa.as<float>(), cg->plane,
+            cg->pk.as<float4>(), cg->qw.as<unsigned>(), flags, st);
+    } else {
+        int *cid = ctx->scratch_a.as<int>();
+        ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, cid + n,
+                                           cid + 2 * n, ctx->scratch_b.as<int>(), cg->cell_start.as<int>(),
+                                           ctx->scratch_c.as<int>(), cg->soa.as<float>(), cg->plane,
+                                           cg->pk.as<float4>(), cg->qw.as<unsigned>(), flags, st);
+    }
     PCF_CU(ctx, cudaGetLastError());
     if (pg1) PCF_CU(ctx, cudaEventRecord(pg1, st));
     // cell table and flags come back through the context's page-locked

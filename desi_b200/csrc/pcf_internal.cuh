@@ -401,6 +401,22 @@ unsigned reference_pair_rule(bool ani, bool bpc, bool cross);
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
                       int *rank, int *perm, int *counts, int *cell_start, int *scan_tmp, float *soa,
                       size_t plane, float4 *pk, unsigned *qw, int *flags, cudaStream_t st);
+// Bucketed counting sort (the build for catalogs of up to ~75M points): Q
+// cells per bucket, K buckets, G CTAs in the count and scatter passes; false
+// when the catalog needs more buckets than the shared histograms hold (the
+// per-point build above then runs).
+bool grid_bucket_plan(int64_t n, int P, int G, int *Q, int *K);
+// ints of each of the two CTA x bucket matrices (G CTAs)
+size_t grid_bucket_scratch_ints(int G, int K);
+cudaError_t grid_bucket_attrs(int device, int K);
+// M, Mx: grid_bucket_scratch_ints each; S: n float4 of scratch; flags zeroed.
+int launch_grid_build_buckets(const float4 *raw, int64_t n, int P, float cell, float box, int G, int Q,
+                              int K, int *M, int *Mx, int *scan_tmp, float4 *S, int *cell_start,
+                              float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
+                              cudaStream_t st);
+// Zeroes the padding past point n of the SoA planes, integer weights and pair
+// blocks (the builds write entries 0 .. n-1); runs before the build.
+int launch_grid_tails(float *soa, size_t plane, int64_t n, float4 *pk, unsigned *qw, cudaStream_t st);
 // Host side of the weight scan (flags[0..2] as written by the grid build):
 // fills g's weight-range fields, including the integer-weight scale.
 void set_weight_range(pcf_grid *g, const unsigned flags[3]);

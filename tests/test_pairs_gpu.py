@@ -140,6 +140,49 @@ def test_grid_is_a_permutation_in_cell_order(ctx):
     assert np.all(np.diff(cid) >= 0)
 
 
+def _cell_table(D, box, P):
+    cell = np.float32(box) / np.float32(P)
+    idx = np.clip((D[:, :3] / cell).astype(np.int64), 0, P - 1)
+    cid = (idx[:, 0] * P + idx[:, 1]) * P + idx[:, 2]
+    return np.concatenate([[0], np.cumsum(np.bincount(cid, minlength=P ** 3))]), cid
+
+
+@pytest.mark.parametrize("case", ["odd_small", "one_cell", "dense_cell", "large"])
+def test_grid_build_cases(ctx, case):
+    """The bucketed build against a host counting sort: the cell table, the
+    multiset of points in cell order, and (through the pair-packed blocks
+    and integer weights) DD against the oracle.  odd_small: an odd catalog
+    in many small buckets (pair blocks straddle buckets); one_cell: every
+    point in a single bucket larger than a shared-memory sort holds;
+    dense_cell: 20000 points inside one cell beside a uniform background;
+    large: 2M points in 64^3 cells."""
+    rng = np.random.default_rng(5)
+    box = 100.0
+    if case == "odd_small":
+        D, P = catalog.uniform(3001, box, seed=3, weights="uniform"), 9
+    elif case == "one_cell":
+        D, P = catalog.uniform(14001, box, seed=7, weights="uniform"), 1
+    elif case == "dense_cell":
+        bg = catalog.uniform(5001, box, seed=4, weights="uniform")
+        dense = bg[:1].repeat(20000, 0)
+        dense[:, :3] = rng.uniform(40.5, 49.5, size=(20000, 3)).astype(np.float32)
+        D, P = np.ascontiguousarray(np.concatenate([bg, dense])), 10
+    else:
+        D, P = catalog.uniform(1 << 21, box, seed=6), 64
+    g = ctx.grid(D, box, partitions=P)
+    pts, cs = g.download()
+    want_cs, cid = _cell_table(D, box, P)
+    assert np.array_equal(cs, want_cs)
+    key = lambda a: np.lexsort(a.T)
+    assert np.array_equal(pts[key(pts)], D[key(D)])
+    _, cid_out = _cell_table(pts, box, P)
+    assert np.all(np.diff(cid_out) >= 0)
+    if case != "large":
+        got = ctx.count_pairs(g, None, bins=12, dmax=30.0)
+        want = oracle.pairs(D, None, box=box, bins=12, dmax=30.0)
+        np.testing.assert_allclose(got, want, rtol=RTOL_W, atol=0)
+
+
 def _weighted(pts, rng, kind):
     out = pts.copy()
     n = len(out)
