@@ -457,19 +457,22 @@ def run_grid_build(ctx, torch, n=1 << 25, box=1000.0, partitions=128, reps=3):
     del pts
     torch.cuda.empty_cache()
     gbs = GRID_BYTES_PER_POINT * npts / (ms * 1e-3) / 1e9
-    peak = measured_hbm_gbs()
+    peak, peak_source = measured_hbm_gbs()
     return {"workload": f"{n} uniform points, box {box}, {partitions}^3 cells", "builds": builds,
             "ms_per_build": ms / max(builds, 1), "bytes_per_point": GRID_BYTES_PER_POINT,
             "achieved_gbs": round(gbs, 1), "peak_gbs": peak,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy, read + write)",
+            "peak_source": peak_source,
             "frac": round(gbs / peak, 4) if peak else None}
 
 
 def measured_hbm_gbs():
+    """(GB/s, source): the driver-measured copy bandwidth when
+    MEASURED_PEAKS.json is present, else the pool's earlier copy measurement."""
     try:
-        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        v = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return v, "MEASURED_PEAKS.json hbm_gbs (copy, read + write)"
     except Exception:
-        return 6650.0  # the pool's earlier copy measurement
+        return 6650.0, "fallback: 6.65 TB/s, an earlier copy measurement on this pool (MEASURED_PEAKS.json absent)"
 
 
 def _timed_ms(torch, stream, fn, reps=1):

@@ -6,7 +6,7 @@
 // Cell id = (ix*P + iy)*P + iz with ix = (int)(x / cell), the reference's
 // binning (create_grid.cuh:131-133) clamped to [0, P-1].
 //
-// The build for catalogs of up to ~75M points is bucketed (runs of cells),
+// The build for catalogs of up to ~134M points is bucketed (runs of cells),
 // three streaming passes with shared-memory histograms and no per-point
 // global atomic:
 //   1. per CTA, a histogram of its slice of the input over the buckets, with
@@ -25,6 +25,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+
+#include <cooperative_groups.h>
 
 #include "pcf_internal.cuh"
 
@@ -316,24 +318,35 @@ __global__ void k_tile_emit(const int *__restrict__ start, const int *__restrict
 }
 
 // ---- bucketed build -------------------------------------------------------
-// Buckets are runs of Q consecutive cells.  The count pass gives every CTA a
-// shared histogram of its own contiguous slice of the input; one scan of the
-// CTA x bucket matrix (bucket-major) then hands each CTA a private, exact
-// write range per bucket, so the scatter pass places points with shared
-// atomics only (no per-point global atomic: those run at ~1e11/s on this
-// part, a third of a millisecond for 33.5M points).  Each CTA's range in a
-// bucket fills front to back, so the partially written sectors sit at the
-// ranges' fronts in L2 and reach DRAM whole.  The sort pass then takes one
-// bucket per CTA: a shared counting sort by cell, the cell table of the
-// bucket's cells, and the cell-ordered copies written coalesced.
-constexpr int kBktThreads = 1024;      // count and scatter CTAs, one per SM
-constexpr int kBktTarget = 6144;       // mean points per bucket
-constexpr int kBktCap = 12288;         // most points a bucket sorts in shared memory
-constexpr int kBktMaxCells = 4096;     // cells per bucket (the sort's counters)
-constexpr int kBktMaxBuckets = 12288;  // buckets (the count and scatter histograms)
+// Buckets are runs of Q consecutive cells (at most kBktMaxCells), about
+// kBktTarget points each.  The count pass gives every CTA a shared histogram
+// of its own contiguous slice of the input; one scan of the CTA x bucket
+// matrix (bucket-major) hands each CTA a private, exact write range per
+// bucket.  The scatter pass then sorts each 8192-point chunk of its slice by
+// bucket in shared memory and writes every bucket's run of the chunk to the
+// front of its range, so stores leave as coalesced runs instead of one random
+// 16-byte store per point (those ran at ~6e10/s: partial sectors scattered
+// over the whole scratch array).  No pass makes a per-point global atomic.
+// The sort pass takes one bucket per cluster of kCluster CTAs: the CTAs count
+// their shares of the bucket per cell, merge the counts through distributed
+// shared memory into the bucket's cell table, place every point into the
+// shared memory of the CTA that owns its destination, and write the
+// cell-ordered copies (SoA planes, pair-packed blocks, integer weights)
+// coalesced.
+constexpr int kBktThreads = 1024;                   // count and scatter CTAs, one per SM
+constexpr int kBktUnroll = 8;                       // loads in flight per thread in every pass
+constexpr int kChunk = kBktThreads * kBktUnroll;    // points per scatter round
+constexpr int kBktTarget = 32768;                   // mean points per bucket
+constexpr int kBktMinBuckets = 128;                 // buckets of a small catalog (sort-pass parallelism)
+constexpr int kBktMaxCells = 4096;                  // cells per bucket (the sort's counters)
+constexpr int kBktMaxBuckets = 4096;                // buckets (count / scatter shared arrays)
+constexpr int kCluster = 4;                         // CTAs sorting one bucket
 constexpr int kSortThreads = 1024;
-constexpr int kBktUnroll = 8;          // loads in flight per thread in every pass
-constexpr size_t kSortSmem = (size_t)kBktCap * sizeof(float4) + (size_t)kBktMaxCells * sizeof(int);
+constexpr int kClusterCap = 11264;                  // points staged per CTA of a sorting cluster
+constexpr size_t kSortSmem = (size_t)kClusterCap * sizeof(float4) + 2 * (size_t)kBktMaxCells * sizeof(int);
+inline size_t scatter_smem(int K) {
+    return (size_t)kChunk * (sizeof(float4) + sizeof(unsigned short)) + 2 * sizeof(int) * (size_t)K;
+}
 
 __device__ __forceinline__ unsigned weight_q(float w, int emin) {
     const unsigned b = __float_as_uint(w) & 0x7FFFFFFFu;  // +0 and -0 give 0
@@ -351,63 +364,9 @@ __device__ __forceinline__ void pk_put(float4 *pk, int64_t d, const float4 &p) {
     b[2 + h] = p.w;
 }
 
-__global__ void __launch_bounds__(kBktThreads) k_bkt_count(const float4 *__restrict__ pts, int64_t n,
-                                                           int64_t span, int P, float cell, float box,
-                                                           int Q, float rq, int K, int *__restrict__ M,
-                                                           int *__restrict__ flags) {
-    extern __shared__ int hist[];
-    for (int k = threadIdx.x; k < K; k += blockDim.x) hist[k] = 0;
-    __syncthreads();
-    const int64_t i0 = (int64_t)blockIdx.x * span, i1 = min(n, i0 + span);
-    const int64_t T = blockDim.x;
-    unsigned f = 0u, wmax = 0u, wminc = 0u;
-    int64_t i = i0 + threadIdx.x;
-    for (; i + (kBktUnroll - 1) * T < i1; i += kBktUnroll * T) {  // kBktUnroll loads in flight per thread
-        float4 p[kBktUnroll];
-#pragma unroll
-        for (int u = 0; u < kBktUnroll; ++u) p[u] = pts[i + u * T];
-#pragma unroll
-        for (int u = 0; u < kBktUnroll; ++u) {
-            point_flags(p[u], box, f, wmax, wminc);
-            atomicAdd(&hist[div_q(cell_of_point(p[u], P, cell), Q, rq)], 1);
-        }
-    }
-    for (; i < i1; i += T) {
-        const float4 p = pts[i];
-        point_flags(p, box, f, wmax, wminc);
-        atomicAdd(&hist[div_q(cell_of_point(p, P, cell), Q, rq)], 1);
-    }
-    flush_flags(f, wmax, wminc, flags);  // ends with the block's histogram complete
-    const int64_t G = gridDim.x;
-    for (int k = threadIdx.x; k < K; k += blockDim.x) M[k * G + blockIdx.x] = hist[k];
-}
-
-__global__ void __launch_bounds__(kBktThreads) k_bkt_scatter(const float4 *__restrict__ pts, int64_t n,
-                                                             int64_t span, int P, float cell, int Q,
-                                                             float rq, int K, const int *__restrict__ base,
-                                                             float4 *__restrict__ S) {
-    extern __shared__ int cur[];
-    const int64_t G = gridDim.x;
-    for (int k = threadIdx.x; k < K; k += blockDim.x) cur[k] = base[k * G + blockIdx.x];
-    __syncthreads();
-    const int64_t i0 = (int64_t)blockIdx.x * span, i1 = min(n, i0 + span);
-    const int64_t T = blockDim.x;
-    int64_t i = i0 + threadIdx.x;
-    for (; i + (kBktUnroll - 1) * T < i1; i += kBktUnroll * T) {
-        float4 p[kBktUnroll];
-#pragma unroll
-        for (int u = 0; u < kBktUnroll; ++u) p[u] = pts[i + u * T];
-#pragma unroll
-        for (int u = 0; u < kBktUnroll; ++u) S[atomicAdd(&cur[div_q(cell_of_point(p[u], P, cell), Q, rq)], 1)] = p[u];
-    }
-    for (; i < i1; i += T) {
-        const float4 p = pts[i];
-        S[atomicAdd(&cur[div_q(cell_of_point(p, P, cell), Q, rq)], 1)] = p;
-    }
-}
-
 // Exclusive scan of a[0..q) in place, q <= 4 * blockDim.x, blockDim.x a
-// multiple of 32 and at most 1024.  Called by every thread of the block.
+// multiple of 32 and at most 1024.  Called by every thread of the block;
+// ends with the block synchronised.
 __device__ void block_excl_scan4(int *a, int q, int *wsum) {
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     int v[4], s = 0;
@@ -446,91 +405,213 @@ __device__ void block_excl_scan4(int *a, int q, int *wsum) {
     __syncthreads();
 }
 
-// One bucket per CTA: count its points per cell, write the bucket's part of
-// the cell table, place the points in cell order in shared memory and write
-// the copies coalesced.  A bucket above kBktCap points (a very dense region)
-// takes the same counting sort with the copies written point by point.
-__global__ void __launch_bounds__(kSortThreads) k_bkt_sort(
+__global__ void __launch_bounds__(kBktThreads) k_bkt_count(const float4 *__restrict__ pts, int64_t n,
+                                                           int64_t span, int P, float cell, float box,
+                                                           int Q, float rq, int K, int *__restrict__ M,
+                                                           int *__restrict__ flags) {
+    extern __shared__ int hist[];
+    for (int k = threadIdx.x; k < K; k += blockDim.x) hist[k] = 0;
+    __syncthreads();
+    const int64_t i0 = (int64_t)blockIdx.x * span, i1 = min(n, i0 + span);
+    const int64_t T = blockDim.x;
+    unsigned f = 0u, wmax = 0u, wminc = 0u;
+    int64_t i = i0 + threadIdx.x;
+    for (; i + (kBktUnroll - 1) * T < i1; i += kBktUnroll * T) {
+        float4 p[kBktUnroll];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) p[u] = pts[i + u * T];
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) {
+            point_flags(p[u], box, f, wmax, wminc);
+            atomicAdd(&hist[div_q(cell_of_point(p[u], P, cell), Q, rq)], 1);
+        }
+    }
+    for (; i < i1; i += T) {
+        const float4 p = pts[i];
+        point_flags(p, box, f, wmax, wminc);
+        atomicAdd(&hist[div_q(cell_of_point(p, P, cell), Q, rq)], 1);
+    }
+    flush_flags(f, wmax, wminc, flags);  // ends with the block's histogram complete
+    const int64_t G = gridDim.x;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) M[k * G + blockIdx.x] = hist[k];
+}
+
+// Rounds of kChunk points: the round's count per bucket (shared counters), a
+// scan of the counts into run starts, each point staged in its bucket's run
+// (a second shared atomic hands out the slots), then each staged point stored
+// at its bucket's cursor + its offset in the run.
+__global__ void __launch_bounds__(kBktThreads) k_bkt_scatter(const float4 *__restrict__ pts, int64_t n,
+                                                             int64_t span, int P, float cell, int Q,
+                                                             float rq, int K, const int *__restrict__ base,
+                                                             float4 *__restrict__ S) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float4 *stg = reinterpret_cast<float4 *>(smem);
+    int *cur = reinterpret_cast<int *>(smem + (size_t)kChunk * sizeof(float4));  // K write cursors
+    int *cnt = cur + K;                                                            // K: counts, then run starts
+    unsigned short *skb = reinterpret_cast<unsigned short *>(cnt + K);            // bucket of each staged point
+    __shared__ int wsum[32];
+    const int64_t G = gridDim.x;
+    const int T = blockDim.x;
+    for (int k = threadIdx.x; k < K; k += T) cur[k] = base[k * G + blockIdx.x];
+    const int64_t i0 = (int64_t)blockIdx.x * span, i1 = min(n, i0 + span);
+    for (int64_t r0 = i0; r0 < i1; r0 += kChunk) {
+        for (int k = threadIdx.x; k < K; k += T) cnt[k] = 0;
+        __syncthreads();
+        float4 p[kBktUnroll];
+        int kbs[kBktUnroll];  // bucket, or -1 past the slice
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) {
+            const int64_t i = r0 + u * T + threadIdx.x;
+            if (i < i1) p[u] = pts[i];
+        }
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) {
+            const int64_t i = r0 + u * T + threadIdx.x;
+            kbs[u] = -1;
+            if (i < i1) {
+                kbs[u] = div_q(cell_of_point(p[u], P, cell), Q, rq);
+                atomicAdd(&cnt[kbs[u]], 1);
+            }
+        }
+        __syncthreads();
+        block_excl_scan4(cnt, K, wsum);  // run starts; the slots below turn each into its run's end
+#pragma unroll
+        for (int u = 0; u < kBktUnroll; ++u) {
+            if (kbs[u] < 0) continue;
+            const int s = atomicAdd(&cnt[kbs[u]], 1);
+            stg[s] = p[u];
+            skb[s] = (unsigned short)kbs[u];
+        }
+        __syncthreads();
+        const int cn = (int)min((int64_t)kChunk, i1 - r0);
+        for (int t = threadIdx.x; t < cn; t += T) {
+            const int kb = skb[t];
+            S[cur[kb] + (t - (kb ? cnt[kb - 1] : 0))] = stg[t];
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < K; k += T) cur[k] += cnt[k] - (k ? cnt[k - 1] : 0);
+        __syncthreads();
+    }
+}
+
+// Cell-ordered copies of point d = b0 + t of a CTA's output share [t0, t1)
+// (ord holds the share).  A pair block whose partner lies in another share,
+// bucket or nowhere (the catalog's last point) is written half by half.
+__device__ __forceinline__ void emit_point(const float4 *ord, int t, int t0, int t1, int64_t d, int64_t n,
+                                           float *soa, size_t plane, float4 *pk, unsigned *qw, bool fix,
+                                           int emin) {
+    const float4 p = ord[t - t0];
+    if (soa) {
+        soa[d] = p.x;
+        soa[plane + d] = p.y;
+        soa[2 * plane + d] = p.z;
+        soa[3 * plane + d] = p.w;
+    }
+    if (qw) qw[d] = fix ? weight_q(p.w, emin) : 0u;
+    if (!(d & 1)) {
+        if (t + 1 < t1) {  // block d/2 lies inside the share
+            const float4 o = ord[t + 1 - t0];
+            pk[d] = make_float4(p.x, o.x, p.y, o.y);
+            pk[d + 1] = make_float4(p.z, o.z, p.w, o.w);
+        } else if (d + 1 >= n) {
+            pk[d] = make_float4(p.x, 0.f, p.y, 0.f);
+            pk[d + 1] = make_float4(p.z, 0.f, p.w, 0.f);
+        } else {
+            pk_put(pk, d, p);  // the partner opens the next share
+        }
+    } else if (t == t0) {
+        pk_put(pk, d, p);  // the partner closes an earlier share
+    }
+}
+
+// One bucket per cluster of kCluster CTAs (CTA r reads the r-th share of the
+// bucket's points in S and writes the r-th share of its cell-ordered output).
+// A bucket above kCluster * kClusterCap points (a very dense region) takes
+// the same counting sort with each point's copies written where they land.
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kSortThreads) k_bkt_sort(
     const float4 *__restrict__ S, const int *__restrict__ base, int G, int K, int n, int P, float cell,
     int Q, int ncell, int *__restrict__ cell_start, float *__restrict__ soa, size_t plane,
     float4 *__restrict__ pk, unsigned *__restrict__ qw, const int *__restrict__ flags) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem[];
     float4 *ord = reinterpret_cast<float4 *>(smem);
-    int *cnt = reinterpret_cast<int *>(smem + (size_t)kBktCap * sizeof(float4));
+    int *cnt = reinterpret_cast<int *>(smem + (size_t)kClusterCap * sizeof(float4));  // own counts per cell
+    int *off = cnt + kBktMaxCells;                      // this CTA's next slot per cell
+    int *tot = reinterpret_cast<int *>(smem);           // cluster counts, then cell starts (in ord's space)
     __shared__ int wsum[32];
-    const int k = blockIdx.x;
+    const int r = (int)cl.block_rank();
+    const int k = blockIdx.x / kCluster;
+    const int T = blockDim.x;
     const int b0 = base[(int64_t)k * G];
     const int b1 = k + 1 < K ? base[(int64_t)(k + 1) * G] : n;
     const int m = b1 - b0;
     const int c0 = k * Q, q = min(Q, ncell - c0);
-    for (int i = threadIdx.x; i < q; i += blockDim.x) cnt[i] = 0;
+    const int per = (m + kCluster - 1) / kCluster;  // input and output share of a CTA
+    const int j0 = min(m, r * per), j1 = min(m, j0 + per);
+    for (int i = threadIdx.x; i < q; i += T) cnt[i] = 0;
     __syncthreads();
-    const int T = blockDim.x;
-    for (int j = threadIdx.x; j < m; j += kBktUnroll * T) {
+    for (int j = j0 + threadIdx.x; j < j1; j += kBktUnroll * T) {
         float4 p[kBktUnroll];
 #pragma unroll
         for (int u = 0; u < kBktUnroll; ++u)
-            if (j + u * T < m) p[u] = S[b0 + j + u * T];
+            if (j + u * T < j1) p[u] = S[b0 + j + u * T];
 #pragma unroll
         for (int u = 0; u < kBktUnroll; ++u) {
-            if (j + u * T >= m) break;
+            if (j + u * T >= j1) break;
             const int lc = cell_of_point(p[u], P, cell) - c0;
             if ((unsigned)lc < (unsigned)q) atomicAdd(&cnt[lc], 1);
         }
     }
+    cl.sync();  // every CTA's counts are complete
+    for (int i = threadIdx.x; i < q; i += T) {
+        int t = 0, pre = 0;
+#pragma unroll
+        for (int r2 = 0; r2 < kCluster; ++r2) {
+            const int v = cl.map_shared_rank(cnt, r2)[i];
+            pre += r2 < r ? v : 0;
+            t += v;
+        }
+        tot[i] = t;
+        off[i] = pre;
+    }
     __syncthreads();
-    block_excl_scan4(cnt, q, wsum);
-    for (int i = threadIdx.x; i < q; i += blockDim.x) cell_start[c0 + i] = b0 + cnt[i];
-    if (k == K - 1 && threadIdx.x == 0) cell_start[ncell] = n;
-    __syncthreads();  // the counters become placement cursors below
+    block_excl_scan4(tot, q, wsum);
+    for (int i = threadIdx.x; i < q; i += T) {
+        off[i] += tot[i];
+        if (r == 0) cell_start[c0 + i] = b0 + tot[i];
+    }
+    if (k == K - 1 && r == 0 && threadIdx.x == 0) cell_start[ncell] = n;
     int emin, emax;
     const unsigned *uf = reinterpret_cast<const unsigned *>(flags);
     const bool fix = weight_fix_range(uf[0], uf[1], uf[2], &emin, &emax);
-    if (m <= kBktCap) {
-        for (int j = threadIdx.x; j < m; j += kBktUnroll * T) {  // second read of the bucket: L2
+    cl.sync();  // no CTA reads counts any more, and none still uses tot (ord's space)
+    if (per <= kClusterCap) {
+        const float rper = 1.0f / (float)per;
+        for (int j = j0 + threadIdx.x; j < j1; j += kBktUnroll * T) {
             float4 p[kBktUnroll];
 #pragma unroll
             for (int u = 0; u < kBktUnroll; ++u)
-                if (j + u * T < m) p[u] = S[b0 + j + u * T];
+                if (j + u * T < j1) p[u] = S[b0 + j + u * T];  // second read of the share: L2
 #pragma unroll
             for (int u = 0; u < kBktUnroll; ++u) {
-                if (j + u * T >= m) break;
+                if (j + u * T >= j1) break;
                 const int lc = cell_of_point(p[u], P, cell) - c0;
-                if ((unsigned)lc < (unsigned)q) ord[atomicAdd(&cnt[lc], 1)] = p[u];
+                if ((unsigned)lc >= (unsigned)q) continue;
+                const int slot = atomicAdd(&off[lc], 1);
+                const int o = div_q(slot, per, rper);
+                cl.map_shared_rank(ord, o)[slot - o * per] = p[u];
             }
         }
-        __syncthreads();
-        for (int t = threadIdx.x; t < m; t += T) {
-            const float4 p = ord[t];
-            const int64_t d = (int64_t)b0 + t;
-            if (soa) {
-                soa[d] = p.x;
-                soa[plane + d] = p.y;
-                soa[2 * plane + d] = p.z;
-                soa[3 * plane + d] = p.w;
-            }
-            if (qw) qw[d] = fix ? weight_q(p.w, emin) : 0u;
-            if (!(d & 1)) {
-                if (t + 1 < m) {  // block d/2 lies inside the bucket
-                    const float4 o = ord[t + 1];
-                    pk[d] = make_float4(p.x, o.x, p.y, o.y);
-                    pk[d + 1] = make_float4(p.z, o.z, p.w, o.w);
-                } else if (d + 1 >= n) {  // the catalog's last point, without a partner
-                    pk[d] = make_float4(p.x, 0.f, p.y, 0.f);
-                    pk[d + 1] = make_float4(p.z, 0.f, p.w, 0.f);
-                } else {
-                    pk_put(pk, d, p);  // the partner opens the next bucket
-                }
-            } else if (t == 0) {
-                pk_put(pk, d, p);  // the partner closes an earlier bucket
-            }
-        }
+        cl.sync();  // every share is in place
+        for (int t = j0 + threadIdx.x; t < j1; t += T)
+            emit_point(ord, t, j0, j1, (int64_t)b0 + t, n, soa, plane, pk, qw, fix, emin);
     } else {
-        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+        for (int j = j0 + threadIdx.x; j < j1; j += T) {
             const float4 p = S[b0 + j];
             const int lc = cell_of_point(p, P, cell) - c0;
             if ((unsigned)lc >= (unsigned)q) continue;
-            const int64_t d = (int64_t)b0 + atomicAdd(&cnt[lc], 1);
+            const int64_t d = (int64_t)b0 + atomicAdd(&off[lc], 1);
             if (soa) {
                 soa[d] = p.x;
                 soa[plane + d] = p.y;
@@ -572,13 +653,13 @@ int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box
     return launches + 2;
 }
 
-bool grid_bucket_plan(int64_t n, int P, int G, int *Q, int *K) {
+bool grid_bucket_plan(int64_t n, int P, int *Q, int *K) {
     const int64_t ncell = (int64_t)P * P * P;
     if (n < 1 || n > ((int64_t)1 << 30)) return false;
-    // mean bucket near kBktTarget points, at least two buckets per CTA of the
-    // count pass where the cells allow (a small catalog still fills the GPU
-    // in the sort pass), at most kBktMaxCells cells per bucket
-    int64_t k = std::max<int64_t>((n + kBktTarget - 1) / kBktTarget, 2 * (int64_t)G);
+    // mean bucket near kBktTarget points, at least kBktMinBuckets buckets (the
+    // sort pass fills the GPU for a small catalog), at most kBktMaxCells
+    // cells per bucket
+    int64_t k = std::max<int64_t>((n + kBktTarget - 1) / kBktTarget, kBktMinBuckets);
     k = std::max<int64_t>(k, (ncell + kBktMaxCells - 1) / kBktMaxCells);
     k = std::max<int64_t>(1, std::min<int64_t>(k, ncell));
     const int64_t q = (ncell + k - 1) / k;
@@ -595,7 +676,7 @@ cudaError_t grid_bucket_attrs(int device, int K) {
     cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(k_bkt_count), device,
                                       sizeof(int) * (size_t)K);
     if (e == cudaSuccess)
-        e = ensure_smem_limit(reinterpret_cast<const void *>(k_bkt_scatter), device, sizeof(int) * (size_t)K);
+        e = ensure_smem_limit(reinterpret_cast<const void *>(k_bkt_scatter), device, scatter_smem(K));
     if (e == cudaSuccess)
         e = ensure_smem_limit(reinterpret_cast<const void *>(k_bkt_sort), device, kSortSmem);
     return e;
@@ -611,9 +692,9 @@ int launch_grid_build_buckets(const float4 *raw, int64_t n, int P, float cell, f
     const float rq = 1.0f / (float)Q;
     k_bkt_count<<<G, kBktThreads, hs, st>>>(raw, n, span, P, cell, box, Q, rq, K, M, flags);
     int launches = 1 + scan_exclusive(M, Mx, (int64_t)G * K, scan_tmp, st);
-    k_bkt_scatter<<<G, kBktThreads, hs, st>>>(raw, n, span, P, cell, Q, rq, K, Mx, S);
-    k_bkt_sort<<<K, kSortThreads, kSortSmem, st>>>(S, Mx, G, K, (int)n, P, cell, Q, ncell, cell_start, soa,
-                                                  plane, pk, qw, flags);
+    k_bkt_scatter<<<G, kBktThreads, scatter_smem(K), st>>>(raw, n, span, P, cell, Q, rq, K, Mx, S);
+    k_bkt_sort<<<K * kCluster, kSortThreads, kSortSmem, st>>>(S, Mx, G, K, (int)n, P, cell, Q, ncell,
+                                                              cell_start, soa, plane, pk, qw, flags);
     return launches + 2;
 }
 
@@ -702,7 +783,7 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     PCF_CU(ctx, cg->cell_start.ensure(sizeof(int) * (size_t)(ncell + 1)));
     int Q = 0, K = 0;
     const int G = ctx->sm_count;
-    const bool buckets = grid_bucket_plan(n, P, G, &Q, &K);
+    const bool buckets = grid_bucket_plan(n, P, &Q, &K);
     const size_t mat = buckets ? grid_bucket_scratch_ints(G, K) : 0;
     if (buckets) {
         // scratch: the bucketed copy of the catalog (n float4); the CTA x

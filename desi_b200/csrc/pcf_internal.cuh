@@ -401,11 +401,10 @@ unsigned reference_pair_rule(bool ani, bool bpc, bool cross);
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
                       int *rank, int *perm, int *counts, int *cell_start, int *scan_tmp, float *soa,
                       size_t plane, float4 *pk, unsigned *qw, int *flags, cudaStream_t st);
-// Bucketed counting sort (the build for catalogs of up to ~75M points): Q
-// cells per bucket, K buckets, G CTAs in the count and scatter passes; false
-// when the catalog needs more buckets than the shared histograms hold (the
-// per-point build above then runs).
-bool grid_bucket_plan(int64_t n, int P, int G, int *Q, int *K);
+// Bucketed counting sort (the build for catalogs of up to ~134M points): Q
+// cells per bucket, K buckets; false when the catalog needs more buckets
+// than the shared arrays hold (the per-point build above then runs).
+bool grid_bucket_plan(int64_t n, int P, int *Q, int *K);
 // ints of each of the two CTA x bucket matrices (G CTAs)
 size_t grid_bucket_scratch_ints(int G, int K);
 cudaError_t grid_bucket_attrs(int device, int K);
