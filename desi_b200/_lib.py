@@ -38,7 +38,8 @@ class PcfError(RuntimeError):
 
 class TuneResult(ctypes.Structure):
     _fields_ = [("refine", ctypes.c_int), ("hist_mode", ctypes.c_int), ("best_ms", ctypes.c_float),
-                ("default_ms", ctypes.c_float), ("tried", ctypes.c_int), ("tile", ctypes.c_int)]
+                ("default_ms", ctypes.c_float), ("tried", ctypes.c_int), ("tile", ctypes.c_int),
+                ("chunk", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -422,7 +422,8 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     const bool bpc = (flags & PCF_BPC) != 0, cross = b != nullptr;
     const bool weighted = !(a->unit_weights && (!cross || b->unit_weights));
     TuneEntry te;
-    if (ctx->tune_override.refine > 0 || ctx->tune_override.hist_mode >= 0 || ctx->tune_override.tile) {
+    if (ctx->tune_override.refine > 0 || ctx->tune_override.hist_mode >= 0 || ctx->tune_override.tile ||
+        ctx->tune_override.chunk) {
         te = ctx->tune_override;
     } else if (!ctx->tune.empty()) {
         auto it = ctx->tune.find(tune_key(kind, bpc, cross, weighted, bins,
@@ -491,6 +492,7 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     pl.status = ctx->d_status;
     pl.variant = ctx->pair_variant;
     pl.tile_cap = tile_cap;
+    pl.chunk_cap = te.chunk;
     s = launch_pairs(ctx, plan, *a->cells, cross ? *b->cells : *a->cells, a->box, pl, d_cnt, d_ws,
                      d_stats);
     if (s != PCF_OK) return s;

@@ -1046,10 +1046,12 @@ static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items,
     }
     const long long want = (n_items + kWarps - 1) / kWarps;
     const int grid = (int)std::max(1LL, std::min<long long>(want, (long long)sm_count * per_sm));
-    // runs of k items per ticket while a queue holds >= 32 runs per warp
+    // runs of k items per ticket while a queue holds >= 32 runs per warp (k at
+    // most 8, or the tuned cap that A.kchunk carries in)
     PairArgs B = A;
     const long long warps = (long long)grid * kWarps;
-    B.kchunk = (int)std::max(1LL, std::min<long long>(kChunkMax, n_items / (warps * 32)));
+    const long long cap = A.kchunk > 0 ? std::min<long long>(A.kchunk, kChunkMax) : kChunkMax;
+    B.kchunk = (int)std::max(1LL, std::min<long long>(cap, n_items / (warps * 32)));
     B.n_chunked = B.kchunk > 1 ? std::max(0LL, n_items - 2 * warps) : 0;
     B.t_chunked = (B.n_chunked + B.kchunk - 1) / B.kchunk;
     // a warp can take at most every ticket of the queue plus the one that
@@ -1172,6 +1174,7 @@ static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
     A.ctrl = pl.ctrl;
     A.status = pl.status;
     A.max_tickets = n_items + 2;  // refined per launch shape in launch_one
+    A.kchunk = pl.chunk_cap;      // a cap here; launch_one sets the run length
     return A;
 }
 

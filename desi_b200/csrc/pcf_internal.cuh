@@ -230,6 +230,7 @@ struct TuneEntry {
     int hist_mode = -1;  // histogram privatisation (-1: default rule)
     float ms = 0.f;      // best kernel time seen while tuning
     int tile = 0;        // home points per tile: 0 or 32 (kTileCap), or 16
+    int chunk = 0;       // work items per ticket at most: 0 (the launch rule's 8), 1 or 4
 };
 
 struct pcf_ctx {
@@ -344,6 +345,7 @@ struct PairLaunch {
     unsigned *status = nullptr;
     int variant = 0;     // one-pass kernel variant (PCF_OPT_PAIR_VARIANT; pairs.cu)
     int tile_cap = kTileCap;  // home points per tile (32, or 16 when tuned so)
+    int chunk_cap = 0;        // work items per ticket at most (0: the launch rule's 8)
 };
 // Enables the fixed-point weighted histograms when every grid of the launch
 // has exact integer weights and any product fits the three-limb budget.

@@ -87,6 +87,25 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
             best.ms = ms;
             best.tile = 16;
         }
+        // work items per ticket: runs of up to 8 (the launch rule), 4, or
+        // one item per ticket, at the best shape so far
+        ctx->tune_override.tile = best.tile;
+        for (int c : {4, 1}) {
+            ctx->tune_override.chunk = c;
+            ms = 1e30f;
+            for (int rep = 0; rep < 2; ++rep) {
+                pcf_stats st{};
+                pcf_status s = pcf_count_pairs(ctx, kind, a, b, bins, dmax, flags | PCF_DEVICE_OUT,
+                                               out.as<double>(), &st);
+                if (s != PCF_OK) { ms = 1e30f; break; }
+                ms = std::min(ms, st.kernel_ms);
+            }
+            ++tried;
+            if (ms < best.ms) {
+                best.ms = ms;
+                best.chunk = c;
+            }
+        }
     }
     ctx->tune_override = TuneEntry();
     ctx->tune_timing = false;
@@ -95,6 +114,7 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
         res->refine = best.refine;
         res->hist_mode = best.hist_mode;
         res->tile = best.tile ? best.tile : kTileCap;
+        res->chunk = best.chunk ? best.chunk : 8;
         res->best_ms = best.ms;
         res->default_ms = default_ms;
         res->tried = tried;
@@ -108,7 +128,8 @@ extern "C" pcf_status pcf_tune_save(const pcf_ctx *ctx, const char *path) {
     if (!f) return PCF_ERR_IO;
     for (const auto &kv : ctx->tune)
         f << kv.first << ' ' << kv.second.refine << ' ' << kv.second.hist_mode << ' ' << kv.second.ms
-          << ' ' << (kv.second.tile ? kv.second.tile : kTileCap) << '\n';
+          << ' ' << (kv.second.tile ? kv.second.tile : kTileCap) << ' '
+          << (kv.second.chunk ? kv.second.chunk : 8) << '\n';
     return f ? PCF_OK : PCF_ERR_IO;
 }
 
@@ -117,13 +138,14 @@ extern "C" pcf_status pcf_tune_load(pcf_ctx *ctx, const char *path) {
     std::ifstream f(path);
     if (!f) return PCF_ERR_IO;
     std::string line;
-    while (std::getline(f, line)) {  // "key refine hist_mode ms [tile]"
+    while (std::getline(f, line)) {  // "key refine hist_mode ms [tile [chunk]]"
         std::istringstream is(line);
         std::string key;
         TuneEntry e;
         if (!(is >> key >> e.refine >> e.hist_mode >> e.ms)) continue;
-        int tile = 0;
+        int tile = 0, chunk = 0;
         if (is >> tile) e.tile = tile == 16 ? 16 : 0;
+        if (is >> chunk) e.chunk = (chunk == 1 || chunk == 4) ? chunk : 0;
         ctx->tune[key] = e;
     }
     return PCF_OK;

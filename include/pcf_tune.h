@@ -32,14 +32,15 @@ typedef struct pcf_tune_result {
     float default_ms; /* kernel time of the default shape           */
     int tried;        /* candidates timed                           */
     int tile;         /* chosen home points per tile (32 or 16)     */
+    int chunk;        /* chosen work items per ticket at most (8, 4 or 1) */
 } pcf_tune_result;
 
 /* Times the candidates for one pair histogram (arguments as pcf_count_pairs)
  * and stores the winner in the context's table. */
 pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid *a, const pcf_grid *b,
                               int bins, float dmax, uint32_t flags, pcf_tune_result *res);
-/* Text form: one line "key refine hist_mode ms tile" per class (tile may be
- * omitted: 32). */
+/* Text form: one line "key refine hist_mode ms tile chunk" per class (tile
+ * and chunk may be omitted: 32 and 8). */
 pcf_status pcf_tune_save(const pcf_ctx *ctx, const char *path);
 pcf_status pcf_tune_load(pcf_ctx *ctx, const char *path);
 /* Number of classes in the table. */

@@ -69,13 +69,15 @@ def test_autotune_and_estimator(ctx, tmp_path):
     R = catalog.uniform(6000, box, seed=112)
     gd, gr = ctx.grid(D, box), ctx.grid(R, box)
     res = ctx.autotune_pairs(gd, gr, bins=bins, dmax=dmax, bpc=True)
-    assert res["tried"] >= 10 and res["best_ms"] <= res["default_ms"] + 1e-6
+    assert res["tried"] >= 12 and res["best_ms"] <= res["default_ms"] + 1e-6
+    assert res["tile"] in (16, 32) and res["chunk"] in (1, 4, 8)
     assert ctx.tune_size == 1
     # counts with the tuned shape still match the oracle bit for bit
     dr = ctx.count_pairs(gd, gr, bins=bins, dmax=dmax, bpc=True)
     assert np.array_equal(dr, oracle.pairs(D, R, box=box, bins=bins, dmax=dmax, bpc=True))
     p = str(tmp_path / "tune.txt")
     ctx.tune_save(p)
+    assert len(open(p).read().split()) == 6  # key refine hist_mode ms tile chunk
     from desi_b200 import api
     c2 = api.Context(0)
     c2.tune_load(p)
