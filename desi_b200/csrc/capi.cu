@@ -145,6 +145,10 @@ pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value) {
         if (value < 0 || value > 2) return PCF_ERR_INVALID_ARG;
         ctx->pair_variant = (int)value;
         return PCF_OK;
+    case PCF_OPT_GRID_BUILD:
+        if (value < 0 || value > 2) return PCF_ERR_INVALID_ARG;
+        ctx->grid_build = (int)value;
+        return PCF_OK;
     }
     return PCF_ERR_INVALID_ARG;
 }

@@ -6,7 +6,7 @@
 // Cell id = (ix*P + iy)*P + iz with ix = (int)(x / cell), the reference's
 // binning (create_grid.cuh:131-133) clamped to [0, P-1].
 //
-// The build for catalogs of up to ~134M points is bucketed (runs of cells),
+// Catalogs of 6M to ~134M points take a bucketed build (runs of cells):
 // three streaming passes with shared-memory histograms and no per-point
 // global atomic:
 //   1. per CTA, a histogram of its slice of the input over the buckets, with
@@ -16,9 +16,10 @@
 //   3. per bucket, a counting sort by cell in shared memory that writes the
 //      bucket's cell table and the cell-ordered copies (SoA planes,
 //      pair-packed blocks, integer weights) coalesced.
-// Larger catalogs take the per-point build: cell id + per-cell count
+// Other catalogs take the per-point build: cell id + per-cell count
 // (atomic), a scan, the destination of every point (a scattered write) and a
-// gather in destination order.
+// gather in destination order; below 6M points its atomics and gathers stay
+// in L2 and it is the faster of the two.
 #include <algorithm>
 #include <atomic>
 #include <map>
@@ -783,7 +784,12 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     PCF_CU(ctx, cg->cell_start.ensure(sizeof(int) * (size_t)(ncell + 1)));
     int Q = 0, K = 0;
     const int G = ctx->sm_count;
-    const bool buckets = grid_bucket_plan(n, P, &Q, &K);
+    // the bucketed build pays a fixed cost per bucket (a cluster of four
+    // CTAs and three cluster barriers): below ~6M points the per-point build,
+    // whose atomics and gathers then stay in L2, is faster (32768 points: 22
+    // vs 46 us; 8.4M: 0.36 vs 0.35 ms; 33.5M: 2.04 vs 1.31 ms)
+    const bool want_buckets = ctx->grid_build == 2 || (ctx->grid_build == 0 && n >= kBucketBuildMin);
+    const bool buckets = want_buckets && grid_bucket_plan(n, P, &Q, &K);
     const size_t mat = buckets ? grid_bucket_scratch_ints(G, K) : 0;
     if (buckets) {
         // scratch: the bucketed copy of the catalog (n float4); the CTA x

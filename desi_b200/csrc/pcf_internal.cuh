@@ -275,6 +275,7 @@ struct pcf_ctx {
     // adds a triplet kernel's shared u32 histogram absorbs between flushes
     unsigned long long trip_flush_budget = 1ull << 31;
     int pair_variant = 0;  // PCF_OPT_PAIR_VARIANT
+    int grid_build = 0;    // PCF_OPT_GRID_BUILD: 0 by size, 1 per-point, 2 bucketed
     std::map<std::string, std::shared_ptr<struct BatchGraph>> graphs;  // pcf_batch_pairs(PCF_GRAPH)
 };
 
@@ -403,9 +404,11 @@ unsigned reference_pair_rule(bool ani, bool bpc, bool cross);
 int launch_grid_build(const float4 *raw, int64_t n, int P, float cell, float box, int *cid,
                       int *rank, int *perm, int *counts, int *cell_start, int *scan_tmp, float *soa,
                       size_t plane, float4 *pk, unsigned *qw, int *flags, cudaStream_t st);
-// Bucketed counting sort (the build for catalogs of up to ~134M points): Q
-// cells per bucket, K buckets; false when the catalog needs more buckets
-// than the shared arrays hold (the per-point build above then runs).
+// Bucketed counting sort (the build for catalogs of 6M to ~134M points, or
+// any size when forced): Q cells per bucket, K buckets; false when the
+// catalog needs more buckets than the shared arrays hold (the per-point
+// build above then runs).
+constexpr int64_t kBucketBuildMin = (int64_t)6 << 20;
 bool grid_bucket_plan(int64_t n, int P, int *Q, int *K);
 // ints of each of the two CTA x bucket matrices (G CTAs)
 size_t grid_bucket_scratch_ints(int G, int K);

@@ -41,8 +41,19 @@ pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
  *                              sub-copies; 2 two sub-copies and candidates
  *                              staged into shared memory by cp.async (the
  *                              measured A/B of staging).  Results are the
- *                              same in every variant. */
-enum { PCF_OPT_TRIP_FLUSH_BUDGET = 1, PCF_OPT_ABORT_HOST_CHECK = 2, PCF_OPT_PAIR_VARIANT = 3 };
+ *                              same in every variant.
+ *   PCF_OPT_GRID_BUILD         the grid build: 0 (default) by size (the
+ *                              bucketed counting sort from 6M points, the
+ *                              per-point one below), 1 per-point, 2
+ *                              bucketed wherever its shared arrays allow.
+ *                              Grids are the same either way up to the
+ *                              order of points inside a cell. */
+enum {
+    PCF_OPT_TRIP_FLUSH_BUDGET = 1,
+    PCF_OPT_ABORT_HOST_CHECK = 2,
+    PCF_OPT_PAIR_VARIANT = 3,
+    PCF_OPT_GRID_BUILD = 4
+};
 pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value);
 
 /* Kernels this context has launched since it was created. */

@@ -147,15 +147,28 @@ def _cell_table(D, box, P):
     return np.concatenate([[0], np.cumsum(np.bincount(cid, minlength=P ** 3))]), cid
 
 
-@pytest.mark.parametrize("case", ["odd_small", "one_cell", "dense_cell", "large"])
-def test_grid_build_cases(ctx, case):
-    """The bucketed build against a host counting sort: the cell table, the
+@pytest.mark.parametrize("build", [1, 2])
+@pytest.mark.parametrize("case", ["odd_small", "one_cell", "dense_cell", "large", "per_point"])
+def test_grid_build_cases(ctx, case, build):
+    """Both grid builds (PCF_OPT_GRID_BUILD 1: per-point, 2: bucketed; the
+    default picks by size) against a host counting sort: the cell table, the
     multiset of points in cell order, and (through the pair-packed blocks
     and integer weights) DD against the oracle.  odd_small: an odd catalog
-    in many small buckets (pair blocks straddle buckets); one_cell: every
-    point in a single bucket larger than a shared-memory sort holds;
-    dense_cell: 20000 points inside one cell beside a uniform background;
-    large: 2M points in 64^3 cells."""
+    in many small buckets (pair blocks straddle buckets and cluster shares);
+    one_cell: every point in a single bucket larger than a cluster sorts in
+    shared memory; dense_cell: 20000 points inside one cell beside a uniform
+    background; large: 2M points in 64^3 cells; per_point: 300^3 cells, more
+    buckets than the bucketed build's shared arrays hold, so the per-point
+    build runs either way."""
+    from desi_b200.api import PCF_OPT_GRID_BUILD
+    ctx.set_option(PCF_OPT_GRID_BUILD, build)
+    try:
+        _grid_build_case(ctx, case)
+    finally:
+        ctx.set_option(PCF_OPT_GRID_BUILD, 0)
+
+
+def _grid_build_case(ctx, case):
     rng = np.random.default_rng(5)
     box = 100.0
     if case == "odd_small":
@@ -167,8 +180,10 @@ def test_grid_build_cases(ctx, case):
         dense = bg[:1].repeat(20000, 0)
         dense[:, :3] = rng.uniform(40.5, 49.5, size=(20000, 3)).astype(np.float32)
         D, P = np.ascontiguousarray(np.concatenate([bg, dense])), 10
-    else:
+    elif case == "large":
         D, P = catalog.uniform(1 << 21, box, seed=6), 64
+    else:
+        D, P = catalog.uniform(200001, box, seed=8, weights="uniform"), 300
     g = ctx.grid(D, box, partitions=P)
     pts, cs = g.download()
     want_cs, cid = _cell_table(D, box, P)
@@ -177,7 +192,11 @@ def test_grid_build_cases(ctx, case):
     assert np.array_equal(pts[key(pts)], D[key(D)])
     _, cid_out = _cell_table(pts, box, P)
     assert np.all(np.diff(cid_out) >= 0)
-    if case != "large":
+    if case == "per_point":  # counts on the 300^3 cells themselves (the grid's partitions)
+        got = ctx.count_pairs(g, None, bins=5, dmax=1.0)
+        want = oracle.pairs(D, None, box=box, bins=5, dmax=1.0)
+        np.testing.assert_allclose(got, want, rtol=RTOL_W, atol=0)
+    elif case != "large":
         got = ctx.count_pairs(g, None, bins=12, dmax=30.0)
         want = oracle.pairs(D, None, box=box, bins=12, dmax=30.0)
         np.testing.assert_allclose(got, want, rtol=RTOL_W, atol=0)
