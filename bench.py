@@ -847,9 +847,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--pair-variant", type=int, default=0, choices=[0, 1, 2],
-                    help="one-pass pair kernel variant (A/B of shared-memory staging; "
-                         "include/pcf_bench.h PCF_OPT_PAIR_VARIANT)")
+    ap.add_argument("--pair-variant", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="one-pass pair kernel variant (A/B of shared-memory staging and of "
+                         "pair-shared copies; include/pcf_bench.h PCF_OPT_PAIR_VARIANT)")
     ap.add_argument("--served-requests", type=int, default=300,
                     help="requests of the served stream (the workload's own count: 300)")
     ap.add_argument("--no-parity", action="store_true",

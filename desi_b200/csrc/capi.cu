@@ -142,7 +142,7 @@ pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value) {
         ctx->abort_host_check = value != 0;
         return PCF_OK;
     case PCF_OPT_PAIR_VARIANT:
-        if (value < 0 || value > 2) return PCF_ERR_INVALID_ARG;
+        if (value < 0 || value > 3) return PCF_ERR_INVALID_ARG;
         ctx->pair_variant = (int)value;
         return PCF_OK;
     case PCF_OPT_GRID_BUILD:

@@ -228,7 +228,7 @@ __host__ __device__ __forceinline__ int copy_words(int nb) {
 
 // Adds this warp's copy (nb bins) into the launch's accumulators at `off`
 // and clears it.
-template <bool WEIGHTED, int HM>
+template <bool WEIGHTED, int HM, bool XCHG = false>
 __device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, size_t off, double unscale) {
     if (HM == H_GLOBAL) return;
     __syncwarp();
@@ -266,8 +266,17 @@ __device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, si
         unsigned *mine = static_cast<unsigned *>(mine_v);
         for (int k = lane; k < nb; k += 32) {
             unsigned *c = mine + k * kLimbs;
-            const unsigned l0 = c[0], l1 = c[1], l2 = c[2];
-            c[0] = c[1] = c[2] = 0u;
+            unsigned l0, l1, l2;
+            if (XCHG) {  // a copy shared with a warp that may be adding: each limb read and cleared at once
+                l0 = atomicExch(c, 0u);
+                l1 = atomicExch(c + 1, 0u);
+                l2 = atomicExch(c + 2, 0u);
+            } else {
+                l0 = c[0];
+                l1 = c[1];
+                l2 = c[2];
+                c[0] = c[1] = c[2] = 0u;
+            }
             if (l0 | l1 | l2) {  // each term exact; the sum rounds at most twice
                 const double v = (double)l2 * 0x1p32 + ((double)l1 * 0x1p16 + (double)l0);
                 atomicAdd(A.g_wsum + off + k, v * unscale);
@@ -310,9 +319,9 @@ __device__ void flush_copy(void *mine_v, int nb, int lane, const PairArgs &A, si
 #endif
 // CTAs per SM the shared-memory footprint allows at 30 / 900 bins (the
 // register cap of the launch bounds follows from it)
-template <int KIND, int HM>
+template <int KIND, int HM, int VAR = 0>
 struct MinBlocks {
-    static constexpr int value = KIND == 2 ? (HM == H_WFIX ? 4 : 5)
+    static constexpr int value = KIND == 2 ? (HM == H_WFIX ? (VAR == 3 ? 5 : 4) : 5)
                                : HM == H_LFIX ? 4 : HM == H_WFIX ? 5 : PCF_PAIR_MINB;
 };
 
@@ -324,7 +333,8 @@ enum { K_ISO = 0, K_ANI = 1, K_BOTH = 2 };
 // lane-private counts, four per-warp fixed-point sub-copies, else per-warp
 // copies of the same element type.
 __host__ __device__ constexpr int iso_scheme(bool weighted, int hm, int var = 0) {
-    return hm == H_WARP ? (weighted ? H_WARP : H_LANE) : hm == H_WFIX ? (var ? H_WFIX2 : H_WFIX4) : hm;
+    return hm == H_WARP ? (weighted ? H_WARP : H_LANE)
+         : hm == H_WFIX ? ((var == 1 || var == 2) ? H_WFIX2 : H_WFIX4) : hm;
 }
 template <bool WEIGHTED, int HM, int VAR>
 struct IsoScheme {
@@ -386,11 +396,17 @@ struct WarpState {
 // COUNT: also count the in-range pairs (weighted histograms, statistics on).
 // HM is the scheme of the anisotropic copy for K_ANI / K_BOTH launches.
 template <int KIND, bool WEIGHTED, int HM, bool COUNT, int VAR = 0>
-__global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(const PairArgs A) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM, VAR>::value) k_pairs(const PairArgs A) {
     constexpr bool FIX = HM == H_WFIX || HM == H_LFIX;
     constexpr bool DO_I = KIND != K_ANI, DO_A = KIND != K_ISO;
     constexpr bool kPrefetch = KIND == K_BOTH && HM == H_WFIX;  // measured: helps only here
     constexpr bool kStage = VAR == 2;  // candidates of full tiles through shared memory
+    // VAR 3 (single-job launches only): warps 2k and 2k+1 share one
+    // anisotropic copy, each with its own dummy region, so a CTA's copies fit
+    // five CTAs per SM; a shared copy is flushed by atomic exchange, so
+    // either warp may flush while the other adds, and each warp flushes
+    // within half the budget
+    constexpr bool kPairCopy = VAR == 3 && KIND == K_BOTH && HM == H_WFIX;
     // with the next step's loads in flight, a vote per step ran 1.4% faster
     // than one per two steps (periodic 2iso+2ani step, A/B on one box)
     constexpr int kGroup = kPrefetch ? 1 : KIND == K_ISO ? PCF_GROUP_ISO : PCF_GROUP_ANI;
@@ -406,8 +422,12 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
     const int nbi = bins, nba = bins * bins;
     const int nbt = (DO_I ? nbi : 0) + (DO_A ? nba : 0);  // accumulators per job slot
     const int wi = DO_I ? copy_words<HMI>(nbi) : 0, wa = DO_A ? copy_words<HM>(nba) : 0;
-    HT *mine_i = reinterpret_cast<HT *>(smem_raw) + warp * (wi + wa);
-    HT *mine_a = mine_i + wi;
+    constexpr int kDummy = 32 + kLimbs - 1;  // words of one warp's dummy region (kPairCopy)
+    const int wpair = kPairCopy ? nba * kLimbs + 2 * kDummy : 0;  // words of one shared copy
+    HT *mine_i = kPairCopy ? reinterpret_cast<HT *>(smem_raw) + warp * wi
+                           : reinterpret_cast<HT *>(smem_raw) + warp * (wi + wa);
+    HT *mine_a = kPairCopy ? reinterpret_cast<HT *>(smem_raw) + kWarps * wi + (warp >> 1) * wpair
+                           : mine_i + wi;
     // staging windows (kStage): two of kStageCands candidates per warp after
     // every warp's copies: pair-packed blocks, then their integer weights
     float4 *stg_f4 = nullptr;
@@ -418,18 +438,28 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
         stg_f4 = reinterpret_cast<float4 *>(sb);
         stg_q = reinterpret_cast<unsigned *>(sb + 2 * kStageCands * 16);
     }
-    for (int k = lane; k < wi + wa; k += 32) mine_i[k] = (HT)0;
+    if (kPairCopy) {  // both warps of a pair zero the shared copy before either adds
+        for (int k = lane; k < wi; k += 32) mine_i[k] = (HT)0;
+        for (int k = lane; k < wpair; k += 32) mine_a[k] = (HT)0;
+        __syncthreads();
+    } else {
+        for (int k = lane; k < wi + wa; k += 32) mine_i[k] = (HT)0;
+    }
     const unsigned bias_i = kBinBias, bias_a = kBinBias * (unsigned)(bins + 1);
     Sink<WEIGHTED, HMI> sink_i;
     Sink<WEIGHTED, HM> sink_a;
     if (DO_I) setup_sink<WEIGHTED, HMI>(sink_i, (unsigned)__cvta_generic_to_shared(mine_i), mine_i, lane, bias_i, nbi);
     if (DO_A) setup_sink<WEIGHTED, HM>(sink_a, (unsigned)__cvta_generic_to_shared(mine_a), mine_a, lane, bias_a, nba);
+    if (kPairCopy)
+        sink_a.dummy = (unsigned)__cvta_generic_to_shared(mine_a) +
+                       (unsigned)(nba * kLimbs + (warp & 1) * kDummy + lane) * 4u;
     // flushes both copies of this warp into job slot `slot`
     auto flush = [&](int slot, double unscale) {
         const size_t off = (size_t)slot * nbt;
         if (DO_I) flush_copy<WEIGHTED, HMI>(mine_i, nbi, lane, A, off, unscale);
-        if (DO_A) flush_copy<WEIGHTED, HM>(mine_a, nba, lane, A, off + (DO_I ? nbi : 0), unscale);
+        if (DO_A) flush_copy<WEIGHTED, HM, kPairCopy>(mine_a, nba, lane, A, off + (DO_I ? nbi : 0), unscale);
     };
+    const int budget = kPairCopy ? A.budget / 2 : A.budget;
     if (lane == 0) {
         ws.n_cand = 0;
         ws.job_end = -1;
@@ -821,7 +851,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM>::value) k_pairs(
                     if (HM != H_GLOBAL) {
                         const int c = hi_i - lo_i;
                         const int adds = (HM == H_LANE || HM == H_LFIX) ? c / S + 2 : c * H;
-                        if (since + adds > A.budget) {
+                        if (since + adds > budget) {
                             flush(ws.slot, J.wunscale);
                             since = 0;
                         }
@@ -1013,8 +1043,9 @@ static int copy_words_host(int hm, int nb) {
 
 // The one-pass variant of a launch (PCF_OPT_PAIR_VARIANT): only the weighted
 // both-kinds kernel with per-warp fixed-point copies has variants.
-static int pair_variant(const PairLaunch &pl, int hm) {
-    return (pl.both && pl.weighted && hm == H_WFIX && !pl.count) ? pl.variant : 0;
+static int pair_variant(const PairLaunch &pl, int hm, int n_jobs = 1) {
+    const int v = (pl.both && pl.weighted && hm == H_WFIX && !pl.count) ? pl.variant : 0;
+    return (v == 3 && n_jobs != 1) ? 0 : v;  // shared copies hold one job's adds only
 }
 
 template <int KIND, bool W, int HM, bool C, int VAR = 0>
@@ -1063,11 +1094,14 @@ static cudaError_t launch_one(const PairArgs &A, size_t smem, long long n_items,
 
 // Shared-memory bytes per CTA of histogram scheme hm for launch pl (both
 // kinds: the anisotropic copy plus the isotropic one).
-static size_t scheme_bytes(const PairLaunch &pl, int hm) {
+static size_t scheme_bytes(const PairLaunch &pl, int hm, int n_jobs = 1) {
     const int bins = pl.rule.bins;
     const int nb = pl.ani ? bins * bins : bins;
     const size_t e = (hm == H_WFIX || hm == H_LFIX) ? 4 : (pl.weighted ? 8 : 4);
-    const int var = pair_variant(pl, hm);
+    const int var = pair_variant(pl, hm, n_jobs);
+    if (var == 3)  // per-warp isotropic copies, one anisotropic copy per warp pair
+        return e * ((size_t)kWarps * copy_words_host(iso_scheme(pl.weighted, hm, var), bins) +
+                    (size_t)(kWarps / 2) * ((size_t)nb * kLimbs + 2 * (32 + kLimbs - 1)));
     size_t w = (size_t)copy_words_host(hm, nb);
     if (pl.both) w += (size_t)copy_words_host(iso_scheme(pl.weighted, hm, var), bins);
     size_t b = w * e * kWarps;
@@ -1107,7 +1141,7 @@ static int pair_scheme(const PairLaunch &pl) {
 static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t st,
                                   int sm_count, int device) {
     const int hm = pair_scheme(pl);
-    const size_t smem = hm == H_GLOBAL ? 0 : scheme_bytes(pl, hm);
+    const size_t smem = hm == H_GLOBAL ? 0 : scheme_bytes(pl, hm, A.n_jobs);
     // budget: adds one shared counter absorbs between flushes; chunk:
     // candidates per budget check (one chunk alone stays within the budget)
     if (hm == H_WFIX || hm == H_LFIX) {
@@ -1134,8 +1168,9 @@ static cudaError_t dispatch_pairs(PairArgs A, const PairLaunch &pl, cudaStream_t
         if (hm == H_WARP) return launch_one<K_ISO, false, H_WARP, false>(A, smem, n, st, sm_count, device);
         return launch_one<K_ISO, false, H_GLOBAL, false>(A, smem, n, st, sm_count, device);
     }
-    const int var = pair_variant(pl, hm);
+    const int var = pair_variant(pl, hm, A.n_jobs);
     if (pl.both && var == 1) return launch_one<K_BOTH, true, H_WFIX, false, 1>(A, smem, n, st, sm_count, device);
+    if (pl.both && var == 3) return launch_one<K_BOTH, true, H_WFIX, false, 3>(A, smem, n, st, sm_count, device);
     if (pl.both && var == 2) return launch_one<K_BOTH, true, H_WFIX, false, 2>(A, smem, n, st, sm_count, device);
 #define PCF_DISPATCH_A(K_)                                                                         \
     if (pl.weighted) {                                                                             \

@@ -40,8 +40,10 @@ pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
  *                              candidates through the L1 path; 1 two
  *                              sub-copies; 2 two sub-copies and candidates
  *                              staged into shared memory by cp.async (the
- *                              measured A/B of staging).  Results are the
- *                              same in every variant.
+ *                              measured A/B of staging); 3 the anisotropic
+ *                              copy shared by each warp pair, five CTAs per
+ *                              SM (single-job launches; others use 0).
+ *                              Results are the same in every variant.
  *   PCF_OPT_GRID_BUILD         the grid build: 0 (default) by size (the
  *                              bucketed counting sort from 6M points, the
  *                              per-point one below), 1 per-point, 2

@@ -72,12 +72,13 @@ def test_headline_step_tuned(headline_catalogs):
         np.testing.assert_allclose(got[k], want[k], rtol=1e-12, atol=0)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_headline_step_forced_one_pass(headline_catalogs, tmp_path, variant):
     """Both kinds in one pass with per-warp fixed-point limbs (scheme 3) at
     the headline size, P = 12, in each kernel variant: the isotropic copy in
-    four sub-copies (0), in two (1), and two with the candidates staged into
-    shared memory by cp.async (2)."""
+    four sub-copies (0), in two (1), two with the candidates staged into
+    shared memory by cp.async (2), and four with the anisotropic copy shared
+    by each warp pair (3, five CTAs per SM)."""
     D, R, want = headline_catalogs
     W = bench.WORKLOAD
     path = str(tmp_path / "tune.txt")
