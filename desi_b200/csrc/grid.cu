@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <atomic>
 #include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -343,6 +344,7 @@ constexpr int kBktMaxCells = 4096;                  // cells per bucket (the sor
 constexpr int kBktMaxBuckets = 4096;                // buckets (count / scatter shared arrays)
 constexpr int kCluster = 4;                         // CTAs sorting one bucket
 constexpr int kSortThreads = 1024;
+constexpr int kSortUnroll = 4;         // loads in flight per thread in the sort (its shares are prefetched into L2)
 constexpr int kClusterCap = 11264;                  // points staged per CTA of a sorting cluster
 constexpr size_t kSortSmem = (size_t)kClusterCap * sizeof(float4) + 2 * (size_t)kBktMaxCells * sizeof(int);
 inline size_t scatter_smem(int K) {
@@ -363,6 +365,19 @@ __device__ __forceinline__ void pk_put(float4 *pk, int64_t d, const float4 &p) {
     a[2 + h] = p.y;
     b[h] = p.z;
     b[2 + h] = p.w;
+}
+
+// Asks L2 to fetch [p, p + bytes) (p 16-byte aligned) ahead of its use, in
+// bulk requests of at most 64 KB; no shared memory or registers are held.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+    const char *c = static_cast<const char *>(p);
+    bytes &= ~(size_t)15;
+    while (bytes) {
+        const unsigned sz = (unsigned)min(bytes, (size_t)65536);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c), "r"(sz) : "memory");
+        c += sz;
+        bytes -= sz;
+    }
 }
 
 // Exclusive scan of a[0..q) in place, q <= 4 * blockDim.x, blockDim.x a
@@ -418,6 +433,10 @@ __global__ void __launch_bounds__(kBktThreads) k_bkt_count(const float4 *__restr
     unsigned f = 0u, wmax = 0u, wminc = 0u;
     int64_t i = i0 + threadIdx.x;
     for (; i + (kBktUnroll - 1) * T < i1; i += kBktUnroll * T) {
+        if (threadIdx.x == 0) {  // the next block of the slice into L2 meanwhile
+            const int64_t nb = i + kBktUnroll * T, ne = min(i1, nb + kBktUnroll * T);
+            if (nb < ne) prefetch_l2(pts + nb, (size_t)(ne - nb) * sizeof(float4));
+        }
         float4 p[kBktUnroll];
 #pragma unroll
         for (int u = 0; u < kBktUnroll; ++u) p[u] = pts[i + u * T];
@@ -456,6 +475,10 @@ __global__ void __launch_bounds__(kBktThreads) k_bkt_scatter(const float4 *__res
     for (int k = threadIdx.x; k < K; k += T) cur[k] = base[k * G + blockIdx.x];
     const int64_t i0 = (int64_t)blockIdx.x * span, i1 = min(n, i0 + span);
     for (int64_t r0 = i0; r0 < i1; r0 += kChunk) {
+        if (threadIdx.x == 0) {  // the next round's points into L2 while this one runs
+            const int64_t nb = r0 + kChunk, ne = min(i1, nb + kChunk);
+            if (nb < ne) prefetch_l2(pts + nb, (size_t)(ne - nb) * sizeof(float4));
+        }
         for (int k = threadIdx.x; k < K; k += T) cnt[k] = 0;
         __syncthreads();
         float4 p[kBktUnroll];
@@ -525,10 +548,13 @@ __device__ __forceinline__ void emit_point(const float4 *ord, int t, int t0, int
     }
 }
 
-// One bucket per cluster of kCluster CTAs (CTA r reads the r-th share of the
-// bucket's points in S and writes the r-th share of its cell-ordered output).
-// A bucket above kCluster * kClusterCap points (a very dense region) takes
-// the same counting sort with each point's copies written where they land.
+// Buckets k = c, c + C, ... for cluster c of C (persistent: a cluster's
+// launch and barriers are paid once, and while a bucket's copies are written
+// the next bucket's share is prefetched into L2).  Per bucket, CTA r of the
+// cluster reads the r-th share of the bucket's points in S and writes the
+// r-th share of its cell-ordered output.  A bucket above kCluster *
+// kClusterCap points (a very dense region) takes the same counting sort with
+// each point's copies written where they land.
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kSortThreads) k_bkt_sort(
     const float4 *__restrict__ S, const int *__restrict__ base, int G, int K, int n, int P, float cell,
     int Q, int ncell, int *__restrict__ cell_start, float *__restrict__ soa, size_t plane,
@@ -542,86 +568,99 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kSortThreads)
     int *tot = reinterpret_cast<int *>(smem);           // cluster counts, then cell starts (in ord's space)
     __shared__ int wsum[32];
     const int r = (int)cl.block_rank();
-    const int k = blockIdx.x / kCluster;
     const int T = blockDim.x;
-    const int b0 = base[(int64_t)k * G];
-    const int b1 = k + 1 < K ? base[(int64_t)(k + 1) * G] : n;
-    const int m = b1 - b0;
-    const int c0 = k * Q, q = min(Q, ncell - c0);
-    const int per = (m + kCluster - 1) / kCluster;  // input and output share of a CTA
-    const int j0 = min(m, r * per), j1 = min(m, j0 + per);
-    for (int i = threadIdx.x; i < q; i += T) cnt[i] = 0;
-    __syncthreads();
-    for (int j = j0 + threadIdx.x; j < j1; j += kBktUnroll * T) {
-        float4 p[kBktUnroll];
-#pragma unroll
-        for (int u = 0; u < kBktUnroll; ++u)
-            if (j + u * T < j1) p[u] = S[b0 + j + u * T];
-#pragma unroll
-        for (int u = 0; u < kBktUnroll; ++u) {
-            if (j + u * T >= j1) break;
-            const int lc = cell_of_point(p[u], P, cell) - c0;
-            if ((unsigned)lc < (unsigned)q) atomicAdd(&cnt[lc], 1);
-        }
-    }
-    cl.sync();  // every CTA's counts are complete
-    for (int i = threadIdx.x; i < q; i += T) {
-        int t = 0, pre = 0;
-#pragma unroll
-        for (int r2 = 0; r2 < kCluster; ++r2) {
-            const int v = cl.map_shared_rank(cnt, r2)[i];
-            pre += r2 < r ? v : 0;
-            t += v;
-        }
-        tot[i] = t;
-        off[i] = pre;
-    }
-    __syncthreads();
-    block_excl_scan4(tot, q, wsum);
-    for (int i = threadIdx.x; i < q; i += T) {
-        off[i] += tot[i];
-        if (r == 0) cell_start[c0 + i] = b0 + tot[i];
-    }
-    if (k == K - 1 && r == 0 && threadIdx.x == 0) cell_start[ncell] = n;
+    const int C = gridDim.x / kCluster;
     int emin, emax;
     const unsigned *uf = reinterpret_cast<const unsigned *>(flags);
     const bool fix = weight_fix_range(uf[0], uf[1], uf[2], &emin, &emax);
-    cl.sync();  // no CTA reads counts any more, and none still uses tot (ord's space)
-    if (per <= kClusterCap) {
-        const float rper = 1.0f / (float)per;
-        for (int j = j0 + threadIdx.x; j < j1; j += kBktUnroll * T) {
-            float4 p[kBktUnroll];
+    // the r-th share [j0, j1) of bucket k: offset b0, m points, per per CTA
+    auto share = [&](int k, int &b0, int &m, int &per, int &j0, int &j1) {
+        b0 = base[(int64_t)k * G];
+        m = (k + 1 < K ? base[(int64_t)(k + 1) * G] : n) - b0;
+        per = (m + kCluster - 1) / kCluster;
+        j0 = min(m, r * per);
+        j1 = min(m, j0 + per);
+    };
+    for (int k = blockIdx.x / kCluster; k < K; k += C) {
+        int b0, m, per, j0, j1;
+        share(k, b0, m, per, j0, j1);
+        const int c0 = k * Q, q = min(Q, ncell - c0);
+        for (int i = threadIdx.x; i < q; i += T) cnt[i] = 0;
+        __syncthreads();
+        for (int j = j0 + threadIdx.x; j < j1; j += kSortUnroll * T) {
+            float4 p[kSortUnroll];
 #pragma unroll
-            for (int u = 0; u < kBktUnroll; ++u)
-                if (j + u * T < j1) p[u] = S[b0 + j + u * T];  // second read of the share: L2
+            for (int u = 0; u < kSortUnroll; ++u)
+                if (j + u * T < j1) p[u] = S[b0 + j + u * T];
 #pragma unroll
-            for (int u = 0; u < kBktUnroll; ++u) {
+            for (int u = 0; u < kSortUnroll; ++u) {
                 if (j + u * T >= j1) break;
                 const int lc = cell_of_point(p[u], P, cell) - c0;
+                if ((unsigned)lc < (unsigned)q) atomicAdd(&cnt[lc], 1);
+            }
+        }
+        cl.sync();  // every CTA's counts are complete (and every CTA is done with the last bucket's ord)
+        for (int i = threadIdx.x; i < q; i += T) {
+            int t = 0, pre = 0;
+#pragma unroll
+            for (int r2 = 0; r2 < kCluster; ++r2) {
+                const int v = cl.map_shared_rank(cnt, r2)[i];
+                pre += r2 < r ? v : 0;
+                t += v;
+            }
+            tot[i] = t;
+            off[i] = pre;
+        }
+        __syncthreads();
+        block_excl_scan4(tot, q, wsum);
+        for (int i = threadIdx.x; i < q; i += T) {
+            off[i] += tot[i];
+            if (r == 0) cell_start[c0 + i] = b0 + tot[i];
+        }
+        if (k == K - 1 && r == 0 && threadIdx.x == 0) cell_start[ncell] = n;
+        cl.sync();  // no CTA reads counts any more, and none still uses tot (ord's space)
+        if (per <= kClusterCap) {
+            for (int j = j0 + threadIdx.x; j < j1; j += kSortUnroll * T) {
+                float4 p[kSortUnroll];
+#pragma unroll
+                for (int u = 0; u < kSortUnroll; ++u)
+                    if (j + u * T < j1) p[u] = S[b0 + j + u * T];  // second read of the share: L2
+                const float rper = 1.0f / (float)per;
+#pragma unroll
+                for (int u = 0; u < kSortUnroll; ++u) {
+                    if (j + u * T >= j1) break;
+                    const int lc = cell_of_point(p[u], P, cell) - c0;
+                    if ((unsigned)lc >= (unsigned)q) continue;
+                    const int slot = atomicAdd(&off[lc], 1);
+                    const int o = div_q(slot, per, rper);
+                    cl.map_shared_rank(ord, o)[slot - o * per] = p[u];
+                }
+            }
+            cl.sync();  // every share is in place
+            if (threadIdx.x == 0 && k + C < K) {  // the next bucket's share into L2 meanwhile
+                int nb0, nm, nper, nj0, nj1;
+                share(k + C, nb0, nm, nper, nj0, nj1);
+                if (nj1 > nj0) prefetch_l2(S + nb0 + nj0, (size_t)(nj1 - nj0) * sizeof(float4));
+            }
+            for (int t = j0 + threadIdx.x; t < j1; t += T)
+                emit_point(ord, t, j0, j1, (int64_t)b0 + t, n, soa, plane, pk, qw, fix, emin);
+        } else {
+            for (int j = j0 + threadIdx.x; j < j1; j += T) {
+                const float4 p = S[b0 + j];
+                const int lc = cell_of_point(p, P, cell) - c0;
                 if ((unsigned)lc >= (unsigned)q) continue;
-                const int slot = atomicAdd(&off[lc], 1);
-                const int o = div_q(slot, per, rper);
-                cl.map_shared_rank(ord, o)[slot - o * per] = p[u];
+                const int64_t d = (int64_t)b0 + atomicAdd(&off[lc], 1);
+                if (soa) {
+                    soa[d] = p.x;
+                    soa[plane + d] = p.y;
+                    soa[2 * plane + d] = p.z;
+                    soa[3 * plane + d] = p.w;
+                }
+                if (qw) qw[d] = fix ? weight_q(p.w, emin) : 0u;
+                pk_put(pk, d, p);  // the partner slot of an odd n's last block is zeroed beforehand
             }
         }
-        cl.sync();  // every share is in place
-        for (int t = j0 + threadIdx.x; t < j1; t += T)
-            emit_point(ord, t, j0, j1, (int64_t)b0 + t, n, soa, plane, pk, qw, fix, emin);
-    } else {
-        for (int j = j0 + threadIdx.x; j < j1; j += T) {
-            const float4 p = S[b0 + j];
-            const int lc = cell_of_point(p, P, cell) - c0;
-            if ((unsigned)lc >= (unsigned)q) continue;
-            const int64_t d = (int64_t)b0 + atomicAdd(&off[lc], 1);
-            if (soa) {
-                soa[d] = p.x;
-                soa[plane + d] = p.y;
-                soa[2 * plane + d] = p.z;
-                soa[3 * plane + d] = p.w;
-            }
-            if (qw) qw[d] = fix ? weight_q(p.w, emin) : 0u;
-            pk_put(pk, d, p);  // the partner slot of an odd n's last block is zeroed beforehand
-        }
+        __syncthreads();  // this CTA's emit is done before its counters are zeroed again
     }
 }
 
@@ -683,10 +722,32 @@ cudaError_t grid_bucket_attrs(int device, int K) {
     return e;
 }
 
+// Clusters of the sort that the device runs at once (persistent grid size),
+// per device, after the kernel's shared-memory limit is raised.
+static int sort_clusters(int device) {
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(device);
+    if (it != cache.end()) return it->second;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kCluster * 256);
+    cfg.blockDim = dim3(kSortThreads);
+    cfg.dynamicSmemBytes = kSortSmem;
+    int num = 0;
+    if (cudaOccupancyMaxActiveClusters(&num, reinterpret_cast<const void *>(k_bkt_sort), &cfg) != cudaSuccess ||
+        num < 1) {
+        cudaGetLastError();
+        num = 16;
+    }
+    cache[device] = num;
+    return num;
+}
+
 int launch_grid_build_buckets(const float4 *raw, int64_t n, int P, float cell, float box, int G, int Q,
                               int K, int *M, int *Mx, int *scan_tmp, float4 *S, int *cell_start,
                               float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
-                              cudaStream_t st) {
+                              int device, cudaStream_t st) {
     const int ncell = P * P * P;
     const int64_t span = (n + G - 1) / G;
     const size_t hs = sizeof(int) * (size_t)K;
@@ -694,7 +755,8 @@ int launch_grid_build_buckets(const float4 *raw, int64_t n, int P, float cell, f
     k_bkt_count<<<G, kBktThreads, hs, st>>>(raw, n, span, P, cell, box, Q, rq, K, M, flags);
     int launches = 1 + scan_exclusive(M, Mx, (int64_t)G * K, scan_tmp, st);
     k_bkt_scatter<<<G, kBktThreads, scatter_smem(K), st>>>(raw, n, span, P, cell, Q, rq, K, Mx, S);
-    k_bkt_sort<<<K * kCluster, kSortThreads, kSortSmem, st>>>(S, Mx, G, K, (int)n, P, cell, Q, ncell,
+    const int nclus = std::min(K, sort_clusters(device));
+    k_bkt_sort<<<nclus * kCluster, kSortThreads, kSortSmem, st>>>(S, Mx, G, K, (int)n, P, cell, Q, ncell,
                                                               cell_start, soa, plane, pk, qw, flags);
     return launches + 2;
 }
@@ -829,7 +891,7 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
         ctx->launches += launch_grid_build_buckets(
             g->raw.as<float4>(), n, P, cg->cell, g->box, G, Q, K, M, M + mat, ctx->scratch_c.as<int>(),
             ctx->scratch_a.as<float4>(), cg->cell_start.as<int>(), cg->soa.as<float>(), cg->plane,
-            cg->pk.as<float4>(), cg->qw.as<unsigned>(), flags, st);
+            cg->pk.as<float4>(), cg->qw.as<unsigned>(), flags, ctx->device, st);
     } else {
         int *cid = ctx->scratch_a.as<int>();
         ctx->launches += launch_grid_build(g->raw.as<float4>(), n, P, cg->cell, g->box, cid, cid + n,

@@ -417,7 +417,7 @@ cudaError_t grid_bucket_attrs(int device, int K);
 int launch_grid_build_buckets(const float4 *raw, int64_t n, int P, float cell, float box, int G, int Q,
                               int K, int *M, int *Mx, int *scan_tmp, float4 *S, int *cell_start,
                               float *soa, size_t plane, float4 *pk, unsigned *qw, int *flags,
-                              cudaStream_t st);
+                              int device, cudaStream_t st);
 // Zeroes the padding past point n of the SoA planes, integer weights and pair
 // blocks (the builds write entries 0 .. n-1); runs before the build.
 int launch_grid_tails(float *soa, size_t plane, int64_t n, float4 *pk, unsigned *qw, cudaStream_t st);
