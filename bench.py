@@ -420,6 +420,8 @@ def run_ours(args, rank, world, local_rank):
                          "rtol": 1e-12, "bins_compared": int(sum(v.size for v in got.values())),
                          "mismatched_bins": int(sum(mm.values())),
                          "oracle_s": round(time.perf_counter() - t0, 2)}
+    if args.iso_plain:
+        out["plain_2iso"] = run_plain_2iso(ctx, torch, stream)
     if not args.no_extras:
         # the other north-star forms, measured beside the headline (not the metric)
         out["grid_build"] = run_grid_build(ctx, torch)
@@ -437,6 +439,35 @@ def run_ours(args, rank, world, local_rank):
 # permutation (28 B per point of scratch traffic) and the O(cells) scan are
 # not counted.
 GRID_BYTES_PER_POINT = 16 + 16 + 16 + 4
+
+
+def run_plain_2iso(ctx, torch, stream, reps=5):
+    """This library's plain per-call form of the reference's `2iso -bpc` on the
+    catalogs of the reference CUDA run (unit weights): DD, RR, DR as three
+    calls with the library's default partition choice, device outputs, then
+    one D2H read; the grids are built before the timed region, as the
+    reference's host grid is built before its timer starts."""
+    W = WORKLOAD
+    D, R = ref_gpu_catalogs()
+    dev = torch.device("cuda", ctx.device)
+    out = torch.zeros(3 * W["bins"], dtype=torch.float64, device=dev)
+    gd, gr = ctx.grid(D, W["box"]), ctx.grid(R, W["box"])
+
+    def calls():
+        for k, (a, b) in enumerate(((gd, None), (gr, None), (gd, gr))):
+            ctx.count_pairs(a, b, bins=W["bins"], dmax=W["dmax"], bpc=True,
+                            out_device_ptr=out[k * W["bins"]:].data_ptr())
+        return out.cpu()
+
+    calls()  # warm: cell structures at the call's partition count
+    ms, h = _timed_ms(torch, stream, calls, reps)
+    gd.free()
+    gr.free()
+    h = h.numpy()
+    B = W["bins"]
+    pairs = float(h[:B].sum()) / 2 + float(h[B:2 * B].sum()) / 2 + float(h[2 * B:].sum())
+    return {"workload": "2iso -bpc (DD, RR, DR) of the bench catalogs, unit weights, three plain "
+                        "calls", "ms": ms, "pairs": pairs, "pairs_per_s": pairs / (ms * 1e-3)}
 
 
 def run_grid_build(ctx, torch, n=1 << 25, box=1000.0, partitions=128, reps=3):
@@ -800,6 +831,45 @@ def cpu_triplet_baseline(threads, n=8192):
             "seconds": dt}
 
 
+def ref_gpu_catalogs():
+    """The bench catalogs for the side-by-side 2iso -bpc run against the
+    reference's CUDA program: coordinates at least 1e-3 inside the box (its
+    host grid does not clamp cell indices) and unit weights, so its
+    histograms are pair counts."""
+    D, R = catalogs()
+    box = WORKLOAD["box"]
+    out = []
+    for X in (D, R):
+        Y = np.array(X, dtype=np.float32, copy=True)
+        Y[:, :3] = np.clip(Y[:, :3], 0.0, np.float32(box - 1e-3))
+        Y[:, 3] = 1.0
+        out.append(Y)
+    return out
+
+
+def run_reference_cuda():
+    """The reference's CUDA program (cuda/main.cu, built unmodified for sm_100a
+    by oracle/Makefile) on `2iso -bpc`, one random file, the bench catalogs;
+    its own event timer (kernels + D2H + histogram files)."""
+    import tempfile
+    from oracle import ref_cuda
+    if not ref_cuda.available():
+        return {"unavailable": "oracle/_ref/PCF_ref_cuda.out not built"}
+    D, R = ref_gpu_catalogs()
+    W = WORKLOAD
+    runs = []
+    with tempfile.TemporaryDirectory() as wd:
+        for _ in range(2):  # the first run also pays module loading on the device
+            runs.append(ref_cuda.run_2iso_bpc(D, R, W["box"], W["bins"], W["dmax"], wd))
+    best = min(runs, key=lambda r: r["ms"])
+    pairs = float(best["DD"].sum()) / 2 + float(best["RR"].sum()) / 2 + float(best["DR"].sum())
+    return {"workload": "2iso -bpc (DD, RR, DR) of the bench catalogs, unit weights, default 35 "
+                        "partitions, one random file", "ms": best["ms"],
+            "ms_runs": [r["ms"] for r in runs], "pairs": pairs,
+            "pairs_per_s": pairs / (best["ms"] * 1e-3),
+            "timer": "the program's own CUDA events around kernels, D2H copies and file writes"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -823,7 +893,9 @@ def run_reference(args, rank, world):
             break
     tot = sum(times)
     value = pairs_step * len(times) / tot
+    extra = {"reference_cuda": run_reference_cuda()} if args.ref_gpu else {}
     return {
+        **extra,
         "impl": "reference", "metric": "pairs/s", "value": value, "unit": "pairs/s",
         "n_gpus": world, "steps": len(times), "steps_requested": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "weak",
@@ -856,6 +928,12 @@ def main():
                     help="skip the check of the timed step against the FP64 oracle")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the triplet / batched / served measurements")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="with --impl reference: also run the reference's CUDA program "
+                         "(2iso -bpc on the bench catalogs) and report its time")
+    ap.add_argument("--iso-plain", action="store_true",
+                    help="with --impl ours: also time this library's plain per-call 2iso -bpc "
+                         "(DD, RR, DR) on the catalogs of --ref-gpu")
     ap.add_argument("--triplets-only", type=int, default=0, metavar="N",
                     help="run only the 3iso section on N + N points and print its result "
                          "(a small case for profiling; not the bench line)")

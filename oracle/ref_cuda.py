@@ -1,0 +1,72 @@
+"""Runner of the reference's own CUDA program (baseline infrastructure only).
+
+`oracle/Makefile` target `ref_cuda` builds cuda/main.cu of the reference
+tree, unmodified, with nvcc for sm_100a into oracle/_ref/PCF_ref_cuda.out.
+This module runs it on given catalogs the way its CLI expects them:
+
+* catalogs are read as text rows "x y z w" from ../data/<name> relative to
+  the working directory (cuda/create_grid.cuh:35-78, open_files);
+* histograms are written as text to ../results/<kind>_<name>
+  (create_grid.cuh:141-160, save_histogram1D);
+* the time it prints ("Spent <ms> miliseconds ...", pcf2isoBPC.cuh:137-139)
+  is a CUDA-event interval around the kernels, the D2H copies and the file
+  writes.
+
+Only the periodic isotropic path (`2iso -bpc`, one random file) is driven:
+its kernels guard every histogram index (cuda/kernels/2isoBPC_k.cuh, the
+`bin>(bn-1)` checks before each atomicAdd) and read points only inside node
+ranges.  The host grid (make_nodos, create_grid.cuh:130-133) indexes cells by
+(int)(x / size_node) without a clamp, so coordinates are kept at least 1e-3
+inside the box.  The `-a` path and the anisotropic cross kernels are not
+run.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+EXE = os.path.join(HERE, "_ref", "PCF_ref_cuda.out")
+
+
+def available():
+    return os.path.exists(EXE)
+
+
+def inside_box(pts, box, margin=1e-3):
+    """The catalog with coordinates clamped to [0, box - margin]."""
+    out = np.array(pts, dtype=np.float32, copy=True)
+    out[:, :3] = np.clip(out[:, :3], 0.0, np.float32(box - margin))
+    return out
+
+
+def _write(path, pts):
+    with open(path, "w") as f:
+        for x, y, z, w in pts.astype(np.float64):
+            f.write(f"{x:.9g} {y:.9g} {z:.9g} {w:.9g}\n")
+
+
+def run_2iso_bpc(D, R, box, bins, dmax, workdir, timeout=600):
+    """Runs `2iso -bpc` on D (data) and R (one random catalog), both with
+    len(D) == len(R) rows; returns {"ms", "DD", "RR", "DR", "stdout"}."""
+    if len(D) != len(R):
+        raise ValueError("the reference reads -n rows from each file")
+    for sub in ("data", "results", "run"):
+        os.makedirs(os.path.join(workdir, sub), exist_ok=True)
+    _write(os.path.join(workdir, "data", "data.dat"), D)
+    _write(os.path.join(workdir, "data", "rand.dat"), R)
+    cmd = [EXE, "2iso", "-bpc", "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)),
+           "-b", str(int(bins)), "-d", repr(float(dmax)), "-s", repr(float(box))]
+    p = subprocess.run(cmd, cwd=os.path.join(workdir, "run"), capture_output=True, text=True,
+                       timeout=timeout)
+    if p.returncode != 0:
+        raise RuntimeError(f"reference CUDA program exited {p.returncode}: {p.stdout[-300:]} {p.stderr[-300:]}")
+    m = re.search(r"Spent\s+([0-9.eE+-]+)\s+miliseconds", p.stdout)
+    if not m:
+        raise RuntimeError("no timer line in the reference's output: " + p.stdout[-300:])
+    res = {"ms": float(m.group(1)), "stdout": p.stdout}
+    for kind in ("DD", "RR", "DR"):
+        name = {"DD": "data.dat", "RR": "rand.dat", "DR": "rand.dat"}[kind]
+        res[kind] = np.loadtxt(os.path.join(workdir, "results", f"{kind}iso_BPC_{name}"))
+    return res
