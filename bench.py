@@ -467,7 +467,40 @@ def run_plain_2iso(ctx, torch, stream, reps=5):
     B = W["bins"]
     pairs = float(h[:B].sum()) / 2 + float(h[B:2 * B].sum()) / 2 + float(h[2 * B:].sum())
     return {"workload": "2iso -bpc (DD, RR, DR) of the bench catalogs, unit weights, three plain "
-                        "calls", "ms": ms, "pairs": pairs, "pairs_per_s": pairs / (ms * 1e-3)}
+                        "calls", "ms": ms, "pairs": pairs, "pairs_per_s": pairs / (ms * 1e-3),
+            "cli": run_cli_2iso(D, R)}
+
+
+def run_cli_2iso(D, R):
+    """This library's PCF.out on the same files and flags as the reference CUDA
+    run (`2iso -bpc -f data.dat -r rand.dat -n N -b 30 -d 80 -s 250`, catalogs
+    in ../data, histograms to ../results): its printed time and the whole
+    process's wall time, the best of two runs."""
+    import re
+    import subprocess
+    import tempfile
+    W = WORKLOAD
+    exe = os.path.join(ROOT, "desi_b200", "PCF.out")
+    best = None
+    with tempfile.TemporaryDirectory() as wd:
+        for sub in ("data", "results", "run"):
+            os.makedirs(os.path.join(wd, sub))
+        for name, X in (("data.dat", D), ("rand.dat", R)):
+            np.savetxt(os.path.join(wd, "data", name), X.astype(np.float64), fmt="%.9g")
+        cmd = [exe, "2iso", "-bpc", "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)),
+               "-b", str(W["bins"]), "-d", repr(W["dmax"]), "-s", repr(W["box"])]
+        for _ in range(2):
+            t0 = time.perf_counter()
+            p = subprocess.run(cmd, cwd=os.path.join(wd, "run"), capture_output=True, text=True,
+                               timeout=300)
+            wall = time.perf_counter() - t0
+            if p.returncode != 0:
+                return {"error": p.stdout[-300:] + p.stderr[-300:]}
+            m = re.search(r"Spent\s+([0-9.eE+-]+)\s+miliseconds", p.stdout)
+            r = {"ms": float(m.group(1)) if m else None, "wall_s": wall}
+            if best is None or wall < best["wall_s"]:
+                best = r
+    return best
 
 
 def run_grid_build(ctx, torch, n=1 << 25, box=1000.0, partitions=128, reps=3):
@@ -865,7 +898,8 @@ def run_reference_cuda():
     pairs = float(best["DD"].sum()) / 2 + float(best["RR"].sum()) / 2 + float(best["DR"].sum())
     return {"workload": "2iso -bpc (DD, RR, DR) of the bench catalogs, unit weights, default 35 "
                         "partitions, one random file", "ms": best["ms"],
-            "ms_runs": [r["ms"] for r in runs], "pairs": pairs,
+            "ms_runs": [r["ms"] for r in runs], "wall_s": min(r["wall_s"] for r in runs),
+            "pairs": pairs,
             "pairs_per_s": pairs / (best["ms"] * 1e-3),
             "timer": "the program's own CUDA events around kernels, D2H copies and file writes"}
 

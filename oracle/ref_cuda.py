@@ -23,6 +23,7 @@ run.
 import os
 import re
 import subprocess
+import time
 
 import numpy as np
 
@@ -49,7 +50,8 @@ def _write(path, pts):
 
 def run_2iso_bpc(D, R, box, bins, dmax, workdir, timeout=600):
     """Runs `2iso -bpc` on D (data) and R (one random catalog), both with
-    len(D) == len(R) rows; returns {"ms", "DD", "RR", "DR", "stdout"}."""
+    len(D) == len(R) rows; returns {"ms", "wall_s", "DD", "RR", "DR", "stdout"}
+    (wall_s: the whole process, reading, host grid and device set-up included)."""
     if len(D) != len(R):
         raise ValueError("the reference reads -n rows from each file")
     for sub in ("data", "results", "run"):
@@ -58,14 +60,16 @@ def run_2iso_bpc(D, R, box, bins, dmax, workdir, timeout=600):
     _write(os.path.join(workdir, "data", "rand.dat"), R)
     cmd = [EXE, "2iso", "-bpc", "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)),
            "-b", str(int(bins)), "-d", repr(float(dmax)), "-s", repr(float(box))]
+    t0 = time.perf_counter()
     p = subprocess.run(cmd, cwd=os.path.join(workdir, "run"), capture_output=True, text=True,
                        timeout=timeout)
+    wall = time.perf_counter() - t0
     if p.returncode != 0:
         raise RuntimeError(f"reference CUDA program exited {p.returncode}: {p.stdout[-300:]} {p.stderr[-300:]}")
     m = re.search(r"Spent\s+([0-9.eE+-]+)\s+miliseconds", p.stdout)
     if not m:
         raise RuntimeError("no timer line in the reference's output: " + p.stdout[-300:])
-    res = {"ms": float(m.group(1)), "stdout": p.stdout}
+    res = {"ms": float(m.group(1)), "wall_s": wall, "stdout": p.stdout}
     for kind in ("DD", "RR", "DR"):
         name = {"DD": "data.dat", "RR": "rand.dat", "DR": "rand.dat"}[kind]
         res[kind] = np.loadtxt(os.path.join(workdir, "results", f"{kind}iso_BPC_{name}"))
