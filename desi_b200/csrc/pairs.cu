@@ -102,6 +102,7 @@ struct PairArgs {
     int kchunk;
     float box;
     int bpc;
+    float zreach;  // dmax * (1 + 1e-5): the z reach of a home tile's rows
     PairRule rule;
     FastCuts fc;
     unsigned long long *g_count;
@@ -537,6 +538,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM, VAR>::value) k_p
         const int sidx = lane / H;             // this lane's stream
         const int hidx = t.start + (lane - sidx * H);
         W hw = (W)0;
+        float zmn, zmx;  // the home points' z extent (NaN lanes drop out of fminf / fmaxf)
         {
             float4 h;
             if (sidx < S) {
@@ -548,6 +550,12 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM, VAR>::value) k_p
                 h.w = 0.f;
             }
             ws.home[lane] = h;
+            zmn = zmx = h.z;
+            #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                zmn = fminf(zmn, __shfl_xor_sync(kFull, zmn, o));
+                zmx = fmaxf(zmx, __shfl_xor_sync(kFull, zmx, o));
+            }
         }
         // Candidate ranges of all rows of the item, one row per lane, so the
         // dependent cell-table loads of different rows overlap.
@@ -565,7 +573,16 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM, VAR>::value) k_p
             }
             if (ok) {
                 const int col = (nx * P + ny) * P;
-                const int zhi = t.z1 + rw.kz;
+                // the row's cells, clipped to those the home points reach in z:
+                // a candidate within dmax of a home point has z in (zmn - dmax,
+                // zmx + dmax), so its cell lies in [zcut_lo, zcut_hi] (with
+                // 1e-3 of a cell to spare for the rounding of z / cell here
+                // and in the grid build; the tile's own cells always stay);
+                // periodic images follow the same cell arithmetic past 0 and P
+                const float rcell = (float)P / A.box;
+                const int zcut_lo = min((int)floorf((zmn - A.zreach) * rcell - 1e-3f), (int)t.z0);
+                const int zcut_hi = max((int)floorf((zmx + A.zreach) * rcell + 1e-3f), (int)t.z1);
+                const int zhi = min(t.z1 + rw.kz, zcut_hi);
                 rr.kind = rw.kind;
                 const int *cs = J.cand.cstart;
                 if (rw.kind == 1) {  // forward half of the home column (XX): j > home index
@@ -573,7 +590,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<KIND, HM, VAR>::value) k_p
                     rr.b0 = cs[col + min(zhi, P - 1) + 1];
                     if (A.bpc && zhi >= P) { rr.a1 = cs[col]; rr.b1 = cs[col + zhi - P + 1]; rr.sz1 = A.box; }
                 } else {
-                    const int zlo = t.z0 - rw.kz;
+                    const int zlo = max(t.z0 - rw.kz, zcut_lo);
                     rr.a0 = cs[col + max(zlo, 0)];
                     rr.b0 = cs[col + min(zhi, P - 1) + 1];
                     if (A.bpc) {
@@ -1200,6 +1217,7 @@ static PairArgs make_args(const PairJob *jobs, int n_jobs, long long n_items,
     A.bpc = pl.bpc ? 1 : 0;
     A.rule = pl.rule;
     A.fc = make_cuts(pl.rule, box, std::sqrt((float)pl.rule.dd));
+    A.zreach = (float)(std::sqrt(pl.rule.dd) * (1.0 + 1e-5));
     A.g_count = d_count;
     A.g_wsum = d_wsum;
     A.g_stats = d_stats;
