@@ -247,6 +247,10 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     if args.pair_variant:
         ctx.set_option(api.PCF_OPT_PAIR_VARIANT, args.pair_variant)
+    if not args.no_grid_defer:
+        # both grids of a step are queued before either is completed, so the
+        # host work of one build overlaps the other build on the device
+        ctx.set_option(api.PCF_OPT_GRID_DEFER, 1)
     P, fused, tuned = tune_step(ctx, D, R)
     kinds = ("both",) if fused else (False, True)
     # a both-kinds call tuned to the library's default rule (-1) runs as two
@@ -397,6 +401,8 @@ def run_ours(args, rank, world, local_rank):
                 "the workload)",
         "config": dict(W, partitions=P, kinds_in_one_pass=one_pass, schemes=tuned,
                        pair_kernel_variant=args.pair_variant,
+                       grid_builds="complete in pcf_grid_build" if args.no_grid_defer else
+                       "deferred to first use (PCF_OPT_GRID_DEFER)",
                        parallelism=f"replicas x{world}",
                        l2="flushed between steps (512 MB write)",
                        pairs_per_step=pairs_step),
@@ -956,6 +962,8 @@ def main():
     ap.add_argument("--pair-variant", type=int, default=0, choices=[0, 1, 2, 3],
                     help="one-pass pair kernel variant (A/B of shared-memory staging and of "
                          "pair-shared copies; include/pcf_bench.h PCF_OPT_PAIR_VARIANT)")
+    ap.add_argument("--no-grid-defer", action="store_true",
+                    help="complete each grid build inside pcf_grid_build (PCF_OPT_GRID_DEFER 0)")
     ap.add_argument("--served-requests", type=int, default=300,
                     help="requests of the served stream (the workload's own count: 300)")
     ap.add_argument("--no-parity", action="store_true",

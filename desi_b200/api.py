@@ -15,7 +15,8 @@ import numpy as np
 from . import _lib
 from ._lib import (PCF_ANI, PCF_BOTH, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT,  # noqa: F401
                    PCF_ERR_TIMEOUT, PCF_GRAPH, PCF_ISO, PCF_OPT_ABORT_HOST_CHECK,
-                   PCF_OPT_GRID_BUILD, PCF_OPT_PAIR_VARIANT, PCF_OPT_TRIP_FLUSH_BUDGET,
+                   PCF_OPT_GRID_BUILD, PCF_OPT_GRID_DEFER, PCF_OPT_PAIR_VARIANT,
+                   PCF_OPT_TRIP_FLUSH_BUDGET,
                    PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO, PCF_RULE_INCLUSIVE, PcfError, Stats)
 
 
@@ -68,7 +69,7 @@ class Context:
 
     def set_option(self, option: int, value: int) -> None:
         """pcf_ctx_set_option (include/pcf_bench.h): PCF_OPT_TRIP_FLUSH_BUDGET,
-        PCF_OPT_ABORT_HOST_CHECK, PCF_OPT_PAIR_VARIANT, PCF_OPT_GRID_BUILD."""
+        PCF_OPT_ABORT_HOST_CHECK, PCF_OPT_PAIR_VARIANT, PCF_OPT_GRID_BUILD, PCF_OPT_GRID_DEFER."""
         _check(self.handle, self._lib.pcf_ctx_set_option(self.handle, int(option), int(value)),
                "pcf_ctx_set_option")
 
@@ -104,7 +105,9 @@ class Context:
         _check(self.handle,
                self._lib.pcf_grid_build(self.handle, ptr, count, float(box), int(partitions),
                                         ctypes.byref(h)), "pcf_grid_build")
-        return Grid(self, h, count, float(box))
+        g = Grid(self, h, count, float(box))
+        g._points = keep  # a deferred build reads them until its first use
+        return g
 
     # -- counting ------------------------------------------------------------
     def count_pairs(self, a: "Grid", b: "Grid | None" = None, *, bins: int, dmax: float,

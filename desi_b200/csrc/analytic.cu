@@ -254,6 +254,10 @@ extern "C" pcf_status pcf_analytic_3iso(pcf_ctx *ctx, const pcf_grid *d_, int bi
     if (bn_ref <= 0) bn_ref = 200;
     if (bn_ref > kRefMax) return PCF_ERR_UNSUPPORTED;
     cudaSetDevice(ctx->device);
+    {
+        pcf_status s0 = grid_finish(ctx, d_);
+        if (s0 != PCF_OK) return s0;
+    }
     pcf_grid *D = const_cast<pcf_grid *>(d_);
     const float L = D->box;
     if (!(2.0 * (double)dmax < (double)L)) return PCF_ERR_UNSUPPORTED;

@@ -85,6 +85,12 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
     if (kind == PCF_BOTH) return batch_both_split(ctx, d_, r_, n_rand, bins, dmax, flags, dd, rr, dr, stats);
     if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
     cudaSetDevice(ctx->device);
+    {
+        pcf_status s0 = grid_finish(ctx, d_);
+        for (int i = 0; s0 == PCF_OK && i < n_rand; ++i)
+            if (r_[i]) s0 = grid_finish(ctx, r_[i]);
+        if (s0 != PCF_OK) return s0;
+    }
     const bool ani = kind == PCF_ANI, bpc = (flags & PCF_BPC) != 0;
     pcf_grid *D = const_cast<pcf_grid *>(d_);
     std::vector<pcf_grid *> R((size_t)n_rand);

@@ -149,6 +149,9 @@ pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value) {
         if (value < 0 || value > 2) return PCF_ERR_INVALID_ARG;
         ctx->grid_build = (int)value;
         return PCF_OK;
+    case PCF_OPT_GRID_DEFER:
+        ctx->grid_defer = value != 0;
+        return PCF_OK;
     }
     return PCF_ERR_INVALID_ARG;
 }
@@ -261,7 +264,8 @@ pcf_status pcf_grid_build(pcf_ctx *ctx, const pcf_point *pts, int64_t n, float b
                                 ctx->stream));
     g->user_P = partitions;
     int P = partitions > 0 ? partitions : choose_partitions(n, box, box / 8.f, PCF_ISO, false, 4);
-    pcf_status s = grid_ensure_cells(ctx, g.get(), P);
+    g->owner = ctx;
+    pcf_status s = grid_ensure_cells(ctx, g.get(), P, ctx->grid_defer);
     if (s != PCF_OK) return s;
     *out = g.release();
     return PCF_OK;
@@ -279,6 +283,11 @@ pcf_status pcf_grid_free(pcf_ctx *ctx, pcf_grid *g) {
 pcf_status pcf_grid_info(const pcf_grid *g, int64_t *n, float *box, int *partitions,
                          int64_t *nonempty_cells, int *unit_weights) {
     if (!g) return PCF_ERR_INVALID_ARG;
+    if (g->owner) {  // a deferred build completes here
+        cudaSetDevice(g->owner->device);
+        pcf_status s = grid_finish(g->owner, g);
+        if (s != PCF_OK) return s;
+    }
     if (n) *n = g->n;
     if (box) *box = g->box;
     if (partitions) *partitions = g->cells ? g->cells->P : 0;
@@ -298,6 +307,10 @@ pcf_status pcf_grid_download(pcf_ctx *ctx, const pcf_grid *g, pcf_point *pts_out
                              int32_t *cell_start_out) {
     if (!ctx || !g || !g->cells) return PCF_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
+    {
+        pcf_status s0 = grid_finish(ctx, g);
+        if (s0 != PCF_OK) return s0;
+    }
     std::vector<float> planes;
     if (pts_out) {  // the cell-ordered SoA planes, interleaved on the host
         const CellGrid &c = *g->cells;
@@ -419,6 +432,11 @@ static pcf_status count_pairs_impl(pcf_ctx *ctx, int kind, const pcf_grid *a_, c
     if (kind != PCF_ISO && (int64_t)bins * bins > (1 << 24)) return PCF_ERR_UNSUPPORTED;
     if (kind == PCF_BOTH && ds_override > 0) return PCF_ERR_INVALID_ARG;
     if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
+    {
+        pcf_status s0 = grid_finish(ctx, a_);
+        if (s0 == PCF_OK && b_) s0 = grid_finish(ctx, b_);
+        if (s0 != PCF_OK) return s0;
+    }
     cudaSetDevice(ctx->device);
     pcf_grid *a = const_cast<pcf_grid *>(a_);
     pcf_grid *b = const_cast<pcf_grid *>(b_);

@@ -72,6 +72,38 @@ DevBuf::~DevBuf() {
     else cudaFree(p);
 }
 
+cudaError_t PinnedPool::get(size_t n, void **p, size_t *got) {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = free_blocks.lower_bound(n);
+    if (it != free_blocks.end() && it->first <= 4 * n + (64u << 10)) {
+        *p = it->second;
+        *got = it->first;
+        free_blocks.erase(it);
+        return cudaSuccess;
+    }
+    const size_t want = std::max<size_t>(n, 64u << 10);
+    cudaError_t e = cudaMallocHost(p, want);
+    if (e == cudaSuccess) *got = want;
+    return e;
+}
+
+void PinnedPool::put(void *p, size_t n) {
+    std::lock_guard<std::mutex> lk(mu);
+    free_blocks.insert({n, p});
+}
+
+PinnedPool::~PinnedPool() {
+    for (auto &kv : free_blocks) cudaFreeHost(kv.second);
+}
+
+CellGrid::~CellGrid() {
+    if (ready) {  // the stage may still feed the tile table's copy
+        cudaEventSynchronize(ready);
+        cudaEventDestroy(ready);
+    }
+    if (stage && pinned) pinned->put(stage, stage_bytes);
+}
+
 cudaError_t DevBuf::ensure(size_t n) {
     if (n <= bytes && p) return cudaSuccess;
     if (p) {
@@ -818,7 +850,9 @@ pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes) {
 // A grid keeps the cell structures of the last few partition counts it was
 // counted at, so classes of histograms tuned to different partitions do not
 // rebuild (and synchronise) on every switch.
-pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
+pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P, bool defer) {
+    pcf_status s0 = grid_finish(ctx, g);  // the current structure first
+    if (s0 != PCF_OK) return s0;
     if (g->cells && g->cells->P == P) return PCF_OK;
     if (P < 1 || P > 320) return PCF_ERR_INVALID_ARG;
     for (size_t i = 0; i < g->cell_cache.size(); ++i) {
@@ -901,21 +935,50 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     }
     PCF_CU(ctx, cudaGetLastError());
     if (pg1) PCF_CU(ctx, cudaEventRecord(pg1, st));
-    // cell table and flags come back through the context's page-locked
-    // buffer (pageable copies go through the driver's staging, where
-    // concurrent contexts were seen to stall one another)
+    // this build's own page-locked block: the cell table and flags come back
+    // into it, and the tile table later goes out from it (pageable copies go
+    // through the driver's staging, where concurrent contexts were seen to
+    // stall one another); sized for both (tiles <= n / kTileCap + the
+    // non-empty cells + 1)
     const size_t sb = sizeof(int) * (size_t)(ncell + 1);
-    pcf_status ps = pcf_ensure_pinned(ctx, sb + 64);
-    if (ps != PCF_OK) return ps;
-    char *hp = static_cast<char *>(ctx->h_pinned);
+    const size_t tile_max = sizeof(TileDesc) * (size_t)(std::min<int64_t>(ncell, n) + n / kTileCap + 2);
+    cg->pinned = ctx->pinned;
+    PCF_CU(ctx, ctx->pinned->get(std::max(sb + 64, tile_max), &cg->stage, &cg->stage_bytes));
+    char *hp = static_cast<char *>(cg->stage);
     PCF_CU(ctx, cudaMemcpyAsync(hp, cg->cell_start.p, sb, cudaMemcpyDeviceToHost, st));
     PCF_CU(ctx, cudaMemcpyAsync(hp + sb, flags, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    PCF_CU(ctx, cudaStreamSynchronize(st));
+    PCF_CU(ctx, cudaEventCreateWithFlags(&cg->ready, cudaEventDisableTiming));
+    PCF_CU(ctx, cudaEventRecord(cg->ready, st));
+    cg->pending = true;
+    if (g->cells) {
+        g->cell_cache.push_back(std::move(g->cells));
+        if ((int)g->cell_cache.size() > kCellCache) g->cell_cache.erase(g->cell_cache.begin());
+    }
+    g->cells = std::move(cg);
+    return defer ? PCF_OK : grid_finish(ctx, g);
+}
+
+// Completes a queued build: waits for its cell table, checks the catalog's
+// flags, sets the weight range and sends the tile table.  A catalog found
+// invalid stays marked, so every later use reports it.
+pcf_status grid_finish(pcf_ctx *ctx, const pcf_grid *g_) {
+    pcf_grid *g = const_cast<pcf_grid *>(g_);
+    if (g->bad != PCF_OK) {
+        ctx->last_error = "a coordinate lies outside [0, box)";
+        return g->bad;
+    }
+    CellGrid *cg = g->cells.get();
+    if (!cg || !cg->pending) return PCF_OK;
+    cg->pending = false;
+    PCF_CU(ctx, cudaEventSynchronize(cg->ready));
+    const int64_t ncell = (int64_t)cg->P * cg->P * cg->P;
+    const size_t sb = sizeof(int) * (size_t)(ncell + 1);
+    const char *hp = static_cast<const char *>(cg->stage);
     cg->h_start.assign(reinterpret_cast<const int *>(hp), reinterpret_cast<const int *>(hp) + ncell + 1);
     unsigned hf[3];
     memcpy(hf, hp + sb, sizeof(hf));
-    const int hflags = (int)hf[0];
-    if (hflags & 1) {
+    if (hf[0] & 1u) {
+        g->bad = PCF_ERR_OUT_OF_BOX;
         ctx->last_error = "a coordinate lies outside [0, box)";
         return PCF_ERR_OUT_OF_BOX;
     }
@@ -924,18 +987,15 @@ pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P) {
     cg->d_tiles.pool = g->pool;
     PCF_CU(ctx, cg->d_tiles.ensure(sizeof(TileDesc) * std::max<size_t>(1, cg->tiles.size())));
     if (!cg->tiles.empty()) {
-        // staged in the page-locked buffer: every later host write to it
-        // follows a synchronisation of this stream
         const size_t tb = sizeof(TileDesc) * cg->tiles.size();
-        if ((ps = pcf_ensure_pinned(ctx, tb)) != PCF_OK) return ps;
-        memcpy(ctx->h_pinned, cg->tiles.data(), tb);
-        PCF_CU(ctx, cudaMemcpyAsync(cg->d_tiles.p, ctx->h_pinned, tb, cudaMemcpyHostToDevice, st));
+        if (tb > cg->stage_bytes) {  // cannot happen: the staging is sized by the bound above
+            ctx->last_error = "tile table larger than its staging block";
+            return PCF_ERR_CUDA;
+        }
+        memcpy(cg->stage, cg->tiles.data(), tb);  // the cell table's copy into it has completed
+        PCF_CU(ctx, cudaMemcpyAsync(cg->d_tiles.p, cg->stage, tb, cudaMemcpyHostToDevice, ctx->stream));
+        PCF_CU(ctx, cudaEventRecord(cg->ready, ctx->stream));
     }
-    if (g->cells) {
-        g->cell_cache.push_back(std::move(g->cells));
-        if ((int)g->cell_cache.size() > kCellCache) g->cell_cache.erase(g->cell_cache.begin());
-    }
-    g->cells = std::move(cg);
     return PCF_OK;
 }
 

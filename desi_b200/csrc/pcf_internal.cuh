@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -155,8 +156,30 @@ struct DevBuf {
 
 constexpr int kTileCap = 32;  // home points per warp item
 
+// Page-locked host blocks for the grid builds' staging (the cell table read
+// back, the tile table sent), reused by size; shared by a context and its
+// cell structures, so a structure that outlives its context still returns
+// its block.
+struct PinnedPool {
+    std::mutex mu;
+    std::multimap<size_t, void *> free_blocks;
+    cudaError_t get(size_t n, void **p, size_t *got);
+    void put(void *p, size_t n);
+    ~PinnedPool();
+};
+
 struct CellGrid {
     int P = 0;
+    // a build whose cell table is still on its way to the host (deferred
+    // builds): `ready` follows its copy into `stage`; grid_finish completes
+    // it.  `stage` (from `pinned`) then feeds the tile table's copy and is
+    // returned once `ready`, recorded after that copy, has passed.
+    bool pending = false;
+    cudaEvent_t ready = nullptr;
+    void *stage = nullptr;
+    size_t stage_bytes = 0;
+    std::shared_ptr<PinnedPool> pinned;
+    ~CellGrid();
     uint64_t serial = 0;          // unique per build (keys captured graphs)
     float cell = 0.f;             // box / P
     DevBuf soa;                   // x | y | z | w planes, n + kSoaPad floats each
@@ -211,6 +234,8 @@ struct pcf_grid {
     // cell structures are shared: a captured batch graph keeps the ones it reads alive
     std::shared_ptr<CellGrid> cells;                    // the current cell structure
     std::vector<std::shared_ptr<CellGrid>> cell_cache;  // earlier ones, most recent last
+    pcf_ctx *owner = nullptr;       // the context that built it (finishes a deferred build)
+    pcf_status bad = PCF_OK;        // set when a deferred build found the catalog invalid
 };
 constexpr int kCellCache = 2;  // cell structures kept besides the current one
 
@@ -276,6 +301,8 @@ struct pcf_ctx {
     unsigned long long trip_flush_budget = 1ull << 31;
     int pair_variant = 0;  // PCF_OPT_PAIR_VARIANT
     int grid_build = 0;    // PCF_OPT_GRID_BUILD: 0 by size, 1 per-point, 2 bucketed
+    bool grid_defer = false;  // PCF_OPT_GRID_DEFER: pcf_grid_build returns once queued
+    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     std::map<std::string, std::shared_ptr<struct BatchGraph>> graphs;  // pcf_batch_pairs(PCF_GRAPH)
 };
 
@@ -294,7 +321,12 @@ cudaError_t ensure_smem_limit(const void *fn, int device, size_t bytes);
         if (_e != cudaSuccess) return pcf_fail(ctx, _e, #call); \
     } while (0)
 
-pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P);
+// defer: return once the build is queued (its cell table read back
+// asynchronously); grid_finish then completes it (host cell table, catalog
+// checks, tile table).  Every use of a grid's host-side fields goes through
+// grid_finish first; it is a no-op for a finished grid.
+pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P, bool defer = false);
+pcf_status grid_finish(pcf_ctx *ctx, const pcf_grid *g);
 int choose_partitions(int64_t n, float box, float dmax, int kind, bool bpc, int npoint_kind);
 
 // Stencil of one pair launch (host).  Work items are implicit: item i is

@@ -869,6 +869,11 @@ extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid 
     if (kind != PCF_ISO) return PCF_ERR_INVALID_ARG;
     if (bins > 255 || (int64_t)bins * bins * bins > (1 << 26)) return PCF_ERR_UNSUPPORTED;
     cudaSetDevice(ctx->device);
+    {
+        pcf_status s0 = grid_finish(ctx, x_);
+        if (s0 == PCF_OK && y_) s0 = grid_finish(ctx, y_);
+        if (s0 != PCF_OK) return s0;
+    }
     pcf_grid *X = const_cast<pcf_grid *>(x_);
     pcf_grid *Y = const_cast<pcf_grid *>(y_);
     const bool bpc = (flags & PCF_BPC) != 0, mixed = Y != nullptr;
@@ -969,6 +974,12 @@ extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const
     if (bins > 255 || (int64_t)bins * bins * bins > (1 << 26)) return PCF_ERR_UNSUPPORTED;
     if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
     cudaSetDevice(ctx->device);
+    {
+        pcf_status s0 = grid_finish(ctx, d_);
+        for (int i = 0; s0 == PCF_OK && i < n_rand; ++i)
+            if (r_[i]) s0 = grid_finish(ctx, r_[i]);
+        if (s0 != PCF_OK) return s0;
+    }
     const bool bpc = (flags & PCF_BPC) != 0;
     pcf_grid *D = const_cast<pcf_grid *>(d_);
     std::vector<pcf_grid *> R((size_t)n_rand);
@@ -1139,6 +1150,11 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     if (bins > 255 || (int64_t)bins * bins * bins * bins * bins > ((int64_t)1 << 31))
         return PCF_ERR_UNSUPPORTED;
     cudaSetDevice(ctx->device);
+    {
+        pcf_status s0 = grid_finish(ctx, x_);
+        if (s0 == PCF_OK && y_) s0 = grid_finish(ctx, y_);
+        if (s0 != PCF_OK) return s0;
+    }
     pcf_grid *X = const_cast<pcf_grid *>(x_);
     pcf_grid *Y = const_cast<pcf_grid *>(y_);
     const bool bpc = (flags & PCF_BPC) != 0, mixed = Y != nullptr;

@@ -23,6 +23,12 @@ extern "C" pcf_status pcf_autotune_pairs(pcf_ctx *ctx, int kind, const pcf_grid 
                                          const pcf_grid *b, int bins, float dmax, uint32_t flags,
                                          pcf_tune_result *res) {
     if (!ctx || !a || bins < 1 || !(dmax > 0.f)) return PCF_ERR_INVALID_ARG;
+    {
+        cudaSetDevice(ctx->device);
+        pcf_status s0 = grid_finish(ctx, a);
+        if (s0 == PCF_OK && b) s0 = grid_finish(ctx, b);
+        if (s0 != PCF_OK) return s0;
+    }
     const bool ani = kind != PCF_ISO, cross = b != nullptr;
     const bool weighted = !(a->unit_weights && (!cross || b->unit_weights));
     const std::string key = tune_key(kind, (flags & PCF_BPC) != 0, cross, weighted, bins,

@@ -49,12 +49,25 @@ pcf_status pcf_microbench(pcf_ctx *ctx, int which, double *result);
  *                              per-point one below), 1 per-point, 2
  *                              bucketed wherever its shared arrays allow.
  *                              Grids are the same either way up to the
- *                              order of points inside a cell. */
+ *                              order of points inside a cell.
+ *   PCF_OPT_GRID_DEFER         0 (default): pcf_grid_build returns a
+ *                              complete grid, or the catalog's error.  1:
+ *                              it returns once the build is queued; the
+ *                              first call that uses the grid completes it
+ *                              (waiting only for this build's cell table)
+ *                              and reports a catalog error such as
+ *                              PCF_ERR_OUT_OF_BOX, as does every later use.
+ *                              Building several grids before counting then
+ *                              overlaps each build's host work with the next
+ *                              build on the device.  Host points passed to a
+ *                              deferred build must stay unchanged until that
+ *                              first use. */
 enum {
     PCF_OPT_TRIP_FLUSH_BUDGET = 1,
     PCF_OPT_ABORT_HOST_CHECK = 2,
     PCF_OPT_PAIR_VARIANT = 3,
-    PCF_OPT_GRID_BUILD = 4
+    PCF_OPT_GRID_BUILD = 4,
+    PCF_OPT_GRID_DEFER = 5
 };
 pcf_status pcf_ctx_set_option(pcf_ctx *ctx, int option, int64_t value);
 

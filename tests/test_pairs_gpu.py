@@ -202,6 +202,43 @@ def _grid_build_case(ctx, case):
         np.testing.assert_allclose(got, want, rtol=RTOL_W, atol=0)
 
 
+def test_deferred_grid_builds(ctx):
+    """PCF_OPT_GRID_DEFER: grids built back to back and completed by their
+    first use (in another order than built) give the histograms of complete
+    builds; an invalid catalog is reported by its first use and every later
+    one."""
+    from desi_b200.api import PCF_OPT_GRID_DEFER, PcfError
+    box = 250.0
+    cats = [catalog.neyman_scott(4000, box, seed=71), catalog.uniform(4100, box, seed=72),
+            catalog.uniform(3900, box, seed=73, weights="uniform")]
+    want = [ctx.count_pairs(ctx.grid(c, box), None, bins=20, dmax=60.0, ani="both", bpc=True)
+            for c in cats]
+    from desi_b200 import api
+    c2 = api.Context(0)
+    try:
+        c2.set_option(PCF_OPT_GRID_DEFER, 1)
+        gs = [c2.grid(c, box) for c in cats]
+        for k in (2, 0, 1):
+            got = c2.count_pairs(gs[k], None, bins=20, dmax=60.0, ani="both", bpc=True)
+            for g_, w_ in zip(got, want[k]):
+                np.testing.assert_allclose(g_, w_, rtol=1e-12, atol=0)
+        dr = c2.count_pairs(gs[0], gs[1], bins=20, dmax=60.0, bpc=True)
+        np.testing.assert_array_equal(dr, oracle.pairs(cats[0], cats[1], box=box, bins=20,
+                                                        dmax=60.0, bpc=True))
+        bad = cats[1].copy()
+        bad[7, 0] = box + 1.0
+        gb = c2.grid(bad, box)  # queued: the check comes with the first use
+        for _ in range(2):
+            with pytest.raises(PcfError):
+                c2.count_pairs(gb, None, bins=20, dmax=60.0)
+        with pytest.raises(PcfError):
+            gb.info()
+        gb.free()
+        assert gs[2].info()["unit_weights"] is False
+    finally:
+        c2.close()
+
+
 def _weighted(pts, rng, kind):
     out = pts.copy()
     n = len(out)
