@@ -125,6 +125,16 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         if (dr) add_job(D, R[i], false, 1.0);
     }
     pcf_status s = PCF_OK;
+    // every structure queued before the first is completed (a structure a
+    // later job replaces is completed at that point), so the builds' host
+    // work overlaps the device
+    for (auto &j : js) {
+        if ((s = grid_ensure_cells(ctx, j.h, j.P, true)) != PCF_OK) return s;
+        if ((s = grid_ensure_cells(ctx, j.c, j.P, true)) != PCF_OK) return s;
+    }
+    for (auto &j : js) {
+        if ((s = grid_finish(ctx, j.h)) != PCF_OK || (s = grid_finish(ctx, j.c)) != PCF_OK) return s;
+    }
     for (auto &j : js) {
         if ((s = grid_ensure_cells(ctx, j.h, j.P)) != PCF_OK) return s;
         j.hc = j.h->cells;

@@ -397,10 +397,14 @@ pcf_status prepare_grids(pcf_ctx *ctx, pcf_grid *a, pcf_grid *b, float dmax, int
             return PCF_ERR_UNSUPPORTED;
         }
     }
-    pcf_status s = grid_ensure_cells(ctx, a, P);
+    // both structures queued before either is completed: a's host work
+    // (cell table, tiles) overlaps b's build on the device
+    pcf_status s = grid_ensure_cells(ctx, a, P, b != nullptr);
     if (s != PCF_OK) return s;
     if (b) {
-        s = grid_ensure_cells(ctx, b, P);
+        s = grid_ensure_cells(ctx, b, P, true);
+        if (s == PCF_OK) s = grid_finish(ctx, a);
+        if (s == PCF_OK) s = grid_finish(ctx, b);
         if (s != PCF_OK) return s;
     }
     *P_out = P;

@@ -997,9 +997,13 @@ extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const
     int P = 0;
     pcf_status s = prepare_grids(ctx, big, nullptr, dmax, PCF_ISO, bpc, &P);
     if (s != PCF_OK) return s;
-    if ((s = grid_ensure_cells(ctx, D, P)) != PCF_OK) return s;
+    // every structure queued before the first is completed
+    if ((s = grid_ensure_cells(ctx, D, P, true)) != PCF_OK) return s;
     for (pcf_grid *g : R)
-        if ((s = grid_ensure_cells(ctx, g, P)) != PCF_OK) return s;
+        if ((s = grid_ensure_cells(ctx, g, P, true)) != PCF_OK) return s;
+    if ((s = grid_finish(ctx, D)) != PCF_OK) return s;
+    for (pcf_grid *g : R)
+        if ((s = grid_finish(ctx, g)) != PCF_OK) return s;
     PairPlan plan;
     plan_pairs(*D->cells, D->box, dmax, false, false, plan, ctx->sm_count * 24);
     const int n3 = bins * bins * bins;
