@@ -125,21 +125,18 @@ extern "C" pcf_status pcf_batch_pairs(pcf_ctx *ctx, int kind, const pcf_grid *d_
         if (dr) add_job(D, R[i], false, 1.0);
     }
     pcf_status s = PCF_OK;
-    // every structure queued before the first is completed (a structure a
-    // later job replaces is completed at that point), so the builds' host
-    // work overlaps the device
+    // every structure queued before the first is completed, so the builds'
+    // host work overlaps the device; each job holds its structures, and a
+    // structure that a later job's partition count replaces is completed at
+    // that point, the grids' current ones after the loop
     for (auto &j : js) {
         if ((s = grid_ensure_cells(ctx, j.h, j.P, true)) != PCF_OK) return s;
+        j.hc = j.h->cells;
         if ((s = grid_ensure_cells(ctx, j.c, j.P, true)) != PCF_OK) return s;
+        j.cc = j.c->cells;
     }
     for (auto &j : js) {
         if ((s = grid_finish(ctx, j.h)) != PCF_OK || (s = grid_finish(ctx, j.c)) != PCF_OK) return s;
-    }
-    for (auto &j : js) {
-        if ((s = grid_ensure_cells(ctx, j.h, j.P)) != PCF_OK) return s;
-        j.hc = j.h->cells;
-        if ((s = grid_ensure_cells(ctx, j.c, j.P)) != PCF_OK) return s;
-        j.cc = j.c->cells;
     }
     const int nb = ani ? bins * bins : bins;
     bool weighted = !D->unit_weights;

@@ -72,16 +72,20 @@ DevBuf::~DevBuf() {
     else cudaFree(p);
 }
 
+// Blocks come in power-of-two sizes from 64 KB, so a freed block serves any
+// later request of its size class: pinning new pages (cudaMallocHost) is slow
+// and serialises the threads that share the device.
 cudaError_t PinnedPool::get(size_t n, void **p, size_t *got) {
+    size_t want = 64u << 10;
+    while (want < n) want <<= 1;
     std::lock_guard<std::mutex> lk(mu);
-    auto it = free_blocks.lower_bound(n);
-    if (it != free_blocks.end() && it->first <= 4 * n + (64u << 10)) {
+    auto it = free_blocks.find(want);
+    if (it != free_blocks.end()) {
         *p = it->second;
         *got = it->first;
         free_blocks.erase(it);
         return cudaSuccess;
     }
-    const size_t want = std::max<size_t>(n, 64u << 10);
     cudaError_t e = cudaMallocHost(p, want);
     if (e == cudaSuccess) *got = want;
     return e;
@@ -851,9 +855,9 @@ pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes) {
 // counted at, so classes of histograms tuned to different partitions do not
 // rebuild (and synchronise) on every switch.
 pcf_status grid_ensure_cells(pcf_ctx *ctx, pcf_grid *g, int P, bool defer) {
-    pcf_status s0 = grid_finish(ctx, g);  // the current structure first
+    if (g->cells && g->cells->P == P) return defer ? PCF_OK : grid_finish(ctx, g);
+    pcf_status s0 = grid_finish(ctx, g);  // the current structure, before it is replaced
     if (s0 != PCF_OK) return s0;
-    if (g->cells && g->cells->P == P) return PCF_OK;
     if (P < 1 || P > 320) return PCF_ERR_INVALID_ARG;
     for (size_t i = 0; i < g->cell_cache.size(); ++i) {
         if (g->cell_cache[i]->P != P) continue;
