@@ -821,7 +821,8 @@ def cpu_baseline(pairs_step=None, steps=1):
                           f"{steps} step(s), {dt:.3f} s per step",
                 "seconds_per_step": dt,
                 "as_shipped_2_threads": {"value": pairs_step / dt2, "seconds_per_step": dt2},
-                "triplets": cpu_triplet_baseline(threads)}
+                "triplets": cpu_triplet_baseline(threads),
+                "ingest": ingest_baseline()}
     # fallback: the oracle port (brute force) on a bounded sample
     import oracle
     n = 8192
@@ -843,6 +844,34 @@ def cpu_baseline(pairs_step=None, steps=1):
             cnt += h.sum() / (2 if B is None else 1)
     return {"value": 2 * cnt / dt, "unit": "pairs/s", "cores": threads, "kind": "port",
             "sample": f"oracle brute force on the first {n} points of each catalog"}
+
+
+def ingest_baseline(n=1_000_000):
+    """Catalog reading: the reference's open_files (cuda/create_grid.cuh:35-78,
+    one thread, ifstream >>) against this library's reader (pcf_read_catalog,
+    all host threads) on the same n-row text catalog of 9-digit decimals."""
+    import tempfile
+    try:
+        import oracle
+        from desi_b200 import catalog
+        rng = np.random.default_rng(77)
+        v = rng.uniform(0.0, 1000.0, (n, 4)).astype(np.float32)
+        v[:, 3] = rng.uniform(0.5, 1.5, n).astype(np.float32)
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "catalog.dat")
+            np.savetxt(path, v.astype(np.float64), fmt="%.9g")
+            mb = os.path.getsize(path) / 1e6
+            t0 = time.perf_counter()
+            ours, _ = catalog.load(path, n)
+            t_ours = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            ref, _ = oracle.ref_read_catalog(path, n)
+            t_ref = time.perf_counter() - t0
+        return {"rows": n, "mb": round(mb, 1), "reference_s": t_ref, "reference_mb_per_s": mb / t_ref,
+                "ours_s": t_ours, "ours_mb_per_s": mb / t_ours, "ours_threads": os.cpu_count(),
+                "identical": bool(np.array_equal(ours.view(np.uint32), ref.view(np.uint32)))}
+    except Exception as e:  # the reference reader is built only with the reference tree
+        return {"unavailable": str(e)[:200]}
 
 
 def cpu_triplet_baseline(threads, n=8192):

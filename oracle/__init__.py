@@ -257,6 +257,32 @@ class RefEngine:
         return out.reshape(bins, bins) if self.is2d else out
 
 
+def ref_read_catalog(path: str, n: int, box: float = 0.0):
+    """The reference's own reader (open_files, cuda/create_grid.cuh:35-78,
+    through _ref/libref_io.so) on the first n rows of `path`: (points as an
+    (n, 4) float32 array, box).  box <= 0 asks for the reader's automatic box
+    ceil(max component + 1).  The reader opens "../data/<name>" from the
+    working directory, so the call runs from a scratch directory that links
+    the file there."""
+    import tempfile
+    lib = ctypes.CDLL(os.path.join(HERE, "_ref", "libref_io.so"))
+    lib.ref_open_files.argtypes = [ctypes.c_char_p, ctypes.c_int, _fptr,
+                                   ctypes.POINTER(ctypes.c_float)]
+    out = np.zeros((n, 4), np.float32)
+    b = ctypes.c_float(box)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as wd:
+        os.makedirs(os.path.join(wd, "data"))
+        os.makedirs(os.path.join(wd, "run"))
+        os.symlink(os.path.abspath(path), os.path.join(wd, "data", "cat.dat"))
+        os.chdir(os.path.join(wd, "run"))
+        try:
+            lib.ref_open_files(b"cat.dat", int(n), _p(out), ctypes.byref(b))
+        finally:
+            os.chdir(cwd)
+    return out, float(b.value)
+
+
 class RefAnalyticRR:
     """The reference's CPU periodic 2-point engine with the analytic RR
     (cpp/2PCFisotropic/BPC_analitic/2PCF.h), compiled in place."""

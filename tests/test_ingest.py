@@ -1,6 +1,8 @@
 """CPU: the parallel catalog reader (pcf_read_catalog) parses the reference's
 text format exactly as ifstream >> float does, and the binary .f4 form
 round-trips."""
+import os
+
 import numpy as np
 import pytest
 
@@ -48,3 +50,39 @@ def test_f4_round_trip(tmp_path):
     catalog.save_f4(p, pts)
     got, _ = catalog.load(p, 5000)
     assert np.array_equal(got, pts)
+
+
+_REF_IO = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "libref_io.so")
+
+
+@pytest.mark.skipif(not os.path.exists(_REF_IO), reason="needs oracle/_ref (reference tree at build)")
+def test_text_reader_matches_reference_open_files(tmp_path):
+    """The threaded reader against the reference's own open_files
+    (cuda/create_grid.cuh:35-78, compiled in place): bit-equal points and the
+    same automatic box, on decimals that do not round-trip to float32
+    (17 significant digits), exponents, integers and mixed whitespace."""
+    import oracle
+    rng = np.random.default_rng(11)
+    n = 30011
+    v = rng.uniform(0.0, 250.0, size=(n, 4))
+    v[:, 3] = rng.uniform(0.5, 1.5, n)
+    rows = []
+    for i, r in enumerate(v):
+        if i % 5 == 0:
+            s = " ".join(f"{x:.17g}" for x in r)
+        elif i % 5 == 1:
+            s = "\t".join(f"{x:.6e}" for x in r)
+        elif i % 5 == 2:
+            s = "  ".join(f"{x:.3f}" for x in r)
+        elif i % 5 == 3:
+            s = " ".join(str(int(x)) for x in r[:3]) + f" {r[3]:.9g}"
+        else:
+            s = " ".join(f"{x:.12g}" for x in r)
+        rows.append(s)
+    p = tmp_path / "mix.dat"
+    p.write_text("\n".join(rows) + "\n")
+    want, wbox = oracle.ref_read_catalog(str(p), n)
+    got, box = catalog.load(str(p), n)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert box == wbox
