@@ -283,6 +283,29 @@ def ref_read_catalog(path: str, n: int, box: float = 0.0):
     return out, float(b.value)
 
 
+def ref_save_histogram(h, out_path: str) -> None:
+    """Writes histogram h (bn, bn x bn or bn^3 doubles; dims from h.ndim)
+    through the reference's own writers (save_histogram1D/2D/3D,
+    cuda/create_grid.cuh:141-229, through _ref/libref_io.so) to out_path."""
+    import shutil
+    import tempfile
+    lib = ctypes.CDLL(os.path.join(HERE, "_ref", "libref_io.so"))
+    lib.ref_save_histogram.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dptr]
+    a = np.ascontiguousarray(h, dtype=np.float64)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as wd:
+        os.makedirs(os.path.join(wd, "results"))
+        os.makedirs(os.path.join(wd, "run"))
+        os.chdir(os.path.join(wd, "run"))
+        try:
+            rc = lib.ref_save_histogram(a.ndim, b"h.dat", a.shape[0], _d(a))
+        finally:
+            os.chdir(cwd)
+        if rc != 0:
+            raise ValueError("1, 2 or 3 dimensions")
+        shutil.copy(os.path.join(wd, "results", "h.dat"), out_path)
+
+
 class RefAnalyticRR:
     """The reference's CPU periodic 2-point engine with the analytic RR
     (cpp/2PCFisotropic/BPC_analitic/2PCF.h), compiled in place."""

@@ -1,6 +1,7 @@
 """CPU: the parallel catalog reader (pcf_read_catalog) parses the reference's
 text format exactly as ifstream >> float does, and the binary .f4 form
-round-trips."""
+round-trips; the reader and PCF.out's histogram writers are pinned to the
+reference's own open_files and save_histogram* (compiled in place)."""
 import os
 
 import numpy as np
@@ -86,3 +87,34 @@ def test_text_reader_matches_reference_open_files(tmp_path):
     got, box = catalog.load(str(p), n)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     assert box == wbox
+
+
+@pytest.mark.skipif(not os.path.exists(_REF_IO), reason="needs oracle/_ref (reference tree at build)")
+@pytest.mark.parametrize("dims", [1, 2, 3])
+def test_histogram_files_match_reference_writers(tmp_path, dims):
+    """PCF.out's histogram writers (desi_b200/csrc/pcf_io.hpp) write the same
+    bytes as the reference's save_histogram1D/2D/3D (compiled in place) for
+    counts, weighted sums, tiny values and zeros."""
+    import subprocess
+
+    import oracle
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "io_writer")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(root, "desi_b200", "csrc"),
+                    "-I", os.path.join(root, "include"), os.path.join(root, "tests", "io_writer.cpp"),
+                    "-o", exe], check=True)
+    rng = np.random.default_rng(dims)
+    bn = 7
+    h = rng.uniform(0, 1e6, size=(bn,) * dims)
+    flat = h.reshape(-1)
+    flat[::5] = np.round(flat[::5] * 1e6)           # large integer counts
+    flat[1::7] = rng.uniform(0, 1e-9, flat[1::7].size)  # tiny sums
+    flat[2::9] = 0.0
+    raw = tmp_path / "h.raw"
+    raw.write_bytes(h.astype(np.float64).tobytes())
+    (tmp_path / "results").mkdir()
+    (tmp_path / "run").mkdir()
+    subprocess.run([exe, str(dims), str(bn), str(raw), "ours.dat"], cwd=tmp_path / "run", check=True)
+    want = tmp_path / "ref.dat"
+    oracle.ref_save_histogram(h, str(want))
+    assert (tmp_path / "results" / "ours.dat").read_bytes() == want.read_bytes()
