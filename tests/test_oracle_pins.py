@@ -300,3 +300,19 @@ def test_ref_3iso_analytic_ff_ref(tmp_path):
     got = oracle.ff_average_ref(dd, _cpu_rr(len(D), 250.0, dmax, nref, False), bins=bins,
                                 dmax=dmax)
     np.testing.assert_allclose(got, ffr, rtol=1e-10, atol=1e-10)
+
+
+def test_oracle_3ani_matches_reference_kernels():
+    """The anisotropic 3-point oracle against the reference's own plain 3ani
+    CUDA kernels (XXX3ani / XXY3ani, cuda/kernels/3ani_k.cuh:8,109), all bn^5
+    bins of DDD, RRR, DDR and DRR, from the committed fixture
+    (tests/golden/make_golden_3ani.py): bit-equal counts."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_3ani.npz"))
+    kw = dict(box=float(g["box"]), bins=int(g["bins"]), dmax=float(g["dmax"]))
+    D, R = g["D"], g["R"]
+    for name, x, y in (("DDD", D, None), ("RRR", R, None), ("DDR", D, R), ("DRR", R, D)):
+        got = oracle.triplets_ani(x, y, **kw)
+        want = g[name]
+        assert want.sum() > 1e6
+        assert np.array_equal(got, want), (name, float(np.abs(got - want).sum()))

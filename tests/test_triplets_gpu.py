@@ -98,6 +98,18 @@ def test_triplets_ani(ctx, bpc, w):
          oracle.triplets_ani(D, R, box=box, bins=bins, dmax=dmax, bpc=bpc), weighted)
 
 
+def test_triplets_ani_equal_reference_kernels(ctx):
+    """The GPU 3ani histograms (DDD, RRR, DDR, DRR) equal the reference's own
+    plain 3ani CUDA kernels bin for bin (committed fixture,
+    tests/golden/make_golden_3ani.py)."""
+    g = np.load(os.path.join(GOLDEN, "golden_3ani.npz"))
+    box, bins, dmax = float(g["box"]), int(g["bins"]), float(g["dmax"])
+    gd, gr = ctx.grid(g["D"], box), ctx.grid(g["R"], box)
+    for name, x, y in (("DDD", gd, None), ("RRR", gr, None), ("DDR", gd, gr), ("DRR", gr, gd)):
+        got = ctx.count_triplets(x, y, bins=bins, dmax=dmax, ani=True)
+        assert np.array_equal(got, g[name]), name
+
+
 def test_wide_histogram_through_grown_staging(ctx):
     """A 70^3 histogram (2.7 MB of doubles) is larger than a context's initial
     page-locked staging buffer: the buffer grows and the result still equals
