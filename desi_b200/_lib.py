@@ -19,6 +19,7 @@ PCF_RULE_EXCL_ZERO = 1 << 3
 PCF_RULE_INCLUSIVE = 1 << 4
 PCF_DEVICE_OUT = 1 << 5
 PCF_GRAPH = 1 << 7
+PCF_REF_NODE_GATES = 1 << 8
 PCF_ERR_TIMEOUT = -6
 (PCF_OPT_TRIP_FLUSH_BUDGET, PCF_OPT_ABORT_HOST_CHECK, PCF_OPT_PAIR_VARIANT, PCF_OPT_GRID_BUILD,
  PCF_OPT_GRID_DEFER) = 1, 2, 3, 4, 5

@@ -16,7 +16,7 @@ from . import _lib
 from ._lib import (PCF_ANI, PCF_BOTH, PCF_BPC, PCF_DEVICE_OUT, PCF_DS_EXACT,  # noqa: F401
                    PCF_ERR_TIMEOUT, PCF_GRAPH, PCF_ISO, PCF_OPT_ABORT_HOST_CHECK,
                    PCF_OPT_GRID_BUILD, PCF_OPT_GRID_DEFER, PCF_OPT_PAIR_VARIANT,
-                   PCF_OPT_TRIP_FLUSH_BUDGET,
+                   PCF_OPT_TRIP_FLUSH_BUDGET, PCF_REF_NODE_GATES,
                    PCF_RULE_CUSTOM, PCF_RULE_EXCL_ZERO, PCF_RULE_INCLUSIVE, PcfError, Stats)
 
 
@@ -142,12 +142,16 @@ class Context:
 
     def count_triplets(self, x: "Grid", y: "Grid | None" = None, *, bins: int, dmax: float,
                        ani: bool = False, bpc: bool = False, flags: int = 0,
-                       stats: bool = False, out_device_ptr: int | None = None):
+                       stats: bool = False, out_device_ptr: int | None = None,
+                       ref_gates: bool = False):
         """One triplet histogram (XXX with y None, else XXY); out_device_ptr:
-        write it to device memory without waiting for it (isotropic only)."""
+        write it to device memory without waiting for it (isotropic only).
+        ref_gates (periodic): count as the reference's periodic CUDA kernels
+        do on the node grid of the partitions the grids were built with
+        (PCF_REF_NODE_GATES)."""
         nb = bins ** 5 if ani else bins ** 3
         st = Stats()
-        f = flags | (PCF_BPC if bpc else 0)
+        f = flags | (PCF_BPC if bpc else 0) | (PCF_REF_NODE_GATES if ref_gates else 0)
         if out_device_ptr is not None:
             f |= PCF_DEVICE_OUT
             out, outp = None, ctypes.c_void_p(out_device_ptr)

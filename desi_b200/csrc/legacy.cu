@@ -135,9 +135,12 @@ void two_point(std::string *names, DNode *dD, PointW3D *pD, int nD, DNode *dR, P
     pcf_grid_free(S.ctx, gD);
 }
 
-// 3-point family: DDD, and RRR / DDR / DRR per random file.
+// 3-point family: DDD, and RRR / DDR / DRR per random file.  Periodic:
+// counted as the reference's kernels count on the caller's node grid
+// (PCF_REF_NODE_GATES, partitions = box / size_node).
 void three_point(std::string *names, DNode *dD, PointW3D *pD, int nD, DNode *dR, PointW3D *pR,
-                 int *nR, int *accR, int nrand, int bn, float box, float dmax, bool ani, bool bpc) {
+                 int *nR, int *accR, int nrand, int bn, float size_node, float box, float dmax, bool ani,
+                 bool bpc) {
     Session S;
     DevCat D;
     std::vector<DevCat> R((size_t)std::max(nrand, 0));
@@ -146,19 +149,20 @@ void three_point(std::string *names, DNode *dD, PointW3D *pD, int nD, DNode *dR,
         if (!device_catalog(dR, pR, accR[i], nR[i], R[i])) { S.check(PCF_ERR_CUDA, "node table"); return; }
     if (!bpc && !auto_box(D, R, box)) { S.check(PCF_ERR_CUDA, "box"); return; }
     const int kind = ani ? PCF_ANI : PCF_ISO;
-    const uint32_t f = bpc ? PCF_BPC : 0u;
+    const int parts = bpc && size_node > 0.f ? (int)std::lround(box / size_node) : 0;
+    const uint32_t f = bpc ? (PCF_BPC | (parts > 0 ? (uint32_t)PCF_REF_NODE_GATES : 0u)) : 0u;
     const std::string tag = std::string(ani ? "ani_" : "iso_") + (bpc ? "BPC_" : "");
     const size_t nb = ani ? (size_t)bn * bn * bn * bn * bn : (size_t)bn * bn * bn;
     std::vector<double> h(nb);
     auto save = [&](const std::string &n) { ani ? pcfio::save5d(n, bn, h.data()) : pcfio::save3d(n, bn, h.data()); };
     pcf_grid *gD = nullptr;
     auto pts = [](const DevCat &c) { return reinterpret_cast<const pcf_point *>(c.p); };
-    if (!S.check(pcf_grid_build(S.ctx, pts(D), D.n, box, 0, &gD), "grid")) return;
+    if (!S.check(pcf_grid_build(S.ctx, pts(D), D.n, box, parts, &gD), "grid")) return;
     if (S.check(pcf_count_triplets(S.ctx, kind, gD, nullptr, bn, dmax, f, h.data(), nullptr), "DDD"))
         save("DDD" + tag + names[0]);
     for (int i = 0; i < nrand && S.ok; ++i) {
         pcf_grid *gR = nullptr;
-        if (!S.check(pcf_grid_build(S.ctx, pts(R[i]), R[i].n, box, 0, &gR), "grid")) break;
+        if (!S.check(pcf_grid_build(S.ctx, pts(R[i]), R[i].n, box, parts, &gR), "grid")) break;
         if (S.check(pcf_count_triplets(S.ctx, kind, gR, nullptr, bn, dmax, f, h.data(), nullptr), "RRR"))
             save("RRR" + tag + names[i + 1]);
         if (S.check(pcf_count_triplets(S.ctx, kind, gD, gR, bn, dmax, f, h.data(), nullptr), "DDR"))
@@ -190,19 +194,19 @@ void pcf_2aniBPC(std::string *n, DNode *dD, PointW3D *pD, int nD, DNode *dR, Poi
 }
 void pcf_3iso(std::string *n, DNode *dD, PointW3D *pD, int nD, DNode *dR, PointW3D *pR, int *nR,
               int *aR, int nr, int bn, float, float dmax) {
-    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, 0.f, dmax, false, false);
+    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, 0.f, 0.f, dmax, false, false);
 }
 void pcf_3isoBPC(std::string *n, DNode *dD, PointW3D *pD, int nD, DNode *dR, PointW3D *pR,
-                 int *nR, int *aR, int nr, int bn, float, float box, float dmax) {
-    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, box, dmax, false, true);
+                 int *nR, int *aR, int nr, int bn, float size_node, float box, float dmax) {
+    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, size_node, box, dmax, false, true);
 }
 void pcf_3ani(std::string *n, DNode *dD, PointW3D *pD, int nD, DNode *dR, PointW3D *pR, int *nR,
               int *aR, int nr, int bn, float, float dmax) {
-    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, 0.f, dmax, true, false);
+    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, 0.f, 0.f, dmax, true, false);
 }
 void pcf_3aniBPC(std::string *n, DNode *dD, PointW3D *pD, int nD, DNode *dR, PointW3D *pR,
-                 int *nR, int *aR, int nr, int bn, float, float box, float dmax) {
-    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, box, dmax, true, true);
+                 int *nR, int *aR, int nr, int bn, float size_node, float box, float dmax) {
+    three_point(n, dD, pD, nD, dR, pR, nR, aR, nr, bn, size_node, box, dmax, true, true);
 }
 
 void pcf_2iso_BPCanalytic(std::string name, DNode *dD, PointW3D *pD, int nD, int bn, int np, float,

@@ -12,9 +12,14 @@
 // (bins^5, save_histogram5D) rather than their first bins^3 values; -p sets
 // the cells per box side, which the library uses when a periodic stencil
 // fits them (2*ceil(dmax/cell) + 2 <= P) and otherwise replaces with its own
-// choice (results do not depend on it); -rd counts RR and DR (3iso: DDD,
-// RRR, DDR, DRR) of every random catalog of the directory in one persistent
-// launch (pcf_batch_pairs, pcf_batch_triplets).
+// choice (pair results do not depend on it); -rd counts RR and DR (3iso:
+// DDD, RRR, DDR, DRR) of every random catalog of the directory in one
+// persistent launch (pcf_batch_pairs, pcf_batch_triplets).  Periodic
+// triplets (3iso / 3ani -bpc) count as the reference's CUDA kernels count on
+// their node grid of -p nodes per side (PCF_REF_NODE_GATES, whose gates miss
+// some triangles near the box edges), so the files match the reference's;
+// the added switch -exact counts every triangle in range once instead (the
+// reference's CPU engines' count).
 #include <dirent.h>
 
 #include <algorithm>
@@ -43,6 +48,8 @@ static void show_help() {
             "  -rd DIR/  uses every file of ../data/DIR/ as a random catalog\n"
             "  -bpc -a   isotropic only: RR / DDR / RRR from the analytic periodic formulas\n"
             "  -s BOX    box side (default: ceil(max coordinate + 1) over the files)\n"
+            "  -exact    3iso / 3ani -bpc: count every triangle in range once, not through\n"
+            "            the reference kernels' node gates on the -p grid\n"
             "Histograms are written to ../results/." << endl;
 }
 
@@ -72,6 +79,7 @@ int main(int argc, char **argv) {
     const string type = argv[1];
     int np = 0, bn = 0, partitions = 35;
     bool bpc = false, analytic = false, rand_dir = false, size_box_provided = false, rand_required = false;
+    bool exact = false;
     float size_box = 0, dmax = 0;
     string data_name, rand_name = "";
     for (int i = 2; i < argc; i++) {
@@ -85,6 +93,7 @@ int main(int argc, char **argv) {
         else if (strcmp(argv[i], "-d") == 0 && has) { dmax = std::stof(argv[++i]); }
         else if (strcmp(argv[i], "-bpc") == 0) { bpc = true; }
         else if (strcmp(argv[i], "-a") == 0) { analytic = true; }
+        else if (strcmp(argv[i], "-exact") == 0) { exact = true; }
         else if (strcmp(argv[i], "-p") == 0 && has) { partitions = (int)std::stof(argv[++i]); }
         else if (strcmp(argv[i], "-s") == 0 && has) { size_box = std::stof(argv[++i]); size_box_provided = true; }
     }
@@ -180,7 +189,8 @@ int main(int argc, char **argv) {
     } else {
         const bool ani = type == "3ani";
         const int kind = ani ? PCF_ANI : PCF_ISO;
-        const uint32_t f = bpc ? PCF_BPC : 0u;
+        const bool gated = bpc && !exact;
+        const uint32_t f = bpc ? (PCF_BPC | (gated ? (uint32_t)PCF_REF_NODE_GATES : 0u)) : 0u;
         const string sfx = ani ? "ani_" : "iso_";
         std::vector<double> h(ani ? b5 : b3);
         auto save = [&](const string &n) { ani ? pcfio::save5d(n, bn, h.data()) : pcfio::save3d(n, bn, h.data()); };
@@ -191,7 +201,7 @@ int main(int argc, char **argv) {
             pcfio::save3d("DDR" + sfx + tag + data_name, bn, ddr.data());
             pcfio::save3d("DRR" + sfx + tag + data_name, bn, ddr.data());  // pcf3isoBPC.cuh:340
             pcfio::save3d("RRR" + sfx + tag + data_name, bn, rrr.data());
-        } else if (!ani && gR.size() > 1) {
+        } else if (!ani && gR.size() > 1 && !gated) {
             // -rd: DDD, and RRR / DDR / DRR of every random catalog, in one
             // persistent launch (the reference launches per file,
             // cuda/pcf3iso.cuh:101-112)

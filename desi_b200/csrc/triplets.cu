@@ -30,6 +30,7 @@
 #include <type_traits>
 
 #include "pcf_internal.cuh"
+#include "node_gates.cuh"
 
 namespace {
 
@@ -84,6 +85,7 @@ struct TripArgs {
     // queue's [anchor_begin, anchor_begin + nX); mixed: XXY
     long long anchor_begin;
     int mixed;
+    GateGeom gate;  // the reference's node grid (PCF_REF_NODE_GATES)
 };
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -144,7 +146,7 @@ __device__ __forceinline__ int fast_bin(float d2, const TripCuts &c, int bins) {
 // XXY).  Entries: {dx, dy, dz, bits(idx << 8 | bin)}.
 // Angle bin of the anisotropic 3-point histograms for the side anchor->point:
 // t = (int)((1 + dz/d) * (float)(bins/2)) (3ani_k.cuh:79-91), dz signed, or
-// with periodic boxes dz = |z2-z1| - L*f (3aniBPC_k.cuh:18,34); -1 when >= bins.
+// with periodic boxes dz = |z2-z1| - L*f (3aniBPC_k.cuh:57,73); -1 when >= bins.
 __device__ __noinline__ int exact_angle(float ax, float ay, float az, float bx, float by, float bz,
                                         int bpc, float box, int bins, float ds_th) {
     double dx, dy, dz;
@@ -629,7 +631,12 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_batch(const __grid_co
 // for XXY every Y) neighbour with its exact side bin and angle bin, and all
 // ordered (j, k), j != k, are counted into the bins^5 histogram
 // [b(d12)][b(d31)][b(d23)][t12][t31] in global memory.
-template <bool MIXED, bool WEIGHTED>
+// GATES (periodic, PCF_REF_NODE_GATES): each ordered triangle counts as many
+// times as the reference's node-gate blocks count it (node_gates.cuh), on the
+// reference's node grid A.gate.  ISO3 (with GATES): the isotropic bins^3
+// histogram [b(d12)][b(d23)][b(d31)] of the same ordered triangles
+// (3isoBPC_k.cuh:191,940), from lists without angle bins.
+template <bool MIXED, bool WEIGHTED, bool GATES = false, bool ISO3 = false>
 __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int bins = A.rXX.bins;
@@ -665,11 +672,13 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
         const int cix = min(max((int)__fdiv_rn(hx, A.cell), 0), P - 1);
         const int ciy = min(max((int)__fdiv_rn(hy, A.cell), 0), P - 1);
         const int ciz = min(max((int)__fdiv_rn(hz, A.cell), 0), P - 1);
-        build_list<true>(A, A.X, hx, hy, hz, cix, ciy, ciz, -1, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
-                         A.capJ, &s_nJ, n_rechk, aJ);
+        build_list<!ISO3>(A, A.X, hx, hy, hz, cix, ciy, ciz, -1, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
+                          A.capJ, &s_nJ, n_rechk, aJ);
         if (MIXED)
-            build_list<true>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK,
-                             WEIGHTED ? swK : nullptr, A.capK, &s_nK, n_rechk, aK);
+            build_list<!ISO3>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK,
+                              WEIGHTED ? swK : nullptr, A.capK, &s_nK, n_rechk, aK);
+        float n1[3];
+        if (GATES) gate_corner(A.gate, hx, hy, hz, n1);
         __syncthreads();
         const int nJ = s_nJ, nK = MIXED ? s_nK : s_nJ;
         if (nJ > A.capJ || (MIXED && nK > A.capK)) {
@@ -684,9 +693,16 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
         for (int jj = warp; jj < nJ; jj += kTWarps) {
             const float4 ej = sJ[jj];
             const int jidx = (int)((unsigned)__float_as_int(ej.w) >> 8);
-            const unsigned short pj = aJ[jj];
-            const long long base = (long long)(pj & 255) * B4 + (long long)(pj >> 8) * B;
+            const unsigned short pj = ISO3 ? (unsigned short)(__float_as_int(ej.w) & 255) : aJ[jj];
+            const long long base = ISO3 ? (long long)pj * B2 : (long long)(pj & 255) * B4 + (long long)(pj >> 8) * B;
             const double wij = WEIGHTED ? (double)hw * (double)swJ[jj] : 1.0;
+            float n2[3];
+            unsigned s2 = 0;
+            if (GATES) {
+                const float xj = A.X.x[jidx], yj = A.X.y[jidx], zj = A.X.z[jidx];
+                gate_corner(A.gate, xj, yj, zj, n2);
+                s2 = gate_wrap(hx, hy, hz, xj, yj, zj, A.box);
+            }
             for (int kk = lane; kk < nK; kk += 32) {
                 if (!MIXED && kk == jj) continue;
                 const float4 ek = LK[kk];
@@ -702,11 +718,26 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
                                     CK.y[kidx], CK.z[kidx], A.bpc, A.box, r3);
                 }
                 if (c >= 0) {
-                    const unsigned short pk = AK[kk];
-                    const long long slot = base + (long long)(pk & 255) * B3 + (long long)c * B2 + (pk >> 8);
-                    ++n_tri;
-                    if (WEIGHTED) atomicAdd(A.g_wsum + slot, wij * (double)WK[kk]);
-                    else atomicAdd(A.g_count + slot, 1ull);
+                    int mult = 1;
+                    if (GATES) {
+                        const int kidx = (int)((unsigned)__float_as_int(ek.w) >> 8);
+                        const Cat &CK = MIXED ? A.Y : A.X;
+                        const float xk = CK.x[kidx], yk = CK.y[kidx], zk = CK.z[kidx];
+                        float n3[3];
+                        gate_corner(A.gate, xk, yk, zk, n3);
+                        mult = gate_mult(A.gate, n1, n2, n3, s2, gate_wrap(hx, hy, hz, xk, yk, zk, A.box));
+                        if (mult == 0) continue;
+                    }
+                    long long slot;
+                    if (ISO3) {
+                        slot = base + (long long)c * B + (__float_as_int(ek.w) & 255);
+                    } else {
+                        const unsigned short pk = AK[kk];
+                        slot = base + (long long)(pk & 255) * B3 + (long long)c * B2 + (pk >> 8);
+                    }
+                    n_tri += (unsigned long long)mult;
+                    if (WEIGHTED) atomicAdd(A.g_wsum + slot, wij * (double)WK[kk] * (double)mult);
+                    else atomicAdd(A.g_count + slot, (unsigned long long)mult);
                 }
             }
         }
@@ -861,12 +892,18 @@ static pcf_status trip_overflow(pcf_ctx *ctx, int64_t gmax, bool mixed, bool wei
     return PCF_OK;
 }
 
+static pcf_status count_triplets_ordered(pcf_ctx *ctx, const pcf_grid *x_, const pcf_grid *y_, int bins,
+                                         float dmax, uint32_t flags, double *hist, pcf_stats *stats,
+                                         bool iso3);
+
 extern "C" pcf_status pcf_count_triplets(pcf_ctx *ctx, int kind, const pcf_grid *x_,
                                          const pcf_grid *y_, int bins, float dmax, uint32_t flags,
                                          double *hist, pcf_stats *stats) {
     if (!ctx || !x_ || !hist || bins < 1 || !(dmax > 0.f)) return PCF_ERR_INVALID_ARG;
     if (kind == PCF_ANI) return pcf_count_triplets_ani(ctx, x_, y_, bins, dmax, flags, hist, stats);
     if (kind != PCF_ISO) return PCF_ERR_INVALID_ARG;
+    if (flags & PCF_REF_NODE_GATES)
+        return count_triplets_ordered(ctx, x_, y_, bins, dmax, flags, hist, stats, true);
     if (bins > 255 || (int64_t)bins * bins * bins > (1 << 26)) return PCF_ERR_UNSUPPORTED;
     cudaSetDevice(ctx->device);
     {
@@ -972,6 +1009,10 @@ extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const
         (!ddd && !rrr && !ddr && !drr))
         return PCF_ERR_INVALID_ARG;
     if (bins > 255 || (int64_t)bins * bins * bins > (1 << 26)) return PCF_ERR_UNSUPPORTED;
+    if (flags & PCF_REF_NODE_GATES) {
+        ctx->last_error = "PCF_REF_NODE_GATES counts run per call (pcf_count_triplets)";
+        return PCF_ERR_UNSUPPORTED;
+    }
     if (ctx_abort_requested(ctx) != PCF_OK) return PCF_ERR_TIMEOUT;
     cudaSetDevice(ctx->device);
     {
@@ -1149,10 +1190,25 @@ extern "C" pcf_status pcf_batch_triplets(pcf_ctx *ctx, const pcf_grid *d_, const
 // Anisotropic triplets (bins^5).  The histogram lives in global memory (u64
 // counts or FP64 sums); lists stay in shared memory (an anchor whose lists
 // do not fit makes the call fail with PCF_ERR_UNSUPPORTED).
-pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_grid *y_, int bins,
-                                  float dmax, uint32_t flags, double *hist, pcf_stats *stats) {
-    if (bins > 255 || (int64_t)bins * bins * bins * bins * bins > ((int64_t)1 << 31))
-        return PCF_ERR_UNSUPPORTED;
+// Ordered-triangle counts through k_triplets_ani: the bins^5 anisotropic
+// histogram, or (iso3, with PCF_REF_NODE_GATES) the bins^3 isotropic one.
+static pcf_status count_triplets_ordered(pcf_ctx *ctx, const pcf_grid *x_, const pcf_grid *y_, int bins,
+                                         float dmax, uint32_t flags, double *hist, pcf_stats *stats,
+                                         bool iso3) {
+    const int64_t nh = iso3 ? (int64_t)bins * bins * bins : (int64_t)bins * bins * bins * bins * bins;
+    if (bins > 255 || nh > ((int64_t)1 << 31)) return PCF_ERR_UNSUPPORTED;
+    const bool gates = (flags & PCF_REF_NODE_GATES) != 0;
+    if (gates) {
+        if (!(flags & PCF_BPC)) {
+            ctx->last_error = "PCF_REF_NODE_GATES applies to periodic counts (PCF_BPC)";
+            return PCF_ERR_INVALID_ARG;
+        }
+        if (x_->user_P < 1 || (y_ && (y_->user_P != x_->user_P || y_->box != x_->box))) {
+            ctx->last_error = "PCF_REF_NODE_GATES: the reference's node grid is the partitions given to "
+                              "pcf_grid_build, the same for both grids";
+            return PCF_ERR_INVALID_ARG;
+        }
+    }
     cudaSetDevice(ctx->device);
     {
         pcf_status s0 = grid_finish(ctx, x_);
@@ -1189,6 +1245,7 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     A.rXY = rXY;
     A.ctrl = ctx->d_abort;
     A.status = ctx->d_status;
+    if (gates) A.gate = gate_geometry(X->box, dmax, X->user_P);
     {
         const double dd = rXX.dd;
         const double rmax = (double)dmax * rXX.ds + 1.0;
@@ -1212,7 +1269,7 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
         A.capK = 0;
     }
     const size_t smem = (size_t)(A.capJ + A.capK) * ent + 64;
-    const int64_t n5 = (int64_t)bins * bins * bins * bins * bins;
+    const int64_t n5 = nh;
     PlanSlot *sl = nullptr;
     s = stage_plan(ctx, plan, &sl);
     if (s != PCF_OK) return s;
@@ -1225,8 +1282,16 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
     A.g_stats = reinterpret_cast<unsigned long long *>(hp + (size_t)n5 * 8);
     double *d_out = reinterpret_cast<double *>(hp + (size_t)n5 * 8 + 128);
     PCF_CU(ctx, cudaMemsetAsync(hp, 0, (size_t)n5 * 8 + 128, ctx->stream));
-    auto kfn = mixed ? (weighted ? k_triplets_ani<true, true> : k_triplets_ani<true, false>)
-                     : (weighted ? k_triplets_ani<false, true> : k_triplets_ani<false, false>);
+    void (*kfn)(const TripArgs);
+    if (iso3)
+        kfn = mixed ? (weighted ? k_triplets_ani<true, true, true, true> : k_triplets_ani<true, false, true, true>)
+                    : (weighted ? k_triplets_ani<false, true, true, true> : k_triplets_ani<false, false, true, true>);
+    else if (gates)
+        kfn = mixed ? (weighted ? k_triplets_ani<true, true, true> : k_triplets_ani<true, false, true>)
+                    : (weighted ? k_triplets_ani<false, true, true> : k_triplets_ani<false, false, true>);
+    else
+        kfn = mixed ? (weighted ? k_triplets_ani<true, true> : k_triplets_ani<true, false>)
+                    : (weighted ? k_triplets_ani<false, true> : k_triplets_ani<false, false>);
     PCF_CU(ctx, ensure_smem_limit(reinterpret_cast<const void *>(kfn), ctx->device, smem));
     PCF_CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     kfn<<<ctx->sm_count, kTThreads, smem, ctx->stream>>>(A);
@@ -1260,4 +1325,9 @@ pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_gr
         stats->work_items = (int)X->n;
     }
     return PCF_OK;
+}
+
+pcf_status pcf_count_triplets_ani(pcf_ctx *ctx, const pcf_grid *x_, const pcf_grid *y_, int bins,
+                                  float dmax, uint32_t flags, double *hist, pcf_stats *stats) {
+    return count_triplets_ordered(ctx, x_, y_, bins, dmax, flags, hist, stats, false);
 }

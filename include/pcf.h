@@ -76,9 +76,21 @@ enum {
     PCF_RULE_INCLUSIVE = 1u << 4, /* d^2 <= dmax^2 instead of <                        */
     PCF_DEVICE_OUT = 1u << 5,  /* hist points to device memory; the call returns
                                   without synchronising the context stream           */
-    PCF_GRAPH = 1u << 7        /* pcf_batch_pairs: capture the launch in a CUDA graph the
+    PCF_GRAPH = 1u << 7,       /* pcf_batch_pairs: capture the launch in a CUDA graph the
                                   first time and replay it on later calls with the same
                                   grids and parameters                               */
+    PCF_REF_NODE_GATES = 1u << 8 /* periodic triplet counts (PCF_BPC): count each ordered
+                                  triangle as many times as the reference's periodic CUDA
+                                  kernels do (XXX3iso_BPC / XXY3iso_BPC, 3isoBPC_k.cuh:191,940;
+                                  XXX3ani_BPC / XXY3ani_BPC, 3aniBPC_k.cuh:210,959) on their
+                                  node grid of box / partitions, partitions being the value
+                                  given to pcf_grid_build (nonzero, the same for x and y).
+                                  Those kernels gate node triples per periodic image case and
+                                  five of their 64 gates differ from the geometry, so they
+                                  miss some triangles near box edges and count a few twice;
+                                  this flag reproduces that count (PCF.out's 3iso / 3ani
+                                  -bpc).  Without it every triangle in range is counted once,
+                                  as the reference's CPU engines count it.              */
 };
 
 /* Counters a counting call can report (any pointer argument may be NULL). */

@@ -51,10 +51,10 @@ def _load():
     lib.orc_pairs_m.argtypes = lib.orc_pairs.argtypes + [ctypes.c_int]
     lib.orc_triplets_iso.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _fptr,
                                      ctypes.c_long, _fptr, ctypes.c_long, ctypes.c_float,
-                                     ctypes.c_int, ctypes.c_float, _dptr]
+                                     ctypes.c_int, ctypes.c_float, ctypes.c_int, _dptr]
     lib.orc_triplets_ani.argtypes = [ctypes.c_int, ctypes.c_int, _fptr, ctypes.c_long,
                                      _fptr, ctypes.c_long, ctypes.c_float, ctypes.c_int,
-                                     ctypes.c_float, _dptr]
+                                     ctypes.c_float, ctypes.c_int, _dptr]
     lib.orc_analytic_rr.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_int, _dptr]
     lib.orc_analytic_3iso.argtypes = [_fptr, ctypes.c_long, ctypes.c_float, ctypes.c_int,
@@ -144,24 +144,31 @@ def reference_rule(*, ani: bool, bpc: bool, cross: bool) -> int:
 
 
 def triplets_iso(X, Y=None, *, box: float, bins: int, dmax: float, bpc: bool = False,
-                 prec: int = FP64):
+                 prec: int = FP64, ref_gates: int = 0):
+    """ref_gates > 0 (periodic only): count each ordered triangle as often as
+    the reference's periodic CUDA node gates do on a grid of ref_gates nodes
+    per side (3isoBPC_k.cuh:191,940), its gate defects included."""
     X = _pts(X)
     mixed = Y is not None
     Yp = _pts(Y) if mixed else X
     out = np.zeros(bins ** 3, np.float64)
     rc = lib().orc_triplets_iso(int(bpc), int(mixed), prec, _p(X), len(X), _p(Yp), len(Yp),
-                                box, bins, dmax, _d(out))
+                                box, bins, dmax, int(ref_gates), _d(out))
     assert rc == 0
     return out.reshape(bins, bins, bins)
 
 
-def triplets_ani(X, Y=None, *, box: float, bins: int, dmax: float, bpc: bool = False):
+def triplets_ani(X, Y=None, *, box: float, bins: int, dmax: float, bpc: bool = False,
+                 ref_gates: int = 0):
+    """ref_gates > 0 (periodic only): count each ordered triangle as often as
+    the reference's periodic node gates do on a grid of ref_gates nodes per
+    side (3aniBPC_k.cuh:210,959), its gate defects included."""
     X = _pts(X)
     mixed = Y is not None
     Yp = _pts(Y) if mixed else X
     out = np.zeros(bins ** 5, np.float64)
     rc = lib().orc_triplets_ani(int(bpc), int(mixed), _p(X), len(X), _p(Yp), len(Yp), box,
-                                bins, dmax, _d(out))
+                                bins, dmax, int(ref_gates), _d(out))
     assert rc == 0
     return out.reshape((bins,) * 5)
 
@@ -373,3 +380,27 @@ def available_ref_engines():
     if not os.path.isdir(d):
         return []
     return sorted(f[len("libref_"):-3] for f in os.listdir(d) if f.startswith("libref_"))
+
+def ref_kernels_3pt(D, R=None, *, ani: bool, bpc: bool, box: float, bins: int, dmax: float,
+                    partitions: int):
+    """The reference's own 3-point CUDA kernels (XXX3iso/XXY3iso,
+    XXX3iso_BPC/XXY3iso_BPC, XXX3ani/XXY3ani, XXX3ani_BPC/XXY3ani_BPC in
+    cuda/kernels/3{iso,ani}{,BPC}_k.cuh) compiled for the host
+    (_ref/libref_3pt_host.so, ref_3pt_host.cpp), on nodes of box/partitions:
+    {"DDD": ...} or, with R, {"DDD", "RRR", "DDR", "DRR"}, each bins^3 (iso)
+    or bins^5 (ani).  Unit weights only (see ref_3pt_host.cpp)."""
+    path = os.path.join(HERE, "_ref", "libref_3pt_host.so")
+    lib = ctypes.CDLL(path)
+    lib.ref3_hist.argtypes = [ctypes.c_int, ctypes.c_int, _fptr, ctypes.c_int, _fptr, ctypes.c_int,
+                              ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_float, _dptr]
+    D = _pts(D)
+    Rp = _pts(R) if R is not None else None
+    shape = (bins,) * (5 if ani else 3)
+    nb = int(np.prod(shape))
+    out = np.zeros(nb * (4 if Rp is not None else 1), np.float64)
+    rc = lib.ref3_hist(int(ani), int(bpc), _p(D), len(D), _p(Rp) if Rp is not None else None,
+                       len(Rp) if Rp is not None else 0, bins, dmax, partitions, box, _d(out))
+    if rc != 0:
+        raise ValueError(f"ref3_hist returned {rc} (a coordinate outside the node grid?)")
+    names = ("DDD", "RRR", "DDR", "DRR") if Rp is not None else ("DDD",)
+    return {k: out[i * nb:(i + 1) * nb].reshape(shape) for i, k in enumerate(names)}

@@ -16,6 +16,8 @@
  *   cuda/kernels/3isoBPC_k.cuh:1694-2119 DD2iso_forBPC, make_ff_av(_ref),
  *                                        make_histo_analitic
  *   cuda/kernels/3ani_k.cuh:8-209        XXX3ani / XXY3ani
+ *   cuda/kernels/3aniBPC_k.cuh:8-207     count123_ani / count123_animixed
+ *                                        (XXX3ani_BPC / XXY3ani_BPC)
  *   cuda/pcf2isoBPC.cuh:199-202, cuda/pcf3isoBPC.cuh:233-247 (constants)
  *
  * Canonical (FP64) rule, shared with the CUDA library:
@@ -393,6 +395,180 @@ static nbr_t *neighbours(const opt *p, const opt *Q, long j0, long nQ, int bpc, 
     return a;
 }
 
+/* ----------------------------------------------------------------------- */
+/* The reference's periodic 3-point node gates (3aniBPC_k.cuh:210-957        */
+/* XXX3ani_BPC, :959-1708 XXY3ani_BPC; 3isoBPC_k.cuh:191-939, 940-1693 hold   */
+/* the same 64 blocks).  Each thread takes one ordered node triple           */
+/* (n1, n2, n3) of the reference's grid (size s = box / partitions, node     */
+/* corner = (float)(int)(x / s) * s, create_grid.cuh:120-135) and runs the   */
+/* point loop once per block whose gate passes, with that block's image      */
+/* flags F2 (node 2 seen through its x/y/z image) and F3.  A triangle in     */
+/* range through the images (S2, S3) of its sides 12 and 31 is therefore     */
+/* counted once per passing block with (F2, F3) == (S2, S3).  A gate needs   */
+/* the edge flags A2 / A3 (fa_k: nodes 1 and k within dmax + s of opposite   */
+/* faces along a) and up to three node-distance tests, pair p in {12, 23,    */
+/* 31}:  dd_p + k*L^2 - 2*(sum of dn_p over the listed axes)*L <= M,         */
+/* M = (dmax + s*sqrt(3))^2, k = 0 with no axes meaning dd_p <= M.           */
+/* The table is the reference's blocks in source order, as written there:    */
+/* four same-image blocks (xy, xz, yz, xyz) test 23 through the image where  */
+/* 31 is meant, block (F2 = x, A2 = y, F3 = xyz) is gated for node 2's y     */
+/* image but counts with its x image (no block counts S2 = y, S3 = xyz),     */
+/* block (xy, z) sums dz23 twice, block (xyz, xz) adds 3L^2 for one axis.    */
+/* Gates evaluate in FP32 with the multiply-adds fused, the reference's      */
+/* kernels being built with contraction on; exact whenever the node corners  */
+/* and their sums are exact (e.g. integer lattices).                          */
+/* ----------------------------------------------------------------------- */
+typedef struct { signed char pair, k, ax[3]; } gate_test;
+typedef struct { unsigned char f2, f3, a2, a3; gate_test t[3]; } gate_block;
+static const gate_block kGates[64] = {
+    {0, 0, 0, 0, {{0, 0, {-1, -1, -1}}, {1, 0, {-1, -1, -1}}, {2, 0, {-1, -1, -1}}}},
+    {0, 1, 0, 1, {{0, 0, {-1, -1, -1}}, {1, 1, {0, -1, -1}}, {2, 1, {0, -1, -1}}}},
+    {0, 2, 0, 2, {{0, 0, {-1, -1, -1}}, {1, 1, {1, -1, -1}}, {2, 1, {1, -1, -1}}}},
+    {0, 4, 0, 4, {{0, 0, {-1, -1, -1}}, {1, 1, {2, -1, -1}}, {2, 1, {2, -1, -1}}}},
+    {0, 3, 0, 3, {{0, 0, {-1, -1, -1}}, {1, 2, {0, 1, -1}}, {2, 2, {0, 1, -1}}}},
+    {0, 5, 0, 5, {{0, 0, {-1, -1, -1}}, {1, 2, {0, 2, -1}}, {2, 2, {0, 2, -1}}}},
+    {0, 6, 0, 6, {{0, 0, {-1, -1, -1}}, {1, 2, {1, 2, -1}}, {2, 2, {1, 2, -1}}}},
+    {0, 7, 0, 7, {{0, 0, {-1, -1, -1}}, {1, 3, {0, 1, 2}}, {2, 3, {0, 1, 2}}}},
+    {1, 0, 1, 0, {{2, 0, {-1, -1, -1}}, {1, 1, {0, -1, -1}}, {0, 1, {0, -1, -1}}}},
+    {2, 0, 2, 0, {{2, 0, {-1, -1, -1}}, {1, 1, {1, -1, -1}}, {0, 1, {1, -1, -1}}}},
+    {4, 0, 4, 0, {{2, 0, {-1, -1, -1}}, {1, 1, {2, -1, -1}}, {0, 1, {2, -1, -1}}}},
+    {3, 0, 3, 0, {{2, 0, {-1, -1, -1}}, {1, 2, {0, 1, -1}}, {0, 2, {0, 1, -1}}}},
+    {5, 0, 5, 0, {{2, 0, {-1, -1, -1}}, {1, 2, {0, 2, -1}}, {0, 2, {0, 2, -1}}}},
+    {6, 0, 6, 0, {{2, 0, {-1, -1, -1}}, {1, 2, {1, 2, -1}}, {0, 2, {1, 2, -1}}}},
+    {7, 0, 7, 0, {{2, 0, {-1, -1, -1}}, {1, 3, {0, 1, 2}}, {0, 3, {0, 1, 2}}}},
+    {1, 1, 1, 1, {{1, 0, {-1, -1, -1}}, {2, 1, {0, -1, -1}}, {0, 1, {0, -1, -1}}}},
+    {2, 2, 2, 2, {{1, 0, {-1, -1, -1}}, {2, 1, {1, -1, -1}}, {0, 1, {1, -1, -1}}}},
+    {4, 4, 4, 4, {{1, 0, {-1, -1, -1}}, {2, 1, {2, -1, -1}}, {0, 1, {2, -1, -1}}}},
+    {3, 3, 3, 3, {{1, 0, {-1, -1, -1}}, {1, 2, {0, 1, -1}}, {0, 2, {0, 1, -1}}}},
+    {5, 5, 5, 5, {{1, 0, {-1, -1, -1}}, {1, 2, {0, 2, -1}}, {0, 2, {0, 2, -1}}}},
+    {6, 6, 6, 6, {{1, 0, {-1, -1, -1}}, {1, 2, {1, 2, -1}}, {0, 2, {1, 2, -1}}}},
+    {7, 7, 7, 7, {{1, 0, {-1, -1, -1}}, {1, 3, {0, 1, 2}}, {0, 3, {0, 1, 2}}}},
+    {1, 2, 1, 2, {{0, 1, {0, -1, -1}}, {2, 1, {1, -1, -1}}, {1, 2, {0, 1, -1}}}},
+    {1, 4, 1, 4, {{0, 1, {0, -1, -1}}, {2, 1, {2, -1, -1}}, {1, 2, {0, 2, -1}}}},
+    {1, 3, 1, 3, {{0, 1, {0, -1, -1}}, {2, 2, {0, 1, -1}}, {1, 1, {1, -1, -1}}}},
+    {1, 5, 1, 5, {{0, 1, {0, -1, -1}}, {2, 2, {0, 2, -1}}, {1, 1, {2, -1, -1}}}},
+    {1, 6, 1, 6, {{0, 1, {0, -1, -1}}, {2, 2, {1, 2, -1}}, {1, 3, {0, 1, 2}}}},
+    {1, 7, 1, 7, {{0, 1, {0, -1, -1}}, {2, 3, {0, 1, 2}}, {1, 2, {1, 2, -1}}}},
+    {2, 1, 2, 1, {{0, 1, {1, -1, -1}}, {2, 1, {0, -1, -1}}, {1, 2, {0, 1, -1}}}},
+    {2, 4, 2, 4, {{0, 1, {1, -1, -1}}, {2, 1, {2, -1, -1}}, {1, 2, {1, 2, -1}}}},
+    {2, 3, 2, 3, {{0, 1, {1, -1, -1}}, {2, 2, {0, 1, -1}}, {1, 1, {0, -1, -1}}}},
+    {2, 5, 2, 5, {{0, 1, {1, -1, -1}}, {2, 2, {0, 2, -1}}, {1, 3, {0, 1, 2}}}},
+    {2, 6, 2, 6, {{0, 1, {1, -1, -1}}, {2, 2, {1, 2, -1}}, {1, 1, {2, -1, -1}}}},
+    {1, 7, 2, 7, {{0, 1, {1, -1, -1}}, {2, 3, {0, 1, 2}}, {1, 2, {0, 2, -1}}}},
+    {4, 1, 4, 1, {{0, 1, {2, -1, -1}}, {2, 1, {0, -1, -1}}, {1, 2, {0, 2, -1}}}},
+    {4, 2, 4, 2, {{0, 1, {2, -1, -1}}, {2, 1, {1, -1, -1}}, {1, 2, {1, 2, -1}}}},
+    {4, 3, 4, 3, {{0, 1, {2, -1, -1}}, {2, 2, {0, 1, -1}}, {1, 3, {0, 1, 2}}}},
+    {4, 5, 4, 5, {{0, 1, {2, -1, -1}}, {2, 2, {0, 2, -1}}, {1, 1, {0, -1, -1}}}},
+    {4, 6, 4, 6, {{0, 1, {2, -1, -1}}, {2, 2, {1, 2, -1}}, {1, 1, {1, -1, -1}}}},
+    {4, 7, 4, 7, {{0, 1, {2, -1, -1}}, {2, 3, {0, 1, 2}}, {1, 2, {0, 1, -1}}}},
+    {3, 1, 3, 1, {{0, 2, {0, 1, -1}}, {2, 1, {0, -1, -1}}, {1, 1, {1, -1, -1}}}},
+    {3, 2, 3, 2, {{0, 2, {0, 1, -1}}, {2, 1, {1, -1, -1}}, {1, 1, {0, -1, -1}}}},
+    {3, 4, 3, 4, {{0, 2, {0, 1, -1}}, {2, 1, {2, -1, -1}}, {1, 3, {2, 1, 2}}}},
+    {3, 5, 3, 5, {{0, 2, {0, 1, -1}}, {2, 2, {0, 2, -1}}, {1, 2, {1, 2, -1}}}},
+    {3, 6, 3, 6, {{0, 2, {0, 1, -1}}, {2, 2, {1, 2, -1}}, {1, 2, {0, 2, -1}}}},
+    {3, 7, 3, 7, {{0, 2, {0, 1, -1}}, {2, 3, {0, 1, 2}}, {1, 1, {2, -1, -1}}}},
+    {5, 1, 5, 1, {{0, 2, {0, 2, -1}}, {2, 1, {0, -1, -1}}, {1, 1, {2, -1, -1}}}},
+    {5, 2, 5, 2, {{0, 2, {0, 2, -1}}, {2, 1, {1, -1, -1}}, {1, 3, {0, 1, 2}}}},
+    {5, 4, 5, 4, {{0, 2, {0, 2, -1}}, {2, 1, {2, -1, -1}}, {1, 1, {0, -1, -1}}}},
+    {5, 3, 5, 3, {{0, 2, {0, 2, -1}}, {2, 2, {0, 1, -1}}, {1, 2, {1, 2, -1}}}},
+    {5, 6, 5, 6, {{0, 2, {0, 2, -1}}, {2, 2, {1, 2, -1}}, {1, 2, {0, 1, -1}}}},
+    {5, 7, 5, 7, {{0, 2, {0, 2, -1}}, {2, 3, {0, 1, 2}}, {1, 1, {1, -1, -1}}}},
+    {6, 1, 6, 1, {{0, 2, {2, 1, -1}}, {2, 1, {0, -1, -1}}, {1, 3, {0, 1, 2}}}},
+    {6, 2, 6, 2, {{0, 2, {2, 1, -1}}, {2, 1, {1, -1, -1}}, {1, 1, {2, -1, -1}}}},
+    {6, 4, 6, 4, {{0, 2, {2, 1, -1}}, {2, 1, {2, -1, -1}}, {1, 1, {1, -1, -1}}}},
+    {6, 3, 6, 3, {{0, 2, {2, 1, -1}}, {2, 2, {0, 1, -1}}, {1, 2, {0, 2, -1}}}},
+    {6, 5, 6, 5, {{0, 2, {2, 1, -1}}, {2, 2, {0, 2, -1}}, {1, 2, {0, 1, -1}}}},
+    {6, 7, 6, 7, {{0, 2, {2, 1, -1}}, {2, 3, {0, 1, 2}}, {1, 1, {0, -1, -1}}}},
+    {7, 1, 7, 1, {{0, 3, {0, 1, 2}}, {2, 1, {0, -1, -1}}, {1, 2, {1, 2, -1}}}},
+    {7, 2, 7, 2, {{0, 3, {0, 1, 2}}, {2, 1, {1, -1, -1}}, {1, 2, {0, 2, -1}}}},
+    {7, 4, 7, 4, {{0, 3, {0, 1, 2}}, {2, 1, {2, -1, -1}}, {1, 2, {0, 1, -1}}}},
+    {7, 3, 7, 3, {{0, 3, {0, 1, 2}}, {2, 2, {0, 1, -1}}, {1, 1, {2, -1, -1}}}},
+    {7, 5, 7, 5, {{0, 3, {0, 1, 2}}, {2, 2, {0, 2, -1}}, {1, 3, {1, -1, -1}}}},
+    {7, 6, 7, 6, {{0, 3, {0, 1, 2}}, {2, 2, {1, 2, -1}}, {1, 1, {0, -1, -1}}}},
+};
+
+typedef struct {
+    float s, L, L2, M, fd, fdn;
+    int P;
+} gate_geom;
+
+static gate_geom gate_setup(float L, float dmax, int P)
+{
+    gate_geom g;
+    g.P = P;
+    g.s = L / (float)P;                                 /* main.cu:216 */
+    g.L = L;
+    g.L2 = L * L;
+    float dmn = (float)((double)dmax + (double)g.s * sqrt(3.0)); /* pcf3aniBPC.cuh:59-60 */
+    g.M = dmn * dmn;
+    g.fd = dmax + g.s;
+    g.fdn = L - g.fd;
+    return g;
+}
+
+static inline void gate_corner(const gate_geom *g, const opt *p, float n[3])
+{
+    const float c[3] = {p->x, p->y, p->z};
+    for (int a = 0; a < 3; ++a) {
+        int r = (int)(c[a] / g->s);
+        if (r > g->P - 1) r = g->P - 1;
+        if (r < 0) r = 0;
+        n[a] = (float)r * g->s;
+    }
+}
+
+static inline unsigned wrap_bits(const opt *p, const opt *q, double L)
+{
+    const double d[3] = {(double)q->x - (double)p->x, (double)q->y - (double)p->y,
+                         (double)q->z - (double)p->z};
+    unsigned b = 0;
+    for (int a = 0; a < 3; ++a)
+        if (d[a] > 0.5 * L || d[a] < -0.5 * L) b |= 1u << a;
+    return b;
+}
+
+/* Number of reference blocks that count the ordered triangle (1, 2, 3) with
+ * node corners n1, n2, n3 whose sides 12 and 31 are in range through the
+ * images s2, s3. */
+static int gate_mult(const gate_geom *g, const float n1[3], const float n2[3], const float n3[3],
+                     unsigned s2, unsigned s3)
+{
+    float dn[3][3], dd[3];
+    for (int a = 0; a < 3; ++a) {
+        dn[0][a] = fabsf(n2[a] - n1[a]);
+        dn[1][a] = fabsf(n3[a] - n2[a]);
+        dn[2][a] = fabsf(n1[a] - n3[a]);
+    }
+    for (int q = 0; q < 3; ++q)
+        dd[q] = fmaf(dn[q][2], dn[q][2], fmaf(dn[q][1], dn[q][1], dn[q][0] * dn[q][0]));
+    unsigned f2 = 0, f3 = 0;
+    for (int a = 0; a < 3; ++a) {
+        if ((n1[a] <= g->fd && n2[a] >= g->fdn) || (n2[a] <= g->fd && n1[a] >= g->fdn)) f2 |= 1u << a;
+        if ((n1[a] <= g->fd && n3[a] >= g->fdn) || (n3[a] <= g->fd && n1[a] >= g->fdn)) f3 |= 1u << a;
+    }
+    int m = 0;
+    for (int b = 0; b < 64; ++b) {
+        const gate_block *B = &kGates[b];
+        if (B->f2 != s2 || B->f3 != s3) continue;
+        if ((f2 & B->a2) != B->a2 || (f3 & B->a3) != B->a3) continue;
+        int ok = 1;
+        for (int t = 0; t < 3 && ok; ++t) {
+            const gate_test *T = &B->t[t];
+            float v = dd[T->pair];
+            if (T->ax[0] >= 0) {
+                float sm = dn[T->pair][T->ax[0]];
+                if (T->ax[1] >= 0) sm = sm + dn[T->pair][T->ax[1]];
+                if (T->ax[2] >= 0) sm = sm + dn[T->pair][T->ax[2]];
+                v = fmaf((float)T->k, g->L2, v);
+                v = fmaf(-(2.0f * sm), g->L, v);
+            }
+            ok = v <= g->M;
+        }
+        m += ok;
+    }
+    return m;
+}
+
 /*
  * mixed == 0: XXX over X (all three sides: 0 < d2 < dd_max).
  * mixed != 0: XXY with points 1,2 from X and point 3 from Y; side 12 needs
@@ -401,9 +577,11 @@ static nbr_t *neighbours(const opt *p, const opt *Q, long j0, long nQ, int bpc, 
  * out: bins^3 doubles, overwritten.
  */
 int orc_triplets_iso(int bpc, int mixed, int prec, const opt *X, long nX, const opt *Y, long nY,
-                     float L, int bins, float dmax, double *out)
+                     float L, int bins, float dmax, int gate_P, double *out)
 {
     if (bpc) prec = ORC_FP64; /* FP32 emulation covers the plain kernels only */
+    const int gated = bpc && gate_P > 0;
+    gate_geom gg = gate_setup(L, dmax, gated ? gate_P : 1);
     const long nb = (long)bins * bins * bins;
     const double ds = orc_ds(bins, dmax, 0);
     const float ddf = dmax * dmax;
@@ -436,12 +614,26 @@ int orc_triplets_iso(int bpc, int mixed, int prec, const opt *X, long nX, const 
                         if (bjk < 0) continue;
                         double w = wij * (double)X[r->idx].w;
                         long A = q->bin, Bb = bjk, C = r->bin; /* (ij, jk, ki) */
-                        h[A * b2 + Bb * bins + C] += w;
-                        h[Bb * b2 + C * bins + A] += w;
-                        h[C * b2 + A * bins + Bb] += w;
-                        h[C * b2 + Bb * bins + A] += w;
-                        h[Bb * b2 + A * bins + C] += w;
-                        h[A * b2 + C * bins + Bb] += w;
+                        /* orderings (1,2,3): (i,q,r) (q,r,i) (r,i,q) (i,r,q) (r,q,i) (q,i,r) */
+                        double m[6] = {1, 1, 1, 1, 1, 1};
+                        if (gated) {
+                            const opt *P3[3] = {p, &X[q->idx], &X[r->idx]};
+                            float nc[3][3];
+                            for (int u = 0; u < 3; ++u) gate_corner(&gg, P3[u], nc[u]);
+                            static const int ord[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1},
+                                                          {0, 2, 1}, {2, 1, 0}, {1, 0, 2}};
+                            for (int o = 0; o < 6; ++o) {
+                                const int u = ord[o][0], t2 = ord[o][1], t3 = ord[o][2];
+                                m[o] = gate_mult(&gg, nc[u], nc[t2], nc[t3], wrap_bits(P3[u], P3[t2], Ld),
+                                                 wrap_bits(P3[u], P3[t3], Ld));
+                            }
+                        }
+                        h[A * b2 + Bb * bins + C] += w * m[0];
+                        h[Bb * b2 + C * bins + A] += w * m[1];
+                        h[C * b2 + A * bins + Bb] += w * m[2];
+                        h[C * b2 + Bb * bins + A] += w * m[3];
+                        h[Bb * b2 + A * bins + C] += w * m[4];
+                        h[A * b2 + C * bins + Bb] += w * m[5];
                     }
                 }
             } else {
@@ -457,8 +649,20 @@ int orc_triplets_iso(int bpc, int mixed, int prec, const opt *X, long nX, const 
                         if (bjk < 0) continue;
                         double w = wij * (double)Y[r->idx].w;
                         long A = q->bin, Bb = bjk, C = r->bin;
-                        h[A * b2 + Bb * bins + C] += w;
-                        h[A * b2 + C * bins + Bb] += w;
+                        /* orderings (1,2,3): (i,q,r) and (q,i,r), point 3 from Y */
+                        double m0 = 1, m1 = 1;
+                        if (gated) {
+                            float c1[3], c2[3], c3[3];
+                            gate_corner(&gg, p, c1);
+                            gate_corner(&gg, &X[q->idx], c2);
+                            gate_corner(&gg, &Y[r->idx], c3);
+                            m0 = gate_mult(&gg, c1, c2, c3, wrap_bits(p, &X[q->idx], Ld),
+                                           wrap_bits(p, &Y[r->idx], Ld));
+                            m1 = gate_mult(&gg, c2, c1, c3, wrap_bits(&X[q->idx], p, Ld),
+                                           wrap_bits(&X[q->idx], &Y[r->idx], Ld));
+                        }
+                        h[A * b2 + Bb * bins + C] += w * m0;
+                        h[A * b2 + C * bins + Bb] += w * m1;
                     }
                 }
                 free(N3);
@@ -475,7 +679,7 @@ int orc_triplets_iso(int bpc, int mixed, int prec, const opt *X, long nX, const 
 /* ----------------------------------------------------------------------- */
 /* Triplets (anisotropic, bins^5): a=b(d12), b=b(d31), c=b(d23),            */
 /* With periodic boundaries the reference folds the sign of dz:             */
-/* dz = |z2 - z1| - L*f (3aniBPC_k.cuh:18,34), f = 1 when the pair uses its */
+/* dz = |z2 - z1| - L*f (3aniBPC_k.cuh:57,73), f = 1 when the pair uses its */
 /* z image, i.e. +|dz| without a z wrap and -|dz_min| with one.             */
 /* t=(int)((1+dz12/d12)*bins/2), p=(int)((1+dz31/d31)*bins/2)               */
 /* (3ani_k.cuh:75-91), each dropped when >= bins.  Ordered triples are      */
@@ -496,7 +700,7 @@ static inline int ani_angle_bin(double dz, double d, int bins)
 }
 
 int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, long nY, float L,
-                     int bins, float dmax, double *out)
+                     int bins, float dmax, int gate_P, double *out)
 {
     const long B = bins;
     const long nb = B * B * B * B * B;
@@ -507,6 +711,8 @@ int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, lo
     const unsigned rXX = RULE_EXCL_ZERO;
     const unsigned rXY = bpc ? RULE_EXCL_ZERO : 0u;
     if (!mixed) { Y = X; nY = nX; }
+    const int gated = bpc && gate_P > 0;
+    gate_geom gg = gate_setup(L, dmax, gated ? gate_P : 1);
     memset(out, 0, sizeof(double) * (size_t)nb);
     int nt = omp_get_max_threads();
     double *priv = (double *)calloc((size_t)nt * nb, sizeof(double));
@@ -518,6 +724,8 @@ int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, lo
         for (long i = 0; i < nX; ++i) {
             const opt *p = &X[i];
             long n2, n3;
+            float n1c[3], n2c[3], n3c[3];
+            if (gated) gate_corner(&gg, p, n1c);
             nbr_t *N2 = neighbours(p, X, 0, nX, bpc, Ld, rXX, ddmax, ds, bins, 0, &n2);
             nbr_t *N3 = neighbours(p, Y, 0, nY, bpc, Ld, mixed ? rXY : rXX, ddmax, ds, bins, 0, &n3);
             for (long a = 0; a < n2; ++a) {
@@ -527,6 +735,11 @@ int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, lo
                 int t = ani_angle_bin(bpc ? bpc_dz(p->z, X[q->idx].z, Ld) : q->v[2], d12, bins);
                 if (t < 0) continue;
                 double wij = (double)p->w * (double)X[q->idx].w;
+                unsigned s2 = 0;
+                if (gated) {
+                    gate_corner(&gg, &X[q->idx], n2c);
+                    s2 = wrap_bits(p, &X[q->idx], Ld);
+                }
                 for (long b = 0; b < n3; ++b) {
                     const nbr_t *r = &N3[b];
                     if (!mixed && (r->idx == i || r->idx == q->idx)) continue;
@@ -537,6 +750,12 @@ int orc_triplets_ani(int bpc, int mixed, const opt *X, long nX, const opt *Y, lo
                     int pp = ani_angle_bin(bpc ? bpc_dz(p->z, Y[r->idx].z, Ld) : r->v[2], d31, bins);
                     if (pp < 0) continue;
                     double w = wij * (double)Y[r->idx].w;
+                    if (gated) {
+                        gate_corner(&gg, &Y[r->idx], n3c);
+                        int m = gate_mult(&gg, n1c, n2c, n3c, s2, wrap_bits(p, &Y[r->idx], Ld));
+                        if (m == 0) continue;
+                        w *= (double)m;
+                    }
                     long slot = (((q->bin * B + r->bin) * B + c) * B + t) * B + pp;
                     h[slot] += w;
                 }

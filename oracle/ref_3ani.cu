@@ -1,16 +1,18 @@
-// Harness over the reference's plain anisotropic 3-point kernels (XXX3ani,
-// XXY3ani: cuda/kernels/3ani_k.cuh:8,109) -- fixture generation only.  The
-// reference's own writer keeps only bn^3 of the bn^5 histogram
-// (pcf3ani.cuh:123); this harness launches the kernels the way pcf_3ani does
-// (pcf3ani.cuh:77-112: 8x8x8 threads per block, one block index per node
-// triple, d_max_node = (dmax + size_node*sqrt(3))^2) and copies every bin
-// back.  Nodes are built as main.cu:219-329 builds them (make_nodos, then the
+// Harness over the reference's anisotropic 3-point kernels -- fixture
+// generation only.  Plain: XXX3ani, XXY3ani (cuda/kernels/3ani_k.cuh:8,109),
+// launched as pcf_3ani does (pcf3ani.cuh:77-112).  Periodic: XXX3ani_BPC,
+// XXY3ani_BPC (cuda/kernels/3aniBPC_k.cuh:210,959), launched as pcf_3aniBPC
+// does (pcf3aniBPC.cuh:87-115).  Both: 8x8x8 threads per block, one thread
+// per ordered node triple, d_max_node = (dmax + size_node*sqrt(3))^2, one
+// random file (node and bin offsets 0).  The reference's own writer keeps
+// only bn^3 of the bn^5 histogram (pcf3ani.cuh:123, pcf3aniBPC.cuh:123);
+// this harness copies every bin back.  Nodes are built as main.cu:219-329 builds them (make_nodos, then the
 // non-empty nodes in (row, col, mom) order with their points contiguous).
 // The headers are included unmodified from the reference tree (-I<ref>/cuda).
 //
-//   ref_3ani.out D.f4 R.f4 N BINS DMAX PARTITIONS BOX OUT.bin
-//     D.f4, R.f4: N points each, float32 x y z w; OUT.bin: DDD, RRR, DDR,
-//     DRR, bins^5 doubles each.
+//   ref_3ani.out D.f4 R.f4 N BINS DMAX PARTITIONS BOX BPC OUT.bin
+//     D.f4, R.f4: N points each, float32 x y z w; BPC: 0 plain, 1 periodic;
+//     OUT.bin: DDD, RRR, DDR, DRR, bins^5 doubles each.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -19,6 +21,7 @@
 
 #include "create_grid.cuh"
 #include "kernels/3ani_k.cuh"
+#include "kernels/3aniBPC_k.cuh"
 
 #define CK(call)                                                                   \
     do {                                                                           \
@@ -78,11 +81,12 @@ static std::vector<PointW3D> read_f4(const char *path, int n) {
 }
 
 int main(int argc, char **argv) {
-    if (argc != 9) {
-        fprintf(stderr, "usage: %s D.f4 R.f4 N BINS DMAX PARTITIONS BOX OUT.bin\n", argv[0]);
+    if (argc != 10) {
+        fprintf(stderr, "usage: %s D.f4 R.f4 N BINS DMAX PARTITIONS BOX BPC OUT.bin\n", argv[0]);
         return 1;
     }
     const int np = atoi(argv[3]), bn = atoi(argv[4]), partitions = atoi(argv[6]);
+    const bool bpc = atoi(argv[8]) != 0;
     const float dmax = (float)atof(argv[5]), box = (float)atof(argv[7]);
     std::vector<PointW3D> D = read_f4(argv[1], np), R = read_f4(argv[2], np);
     const float size_node = box / (float)partitions;
@@ -112,15 +116,24 @@ int main(int argc, char **argv) {
     const int t = 8;
     const int bD = (nD + t - 1) / t, bR = (nR + t - 1) / t;
     const dim3 thr(t, t, t);
-    XXX3ani<<<dim3(bD, bD, bD), thr>>>(h[0], dpD, dnD, nD, bn, dmax, d_max_node);
-    XXX3ani<<<dim3(bR, bR, bR), thr>>>(h[1], dpR, dnR, nR, bn, dmax, d_max_node, 0, 0);
-    XXY3ani<<<dim3(bD, bD, bR), thr>>>(h[2], dpD, dnD, nD, dpR, dnR, nR, bn, dmax, d_max_node, 0, 0, true);
-    XXY3ani<<<dim3(bR, bR, bD), thr>>>(h[3], dpR, dnR, nR, dpD, dnD, nD, bn, dmax, d_max_node, 0, 0, false);
+    if (bpc) {
+        XXX3ani_BPC<<<dim3(bD, bD, bD), thr>>>(h[0], dpD, dnD, nD, bn, dmax, d_max_node, box, size_node);
+        XXX3ani_BPC<<<dim3(bR, bR, bR), thr>>>(h[1], dpR, dnR, nR, bn, dmax, d_max_node, box, size_node, 0, 0);
+        XXY3ani_BPC<<<dim3(bD, bD, bR), thr>>>(h[2], dpD, dnD, nD, dpR, dnR, nR, bn, dmax, d_max_node, box,
+                                               size_node, 0, 0, true);
+        XXY3ani_BPC<<<dim3(bR, bR, bD), thr>>>(h[3], dpR, dnR, nR, dpD, dnD, nD, bn, dmax, d_max_node, box,
+                                               size_node, 0, 0, false);
+    } else {
+        XXX3ani<<<dim3(bD, bD, bD), thr>>>(h[0], dpD, dnD, nD, bn, dmax, d_max_node);
+        XXX3ani<<<dim3(bR, bR, bR), thr>>>(h[1], dpR, dnR, nR, bn, dmax, d_max_node, 0, 0);
+        XXY3ani<<<dim3(bD, bD, bR), thr>>>(h[2], dpD, dnD, nD, dpR, dnR, nR, bn, dmax, d_max_node, 0, 0, true);
+        XXY3ani<<<dim3(bR, bR, bD), thr>>>(h[3], dpR, dnR, nR, dpD, dnD, nD, bn, dmax, d_max_node, 0, 0, false);
+    }
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
 
     std::vector<double> out(nb5);
-    FILE *fo = fopen(argv[8], "wb");
+    FILE *fo = fopen(argv[9], "wb");
     if (!fo) return 1;
     for (int k = 0; k < 4; ++k) {
         CK(cudaMemcpy(out.data(), h[k], sizeof(double) * nb5, cudaMemcpyDeviceToHost));

@@ -121,15 +121,19 @@ def test_cli_3iso_and_file_format(layout):
 
 
 @pytest.mark.gpu
-def test_cli_3iso_rd_batched(layout):
-    """PCF.out 3iso -rd: DDD and every random file's RRR / DDR / DRR from one
-    batched launch, each equal to the oracle."""
+@pytest.mark.parametrize("exact", [True, False], ids=["exact", "reference_gates"])
+def test_cli_3iso_rd_batched(layout, exact):
+    """PCF.out 3iso -rd -bpc: DDD and every random file's RRR / DDR / DRR.
+    With -exact from one batched launch, each equal to the oracle's count of
+    every triangle in range; by default per call through the reference's node
+    gates on its -p grid (35 nodes per side), equal to the oracle's
+    restatement of those gates (PCF_REF_NODE_GATES)."""
     D, R, R2 = _cats(layout, n=700)
     box = 100.0
     _run(["3iso", "-n", "700", "-f", "d.dat", "-rd", "rands/", "-b", "8", "-d", "20", "-bpc",
-          "-s", str(box)], layout / "cuda")
+          "-s", str(box)] + (["-exact"] if exact else []), layout / "cuda")
     res = layout / "results"
-    kw = dict(box=box, bins=8, dmax=20.0, bpc=True)
+    kw = dict(box=box, bins=8, dmax=20.0, bpc=True, ref_gates=0 if exact else 35)
     rd = lambda name: _read(res / name).reshape(8, 8, 8)  # noqa: E731
     assert np.array_equal(rd("DDDiso_BPC_d.dat"), oracle.triplets_iso(D, **kw))
     for lab, RR in (("ra", R), ("rb", R2)):
@@ -169,10 +173,14 @@ def test_legacy_signatures(layout, tmp_path):
                     "-Wl,-rpath," + os.path.join(ROOT, "desi_b200")], check=True)
     D, R, _ = _cats(layout, n=900)
     d, r = str(layout / "data" / "d.dat"), str(layout / "data" / "r.dat")
-    for kind in ("2iso", "2aniBPC", "3iso", "2isoBPCa"):
+    for kind in ("2iso", "2aniBPC", "3iso", "2isoBPCa", "3isoBPC"):
         subprocess.run([exe, kind, d, r, "900", "10", "20", "100"], cwd=layout / "cuda", check=True,
                        timeout=300)
     res = layout / "results"
+    # pcf_3isoBPC counts through the reference's node gates on the caller's
+    # grid (size_node = box / 10 in the driver)
+    assert np.array_equal(_read(res / "RRRiso_BPC_rand").reshape(10, 10, 10),
+                          oracle.triplets_iso(R, box=100.0, bins=10, dmax=20.0, bpc=True, ref_gates=10))
     assert np.array_equal(_read(res / "DDiso_data"), oracle.pairs(D, box=100.0, bins=10, dmax=20.0))
     assert np.array_equal(_read(res / "DRani_BPC_rand").reshape(10, 10),
                           oracle.pairs(D, R, box=100.0, bins=10, dmax=20.0, ani=True, bpc=True))

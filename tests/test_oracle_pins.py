@@ -302,17 +302,91 @@ def test_ref_3iso_analytic_ff_ref(tmp_path):
     np.testing.assert_allclose(got, ffr, rtol=1e-10, atol=1e-10)
 
 
-def test_oracle_3ani_matches_reference_kernels():
-    """The anisotropic 3-point oracle against the reference's own plain 3ani
-    CUDA kernels (XXX3ani / XXY3ani, cuda/kernels/3ani_k.cuh:8,109), all bn^5
-    bins of DDD, RRR, DDR and DRR, from the committed fixture
-    (tests/golden/make_golden_3ani.py): bit-equal counts."""
-    import os
-    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_3ani.npz"))
-    kw = dict(box=float(g["box"]), bins=int(g["bins"]), dmax=float(g["dmax"]))
+@pytest.mark.parametrize("bpc", [False, True], ids=["plain", "periodic"])
+def test_oracle_3ani_matches_reference_kernels(bpc):
+    """The anisotropic 3-point oracle against the reference's own 3ani CUDA
+    kernels, all bn^5 bins of DDD, RRR, DDR and DRR, from the committed
+    fixtures (tests/golden/make_golden_3ani.py): plain XXX3ani / XXY3ani
+    (cuda/kernels/3ani_k.cuh:8,109) and periodic XXX3ani_BPC / XXY3ani_BPC
+    (cuda/kernels/3aniBPC_k.cuh:210,959, whose angle takes dz = |dz| - box
+    for a pair joined through its z image, and which count through the
+    reference's node gates: the oracle's ref_gates mode on the fixture's
+    node grid).  Bit-equal counts."""
+    name_ = "golden_3ani_bpc.npz" if bpc else "golden_3ani.npz"
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", name_))
+    kw = dict(box=float(g["box"]), bins=int(g["bins"]), dmax=float(g["dmax"]), bpc=bpc,
+              ref_gates=int(g["partitions"]) if bpc else 0)
     D, R = g["D"], g["R"]
     for name, x, y in (("DDD", D, None), ("RRR", R, None), ("DDR", D, R), ("DRR", R, D)):
         got = oracle.triplets_ani(x, y, **kw)
         want = g[name]
         assert want.sum() > 1e6
         assert np.array_equal(got, want), (name, float(np.abs(got - want).sum()))
+
+
+def _host_kernels():
+    if not os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libref_3pt_host.so")):
+        pytest.skip("oracle/_ref/libref_3pt_host.so not built")
+    return oracle.ref_kernels_3pt
+
+
+def _lattice(n, seed):
+    """Data on even, randoms on odd integer coordinates of a 60-box: every
+    FP32 sum the reference's kernels form is exact."""
+    rng = np.random.default_rng(seed)
+    D = np.ones((n, 4), np.float32)
+    R = np.ones((n, 4), np.float32)
+    D[:, :3] = 2 * rng.integers(0, 30, size=(n, 3))
+    R[:, :3] = 2 * rng.integers(0, 30, size=(n, 3)) + 1
+    return D, R
+
+
+@pytest.mark.parametrize("bpc", [False, True], ids=["plain", "periodic"])
+def test_host_build_of_reference_kernels_equals_b200_run(bpc):
+    """The reference's 3ani kernels compiled for the host
+    (oracle/ref_3pt_host.cpp) give the B200 run of the same kernels
+    (tests/golden/golden_3ani*.npz) bin for bin: the host build is a pin at
+    any configuration, not only at the fixture's."""
+    ref = _host_kernels()
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden",
+                             "golden_3ani_bpc.npz" if bpc else "golden_3ani.npz"))
+    h = ref(g["D"], g["R"], ani=True, bpc=bpc, box=float(g["box"]), bins=int(g["bins"]),
+            dmax=float(g["dmax"]), partitions=int(g["partitions"]))
+    for name in ("DDD", "RRR", "DDR", "DRR"):
+        assert np.array_equal(h[name], g[name]), name
+
+
+@pytest.mark.parametrize("ani", [False, True], ids=["3iso", "3ani"])
+@pytest.mark.parametrize("P,dmax,bins,n", [(6, 20.0, 8, 700), (3, 20.0, 6, 300), (4, 18.0, 5, 400),
+                                           (7, 12.0, 6, 500), (2, 16.0, 5, 200)])
+def test_oracle_reference_gates_equal_reference_kernels(ani, P, dmax, bins, n):
+    """Periodic triplets: the reference's CUDA kernels (XXX3iso_BPC /
+    XXY3iso_BPC, 3isoBPC_k.cuh:191,940; XXX3ani_BPC / XXY3ani_BPC,
+    3aniBPC_k.cuh:210,959) count a triangle once per node-gate block that
+    passes.  The oracle's ref_gates mode (the 64 blocks as a table, with the
+    reference's defective gates) equals them in DDD, RRR, DDR and DRR on
+    coarse and fine node grids; the nearest-image count (the default, which
+    the reference's CPU engine follows) is larger wherever a defective gate
+    drops triangles."""
+    ref = _host_kernels()
+    D, R = _lattice(n, 100 + P)
+    L = 60.0
+    h = ref(D, R, ani=ani, bpc=True, box=L, bins=bins, dmax=dmax, partitions=P)
+    f = oracle.triplets_ani if ani else oracle.triplets_iso
+    for name, x, y in (("DDD", D, None), ("RRR", R, None), ("DDR", D, R), ("DRR", R, D)):
+        got = f(x, y, box=L, bins=bins, dmax=dmax, bpc=True, ref_gates=P)
+        assert np.array_equal(got, h[name]), name
+        full = f(x, y, box=L, bins=bins, dmax=dmax, bpc=True)
+        assert full.sum() >= got.sum()
+
+
+def test_oracle_plain_3iso_equals_reference_kernels():
+    """Without periodic boundaries the reference's 3iso kernels (XXX3iso /
+    XXY3iso, 3iso_k.cuh:8,94) have no node gates to get wrong: they equal the
+    oracle's default rule."""
+    ref = _host_kernels()
+    D, R = _lattice(800, 5)
+    L, bins, dmax = 60.0, 8, 20.0
+    h = ref(D, R, ani=False, bpc=False, box=L, bins=bins, dmax=dmax, partitions=6)
+    for name, x, y in (("DDD", D, None), ("RRR", R, None), ("DDR", D, R), ("DRR", R, D)):
+        assert np.array_equal(oracle.triplets_iso(x, y, box=L, bins=bins, dmax=dmax), h[name]), name

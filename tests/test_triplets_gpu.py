@@ -7,6 +7,7 @@ import pytest
 
 import oracle
 from desi_b200 import catalog
+from desi_b200.api import PcfError
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -98,16 +99,77 @@ def test_triplets_ani(ctx, bpc, w):
          oracle.triplets_ani(D, R, box=box, bins=bins, dmax=dmax, bpc=bpc), weighted)
 
 
-def test_triplets_ani_equal_reference_kernels(ctx):
+@pytest.mark.parametrize("bpc", [False, True], ids=["plain", "periodic"])
+def test_triplets_ani_equal_reference_kernels(ctx, bpc):
     """The GPU 3ani histograms (DDD, RRR, DDR, DRR) equal the reference's own
-    plain 3ani CUDA kernels bin for bin (committed fixture,
-    tests/golden/make_golden_3ani.py)."""
-    g = np.load(os.path.join(GOLDEN, "golden_3ani.npz"))
-    box, bins, dmax = float(g["box"]), int(g["bins"]), float(g["dmax"])
-    gd, gr = ctx.grid(g["D"], box), ctx.grid(g["R"], box)
+    3ani CUDA kernels, plain and periodic, bin for bin (committed fixtures,
+    tests/golden/make_golden_3ani.py).  Periodic: through
+    PCF_REF_NODE_GATES on the fixture's node grid; the default count, every
+    triangle in range once, is larger."""
+    g = np.load(os.path.join(GOLDEN, "golden_3ani_bpc.npz" if bpc else "golden_3ani.npz"))
+    box, bins, dmax, P = float(g["box"]), int(g["bins"]), float(g["dmax"]), int(g["partitions"])
+    gd, gr = ctx.grid(g["D"], box, partitions=P), ctx.grid(g["R"], box, partitions=P)
     for name, x, y in (("DDD", gd, None), ("RRR", gr, None), ("DDR", gd, gr), ("DRR", gr, gd)):
-        got = ctx.count_triplets(x, y, bins=bins, dmax=dmax, ani=True)
+        got = ctx.count_triplets(x, y, bins=bins, dmax=dmax, ani=True, bpc=bpc, ref_gates=bpc)
         assert np.array_equal(got, g[name]), name
+        if bpc:
+            full = ctx.count_triplets(x, y, bins=bins, dmax=dmax, ani=True, bpc=True)
+            assert full.sum() > got.sum()
+
+
+def _lattice(n, seed, box_half=30):
+    rng = np.random.default_rng(seed)
+    D = np.ones((n, 4), np.float32)
+    R = np.ones((n, 4), np.float32)
+    D[:, :3] = 2 * rng.integers(0, box_half, size=(n, 3))
+    R[:, :3] = 2 * rng.integers(0, box_half, size=(n, 3)) + 1
+    return D, R
+
+
+@pytest.mark.parametrize("ani", [False, True], ids=["3iso", "3ani"])
+@pytest.mark.parametrize("P,dmax,bins", [(3, 20.0, 6), (6, 20.0, 8), (7, 12.0, 6)])
+def test_triplets_ref_gates_equal_oracle(ctx, ani, P, dmax, bins):
+    """PCF_REF_NODE_GATES: the periodic 3iso and 3ani counts of the
+    reference's CUDA kernels (3isoBPC_k.cuh:191,940, 3aniBPC_k.cuh:210,959)
+    equal the oracle's restatement of their node gates (which the CPU suite
+    pins to a host build of those kernels) in DDD, RRR, DDR and DRR."""
+    D, R = _lattice(600, 40 + P)
+    box = 60.0
+    gd, gr = ctx.grid(D, box, partitions=P), ctx.grid(R, box, partitions=P)
+    f = oracle.triplets_ani if ani else oracle.triplets_iso
+    for x, y, cx, cy in ((gd, None, D, None), (gr, None, R, None), (gd, gr, D, R), (gr, gd, R, D)):
+        got = ctx.count_triplets(x, y, bins=bins, dmax=dmax, ani=ani, bpc=True, ref_gates=True)
+        want = f(cx, cy, box=box, bins=bins, dmax=dmax, bpc=True, ref_gates=P)
+        assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("ani", [False, True], ids=["3iso", "3ani"])
+def test_triplets_ref_gates_weighted_clustered(ctx, ani):
+    """The gated counts off the lattice: clustered data, weights U(0.5, 1.5),
+    the reference's default 35 nodes per side, against the oracle."""
+    box, bins, dmax, P = 250.0, 6 if ani else 10, 40.0, 35
+    D = catalog.neyman_scott(900, box, seed=77)
+    D[:, 3] = np.random.default_rng(3).uniform(0.5, 1.5, len(D)).astype(np.float32)
+    R = catalog.uniform(700, box, seed=78)
+    gd, gr = ctx.grid(D, box, partitions=P), ctx.grid(R, box, partitions=P)
+    f = oracle.triplets_ani if ani else oracle.triplets_iso
+    for x, y, cx, cy in ((gd, None, D, None), (gd, gr, D, R)):
+        got = ctx.count_triplets(x, y, bins=bins, dmax=dmax, ani=ani, bpc=True, ref_gates=True)
+        _cmp(got, f(cx, cy, box=box, bins=bins, dmax=dmax, bpc=True, ref_gates=P), True)
+
+
+def test_triplets_ref_gates_arguments(ctx):
+    """The gates need periodic counts and the caller's node grid."""
+    D, R = _lattice(200, 9)
+    g0 = ctx.grid(D, 60.0)
+    g6 = ctx.grid(D, 60.0, partitions=6)
+    g5 = ctx.grid(R, 60.0, partitions=5)
+    with pytest.raises(PcfError):
+        ctx.count_triplets(g6, bins=6, dmax=20.0, ani=True, bpc=False, ref_gates=True)
+    with pytest.raises(PcfError):
+        ctx.count_triplets(g0, bins=6, dmax=20.0, bpc=True, ref_gates=True)
+    with pytest.raises(PcfError):
+        ctx.count_triplets(g6, g5, bins=6, dmax=20.0, ani=True, bpc=True, ref_gates=True)
 
 
 def test_wide_histogram_through_grown_staging(ctx):
