@@ -381,26 +381,55 @@ def available_ref_engines():
         return []
     return sorted(f[len("libref_"):-3] for f in os.listdir(d) if f.startswith("libref_"))
 
+def _kernels_lib():
+    lib = ctypes.CDLL(os.path.join(HERE, "_ref", "libref_kernels_host.so"))
+    args = [ctypes.c_int, ctypes.c_int, _fptr, ctypes.c_int, _fptr, ctypes.c_int, ctypes.c_int,
+            ctypes.c_float, ctypes.c_int, ctypes.c_float, _dptr]
+    lib.ref2_hist.argtypes = args
+    lib.ref3_hist.argtypes = args
+    return lib
+
+
+def ref_kernels_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_kernels_host.so"))
+
+
 def ref_kernels_3pt(D, R=None, *, ani: bool, bpc: bool, box: float, bins: int, dmax: float,
                     partitions: int):
     """The reference's own 3-point CUDA kernels (XXX3iso/XXY3iso,
     XXX3iso_BPC/XXY3iso_BPC, XXX3ani/XXY3ani, XXX3ani_BPC/XXY3ani_BPC in
     cuda/kernels/3{iso,ani}{,BPC}_k.cuh) compiled for the host
-    (_ref/libref_3pt_host.so, ref_3pt_host.cpp), on nodes of box/partitions:
-    {"DDD": ...} or, with R, {"DDD", "RRR", "DDR", "DRR"}, each bins^3 (iso)
-    or bins^5 (ani).  Unit weights only (see ref_3pt_host.cpp)."""
-    path = os.path.join(HERE, "_ref", "libref_3pt_host.so")
-    lib = ctypes.CDLL(path)
-    lib.ref3_hist.argtypes = [ctypes.c_int, ctypes.c_int, _fptr, ctypes.c_int, _fptr, ctypes.c_int,
-                              ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_float, _dptr]
+    (_ref/libref_kernels_host.so, ref_kernels_host.cpp), on nodes of
+    box/partitions: {"DDD": ...} or, with R, {"DDD", "RRR", "DDR", "DRR"},
+    each bins^3 (iso) or bins^5 (ani).  Unit weights only (see
+    ref_kernels_host.cpp)."""
     D = _pts(D)
     Rp = _pts(R) if R is not None else None
     shape = (bins,) * (5 if ani else 3)
     nb = int(np.prod(shape))
     out = np.zeros(nb * (4 if Rp is not None else 1), np.float64)
-    rc = lib.ref3_hist(int(ani), int(bpc), _p(D), len(D), _p(Rp) if Rp is not None else None,
-                       len(Rp) if Rp is not None else 0, bins, dmax, partitions, box, _d(out))
+    rc = _kernels_lib().ref3_hist(int(ani), int(bpc), _p(D), len(D), _p(Rp) if Rp is not None else None,
+                                  len(Rp) if Rp is not None else 0, bins, dmax, partitions, box, _d(out))
     if rc != 0:
         raise ValueError(f"ref3_hist returned {rc} (a coordinate outside the node grid?)")
     names = ("DDD", "RRR", "DDR", "DRR") if Rp is not None else ("DDD",)
     return {k: out[i * nb:(i + 1) * nb].reshape(shape) for i, k in enumerate(names)}
+
+
+def ref_kernels_2pt(D, R, *, ani: bool, bpc: bool, box: float, bins: int, dmax: float,
+                    partitions: int):
+    """The reference's own pair CUDA kernels (XX2iso/XY2iso,
+    XX2iso_BPC/XY2iso_BPC, XX2ani, XX2ani_BPC in
+    cuda/kernels/2{iso,ani}{,BPC}_k.cuh) compiled for the host, on nodes of
+    box/partitions: {"DD", "RR", "DR"}, each bins (iso) or bins x bins (ani).
+    The anisotropic DR is NaN: its kernels read an out-of-range weight
+    (XY2ani) or an unset one (XY2ani_BPC), see ref_kernels_host.cpp."""
+    D, Rp = _pts(D), _pts(R)
+    shape = (bins, bins) if ani else (bins,)
+    nb = int(np.prod(shape))
+    out = np.zeros(3 * nb, np.float64)
+    rc = _kernels_lib().ref2_hist(int(ani), int(bpc), _p(D), len(D), _p(Rp), len(Rp), bins, dmax,
+                                  partitions, box, _d(out))
+    if rc != 0:
+        raise ValueError(f"ref2_hist returned {rc} (a coordinate outside the node grid?)")
+    return {k: out[i * nb:(i + 1) * nb].reshape(shape) for i, k in enumerate(("DD", "RR", "DR"))}

@@ -325,8 +325,8 @@ def test_oracle_3ani_matches_reference_kernels(bpc):
 
 
 def _host_kernels():
-    if not os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libref_3pt_host.so")):
-        pytest.skip("oracle/_ref/libref_3pt_host.so not built")
+    if not oracle.ref_kernels_available():
+        pytest.skip("oracle/_ref/libref_kernels_host.so not built")
     return oracle.ref_kernels_3pt
 
 
@@ -344,7 +344,7 @@ def _lattice(n, seed):
 @pytest.mark.parametrize("bpc", [False, True], ids=["plain", "periodic"])
 def test_host_build_of_reference_kernels_equals_b200_run(bpc):
     """The reference's 3ani kernels compiled for the host
-    (oracle/ref_3pt_host.cpp) give the B200 run of the same kernels
+    (oracle/ref_kernels_host.cpp) give the B200 run of the same kernels
     (tests/golden/golden_3ani*.npz) bin for bin: the host build is a pin at
     any configuration, not only at the fixture's."""
     ref = _host_kernels()
@@ -390,3 +390,29 @@ def test_oracle_plain_3iso_equals_reference_kernels():
     h = ref(D, R, ani=False, bpc=False, box=L, bins=bins, dmax=dmax, partitions=6)
     for name, x, y in (("DDD", D, None), ("RRR", R, None), ("DDR", D, R), ("DRR", R, D)):
         assert np.array_equal(oracle.triplets_iso(x, y, box=L, bins=bins, dmax=dmax), h[name]), name
+
+
+@pytest.mark.parametrize("bpc", [False, True], ids=["plain", "periodic"])
+@pytest.mark.parametrize("P,dmax,bins", [(6, 20.0, 8), (3, 20.0, 6), (7, 12.0, 6), (35, 20.0, 10)])
+def test_oracle_pairs_equal_reference_kernels(bpc, P, dmax, bins):
+    """The pair rules of the headline step against the reference's own CUDA
+    pair kernels compiled for the host (XX2iso / XY2iso, 2iso_k.cuh:8,63;
+    XX2iso_BPC / XY2iso_BPC, 2isoBPC_k.cuh:8,284; XX2ani, 2ani_k.cuh:7;
+    XX2ani_BPC, 2aniBPC_k.cuh:8) on lattice catalogs and node grids of 3 to
+    35 per side: DD, RR and DR (iso), DD and RR (ani) bit-equal.  The
+    anisotropic cross kernels read an out-of-range (XY2ani) or unset
+    (XY2ani_BPC) weight; the anisotropic DR is pinned to the reference's CPU
+    engines instead (test_ref_cpu_bpc_bitexact, test_ref_cpu_bpc_weighted)."""
+    if not oracle.ref_kernels_available():
+        pytest.skip("oracle/_ref/libref_kernels_host.so not built")
+    D, R = _lattice(2500, 200 + P)
+    L = 60.0
+    for ani in (False, True):
+        h = oracle.ref_kernels_2pt(D, R, ani=ani, bpc=bpc, box=L, bins=bins, dmax=dmax, partitions=P)
+        kw = dict(box=L, bins=bins, dmax=dmax, bpc=bpc, ani=ani, ds_exact=bpc and not ani)
+        assert np.array_equal(h["DD"], oracle.pairs(D, None, **kw)), ("DD", ani)
+        assert np.array_equal(h["RR"], oracle.pairs(R, None, **kw)), ("RR", ani)
+        if not ani:
+            assert np.array_equal(h["DR"], oracle.pairs(D, R, **kw)), "DR"
+        else:
+            assert np.isnan(h["DR"]).all()
