@@ -756,7 +756,9 @@ def run_served(n_requests=300, load=0.7):
     rep["closed_loop"] = {k: closed[k] for k in ("wall_s", "pairs_per_s", "triplets_per_s",
                                                  "overlapping_starts")}
     rep["closed_loop"]["passes_wall_s"] = [r["wall_s"] for r in passes]
+    rep["closed_loop"]["passes_allocations"] = [r["allocations"] for r in passes]
     rep["plain_passes_wall_s"] = [r["wall_s"] for r in plains]
+    rep["plain_passes_allocations"] = [r["allocations"] for r in plains]
     rep["plain_per_call"] = {k: plain[k] for k in ("wall_s", "pairs_per_s", "triplets_per_s",
                                                    "latency_ms")}
     rep["served_vs_plain"] = {

@@ -116,7 +116,18 @@ _SIGS = {
                                             ctypes.POINTER(_i64)]),
     "pcf_ctx_profile_read_grid": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double),
                                                  ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "pcf_alloc_counters": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64)]),
 }
+
+
+def alloc_counters() -> dict:
+    """Process-wide allocation counters of the library (pcf_alloc_counters):
+    device and page-locked host allocations, their bytes and the seconds
+    spent in those calls."""
+    out = (ctypes.c_uint64 * 6)()
+    lib().pcf_alloc_counters(out)
+    return {"device_allocs": out[0], "device_bytes": out[1], "device_s": out[2] * 1e-9,
+            "host_allocs": out[3], "host_bytes": out[4], "host_s": out[5] * 1e-9}
 
 
 def exported_symbols():

@@ -44,6 +44,9 @@ pcf_status pcf_ctx_create(int device, pcf_ctx **out) {
     if (device < 0 || device >= ndev) return PCF_ERR_INVALID_ARG;
     pcf_ctx *c = new pcf_ctx;
     c->device = device;
+    for (DevBuf *b : {&c->scratch_a, &c->scratch_b, &c->scratch_c, &c->d_hist, &c->d_flag})
+        b->pool = c->scratch_pool;
+    for (PlanSlot &sl : c->slots) sl.d_rows.pool = sl.d_counter.pool = c->scratch_pool;
     if (cudaSetDevice(device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
@@ -81,6 +84,7 @@ pcf_status pcf_ctx_destroy(pcf_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->pool->release();
+    ctx->scratch_pool->release();
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
     if (ctx->d_abort) cudaFree(ctx->d_abort);

@@ -22,6 +22,7 @@
 // in L2 and it is the faster of the two.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <cmath>
@@ -31,6 +32,56 @@
 #include <cooperative_groups.h>
 
 #include "pcf_internal.cuh"
+
+namespace {
+std::atomic<unsigned long long> g_alloc[6];  // device n, bytes, ns; host n, bytes, ns
+
+template <class F>
+cudaError_t counted(int slot, size_t n, F call) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const cudaError_t e = call();
+    const auto t1 = std::chrono::steady_clock::now();
+    if (e == cudaSuccess) {
+        g_alloc[slot].fetch_add(1);
+        g_alloc[slot + 1].fetch_add(n);
+    }
+    g_alloc[slot + 2].fetch_add(
+        (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
+    return e;
+}
+}  // namespace
+
+cudaError_t counted_malloc(void **p, size_t n) {
+    return counted(0, n, [&] { return cudaMalloc(p, n); });
+}
+
+cudaError_t counted_malloc_host(void **p, size_t n) {
+    return counted(3, n, [&] { return cudaHostAlloc(p, n, cudaHostAllocPortable); });
+}
+
+std::shared_ptr<PinnedPool> shared_pinned_pool() {
+    // never destroyed: its blocks are released by the process's exit, after
+    // which the CUDA runtime can no longer be called from a destructor
+    static std::shared_ptr<PinnedPool> *pool = new std::shared_ptr<PinnedPool>(std::make_shared<PinnedPool>());
+    return *pool;
+}
+
+namespace {
+// Size classes of the device pool: four per power of two above 4 KB, so
+// catalogs of nearby sizes reuse one another's blocks.
+size_t pool_class(size_t n) {
+    if (n <= 4096) return 4096;
+    const int k = 63 - __builtin_clzll((unsigned long long)(n - 1));
+    const size_t base = (size_t)1 << k, step = base >> 2;
+    return base + (n - base + step - 1) / step * step;
+}
+}  // namespace
+
+extern "C" pcf_status pcf_alloc_counters(uint64_t out[6]) {
+    if (!out) return PCF_ERR_INVALID_ARG;
+    for (int k = 0; k < 6; ++k) out[k] = g_alloc[k].load();
+    return PCF_OK;
+}
 
 // The smallest cached block that holds n bytes is reused if it is at most
 // 8n + 1 MB: a cudaMalloc can stall other threads' work on the device (the
@@ -44,12 +95,12 @@ cudaError_t MemPool::get(size_t n, void **p, size_t *got) {
         free_blocks.erase(it);
         return cudaSuccess;
     }
-    size_t want = std::max<size_t>(256, (n + 255) & ~(size_t)255);
-    cudaError_t e = cudaMalloc(p, want);
+    const size_t want = pool_class(n);
+    cudaError_t e = counted_malloc(p, want);
     if (e == cudaErrorMemoryAllocation && !free_blocks.empty()) {
         cudaGetLastError();
         release();
-        e = cudaMalloc(p, want);
+        e = counted_malloc(p, want);
     }
     if (e == cudaSuccess) *got = want;
     return e;
@@ -86,7 +137,7 @@ cudaError_t PinnedPool::get(size_t n, void **p, size_t *got) {
         free_blocks.erase(it);
         return cudaSuccess;
     }
-    cudaError_t e = cudaMallocHost(p, want);
+    cudaError_t e = counted_malloc_host(p, want);
     if (e == cudaSuccess) *got = want;
     return e;
 }
@@ -118,7 +169,7 @@ cudaError_t DevBuf::ensure(size_t n) {
     bytes = 0;
     if (pool) return pool->get(std::max<size_t>(n, 256), &p, &bytes);
     size_t want = std::max<size_t>(n, 256);
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = counted_malloc(&p, want);
     if (e == cudaSuccess) bytes = want;
     return e;
 }
@@ -845,7 +896,7 @@ pcf_status pcf_ensure_pinned(pcf_ctx *ctx, size_t bytes) {
     ctx->h_pinned = nullptr;
     ctx->h_pinned_bytes = 0;
     size_t want = std::max<size_t>(bytes, 1 << 20);
-    PCF_CU(ctx, cudaMallocHost(&ctx->h_pinned, want));
+    PCF_CU(ctx, counted_malloc_host(&ctx->h_pinned, want));
     ctx->h_pinned_bytes = want;
     return PCF_OK;
 }

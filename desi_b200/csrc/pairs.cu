@@ -1324,7 +1324,7 @@ pcf_status stage_plan(pcf_ctx *ctx, const PairPlan &plan, PlanSlot **out) {
         sl.h_pinned = nullptr;
         sl.h_bytes = 0;
         const size_t want = std::max<size_t>((rb + jb) * 2 + 256, 1 << 16);
-        PCF_CU(ctx, cudaMallocHost(&sl.h_pinned, want));
+        PCF_CU(ctx, counted_malloc_host(&sl.h_pinned, want));
         sl.h_bytes = want;
     }
     PCF_CU(ctx, sl.d_rows.ensure(rb + jb + 256));

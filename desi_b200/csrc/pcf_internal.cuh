@@ -142,6 +142,11 @@ struct MemPool {
     ~MemPool() { release(); }
 };
 
+// Every cudaMalloc / cudaMallocHost of the library goes through these, so
+// pcf_alloc_counters can report how many there were and how long they took.
+cudaError_t counted_malloc(void **p, size_t n);
+cudaError_t counted_malloc_host(void **p, size_t n);
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -258,8 +263,18 @@ struct TuneEntry {
     int chunk = 0;       // work items per ticket at most: 0 (the launch rule's 8), 1 or 4
 };
 
+// The page-locked staging pool shared by every context of the process: its
+// blocks go back only once their copies are done (CellGrid's `ready`), so any
+// context may reuse them, and a stream of requests over several contexts
+// reaches a steady set of blocks instead of one per context.
+std::shared_ptr<PinnedPool> shared_pinned_pool();
+
 struct pcf_ctx {
     std::shared_ptr<MemPool> pool = std::make_shared<MemPool>();
+    // the context's own buffers (scratch, histograms, plan slots): reused
+    // only by this context's stream, so a block returned while the
+    // context's kernels still read it is taken again only after them
+    std::shared_ptr<MemPool> scratch_pool = std::make_shared<MemPool>();
     std::map<std::string, TuneEntry> tune;
     TuneEntry tune_override;  // set while the autotuner times a candidate
     bool tune_timing = false; // autotuner: statistics carry kernel time only (no pair
@@ -302,7 +317,7 @@ struct pcf_ctx {
     int pair_variant = 0;  // PCF_OPT_PAIR_VARIANT
     int grid_build = 0;    // PCF_OPT_GRID_BUILD: 0 by size, 1 per-point, 2 bucketed
     bool grid_defer = false;  // PCF_OPT_GRID_DEFER: pcf_grid_build returns once queued
-    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
+    std::shared_ptr<PinnedPool> pinned = shared_pinned_pool();
     std::map<std::string, std::shared_ptr<struct BatchGraph>> graphs;  // pcf_batch_pairs(PCF_GRAPH)
 };
 

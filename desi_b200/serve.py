@@ -40,7 +40,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import api
+from . import _lib, api
 
 KINDS = ("2iso", "2ani", "3iso")
 
@@ -390,6 +390,7 @@ class PcfServer:
     # -- a timed stream ----------------------------------------------------
     def run_stream(self, reqs: list[Request]) -> dict:
         """Submit requests at their arrival times; wait for all; report."""
+        a0 = _lib.alloc_counters()
         t0 = time.perf_counter()
         for r in sorted(reqs, key=lambda r: r.arrival):
             delay = t0 + r.arrival - time.perf_counter()
@@ -398,13 +399,14 @@ class PcfServer:
             self.submit(r)
         results = [r.future.result() for r in reqs]
         t1 = time.perf_counter()
-        return self._report(reqs, results, t1 - t0)
+        return self._report(reqs, results, t1 - t0, a0)
 
     def run_serial(self, reqs: list[Request]) -> dict:
         """The plain per-call form of the same requests: one at a time, in
         arrival order, each submitted when the previous one has completed
         (no overlap on the device), and each gridding its catalogs from host
         memory (no resident grids kept between requests)."""
+        a0 = _lib.alloc_counters()
         t0 = time.perf_counter()
         results = []
         for r in sorted(reqs, key=lambda r: r.arrival):
@@ -412,10 +414,10 @@ class PcfServer:
             self.drop_grids()
         t1 = time.perf_counter()
         order = sorted(reqs, key=lambda r: r.arrival)
-        return self._report(order, results, t1 - t0)
+        return self._report(order, results, t1 - t0, a0)
 
     @staticmethod
-    def _report(reqs, results, wall) -> dict:
+    def _report(reqs, results, wall, allocs0=None) -> dict:
         lat = np.array([(r.t_end - r.t_submit) * 1e3 for r in reqs])
         units = sum(res.get("_units", 0.0) for res in results)
         tri = sum(res.get("_triangles", 0.0) for res in results)
@@ -432,7 +434,16 @@ class PcfServer:
                 "pairs": units, "triangles": tri,
                 "pairs_per_s": units / wall, "triplets_per_s": tri / wall,
                 "overlapping_starts": overlap, "slot_seconds_by_kind": busy,
+                "allocations": _alloc_delta(allocs0),
                 "results": results}
+
+
+def _alloc_delta(a0):
+    """Library allocations (pcf_alloc_counters) since the counters `a0`."""
+    if a0 is None:
+        return None
+    a1 = _lib.alloc_counters()
+    return {k: a1[k] - a0[k] for k in a1}
 
 
 def make_stream_mixed(n_requests: int, rate_hz: float, seed: int = 6000, n_max: int = 1_000_000,

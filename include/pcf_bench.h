@@ -85,6 +85,13 @@ pcf_status pcf_ctx_profile_read(pcf_ctx *ctx, double *total_ms, int64_t *launche
 pcf_status pcf_ctx_profile_read_grid(pcf_ctx *ctx, double *total_ms, int64_t *builds,
                                      int64_t *points);
 
+/* Process-wide allocation counters: device allocations (cudaMalloc) and
+ * page-locked host allocations (cudaMallocHost) the library has made, their
+ * bytes and the wall time spent in those calls (each of which can stall other
+ * threads' work on the device).  out[0..5] = device count, device bytes,
+ * device ns, host count, host bytes, host ns. */
+pcf_status pcf_alloc_counters(uint64_t out[6]);
+
 #ifdef __cplusplus
 }
 #endif
