@@ -46,3 +46,16 @@ def test_ctx_create_fails_cleanly_without_gpu():
     from desi_b200 import _lib
     h = ctypes.c_void_p()
     assert _lib.lib().pcf_ctx_create(0, ctypes.byref(h)) != 0
+
+
+def test_alloc_counters_read_on_the_host():
+    """pcf_alloc_counters (include/pcf_bench.h) reads process-wide counters
+    without touching a device: six values, never decreasing."""
+    from desi_b200 import _lib
+    a = _lib.alloc_counters()
+    assert set(a) == {"device_allocs", "device_bytes", "device_s", "host_allocs", "host_bytes",
+                      "host_s"}
+    assert all(v >= 0 for v in a.values())
+    b = _lib.alloc_counters()
+    assert all(b[k] >= a[k] for k in a)
+    assert _lib.lib().pcf_alloc_counters(None) == -1  # PCF_ERR_INVALID_ARG
