@@ -12,13 +12,13 @@ This module runs it on given catalogs the way its CLI expects them:
   is a CUDA-event interval around the kernels, the D2H copies and the file
   writes.
 
-Only the periodic isotropic path (`2iso -bpc`, one random file) is driven:
-its kernels guard every histogram index (cuda/kernels/2isoBPC_k.cuh, the
-`bin>(bn-1)` checks before each atomicAdd) and read points only inside node
-ranges.  The host grid (make_nodos, create_grid.cuh:130-133) indexes cells by
-(int)(x / size_node) without a clamp, so coordinates are kept at least 1e-3
-inside the box.  The `-a` path and the anisotropic cross kernels are not
-run.
+Driven: the periodic paths `2iso -bpc`, `3iso -bpc` and `3ani -bpc`, one
+random file.  Their kernels guard every histogram index (the `bin>(bn-1)`
+checks before each atomicAdd in 2isoBPC_k.cuh, 3isoBPC_k.cuh and
+3aniBPC_k.cuh) and read points only inside node ranges.  The host grid
+(make_nodos, create_grid.cuh:130-133) indexes cells by (int)(x / size_node)
+without a clamp, so coordinates are kept at least 1e-3 inside the box.  The
+`-a` path and the anisotropic pair cross kernels are not run.
 """
 import os
 import re
@@ -73,4 +73,46 @@ def run_2iso_bpc(D, R, box, bins, dmax, workdir, timeout=600):
     for kind in ("DD", "RR", "DR"):
         name = {"DD": "data.dat", "RR": "rand.dat", "DR": "rand.dat"}[kind]
         res[kind] = np.loadtxt(os.path.join(workdir, "results", f"{kind}iso_BPC_{name}"))
+    return res
+
+
+def _run_cli(exe, args, workdir, timeout):
+    t0 = time.perf_counter()
+    p = subprocess.run([exe] + args, cwd=os.path.join(workdir, "run"), capture_output=True,
+                       text=True, timeout=timeout)
+    wall = time.perf_counter() - t0
+    if p.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(exe)} exited {p.returncode}: {p.stdout[-300:]} {p.stderr[-300:]}")
+    m = re.search(r"Spent\s+([0-9.eE+-]+)\s+miliseconds", p.stdout)
+    return (float(m.group(1)) if m else None), wall
+
+
+def run_3pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, timeout=600, extra=()):
+    """Runs `<kind> -bpc -p partitions` (kind "3iso" or "3ani") of the
+    reference's CUDA program, or of another program with the same command
+    line (exe, e.g. this library's PCF.out), on D and one random catalog R
+    (len(D) == len(R)); returns {"ms", "wall_s", "DDD", "RRR", "DDR", "DRR"}
+    with each histogram as written: bins^3 values (the reference's 3ani
+    writer keeps the first bins^3 of its bins^5 histogram, pcf3aniBPC.cuh:123,
+    create_grid.cuh:197) or, for a writer of the full 3ani histogram, all
+    bins^5.  The reference's kernels read points only inside node ranges and
+    check every bin index (3isoBPC_k.cuh:80-85, 3aniBPC_k.cuh:77-85); its
+    host grid does not clamp cell indices, so coordinates are kept 1e-3 inside
+    the box by the caller (inside_box).  extra: more command-line flags (this
+    library's -exact)."""
+    if len(D) != len(R):
+        raise ValueError("the reference reads -n rows from each file")
+    exe = exe or EXE
+    for sub in ("data", "results", "run"):
+        os.makedirs(os.path.join(workdir, sub), exist_ok=True)
+    _write(os.path.join(workdir, "data", "data.dat"), D)
+    _write(os.path.join(workdir, "data", "rand.dat"), R)
+    args = [kind, "-bpc", "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)), "-b", str(int(bins)),
+            "-d", repr(float(dmax)), "-s", repr(float(box)), "-p", str(int(partitions))] + list(extra)
+    ms, wall = _run_cli(exe, args, workdir, timeout)
+    res = {"ms": ms, "wall_s": wall}
+    sfx = "ani" if kind == "3ani" else "iso"
+    for h in ("DDD", "RRR", "DDR", "DRR"):
+        name = "data.dat" if h == "DDD" else "rand.dat"
+        res[h] = np.loadtxt(os.path.join(workdir, "results", f"{h}{sfx}_BPC_{name}")).ravel()
     return res
