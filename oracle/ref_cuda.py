@@ -116,3 +116,28 @@ def run_3pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, time
         name = "data.dat" if h == "DDD" else "rand.dat"
         res[h] = np.loadtxt(os.path.join(workdir, "results", f"{h}{sfx}_BPC_{name}")).ravel()
     return res
+
+
+def run_2pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, timeout=600):
+    """Runs `<kind> -bpc -p partitions` (kind "2iso" or "2ani") of the
+    reference's CUDA program, or of another program with the same command
+    line (exe), on D and one random catalog R; returns {"ms", "wall_s", "DD",
+    "RR", "DR"} as written (bins values, or bins x bins for 2ani).  The
+    reference's XY2ani_BPC weights most pairs by an unset variable
+    (2aniBPC_k.cuh:372,410,429), so its 2ani DR is not a result."""
+    if len(D) != len(R):
+        raise ValueError("the reference reads -n rows from each file")
+    exe = exe or EXE
+    for sub in ("data", "results", "run"):
+        os.makedirs(os.path.join(workdir, sub), exist_ok=True)
+    _write(os.path.join(workdir, "data", "data.dat"), D)
+    _write(os.path.join(workdir, "data", "rand.dat"), R)
+    args = [kind, "-bpc", "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)), "-b", str(int(bins)),
+            "-d", repr(float(dmax)), "-s", repr(float(box)), "-p", str(int(partitions))]
+    ms, wall = _run_cli(exe, args, workdir, timeout)
+    res = {"ms": ms, "wall_s": wall}
+    sfx = "ani" if kind == "2ani" else "iso"
+    for h in ("DD", "RR", "DR"):
+        name = "data.dat" if h == "DD" else "rand.dat"
+        res[h] = np.loadtxt(os.path.join(workdir, "results", f"{h}{sfx}_BPC_{name}"))
+    return res

@@ -45,3 +45,30 @@ def test_pcf_out_equals_reference_program(kind, bins, dmax):
         assert runs["exact"][h][:ref.size].sum() >= ref.sum(), h
     if kind == "3iso":
         assert runs["exact"]["DDD"].sum() > runs["ref"]["DDD"].sum()
+
+
+@pytest.mark.parametrize("kind", ["2iso", "2ani"])
+def test_pcf_out_pairs_equal_reference_program(kind):
+    """`2iso -bpc` and `2ani -bpc` of the reference's program and of this
+    PCF.out on lattice catalogs (integer coordinates of a 60 box, weights in
+    {0.5, 1, 1.5, 2}: every FP32 separation and weight product, and every
+    sum, is exact in both) are equal bit for bit: DD, RR and DR, and for 2ani
+    DD and RR (the reference's XY2ani_BPC weights most pairs by an unset
+    variable, 2aniBPC_k.cuh:410)."""
+    if not ref_cuda.available():
+        pytest.skip("oracle/_ref/PCF_ref_cuda.out not built")
+    rng = np.random.default_rng(77)
+    n, box, bins, dmax, P = 3000, 60.0, 10, 20.0, 12
+    D = np.empty((n, 4), np.float32)
+    R = np.empty((n, 4), np.float32)
+    D[:, :3] = 2 * rng.integers(0, 30, size=(n, 3))
+    R[:, :3] = 2 * rng.integers(0, 30, size=(n, 3)) + 1
+    D[:, 3] = rng.choice([0.5, 1.0, 1.5, 2.0], n)
+    R[:, 3] = rng.choice([0.5, 1.0, 1.5, 2.0], n)
+    runs = {}
+    for who, exe in (("ref", None), ("ours", OURS)):
+        with tempfile.TemporaryDirectory() as wd:
+            runs[who] = ref_cuda.run_2pt_bpc(kind, D, R, box, bins, dmax, P, wd, exe=exe, timeout=300)
+    for h in ("DD", "RR") + (("DR",) if kind == "2iso" else ()):
+        assert runs["ref"][h].sum() > 0, h
+        assert np.array_equal(runs["ours"][h], runs["ref"][h]), h
