@@ -87,7 +87,8 @@ def _run_cli(exe, args, workdir, timeout):
     return (float(m.group(1)) if m else None), wall
 
 
-def run_3pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, timeout=600, extra=()):
+def run_3pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, timeout=600, extra=(),
+                bpc=True):
     """Runs `<kind> -bpc -p partitions` (kind "3iso" or "3ani") of the
     reference's CUDA program, or of another program with the same command
     line (exe, e.g. this library's PCF.out), on D and one random catalog R
@@ -99,7 +100,8 @@ def run_3pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, time
     check every bin index (3isoBPC_k.cuh:80-85, 3aniBPC_k.cuh:77-85); its
     host grid does not clamp cell indices, so coordinates are kept 1e-3 inside
     the box by the caller (inside_box).  extra: more command-line flags (this
-    library's -exact)."""
+    library's -exact); bpc=False runs the plain path (`<kind>` without -bpc:
+    XXX3iso / XXY3iso, XXX3ani / XXY3ani)."""
     if len(D) != len(R):
         raise ValueError("the reference reads -n rows from each file")
     exe = exe or EXE
@@ -107,24 +109,29 @@ def run_3pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, time
         os.makedirs(os.path.join(workdir, sub), exist_ok=True)
     _write(os.path.join(workdir, "data", "data.dat"), D)
     _write(os.path.join(workdir, "data", "rand.dat"), R)
-    args = [kind, "-bpc", "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)), "-b", str(int(bins)),
-            "-d", repr(float(dmax)), "-s", repr(float(box)), "-p", str(int(partitions))] + list(extra)
+    args = [kind] + (["-bpc"] if bpc else []) + [
+        "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)), "-b", str(int(bins)),
+        "-d", repr(float(dmax)), "-s", repr(float(box)), "-p", str(int(partitions))] + list(extra)
     ms, wall = _run_cli(exe, args, workdir, timeout)
     res = {"ms": ms, "wall_s": wall}
-    sfx = "ani" if kind == "3ani" else "iso"
+    sfx = ("ani" if kind == "3ani" else "iso") + ("_BPC" if bpc else "")
     for h in ("DDD", "RRR", "DDR", "DRR"):
         name = "data.dat" if h == "DDD" else "rand.dat"
-        res[h] = np.loadtxt(os.path.join(workdir, "results", f"{h}{sfx}_BPC_{name}")).ravel()
+        res[h] = np.loadtxt(os.path.join(workdir, "results", f"{h}{sfx}_{name}")).ravel()
     return res
 
 
-def run_2pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, timeout=600):
+def run_2pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, timeout=600, bpc=True):
     """Runs `<kind> -bpc -p partitions` (kind "2iso" or "2ani") of the
     reference's CUDA program, or of another program with the same command
     line (exe), on D and one random catalog R; returns {"ms", "wall_s", "DD",
     "RR", "DR"} as written (bins values, or bins x bins for 2ani).  The
     reference's XY2ani_BPC weights most pairs by an unset variable
-    (2aniBPC_k.cuh:372,410,429), so its 2ani DR is not a result."""
+    (2aniBPC_k.cuh:372,410,429), so its 2ani DR is not a result.  bpc=False
+    runs the plain path (XX2iso / XY2iso, XX2ani / XY2ani), whose XY2ani
+    takes the weight of its R point from the D array at the R index
+    (2ani_k.cuh:128): in bounds with one random file of the same length, so
+    its DR is a result with unit weights only."""
     if len(D) != len(R):
         raise ValueError("the reference reads -n rows from each file")
     exe = exe or EXE
@@ -132,12 +139,13 @@ def run_2pt_bpc(kind, D, R, box, bins, dmax, partitions, workdir, exe=None, time
         os.makedirs(os.path.join(workdir, sub), exist_ok=True)
     _write(os.path.join(workdir, "data", "data.dat"), D)
     _write(os.path.join(workdir, "data", "rand.dat"), R)
-    args = [kind, "-bpc", "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)), "-b", str(int(bins)),
-            "-d", repr(float(dmax)), "-s", repr(float(box)), "-p", str(int(partitions))]
+    args = [kind] + (["-bpc"] if bpc else []) + [
+        "-f", "data.dat", "-r", "rand.dat", "-n", str(len(D)), "-b", str(int(bins)),
+        "-d", repr(float(dmax)), "-s", repr(float(box)), "-p", str(int(partitions))]
     ms, wall = _run_cli(exe, args, workdir, timeout)
     res = {"ms": ms, "wall_s": wall}
-    sfx = "ani" if kind == "2ani" else "iso"
+    sfx = ("ani" if kind == "2ani" else "iso") + ("_BPC" if bpc else "")
     for h in ("DD", "RR", "DR"):
         name = "data.dat" if h == "DD" else "rand.dat"
-        res[h] = np.loadtxt(os.path.join(workdir, "results", f"{h}{sfx}_BPC_{name}"))
+        res[h] = np.loadtxt(os.path.join(workdir, "results", f"{h}{sfx}_{name}"))
     return res

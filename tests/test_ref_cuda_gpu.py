@@ -72,3 +72,42 @@ def test_pcf_out_pairs_equal_reference_program(kind):
     for h in ("DD", "RR") + (("DR",) if kind == "2iso" else ()):
         assert runs["ref"][h].sum() > 0, h
         assert np.array_equal(runs["ours"][h], runs["ref"][h]), h
+
+
+def _lattice(n, seed, weights):
+    rng = np.random.default_rng(seed)
+    D = np.empty((n, 4), np.float32)
+    R = np.empty((n, 4), np.float32)
+    D[:, :3] = 2 * rng.integers(0, 30, size=(n, 3))
+    R[:, :3] = 2 * rng.integers(0, 30, size=(n, 3)) + 1
+    D[:, 3] = rng.choice(weights, n)
+    R[:, 3] = rng.choice(weights, n)
+    return D, R
+
+
+@pytest.mark.parametrize("kind", ["2iso", "2ani", "3iso", "3ani"])
+def test_pcf_out_plain_equals_reference_program(kind):
+    """The plain paths (no -bpc) of the reference's program and of this
+    PCF.out on lattice catalogs of a 60 box, where every FP32 separation is
+    exact: every histogram equal bit for bit.  Weights in {0.5, 1, 1.5, 2}
+    for 2iso; unit weights for 2ani (the reference's XY2ani takes the R
+    point's weight from the D array, 2ani_k.cuh:128) and for the 3-point
+    kernels (which multiply every third point's weight into a running
+    product)."""
+    if not ref_cuda.available():
+        pytest.skip("oracle/_ref/PCF_ref_cuda.out not built")
+    box, dmax, P = 60.0, 20.0, 12
+    three = kind.startswith("3")
+    n = 1000 if three else 3000
+    bins = 6 if kind == "3ani" else 10
+    D, R = _lattice(n, 91, [1.0] if kind != "2iso" else [0.5, 1.0, 1.5, 2.0])
+    run = ref_cuda.run_3pt_bpc if three else ref_cuda.run_2pt_bpc
+    runs = {}
+    for who, exe in (("ref", None), ("ours", OURS)):
+        with tempfile.TemporaryDirectory() as wd:
+            runs[who] = run(kind, D, R, box, bins, dmax, P, wd, exe=exe, timeout=300, bpc=False)
+    for h in (("DDD", "RRR", "DDR", "DRR") if three else ("DD", "RR", "DR")):
+        ref = runs["ref"][h]
+        assert ref.sum() > 0, h
+        got = runs["ours"][h].ravel()[:ref.size].reshape(ref.shape)
+        assert np.array_equal(got, ref), h
