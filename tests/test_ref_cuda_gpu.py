@@ -111,3 +111,27 @@ def test_pcf_out_plain_equals_reference_program(kind):
         assert ref.sum() > 0, h
         got = runs["ours"][h].ravel()[:ref.size].reshape(ref.shape)
         assert np.array_equal(got, ref), h
+
+
+def test_pcf_out_analytic_rr_equals_reference_program():
+    """`2iso -bpc -a` (the periodic DD counted, RR and DR from the analytic
+    formula, pcf2isoBPC.cuh:166-270) of the reference's program and of this
+    PCF.out on a weighted lattice: the three files equal bit for bit.  (The
+    3iso analytic path is not run: its DD2iso_forBPC bins a separation just
+    below dmax with no bound check, 3isoBPC_k.cuh:1754-1757.)"""
+    if not ref_cuda.available():
+        pytest.skip("oracle/_ref/PCF_ref_cuda.out not built")
+    D, _ = _lattice(3000, 93, [0.5, 1.0, 1.5, 2.0])
+    res = {}
+    for who, exe in (("ref", ref_cuda.EXE), ("ours", OURS)):
+        with tempfile.TemporaryDirectory() as wd:
+            for sub in ("data", "results", "run"):
+                os.makedirs(os.path.join(wd, sub))
+            ref_cuda._write(os.path.join(wd, "data", "data.dat"), D)
+            ref_cuda._run_cli(exe, ["2iso", "-bpc", "-a", "-f", "data.dat", "-n", str(len(D)), "-b", "10",
+                                    "-d", "20.0", "-s", "60.0", "-p", "12"], wd, 300)
+            res[who] = {h: np.loadtxt(os.path.join(wd, "results", f"{h}iso_BPCanalytic_data.dat"))
+                        for h in ("DD", "RR", "DR")}
+    for h in ("DD", "RR", "DR"):
+        assert res["ref"][h].sum() > 0, h
+        assert np.array_equal(res["ours"][h], res["ref"][h]), (h, res["ours"][h], res["ref"][h])
