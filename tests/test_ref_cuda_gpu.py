@@ -135,3 +135,37 @@ def test_pcf_out_analytic_rr_equals_reference_program():
     for h in ("DD", "RR", "DR"):
         assert res["ref"][h].sum() > 0, h
         assert np.array_equal(res["ours"][h], res["ref"][h]), (h, res["ours"][h], res["ref"][h])
+
+
+@pytest.mark.parametrize("bpc", [False, True], ids=["plain", "periodic"])
+def test_pcf_out_random_directory_equals_reference_program(bpc):
+    """`2iso -rd DIR/` (one data catalog against every file of the directory,
+    cuda/main.cu:157-192, pcf2iso.cuh:96-104 with its node and bin offsets per
+    random file) of the reference's program and of this PCF.out (one batched
+    launch) on weighted lattices: DD and every RR / DR file equal bit for bit.
+    (2ani -rd is not run: the reference's XY2ani reads the R weight from the D
+    array at an R index that passes D's end from the second random file on,
+    2ani_k.cuh:128.)"""
+    if not ref_cuda.available():
+        pytest.skip("oracle/_ref/PCF_ref_cuda.out not built")
+    n, w = 2000, [0.5, 1.0, 1.5, 2.0]
+    D, R1 = _lattice(n, 95, w)
+    _, R2 = _lattice(n, 96, w)
+    _, R3 = _lattice(n, 97, w)
+    res = {}
+    for who, exe in (("ref", ref_cuda.EXE), ("ours", OURS)):
+        with tempfile.TemporaryDirectory() as wd:
+            for sub in ("data", "data/rands", "results", "run"):
+                os.makedirs(os.path.join(wd, sub))
+            ref_cuda._write(os.path.join(wd, "data", "data.dat"), D)
+            for k, R in enumerate((R1, R2, R3)):
+                ref_cuda._write(os.path.join(wd, "data", "rands", f"r{k}.dat"), R)
+            ref_cuda._run_cli(exe, ["2iso"] + (["-bpc"] if bpc else []) + [
+                "-f", "data.dat", "-rd", "rands/", "-n", str(n), "-b", "10", "-d", "20.0",
+                "-s", "60.0", "-p", "12"], wd, 300)
+            tag = "iso_BPC_" if bpc else "iso_"
+            names = [f"DD{tag}data.dat"] + [f"{h}{tag}r{k}.dat" for k in range(3) for h in ("RR", "DR")]
+            res[who] = {nm: np.loadtxt(os.path.join(wd, "results", nm)) for nm in names}
+    for nm, ref in res["ref"].items():
+        assert ref.sum() > 0, nm
+        assert np.array_equal(res["ours"][nm], ref), nm
