@@ -143,55 +143,77 @@ __device__ __forceinline__ void gate_corner(const GateGeom &g, float x, float y,
     }
 }
 
-// Axes along which q is joined to p through its periodic image.
-__device__ __forceinline__ unsigned gate_wrap(float px, float py, float pz, float qx, float qy, float qz,
-                                              float L) {
-    const double h = 0.5 * (double)L;
-    const double d[3] = {(double)qx - (double)px, (double)qy - (double)py, (double)qz - (double)pz};
-    unsigned b = 0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-        if (d[a] > h || d[a] < -h) b |= 1u << a;
-    return b;
+// One list entry's node and image: node indices of the reference's grid (9
+// bits per axis, partitions <= 512) and the axes along which the entry is
+// joined to the anchor through its periodic image (bits 27-29).
+__device__ __forceinline__ unsigned gate_pack(const GateGeom &g, float x, float y, float z, unsigned wrap) {
+    const int rx = min(max((int)__fdiv_rn(x, g.s), 0), g.P - 1);
+    const int ry = min(max((int)__fdiv_rn(y, g.s), 0), g.P - 1);
+    const int rz = min(max((int)__fdiv_rn(z, g.s), 0), g.P - 1);
+    return (unsigned)rx | ((unsigned)ry << 9) | ((unsigned)rz << 18) | (wrap << 27);
+}
+
+struct GateNode {
+    float x, y, z;  // node corner
+    unsigned wrap;  // image axes relative to the anchor
+};
+
+__device__ __forceinline__ GateNode gate_unpack(const GateGeom &g, unsigned v) {
+    GateNode n;
+    n.x = __fmul_rn((float)(v & 511u), g.s);
+    n.y = __fmul_rn((float)((v >> 9) & 511u), g.s);
+    n.z = __fmul_rn((float)((v >> 18) & 511u), g.s);
+    n.wrap = (v >> 27) & 7u;
+    return n;
+}
+
+__device__ __forceinline__ float gate_pick(int i, float a, float b, float c) {
+    return i == 0 ? a : (i == 1 ? b : c);
 }
 
 // Times the reference's blocks count the ordered triangle (1, 2, 3) with node
-// corners n1, n2, n3 whose sides 12 and 31 are in range through the images
-// s2 and s3: 0, 1 or 2.
-__device__ __noinline__ int gate_mult(const GateGeom &g, const float *n1, const float *n2, const float *n3,
-                                      unsigned s2, unsigned s3) {
-    const signed char *blk = kGateByImage[s2 | (s3 << 3)];
+// corners n1, n2, n3, its sides 12 and 31 in range through the images
+// n2.wrap and n3.wrap: 0, 1 or 2.  blocks / by_image: kGateBlocks and
+// kGateByImage (copied to shared memory by the caller).
+__device__ __forceinline__ int gate_mult(const GateGeom &g, const GateNode &n1, const GateNode &n2,
+                                         const GateNode &n3, const GateBlock *blocks,
+                                         const signed char (*by_image)[2]) {
+    const signed char *blk = by_image[n2.wrap | (n3.wrap << 3)];
     if (blk[0] < 0) return 0;
-    float dn[3][3], dd[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        dn[0][a] = fabsf(__fsub_rn(n2[a], n1[a]));
-        dn[1][a] = fabsf(__fsub_rn(n3[a], n2[a]));
-        dn[2][a] = fabsf(__fsub_rn(n1[a], n3[a]));
-    }
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-        dd[q] = __fmaf_rn(dn[q][2], dn[q][2], __fmaf_rn(dn[q][1], dn[q][1], __fmul_rn(dn[q][0], dn[q][0])));
+    // |dn| per pair (12, 23, 31) and axis, and the squared node distances
+    const float x12 = fabsf(__fsub_rn(n2.x, n1.x)), y12 = fabsf(__fsub_rn(n2.y, n1.y)),
+                z12 = fabsf(__fsub_rn(n2.z, n1.z));
+    const float x23 = fabsf(__fsub_rn(n3.x, n2.x)), y23 = fabsf(__fsub_rn(n3.y, n2.y)),
+                z23 = fabsf(__fsub_rn(n3.z, n2.z));
+    const float x31 = fabsf(__fsub_rn(n1.x, n3.x)), y31 = fabsf(__fsub_rn(n1.y, n3.y)),
+                z31 = fabsf(__fsub_rn(n1.z, n3.z));
+    const float d12 = __fmaf_rn(z12, z12, __fmaf_rn(y12, y12, __fmul_rn(x12, x12)));
+    const float d23 = __fmaf_rn(z23, z23, __fmaf_rn(y23, y23, __fmul_rn(x23, x23)));
+    const float d31 = __fmaf_rn(z31, z31, __fmaf_rn(y31, y31, __fmul_rn(x31, x31)));
     unsigned f2 = 0, f3 = 0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        if ((n1[a] <= g.fd && n2[a] >= g.fdn) || (n2[a] <= g.fd && n1[a] >= g.fdn)) f2 |= 1u << a;
-        if ((n1[a] <= g.fd && n3[a] >= g.fdn) || (n3[a] <= g.fd && n1[a] >= g.fdn)) f3 |= 1u << a;
-    }
+    f2 |= ((n1.x <= g.fd && n2.x >= g.fdn) || (n2.x <= g.fd && n1.x >= g.fdn)) ? 1u : 0u;
+    f2 |= ((n1.y <= g.fd && n2.y >= g.fdn) || (n2.y <= g.fd && n1.y >= g.fdn)) ? 2u : 0u;
+    f2 |= ((n1.z <= g.fd && n2.z >= g.fdn) || (n2.z <= g.fd && n1.z >= g.fdn)) ? 4u : 0u;
+    f3 |= ((n1.x <= g.fd && n3.x >= g.fdn) || (n3.x <= g.fd && n1.x >= g.fdn)) ? 1u : 0u;
+    f3 |= ((n1.y <= g.fd && n3.y >= g.fdn) || (n3.y <= g.fd && n1.y >= g.fdn)) ? 2u : 0u;
+    f3 |= ((n1.z <= g.fd && n3.z >= g.fdn) || (n3.z <= g.fd && n1.z >= g.fdn)) ? 4u : 0u;
     int m = 0;
     for (int e = 0; e < 2; ++e) {
         const int b = blk[e];
         if (b < 0) break;
-        const GateBlock &B = kGateBlocks[b];
+        const GateBlock &B = blocks[b];
         if ((f2 & B.a2) != B.a2 || (f3 & B.a3) != B.a3) continue;
         bool ok = true;
         for (int t = 0; t < 3 && ok; ++t) {
             const GateTest &T = B.t[t];
-            float v = dd[T.pair];
+            const int p = T.pair;
+            float v = gate_pick(p, d12, d23, d31);
             if (T.ax[0] >= 0) {
-                float sm = dn[T.pair][T.ax[0]];
-                if (T.ax[1] >= 0) sm = __fadd_rn(sm, dn[T.pair][T.ax[1]]);
-                if (T.ax[2] >= 0) sm = __fadd_rn(sm, dn[T.pair][T.ax[2]]);
+                const float dx = gate_pick(p, x12, x23, x31), dy = gate_pick(p, y12, y23, y31),
+                            dz = gate_pick(p, z12, z23, z31);
+                float sm = gate_pick(T.ax[0], dx, dy, dz);
+                if (T.ax[1] >= 0) sm = __fadd_rn(sm, gate_pick(T.ax[1], dx, dy, dz));
+                if (T.ax[2] >= 0) sm = __fadd_rn(sm, gate_pick(T.ax[2], dx, dy, dz));
                 v = __fmaf_rn((float)T.k, g.L2, v);
                 v = __fmaf_rn(-__fmul_rn(2.0f, sm), g.L, v);
             }

@@ -162,11 +162,13 @@ __device__ __noinline__ int exact_angle(float ax, float ay, float az, float bx, 
     return (t >= 0 && t < bins) ? t : -1;
 }
 
+// ginfo (PCF_REF_NODE_GATES): per entry, its node on the reference's grid
+// and the axes of its image relative to the anchor (gate_pack).
 template <bool ANG>
 __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, float hz, int hcell_ix,
                            int hcell_iy, int hcell_iz, int only_after, const PairRule &rule,
                            float4 *list, float *wlist, int cap, int *s_n, unsigned &n_rechk,
-                           unsigned short *ang = nullptr, int step = 1) {
+                           unsigned short *ang = nullptr, int step = 1, unsigned *ginfo = nullptr) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int P = A.P;
     for (int r = 0; r < A.n_rows; ++r) {
@@ -229,6 +231,10 @@ __device__ void build_list(const TripArgs &A, const Cat &C, float hx, float hy, 
                         list[step * pos] = make_float4(vx, vy, vz, __int_as_float((c << 8) | bin));
                         if (wlist) wlist[pos] = C.w[c];
                         if (ANG) ang[pos] = (unsigned short)(bin | (tang << 8));
+                        if (ginfo)
+                            ginfo[pos] = gate_pack(A.gate, C.x[c], C.y[c], C.z[c],
+                                                   (sx != 0.f ? 1u : 0u) | (sy != 0.f ? 2u : 0u) |
+                                                       (rz[sgi] != 0.f ? 4u : 0u));
                     }
                 }
             }
@@ -646,9 +652,22 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
     unsigned short *aK = aJ + A.capJ;
     float *swJ = reinterpret_cast<float *>(aK + (MIXED ? A.capK : 0) + 8);
     float *swK = swJ + (WEIGHTED ? A.capJ : 0);
+    // node / image words of the gated counts, 16-byte aligned past the weights
+    unsigned *gJ = reinterpret_cast<unsigned *>(
+        (reinterpret_cast<uintptr_t>(swK + (WEIGHTED && MIXED ? A.capK : 0)) + 15) & ~(uintptr_t)15);
+    unsigned *gK = gJ + A.capJ;
     __shared__ int s_anchor, s_nJ, s_nK;
     __shared__ unsigned s_stop;
+    __shared__ GateBlock s_gates[GATES ? 64 : 1];
+    __shared__ signed char s_gate_by[GATES ? 64 : 1][2];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (GATES) {
+        for (int k = tid; k < 64; k += kTThreads) {
+            s_gates[k] = kGateBlocks[k];
+            s_gate_by[k][0] = kGateByImage[k][0];
+            s_gate_by[k][1] = kGateByImage[k][1];
+        }
+    }
     unsigned n_rechk = 0;
     unsigned long long n_tri = 0;
     long long taken = 0;
@@ -673,12 +692,13 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
         const int ciy = min(max((int)__fdiv_rn(hy, A.cell), 0), P - 1);
         const int ciz = min(max((int)__fdiv_rn(hz, A.cell), 0), P - 1);
         build_list<!ISO3>(A, A.X, hx, hy, hz, cix, ciy, ciz, -1, A.rXX, sJ, WEIGHTED ? swJ : nullptr,
-                          A.capJ, &s_nJ, n_rechk, aJ);
+                          A.capJ, &s_nJ, n_rechk, aJ, 1, GATES ? gJ : nullptr);
         if (MIXED)
             build_list<!ISO3>(A, A.Y, hx, hy, hz, cix, ciy, ciz, -1, A.rXY, sK,
-                              WEIGHTED ? swK : nullptr, A.capK, &s_nK, n_rechk, aK);
-        float n1[3];
-        if (GATES) gate_corner(A.gate, hx, hy, hz, n1);
+                              WEIGHTED ? swK : nullptr, A.capK, &s_nK, n_rechk, aK, 1,
+                              GATES ? gK : nullptr);
+        GateNode n1{};
+        if (GATES) n1 = gate_unpack(A.gate, gate_pack(A.gate, hx, hy, hz, 0u));
         __syncthreads();
         const int nJ = s_nJ, nK = MIXED ? s_nK : s_nJ;
         if (nJ > A.capJ || (MIXED && nK > A.capK)) {
@@ -696,13 +716,9 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
             const unsigned short pj = ISO3 ? (unsigned short)(__float_as_int(ej.w) & 255) : aJ[jj];
             const long long base = ISO3 ? (long long)pj * B2 : (long long)(pj & 255) * B4 + (long long)(pj >> 8) * B;
             const double wij = WEIGHTED ? (double)hw * (double)swJ[jj] : 1.0;
-            float n2[3];
-            unsigned s2 = 0;
-            if (GATES) {
-                const float xj = A.X.x[jidx], yj = A.X.y[jidx], zj = A.X.z[jidx];
-                gate_corner(A.gate, xj, yj, zj, n2);
-                s2 = gate_wrap(hx, hy, hz, xj, yj, zj, A.box);
-            }
+            GateNode n2{};
+            if (GATES) n2 = gate_unpack(A.gate, gJ[jj]);
+            const unsigned *GK = MIXED ? gK : gJ;
             for (int kk = lane; kk < nK; kk += 32) {
                 if (!MIXED && kk == jj) continue;
                 const float4 ek = LK[kk];
@@ -720,12 +736,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_triplets_ani(const TripArgs A)
                 if (c >= 0) {
                     int mult = 1;
                     if (GATES) {
-                        const int kidx = (int)((unsigned)__float_as_int(ek.w) >> 8);
-                        const Cat &CK = MIXED ? A.Y : A.X;
-                        const float xk = CK.x[kidx], yk = CK.y[kidx], zk = CK.z[kidx];
-                        float n3[3];
-                        gate_corner(A.gate, xk, yk, zk, n3);
-                        mult = gate_mult(A.gate, n1, n2, n3, s2, gate_wrap(hx, hy, hz, xk, yk, zk, A.box));
+                        mult = gate_mult(A.gate, n1, n2, gate_unpack(A.gate, GK[kk]), s_gates, s_gate_by);
                         if (mult == 0) continue;
                     }
                     long long slot;
@@ -1203,9 +1214,10 @@ static pcf_status count_triplets_ordered(pcf_ctx *ctx, const pcf_grid *x_, const
             ctx->last_error = "PCF_REF_NODE_GATES applies to periodic counts (PCF_BPC)";
             return PCF_ERR_INVALID_ARG;
         }
-        if (x_->user_P < 1 || (y_ && (y_->user_P != x_->user_P || y_->box != x_->box))) {
+        if (x_->user_P < 1 || x_->user_P > 512 ||
+            (y_ && (y_->user_P != x_->user_P || y_->box != x_->box))) {
             ctx->last_error = "PCF_REF_NODE_GATES: the reference's node grid is the partitions given to "
-                              "pcf_grid_build, the same for both grids";
+                              "pcf_grid_build (1 to 512), the same for both grids";
             return PCF_ERR_INVALID_ARG;
         }
     }
@@ -1259,8 +1271,8 @@ static pcf_status count_triplets_ordered(pcf_ctx *ctx, const pcf_grid *x_, const
         A.fc.w = std::min(8000u, (unsigned)std::ceil((wr + std::ldexp(1.0, -16)) * 32768.0) + 1u);
     }
     const bool weighted = !(X->unit_weights && (!mixed || Y->unit_weights));
-    const size_t ent = 16 + 2 + (weighted ? 4 : 0);
-    const size_t room = 227 * 1024 - 256;
+    const size_t ent = 16 + 2 + (weighted ? 4 : 0) + (gates ? 4 : 0);
+    const size_t room = 227 * 1024 - 256 - (gates ? 64 * sizeof(GateBlock) + 128 + 64 : 0);
     if (mixed) {
         A.capJ = (int)(room / ent / 3);
         A.capK = (int)(room / ent) - A.capJ - 8;
