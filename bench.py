@@ -943,6 +943,46 @@ def run_reference_cuda():
             "timer": "the program's own CUDA events around kernels, D2H copies and file writes"}
 
 
+def run_reference_cuda_3iso(n=2048, bins=20, dmax=60.0, partitions=20):
+    """`3iso -bpc -p 20` of the reference's CUDA program and of this
+    library's PCF.out (which counts through the reference kernels' node gates
+    by default) on the same files: clustered data and uniform randoms of n
+    points in the 250 box, unit weights.  Both programs' own printed times,
+    whether every histogram file is equal, and this library's -exact count of
+    DDD beside the reference's."""
+    import tempfile
+    from desi_b200 import catalog
+    from oracle import ref_cuda
+    if not ref_cuda.available():
+        return {"unavailable": "oracle/_ref/PCF_ref_cuda.out not built"}
+    box = WORKLOAD["box"]
+    D = ref_cuda.inside_box(catalog.neyman_scott(n, box, seed=11), box)
+    R = ref_cuda.inside_box(catalog.uniform(n, box, seed=12), box)
+    D[:, 3] = 1.0
+    R[:, 3] = 1.0
+    ours_exe = os.path.join(ROOT, "desi_b200", "PCF.out")
+    runs = {}
+    for who, exe, extra in (("reference", None, ()), ("ours", ours_exe, ()),
+                            ("ours_exact", ours_exe, ("-exact",))):
+        best = None
+        for _ in range(2):  # the first run also pays module loading
+            with tempfile.TemporaryDirectory() as wd:
+                r = ref_cuda.run_3pt_bpc("3iso", D, R, box, bins, dmax, partitions, wd, exe=exe,
+                                         extra=extra, timeout=600)
+            if best is None or r["ms"] < best["ms"]:
+                best = r
+        runs[who] = best
+    hs = ("DDD", "RRR", "DDR", "DRR")
+    return {"workload": f"3iso -bpc -p {partitions}, {n} Neyman-Scott + {n} uniform, box {box:g}, "
+                        f"{bins}^3 bins, dmax {dmax:g}, unit weights",
+            "reference_ms": runs["reference"]["ms"], "ours_ms": runs["ours"]["ms"],
+            "ours_exact_ms": runs["ours_exact"]["ms"],
+            "files_equal": all(bool(np.array_equal(runs["ours"][h], runs["reference"][h])) for h in hs),
+            "ddd_reference": float(runs["reference"]["DDD"].sum()),
+            "ddd_exact": float(runs["ours_exact"]["DDD"].sum()),
+            "timer": "each program's own printed time (kernels, copies and file writes)"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -966,7 +1006,8 @@ def run_reference(args, rank, world):
             break
     tot = sum(times)
     value = pairs_step * len(times) / tot
-    extra = {"reference_cuda": run_reference_cuda()} if args.ref_gpu else {}
+    extra = ({"reference_cuda": run_reference_cuda(), "reference_cuda_3iso": run_reference_cuda_3iso()}
+             if args.ref_gpu else {})
     return {
         **extra,
         "impl": "reference", "metric": "pairs/s", "value": value, "unit": "pairs/s",
@@ -1005,7 +1046,8 @@ def main():
                     help="skip the triplet / batched / served measurements")
     ap.add_argument("--ref-gpu", action="store_true",
                     help="with --impl reference: also run the reference's CUDA program "
-                         "(2iso -bpc on the bench catalogs) and report its time")
+                         "(2iso -bpc on the bench catalogs; 3iso -bpc beside this PCF.out on "
+                         "2048-point catalogs) and report its times")
     ap.add_argument("--iso-plain", action="store_true",
                     help="with --impl ours: also time this library's plain per-call 2iso -bpc "
                          "(DD, RR, DR) on the catalogs of --ref-gpu")
