@@ -134,15 +134,6 @@ inline GateGeom gate_geometry(float L, float dmax, int P) {
     return g;
 }
 
-__device__ __forceinline__ void gate_corner(const GateGeom &g, float x, float y, float z, float n[3]) {
-    const float c[3] = {x, y, z};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int r = min(max((int)__fdiv_rn(c[a], g.s), 0), g.P - 1);
-        n[a] = __fmul_rn((float)r, g.s);
-    }
-}
-
 // One list entry's node and image: node indices of the reference's grid (9
 // bits per axis, partitions <= 512) and the axes along which the entry is
 // joined to the anchor through its periodic image (bits 27-29).
