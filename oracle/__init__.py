@@ -12,6 +12,12 @@ checker: the shipped library (``desi_b200``) never calls into it.
   OpenMP engines (``cpp/2PCF*/{normal,BPC}``) compiled in place by
   ``oracle/Makefile``; used to pin the restatement and as the timed CPU
   baseline.
+* :func:`ref_kernels_2pt`, :func:`ref_kernels_3pt` wrap
+  ``_ref/libref_kernels_host.so``: the reference's CUDA pair and triplet
+  kernels compiled unmodified for the host (``ref_kernels_host.cpp``).
+* :func:`ref_read_catalog`, :func:`ref_save_histogram` wrap the reference's
+  reader and writers (``_ref/libref_io.so``); ``ref_cuda`` runs the
+  reference's CUDA program.
 """
 from __future__ import annotations
 
