@@ -80,8 +80,10 @@ class Request:
 
 def grid_bytes(n: int, partitions: int = 64) -> int:
     """Device bytes of one gridded catalog: raw copy, cell-ordered SoA planes,
-    pair-packed copy and integer weights, cell table and tiles (upper bound)."""
-    return n * (16 + 16 + 16) + 4 * (partitions ** 3 + 1) + 16 * n + (1 << 20)
+    pair-packed copy and integer weights, cell table and tiles (upper bound),
+    with each buffer rounded up to the library pool's size class (at most a
+    quarter more)."""
+    return (n * (16 + 16 + 16) + 4 * (partitions ** 3 + 1) + 16 * n) * 5 // 4 + (1 << 20)
 
 
 def request_work(req: Request, sizes: dict, boxes: dict) -> float:
