@@ -44,3 +44,18 @@ def test_index_by_image_matches_the_blocks():
     # (x, xyz) twice (its block 33 counts with node 2's x image)
     counts = [sum(1 for b in by[2 * i:2 * i + 2] if b >= 0) for i in range(64)]
     assert counts.count(1) == 62 and counts[2 | (7 << 3)] == 0 and counts[1 | (7 << 3)] == 2
+
+
+def test_gpu_gate_table_is_the_reference_source():
+    """kGateBlocks equals the blocks extracted from the reference's kernel
+    source (tests/golden/gate_table.json, made by
+    tests/golden/make_gate_table.py from 3isoBPC_k.cuh and 3aniBPC_k.cuh,
+    whose four kernels hold the same 64 blocks)."""
+    import json
+    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "gate_table.json")))
+    flat = []
+    for f2, f3, a2, a3, tests in ref:
+        flat += [f2, f3, a2, a3]
+        for pair, k, axes in tests:
+            flat += [pair, k] + axes + [-1] * (3 - len(axes))
+    assert _table("desi_b200/csrc/node_gates.cuh", "kGateBlocks[64]") == flat
