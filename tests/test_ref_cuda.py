@@ -50,3 +50,39 @@ def test_timer_line_parsed(tmp_path, monkeypatch):
     pts = np.zeros((4, 4), np.float32)
     r = ref_cuda.run_2iso_bpc(pts, pts, 250.0, 4, 80.0, str(tmp_path))
     assert r["ms"] == 237.5 and r["DD"].shape == (4,)
+
+
+def test_program_runners_flags_and_files(tmp_path, monkeypatch):
+    """run_2pt_bpc / run_3pt_bpc pass the reference's command line (with -bpc
+    or not, -p, extra flags) and read back the files the reference names
+    (<H><iso|ani>[_BPC]_<catalog>, create_grid.cuh:141-266)."""
+    import subprocess
+    seen = []
+
+    class P:
+        returncode = 0
+        stdout = "Spent 12.5 miliseconds to compute and save all the histograms.\n"
+        stderr = ""
+
+    def fake_run(cmd, cwd, capture_output, text, timeout):
+        seen.append(cmd)
+        res = os.path.join(os.path.dirname(cwd), "results")
+        kind, bpc = cmd[1], "-bpc" in cmd
+        sfx = ("ani" if kind.endswith("ani") else "iso") + ("_BPC" if bpc else "")
+        names = (("DDD", "RRR", "DDR", "DRR") if kind.startswith("3") else ("DD", "RR", "DR"))
+        for h in names:
+            cat = "data.dat" if h in ("DD", "DDD") else "rand.dat"
+            np.savetxt(os.path.join(res, f"{h}{sfx}_{cat}"), np.full(8, len(h), float))
+        return P()
+
+    monkeypatch.setattr(subprocess, "run", fake_run)
+    pts = np.ones((3, 4), np.float32)
+    r = ref_cuda.run_3pt_bpc("3iso", pts, pts, 60.0, 2, 20.0, 6, str(tmp_path / "a"), extra=["-exact"])
+    assert r["ms"] == 12.5 and r["DDD"].sum() == 24 and r["DRR"].size == 8
+    assert seen[-1][1:3] == ["3iso", "-bpc"] and seen[-1][-3:] == ["-p", "6", "-exact"]
+    r = ref_cuda.run_3pt_bpc("3ani", pts, pts, 60.0, 2, 20.0, 6, str(tmp_path / "b"), bpc=False)
+    assert "-bpc" not in seen[-1] and r["RRR"].size == 8
+    r = ref_cuda.run_2pt_bpc("2ani", pts, pts, 60.0, 2, 20.0, 6, str(tmp_path / "c"))
+    assert seen[-1][1:3] == ["2ani", "-bpc"] and r["DR"].sum() == 16
+    r = ref_cuda.run_2pt_bpc("2iso", pts, pts, 60.0, 2, 20.0, 6, str(tmp_path / "d"), bpc=False)
+    assert "-bpc" not in seen[-1] and r["DD"].size == 8
