@@ -429,7 +429,8 @@ def run_ours(args, rank, world, local_rank):
     if args.iso_plain:
         out["plain_2iso"] = run_plain_2iso(ctx, torch, stream)
     if not args.no_extras:
-        # the other north-star forms, measured beside the headline (not the metric)
+        # the grid build, triplets, batched and served forms, measured beside
+        # the headline (not the metric)
         out["grid_build"] = run_grid_build(ctx, torch)
         out["triplets"] = run_triplets(ctx, torch, stream)
         out["batched"] = run_batched(ctx, torch, stream)
