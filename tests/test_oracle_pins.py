@@ -380,16 +380,20 @@ def test_oracle_reference_gates_equal_reference_kernels(ani, P, dmax, bins, n):
         assert full.sum() >= got.sum()
 
 
-def test_oracle_plain_3iso_equals_reference_kernels():
-    """Without periodic boundaries the reference's 3iso kernels (XXX3iso /
-    XXY3iso, 3iso_k.cuh:8,94) have no node gates to get wrong: they equal the
-    oracle's default rule."""
+@pytest.mark.parametrize("ani", [False, True], ids=["3iso", "3ani"])
+@pytest.mark.parametrize("P,dmax,bins", [(6, 20.0, 8), (3, 25.0, 6), (10, 12.0, 5)])
+def test_oracle_plain_3pt_equals_reference_kernels(ani, P, dmax, bins):
+    """Without periodic boundaries the reference's 3-point kernels (XXX3iso /
+    XXY3iso, 3iso_k.cuh:8,94; XXX3ani / XXY3ani, 3ani_k.cuh:8,109) have no
+    node gates to get wrong: on any node grid they equal the oracle's default
+    rule."""
     ref = _host_kernels()
-    D, R = _lattice(800, 5)
-    L, bins, dmax = 60.0, 8, 20.0
-    h = ref(D, R, ani=False, bpc=False, box=L, bins=bins, dmax=dmax, partitions=6)
+    D, R = _lattice(800, 5 + P)
+    L = 60.0
+    h = ref(D, R, ani=ani, bpc=False, box=L, bins=bins, dmax=dmax, partitions=P)
+    f = oracle.triplets_ani if ani else oracle.triplets_iso
     for name, x, y in (("DDD", D, None), ("RRR", R, None), ("DDR", D, R), ("DRR", R, D)):
-        assert np.array_equal(oracle.triplets_iso(x, y, box=L, bins=bins, dmax=dmax), h[name]), name
+        assert np.array_equal(f(x, y, box=L, bins=bins, dmax=dmax), h[name]), name
 
 
 @pytest.mark.parametrize("bpc", [False, True], ids=["plain", "periodic"])
