@@ -60,3 +60,39 @@ def test_served_leg_interleaves_and_keeps_the_best(monkeypatch):
     assert abs(out["served_vs_plain"]["pairs_per_s"] - (100 / 2.0) / (100 / 2.2)) < 1e-12
     assert abs(out["capacity_req_per_s"] - 10 / 2.0) < 1e-12
     assert abs(out["rate_hz"] - 0.7 * 10 / 2.0) < 1e-12
+
+
+def test_served_leg_runs_in_a_fresh_process_or_falls_back(monkeypatch):
+    """run_served_isolated reads the child's JSON report; when the child
+    fails it runs the leg in the bench process and says why."""
+    import subprocess
+
+    import bench
+
+    class Done:
+        returncode = 0
+        stdout = 'noise\n{"served_vs_plain": {"pairs_per_s": 1.09}}\n'
+        stderr = ""
+
+    seen = []
+
+    def ok_run(cmd, capture_output, text, timeout, cwd):
+        seen.append(cmd)
+        return Done()
+
+    monkeypatch.setattr(subprocess, "run", ok_run)
+    rep = bench.run_served_isolated(12)
+    assert rep["served_vs_plain"]["pairs_per_s"] == 1.09
+    assert rep["process"].startswith("fresh process")
+    assert seen[0][0] == sys.executable and "run_served(12)" in seen[0][2]
+
+    class Failed(Done):
+        returncode = 1
+        stdout = ""
+        stderr = "no device"
+
+    monkeypatch.setattr(subprocess, "run", lambda *a, **k: Failed())
+    monkeypatch.setattr(bench, "run_served", lambda n: {"served_vs_plain": {"pairs_per_s": 0.9}})
+    rep = bench.run_served_isolated(12)
+    assert rep["served_vs_plain"]["pairs_per_s"] == 0.9
+    assert "child exited 1" in rep["process"] and "no device" in rep["process"]
